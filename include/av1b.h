@@ -1,0 +1,247 @@
+/*
+ * av1b.h - the C ABI of the B200 AV1 reconstruction backend.
+ *
+ * The reference library (trprkkk/AV1onGPU) exposes its reconstruction path as
+ * the C++ class av1gpu::Decoder (include/av1gpu/av1gpu.hpp:615-787) fed with
+ * av1gpu::FrameSyntax (av1gpu.hpp:476-537). It ships no foreign-function
+ * binding. This header is the binding a non-C++ caller (ctypes, cgo, JNI,
+ * N-API) would use: every entry point maps one Decoder method, takes plain
+ * pointers and sizes, never throws and returns AV1B_OK or a negative code.
+ * The C++ class in include/av1gpu/av1gpu.hpp is implemented on top of it in
+ * the same shared library.
+ *
+ * FrameSyntax crosses the boundary as av1b_frame_syntax: the scalar fields of
+ * the reference struct plus (pointer, count) pairs for each of its vectors.
+ * The per-block vectors (BlockSyntax::transforms, BlockSyntax::obmc) are
+ * flattened into frame-wide arrays addressed by (first, count) in each block,
+ * which is the layout the device upload wants anyway.
+ *
+ * Thread safety: one decoder is driven by one thread at a time; different
+ * decoders may be used from different threads.
+ */
+#ifndef AV1B_H
+#define AV1B_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AV1B_OK 0
+#define AV1B_ERR_ARG (-1)        /* a null pointer, a bad size or slot     */
+#define AV1B_ERR_CUDA (-2)       /* a CUDA call failed                     */
+#define AV1B_ERR_NOMEM (-3)      /* the HBM budget or the slot pool is out */
+#define AV1B_ERR_SYNTAX (-4)     /* the frame syntax is inconsistent        */
+#define AV1B_ERR_TIMEOUT (-5)    /* a device-side dependency wait gave up   */
+#define AV1B_ERR_UNSUPPORTED (-6)
+#define AV1B_ERR_NO_DEVICE (-7)  /* no CUDA device: there is no CPU fallback */
+
+/* TransformBlock (av1gpu.hpp:187-208). */
+typedef struct av1b_transform {
+  int32_t x, y, w, h;
+  int32_t coef_offset;
+  int32_t eob;
+  int32_t tx_type;
+  int32_t level_offset, qindex;
+  int32_t dc_step, ac_step, denominator, qm_off;
+} av1b_transform;
+
+/* ObmcCandidate (av1gpu.hpp:215-225). */
+typedef struct av1b_obmc {
+  int32_t pass, x, y, w, h;
+  int32_t mv[2];
+  int32_t filter, filter_v;
+  int32_t ref;
+} av1b_obmc;
+
+/* BlockSyntax (av1gpu.hpp:229-342), booleans as 0/1 ints, the two vectors as
+ * ranges of the frame-wide transform and OBMC arrays. */
+typedef struct av1b_block {
+  int32_t x, y, w, h, plane, bit_depth;
+  int32_t is_intra, intrabc;
+  int32_t mode;
+  int32_t have_left, have_above, have_above_right, have_below_left;
+  int32_t angle_delta, filter_type;
+  int32_t use_filter_intra, filter_intra_mode;
+  int32_t cfl_alpha;
+  int32_t lossless;
+  int32_t use_palette, palette_size, palette[8], palette_off, palette_stride;
+  int32_t ref[2];
+  int32_t mv[2][2];
+  int32_t filter, filter_v;
+  int32_t motion_mode, compound;
+  int32_t blend[2];
+  int32_t wedge_index, mask_sign;
+  int32_t interintra, interintra_mode, interintra_wedge;
+  int32_t warp[2];
+  int32_t warp_params[2][6];
+  int32_t mask_warp[2];
+  int32_t residual_provided;
+  int32_t tx_first, tx_count;     /* into av1b_frame_syntax::transforms */
+  int32_t obmc_first, obmc_count; /* into av1b_frame_syntax::obmc       */
+} av1b_block;
+
+/* DeblockEdge (av1gpu.hpp:347-358). */
+typedef struct av1b_deblock_edge {
+  int32_t plane, x, y, vertical, length, level, filter_size;
+} av1b_deblock_edge;
+
+/* CdefBlock (av1gpu.hpp:361-369). */
+typedef struct av1b_cdef_block {
+  int32_t plane, x, y, pri_strength, sec_strength, damping, dir;
+} av1b_cdef_block;
+
+/* RestorationUnit (av1gpu.hpp:418-426). */
+typedef struct av1b_restoration_unit {
+  int32_t type;
+  int32_t wiener[2][3];
+  int32_t sgr_set;
+  int32_t sgr_xqd[2];
+} av1b_restoration_unit;
+
+/* FilmGrainParams (av1gpu.hpp:434-468). */
+typedef struct av1b_film_grain {
+  int32_t apply, seed;
+  int32_t num_y_points, point_y_value[16], point_y_scaling[16];
+  int32_t chroma_scaling_from_luma;
+  int32_t num_cb_points, point_cb_value[16], point_cb_scaling[16];
+  int32_t num_cr_points, point_cr_value[16], point_cr_scaling[16];
+  int32_t grain_scaling_minus_8;
+  int32_t ar_coeff_lag;
+  int32_t ar_coeffs_y[24], ar_coeffs_cb[25], ar_coeffs_cr[25];
+  int32_t ar_coeff_shift_minus_6, grain_scale_shift;
+  int32_t cb_mult, cb_luma_mult, cb_offset;
+  int32_t cr_mult, cr_luma_mult, cr_offset;
+  int32_t overlap_flag, clip_to_restricted_range;
+} av1b_film_grain;
+
+/* FrameSyntax (av1gpu.hpp:476-537): the scalars and one (pointer, count) per
+ * vector. Nothing is retained after the call that takes it returns. */
+typedef struct av1b_frame_syntax {
+  int32_t width, coded_width, height, bit_depth, ss_x, ss_y;
+  int32_t base_q_idx, sharpness, enable_intra_edge_filter;
+  int32_t color_matrix, color_range;
+  int32_t reference_width[7], reference_height[7];
+  int32_t restoration_type[3], restoration_unit_log2[3], restoration_unit_cols[3];
+  av1b_film_grain grain;
+
+  const int32_t* reference_slots;          size_t n_reference_slots;
+  const av1b_block* blocks;                size_t n_blocks;
+  const av1b_transform* transforms;        size_t n_transforms;
+  const av1b_obmc* obmc;                   size_t n_obmc;
+  const int32_t* coefficients;             size_t n_coefficients;
+  const int32_t* residual;                 size_t n_residual;
+  const int16_t* levels;                   size_t n_levels;
+  const uint8_t* qm_pool;                  size_t n_qm_pool;
+  const uint8_t* palette_map;              size_t n_palette_map;
+  const av1b_deblock_edge* deblock;        size_t n_deblock;
+  const av1b_cdef_block* cdef;             size_t n_cdef;
+  const av1b_restoration_unit* restoration[3];
+  size_t n_restoration[3];
+} av1b_frame_syntax;
+
+/* Frame (av1gpu.hpp:77-109) as three caller-owned planes of uint16 samples.
+ * `stride` is in samples. Plane sizes follow Frame::plane_width/height. */
+typedef struct av1b_planes {
+  uint16_t* plane[3];
+  int32_t stride[3];
+} av1b_planes;
+
+/* DecodeStats (av1gpu.hpp:544-552). */
+typedef struct av1b_stats {
+  int32_t blocks, waves, kernel_launches;
+  double reconstruct_ms, filter_ms, readback_ms, total_ms;
+} av1b_stats;
+
+typedef struct av1b_decoder av1b_decoder;
+
+/* --- serialized syntax (a flat byte image of av1b_frame_syntax) ------------
+ * A test fixture, a file, or a process boundary carries a frame as one byte
+ * buffer. av1b_syntax_view points a view at such a buffer without copying. The
+ * buffer must stay alive and unmodified while the view is used. */
+int av1b_syntax_view(const uint8_t* blob, size_t len, av1b_frame_syntax* out);
+
+/* --- decoder lifetime: Decoder::create (engine.cpp:1509-1558) -------------- */
+/* `device` is the CUDA ordinal. `hbm_budget_bytes` caps what the decoder may
+ * allocate (0: no cap). A missing device is an error (AV1B_ERR_NO_DEVICE):
+ * there is no CPU path in this library. */
+int av1b_decoder_create(int device, size_t hbm_budget_bytes, av1b_decoder** out);
+int av1b_decoder_destroy(av1b_decoder* dec);
+/* Decoder::reset (engine.cpp:65-71): drops every slot. */
+int av1b_decoder_reset(av1b_decoder* dec);
+
+/* --- decode: Decoder::decode_reference / decode (av1gpu.hpp:635-636, 733) --
+ * Decodes `syntax` and keeps the picture resident in a reference slot when
+ * `keep_reference` is non-zero (its id goes to *out_slot, else -1). `out` may be
+ * null (no read back); otherwise the display picture, film grain included, is
+ * copied into the caller's planes. `error` (nullable, `error_len` bytes)
+ * receives a message on failure. */
+int av1b_decode(av1b_decoder* dec, const av1b_frame_syntax* syntax, int keep_reference,
+                const av1b_planes* out, int* out_slot, char* error, size_t error_len);
+
+/* Decoder::reserve_reference / decode_reference_reserved (av1gpu.hpp:645-661). */
+int av1b_reserve_reference(av1b_decoder* dec, int* out_slot);
+int av1b_decode_reserved(av1b_decoder* dec, const av1b_frame_syntax* syntax, int slot,
+                         const av1b_planes* out, char* error, size_t error_len);
+
+/* Decoder::release_reference (av1gpu.hpp:736). */
+int av1b_release_reference(av1b_decoder* dec, int slot);
+
+/* Decoder::to_nv12 (av1gpu.hpp:745-746): packs `slot` on the device into
+ * `pitch`-byte rows and copies the bytes to `dst` (host, `dst_len` bytes).
+ * The slot of the frame decoded last packs the picture after film grain; an
+ * older slot packs its stored picture, which is the one before film grain
+ * (the reference CPU backend's gather(), cpu_backend.cpp:557-570). */
+int av1b_to_nv12(av1b_decoder* dec, int slot, size_t pitch, uint8_t* dst, size_t dst_len);
+/* Same, but `dst` is device memory: the zero-copy end of the path. */
+int av1b_to_nv12_device(av1b_decoder* dec, int slot, size_t pitch, void* dst_device,
+                        size_t dst_len);
+/* The byte count to_nv12 produces (factory.cpp:236-244's nv12_buffer_size):
+ * 0 for a frame that is not 4:2:0, an odd pitch or a pitch below a chroma row. */
+size_t av1b_nv12_size(int width, int height, int ss_x, int ss_y, size_t pitch);
+
+/* Decoder::to_rgb (av1gpu.hpp:739-740): RGB24, width*height*3 bytes. */
+int av1b_to_rgb(av1b_decoder* dec, int slot, int matrix, int range, uint8_t* dst,
+                size_t dst_len);
+
+/* Decoder::stats (av1gpu.hpp:630). */
+int av1b_get_stats(av1b_decoder* dec, av1b_stats* out);
+
+/* The device status word: non-zero after a device-side wait gave up or a
+ * bounds check refused an access. Reading clears it. */
+int av1b_poll_status(av1b_decoder* dec, int* status);
+
+/* Device pointer and layout of a slot's planes (for callers that hand the
+ * picture on without a host copy). */
+int av1b_slot_planes_device(av1b_decoder* dec, int slot, uint16_t* plane_ptr[3],
+                            int32_t stride[3]);
+
+/* CUDA stream the decoder runs on (a cudaStream_t), so a caller can order its
+ * own work after a decode without a host synchronisation. */
+void* av1b_decoder_stream(av1b_decoder* dec);
+
+/* --- synthetic input -------------------------------------------------------
+ * The seeded synthetic FrameSyntax the benchmarks and tests decode. `config`
+ * selects a workload (1..3, see av1ongpu_b200/csrc/synth.cpp), `scale` divides
+ * its picture size (1 = full size). The frame is returned serialized; its
+ * reference_slots hold frame *distances* (1 = the previous frame), which the
+ * caller rewrites into its own slot ids with av1b_blob_set_refs. The buffer is
+ * owned by the library: release it with av1b_blob_free. */
+int av1b_synth_frame(int config, int scale, uint64_t seed, int frame_index,
+                     uint8_t** blob, size_t* len);
+int av1b_synth_frame_ex(int width, int height, int coded_width, int bit_depth, int sb_size,
+                        int tools, uint64_t seed, int frame_index, int key_interval,
+                        uint8_t** blob, size_t* len);
+void av1b_blob_free(uint8_t* blob);
+/* Rewrites the reference slot list of a serialized frame in place. */
+int av1b_blob_set_refs(uint8_t* blob, size_t len, const int32_t* slots, int n);
+/* Reads the reference slot list (distances for a synthetic frame). */
+int av1b_blob_get_refs(const uint8_t* blob, size_t len, int32_t* slots, int max_n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AV1B_H */

@@ -1,0 +1,180 @@
+/*
+ * ref_shim.cpp - a C entry surface over the reference's own CPU backend.
+ *
+ * TEST INFRASTRUCTURE ONLY. This file is compiled together with the
+ * reference's sources (src/core/*.cpp, src/backends/cpu/cpu_backend.cpp) by
+ * oracle/Makefile into oracle/_ref/libav1ref.so, with the reference namespace
+ * renamed to av1ref so it can share a process with this repository's library.
+ * Only tests/, the smoke check and bench.py's CPU baseline load it; nothing
+ * in the product links it.
+ *
+ * Every call goes through the reference's public API: av1gpu::Decoder
+ * (include/av1gpu/av1gpu.hpp:615-787) created with BackendKind::Cpu, which is
+ * EngineDecoder over CpuBackend (engine.cpp:1509-1558, cpu_backend.cpp:645).
+ * Frames arrive as the serialized av1b_frame_syntax blobs this repository's
+ * tests and benchmark use, and are rebuilt into the reference's FrameSyntax
+ * field by field (av1ongpu_b200/csrc/flat_syntax.hpp).
+ */
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#if defined(_OPENMP)
+#include <omp.h>
+#endif
+
+#include "av1gpu/av1gpu.hpp"
+#include "av1gpu_kernels.h"
+#include "flat_syntax.hpp"
+
+namespace {
+
+struct RefDecoder {
+  std::unique_ptr<av1gpu::Decoder> dec;
+  av1gpu::Frame out;
+  std::string error;
+};
+
+}  // namespace
+
+extern "C" {
+
+__attribute__((visibility("default"))) void av1ref_set_threads(int n) {
+#if defined(_OPENMP)
+  if (n > 0) omp_set_num_threads(n);
+#else
+  (void)n;
+#endif
+}
+
+__attribute__((visibility("default"))) int av1ref_max_threads(void) {
+#if defined(_OPENMP)
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+__attribute__((visibility("default"))) void* av1ref_create(void) {
+  av1gpu::BackendOptions opt;
+  opt.kind = av1gpu::BackendKind::Cpu;
+  opt.allow_cpu_fallback = true;
+  std::string err;
+  auto* r = new RefDecoder;
+  r->dec = av1gpu::Decoder::create(opt, &err);
+  if (!r->dec) {
+    delete r;
+    return nullptr;
+  }
+  return r;
+}
+
+__attribute__((visibility("default"))) void av1ref_destroy(void* h) {
+  delete static_cast<RefDecoder*>(h);
+}
+
+/* Decodes one serialized frame. keep != 0: Decoder::decode_reference, the
+ * return value is the slot; keep == 0: Decoder::decode, the return value is -1
+ * on success. -2 means failure (av1ref_error has the message). When `out` is
+ * not null the display planes are packed into it, plane after plane, each
+ * plane_width * plane_height uint16 samples; `out_len` is its size in
+ * samples. */
+__attribute__((visibility("default"))) int av1ref_decode(void* h, const uint8_t* blob,
+                                                         size_t len, int keep, uint16_t* out,
+                                                         size_t out_len) {
+  RefDecoder* r = static_cast<RefDecoder*>(h);
+  av1b_frame_syntax view;
+  if (!r || !av1b::view_blob(blob, len, &view)) return -2;
+  av1gpu::FrameSyntax syntax;
+  av1b::cpp_from_view(view, &syntax);
+  int slot = -1;
+  r->error.clear();
+  if (keep) {
+    slot = r->dec->decode_reference(syntax, &r->out, &r->error);
+    if (slot < 0) return -2;
+  } else {
+    if (!r->dec->decode(syntax, &r->out, &r->error)) return -2;
+  }
+  if (out) {
+    size_t pos = 0;
+    for (int p = 0; p < 3; ++p) {
+      const int pw = r->out.plane_width(p), ph = r->out.plane_height(p);
+      if (pos + static_cast<size_t>(pw) * ph > out_len) return -2;
+      for (int y = 0; y < ph; ++y) {
+        std::memcpy(out + pos, r->out.plane(p) + static_cast<size_t>(y) * r->out.stride[p],
+                    sizeof(uint16_t) * pw);
+        pos += pw;
+      }
+    }
+  }
+  return slot;
+}
+
+__attribute__((visibility("default"))) const char* av1ref_error(void* h) {
+  return h ? static_cast<RefDecoder*>(h)->error.c_str() : "";
+}
+
+__attribute__((visibility("default"))) void av1ref_release(void* h, int slot) {
+  if (h) static_cast<RefDecoder*>(h)->dec->release_reference(slot);
+}
+
+__attribute__((visibility("default"))) int av1ref_to_nv12(void* h, int slot, size_t pitch,
+                                                          uint8_t* out, size_t out_len) {
+  RefDecoder* r = static_cast<RefDecoder*>(h);
+  std::vector<uint8_t> bytes;
+  if (!r || !r->dec->to_nv12(slot, pitch, &bytes, &r->error)) return -2;
+  if (bytes.size() > out_len) return -2;
+  std::memcpy(out, bytes.data(), bytes.size());
+  return static_cast<int>(bytes.size());
+}
+
+__attribute__((visibility("default"))) int av1ref_to_rgb(void* h, int slot, int matrix,
+                                                         int range, uint8_t* out,
+                                                         size_t out_len) {
+  RefDecoder* r = static_cast<RefDecoder*>(h);
+  std::vector<uint8_t> bytes;
+  if (!r || !r->dec->to_rgb(slot, static_cast<av1gpu::ColorMatrix>(matrix),
+                            static_cast<av1gpu::ColorRange>(range), &bytes, &r->error))
+    return -2;
+  if (bytes.size() > out_len) return -2;
+  std::memcpy(out, bytes.data(), bytes.size());
+  return static_cast<int>(bytes.size());
+}
+
+/* DecodeStats of the last decode: reconstruct, filter, total milliseconds. */
+__attribute__((visibility("default"))) void av1ref_stats(void* h, double* ms3, int* waves) {
+  const av1gpu::DecodeStats& s = static_cast<RefDecoder*>(h)->dec->stats();
+  ms3[0] = s.reconstruct_ms;
+  ms3[1] = s.filter_ms;
+  ms3[2] = s.total_ms;
+  *waves = s.waves;
+}
+
+/* One 2-D inverse transform plus residual add, through the reference's
+ * av1g_itx_row / av1g_itx_col_add (av1gpu_kernels.h:869-930), the way the CPU
+ * backend runs a job (cpu_backend.cpp:319-325). `dst` is w*h samples, row
+ * major, updated in place. */
+__attribute__((visibility("default"))) void av1ref_itx(int w, int h, int tx_type, int lossless,
+                                                       int row_shift, int bitdepth,
+                                                       const int32_t* coef, uint16_t* dst) {
+  Av1gItxJob job;
+  std::memset(&job, 0, sizeof(job));
+  job.coef_off = 0;
+  job.tmp_off = 0;
+  job.dst_off = 0;
+  job.dst_stride = w;
+  job.w = w;
+  job.h = h;
+  job.tx_type = tx_type;
+  job.eob = 1;
+  job.row_shift = row_shift;
+  job.lossless = lossless;
+  job.bitdepth = bitdepth;
+  std::vector<int> tmp(static_cast<size_t>(w) * h + 64, 0);
+  const int maxv = (1 << bitdepth) - 1;
+  for (int y = 0; y < h; ++y) av1g_itx_row(&job, coef, tmp.data(), y);
+  for (int x = 0; x < w; ++x) av1g_itx_col_add(&job, tmp.data(), dst, x, maxv);
+}
+
+}  // extern "C"
