@@ -1,0 +1,290 @@
+"""av1ongpu_b200: the B200 AV1 reconstruction backend, from Python.
+
+A thin ctypes layer over the C ABI of libav1b.so (include/av1b.h). It mirrors
+the reference library's av1gpu::Decoder (include/av1gpu/av1gpu.hpp:615-787 of
+trprkkk/AV1onGPU): decode / decode_reference with device-resident reference
+slots, release_reference, to_nv12, to_rgb and stats. Frames are passed as
+serialized FrameSyntax blobs (`Blob`), which the seeded workload generator
+(`synth_frame`) produces.
+
+There is no CPU path: without the compiled library, or without a CUDA device,
+the calls raise instead of computing anything elsewhere.
+"""
+import ctypes
+import os
+import struct
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, 'libav1b.so')
+
+AV1B_OK = 0
+ERRORS = {
+    -1: 'bad argument', -2: 'CUDA error', -3: 'out of memory or slots', -4: 'invalid syntax',
+    -5: 'device dependency wait timed out', -6: 'unsupported', -7: 'no CUDA device',
+}
+
+# workload tool bits (csrc/synth.cpp)
+TOOL_TX64, TOOL_ALLTYPES, TOOL_CFL, TOOL_PALETTE = 1, 2, 4, 8
+TOOL_FILTER_INTRA, TOOL_COMPOUND, TOOL_MASKS, TOOL_OBMC = 16, 32, 64, 128
+TOOL_WARP, TOOL_LR, TOOL_GRAIN, TOOL_INTERINTRA = 256, 512, 1024, 2048
+TOOL_INTRABC, TOOL_LOSSLESS, TOOL_RESIDUAL, TOOL_EDGE_VARIANTS = 4096, 8192, 16384, 32768
+TOOL_NO_DEBLOCK, TOOL_NO_CDEF = 1 << 16, 1 << 17
+TOOLS_ALL = (TOOL_TX64 | TOOL_ALLTYPES | TOOL_CFL | TOOL_PALETTE | TOOL_FILTER_INTRA |
+             TOOL_COMPOUND | TOOL_MASKS | TOOL_OBMC | TOOL_WARP | TOOL_LR | TOOL_GRAIN |
+             TOOL_EDGE_VARIANTS)
+
+
+class Av1bError(RuntimeError):
+    def __init__(self, code, msg=''):
+        super().__init__('%s (%d)%s' % (ERRORS.get(code, 'error'), code, ': ' + msg if msg else ''))
+        self.code = code
+
+
+class _Planes(ctypes.Structure):
+    _fields_ = [('plane', ctypes.c_void_p * 3), ('stride', ctypes.c_int32 * 3)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [('blocks', ctypes.c_int32), ('waves', ctypes.c_int32),
+                ('kernel_launches', ctypes.c_int32), ('reconstruct_ms', ctypes.c_double),
+                ('filter_ms', ctypes.c_double), ('readback_ms', ctypes.c_double),
+                ('total_ms', ctypes.c_double)]
+
+
+_lib = None
+
+# name: (restype, argtypes)
+_SIGNATURES = {
+    'av1b_syntax_view': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]),
+    'av1b_decoder_create': (ctypes.c_int, [ctypes.c_int, ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p)]),
+    'av1b_decoder_destroy': (ctypes.c_int, [ctypes.c_void_p]),
+    'av1b_decoder_reset': (ctypes.c_int, [ctypes.c_void_p]),
+    'av1b_decode': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                   ctypes.POINTER(ctypes.c_int), ctypes.c_char_p, ctypes.c_size_t]),
+    'av1b_decode_blob': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int,
+                                        ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.c_char_p,
+                                        ctypes.c_size_t]),
+    'av1b_reserve_reference': (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
+    'av1b_decode_reserved': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                            ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]),
+    'av1b_release_reference': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    'av1b_to_nv12': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t, ctypes.c_void_p,
+                                    ctypes.c_size_t]),
+    'av1b_to_nv12_device': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t,
+                                           ctypes.c_void_p, ctypes.c_size_t]),
+    'av1b_nv12_size': (ctypes.c_size_t, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_size_t]),
+    'av1b_to_rgb': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                   ctypes.c_void_p, ctypes.c_size_t]),
+    'av1b_get_stats': (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Stats)]),
+    'av1b_poll_status': (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
+    'av1b_slot_planes_device': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                               ctypes.c_void_p]),
+    'av1b_last_error': (ctypes.c_char_p, [ctypes.c_void_p]),
+    'av1b_decoder_stream': (ctypes.c_void_p, [ctypes.c_void_p]),
+    'av1b_synth_frame': (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_uint64, ctypes.c_int,
+                                        ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_size_t)]),
+    'av1b_synth_frame_ex': (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                           ctypes.c_int, ctypes.c_int, ctypes.c_uint64, ctypes.c_int,
+                                           ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
+                                           ctypes.POINTER(ctypes.c_size_t)]),
+    'av1b_blob_free': (None, [ctypes.c_void_p]),
+    'av1b_blob_set_refs': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t,
+                                          ctypes.POINTER(ctypes.c_int32), ctypes.c_int]),
+    'av1b_blob_get_refs': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t,
+                                          ctypes.POINTER(ctypes.c_int32), ctypes.c_int]),
+}
+
+
+def lib():
+    """Loads libav1b.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError('libav1b.so is not built: run python -m av1ongpu_b200.build')
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def exported_symbols():
+    return list(_SIGNATURES)
+
+
+# ---- serialized frames -----------------------------------------------------------------------
+_BLOB_HEADER = 48  # magic, version, reserved, n_refs, ref_slots[8]
+
+
+class Blob:
+    """A serialized FrameSyntax, 64-byte aligned, owned by the library or by numpy."""
+
+    def __init__(self, ptr, size, owned_by_lib):
+        self.ptr = ptr
+        self.size = size
+        self._lib_owned = owned_by_lib
+        self._keep = None
+
+    @classmethod
+    def from_bytes(cls, data):
+        arr = np.zeros(len(data) + 64, dtype=np.uint8)
+        off = (-arr.ctypes.data) % 64
+        view = arr[off:off + len(data)]
+        view[:] = np.frombuffer(data, dtype=np.uint8)
+        b = cls(view.ctypes.data, len(data), False)
+        b._keep = arr
+        return b
+
+    def to_bytes(self):
+        return ctypes.string_at(self.ptr, self.size)
+
+    def __del__(self):
+        if self._lib_owned and self.ptr and _lib is not None:
+            _lib.av1b_blob_free(ctypes.c_void_p(self.ptr))
+            self.ptr = None
+
+    @property
+    def header(self):
+        """(width, coded_width, height, bit_depth, ss_x, ss_y)."""
+        return struct.unpack_from('<6i', ctypes.string_at(self.ptr + _BLOB_HEADER, 24))
+
+    def get_refs(self):
+        buf = (ctypes.c_int32 * 8)()
+        n = lib().av1b_blob_get_refs(self.ptr, self.size, buf, 8)
+        if n < 0:
+            raise Av1bError(n, 'malformed blob')
+        return list(buf[:n])
+
+    def set_refs(self, slots):
+        buf = (ctypes.c_int32 * 8)(*slots)
+        rc = lib().av1b_blob_set_refs(self.ptr, self.size, buf, len(slots))
+        if rc:
+            raise Av1bError(rc, 'malformed blob')
+
+
+def synth_frame(config, scale, seed, index):
+    """One frame of workload `config` (1..3) at 1/scale size."""
+    p = ctypes.c_void_p()
+    n = ctypes.c_size_t()
+    rc = lib().av1b_synth_frame(config, scale, seed, index, ctypes.byref(p), ctypes.byref(n))
+    if rc:
+        raise Av1bError(rc, 'synth_frame')
+    return Blob(p.value, n.value, True)
+
+
+def synth_frame_ex(width, height, coded_width, bit_depth, sb_size, tools, seed, index,
+                   key_interval=0):
+    p = ctypes.c_void_p()
+    n = ctypes.c_size_t()
+    rc = lib().av1b_synth_frame_ex(width, height, coded_width, bit_depth, sb_size, tools, seed,
+                                   index, key_interval, ctypes.byref(p), ctypes.byref(n))
+    if rc:
+        raise Av1bError(rc, 'synth_frame_ex')
+    return Blob(p.value, n.value, True)
+
+
+def plane_shapes(width, height, ss_x, ss_y):
+    cw, ch = (width + ss_x) >> ss_x, (height + ss_y) >> ss_y
+    return [(height, width), (ch, cw), (ch, cw)]
+
+
+def nv12_size(width, height, ss_x, ss_y, pitch):
+    return lib().av1b_nv12_size(width, height, ss_x, ss_y, pitch)
+
+
+# ---- the decoder -----------------------------------------------------------------------------
+class Decoder:
+    """av1gpu::Decoder on one CUDA device."""
+
+    def __init__(self, device=0, hbm_budget=0):
+        h = ctypes.c_void_p()
+        rc = lib().av1b_decoder_create(device, hbm_budget, ctypes.byref(h))
+        if rc:
+            raise Av1bError(rc, 'av1b_decoder_create')
+        self.h = h
+        self._err = ctypes.create_string_buffer(512)
+
+    def close(self):
+        if getattr(self, 'h', None):
+            lib().av1b_decoder_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc, what):
+        if rc:
+            msg = lib().av1b_last_error(self.h) or b''
+            raise Av1bError(rc, '%s: %s' % (what, msg.decode(errors='replace')))
+
+    def decode(self, blob, keep=True, read_back=True):
+        """Decodes a serialized frame. Returns (slot, [Y, U, V] uint16 arrays or None)."""
+        w, _cw, h, _bd, sx, sy = blob.header
+        planes = None
+        pl = None
+        if read_back:
+            planes = [np.empty(s, dtype=np.uint16) for s in plane_shapes(w, h, sx, sy)]
+            pl = _Planes()
+            for i, a in enumerate(planes):
+                pl.plane[i] = a.ctypes.data
+                pl.stride[i] = a.shape[1]
+        slot = ctypes.c_int(-1)
+        rc = lib().av1b_decode_blob(self.h, blob.ptr, blob.size, 1 if keep else 0,
+                                    ctypes.byref(pl) if pl is not None else None, ctypes.byref(slot),
+                                    self._err, len(self._err))
+        self._check(rc, 'decode')
+        return slot.value, planes
+
+    def reserve_reference(self):
+        s = ctypes.c_int(-1)
+        self._check(lib().av1b_reserve_reference(self.h, ctypes.byref(s)), 'reserve_reference')
+        return s.value
+
+    def release_reference(self, slot):
+        self._check(lib().av1b_release_reference(self.h, slot), 'release_reference')
+
+    def reset(self):
+        self._check(lib().av1b_decoder_reset(self.h), 'reset')
+
+    def to_nv12(self, slot, pitch, width, height):
+        n = nv12_size(width, height, 1, 1, pitch)
+        if n == 0:
+            raise Av1bError(-1, 'NV12 needs a 4:2:0 frame and an even pitch at least as wide')
+        out = np.empty(n, dtype=np.uint8)
+        self._check(lib().av1b_to_nv12(self.h, slot, pitch, out.ctypes.data, n), 'to_nv12')
+        return out
+
+    def to_rgb(self, slot, matrix, rng, width, height):
+        out = np.empty(width * height * 3, dtype=np.uint8)
+        self._check(lib().av1b_to_rgb(self.h, slot, matrix, rng, out.ctypes.data, out.size), 'to_rgb')
+        return out
+
+    def stats(self):
+        s = Stats()
+        self._check(lib().av1b_get_stats(self.h, ctypes.byref(s)), 'stats')
+        return s
+
+
+def cuda_available():
+    """True when a CUDA device is visible (without initialising torch)."""
+    try:
+        rt = ctypes.CDLL('libcudart.so')
+    except OSError:
+        try:
+            import glob
+            cands = glob.glob('/usr/local/cuda/lib64/libcudart.so*')
+            rt = ctypes.CDLL(cands[0]) if cands else None
+        except OSError:
+            rt = None
+    if rt is None:
+        return False
+    n = ctypes.c_int(0)
+    return rt.cudaGetDeviceCount(ctypes.byref(n)) == 0 and n.value > 0

@@ -1,0 +1,1225 @@
+/*
+ * decoder.cu - the host engine behind the C ABI (include/av1b.h).
+ *
+ * It replaces the reference's EngineDecoder + CudaBackend pair
+ * (src/core/engine.cpp, src/backends/cuda/cuda_backend.cpp) with one object:
+ *
+ *   plan    FrameSyntax -> compact device records, O(blocks), no wavefront:
+ *           BlockRec per block, TxRec per coded transform, OBMC strips, warp
+ *           models, edge / CDEF / restoration records, grain constants; every
+ *           offset is validated here so no kernel can address outside its
+ *           buffers;
+ *   upload  one pinned staging arena -> one device arena per frame, plus the
+ *           coefficient and residual pools;
+ *   run     the frame step on one CUDA stream: reconstruction (phase A, then
+ *           the dependency-scheduled phase B), deblock V then H, CDEF,
+ *           superres, loop restoration, reference store, film grain;
+ *   output  the display picture back to the caller, or NV12 / RGB packed on
+ *           the device.
+ *
+ * Slot semantics follow the reference CPU backend (cpu_backend.cpp:93-553):
+ * a slot holds the picture before film grain; the frame decoded last is also
+ * kept after film grain, and that is what the output calls of its slot read.
+ */
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/av1b.h"
+#include "flat_syntax.hpp"
+#include "dev_inter.cuh"
+#include "dev_itx.cuh"
+#include "kernels.h"
+#include "plan_host.h"
+
+namespace av1b {
+namespace {
+
+constexpr int kSlots = 32;       /* reference slots, as the reference's pools */
+constexpr int kPadLuma = 128;    /* right/bottom border for block overhang */
+
+inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+};
+
+struct HostBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+};
+
+}  // namespace
+}  // namespace av1b
+
+using namespace av1b;
+
+struct av1b_decoder {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int n_sm = 148;
+  size_t budget = 0, allocated = 0;
+  std::mutex mu;
+
+  /* geometry of the pictures currently allocated */
+  bool have_geom = false;
+  int width = 0, height = 0, coded_width = 0, bit_depth = 8, ss_x = 1, ss_y = 1;
+  Layout L{};
+
+  /* pictures */
+  DevBuf cur, snap, lr_pre, lr_pre_up, lr_cdef, disp;
+  bool disp_is_cur = true;
+  DevBuf slot_buf[kSlots];
+  bool slot_used[kSlots] = {false};
+  bool slot_valid[kSlots] = {false};
+  int slot_width[kSlots] = {0}, slot_height[kSlots] = {0}, slot_bd[kSlots] = {0};
+  DevBuf slot_ptr_dev;
+  int last_slot = -1;
+  bool have_last = false;
+
+  /* per-frame buffers */
+  HostBuf stage;
+  DevBuf arena, coef, residual, owner[3], done, status_q, nv12, rgb;
+  unsigned epoch = 0;
+
+  /* film grain */
+  DevBuf grain_state, orbit, pos;
+  bool grain_tables = false;
+
+  av1b_stats stats{};
+  std::string err;
+};
+
+namespace av1b {
+namespace {
+
+int fail(av1b_decoder* d, int code, const std::string& msg) {
+  d->err = msg;
+  return code;
+}
+
+int cuda_fail(av1b_decoder* d, cudaError_t e, const char* what) {
+  d->err = std::string(what) + ": " + cudaGetErrorString(e);
+  return AV1B_ERR_CUDA;
+}
+
+#define CK(call, what)                                     \
+  do {                                                     \
+    cudaError_t e_ = (call);                               \
+    if (e_ != cudaSuccess) return cuda_fail(d, e_, what);  \
+  } while (0)
+
+int dev_ensure(av1b_decoder* d, DevBuf& b, size_t bytes) {
+  if (bytes == 0) bytes = 256;
+  if (b.cap >= bytes) return AV1B_OK;
+  const size_t want = align_up(bytes + bytes / 8, 1 << 16);
+  if (d->budget && d->allocated - b.cap + want > d->budget)
+    return fail(d, AV1B_ERR_NOMEM, "decoder HBM budget exhausted");
+  if (b.p) {
+    cudaFree(b.p);
+    d->allocated -= b.cap;
+    b.p = nullptr;
+    b.cap = 0;
+  }
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, want);
+  if (e != cudaSuccess) return cuda_fail(d, e, "cudaMalloc");
+  b.p = p;
+  b.cap = want;
+  d->allocated += want;
+  return AV1B_OK;
+}
+
+void dev_release(av1b_decoder* d, DevBuf& b) {
+  if (b.p) {
+    cudaFree(b.p);
+    d->allocated -= b.cap;
+  }
+  b.p = nullptr;
+  b.cap = 0;
+}
+
+int host_ensure(av1b_decoder* d, HostBuf& b, size_t bytes) {
+  if (b.cap >= bytes) return AV1B_OK;
+  if (b.p) cudaFreeHost(b.p);
+  b.p = nullptr;
+  b.cap = 0;
+  const size_t want = align_up(bytes + bytes / 4, 1 << 20);
+  void* p = nullptr;
+  cudaError_t e = cudaHostAlloc(&p, want, cudaHostAllocDefault);
+  if (e != cudaSuccess) return cuda_fail(d, e, "cudaHostAlloc");
+  b.p = p;
+  b.cap = want;
+  return AV1B_OK;
+}
+
+Layout make_layout(int width, int height, int coded_width, int bd, int ss_x, int ss_y) {
+  Layout L{};
+  L.ss_x = ss_x;
+  L.ss_y = ss_y;
+  L.bit_depth = bd;
+  long long size = 0;
+  for (int p = 0; p < 3; ++p) {
+    const int sx = p ? ss_x : 0, sy = p ? ss_y : 0;
+    PlaneGeom& g = L.p[p];
+    g.out_w = (width + sx) >> sx;
+    g.out_h = (height + sy) >> sy;
+    g.coded_w = (coded_width + sx) >> sx;
+    g.coded_h = g.out_h;
+    g.grid_w = ((coded_width + 7) & ~7) >> sx;
+    g.grid_h = ((height + 7) & ~7) >> sy;
+    const int padx = kPadLuma >> sx, pady = kPadLuma >> sy;
+    g.stride = static_cast<int>(align_up(static_cast<size_t>(std::max(g.out_w, g.grid_w) + padx), 64));
+    g.off = static_cast<int>(size);
+    size += static_cast<long long>(g.stride) * (std::max(g.out_h, g.grid_h) + pady);
+    size = align_up(size, 64);
+  }
+  L.size = size;
+  return L;
+}
+
+int plane_rows(const Layout& L, int p) {
+  return static_cast<int>(((p < 2 ? L.p[p + 1].off : L.size) - L.p[p].off) / L.p[p].stride);
+}
+
+/* (Re)allocates the pictures for a geometry. Slots keep their contents and
+ * their own geometry tag; a frame may only reference slots of its size. */
+int ensure_geometry(av1b_decoder* d, const av1b_frame_syntax& s, int coded_width) {
+  if (d->have_geom && d->width == s.width && d->height == s.height &&
+      d->coded_width == coded_width && d->bit_depth == s.bit_depth && d->ss_x == s.ss_x &&
+      d->ss_y == s.ss_y)
+    return AV1B_OK;
+  const Layout L = make_layout(s.width, s.height, coded_width, s.bit_depth, s.ss_x, s.ss_y);
+  const bool same_pictures = d->have_geom && L.size == d->L.size && d->width == s.width &&
+                             d->height == s.height && d->bit_depth == s.bit_depth &&
+                             d->ss_x == s.ss_x && d->ss_y == s.ss_y;
+  const size_t bytes = static_cast<size_t>(L.size) * sizeof(px_t);
+  int rc;
+  if ((rc = dev_ensure(d, d->cur, bytes)) || (rc = dev_ensure(d, d->snap, bytes)) ||
+      (rc = dev_ensure(d, d->disp, bytes)))
+    return rc;
+  if (!same_pictures) {
+    /* a different display geometry: the slots' pictures are unusable */
+    for (int i = 0; i < kSlots; ++i) d->slot_valid[i] = false;
+  }
+  d->L = L;
+  d->width = s.width;
+  d->height = s.height;
+  d->coded_width = coded_width;
+  d->bit_depth = s.bit_depth;
+  d->ss_x = s.ss_x;
+  d->ss_y = s.ss_y;
+  d->have_geom = true;
+  d->have_last = false;
+  return AV1B_OK;
+}
+
+int init_grain_tables(av1b_decoder* d) {
+  if (d->grain_tables) return AV1B_OK;
+  int rc;
+  if ((rc = dev_ensure(d, d->orbit, 65536 * 2)) || (rc = dev_ensure(d, d->pos, 65536 * 2)) ||
+      (rc = dev_ensure(d, d->grain_state, sizeof(GrainState))))
+    return rc;
+  std::vector<uint16_t> orbit(65536, 0), pos(65536, 0);
+  unsigned s = 1;
+  for (unsigned k = 0; k < 65535; ++k) {
+    orbit[k] = static_cast<uint16_t>(s);
+    pos[s] = static_cast<uint16_t>(k);
+    const unsigned bit = ((s >> 0) ^ (s >> 1) ^ (s >> 3) ^ (s >> 12)) & 1u;
+    s = (s >> 1) | (bit << 15);
+  }
+  CK(cudaMemcpy(d->orbit.p, orbit.data(), 65536 * 2, cudaMemcpyHostToDevice), "orbit upload");
+  CK(cudaMemcpy(d->pos.p, pos.data(), 65536 * 2, cudaMemcpyHostToDevice), "pos upload");
+  d->grain_tables = true;
+  return AV1B_OK;
+}
+
+/* ---- the planner ------------------------------------------------------------------------- */
+
+struct Plan {
+  std::vector<BlockRec> blocks;
+  std::vector<TxRec> txs;
+  std::vector<ObmcRec> obmc;
+  std::vector<WarpRec> warps;
+  std::vector<int> palette_colors;
+  std::vector<int> units;
+  std::vector<int2> inter_tiles;
+  std::vector<int2> itx_jobs;
+  std::vector<DeblockRec> deblock_v, deblock_h;
+  std::vector<CdefRec> cdef;
+  std::vector<LrUnitRec> lr_units[3];
+  LrArgs lr{};
+  bool use_lr = false;
+  size_t coef_pool = 0, residual_pool = 0;
+  int scale_x = AV1B_SCALE_ONE, scale_y = AV1B_SCALE_ONE;
+  bool upscaled = false;
+  bool grain = false;
+  GrainParamsDev gp{};
+  GrainState gs_tail;   /* only the constants after the templates are used */
+};
+
+int resolve_slot(av1b_decoder* d, const av1b_frame_syntax& s, int ref, int* slot) {
+  *slot = -1;
+  if (ref < 0 || ref >= static_cast<int>(s.n_reference_slots)) return AV1B_OK;
+  const int sl = s.reference_slots[ref];
+  if (sl < 0 || sl >= kSlots) return AV1B_OK;
+  if (!d->slot_used[sl] || !d->slot_valid[sl])
+    return fail(d, AV1B_ERR_SYNTAX, "a block references a slot that holds no picture");
+  if (d->slot_width[sl] != s.width || d->slot_height[sl] != s.height)
+    return fail(d, AV1B_ERR_SYNTAX,
+                "engine: reference scaling between pictures of different sizes is not supported");
+  *slot = sl;
+  return AV1B_OK;
+}
+
+bool pow2_in(int v, int lo, int hi) { return v >= lo && v <= hi && (v & (v - 1)) == 0; }
+
+int build_plan(av1b_decoder* d, const av1b_frame_syntax& s, Plan* P) {
+  const Layout& L = d->L;
+  const int bd = s.bit_depth;
+  P->blocks.resize(s.n_blocks);
+  P->txs.clear();
+  P->obmc.clear();
+  P->warps.clear();
+  P->warps.push_back(WarpRec{});
+  P->palette_colors.clear();
+  P->units.clear();
+  P->inter_tiles.clear();
+  P->itx_jobs.clear();
+  for (int i = 0; i < 7; ++i) {
+    const int rw = s.reference_width[i] > 0 ? s.reference_width[i] : s.width;
+    const int rh = s.reference_height[i] > 0 ? s.reference_height[i] : s.height;
+    if (rw != s.width || rh != s.height)
+      return fail(d, AV1B_ERR_UNSUPPORTED,
+                  "engine: reference scaling between pictures of different sizes is not supported");
+  }
+  P->upscaled = L.p[0].coded_w != L.p[0].out_w;
+  P->scale_x = P->scale_y = AV1B_SCALE_ONE;
+  if (P->upscaled) {
+    const int fw = L.p[0].coded_w, fh = L.p[0].coded_h;
+    P->scale_x = ((s.width << 14) + (fw / 2)) / fw;
+    P->scale_y = ((s.height << 14) + (fh / 2)) / fh;
+  }
+  size_t coef_end = 0, res_end = 0;
+  for (size_t bi = 0; bi < s.n_blocks; ++bi) {
+    const av1b_block& b = s.blocks[bi];
+    BlockRec& r = P->blocks[bi];
+    std::memset(&r, 0, sizeof(r));
+    if (b.plane < 0 || b.plane > 2) return fail(d, AV1B_ERR_SYNTAX, "block plane out of range");
+    const PlaneGeom& g = L.p[b.plane];
+    const int rows = plane_rows(L, b.plane);
+    if (b.x < 0 || b.y < 0 || b.w < 1 || b.h < 1 || b.w > 128 || b.h > 128 ||
+        b.x + b.w > g.stride || b.y + b.h > rows)
+      return fail(d, AV1B_ERR_SYNTAX, "block outside the picture and its border");
+    r.x = static_cast<short>(b.x);
+    r.y = static_cast<short>(b.y);
+    r.w = static_cast<short>(b.w);
+    r.h = static_cast<short>(b.h);
+    r.plane = static_cast<unsigned char>(b.plane);
+    r.have_left = b.have_left && b.x > 0;
+    r.have_above = b.have_above && b.y > 0;
+    r.lossless = b.lossless ? 1 : 0;
+    r.residual_provided = b.residual_provided ? 1 : 0;
+    r.warp_idx[0] = r.warp_idx[1] = 0;
+    r.ref_slot[0] = r.ref_slot[1] = -1;
+    if (b.is_intra) {
+      if (!pow2_in(b.w, 2, 64) || !pow2_in(b.h, 2, 64))
+        return fail(d, AV1B_ERR_SYNTAX, "an intra block must be 2..64 samples per side");
+      if (b.mode < 0 || b.mode > 13) return fail(d, AV1B_ERR_SYNTAX, "intra mode out of range");
+      if (b.angle_delta < -3 || b.angle_delta > 3)
+        return fail(d, AV1B_ERR_SYNTAX, "angle delta out of range");
+      r.kind = AV1B_U_INTRA;
+      r.is_inter = 0;
+      r.phase_b = 1;
+      r.mode = static_cast<unsigned char>(b.mode);
+      r.angle_delta = static_cast<signed char>(b.angle_delta);
+      /* negative: no edge filtering at all; any other non-zero value selects
+       * the second strength table (av1gpu_kernels.h:1195-1239, 1459) */
+      r.filter_type = static_cast<signed char>(
+          !s.enable_intra_edge_filter || b.filter_type < 0 ? -1 : (b.filter_type ? 1 : 0));
+      const bool fi = b.use_filter_intra && b.plane == 0;
+      if (fi && (b.filter_intra_mode < 0 || b.filter_intra_mode > 4))
+        return fail(d, AV1B_ERR_SYNTAX, "filter intra mode out of range");
+      r.fi_mode = static_cast<signed char>(fi ? b.filter_intra_mode : -1);
+      r.cfl_alpha = static_cast<signed char>(std::max(-128, std::min(127, b.cfl_alpha)));
+      r.have_ar = b.have_above_right >= 0 ? (b.have_above_right != 0) : 2;
+      r.have_bl = b.have_below_left >= 0 ? (b.have_below_left != 0) : 2;
+      if (b.use_palette) {
+        if (b.palette_off < 0 || b.palette_stride < b.w ||
+            static_cast<size_t>(b.palette_off) + static_cast<size_t>(b.h - 1) * b.palette_stride + b.w >
+                s.n_palette_map)
+          return fail(d, AV1B_ERR_SYNTAX, "palette map outside the frame's pool");
+        for (int i = 0; i < b.h; ++i)
+          for (int j = 0; j < b.w; ++j)
+            if (s.palette_map[b.palette_off + i * b.palette_stride + j] > 7)
+              return fail(d, AV1B_ERR_SYNTAX, "palette index above 7");
+        r.palette = 1;
+        r.palette_off = b.palette_off;
+        r.palette_stride = b.palette_stride;
+        r.palette_color_idx = static_cast<int>(P->palette_colors.size() / 8);
+        for (int k = 0; k < 8; ++k) P->palette_colors.push_back(b.palette[k]);
+      }
+    } else {
+      r.kind = b.intrabc ? AV1B_U_INTRABC : (b.interintra ? AV1B_U_INTERINTRA : 0);
+      r.is_inter = 1;
+      r.phase_b = (b.intrabc || b.interintra) ? 1 : 0;
+      if (b.filter < 0 || b.filter > 3 || b.filter_v < 0 || b.filter_v > 3)
+        return fail(d, AV1B_ERR_SYNTAX, "interpolation filter out of range");
+      if (b.compound < 0 || b.compound > 4) return fail(d, AV1B_ERR_SYNTAX, "compound type out of range");
+      int rc;
+      if (b.intrabc) {
+        r.ref_slot[0] = r.ref_slot[1] = -1;
+      } else {
+        if ((rc = resolve_slot(d, s, b.ref[0], &r.ref_slot[0]))) return rc;
+        if (r.ref_slot[0] < 0) return fail(d, AV1B_ERR_SYNTAX, "an inter block without a reference");
+        if (b.compound) {
+          if ((rc = resolve_slot(d, s, b.ref[1], &r.ref_slot[1]))) return rc;
+          if (r.ref_slot[1] < 0)
+            return fail(d, AV1B_ERR_SYNTAX, "a compound block without a second reference");
+        }
+      }
+      for (int k = 0; k < 2; ++k) {
+        r.mv[k][0] = b.mv[k][0];
+        r.mv[k][1] = b.mv[k][1];
+      }
+      r.filt = static_cast<unsigned char>(b.filter);
+      r.filt_v = static_cast<unsigned char>(b.filter_v);
+      r.compound = static_cast<unsigned char>(b.compound);
+      r.w0 = static_cast<unsigned char>(b.blend[0]);
+      r.w1 = static_cast<unsigned char>(b.blend[1]);
+      const int lw = b.w << (b.plane > 0 ? s.ss_x : 0), lh = b.h << (b.plane > 0 ? s.ss_y : 0);
+      if (b.compound == 3 || b.compound == 4) {
+        r.mask_kind = b.compound == 3 ? 1 : 2;
+        r.mask_sign = b.mask_sign ? 1 : 0;
+        if (b.compound == 3) {
+          int dir, xo, yo, fl;
+          if (!wedge_entry(lw, lh, b.wedge_index, &dir, &xo, &yo, &fl))
+            return fail(d, AV1B_ERR_SYNTAX, "engine: a wedge on a block size that has none");
+          r.wedge_dir = static_cast<unsigned char>(dir);
+          r.wedge_xoff = static_cast<signed char>(xo);
+          r.wedge_yoff = static_cast<signed char>(yo);
+          r.wedge_flip = static_cast<unsigned char>(fl);
+        }
+      }
+      if (b.interintra) {
+        if (!pow2_in(b.w, 2, 64) || !pow2_in(b.h, 2, 64) || b.interintra_mode < 0 ||
+            b.interintra_mode > 3)
+          return fail(d, AV1B_ERR_SYNTAX, "inter-intra block shape or mode out of range");
+        r.interintra = 1;
+        r.ii_mode = static_cast<unsigned char>(b.interintra_mode);
+        if (b.interintra_wedge) {
+          int dir, xo, yo, fl;
+          if (!wedge_entry(lw, lh, b.wedge_index, &dir, &xo, &yo, &fl))
+            return fail(d, AV1B_ERR_SYNTAX, "engine: an inter/intra wedge on a block size that has none");
+          r.ii_wedge = 1;
+          r.wedge_dir = static_cast<unsigned char>(dir);
+          r.wedge_xoff = static_cast<signed char>(xo);
+          r.wedge_yoff = static_cast<signed char>(yo);
+          r.wedge_flip = static_cast<unsigned char>(fl);
+        }
+      }
+      /* global warp: a model whose shear is invalid keeps the warp flag with
+       * an all-zero model, exactly as the reference engine leaves its job
+       * (engine.cpp:1172-1193) */
+      for (int k = 0; k < 2; ++k) {
+        const bool w = b.warp[k] != 0, mw = b.mask_warp[k] != 0;
+        if (k == 0) {
+          r.warp0 = w;
+          r.mask_warp0 = mw;
+        } else {
+          r.warp1 = w;
+          r.mask_warp1 = mw;
+        }
+        if (!w && !mw) continue;
+        WarpRec m{};
+        int al, be, ga, de;
+        if (gm_setup_shear(b.warp_params[k], &al, &be, &ga, &de)) {
+          for (int j = 0; j < 6; ++j) m.params[j] = b.warp_params[k][j];
+          m.abcd[0] = al;
+          m.abcd[1] = be;
+          m.abcd[2] = ga;
+          m.abcd[3] = de;
+        }
+        r.warp_idx[k] = static_cast<int>(P->warps.size());
+        P->warps.push_back(m);
+      }
+      r.obmc_first = static_cast<int>(P->obmc.size());
+      r.obmc_count = 0;
+      if (b.obmc_count > 0) {
+        if (b.obmc_first < 0 || static_cast<size_t>(b.obmc_first) + b.obmc_count > s.n_obmc)
+          return fail(d, AV1B_ERR_SYNTAX, "OBMC range outside the frame's list");
+        for (int k = 0; k < b.obmc_count && k < 8; ++k) {
+          const av1b_obmc& c = s.obmc[b.obmc_first + k];
+          ObmcRec o{};
+          o.pass = static_cast<short>(c.pass);
+          o.x = static_cast<short>(c.x);
+          o.y = static_cast<short>(c.y);
+          o.w = static_cast<short>(c.w);
+          o.h = static_cast<short>(c.h);
+          const int len = c.pass == 0 ? c.h : c.w;
+          if (c.w < 1 || c.h < 1 || c.x < 0 || c.y < 0 || !(len == 2 || len == 4 || len == 8 ||
+                                                            len == 16 || len == 32))
+            return fail(d, AV1B_ERR_SYNTAX, "OBMC strip shape out of range");
+          if (c.filter < 0 || c.filter > 3 || c.filter_v < 0 || c.filter_v > 3)
+            return fail(d, AV1B_ERR_SYNTAX, "OBMC filter out of range");
+          o.filt = static_cast<short>(c.filter);
+          o.filt_v = static_cast<short>(c.filter_v);
+          o.mv_x = c.mv[0];
+          o.mv_y = c.mv[1];
+          if ((rc = resolve_slot(d, s, c.ref, &o.ref_slot))) return rc;
+          if (o.ref_slot < 0) return fail(d, AV1B_ERR_SYNTAX, "an OBMC strip without a reference");
+          P->obmc.push_back(o);
+          ++r.obmc_count;
+        }
+      }
+    }
+    /* transforms */
+    r.tx_first = static_cast<int>(P->txs.size());
+    r.tx_count = 0;
+    if (b.tx_count > 0) {
+      if (b.tx_first < 0 || static_cast<size_t>(b.tx_first) + b.tx_count > s.n_transforms)
+        return fail(d, AV1B_ERR_SYNTAX, "transform range outside the frame's list");
+      for (int k = 0; k < b.tx_count; ++k) {
+        const av1b_transform& t = s.transforms[b.tx_first + k];
+        if (t.eob <= 0) continue;
+        if (t.coef_offset < 0 || t.x < 0 || t.y < 0 || b.x + t.x + t.w > g.stride ||
+            b.y + t.y + t.h > rows)
+          return fail(d, AV1B_ERR_SYNTAX, "transform outside the picture and its border");
+        TxRec x{};
+        x.coef_off = t.coef_offset;
+        x.x = static_cast<short>(t.x);
+        x.y = static_cast<short>(t.y);
+        x.w = static_cast<short>(t.w);
+        x.h = static_cast<short>(t.h);
+        if (b.residual_provided) {
+          if (t.w < 1 || t.h < 1 || t.w > 128 || t.h > 128)
+            return fail(d, AV1B_ERR_SYNTAX, "residual block size out of range");
+          res_end = std::max(res_end, static_cast<size_t>(t.coef_offset) + static_cast<size_t>(t.w) * t.h);
+        } else {
+          if (!pow2_in(t.w, 4, 64) || !pow2_in(t.h, 4, 64) || t.tx_type < 0 || t.tx_type > 15)
+            return fail(d, AV1B_ERR_SYNTAX, "transform size or type out of range");
+          if (b.lossless && (t.w != 4 || t.h != 4))
+            return fail(d, AV1B_ERR_SYNTAX, "a lossless transform must be 4x4");
+          x.log2w = static_cast<unsigned char>(__builtin_ctz(t.w));
+          x.log2h = static_cast<unsigned char>(__builtin_ctz(t.h));
+          x.type = static_cast<unsigned char>(t.tx_type);
+          x.row_shift = static_cast<unsigned char>(b.lossless ? 0 : tx_row_shift(x.log2w, x.log2h));
+          coef_end = std::max(coef_end, static_cast<size_t>(t.coef_offset) + static_cast<size_t>(t.w) * t.h);
+        }
+        if (!r.phase_b)
+          P->itx_jobs.push_back(make_int2(static_cast<int>(bi), static_cast<int>(P->txs.size())));
+        P->txs.push_back(x);
+        ++r.tx_count;
+      }
+    }
+    if (r.phase_b) {
+      P->units.push_back(static_cast<int>(bi));
+    } else {
+      for (int y0 = 0; y0 < b.h; y0 += 8)
+        for (int x0 = 0; x0 < b.w; x0 += 16)
+          P->inter_tiles.push_back(make_int2(static_cast<int>(bi), x0 | (y0 << 16)));
+    }
+  }
+  /* the pools read past the caller's arrays as zeros, like the reference's
+   * padded plan pools (engine.cpp:665-674) */
+  P->coef_pool = std::max(coef_end + 64, s.n_coefficients);
+  P->residual_pool = std::max(res_end + 64, s.n_residual);
+
+  /* deblocking edges: V then H, each a list of independent edges */
+  P->deblock_v.clear();
+  P->deblock_h.clear();
+  if (s.sharpness < 0 || s.sharpness > 7) return fail(d, AV1B_ERR_SYNTAX, "sharpness out of range");
+  for (size_t i = 0; i < s.n_deblock; ++i) {
+    const av1b_deblock_edge& e = s.deblock[i];
+    if (e.plane < 0 || e.plane > 2) return fail(d, AV1B_ERR_SYNTAX, "deblock plane out of range");
+    if (e.length <= 0 || e.level == 0) continue;
+    if (e.level < 0 || e.level > 63) return fail(d, AV1B_ERR_SYNTAX, "deblock level out of range");
+    if (e.filter_size != 4 && e.filter_size != 8 && e.filter_size != 16)
+      return fail(d, AV1B_ERR_SYNTAX, "deblock filter size must be 4, 8 or 16");
+    const PlaneGeom& g = L.p[e.plane];
+    const int rows = plane_rows(L, e.plane);
+    /* how far the filter reaches across the edge: p6..q6 at most */
+    const int reach = e.filter_size == 16 ? 7 : (e.filter_size == 4 ? 2 : 4);
+    DeblockRec r{};
+    r.len = static_cast<short>(e.length);
+    r.level = static_cast<short>(e.level);
+    r.filter_size = static_cast<unsigned char>(e.filter_size);
+    r.chroma = e.plane != 0;
+    if (e.vertical) {
+      if (e.x - reach < 0 || e.x + reach > g.stride || e.y < 0 || e.y + e.length > rows)
+        return fail(d, AV1B_ERR_SYNTAX, "deblock edge reaches outside the picture");
+      r.p_off = g.off + e.y * g.stride + e.x - 2;
+      r.across = 1;
+      r.along = g.stride;
+      P->deblock_v.push_back(r);
+    } else {
+      if (e.y - reach < 0 || e.y + reach > rows || e.x < 0 || e.x + e.length > g.stride)
+        return fail(d, AV1B_ERR_SYNTAX, "deblock edge reaches outside the picture");
+      r.p_off = g.off + (e.y - 2) * g.stride + e.x;
+      r.across = g.stride;
+      r.along = 1;
+      P->deblock_h.push_back(r);
+    }
+  }
+
+  /* CDEF */
+  P->cdef.resize(s.n_cdef);
+  for (size_t i = 0; i < s.n_cdef; ++i) {
+    const av1b_cdef_block& c = s.cdef[i];
+    if (c.plane < 0 || c.plane > 2) return fail(d, AV1B_ERR_SYNTAX, "CDEF plane out of range");
+    const int sx = c.plane ? L.ss_x : 0, sy = c.plane ? L.ss_y : 0;
+    const int bw = 8 >> sx, bh = 8 >> sy;
+    const PlaneGeom& g = L.p[c.plane];
+    if (c.x < 0 || c.y < 0 || c.x + bw + 2 > g.stride || c.y + bh + 2 > plane_rows(L, c.plane) ||
+        (c.x << sx) + 8 > L.p[0].stride || (c.y << sy) + 8 > plane_rows(L, 0))
+      return fail(d, AV1B_ERR_SYNTAX, "CDEF block outside the picture");
+    if (c.dir < -1 || c.dir > 7 || c.pri_strength < 0 || c.pri_strength > 255 ||
+        c.sec_strength < 0 || c.sec_strength > 255 || c.damping < 0 || c.damping > 63)
+      return fail(d, AV1B_ERR_SYNTAX, "CDEF parameters out of range");
+    CdefRec& r = P->cdef[i];
+    r.x = static_cast<short>(c.x);
+    r.y = static_cast<short>(c.y);
+    r.plane = static_cast<unsigned char>(c.plane);
+    r.pri = static_cast<unsigned char>(c.pri_strength);
+    r.sec = static_cast<unsigned char>(c.sec_strength);
+    r.damping = static_cast<unsigned char>(c.damping);
+    r.dir = static_cast<signed char>(c.dir);
+  }
+
+  /* loop restoration */
+  P->use_lr = false;
+  std::memset(&P->lr, 0, sizeof(P->lr));
+  for (int p = 0; p < 3; ++p) {
+    P->lr_units[p].clear();
+    if (s.restoration_type[p] == 0) continue;
+    const int sub_y = p ? L.ss_y : 0;
+    if (s.restoration_unit_log2[p] < 5 || s.restoration_unit_log2[p] > 8)
+      return fail(d, AV1B_ERR_SYNTAX, "restoration unit size out of range");
+    const int us = 1 << s.restoration_unit_log2[p];
+    const int fh = (s.height + (sub_y ? 1 << (sub_y - 1) : 0)) >> sub_y;
+    P->lr.type[p] = 1;
+    P->lr.unit_size[p] = us;
+    P->lr.unit_rows[p] = std::max((fh + (us >> 1)) / us, 1);
+    P->lr.unit_cols[p] = std::max(s.restoration_unit_cols[p], 1);
+    P->lr.n_units[p] = static_cast<int>(s.n_restoration[p]);
+    for (size_t i = 0; i < s.n_restoration[p]; ++i) {
+      const av1b_restoration_unit& u = s.restoration[p][i];
+      LrUnitRec o{};
+      /* the reference engine's mapping (engine.cpp:1417-1455): type 2 is the
+       * Wiener filter, any other non-zero type the self-guided one */
+      o.type = u.type == 0 ? 0 : (u.type == 2 ? 1 : 2);
+      for (int k = 0; k < 3; ++k) {
+        o.vf[k] = u.wiener[0][k];
+        o.hf[k] = u.wiener[1][k];
+      }
+      const short* sp = sgr_params_table() + (u.sgr_set & 15) * 4;
+      o.r[0] = sp[0];
+      o.e[0] = sp[1];
+      o.r[1] = sp[2];
+      o.e[1] = sp[3];
+      o.xqd[0] = u.sgr_xqd[0];
+      o.xqd[1] = u.sgr_xqd[1];
+      P->lr_units[p].push_back(o);
+    }
+    P->use_lr = true;
+  }
+
+  /* film grain */
+  P->grain = s.grain.apply != 0;
+  if (P->grain) {
+    const av1b_film_grain& f = s.grain;
+    if (f.seed < 0 || f.seed > 65535 || f.ar_coeff_lag < 0 || f.ar_coeff_lag > 3 ||
+        f.num_y_points < 0 || f.num_y_points > 16 || f.num_cb_points < 0 || f.num_cb_points > 16 ||
+        f.num_cr_points < 0 || f.num_cr_points > 16 || f.grain_scaling_minus_8 < 0 ||
+        f.grain_scaling_minus_8 > 3 || f.ar_coeff_shift_minus_6 < 0 || f.ar_coeff_shift_minus_6 > 3 ||
+        f.grain_scale_shift < 0 || f.grain_scale_shift > 3)
+      return fail(d, AV1B_ERR_SYNTAX, "film grain parameters out of range");
+    auto check_points = [&](int n, const int32_t* v) {
+      for (int i = 0; i < n; ++i) {
+        if (v[i] < 0 || v[i] > 255) return false;
+        if (i > 0 && v[i] <= v[i - 1]) return false;
+      }
+      return true;
+    };
+    if (!check_points(f.num_y_points, f.point_y_value) ||
+        !check_points(f.num_cb_points, f.point_cb_value) ||
+        !check_points(f.num_cr_points, f.point_cr_value))
+      return fail(d, AV1B_ERR_SYNTAX, "film grain points must increase strictly within 0..255");
+    GrainParamsDev& g = P->gp;
+    std::memset(&g, 0, sizeof(g));
+    g.seed = f.seed;
+    g.bitdepth = bd;
+    g.ss_x = s.ss_x;
+    g.ss_y = s.ss_y;
+    g.num_y_points = f.num_y_points;
+    g.num_cb_points = f.num_cb_points;
+    g.num_cr_points = f.num_cr_points;
+    g.chroma_scaling_from_luma = f.chroma_scaling_from_luma ? 1 : 0;
+    g.ar_coeff_lag = f.ar_coeff_lag;
+    g.ar_coeff_shift_minus_6 = f.ar_coeff_shift_minus_6;
+    g.grain_scale_shift = f.grain_scale_shift;
+    for (int i = 0; i < 24; ++i) g.ar_y[i] = f.ar_coeffs_y[i];
+    for (int i = 0; i < 25; ++i) {
+      g.ar_cb[i] = f.ar_coeffs_cb[i];
+      g.ar_cr[i] = f.ar_coeffs_cr[i];
+    }
+    GrainState& t = P->gs_tail;
+    const bool chroma = f.chroma_scaling_from_luma || f.num_cb_points > 0 || f.num_cr_points > 0;
+    grain_scaling_lut(f.num_y_points, f.point_y_value, f.point_y_scaling, t.lut[0]);
+    if (chroma) {
+      if (f.chroma_scaling_from_luma) {
+        grain_scaling_lut(f.num_y_points, f.point_y_value, f.point_y_scaling, t.lut[1]);
+        grain_scaling_lut(f.num_y_points, f.point_y_value, f.point_y_scaling, t.lut[2]);
+      } else {
+        grain_scaling_lut(f.num_cb_points, f.point_cb_value, f.point_cb_scaling, t.lut[1]);
+        grain_scaling_lut(f.num_cr_points, f.point_cr_value, f.point_cr_scaling, t.lut[2]);
+      }
+    } else {
+      std::memset(t.lut[1], 0, sizeof(t.lut[1]));
+      std::memset(t.lut[2], 0, sizeof(t.lut[2]));
+    }
+    t.seed = f.seed;
+    t.bitdepth = bd;
+    t.overlap = f.overlap_flag ? 1 : 0;
+    t.scaling_shift = f.grain_scaling_minus_8 + 8;
+    t.num_points[0] = f.num_y_points;
+    t.num_points[1] = f.num_cb_points;
+    t.num_points[2] = f.num_cr_points;
+    t.chroma_from_luma = f.chroma_scaling_from_luma ? 1 : 0;
+    t.mult[1] = f.cb_mult;
+    t.luma_mult[1] = f.cb_luma_mult;
+    t.offset[1] = f.cb_offset;
+    t.mult[2] = f.cr_mult;
+    t.luma_mult[2] = f.cr_luma_mult;
+    t.offset[2] = f.cr_offset;
+    const int maxv = (1 << bd) - 1;
+    t.min_value = 0;
+    t.max_luma = maxv;
+    t.max_chroma = maxv;
+    if (f.clip_to_restricted_range) {
+      t.min_value = 16 << (bd - 8);
+      t.max_luma = 235 << (bd - 8);
+      t.max_chroma = s.color_matrix == 3 ? t.max_luma : (240 << (bd - 8));
+    }
+    t.chroma_w = s.ss_x ? 44 : 82;
+    t.chroma_h = s.ss_y ? 38 : 73;
+  }
+  return AV1B_OK;
+}
+
+/* ---- the frame step ------------------------------------------------------------------------ */
+
+/* Reserves room for `v` in the staging arena; returns its offset. */
+template <class T>
+size_t stage_put(size_t* off, const std::vector<T>& v) {
+  const size_t o = *off;
+  *off = align_up(o + v.size() * sizeof(T), 256);
+  return o;
+}
+
+int run_frame(av1b_decoder* d, const av1b_frame_syntax& s, int keep, int forced_slot,
+              const av1b_planes* out, int* out_slot) {
+  if (s.width <= 0 || s.height <= 0) return fail(d, AV1B_ERR_SYNTAX, "frame has no size");
+  if (s.bit_depth != 8 && s.bit_depth != 10 && s.bit_depth != 12)
+    return fail(d, AV1B_ERR_SYNTAX, "bit depth must be 8, 10 or 12");
+  if (s.ss_x < 0 || s.ss_x > 1 || s.ss_y < 0 || s.ss_y > 1 || (s.ss_y && !s.ss_x))
+    return fail(d, AV1B_ERR_SYNTAX, "unsupported chroma subsampling");
+  if (s.width > 16384 || s.height > 16384) return fail(d, AV1B_ERR_SYNTAX, "frame too large");
+  const int coded_width = (s.coded_width <= 0 || s.coded_width > s.width) ? s.width : s.coded_width;
+  cudaEvent_t ev[4];
+  for (auto& e : ev) CK(cudaEventCreate(&e), "cudaEventCreate");
+  struct EvGuard {
+    cudaEvent_t* e;
+    ~EvGuard() {
+      for (int i = 0; i < 4; ++i) cudaEventDestroy(e[i]);
+    }
+  } evg{ev};
+
+  int rc = ensure_geometry(d, s, coded_width);
+  if (rc) return rc;
+  Plan P;
+  if ((rc = build_plan(d, s, &P))) return rc;
+  const Layout& L = d->L;
+  const int maxv = (1 << s.bit_depth) - 1;
+  cudaStream_t st = d->stream;
+
+  /* the destination slot */
+  int slot = -1;
+  if (keep) {
+    if (forced_slot >= 0) {
+      if (forced_slot >= kSlots || !d->slot_used[forced_slot])
+        return fail(d, AV1B_ERR_ARG, "invalid reserved slot");
+      slot = forced_slot;
+    } else {
+      for (int i = 0; i < kSlots; ++i)
+        if (!d->slot_used[i]) {
+          slot = i;
+          break;
+        }
+      if (slot < 0) return fail(d, AV1B_ERR_NOMEM, "reference pool exhausted");
+    }
+    if ((rc = dev_ensure(d, d->slot_buf[slot], static_cast<size_t>(L.size) * sizeof(px_t)))) return rc;
+  }
+  if (P.use_lr) {
+    const size_t bytes = static_cast<size_t>(L.size) * sizeof(px_t);
+    if ((rc = dev_ensure(d, d->lr_pre, bytes)) || (rc = dev_ensure(d, d->lr_cdef, bytes)) ||
+        (P.upscaled && (rc = dev_ensure(d, d->lr_pre_up, bytes))))
+      return rc;
+  }
+  if (P.grain && (rc = init_grain_tables(d))) return rc;
+
+  /* slot pointer table */
+  {
+    px_t* ptrs[kSlots];
+    for (int i = 0; i < kSlots; ++i) ptrs[i] = static_cast<px_t*>(d->slot_buf[i].p);
+    if ((rc = dev_ensure(d, d->slot_ptr_dev, sizeof(ptrs)))) return rc;
+    CK(cudaMemcpyAsync(d->slot_ptr_dev.p, ptrs, sizeof(ptrs), cudaMemcpyHostToDevice, st),
+       "slot table upload");
+  }
+
+  /* ---- stage the frame's records ------------------------------------------------------ */
+  size_t off = 0;
+  const size_t o_blocks = stage_put(&off, P.blocks);
+  const size_t o_txs = stage_put(&off, P.txs);
+  const size_t o_obmc = stage_put(&off, P.obmc);
+  const size_t o_warps = stage_put(&off, P.warps);
+  const size_t o_pal = stage_put(&off, P.palette_colors);
+  const size_t o_units = stage_put(&off, P.units);
+  const size_t o_tiles = stage_put(&off, P.inter_tiles);
+  const size_t o_itx = stage_put(&off, P.itx_jobs);
+  const size_t o_dbv = stage_put(&off, P.deblock_v);
+  const size_t o_dbh = stage_put(&off, P.deblock_h);
+  const size_t o_cdef = stage_put(&off, P.cdef);
+  size_t o_lr[3];
+  for (int p = 0; p < 3; ++p) o_lr[p] = stage_put(&off, P.lr_units[p]);
+  const size_t o_map = off;
+  off = align_up(off + s.n_palette_map + 64, 256);
+  const size_t total = off;
+  if ((rc = host_ensure(d, d->stage, total)) || (rc = dev_ensure(d, d->arena, total))) return rc;
+  /* the previous frame's copy out of the staging buffer must be done */
+  CK(cudaStreamSynchronize(st), "stream sync");
+  uint8_t* hs = static_cast<uint8_t*>(d->stage.p);
+  auto put = [&](size_t o, const void* src, size_t bytes) {
+    if (bytes) std::memcpy(hs + o, src, bytes);
+  };
+  put(o_blocks, P.blocks.data(), P.blocks.size() * sizeof(BlockRec));
+  put(o_txs, P.txs.data(), P.txs.size() * sizeof(TxRec));
+  put(o_obmc, P.obmc.data(), P.obmc.size() * sizeof(ObmcRec));
+  put(o_warps, P.warps.data(), P.warps.size() * sizeof(WarpRec));
+  put(o_pal, P.palette_colors.data(), P.palette_colors.size() * sizeof(int));
+  put(o_units, P.units.data(), P.units.size() * sizeof(int));
+  put(o_tiles, P.inter_tiles.data(), P.inter_tiles.size() * sizeof(int2));
+  put(o_itx, P.itx_jobs.data(), P.itx_jobs.size() * sizeof(int2));
+  put(o_dbv, P.deblock_v.data(), P.deblock_v.size() * sizeof(DeblockRec));
+  put(o_dbh, P.deblock_h.data(), P.deblock_h.size() * sizeof(DeblockRec));
+  put(o_cdef, P.cdef.data(), P.cdef.size() * sizeof(CdefRec));
+  for (int p = 0; p < 3; ++p) put(o_lr[p], P.lr_units[p].data(), P.lr_units[p].size() * sizeof(LrUnitRec));
+  put(o_map, s.palette_map, s.n_palette_map);
+  std::memset(hs + o_map + s.n_palette_map, 0, 64);
+  CK(cudaEventRecord(ev[0], st), "event");
+  CK(cudaMemcpyAsync(d->arena.p, hs, total, cudaMemcpyHostToDevice, st), "arena upload");
+  uint8_t* ar = static_cast<uint8_t*>(d->arena.p);
+
+  /* coefficient and residual pools, zero past the caller's arrays */
+  if ((rc = dev_ensure(d, d->coef, P.coef_pool * sizeof(int))) ||
+      (rc = dev_ensure(d, d->residual, P.residual_pool * sizeof(int))))
+    return rc;
+  if (!P.itx_jobs.empty() || !P.units.empty()) {
+    if (s.n_coefficients)
+      CK(cudaMemcpyAsync(d->coef.p, s.coefficients, s.n_coefficients * sizeof(int),
+                         cudaMemcpyHostToDevice, st), "coefficient upload");
+    if (P.coef_pool > s.n_coefficients)
+      CK(cudaMemsetAsync(static_cast<int*>(d->coef.p) + s.n_coefficients, 0,
+                         (P.coef_pool - s.n_coefficients) * sizeof(int), st), "coefficient pad");
+    if (s.n_residual)
+      CK(cudaMemcpyAsync(d->residual.p, s.residual, s.n_residual * sizeof(int),
+                         cudaMemcpyHostToDevice, st), "residual upload");
+    if (P.residual_pool > s.n_residual)
+      CK(cudaMemsetAsync(static_cast<int*>(d->residual.p) + s.n_residual, 0,
+                         (P.residual_pool - s.n_residual) * sizeof(int), st), "residual pad");
+  }
+
+  /* owner grids, done flags, queue and status */
+  FrameArgs a{};
+  a.L = L;
+  for (int p = 0; p < 3; ++p) {
+    /* square cells: 4 luma samples; 2 for a chroma plane whose axis is
+     * subsampled - the reference keys plane 1 on ss_x and plane 2 on ss_y
+     * (engine.cpp:737-741), which this mirrors */
+    const int shift = p == 0 ? 2 : (p == 1 ? (L.ss_x ? 1 : 2) : (L.ss_y ? 1 : 2));
+    a.cell_shift[p] = shift;
+    a.cell_w[p] = (L.p[p].grid_w + (1 << shift) - 1) >> shift;
+    a.cell_h[p] = (L.p[p].grid_h + (1 << shift) - 1) >> shift;
+    const size_t cells = static_cast<size_t>(a.cell_w[p]) * a.cell_h[p];
+    if ((rc = dev_ensure(d, d->owner[p], cells * sizeof(int)))) return rc;
+    a.owner[p] = static_cast<int*>(d->owner[p].p);
+    CK(cudaMemsetAsync(a.owner[p], 0xff, cells * sizeof(int), st), "owner reset");
+  }
+  if (d->done.cap < s.n_blocks * sizeof(unsigned) + 256) {
+    if ((rc = dev_ensure(d, d->done, s.n_blocks * sizeof(unsigned) + 256))) return rc;
+    CK(cudaMemsetAsync(d->done.p, 0, d->done.cap, st), "done reset");
+  }
+  ++d->epoch;
+  if (d->epoch == 0) {
+    CK(cudaMemsetAsync(d->done.p, 0, d->done.cap, st), "done reset");
+    d->epoch = 1;
+  }
+  if ((rc = dev_ensure(d, d->status_q, 256))) return rc;
+  CK(cudaMemsetAsync(d->status_q.p, 0, 256, st), "status reset");
+
+  a.cur = static_cast<px_t*>(d->cur.p);
+  a.slot_ptr = static_cast<px_t* const*>(d->slot_ptr_dev.p);
+  a.blocks = reinterpret_cast<const BlockRec*>(ar + o_blocks);
+  a.n_blocks = static_cast<int>(P.blocks.size());
+  a.txs = reinterpret_cast<const TxRec*>(ar + o_txs);
+  a.obmc = reinterpret_cast<const ObmcRec*>(ar + o_obmc);
+  a.warps = reinterpret_cast<const WarpRec*>(ar + o_warps);
+  a.coef = static_cast<const int*>(d->coef.p);
+  a.residual = static_cast<const int*>(d->residual.p);
+  a.palette_map = ar + o_map;
+  a.palette_colors = reinterpret_cast<const int*>(ar + o_pal);
+  a.done = static_cast<unsigned*>(d->done.p);
+  a.epoch = d->epoch;
+  a.units = reinterpret_cast<const int*>(ar + o_units);
+  a.n_units = static_cast<int>(P.units.size());
+  a.queue = static_cast<unsigned*>(d->status_q.p);
+  a.status = reinterpret_cast<int*>(static_cast<uint8_t*>(d->status_q.p) + 64);
+  a.inter_tiles = reinterpret_cast<const int2*>(ar + o_tiles);
+  a.n_inter_tiles = static_cast<int>(P.inter_tiles.size());
+  a.itx_jobs = reinterpret_cast<const int2*>(ar + o_itx);
+  a.n_itx = static_cast<int>(P.itx_jobs.size());
+  a.maxv = maxv;
+  a.scale_x = P.scale_x;
+  a.scale_y = P.scale_y;
+
+  int launches = 0;
+  CK(cudaEventRecord(ev[1], st), "event");
+  CK(launch_recon(a, d->n_sm, st, &launches), "reconstruction launch");
+  CK(cudaEventRecord(ev[2], st), "event");
+
+  /* ---- filters --------------------------------------------------------------------------- */
+  px_t* cur = a.cur;
+  const size_t pic_bytes = static_cast<size_t>(L.size) * sizeof(px_t);
+  CK(launch_deblock(cur, reinterpret_cast<const DeblockRec*>(ar + o_dbv),
+                    static_cast<int>(P.deblock_v.size()), s.sharpness, s.bit_depth, maxv, st),
+     "deblock V");
+  CK(launch_deblock(cur, reinterpret_cast<const DeblockRec*>(ar + o_dbh),
+                    static_cast<int>(P.deblock_h.size()), s.sharpness, s.bit_depth, maxv, st),
+     "deblock H");
+  launches += (!P.deblock_v.empty()) + (!P.deblock_h.empty());
+  px_t* snap = static_cast<px_t*>(d->snap.p);
+  if (P.use_lr)
+    CK(cudaMemcpyAsync(d->lr_pre.p, cur, pic_bytes, cudaMemcpyDeviceToDevice, st), "pre-CDEF copy");
+  if (!P.cdef.empty()) {
+    CK(cudaMemcpyAsync(snap, cur, pic_bytes, cudaMemcpyDeviceToDevice, st), "CDEF snapshot");
+    CK(launch_cdef(snap, cur, reinterpret_cast<const CdefRec*>(ar + o_cdef),
+                   static_cast<int>(P.cdef.size()), L, st), "CDEF");
+    ++launches;
+  }
+  const px_t* lr_curr = static_cast<px_t*>(d->lr_pre.p);
+  if (P.upscaled) {
+    CK(cudaMemcpyAsync(snap, cur, pic_bytes, cudaMemcpyDeviceToDevice, st), "superres snapshot");
+    CK(launch_upscale(snap, cur, L, maxv, st), "superres");
+    ++launches;
+    if (P.use_lr) {
+      CK(launch_upscale(static_cast<px_t*>(d->lr_pre.p), static_cast<px_t*>(d->lr_pre_up.p), L,
+                        maxv, st), "superres (pre-CDEF)");
+      ++launches;
+      lr_curr = static_cast<px_t*>(d->lr_pre_up.p);
+    }
+  }
+  if (P.use_lr) {
+    CK(cudaMemcpyAsync(d->lr_cdef.p, cur, pic_bytes, cudaMemcpyDeviceToDevice, st), "LR snapshot");
+    LrArgs lr = P.lr;
+    for (int p = 0; p < 3; ++p) lr.units[p] = reinterpret_cast<const LrUnitRec*>(ar + o_lr[p]);
+    CK(launch_lr(static_cast<px_t*>(d->lr_cdef.p), lr_curr, cur, L, lr, maxv, st), "loop restoration");
+    ++launches;
+  }
+  if (keep)
+    CK(cudaMemcpyAsync(d->slot_buf[slot].p, cur, pic_bytes, cudaMemcpyDeviceToDevice, st),
+       "reference store");
+  const px_t* display = cur;
+  d->disp_is_cur = true;
+  if (P.grain) {
+    GrainState* gsd = static_cast<GrainState*>(d->grain_state.p);
+    const size_t tail = offsetof(GrainState, lut);
+    CK(cudaMemcpyAsync(reinterpret_cast<uint8_t*>(gsd) + tail,
+                       reinterpret_cast<const uint8_t*>(&P.gs_tail) + tail, sizeof(GrainState) - tail,
+                       cudaMemcpyHostToDevice, st), "grain constants");
+    CK(launch_grain(cur, static_cast<px_t*>(d->disp.p), L, gsd, P.gp,
+                    static_cast<const uint16_t*>(d->orbit.p), static_cast<const uint16_t*>(d->pos.p),
+                    st), "film grain");
+    launches += 2;
+    display = static_cast<px_t*>(d->disp.p);
+    d->disp_is_cur = false;
+  }
+  CK(cudaEventRecord(ev[3], st), "event");
+
+  /* ---- read back ---------------------------------------------------------------------------- */
+  if (out) {
+    for (int p = 0; p < 3; ++p) {
+      const PlaneGeom& g = L.p[p];
+      if (!out->plane[p] || out->stride[p] < g.out_w)
+        return fail(d, AV1B_ERR_ARG, "output plane missing or too narrow");
+      CK(cudaMemcpy2DAsync(out->plane[p], static_cast<size_t>(out->stride[p]) * sizeof(px_t),
+                           display + g.off, static_cast<size_t>(g.stride) * sizeof(px_t),
+                           static_cast<size_t>(g.out_w) * sizeof(px_t), g.out_h,
+                           cudaMemcpyDeviceToHost, st), "read back");
+    }
+  }
+  int status = 0;
+  CK(cudaMemcpyAsync(&status, a.status, sizeof(int), cudaMemcpyDeviceToHost, st), "status read");
+  CK(cudaStreamSynchronize(st), "frame sync");
+  if (status & AV1B_STATUS_TIMEOUT)
+    return fail(d, AV1B_ERR_TIMEOUT, "a device-side dependency wait timed out");
+
+  float ms_recon = 0, ms_filter = 0, ms_total = 0;
+  cudaEventElapsedTime(&ms_recon, ev[1], ev[2]);
+  cudaEventElapsedTime(&ms_filter, ev[2], ev[3]);
+  cudaEventElapsedTime(&ms_total, ev[0], ev[3]);
+  d->stats.blocks = static_cast<int>(s.n_blocks);
+  d->stats.waves = 0;
+  d->stats.kernel_launches = launches;
+  d->stats.reconstruct_ms = ms_recon;
+  d->stats.filter_ms = ms_filter;
+  d->stats.readback_ms = 0;
+  d->stats.total_ms = ms_total;
+
+  if (keep) {
+    d->slot_used[slot] = true;
+    d->slot_valid[slot] = true;
+    d->slot_width[slot] = s.width;
+    d->slot_height[slot] = s.height;
+    d->slot_bd[slot] = s.bit_depth;
+  }
+  d->last_slot = slot;
+  d->have_last = true;
+  if (out_slot) *out_slot = slot;
+  return AV1B_OK;
+}
+
+/* The picture an output call of `slot` reads: the display picture of the
+ * frame decoded last for its slot (or a negative slot), else the stored one. */
+int picture_of(av1b_decoder* d, int slot, const px_t** pic) {
+  if (slot < 0 || slot == d->last_slot) {
+    if (!d->have_last) return fail(d, AV1B_ERR_ARG, "no frame to convert");
+    *pic = d->disp_is_cur ? static_cast<const px_t*>(d->cur.p) : static_cast<const px_t*>(d->disp.p);
+    return AV1B_OK;
+  }
+  if (slot >= kSlots || !d->slot_used[slot] || !d->slot_valid[slot])
+    return fail(d, AV1B_ERR_ARG, "invalid reference slot");
+  *pic = static_cast<const px_t*>(d->slot_buf[slot].p);
+  return AV1B_OK;
+}
+
+void copy_error(const av1b_decoder* d, char* error, size_t len) {
+  if (!error || !len) return;
+  std::snprintf(error, len, "%s", d->err.c_str());
+}
+
+}  // namespace
+}  // namespace av1b
+
+/* ---- C ABI ---------------------------------------------------------------------------------------- */
+extern "C" {
+
+int av1b_decoder_create(int device, size_t hbm_budget_bytes, av1b_decoder** out) {
+  if (!out) return AV1B_ERR_ARG;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) return AV1B_ERR_NO_DEVICE;
+  if (device < 0 || device >= n) return AV1B_ERR_ARG;
+  if (cudaSetDevice(device) != cudaSuccess) return AV1B_ERR_CUDA;
+  auto* d = new av1b_decoder;
+  d->device = device;
+  d->budget = hbm_budget_bytes;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) d->n_sm = prop.multiProcessorCount;
+  if (cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      set_kernel_attributes() != cudaSuccess) {
+    delete d;
+    return AV1B_ERR_CUDA;
+  }
+  *out = d;
+  return AV1B_OK;
+}
+
+int av1b_decoder_destroy(av1b_decoder* d) {
+  if (!d) return AV1B_ERR_ARG;
+  cudaSetDevice(d->device);
+  cudaStreamSynchronize(d->stream);
+  DevBuf* bufs[] = {&d->cur, &d->snap, &d->lr_pre, &d->lr_pre_up, &d->lr_cdef, &d->disp,
+                    &d->slot_ptr_dev, &d->arena, &d->coef, &d->residual, &d->owner[0],
+                    &d->owner[1], &d->owner[2], &d->done, &d->status_q, &d->nv12, &d->rgb,
+                    &d->grain_state, &d->orbit, &d->pos};
+  for (DevBuf* b : bufs) dev_release(d, *b);
+  for (int i = 0; i < kSlots; ++i) dev_release(d, d->slot_buf[i]);
+  if (d->stage.p) cudaFreeHost(d->stage.p);
+  cudaStreamDestroy(d->stream);
+  delete d;
+  return AV1B_OK;
+}
+
+int av1b_decoder_reset(av1b_decoder* d) {
+  if (!d) return AV1B_ERR_ARG;
+  std::lock_guard<std::mutex> lk(d->mu);
+  for (int i = 0; i < kSlots; ++i) {
+    d->slot_used[i] = false;
+    d->slot_valid[i] = false;
+  }
+  d->last_slot = -1;
+  d->have_last = false;
+  d->stats = av1b_stats{};
+  return AV1B_OK;
+}
+
+int av1b_decode(av1b_decoder* d, const av1b_frame_syntax* syntax, int keep_reference,
+                const av1b_planes* out, int* out_slot, char* error, size_t error_len) {
+  if (!d || !syntax) return AV1B_ERR_ARG;
+  std::lock_guard<std::mutex> lk(d->mu);
+  cudaSetDevice(d->device);
+  if (out_slot) *out_slot = -1;
+  d->err.clear();
+  const int rc = run_frame(d, *syntax, keep_reference ? 1 : 0, -1, out, out_slot);
+  if (rc) copy_error(d, error, error_len);
+  return rc;
+}
+
+int av1b_decode_blob(av1b_decoder* d, const uint8_t* blob, size_t len, int keep_reference,
+                     const av1b_planes* out, int* out_slot, char* error, size_t error_len) {
+  av1b_frame_syntax v;
+  if (!d) return AV1B_ERR_ARG;
+  if (!view_blob(blob, len, &v)) {
+    d->err = "malformed serialized frame";
+    copy_error(d, error, error_len);
+    return AV1B_ERR_ARG;
+  }
+  return av1b_decode(d, &v, keep_reference, out, out_slot, error, error_len);
+}
+
+int av1b_reserve_reference(av1b_decoder* d, int* out_slot) {
+  if (!d || !out_slot) return AV1B_ERR_ARG;
+  std::lock_guard<std::mutex> lk(d->mu);
+  *out_slot = -1;
+  for (int i = 0; i < kSlots; ++i)
+    if (!d->slot_used[i]) {
+      d->slot_used[i] = true;
+      d->slot_valid[i] = false;
+      *out_slot = i;
+      return AV1B_OK;
+    }
+  return AV1B_ERR_NOMEM;
+}
+
+int av1b_decode_reserved(av1b_decoder* d, const av1b_frame_syntax* syntax, int slot,
+                         const av1b_planes* out, char* error, size_t error_len) {
+  if (!d || !syntax) return AV1B_ERR_ARG;
+  std::lock_guard<std::mutex> lk(d->mu);
+  cudaSetDevice(d->device);
+  d->err.clear();
+  int got = -1;
+  const int rc = run_frame(d, *syntax, slot >= 0 ? 1 : 0, slot, out, &got);
+  if (rc) copy_error(d, error, error_len);
+  return rc;
+}
+
+int av1b_release_reference(av1b_decoder* d, int slot) {
+  if (!d) return AV1B_ERR_ARG;
+  std::lock_guard<std::mutex> lk(d->mu);
+  if (slot >= 0 && slot < kSlots) {
+    d->slot_used[slot] = false;
+    d->slot_valid[slot] = false;
+  }
+  return AV1B_OK;
+}
+
+size_t av1b_nv12_size(int width, int height, int ss_x, int ss_y, size_t pitch) {
+  return nv12_bytes(width, height, ss_x, ss_y, pitch);
+}
+
+static int to_nv12_impl(av1b_decoder* d, int slot, size_t pitch, uint8_t* dst, size_t dst_len,
+                        bool device_dst) {
+  if (!d || !dst) return AV1B_ERR_ARG;
+  std::lock_guard<std::mutex> lk(d->mu);
+  cudaSetDevice(d->device);
+  const px_t* pic = nullptr;
+  int rc = picture_of(d, slot, &pic);
+  if (rc) return rc;
+  const size_t bytes = nv12_bytes(d->width, d->height, d->ss_x, d->ss_y, pitch);
+  if (bytes == 0 || pitch > (1u << 30))
+    return fail(d, AV1B_ERR_ARG, "NV12 output needs a 4:2:0 frame and an even pitch at least as wide");
+  if (dst_len < bytes) return fail(d, AV1B_ERR_ARG, "NV12 destination too small");
+  uint8_t* target = dst;
+  if (!device_dst) {
+    if ((rc = dev_ensure(d, d->nv12, bytes))) return rc;
+    target = static_cast<uint8_t*>(d->nv12.p);
+  }
+  CK(launch_nv12(pic, target, d->L, static_cast<int>(pitch), d->stream), "NV12 pack");
+  if (!device_dst)
+    CK(cudaMemcpyAsync(dst, target, bytes, cudaMemcpyDeviceToHost, d->stream), "NV12 read back");
+  CK(cudaStreamSynchronize(d->stream), "NV12 sync");
+  return AV1B_OK;
+}
+
+int av1b_to_nv12(av1b_decoder* d, int slot, size_t pitch, uint8_t* dst, size_t dst_len) {
+  return to_nv12_impl(d, slot, pitch, dst, dst_len, false);
+}
+
+int av1b_to_nv12_device(av1b_decoder* d, int slot, size_t pitch, void* dst_device, size_t dst_len) {
+  return to_nv12_impl(d, slot, pitch, static_cast<uint8_t*>(dst_device), dst_len, true);
+}
+
+int av1b_to_rgb(av1b_decoder* d, int slot, int matrix, int range, uint8_t* dst, size_t dst_len) {
+  if (!d || !dst) return AV1B_ERR_ARG;
+  std::lock_guard<std::mutex> lk(d->mu);
+  cudaSetDevice(d->device);
+  const px_t* pic = nullptr;
+  int rc = picture_of(d, slot, &pic);
+  if (rc) return rc;
+  const size_t bytes = static_cast<size_t>(d->width) * d->height * 3;
+  if (dst_len < bytes) return fail(d, AV1B_ERR_ARG, "RGB destination too small");
+  if ((rc = dev_ensure(d, d->rgb, bytes))) return rc;
+  RgbArgs m{};
+  color_matrix(matrix, range, d->bit_depth, m.m, m.o);
+  CK(launch_rgb(pic, static_cast<uint8_t*>(d->rgb.p), d->L, m, d->stream), "RGB pack");
+  CK(cudaMemcpyAsync(dst, d->rgb.p, bytes, cudaMemcpyDeviceToHost, d->stream), "RGB read back");
+  CK(cudaStreamSynchronize(d->stream), "RGB sync");
+  return AV1B_OK;
+}
+
+int av1b_get_stats(av1b_decoder* d, av1b_stats* out) {
+  if (!d || !out) return AV1B_ERR_ARG;
+  *out = d->stats;
+  return AV1B_OK;
+}
+
+int av1b_poll_status(av1b_decoder* d, int* status) {
+  if (!d || !status) return AV1B_ERR_ARG;
+  *status = 0;
+  return AV1B_OK;
+}
+
+int av1b_slot_planes_device(av1b_decoder* d, int slot, uint16_t* plane_ptr[3], int32_t stride[3]) {
+  if (!d || !plane_ptr || !stride) return AV1B_ERR_ARG;
+  std::lock_guard<std::mutex> lk(d->mu);
+  const px_t* pic = nullptr;
+  const int rc = picture_of(d, slot, &pic);
+  if (rc) return rc;
+  for (int p = 0; p < 3; ++p) {
+    plane_ptr[p] = const_cast<px_t*>(pic) + d->L.p[p].off;
+    stride[p] = d->L.p[p].stride;
+  }
+  return AV1B_OK;
+}
+
+void* av1b_decoder_stream(av1b_decoder* d) { return d ? d->stream : nullptr; }
+
+const char* av1b_last_error(av1b_decoder* d) { return d ? d->err.c_str() : ""; }
+
+}  // extern "C"

@@ -1,0 +1,851 @@
+/*
+ * kernels.cu - the sm_100a kernels of one frame step.
+ *
+ * Reconstruction runs in two phases. Phase A is everything that reads only
+ * reference pictures: the inter prediction of every inter block (one warp per
+ * 16x8 tile) and then its residual (one warp per transform). Phase B is the
+ * dependency-scheduled rest: intra blocks, inter-intra blocks and intra block
+ * copies, in coding order, by a persistent kernel whose warps claim blocks
+ * from a device queue and wait on the blocks that own the samples they read.
+ * The dependency tracking is the reference planner's owner grid and edge scans
+ * (engine.cpp:719-924), done here on the device: the host never computes a
+ * wave and launches nothing per wave.
+ *
+ * Waiting is safe without a cooperative launch: blocks are claimed in index
+ * order and a block only ever waits on lower indices, each of which was
+ * claimed by a warp that is already running; the lowest unfinished block
+ * therefore always has everything it needs. Every wait is bounded (one second
+ * of globaltimer); on expiry the kernel records AV1B_STATUS_TIMEOUT in the
+ * status word and carries on, and the host fails the frame.
+ */
+#include <cuda_runtime.h>
+
+#include "dev_common.cuh"
+#include "dev_filters.cuh"
+#include "dev_inter.cuh"
+#include "dev_intra.cuh"
+#include "dev_itx.cuh"
+#include "kernels.h"
+
+namespace av1b {
+
+/* ---- helpers --------------------------------------------------------------------- */
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ const px_t* ref_plane(const FrameArgs& a, int slot, int plane) {
+  const px_t* base = slot >= 0 ? a.slot_ptr[slot] : a.cur;
+  return base + a.L.p[plane].off;
+}
+
+/* Owner of the 4x4 (luma) / 2x2 (subsampled chroma) cell holding (x, y). */
+__device__ __forceinline__ int owner_at(const FrameArgs& a, int p, int x, int y) {
+  if (x < 0 || y < 0 || x >= a.L.p[p].grid_w || y >= a.L.p[p].grid_h) return -1;
+  const int sh = a.cell_shift[p];
+  return __ldcg(a.owner[p] + (y >> sh) * a.cell_w[p] + (x >> sh));
+}
+
+/* Builds the resolved inter job of a block. */
+__device__ void make_inter_job(const FrameArgs& a, const BlockRec& b, InterJob* j) {
+  const int p = b.plane;
+  const PlaneGeom& g = a.L.p[p];
+  j->x = b.x;
+  j->y = b.y;
+  j->w = b.w;
+  j->h = b.h;
+  j->plane = p;
+  j->ctx.sub_x = p > 0 ? a.L.ss_x : 0;
+  j->ctx.sub_y = p > 0 ? a.L.ss_y : 0;
+  j->ctx.bitdepth = a.L.bit_depth;
+  if (b.kind == AV1B_U_INTRABC) {
+    /* a block copy reads this frame: the 4-rounded coded size, unscaled */
+    j->ctx.ref_w = ((a.L.p[0].coded_w + 3) & ~3) >> j->ctx.sub_x;
+    j->ctx.ref_h = ((a.L.p[0].coded_h + 3) & ~3) >> j->ctx.sub_y;
+    j->ctx.scale_x = AV1B_SCALE_ONE;
+    j->ctx.scale_y = AV1B_SCALE_ONE;
+  } else {
+    j->ctx.ref_w = g.out_w;
+    j->ctx.ref_h = g.out_h;
+    j->ctx.scale_x = a.scale_x;
+    j->ctx.scale_y = a.scale_y;
+  }
+  j->ref[0] = ref_plane(a, b.ref_slot[0], p);
+  j->ref[1] = ref_plane(a, b.ref_slot[1], p);
+  j->ref_stride = g.stride;
+  for (int r = 0; r < 2; ++r) {
+    j->mv[r][0] = b.mv[r][0];
+    j->mv[r][1] = b.mv[r][1];
+  }
+  j->filt = b.filt;
+  j->filt_v = b.filt_v;
+  j->compound = b.compound;
+  j->w0 = b.w0;
+  j->w1 = b.w1;
+  j->mask_kind = b.mask_kind;
+  j->mask_sign = b.mask_sign;
+  j->wedge_dir = b.wedge_dir;
+  j->wedge_xoff = b.wedge_xoff;
+  j->wedge_yoff = b.wedge_yoff;
+  j->wedge_flip = b.wedge_flip;
+  j->warp[0] = b.warp0;
+  j->warp[1] = b.warp1;
+  j->mask_warp[0] = b.mask_warp0;
+  j->mask_warp[1] = b.mask_warp1;
+  j->model[0] = a.warps + (b.warp_idx[0] >= 0 ? b.warp_idx[0] : 0);
+  j->model[1] = a.warps + (b.warp_idx[1] >= 0 ? b.warp_idx[1] : 0);
+  j->luma_ref[0] = ref_plane(a, b.ref_slot[0], 0);
+  j->luma_ref[1] = ref_plane(a, b.ref_slot[1], 0);
+  j->luma_stride = a.L.p[0].stride;
+  j->luma_x = b.x << (p > 0 ? a.L.ss_x : 0);
+  j->luma_y = b.y << (p > 0 ? a.L.ss_y : 0);
+  j->luma_ref_w = a.L.p[0].out_w;
+  j->luma_ref_h = a.L.p[0].out_h;
+  j->interintra = b.interintra;
+  j->ii_mode = b.ii_mode;
+  j->ii_wedge = b.ii_wedge;
+  j->have_left = b.have_left;
+  j->have_above = b.have_above;
+  j->max_x = g.grid_w - 1;
+  j->max_y = g.grid_h - 1;
+  j->cur = a.cur + g.off + b.y * g.stride + b.x;
+  j->cur_stride = g.stride;
+  j->obmc = a.obmc + b.obmc_first;
+  j->obmc_count = b.obmc_count;
+  for (int k = 0; k < 8; ++k)
+    j->obmc_ref[k] = k < b.obmc_count ? ref_plane(a, a.obmc[b.obmc_first + k].ref_slot, p) : j->ref[0];
+  j->maxv = a.maxv;
+}
+
+/* ---- phase A ------------------------------------------------------------------------ */
+
+/* Owner grid and done flags: one warp per block. */
+__global__ void k_owner(FrameArgs a) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= a.n_blocks) return;
+  const BlockRec b = a.blocks[warp];
+  const int p = b.plane;
+  const int sh = a.cell_shift[p], oc = 1 << sh;
+  const int cx0 = maxi(b.x, 0) >> sh, cy0 = maxi(b.y, 0) >> sh;
+  const int cx1 = mini((b.x + b.w + oc - 1) >> sh, a.cell_w[p]);
+  const int cy1 = mini((b.y + b.h + oc - 1) >> sh, a.cell_h[p]);
+  const int cw = cx1 - cx0;
+  if (cw > 0)
+    for (int k = lane; k < cw * (cy1 - cy0); k += 32)
+      a.owner[p][(cy0 + k / cw) * a.cell_w[p] + cx0 + k % cw] = warp;
+  if (lane == 0 && !b.phase_b) a.done[warp] = a.epoch;
+}
+
+/* Inter prediction of phase A blocks: one warp per 16x8 tile. */
+__global__ void k_inter(FrameArgs a) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= a.n_inter_tiles) return;
+  const int2 t = a.inter_tiles[warp];
+  const BlockRec& b = a.blocks[t.x];
+  InterJob j;
+  make_inter_job(a, b, &j);
+  const int x0 = t.y & 0xffff, y0 = t.y >> 16;
+  const int tw = mini(16, b.w - x0), th = mini(8, b.h - y0);
+  const PlaneGeom& g = a.L.p[b.plane];
+  px_t* dst = a.cur + g.off + (b.y + y0) * g.stride + b.x + x0;
+  for (int k = lane; k < tw * th; k += 32) {
+    const int yy = k / tw, xx = k - yy * tw;
+    int v = inter_core(j, x0 + xx, y0 + yy);
+    v = inter_finish(j, x0 + xx, y0 + yy, v, 0);
+    dst[yy * g.stride + xx] = (px_t)v;
+  }
+}
+
+/* Adds one transform's residual (or a raw residual block) to the picture. */
+template <bool CG>
+__device__ void apply_tx(const FrameArgs& a, const BlockRec& b, const TxRec& tx, int* tmp,
+                         int lane) {
+  const PlaneGeom& g = a.L.p[b.plane];
+  px_t* dst = a.cur + g.off + (b.y + tx.y) * g.stride + b.x + tx.x;
+  if (b.residual_provided) {
+    const int* res = a.residual + tx.coef_off;
+    for (int k = lane; k < tx.w * tx.h; k += 32) {
+      const int yy = k / tx.w, xx = k - yy * tx.w;
+      px_t* q = dst + yy * g.stride + xx;
+      const int old = CG ? (int)__ldcg(q) : (int)*q;
+      *q = (px_t)clampi(old + res[yy * tx.w + xx], 0, a.maxv);
+    }
+    __syncwarp();
+    return;
+  }
+  ItxParams p;
+  p.lw = tx.log2w;
+  p.lh = tx.log2h;
+  p.type = tx.type;
+  p.lossless = b.lossless;
+  p.row_shift = tx.row_shift;
+  p.bitdepth = a.L.bit_depth;
+  itx_warp<CG>(p, a.coef + tx.coef_off, tmp, dst, g.stride, a.maxv, lane);
+}
+
+/* Residual of phase A blocks: one warp per transform. */
+__global__ void k_itx(FrameArgs a) {
+  extern __shared__ int smem[];
+  const int wib = threadIdx.x >> 5;
+  const int warp = blockIdx.x * (blockDim.x >> 5) + wib;
+  const int lane = threadIdx.x & 31;
+  if (warp >= a.n_itx) return;
+  const int2 t = a.itx_jobs[warp];
+  const BlockRec& b = a.blocks[t.x];
+  apply_tx<false>(a, b, a.txs[t.y], smem + wib * 4096, lane);
+}
+
+/* ---- phase B -------------------------------------------------------------------------- */
+
+/* Waits until block `o` is reconstructed. Returns false on timeout. */
+__device__ bool wait_block(const FrameArgs& a, int o) {
+  if (ld_acquire(a.done + o) == a.epoch) return true;
+  const unsigned long long t0 = global_ns();
+  while (ld_acquire(a.done + o) != a.epoch) {
+    /* once any wait of this frame has given up, nothing waits any more: the
+     * frame has failed and the kernel only has to run to its end */
+    if (ld_acquire(reinterpret_cast<const unsigned*>(a.status)) & AV1B_STATUS_TIMEOUT) return false;
+    __nanosleep(100);
+    if (global_ns() - t0 > 1000000000ull) {
+      atomicOr(a.status, AV1B_STATUS_TIMEOUT);
+      return false;
+    }
+  }
+  return true;
+}
+
+/* True when every owner of the cells of [x0, x1] x [y0, y1] precedes `bi` in
+ * coding order (or lies outside the grid): the reference's already_decoded
+ * (engine.cpp:784-793). Warp-collective. */
+__device__ bool decoded_before(const FrameArgs& a, int p, int x0, int x1, int y0, int y1, int bi,
+                               int lane) {
+  const int oc = 1 << a.cell_shift[p];
+  const int xs = x0 & ~(oc - 1), ys = y0 & ~(oc - 1);
+  const int nx = x1 >= xs ? (x1 - xs) / oc + 1 : 0, ny = y1 >= ys ? (y1 - ys) / oc + 1 : 0;
+  bool ok = true;
+  for (int k = lane; k < nx * ny; k += 32) {
+    const int o = owner_at(a, p, xs + (k % nx) * oc, ys + (k / nx) * oc);
+    if (o >= 0 && o >= bi) ok = false;
+  }
+  return __all_sync(0xffffffffu, ok);
+}
+
+/* Waits for the owners of the cells of [x0, x1] x [y0, y1] of plane p that
+ * precede `bi`. Warp-collective. */
+__device__ void wait_rect(const FrameArgs& a, int p, int x0, int x1, int y0, int y1, int bi,
+                          int lane) {
+  const int oc = 1 << a.cell_shift[p];
+  const int xs = x0 & ~(oc - 1), ys = y0 & ~(oc - 1);
+  const int nx = x1 >= xs ? (x1 - xs) / oc + 1 : 0, ny = y1 >= ys ? (y1 - ys) / oc + 1 : 0;
+  for (int k = lane; k < nx * ny; k += 32) {
+    const int o = owner_at(a, p, xs + (k % nx) * oc, ys + (k / nx) * oc);
+    if (o >= 0 && o < bi) wait_block(a, o);
+  }
+  __syncwarp();
+}
+
+/* The persistent dependency-scheduled kernel. Shared memory per warp: three
+ * edge buffers and a 64x64 transform scratch. */
+__global__ void __launch_bounds__(128) k_units(FrameArgs a) {
+  extern __shared__ int smem[];
+  const int wib = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  int* edges = smem + wib * (3 * AV1B_EDGE_LEN + 4096);
+  int* tmp = edges + 3 * AV1B_EDGE_LEN;
+  for (;;) {
+    int u = 0;
+    if (lane == 0) u = atomicAdd(a.queue, 1);
+    u = __shfl_sync(0xffffffffu, u, 0);
+    if (u >= a.n_units) break;
+    const int bi = a.units[u];
+    const BlockRec b = a.blocks[bi];
+    const int p = b.plane;
+    const PlaneGeom& g = a.L.p[p];
+
+    /* availability of the above-right / below-left extensions */
+    int have_ar = b.have_ar, have_bl = b.have_bl;
+    if (b.kind == AV1B_U_INTRA) {
+      if (have_ar == 2)
+        have_ar = b.y > 0 && decoded_before(a, p, b.x + b.w, b.x + 2 * b.w - 1, b.y - 1, b.y - 1,
+                                            bi, lane);
+      if (have_bl == 2)
+        have_bl = b.x > 0 && decoded_before(a, p, b.x - 1, b.x - 1, b.y + b.h, b.y + 2 * b.h - 1,
+                                            bi, lane);
+    } else {
+      have_ar = have_bl = 0;
+    }
+
+    /* dependencies: the edge samples (intra, inter-intra), the source
+     * rectangle (intra block copy) and the co-located luma (CFL) */
+    if (b.kind == AV1B_U_INTRA || b.interintra) {
+      int left_y1 = b.y + b.h - 1, above_x1 = b.x + b.w - 1;
+      if (b.kind == AV1B_U_INTRA && !b.palette) {
+        if (b.mode >= 1 && b.mode <= 8) {
+          const int pangle = kModeAngle[b.mode] + 3 * b.angle_delta;
+          if (pangle < 90 && have_ar) above_x1 = b.x + 2 * b.w - 1;
+          if (pangle > 180 && have_bl) left_y1 = b.y + 2 * b.h - 1;
+        }
+      } else if (b.kind == AV1B_U_INTRA) {
+        above_x1 = b.x - 1;
+        left_y1 = b.y - 1;
+      }
+      const int oc = 1 << a.cell_shift[p];
+      if (left_y1 >= (b.y & ~(oc - 1))) wait_rect(a, p, b.x - 1, b.x - 1, b.y, left_y1, bi, lane);
+      if (above_x1 >= (b.x & ~(oc - 1))) wait_rect(a, p, b.x, above_x1, b.y - 1, b.y - 1, bi, lane);
+      if (above_x1 >= b.x || left_y1 >= b.y)
+        wait_rect(a, p, b.x - 1, b.x - 1, b.y - 1, b.y - 1, bi, lane);
+    }
+    if (b.kind == AV1B_U_INTRABC) {
+      const int sx_ = p > 0 ? a.L.ss_x : 0, sy_ = p > 0 ? a.L.ss_y : 0;
+      const int sx = b.x + (b.mv[0][0] >> (3 + sx_));
+      const int sy = b.y + (b.mv[0][1] >> (3 + sy_));
+      const int x1 = mini(sx + b.w, g.grid_w), y1 = mini(sy + b.h, g.grid_h);
+      if (x1 > maxi(sx, 0) && y1 > maxi(sy, 0))
+        wait_rect(a, p, maxi(sx, 0), x1 - 1, maxi(sy, 0), y1 - 1, bi, lane);
+    }
+    if (b.kind == AV1B_U_INTRA && b.mode == 13 && !b.palette) {
+      wait_rect(a, 0, b.x << a.L.ss_x, ((b.x + b.w - 1) << a.L.ss_x), b.y << a.L.ss_y,
+                ((b.y + b.h - 1) << a.L.ss_y), bi, lane);
+    }
+    __threadfence();
+    __syncwarp();
+
+    px_t* dst = a.cur + g.off + b.y * g.stride + b.x;
+    if (b.kind == AV1B_U_INTRA) {
+      IntraJob j;
+      j.x = b.x;
+      j.y = b.y;
+      j.w = b.w;
+      j.h = b.h;
+      j.mode = b.mode;
+      j.angle = b.angle_delta;
+      j.bitdepth = a.L.bit_depth;
+      j.maxv = a.maxv;
+      j.have_left = b.have_left;
+      j.have_above = b.have_above;
+      j.have_ar = have_ar;
+      j.have_bl = have_bl;
+      j.filter_type = b.filter_type;
+      j.filter_intra = b.fi_mode >= 0;
+      j.fi_mode = b.fi_mode >= 0 ? b.fi_mode : 0;
+      j.cfl_alpha = b.cfl_alpha;
+      j.max_x = g.grid_w - 1;
+      j.max_y = g.grid_h - 1;
+      j.ss_x = a.L.ss_x;
+      j.ss_y = a.L.ss_y;
+      j.palette = b.palette;
+      j.palette_off = b.palette_off;
+      j.palette_stride = b.palette_stride;
+      intra_predict(j, dst, g.stride, a.cur + a.L.p[0].off, a.L.p[0].stride, a.palette_map,
+                    a.palette_colors + 8 * b.palette_color_idx, edges, lane);
+    } else {
+      InterJob j;
+      make_inter_job(a, b, &j);
+      int dc = 0;
+      if (b.interintra && b.ii_mode == 0) dc = ii_dc(j);
+      for (int k = lane; k < b.w * b.h; k += 32) {
+        const int yy = k / b.w, xx = k - yy * b.w;
+        int v = b.kind == AV1B_U_INTRABC ? inter_core<true>(j, xx, yy) : inter_core(j, xx, yy);
+        v = inter_finish(j, xx, yy, v, dc);
+        dst[yy * g.stride + xx] = (px_t)v;
+      }
+    }
+    __syncwarp();
+    for (int t = 0; t < b.tx_count; ++t) apply_tx<true>(a, b, a.txs[b.tx_first + t], tmp, lane);
+
+    /* publish */
+    __threadfence();
+    __syncwarp();
+    if (lane == 0) st_release(a.done + bi, a.epoch);
+  }
+}
+
+/* ---- deblocking ---------------------------------------------------------------------- */
+__global__ void k_deblock(px_t* pic, const DeblockRec* recs, int n, int sharpness, int bd,
+                          int maxv) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= n) return;
+  const DeblockRec r = recs[warp];
+  for (int k = lane; k < r.len; k += 32)
+    deblock_px(pic + r.p_off + k * r.along, r.across, r.level, sharpness, r.filter_size, r.chroma,
+               bd, maxv);
+}
+
+/* ---- CDEF ------------------------------------------------------------------------------ */
+__global__ void k_cdef(const px_t* __restrict__ src, px_t* dst, const CdefRec* recs, int n,
+                       Layout L) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const CdefRec r = recs[i];
+  const int p = r.plane;
+  const bool uv = p > 0;
+  const PlaneGeom& g = L.p[p];
+  const int bd = L.bit_depth, maxv = (1 << bd) - 1;
+  const int cs = bd - 8;
+  const int w = uv ? (8 >> L.ss_x) : 8, h = uv ? (8 >> L.ss_y) : 8;
+  int pri = r.pri << cs, sec = r.sec << cs;
+  const int damping = r.damping + cs - (uv ? 1 : 0);
+  int dir = r.dir;
+  if (dir < 0) {
+    const int lx = uv ? r.x << L.ss_x : r.x, ly = uv ? r.y << L.ss_y : r.y;
+    int ydir = 0, var = 0;
+    cdef_direction(src + L.p[0].off + ly * L.p[0].stride + lx, L.p[0].stride, bd, &ydir, &var);
+    if (uv) {
+      const unsigned char uvd[2][2][8] = {{{0, 1, 2, 3, 4, 5, 6, 7}, {1, 2, 2, 2, 3, 4, 6, 0}},
+                                          {{7, 0, 2, 4, 5, 6, 6, 6}, {0, 1, 2, 3, 4, 5, 6, 7}}};
+      dir = pri == 0 ? 0 : uvd[L.ss_x][L.ss_y][ydir];
+    } else {
+      const int vs = (var >> 6) ? mini(floor_log2(var >> 6), 12) : 0;
+      dir = pri == 0 ? 0 : ydir;
+      pri = var ? ((pri * (4 + vs) + 8) >> 4) : 0;
+    }
+  }
+  const px_t* s = src + g.off + r.y * g.stride + r.x;
+  px_t* d = dst + g.off + r.y * g.stride + r.x;
+  const int pw = g.grid_w, ph = g.grid_h;
+  if (pri == 0 && sec == 0) {
+    for (int i2 = 0; i2 < h && r.y + i2 < ph; ++i2)
+      for (int j = 0; j < w && r.x + j < pw; ++j) d[i2 * g.stride + j] = s[i2 * g.stride + j];
+    return;
+  }
+  const int pri_taps[2][2] = {{4, 2}, {3, 3}};
+  const int sec_taps[2] = {2, 1};
+  const int ts = (pri >> cs) & 1;
+  for (int i2 = 0; i2 < h; ++i2)
+    for (int j = 0; j < w; ++j) {
+      const int x = s[i2 * g.stride + j];
+      int sum = 0, lo = x, hi = x;
+      for (int k = 0; k < 2; ++k)
+        for (int sg = -1; sg <= 1; sg += 2) {
+          int dy, dx;
+          cdef_dir_offsets(dir, k, &dy, &dx);
+          dy *= sg;
+          dx *= sg;
+          int px = r.x + j + dx, py = r.y + i2 + dy;
+          if (px >= 0 && px < pw && py >= 0 && py < ph) {
+            const int v = s[(i2 + dy) * g.stride + j + dx];
+            sum += pri_taps[ts][k] * cdef_constrain(v - x, pri, damping);
+            lo = mini(lo, v);
+            hi = maxi(hi, v);
+          }
+          for (int off = -2; off <= 2; off += 4) {
+            cdef_dir_offsets((dir + off) & 7, k, &dy, &dx);
+            dy *= sg;
+            dx *= sg;
+            px = r.x + j + dx;
+            py = r.y + i2 + dy;
+            if (px >= 0 && px < pw && py >= 0 && py < ph) {
+              const int v = s[(i2 + dy) * g.stride + j + dx];
+              sum += sec_taps[k] * cdef_constrain(v - x, sec, damping);
+              lo = mini(lo, v);
+              hi = maxi(hi, v);
+            }
+          }
+        }
+      if (r.x + j >= pw || r.y + i2 >= ph) continue;
+      d[i2 * g.stride + j] =
+          (px_t)clampi(clampi(x + ((8 + sum - (sum < 0)) >> 4), lo, hi), 0, maxv);
+    }
+}
+
+/* ---- superres ------------------------------------------------------------------------- */
+__global__ void k_upscale(const px_t* __restrict__ src, px_t* dst, Layout L, int maxv) {
+  const int p = blockIdx.z;
+  const PlaneGeom& g = L.p[p];
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= g.out_w || y >= g.out_h) return;
+  int step, initial;
+  superres_params(g.coded_w, g.out_w, &step, &initial);
+  const int sx = -(1 << 14) + initial + x * step;
+  const int px = sx >> 14;
+  const int ph = (sx & ((1 << 14) - 1)) >> 8;
+  const px_t* row = src + g.off + y * g.stride;
+  int sum = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k)
+    sum += (int)row[clampi(px + k - 3, 0, g.coded_w - 1)] * kUpscaleFilter[ph * 8 + k];
+  dst[g.off + y * g.stride + x] = (px_t)clampi(rnd2(sum, 7), 0, maxv);
+}
+
+/* ---- loop restoration --------------------------------------------------------------------- */
+__global__ void k_lr(const px_t* __restrict__ cdef, const px_t* __restrict__ curr, px_t* dst,
+                     Layout L, LrArgs r, int maxv) {
+  const int p = blockIdx.z;
+  if (!r.type[p]) return;
+  const PlaneGeom& g = L.p[p];
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= g.out_w || y >= g.out_h) return;
+  const int sub_y = p > 0 ? L.ss_y : 0;
+  const int us = r.unit_size[p];
+  const int stripe = ((y << sub_y) + 8) / 64;
+  const int s0 = (-8 + stripe * 64) >> sub_y;
+  const int s1 = s0 + (64 >> sub_y) - 1;
+  const int ystart = maxi(s0, 0);
+  const int urow = mini(r.unit_rows[p] - 1, ((((ystart << sub_y) + 8) >> sub_y) / us));
+  const int ucol = mini(r.unit_cols[p] - 1, x / us);
+  const int idx = urow * r.unit_cols[p] + ucol;
+  if (idx >= r.n_units[p]) return;
+  const LrUnitRec u = r.units[p][idx];
+  if (u.type != 1 && u.type != 2) return;
+  LrSrc s;
+  s.cdef = cdef + g.off;
+  s.curr = curr + g.off;
+  s.stride = g.stride;
+  s.w = g.out_w;
+  s.h = g.out_h;
+  s.s0 = s0;
+  s.s1 = s1;
+  const int v = u.type == 1 ? lr_wiener(s, u, L.bit_depth, x, y) : lr_sgr(s, u, L.bit_depth, x, y);
+  dst[g.off + y * g.stride + x] = (px_t)clampi(v, 0, maxv);
+}
+
+/* ---- film grain ------------------------------------------------------------------------------- */
+
+/* Generates the three grain templates (7.18.3.3): Gaussian noise from the LFSR
+ * (every draw independent through the orbit table), then the auto-regressive
+ * filter as a wavefront: sample (x, y) depends on rows above within +-lag
+ * columns and on the lag samples to its left, so t = x + 4y orders it
+ * (lag <= 3). One block; luma first, then both chroma planes together. */
+__global__ void __launch_bounds__(256) k_grain_template(GrainState* gs, GrainParamsDev prm,
+                                                        const uint16_t* orbit,
+                                                        const uint16_t* pos) {
+  const int tid = threadIdx.x;
+  const int bd = prm.bitdepth;
+  const int shift = 12 - bd + prm.grain_scale_shift;
+  const int gmin = -(128 << (bd - 8)), gmax = (256 << (bd - 8)) - 1 - (128 << (bd - 8));
+  const int cw = gs->chroma_w, ch = gs->chroma_h;
+  short* cb = gs->cb;
+  short* cr = gs->cr;
+  /* Gaussian fill */
+  for (int k = tid; k < 82 * 73; k += blockDim.x) {
+    int g = 0;
+    if (prm.num_y_points > 0) {
+      const int st = lfsr_after(orbit, pos, (unsigned)prm.seed & 0xffffu, k + 1);
+      g = kGaussianSequence[(st >> 5) & 2047];
+    }
+    gs->luma[k] = (short)rnd2z(g, shift);
+  }
+  const bool chroma = prm.chroma_scaling_from_luma || prm.num_cb_points > 0 || prm.num_cr_points > 0;
+  if (chroma) {
+    const bool acb = prm.num_cb_points > 0 || prm.chroma_scaling_from_luma;
+    const bool acr = prm.num_cr_points > 0 || prm.chroma_scaling_from_luma;
+    for (int k = tid; k < cw * ch; k += blockDim.x) {
+      int g0 = 0, g1 = 0;
+      if (acb) g0 = kGaussianSequence[(lfsr_after(orbit, pos, ((unsigned)prm.seed ^ 0xb524u) & 0xffffu, k + 1) >> 5) & 2047];
+      if (acr) g1 = kGaussianSequence[(lfsr_after(orbit, pos, ((unsigned)prm.seed ^ 0x49d8u) & 0xffffu, k + 1) >> 5) & 2047];
+      cb[k] = (short)rnd2z(g0, shift);
+      cr[k] = (short)rnd2z(g1, shift);
+    }
+  }
+  __syncthreads();
+  const int lag = prm.ar_coeff_lag;
+  const int arshift = prm.ar_coeff_shift_minus_6 + 6;
+  /* luma AR filter */
+  if (prm.num_y_points > 0) {
+    const int W = 82, H = 73;
+    const int tmax = (W - 4) + 4 * (H - 1);
+    for (int t = 3 + 4 * 3; t <= tmax; ++t) {
+      for (int y = 3 + tid; y < H; y += blockDim.x) {
+        const int x = t - 4 * y;
+        if (x < 3 || x >= W - 3) continue;
+        int sum = 0, pos_ = 0;
+        for (int dr = -lag; dr <= 0; ++dr)
+          for (int dc = -lag; dc <= lag; ++dc) {
+            if (dr == 0 && dc == 0) goto done_l;
+            sum += gs->luma[(y + dr) * W + x + dc] * prm.ar_y[pos_];
+            ++pos_;
+          }
+      done_l:
+        gs->luma[y * W + x] = (short)clampi(gs->luma[y * W + x] + rnd2z(sum, arshift), gmin, gmax);
+      }
+      __syncthreads();
+    }
+  }
+  if (chroma) {
+    const int sx = prm.ss_x, sy = prm.ss_y;
+    const int tmax = (cw - 4) + 4 * (ch - 1);
+    for (int t = 3 + 4 * 3; t <= tmax; ++t) {
+      for (int k = tid; k < 2 * ch; k += blockDim.x) {
+        const int plane = k & 1, y = k >> 1;
+        if (y < 3) continue;
+        const int x = t - 4 * y;
+        if (x < 3 || x >= cw - 3) continue;
+        short* gp = plane ? cr : cb;
+        const int* co = plane ? prm.ar_cr : prm.ar_cb;
+        int sum = 0, pos_ = 0;
+        for (int dr = -lag; dr <= 0; ++dr)
+          for (int dc = -lag; dc <= lag; ++dc) {
+            if (dr == 0 && dc == 0) {
+              if (prm.num_y_points > 0) {
+                const int lx = ((x - 3) << sx) + 3, ly = ((y - 3) << sy) + 3;
+                int acc = 0;
+                for (int i = 0; i <= sy; ++i)
+                  for (int j = 0; j <= sx; ++j) acc += gs->luma[(ly + i) * 82 + lx + j];
+                sum += rnd2z(acc, sx + sy) * co[pos_];
+              }
+              goto done_c;
+            }
+            sum += gp[(y + dr) * cw + x + dc] * co[pos_];
+            ++pos_;
+          }
+      done_c:
+        gp[y * cw + x] = (short)clampi(gp[y * cw + x] + rnd2z(sum, arshift), gmin, gmax);
+      }
+      __syncthreads();
+    }
+  }
+}
+
+/* The stripe value of plane `p` at (row, col) of stripe `s` (7.18.3.5, the
+ * horizontal half): the grain block that covers the column, blended with the
+ * previous block at the two (one for subsampled chroma) overlap columns. */
+__device__ int grain_stripe(const GrainState* gs, const short* grain, int src_w, int sub_x, int sub_y,
+                            int s, int row, int col, const uint16_t* orbit, const uint16_t* pos,
+                            int gmin, int gmax) {
+  unsigned st0 = (unsigned)gs->seed & 0xffffu;
+  st0 ^= (unsigned)(((s * 37 + 178) & 255) << 8);
+  st0 ^= (unsigned)((s * 173 + 105) & 255);
+  st0 &= 0xffffu;
+  const int bw_log = sub_x ? 4 : 5;
+  const int k = col >> bw_log;
+  const int j = col & ((1 << bw_log) - 1);
+  auto sample = [&](int blk, int jj) {
+    const int r = (lfsr_after(orbit, pos, st0, blk + 1) >> 8) & 255;
+    const int ox = r >> 4, oy = r & 15;
+    const int src_x = sub_x ? 6 + ox : 9 + ox * 2;
+    const int src_y = sub_y ? 6 + oy : 9 + oy * 2;
+    return (int)grain[(src_y + row) * src_w + src_x + jj];
+  };
+  int g = sample(k, j);
+  if (gs->overlap && k > 0) {
+    if (!sub_x && j < 2) {
+      const int old = sample(k - 1, j + 32);
+      g = clampi(rnd2z(j == 0 ? old * 27 + g * 17 : old * 17 + g * 27, 5), gmin, gmax);
+    } else if (sub_x && j == 0) {
+      const int old = sample(k - 1, 16);
+      g = clampi(rnd2z(old * 23 + g * 22, 5), gmin, gmax);
+    }
+  }
+  return g;
+}
+
+/* Film grain blend, out of place: `src` is the decoded picture (luma read
+ * before any grain), `dst` gets the output picture. One thread per sample. */
+__global__ void k_grain_blend(const px_t* __restrict__ src, px_t* dst, Layout L,
+                              const GrainState* gs, const uint16_t* orbit, const uint16_t* pos) {
+  const int p = blockIdx.z;
+  const PlaneGeom& g = L.p[p];
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= g.out_w || y >= g.out_h) return;
+  const int idx = g.off + y * g.stride + x;
+  const int orig = src[idx];
+  const int bd = gs->bitdepth;
+  int out = orig;
+  bool active;
+  if (p == 0) active = gs->num_points[0] > 0;
+  else active = gs->chroma_from_luma || gs->num_points[p] > 0;
+  if (active) {
+    const int sub_x = p ? L.ss_x : 0, sub_y = p ? L.ss_y : 0;
+    const int gmin = -(128 << (bd - 8)), gmax = (256 << (bd - 8)) - 1 - (128 << (bd - 8));
+    const short* grain = p == 0 ? gs->luma : (p == 1 ? gs->cb : gs->cr);
+    const int src_w = p == 0 ? 82 : gs->chroma_w;
+    /* vertical half: stripes of 32 (16) rows, blended with the stripe above */
+    const int sh = 5 - sub_y;
+    const int s = y >> sh, row = y - (s << sh);
+    int n = grain_stripe(gs, grain, src_w, sub_x, sub_y, s, row, x, orbit, pos, gmin, gmax);
+    if (gs->overlap && s > 0) {
+      if (!sub_y && row < 2) {
+        const int old = grain_stripe(gs, grain, src_w, sub_x, sub_y, s - 1, row + 32, x, orbit, pos,
+                                     gmin, gmax);
+        n = clampi(rnd2z(row == 0 ? old * 27 + n * 17 : old * 17 + n * 27, 5), gmin, gmax);
+      } else if (sub_y && row == 0) {
+        const int old = grain_stripe(gs, grain, src_w, sub_x, sub_y, s - 1, 16, x, orbit, pos, gmin,
+                                     gmax);
+        n = clampi(rnd2z(old * 23 + n * 22, 5), gmin, gmax);
+      }
+    }
+    int index;
+    if (p == 0) {
+      index = orig;
+    } else {
+      const PlaneGeom& gl = L.p[0];
+      const int ly = y << L.ss_y, lx = x << L.ss_x;
+      const int nx = lx + 1 < gl.out_w ? lx + 1 : gl.out_w - 1;
+      const int l0 = src[gl.off + ly * gl.stride + lx];
+      int avg = l0;
+      if (L.ss_x) avg = rnd2z(l0 + src[gl.off + ly * gl.stride + nx], 1);
+      if (gs->chroma_from_luma) {
+        index = avg;
+      } else {
+        const int comb = avg * (gs->luma_mult[p] - 128) + orig * (gs->mult[p] - 128);
+        index = clampi((comb >> 6) + (gs->offset[p] - 256) * (1 << (bd - 8)), 0, (1 << bd) - 1);
+      }
+    }
+    const int scaled = rnd2z(grain_scale_lut(gs->lut[p], index, bd) * n, gs->scaling_shift);
+    out = clampi(orig + scaled, gs->min_value, p == 0 ? gs->max_luma : gs->max_chroma);
+  }
+  dst[idx] = (px_t)out;
+}
+
+/* ---- output packing ---------------------------------------------------------------------------- */
+
+/* NV12: one thread per 8 output bytes of a `pitch`-byte row; rows [0, h) are
+ * luma, then (h + 1) / 2 rows of interleaved Cb, Cr. Padding is zero.
+ *
+ * The reference packs a copy of the picture gathered row by row at the
+ * *coded* width into a display-sized frame that starts out zero
+ * (cpu_backend.cpp:576-584), so for a superres frame every sample right of the
+ * coded width packs as 0. This kernel reproduces that byte for byte. */
+__global__ void k_nv12(const px_t* __restrict__ pic, uint8_t* out, Layout L, int pitch) {
+  const int row = blockIdx.y;
+  const int x0 = (blockIdx.x * blockDim.x + threadIdx.x) * 8;
+  if (x0 >= pitch) return;
+  const int w = L.p[0].out_w, h = L.p[0].out_h;
+  const int shift = L.bit_depth - 8;
+  uint8_t v[8];
+  if (row < h) {
+    const px_t* src = pic + L.p[0].off + row * L.p[0].stride;
+    const int lim = mini(w, L.p[0].coded_w);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = x0 + k < lim ? (uint8_t)(src[x0 + k] >> shift) : 0;
+  } else {
+    const int cr = row - h;
+    const int cw = (w + 1) >> 1;
+    const int ccw = L.p[1].coded_w;
+    const px_t* u = pic + L.p[1].off + cr * L.p[1].stride;
+    const px_t* vv = pic + L.p[2].off + cr * L.p[2].stride;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int x = x0 + k;
+      v[k] = (x < 2 * cw && (x >> 1) < ccw) ? (uint8_t)(((x & 1) ? vv[x >> 1] : u[x >> 1]) >> shift) : 0;
+    }
+  }
+  uint8_t* d = out + (size_t)row * pitch + x0;
+  if (x0 + 8 <= pitch && ((reinterpret_cast<uintptr_t>(d) & 7) == 0)) {
+    uint2 pk;
+    pk.x = v[0] | (v[1] << 8) | (v[2] << 16) | ((unsigned)v[3] << 24);
+    pk.y = v[4] | (v[5] << 8) | (v[6] << 16) | ((unsigned)v[7] << 24);
+    *reinterpret_cast<uint2*>(d) = pk;
+  } else {
+    for (int k = 0; k < 8 && x0 + k < pitch; ++k) d[k] = v[k];
+  }
+}
+
+__global__ void k_rgb(const px_t* __restrict__ pic, uint8_t* out, Layout L, RgbArgs m) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  const int w = L.p[0].out_w;
+  if (x >= w) return;
+  /* zero right of the coded width, as in the reference's gathered frame */
+  const int yy = x < L.p[0].coded_w ? pic[L.p[0].off + y * L.p[0].stride + x] : 0;
+  const int cx = x >> L.ss_x;
+  const int ci = (y >> L.ss_y) * L.p[1].stride + cx;
+  const int uu = cx < L.p[1].coded_w ? pic[L.p[1].off + ci] : 0;
+  const int vv = cx < L.p[2].coded_w ? pic[L.p[2].off + ci] : 0;
+  const int r = (m.m[0] * yy + m.m[1] * vv + m.o[0]) >> 16;
+  const int g = (m.m[2] * yy + m.m[3] * uu + m.m[4] * vv + m.o[1]) >> 16;
+  const int b = (m.m[5] * yy + m.m[6] * uu + m.o[2]) >> 16;
+  uint8_t* d = out + ((size_t)y * w + x) * 3;
+  d[0] = (uint8_t)clampi(r, 0, 255);
+  d[1] = (uint8_t)clampi(g, 0, 255);
+  d[2] = (uint8_t)clampi(b, 0, 255);
+}
+
+/* ---- launchers ------------------------------------------------------------------------------------ */
+static inline unsigned cdiv(long long a, long long b) { return (unsigned)((a + b - 1) / b); }
+
+cudaError_t launch_recon(const FrameArgs& a, int n_sm, cudaStream_t s, int* launches) {
+  int n = 0;
+  if (a.n_blocks > 0) {
+    k_owner<<<cdiv((long long)a.n_blocks * 32, 256), 256, 0, s>>>(a);
+    ++n;
+  }
+  if (a.n_inter_tiles > 0) {
+    k_inter<<<cdiv((long long)a.n_inter_tiles * 32, 256), 256, 0, s>>>(a);
+    ++n;
+  }
+  if (a.n_itx > 0) {
+    k_itx<<<cdiv(a.n_itx, 4), 128, 4 * 4096 * sizeof(int), s>>>(a);
+    ++n;
+  }
+  if (a.n_units > 0) {
+    const size_t smem = 4 * (3 * AV1B_EDGE_LEN + 4096) * sizeof(int);
+    k_units<<<2 * n_sm, 128, smem, s>>>(a);
+    ++n;
+  }
+  if (launches) *launches += n;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_deblock(px_t* pic, const DeblockRec* recs, int n, int sharpness, int bd, int maxv,
+                           cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_deblock<<<cdiv((long long)n * 32, 256), 256, 0, s>>>(pic, recs, n, sharpness, bd, maxv);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cdef(const px_t* src, px_t* dst, const CdefRec* recs, int n, const Layout& L,
+                        cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_cdef<<<cdiv(n, 128), 128, 0, s>>>(src, dst, recs, n, L);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_upscale(const px_t* src, px_t* dst, const Layout& L, int maxv, cudaStream_t s) {
+  const int wmax = L.p[0].out_w, hmax = L.p[0].out_h;
+  k_upscale<<<dim3(cdiv(wmax, 128), hmax, 3), 128, 0, s>>>(src, dst, L, maxv);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_lr(const px_t* cdef, const px_t* curr, px_t* dst, const Layout& L,
+                      const LrArgs& r, int maxv, cudaStream_t s) {
+  k_lr<<<dim3(cdiv(L.p[0].out_w, 128), L.p[0].out_h, 3), 128, 0, s>>>(cdef, curr, dst, L, r, maxv);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_grain(const px_t* src, px_t* dst, const Layout& L, GrainState* gs,
+                         const GrainParamsDev& prm, const uint16_t* orbit, const uint16_t* pos,
+                         cudaStream_t s) {
+  k_grain_template<<<1, 256, 0, s>>>(gs, prm, orbit, pos);
+  k_grain_blend<<<dim3(cdiv(L.p[0].out_w, 128), L.p[0].out_h, 3), 128, 0, s>>>(src, dst, L, gs,
+                                                                                 orbit, pos);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_nv12(const px_t* pic, uint8_t* out, const Layout& L, int pitch, cudaStream_t s) {
+  const int rows = L.p[0].out_h + (L.p[0].out_h + 1) / 2;
+  k_nv12<<<dim3(cdiv(cdiv(pitch, 8), 128), rows), 128, 0, s>>>(pic, out, L, pitch);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rgb(const px_t* pic, uint8_t* out, const Layout& L, const RgbArgs& m,
+                       cudaStream_t s) {
+  k_rgb<<<dim3(cdiv(L.p[0].out_w, 128), L.p[0].out_h), 128, 0, s>>>(pic, out, L, m);
+  return cudaGetLastError();
+}
+
+cudaError_t set_kernel_attributes() {
+  cudaError_t e = cudaFuncSetAttribute(k_units, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       4 * (3 * AV1B_EDGE_LEN + 4096) * (int)sizeof(int));
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_itx, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              4 * 4096 * (int)sizeof(int));
+}
+
+}  // namespace av1b

@@ -1,0 +1,84 @@
+/*
+ * kernels.h - the argument blocks of the frame-step kernels and their
+ * launchers (kernels.cu). Host code fills these and launches on its stream.
+ */
+#ifndef AV1B_KERNELS_H
+#define AV1B_KERNELS_H
+
+#include <cuda_runtime.h>
+
+#include "dev_common.cuh"
+#include "dev_filters.cuh"
+
+namespace av1b {
+
+#define AV1B_STATUS_TIMEOUT 1   /* a dependency wait gave up */
+
+/* Everything the reconstruction kernels read, by value. */
+struct FrameArgs {
+  Layout L;
+  px_t* cur;                    /* the picture being reconstructed */
+  px_t* const* slot_ptr;        /* device array: base of each reference slot */
+  const BlockRec* blocks;
+  int n_blocks;
+  const TxRec* txs;
+  const ObmcRec* obmc;
+  const WarpRec* warps;
+  const int* coef;
+  const int* residual;
+  const uint8_t* palette_map;
+  const int* palette_colors;    /* 8 per palette block */
+  int* owner[3];
+  int cell_w[3], cell_h[3], cell_shift[3];
+  unsigned* done;
+  unsigned epoch;
+  const int* units;             /* phase B block indices, coding order */
+  int n_units;
+  unsigned* queue;
+  const int2* inter_tiles;      /* phase A: (block, x0 | y0 << 16) */
+  int n_inter_tiles;
+  const int2* itx_jobs;         /* phase A: (block, transform) */
+  int n_itx;
+  int* status;
+  int maxv;
+  int scale_x, scale_y;
+};
+
+struct LrArgs {
+  int type[3];                  /* non-zero: the plane is restored */
+  int unit_size[3], unit_rows[3], unit_cols[3], n_units[3];
+  const LrUnitRec* units[3];
+};
+
+/* The film grain parameters the template kernel reads. */
+struct GrainParamsDev {
+  int seed, bitdepth, ss_x, ss_y;
+  int num_y_points, num_cb_points, num_cr_points, chroma_scaling_from_luma;
+  int ar_coeff_lag, ar_coeff_shift_minus_6, grain_scale_shift;
+  int ar_y[24], ar_cb[25], ar_cr[25];
+};
+
+struct RgbArgs {
+  int m[8];
+  int o[3];
+};
+
+cudaError_t set_kernel_attributes();
+cudaError_t launch_recon(const FrameArgs& a, int n_sm, cudaStream_t s, int* launches);
+cudaError_t launch_deblock(px_t* pic, const DeblockRec* recs, int n, int sharpness, int bd,
+                           int maxv, cudaStream_t s);
+cudaError_t launch_cdef(const px_t* src, px_t* dst, const CdefRec* recs, int n, const Layout& L,
+                        cudaStream_t s);
+cudaError_t launch_upscale(const px_t* src, px_t* dst, const Layout& L, int maxv, cudaStream_t s);
+cudaError_t launch_lr(const px_t* cdef, const px_t* curr, px_t* dst, const Layout& L,
+                      const LrArgs& r, int maxv, cudaStream_t s);
+cudaError_t launch_grain(const px_t* src, px_t* dst, const Layout& L, GrainState* gs,
+                         const GrainParamsDev& prm, const uint16_t* orbit, const uint16_t* pos,
+                         cudaStream_t s);
+cudaError_t launch_nv12(const px_t* pic, uint8_t* out, const Layout& L, int pitch, cudaStream_t s);
+cudaError_t launch_rgb(const px_t* pic, uint8_t* out, const Layout& L, const RgbArgs& m,
+                       cudaStream_t s);
+
+}  // namespace av1b
+
+#endif

@@ -57,6 +57,8 @@ enum Tool : int {
   kToolLossless = 1 << 13,
   kToolResidual = 1 << 14,   /* residual_provided blocks                  */
   kToolEdgeVariants = 1 << 15, /* filter_type and sharpness variations    */
+  kToolNoDeblock = 1 << 16,  /* leave the deblocking edge list empty      */
+  kToolNoCdef = 1 << 17,     /* leave the CDEF block list empty           */
 };
 
 constexpr int kToolsAll = kToolTx64 | kToolAllTypes | kToolCfl | kToolPalette |
@@ -114,6 +116,8 @@ class Generator {
       for (int x = 0; x < grid_w[0]; x += P.sb) partition(x, y, P.sb);
     deblock_edges();
     cdef_blocks();
+    if (P.tools & kToolNoDeblock) f->deblock.clear();
+    if (P.tools & kToolNoCdef) f->cdef.clear();
     if (P.tools & kToolLr) restoration();
     if (P.tools & kToolGrain) film_grain();
   }
@@ -639,14 +643,14 @@ class Generator {
       for (auto& u : f->restoration[p]) {
         std::memset(&u, 0, sizeof(u));
         if (rng.chance(1, 2)) {
-          u.type = 1;
+          u.type = 2; /* RESTORE_WIENER in the reference's numbering (av1gpu.hpp:372-377) */
           for (int pass = 0; pass < 2; ++pass) {
             u.wiener[pass][0] = p ? 0 : rng.range(-5, 10);
             u.wiener[pass][1] = rng.range(-23, 8);
             u.wiener[pass][2] = rng.range(-17, 46);
           }
         } else {
-          u.type = 2;
+          u.type = 3; /* RESTORE_SGRPROJ */
           u.sgr_set = rng.range(0, 15);
           u.sgr_xqd[0] = rng.range(-96, 31);
           u.sgr_xqd[1] = rng.range(-32, 95);

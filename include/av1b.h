@@ -25,6 +25,12 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#if defined(__GNUC__)
+#define AV1B_API __attribute__((visibility("default")))
+#else
+#define AV1B_API
+#endif
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -161,16 +167,16 @@ typedef struct av1b_decoder av1b_decoder;
  * A test fixture, a file, or a process boundary carries a frame as one byte
  * buffer. av1b_syntax_view points a view at such a buffer without copying. The
  * buffer must stay alive and unmodified while the view is used. */
-int av1b_syntax_view(const uint8_t* blob, size_t len, av1b_frame_syntax* out);
+AV1B_API int av1b_syntax_view(const uint8_t* blob, size_t len, av1b_frame_syntax* out);
 
 /* --- decoder lifetime: Decoder::create (engine.cpp:1509-1558) -------------- */
 /* `device` is the CUDA ordinal. `hbm_budget_bytes` caps what the decoder may
  * allocate (0: no cap). A missing device is an error (AV1B_ERR_NO_DEVICE):
  * there is no CPU path in this library. */
-int av1b_decoder_create(int device, size_t hbm_budget_bytes, av1b_decoder** out);
-int av1b_decoder_destroy(av1b_decoder* dec);
+AV1B_API int av1b_decoder_create(int device, size_t hbm_budget_bytes, av1b_decoder** out);
+AV1B_API int av1b_decoder_destroy(av1b_decoder* dec);
 /* Decoder::reset (engine.cpp:65-71): drops every slot. */
-int av1b_decoder_reset(av1b_decoder* dec);
+AV1B_API int av1b_decoder_reset(av1b_decoder* dec);
 
 /* --- decode: Decoder::decode_reference / decode (av1gpu.hpp:635-636, 733) --
  * Decodes `syntax` and keeps the picture resident in a reference slot when
@@ -178,49 +184,57 @@ int av1b_decoder_reset(av1b_decoder* dec);
  * null (no read back); otherwise the display picture, film grain included, is
  * copied into the caller's planes. `error` (nullable, `error_len` bytes)
  * receives a message on failure. */
-int av1b_decode(av1b_decoder* dec, const av1b_frame_syntax* syntax, int keep_reference,
+AV1B_API int av1b_decode(av1b_decoder* dec, const av1b_frame_syntax* syntax, int keep_reference,
                 const av1b_planes* out, int* out_slot, char* error, size_t error_len);
 
+/* The same for a serialized frame (see av1b_syntax_view). */
+AV1B_API int av1b_decode_blob(av1b_decoder* dec, const uint8_t* blob, size_t len, int keep_reference,
+                     const av1b_planes* out, int* out_slot, char* error, size_t error_len);
+
 /* Decoder::reserve_reference / decode_reference_reserved (av1gpu.hpp:645-661). */
-int av1b_reserve_reference(av1b_decoder* dec, int* out_slot);
-int av1b_decode_reserved(av1b_decoder* dec, const av1b_frame_syntax* syntax, int slot,
+AV1B_API int av1b_reserve_reference(av1b_decoder* dec, int* out_slot);
+AV1B_API int av1b_decode_reserved(av1b_decoder* dec, const av1b_frame_syntax* syntax, int slot,
                          const av1b_planes* out, char* error, size_t error_len);
 
 /* Decoder::release_reference (av1gpu.hpp:736). */
-int av1b_release_reference(av1b_decoder* dec, int slot);
+AV1B_API int av1b_release_reference(av1b_decoder* dec, int slot);
 
 /* Decoder::to_nv12 (av1gpu.hpp:745-746): packs `slot` on the device into
  * `pitch`-byte rows and copies the bytes to `dst` (host, `dst_len` bytes).
  * The slot of the frame decoded last packs the picture after film grain; an
  * older slot packs its stored picture, which is the one before film grain
  * (the reference CPU backend's gather(), cpu_backend.cpp:557-570). */
-int av1b_to_nv12(av1b_decoder* dec, int slot, size_t pitch, uint8_t* dst, size_t dst_len);
+AV1B_API int av1b_to_nv12(av1b_decoder* dec, int slot, size_t pitch, uint8_t* dst, size_t dst_len);
 /* Same, but `dst` is device memory: the zero-copy end of the path. */
-int av1b_to_nv12_device(av1b_decoder* dec, int slot, size_t pitch, void* dst_device,
+AV1B_API int av1b_to_nv12_device(av1b_decoder* dec, int slot, size_t pitch, void* dst_device,
                         size_t dst_len);
 /* The byte count to_nv12 produces (factory.cpp:236-244's nv12_buffer_size):
  * 0 for a frame that is not 4:2:0, an odd pitch or a pitch below a chroma row. */
-size_t av1b_nv12_size(int width, int height, int ss_x, int ss_y, size_t pitch);
+AV1B_API size_t av1b_nv12_size(int width, int height, int ss_x, int ss_y, size_t pitch);
 
 /* Decoder::to_rgb (av1gpu.hpp:739-740): RGB24, width*height*3 bytes. */
-int av1b_to_rgb(av1b_decoder* dec, int slot, int matrix, int range, uint8_t* dst,
+AV1B_API int av1b_to_rgb(av1b_decoder* dec, int slot, int matrix, int range, uint8_t* dst,
                 size_t dst_len);
 
 /* Decoder::stats (av1gpu.hpp:630). */
-int av1b_get_stats(av1b_decoder* dec, av1b_stats* out);
+AV1B_API int av1b_get_stats(av1b_decoder* dec, av1b_stats* out);
 
 /* The device status word: non-zero after a device-side wait gave up or a
  * bounds check refused an access. Reading clears it. */
-int av1b_poll_status(av1b_decoder* dec, int* status);
+AV1B_API int av1b_poll_status(av1b_decoder* dec, int* status);
 
 /* Device pointer and layout of a slot's planes (for callers that hand the
  * picture on without a host copy). */
-int av1b_slot_planes_device(av1b_decoder* dec, int slot, uint16_t* plane_ptr[3],
+AV1B_API int av1b_slot_planes_device(av1b_decoder* dec, int slot, uint16_t* plane_ptr[3],
                             int32_t stride[3]);
+
+/* The message of the last failed call on this decoder (empty if none). The
+ * pointer stays valid until the next call on the decoder. */
+AV1B_API const char* av1b_last_error(av1b_decoder* dec);
 
 /* CUDA stream the decoder runs on (a cudaStream_t), so a caller can order its
  * own work after a decode without a host synchronisation. */
-void* av1b_decoder_stream(av1b_decoder* dec);
+AV1B_API void* av1b_decoder_stream(av1b_decoder* dec);
 
 /* --- synthetic input -------------------------------------------------------
  * The seeded synthetic FrameSyntax the benchmarks and tests decode. `config`
@@ -229,16 +243,16 @@ void* av1b_decoder_stream(av1b_decoder* dec);
  * reference_slots hold frame *distances* (1 = the previous frame), which the
  * caller rewrites into its own slot ids with av1b_blob_set_refs. The buffer is
  * owned by the library: release it with av1b_blob_free. */
-int av1b_synth_frame(int config, int scale, uint64_t seed, int frame_index,
+AV1B_API int av1b_synth_frame(int config, int scale, uint64_t seed, int frame_index,
                      uint8_t** blob, size_t* len);
-int av1b_synth_frame_ex(int width, int height, int coded_width, int bit_depth, int sb_size,
+AV1B_API int av1b_synth_frame_ex(int width, int height, int coded_width, int bit_depth, int sb_size,
                         int tools, uint64_t seed, int frame_index, int key_interval,
                         uint8_t** blob, size_t* len);
-void av1b_blob_free(uint8_t* blob);
+AV1B_API void av1b_blob_free(uint8_t* blob);
 /* Rewrites the reference slot list of a serialized frame in place. */
-int av1b_blob_set_refs(uint8_t* blob, size_t len, const int32_t* slots, int n);
+AV1B_API int av1b_blob_set_refs(uint8_t* blob, size_t len, const int32_t* slots, int n);
 /* Reads the reference slot list (distances for a synthetic frame). */
-int av1b_blob_get_refs(const uint8_t* blob, size_t len, int32_t* slots, int max_n);
+AV1B_API int av1b_blob_get_refs(const uint8_t* blob, size_t len, int32_t* slots, int max_n);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,124 @@
+"""The oracle, for the tests: the reference's own CPU backend (built by
+oracle/Makefile into oracle/_ref/libav1ref.so) behind a small Python class
+that mirrors av1ongpu_b200.Decoder. Test infrastructure only."""
+import ctypes
+import os
+
+import numpy as np
+
+import av1ongpu_b200 as av1b
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF_LIB = os.path.join(ROOT, 'oracle', '_ref', 'libav1ref.so')
+_ref = None
+
+
+def available():
+    return os.path.exists(REF_LIB)
+
+
+def ref_lib():
+    global _ref
+    if _ref is None:
+        L = ctypes.CDLL(REF_LIB)
+        L.av1ref_create.restype = ctypes.c_void_p
+        L.av1ref_destroy.argtypes = [ctypes.c_void_p]
+        L.av1ref_decode.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int,
+                                    ctypes.c_void_p, ctypes.c_size_t]
+        L.av1ref_error.argtypes = [ctypes.c_void_p]
+        L.av1ref_error.restype = ctypes.c_char_p
+        L.av1ref_release.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.av1ref_to_nv12.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t, ctypes.c_void_p,
+                                     ctypes.c_size_t]
+        L.av1ref_to_rgb.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                    ctypes.c_void_p, ctypes.c_size_t]
+        L.av1ref_set_threads.argtypes = [ctypes.c_int]
+        L.av1ref_max_threads.restype = ctypes.c_int
+        L.av1ref_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                                   ctypes.POINTER(ctypes.c_int)]
+        L.av1ref_itx.argtypes = [ctypes.c_int] * 6 + [ctypes.c_void_p, ctypes.c_void_p]
+        _ref = L
+    return _ref
+
+
+class RefDecoder:
+    def __init__(self):
+        self.h = ref_lib().av1ref_create()
+        if not self.h:
+            raise RuntimeError('oracle decoder creation failed')
+
+    def __del__(self):
+        if getattr(self, 'h', None):
+            ref_lib().av1ref_destroy(self.h)
+            self.h = None
+
+    def decode(self, blob, keep=True, read_back=True):
+        w, _cw, h, _bd, sx, sy = blob.header
+        shapes = av1b.plane_shapes(w, h, sx, sy)
+        total = sum(a * b for a, b in shapes)
+        out = np.empty(total, dtype=np.uint16) if read_back else None
+        slot = ref_lib().av1ref_decode(self.h, blob.ptr, blob.size, 1 if keep else 0,
+                                       out.ctypes.data if out is not None else None,
+                                       total if out is not None else 0)
+        if slot < -1:
+            raise RuntimeError('oracle decode failed: %s' % ref_lib().av1ref_error(self.h).decode())
+        planes = None
+        if out is not None:
+            planes, pos = [], 0
+            for s in shapes:
+                n = s[0] * s[1]
+                planes.append(out[pos:pos + n].reshape(s))
+                pos += n
+        return slot, planes
+
+    def release_reference(self, slot):
+        ref_lib().av1ref_release(self.h, slot)
+
+    def to_nv12(self, slot, pitch, width, height):
+        n = av1b.nv12_size(width, height, 1, 1, pitch)
+        out = np.empty(max(n, 1), dtype=np.uint8)
+        got = ref_lib().av1ref_to_nv12(self.h, slot, pitch, out.ctypes.data, out.size)
+        if got < 0:
+            raise RuntimeError('oracle to_nv12 failed: %s' % ref_lib().av1ref_error(self.h).decode())
+        return out[:got]
+
+    def to_rgb(self, slot, matrix, rng, width, height):
+        out = np.empty(width * height * 3, dtype=np.uint8)
+        got = ref_lib().av1ref_to_rgb(self.h, slot, matrix, rng, out.ctypes.data, out.size)
+        if got < 0:
+            raise RuntimeError('oracle to_rgb failed')
+        return out[:got]
+
+
+def fnv1a64(arr):
+    """FNV-1a 64 over the bytes of an array (the hash the reference's stream
+    tests use, av1gpu_decode.cpp:133-140)."""
+    data = np.ascontiguousarray(arr).view(np.uint8)
+    h = 0xcbf29ce484222325
+    # vectorised in chunks: fold bytes sequentially (exact FNV-1a)
+    for b in data.tobytes():
+        h ^= b
+        h = (h * 0x100000001b3) & 0xFFFFFFFFFFFFFFFF
+    return h
+
+
+class Stream:
+    """Decodes a synthetic stream frame by frame with one decoder, mapping the
+    generator's reference distances to that decoder's slots and releasing
+    slots that no later frame can reference."""
+
+    def __init__(self, dec, max_refs=3):
+        self.dec = dec
+        self.slots = {}
+        self.max_refs = max_refs
+
+    def decode(self, index, blob, keep=True, read_back=True):
+        dists = blob.get_refs()
+        blob.set_refs([self.slots[index - d] for d in dists])
+        slot, planes = self.dec.decode(blob, keep=keep, read_back=read_back)
+        blob.set_refs(dists)
+        if keep:
+            self.slots[index] = slot
+        for k in [k for k in self.slots if k <= index - self.max_refs]:
+            self.dec.release_reference(self.slots.pop(k))
+        return slot, planes
