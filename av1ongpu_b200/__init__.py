@@ -67,6 +67,17 @@ _SIGNATURES = {
                                         ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.c_char_p,
                                         ctypes.c_size_t]),
     'av1b_reserve_reference': (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
+    'av1b_plan_frame': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
+    'av1b_decode_planned': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                           ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.c_int]),
+    'av1b_plan_free': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    'av1b_sync': (ctypes.c_int, [ctypes.c_void_p]),
+    'av1b_set_profiling': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    'av1b_set_wait_limit': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong]),
+    'av1b_selftest_wait': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, ctypes.POINTER(ctypes.c_int),
+                                          ctypes.POINTER(ctypes.c_double)]),
+    'av1b_profile': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_char_p),
+                                    ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong)]),
     'av1b_decode_reserved': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                             ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]),
     'av1b_release_reference': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
@@ -242,6 +253,71 @@ class Decoder:
                                     self._err, len(self._err))
         self._check(rc, 'decode')
         return slot.value, planes
+
+    def plan(self, blob):
+        """Plans a serialized frame: validation and upload of its device records.
+        Returns an opaque plan handle for decode_planned."""
+        view = ctypes.create_string_buffer(4096)
+        rc = lib().av1b_syntax_view(blob.ptr, blob.size, view)
+        if rc:
+            raise Av1bError(rc, 'malformed blob')
+        h = ctypes.c_void_p()
+        self._check(lib().av1b_plan_frame(self.h, view, ctypes.byref(h)), 'plan_frame')
+        return h
+
+    def decode_planned(self, plan, slot=-1, keep=True, wait=True, planes=None):
+        pl = None
+        if planes is not None:
+            pl = _Planes()
+            for i, a in enumerate(planes):
+                pl.plane[i] = a.ctypes.data
+                pl.stride[i] = a.shape[1]
+        got = ctypes.c_int(-1)
+        rc = lib().av1b_decode_planned(self.h, plan, slot, 1 if keep else 0,
+                                       ctypes.byref(pl) if pl is not None else None,
+                                       ctypes.byref(got), 1 if wait else 0)
+        self._check(rc, 'decode_planned')
+        return got.value
+
+    def free_plan(self, plan):
+        self._check(lib().av1b_plan_free(self.h, plan), 'plan_free')
+
+    def selftest_wait(self, limit_ns):
+        st = ctypes.c_int(0)
+        ms = ctypes.c_double(0)
+        self._check(lib().av1b_selftest_wait(self.h, limit_ns, ctypes.byref(st), ctypes.byref(ms)),
+                    'selftest_wait')
+        return st.value, ms.value
+
+    def set_wait_limit(self, limit_ns):
+        self._check(lib().av1b_set_wait_limit(self.h, limit_ns), 'set_wait_limit')
+
+    def set_profiling(self, on):
+        self._check(lib().av1b_set_profiling(self.h, 1 if on else 0), 'set_profiling')
+
+    def profile(self):
+        """{stage: (total_ms, launches)} since profiling was switched on."""
+        out = {}
+        i = 0
+        while True:
+            name = ctypes.c_char_p()
+            ms = ctypes.c_double()
+            n = ctypes.c_longlong()
+            r = lib().av1b_profile(self.h, i, ctypes.byref(name), ctypes.byref(ms), ctypes.byref(n))
+            if r != 1:
+                break
+            out[name.value.decode()] = (ms.value, n.value)
+            i += 1
+        return out
+
+    def sync(self):
+        self._check(lib().av1b_sync(self.h), 'sync')
+
+    def stream(self):
+        return lib().av1b_decoder_stream(self.h)
+
+    def to_nv12_device(self, slot, pitch, dst_ptr, dst_len):
+        self._check(lib().av1b_to_nv12_device(self.h, slot, pitch, dst_ptr, dst_len), 'to_nv12_device')
 
     def reserve_reference(self):
         s = ctypes.c_int(-1)

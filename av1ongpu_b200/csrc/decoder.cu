@@ -93,7 +93,21 @@ struct av1b_decoder {
   bool grain_tables = false;
 
   av1b_stats stats{};
+  bool stats_pending = false;
   std::string err;
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  int* status_host = nullptr;          /* pinned */
+  void* slot_ptr_host[32] = {nullptr};
+  struct av1b_plan* own_plan = nullptr;
+
+  /* optional per-stage device timing (CUDA events on the decoder's stream) */
+  unsigned long long wait_ns = 1000000000ull;   /* one dependency wait: 1 s */
+  bool profiling = false;
+  std::vector<cudaEvent_t> ev_pool;
+  size_t ev_used = 0;
+  std::vector<std::pair<int, size_t>> marks;   /* (stage, index of its start event) */
+  double prof_ms[16] = {0};
+  long long prof_n[16] = {0};
 };
 
 namespace av1b {
@@ -264,14 +278,18 @@ struct Plan {
   GrainState gs_tail;   /* only the constants after the templates are used */
 };
 
+/* Maps a block's reference index to a device slot. At planning time a slot
+ * only has to be held or reserved (a pipeline plans a frame before the frame
+ * it references has been decoded); execute_plan checks that it holds a
+ * picture of this size by the time the plan runs. */
 int resolve_slot(av1b_decoder* d, const av1b_frame_syntax& s, int ref, int* slot) {
   *slot = -1;
   if (ref < 0 || ref >= static_cast<int>(s.n_reference_slots)) return AV1B_OK;
   const int sl = s.reference_slots[ref];
   if (sl < 0 || sl >= kSlots) return AV1B_OK;
-  if (!d->slot_used[sl] || !d->slot_valid[sl])
-    return fail(d, AV1B_ERR_SYNTAX, "a block references a slot that holds no picture");
-  if (d->slot_width[sl] != s.width || d->slot_height[sl] != s.height)
+  if (!d->slot_used[sl])
+    return fail(d, AV1B_ERR_SYNTAX, "a block references a slot that is neither held nor reserved");
+  if (d->slot_valid[sl] && (d->slot_width[sl] != s.width || d->slot_height[sl] != s.height))
     return fail(d, AV1B_ERR_SYNTAX,
                 "engine: reference scaling between pictures of different sizes is not supported");
   *slot = sl;
@@ -723,31 +741,202 @@ size_t stage_put(size_t* off, const std::vector<T>& v) {
   return o;
 }
 
-int run_frame(av1b_decoder* d, const av1b_frame_syntax& s, int keep, int forced_slot,
-              const av1b_planes* out, int* out_slot) {
+/* Stages the profiler reports (av1b_profile). */
+enum Stage {
+  kStOwner, kStInter, kStItx, kStUnits, kStDeblockV, kStDeblockH, kStCdef, kStUpscale, kStLr,
+  kStGrainTemplate, kStGrainBlend, kStNv12, kStRgb, kStCopy, kStageCount
+};
+const char* const kStageNames[kStageCount] = {
+    "owner", "inter", "itx", "units", "deblock_v", "deblock_h", "cdef", "upscale", "lr",
+    "grain_template", "grain_blend", "nv12", "rgb", "copy"};
+
+cudaEvent_t pool_event(av1b_decoder* d) {
+  if (d->ev_used == d->ev_pool.size()) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    d->ev_pool.push_back(e);
+  }
+  return d->ev_pool[d->ev_used++];
+}
+
+/* Runs `launch`; with profiling on, brackets it with two events. */
+template <class F>
+cudaError_t timed(av1b_decoder* d, int stage, F launch) {
+  if (!d->profiling) return launch();
+  const size_t i0 = d->ev_used;
+  cudaEvent_t a = pool_event(d);
+  cudaEvent_t b = pool_event(d);
+  if (!a || !b) return cudaErrorMemoryAllocation;
+  cudaEventRecord(a, d->stream);
+  const cudaError_t e = launch();
+  cudaEventRecord(b, d->stream);
+  d->marks.push_back(std::make_pair(stage, i0));
+  return e;
+}
+
+/* After a synchronisation: folds the recorded stage times into the totals. */
+void collect_profile(av1b_decoder* d) {
+  for (const auto& m : d->marks) {
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, d->ev_pool[m.second], d->ev_pool[m.second + 1]) == cudaSuccess) {
+      d->prof_ms[m.first] += ms;
+      d->prof_n[m.first] += 1;
+    }
+  }
+  d->marks.clear();
+  d->ev_used = 0;
+}
+
+int check_header(av1b_decoder* d, const av1b_frame_syntax& s) {
   if (s.width <= 0 || s.height <= 0) return fail(d, AV1B_ERR_SYNTAX, "frame has no size");
   if (s.bit_depth != 8 && s.bit_depth != 10 && s.bit_depth != 12)
     return fail(d, AV1B_ERR_SYNTAX, "bit depth must be 8, 10 or 12");
   if (s.ss_x < 0 || s.ss_x > 1 || s.ss_y < 0 || s.ss_y > 1 || (s.ss_y && !s.ss_x))
     return fail(d, AV1B_ERR_SYNTAX, "unsupported chroma subsampling");
   if (s.width > 16384 || s.height > 16384) return fail(d, AV1B_ERR_SYNTAX, "frame too large");
-  const int coded_width = (s.coded_width <= 0 || s.coded_width > s.width) ? s.width : s.coded_width;
-  cudaEvent_t ev[4];
-  for (auto& e : ev) CK(cudaEventCreate(&e), "cudaEventCreate");
-  struct EvGuard {
-    cudaEvent_t* e;
-    ~EvGuard() {
-      for (int i = 0; i < 4; ++i) cudaEventDestroy(e[i]);
-    }
-  } evg{ev};
+  return AV1B_OK;
+}
 
-  int rc = ensure_geometry(d, s, coded_width);
-  if (rc) return rc;
-  Plan P;
+}  // namespace
+}  // namespace av1b
+
+/* A planned frame: the validated device records of one FrameSyntax, already
+ * uploaded into device memory the plan owns (the reference's FramePlan,
+ * backend.hpp:140-206, which stays on the host there). */
+struct av1b_plan {
+  int width = 0, height = 0, coded_width = 0, bit_depth = 8, ss_x = 1, ss_y = 1;
+  int sharpness = 0, color_matrix = 1;
+  av1b::Plan P;                   /* host copy of the counts and constants */
+  av1b::DevBuf arena, coef, residual;
+  size_t o_blocks = 0, o_txs = 0, o_obmc = 0, o_warps = 0, o_pal = 0, o_units = 0;
+  size_t o_tiles = 0, o_itx = 0, o_dbv = 0, o_dbh = 0, o_cdef = 0, o_lr[3] = {0, 0, 0};
+  size_t o_map = 0;
+  int slots_read[kSlots + 1];     /* the reference slots the frame reads, -1 ended */
+  int n_blocks = 0;
+  bool owned_by_decoder = false;
+};
+
+namespace av1b {
+namespace {
+
+/* Plans `s` into `pl`: validation, records, and the upload of records and
+ * coefficient pools (stream ordered, so a decode that follows sees them). */
+int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
+  int rc;
+  if ((rc = check_header(d, s))) return rc;
+  const int coded_width = (s.coded_width <= 0 || s.coded_width > s.width) ? s.width : s.coded_width;
+  if ((rc = ensure_geometry(d, s, coded_width))) return rc;
+  Plan& P = pl->P;
   if ((rc = build_plan(d, s, &P))) return rc;
-  const Layout& L = d->L;
-  const int maxv = (1 << s.bit_depth) - 1;
+  pl->width = s.width;
+  pl->height = s.height;
+  pl->coded_width = coded_width;
+  pl->bit_depth = s.bit_depth;
+  pl->ss_x = s.ss_x;
+  pl->ss_y = s.ss_y;
+  pl->sharpness = s.sharpness;
+  pl->color_matrix = s.color_matrix;
+  pl->n_blocks = static_cast<int>(s.n_blocks);
+  {
+    bool used[kSlots] = {false};
+    for (const BlockRec& b : P.blocks)
+      for (int k = 0; k < 2; ++k)
+        if (b.ref_slot[k] >= 0) used[b.ref_slot[k]] = true;
+    for (const ObmcRec& o : P.obmc)
+      if (o.ref_slot >= 0) used[o.ref_slot] = true;
+    int n = 0;
+    for (int i = 0; i < kSlots; ++i)
+      if (used[i]) pl->slots_read[n++] = i;
+    pl->slots_read[n] = -1;
+  }
   cudaStream_t st = d->stream;
+  size_t off = 0;
+  pl->o_blocks = stage_put(&off, P.blocks);
+  pl->o_txs = stage_put(&off, P.txs);
+  pl->o_obmc = stage_put(&off, P.obmc);
+  pl->o_warps = stage_put(&off, P.warps);
+  pl->o_pal = stage_put(&off, P.palette_colors);
+  pl->o_units = stage_put(&off, P.units);
+  pl->o_tiles = stage_put(&off, P.inter_tiles);
+  pl->o_itx = stage_put(&off, P.itx_jobs);
+  pl->o_dbv = stage_put(&off, P.deblock_v);
+  pl->o_dbh = stage_put(&off, P.deblock_h);
+  pl->o_cdef = stage_put(&off, P.cdef);
+  for (int p = 0; p < 3; ++p) pl->o_lr[p] = stage_put(&off, P.lr_units[p]);
+  pl->o_map = off;
+  off = align_up(off + s.n_palette_map + 64, 256);
+  const size_t total = off;
+  if ((rc = host_ensure(d, d->stage, total)) || (rc = dev_ensure(d, pl->arena, total))) return rc;
+  /* the staging buffer may still feed an earlier upload */
+  CK(cudaStreamSynchronize(st), "stream sync");
+  uint8_t* hs = static_cast<uint8_t*>(d->stage.p);
+  auto put = [&](size_t o, const void* src, size_t bytes) {
+    if (bytes) std::memcpy(hs + o, src, bytes);
+  };
+  put(pl->o_blocks, P.blocks.data(), P.blocks.size() * sizeof(BlockRec));
+  put(pl->o_txs, P.txs.data(), P.txs.size() * sizeof(TxRec));
+  put(pl->o_obmc, P.obmc.data(), P.obmc.size() * sizeof(ObmcRec));
+  put(pl->o_warps, P.warps.data(), P.warps.size() * sizeof(WarpRec));
+  put(pl->o_pal, P.palette_colors.data(), P.palette_colors.size() * sizeof(int));
+  put(pl->o_units, P.units.data(), P.units.size() * sizeof(int));
+  put(pl->o_tiles, P.inter_tiles.data(), P.inter_tiles.size() * sizeof(int2));
+  put(pl->o_itx, P.itx_jobs.data(), P.itx_jobs.size() * sizeof(int2));
+  put(pl->o_dbv, P.deblock_v.data(), P.deblock_v.size() * sizeof(DeblockRec));
+  put(pl->o_dbh, P.deblock_h.data(), P.deblock_h.size() * sizeof(DeblockRec));
+  put(pl->o_cdef, P.cdef.data(), P.cdef.size() * sizeof(CdefRec));
+  for (int p = 0; p < 3; ++p)
+    put(pl->o_lr[p], P.lr_units[p].data(), P.lr_units[p].size() * sizeof(LrUnitRec));
+  put(pl->o_map, s.palette_map, s.n_palette_map);
+  std::memset(hs + pl->o_map + s.n_palette_map, 0, 64);
+  CK(cudaMemcpyAsync(pl->arena.p, hs, total, cudaMemcpyHostToDevice, st), "arena upload");
+
+  /* coefficient and residual pools, zero past the caller's arrays */
+  if ((rc = dev_ensure(d, pl->coef, P.coef_pool * sizeof(int))) ||
+      (rc = dev_ensure(d, pl->residual, P.residual_pool * sizeof(int))))
+    return rc;
+  if (!P.itx_jobs.empty() || !P.units.empty()) {
+    if (s.n_coefficients)
+      CK(cudaMemcpyAsync(pl->coef.p, s.coefficients, s.n_coefficients * sizeof(int),
+                         cudaMemcpyHostToDevice, st), "coefficient upload");
+    if (P.coef_pool > s.n_coefficients)
+      CK(cudaMemsetAsync(static_cast<int*>(pl->coef.p) + s.n_coefficients, 0,
+                         (P.coef_pool - s.n_coefficients) * sizeof(int), st), "coefficient pad");
+    if (s.n_residual)
+      CK(cudaMemcpyAsync(pl->residual.p, s.residual, s.n_residual * sizeof(int),
+                         cudaMemcpyHostToDevice, st), "residual upload");
+    if (P.residual_pool > s.n_residual)
+      CK(cudaMemsetAsync(static_cast<int*>(pl->residual.p) + s.n_residual, 0,
+                         (P.residual_pool - s.n_residual) * sizeof(int), st), "residual pad");
+  }
+  return AV1B_OK;
+}
+
+/* Runs a planned frame on the device: reconstruction, filters, reference
+ * store, film grain, and (with `out`) the read back. `sync`: wait for the
+ * frame and check its status word before returning. */
+int finish_frame(av1b_decoder* d);
+
+int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, const av1b_planes* out,
+                 int* out_slot, bool sync) {
+  int rc;
+  av1b_frame_syntax hdr{};
+  hdr.width = pl->width;
+  hdr.height = pl->height;
+  hdr.bit_depth = pl->bit_depth;
+  hdr.ss_x = pl->ss_x;
+  hdr.ss_y = pl->ss_y;
+  if ((rc = ensure_geometry(d, hdr, pl->coded_width))) return rc;
+  for (int i = 0; pl->slots_read[i] >= 0; ++i) {
+    const int sl = pl->slots_read[i];
+    if (!d->slot_used[sl] || !d->slot_valid[sl] || d->slot_width[sl] != pl->width ||
+        d->slot_height[sl] != pl->height)
+      return fail(d, AV1B_ERR_SYNTAX, "a planned frame reads a slot that holds no picture of its size");
+  }
+  const Plan& P = pl->P;
+  const Layout& L = d->L;
+  const int maxv = (1 << pl->bit_depth) - 1;
+  cudaStream_t st = d->stream;
+  cudaEvent_t* ev = d->ev;
 
   /* the destination slot */
   int slot = -1;
@@ -766,84 +955,26 @@ int run_frame(av1b_decoder* d, const av1b_frame_syntax& s, int keep, int forced_
     }
     if ((rc = dev_ensure(d, d->slot_buf[slot], static_cast<size_t>(L.size) * sizeof(px_t)))) return rc;
   }
+  const size_t pic_bytes = static_cast<size_t>(L.size) * sizeof(px_t);
   if (P.use_lr) {
-    const size_t bytes = static_cast<size_t>(L.size) * sizeof(px_t);
-    if ((rc = dev_ensure(d, d->lr_pre, bytes)) || (rc = dev_ensure(d, d->lr_cdef, bytes)) ||
-        (P.upscaled && (rc = dev_ensure(d, d->lr_pre_up, bytes))))
+    if ((rc = dev_ensure(d, d->lr_pre, pic_bytes)) || (rc = dev_ensure(d, d->lr_cdef, pic_bytes)) ||
+        (P.upscaled && (rc = dev_ensure(d, d->lr_pre_up, pic_bytes))))
       return rc;
   }
   if (P.grain && (rc = init_grain_tables(d))) return rc;
 
-  /* slot pointer table */
+  /* slot pointer table, uploaded when a slot buffer moved */
   {
     px_t* ptrs[kSlots];
     for (int i = 0; i < kSlots; ++i) ptrs[i] = static_cast<px_t*>(d->slot_buf[i].p);
     if ((rc = dev_ensure(d, d->slot_ptr_dev, sizeof(ptrs)))) return rc;
-    CK(cudaMemcpyAsync(d->slot_ptr_dev.p, ptrs, sizeof(ptrs), cudaMemcpyHostToDevice, st),
-       "slot table upload");
+    if (std::memcmp(ptrs, d->slot_ptr_host, sizeof(ptrs)) != 0) {
+      std::memcpy(d->slot_ptr_host, ptrs, sizeof(ptrs));
+      CK(cudaMemcpyAsync(d->slot_ptr_dev.p, d->slot_ptr_host, sizeof(ptrs), cudaMemcpyHostToDevice, st),
+         "slot table upload");
+    }
   }
-
-  /* ---- stage the frame's records ------------------------------------------------------ */
-  size_t off = 0;
-  const size_t o_blocks = stage_put(&off, P.blocks);
-  const size_t o_txs = stage_put(&off, P.txs);
-  const size_t o_obmc = stage_put(&off, P.obmc);
-  const size_t o_warps = stage_put(&off, P.warps);
-  const size_t o_pal = stage_put(&off, P.palette_colors);
-  const size_t o_units = stage_put(&off, P.units);
-  const size_t o_tiles = stage_put(&off, P.inter_tiles);
-  const size_t o_itx = stage_put(&off, P.itx_jobs);
-  const size_t o_dbv = stage_put(&off, P.deblock_v);
-  const size_t o_dbh = stage_put(&off, P.deblock_h);
-  const size_t o_cdef = stage_put(&off, P.cdef);
-  size_t o_lr[3];
-  for (int p = 0; p < 3; ++p) o_lr[p] = stage_put(&off, P.lr_units[p]);
-  const size_t o_map = off;
-  off = align_up(off + s.n_palette_map + 64, 256);
-  const size_t total = off;
-  if ((rc = host_ensure(d, d->stage, total)) || (rc = dev_ensure(d, d->arena, total))) return rc;
-  /* the previous frame's copy out of the staging buffer must be done */
-  CK(cudaStreamSynchronize(st), "stream sync");
-  uint8_t* hs = static_cast<uint8_t*>(d->stage.p);
-  auto put = [&](size_t o, const void* src, size_t bytes) {
-    if (bytes) std::memcpy(hs + o, src, bytes);
-  };
-  put(o_blocks, P.blocks.data(), P.blocks.size() * sizeof(BlockRec));
-  put(o_txs, P.txs.data(), P.txs.size() * sizeof(TxRec));
-  put(o_obmc, P.obmc.data(), P.obmc.size() * sizeof(ObmcRec));
-  put(o_warps, P.warps.data(), P.warps.size() * sizeof(WarpRec));
-  put(o_pal, P.palette_colors.data(), P.palette_colors.size() * sizeof(int));
-  put(o_units, P.units.data(), P.units.size() * sizeof(int));
-  put(o_tiles, P.inter_tiles.data(), P.inter_tiles.size() * sizeof(int2));
-  put(o_itx, P.itx_jobs.data(), P.itx_jobs.size() * sizeof(int2));
-  put(o_dbv, P.deblock_v.data(), P.deblock_v.size() * sizeof(DeblockRec));
-  put(o_dbh, P.deblock_h.data(), P.deblock_h.size() * sizeof(DeblockRec));
-  put(o_cdef, P.cdef.data(), P.cdef.size() * sizeof(CdefRec));
-  for (int p = 0; p < 3; ++p) put(o_lr[p], P.lr_units[p].data(), P.lr_units[p].size() * sizeof(LrUnitRec));
-  put(o_map, s.palette_map, s.n_palette_map);
-  std::memset(hs + o_map + s.n_palette_map, 0, 64);
-  CK(cudaEventRecord(ev[0], st), "event");
-  CK(cudaMemcpyAsync(d->arena.p, hs, total, cudaMemcpyHostToDevice, st), "arena upload");
-  uint8_t* ar = static_cast<uint8_t*>(d->arena.p);
-
-  /* coefficient and residual pools, zero past the caller's arrays */
-  if ((rc = dev_ensure(d, d->coef, P.coef_pool * sizeof(int))) ||
-      (rc = dev_ensure(d, d->residual, P.residual_pool * sizeof(int))))
-    return rc;
-  if (!P.itx_jobs.empty() || !P.units.empty()) {
-    if (s.n_coefficients)
-      CK(cudaMemcpyAsync(d->coef.p, s.coefficients, s.n_coefficients * sizeof(int),
-                         cudaMemcpyHostToDevice, st), "coefficient upload");
-    if (P.coef_pool > s.n_coefficients)
-      CK(cudaMemsetAsync(static_cast<int*>(d->coef.p) + s.n_coefficients, 0,
-                         (P.coef_pool - s.n_coefficients) * sizeof(int), st), "coefficient pad");
-    if (s.n_residual)
-      CK(cudaMemcpyAsync(d->residual.p, s.residual, s.n_residual * sizeof(int),
-                         cudaMemcpyHostToDevice, st), "residual upload");
-    if (P.residual_pool > s.n_residual)
-      CK(cudaMemsetAsync(static_cast<int*>(d->residual.p) + s.n_residual, 0,
-                         (P.residual_pool - s.n_residual) * sizeof(int), st), "residual pad");
-  }
+  uint8_t* ar = static_cast<uint8_t*>(pl->arena.p);
 
   /* owner grids, done flags, queue and status */
   FrameArgs a{};
@@ -859,10 +990,11 @@ int run_frame(av1b_decoder* d, const av1b_frame_syntax& s, int keep, int forced_
     const size_t cells = static_cast<size_t>(a.cell_w[p]) * a.cell_h[p];
     if ((rc = dev_ensure(d, d->owner[p], cells * sizeof(int)))) return rc;
     a.owner[p] = static_cast<int*>(d->owner[p].p);
-    CK(cudaMemsetAsync(a.owner[p], 0xff, cells * sizeof(int), st), "owner reset");
+    if (!P.units.empty()) CK(cudaMemsetAsync(a.owner[p], 0xff, cells * sizeof(int), st), "owner reset");
   }
-  if (d->done.cap < s.n_blocks * sizeof(unsigned) + 256) {
-    if ((rc = dev_ensure(d, d->done, s.n_blocks * sizeof(unsigned) + 256))) return rc;
+  const size_t done_bytes = static_cast<size_t>(pl->n_blocks) * sizeof(unsigned) + 256;
+  if (d->done.cap < done_bytes) {
+    if ((rc = dev_ensure(d, d->done, done_bytes))) return rc;
     CK(cudaMemsetAsync(d->done.p, 0, d->done.cap, st), "done reset");
   }
   ++d->epoch;
@@ -870,80 +1002,113 @@ int run_frame(av1b_decoder* d, const av1b_frame_syntax& s, int keep, int forced_
     CK(cudaMemsetAsync(d->done.p, 0, d->done.cap, st), "done reset");
     d->epoch = 1;
   }
-  if ((rc = dev_ensure(d, d->status_q, 256))) return rc;
-  CK(cudaMemsetAsync(d->status_q.p, 0, 256, st), "status reset");
+  if (!d->status_q.p) {
+    if ((rc = dev_ensure(d, d->status_q, 256))) return rc;
+    CK(cudaMemsetAsync(d->status_q.p, 0, 256, st), "status reset");
+  }
+  /* the claim counter restarts every frame; the status word is sticky until
+   * finish_frame has read it, so frames queued without a wait are covered */
+  CK(cudaMemsetAsync(d->status_q.p, 0, sizeof(unsigned), st), "queue reset");
 
   a.cur = static_cast<px_t*>(d->cur.p);
   a.slot_ptr = static_cast<px_t* const*>(d->slot_ptr_dev.p);
-  a.blocks = reinterpret_cast<const BlockRec*>(ar + o_blocks);
+  a.blocks = reinterpret_cast<const BlockRec*>(ar + pl->o_blocks);
   a.n_blocks = static_cast<int>(P.blocks.size());
-  a.txs = reinterpret_cast<const TxRec*>(ar + o_txs);
-  a.obmc = reinterpret_cast<const ObmcRec*>(ar + o_obmc);
-  a.warps = reinterpret_cast<const WarpRec*>(ar + o_warps);
-  a.coef = static_cast<const int*>(d->coef.p);
-  a.residual = static_cast<const int*>(d->residual.p);
-  a.palette_map = ar + o_map;
-  a.palette_colors = reinterpret_cast<const int*>(ar + o_pal);
+  a.txs = reinterpret_cast<const TxRec*>(ar + pl->o_txs);
+  a.obmc = reinterpret_cast<const ObmcRec*>(ar + pl->o_obmc);
+  a.warps = reinterpret_cast<const WarpRec*>(ar + pl->o_warps);
+  a.coef = static_cast<const int*>(pl->coef.p);
+  a.residual = static_cast<const int*>(pl->residual.p);
+  a.palette_map = ar + pl->o_map;
+  a.palette_colors = reinterpret_cast<const int*>(ar + pl->o_pal);
   a.done = static_cast<unsigned*>(d->done.p);
   a.epoch = d->epoch;
-  a.units = reinterpret_cast<const int*>(ar + o_units);
+  a.units = reinterpret_cast<const int*>(ar + pl->o_units);
   a.n_units = static_cast<int>(P.units.size());
   a.queue = static_cast<unsigned*>(d->status_q.p);
   a.status = reinterpret_cast<int*>(static_cast<uint8_t*>(d->status_q.p) + 64);
-  a.inter_tiles = reinterpret_cast<const int2*>(ar + o_tiles);
+  a.inter_tiles = reinterpret_cast<const int2*>(ar + pl->o_tiles);
   a.n_inter_tiles = static_cast<int>(P.inter_tiles.size());
-  a.itx_jobs = reinterpret_cast<const int2*>(ar + o_itx);
+  a.itx_jobs = reinterpret_cast<const int2*>(ar + pl->o_itx);
   a.n_itx = static_cast<int>(P.itx_jobs.size());
   a.maxv = maxv;
   a.scale_x = P.scale_x;
   a.scale_y = P.scale_y;
+  a.wait_ns = d->wait_ns;
 
   int launches = 0;
+  CK(cudaEventRecord(ev[0], st), "event");
+  for (int stage = 0; stage < 4; ++stage) {
+    const bool any = stage == 0 ? a.n_blocks > 0
+                                : (stage == 1 ? a.n_inter_tiles > 0 : (stage == 2 ? a.n_itx > 0 : a.n_units > 0));
+    if (!any) continue;
+    CK(timed(d, kStOwner + stage, [&] { return launch_recon_stage(stage, a, d->n_sm, st); }),
+       "reconstruction launch");
+    ++launches;
+  }
   CK(cudaEventRecord(ev[1], st), "event");
-  CK(launch_recon(a, d->n_sm, st, &launches), "reconstruction launch");
-  CK(cudaEventRecord(ev[2], st), "event");
 
   /* ---- filters --------------------------------------------------------------------------- */
   px_t* cur = a.cur;
-  const size_t pic_bytes = static_cast<size_t>(L.size) * sizeof(px_t);
-  CK(launch_deblock(cur, reinterpret_cast<const DeblockRec*>(ar + o_dbv),
-                    static_cast<int>(P.deblock_v.size()), s.sharpness, s.bit_depth, maxv, st),
-     "deblock V");
-  CK(launch_deblock(cur, reinterpret_cast<const DeblockRec*>(ar + o_dbh),
-                    static_cast<int>(P.deblock_h.size()), s.sharpness, s.bit_depth, maxv, st),
-     "deblock H");
+  if (!P.deblock_v.empty())
+    CK(timed(d, kStDeblockV, [&] {
+         return launch_deblock(cur, reinterpret_cast<const DeblockRec*>(ar + pl->o_dbv),
+                               static_cast<int>(P.deblock_v.size()), pl->sharpness, pl->bit_depth,
+                               maxv, st);
+       }), "deblock V");
+  if (!P.deblock_h.empty())
+    CK(timed(d, kStDeblockH, [&] {
+         return launch_deblock(cur, reinterpret_cast<const DeblockRec*>(ar + pl->o_dbh),
+                               static_cast<int>(P.deblock_h.size()), pl->sharpness, pl->bit_depth,
+                               maxv, st);
+       }), "deblock H");
   launches += (!P.deblock_v.empty()) + (!P.deblock_h.empty());
   px_t* snap = static_cast<px_t*>(d->snap.p);
   if (P.use_lr)
-    CK(cudaMemcpyAsync(d->lr_pre.p, cur, pic_bytes, cudaMemcpyDeviceToDevice, st), "pre-CDEF copy");
+    CK(timed(d, kStCopy, [&] {
+         return cudaMemcpyAsync(d->lr_pre.p, cur, pic_bytes, cudaMemcpyDeviceToDevice, st);
+       }), "pre-CDEF copy");
   if (!P.cdef.empty()) {
-    CK(cudaMemcpyAsync(snap, cur, pic_bytes, cudaMemcpyDeviceToDevice, st), "CDEF snapshot");
-    CK(launch_cdef(snap, cur, reinterpret_cast<const CdefRec*>(ar + o_cdef),
-                   static_cast<int>(P.cdef.size()), L, st), "CDEF");
+    CK(timed(d, kStCopy, [&] {
+         return cudaMemcpyAsync(snap, cur, pic_bytes, cudaMemcpyDeviceToDevice, st);
+       }), "CDEF snapshot");
+    CK(timed(d, kStCdef, [&] {
+         return launch_cdef(snap, cur, reinterpret_cast<const CdefRec*>(ar + pl->o_cdef),
+                            static_cast<int>(P.cdef.size()), L, st);
+       }), "CDEF");
     ++launches;
   }
   const px_t* lr_curr = static_cast<px_t*>(d->lr_pre.p);
   if (P.upscaled) {
-    CK(cudaMemcpyAsync(snap, cur, pic_bytes, cudaMemcpyDeviceToDevice, st), "superres snapshot");
-    CK(launch_upscale(snap, cur, L, maxv, st), "superres");
+    CK(timed(d, kStCopy, [&] {
+         return cudaMemcpyAsync(snap, cur, pic_bytes, cudaMemcpyDeviceToDevice, st);
+       }), "superres snapshot");
+    CK(timed(d, kStUpscale, [&] { return launch_upscale(snap, cur, L, maxv, st); }), "superres");
     ++launches;
     if (P.use_lr) {
-      CK(launch_upscale(static_cast<px_t*>(d->lr_pre.p), static_cast<px_t*>(d->lr_pre_up.p), L,
-                        maxv, st), "superres (pre-CDEF)");
+      CK(timed(d, kStUpscale, [&] {
+           return launch_upscale(static_cast<px_t*>(d->lr_pre.p), static_cast<px_t*>(d->lr_pre_up.p),
+                                 L, maxv, st);
+         }), "superres (pre-CDEF)");
       ++launches;
       lr_curr = static_cast<px_t*>(d->lr_pre_up.p);
     }
   }
   if (P.use_lr) {
-    CK(cudaMemcpyAsync(d->lr_cdef.p, cur, pic_bytes, cudaMemcpyDeviceToDevice, st), "LR snapshot");
+    CK(timed(d, kStCopy, [&] {
+         return cudaMemcpyAsync(d->lr_cdef.p, cur, pic_bytes, cudaMemcpyDeviceToDevice, st);
+       }), "LR snapshot");
     LrArgs lr = P.lr;
-    for (int p = 0; p < 3; ++p) lr.units[p] = reinterpret_cast<const LrUnitRec*>(ar + o_lr[p]);
-    CK(launch_lr(static_cast<px_t*>(d->lr_cdef.p), lr_curr, cur, L, lr, maxv, st), "loop restoration");
+    for (int p = 0; p < 3; ++p) lr.units[p] = reinterpret_cast<const LrUnitRec*>(ar + pl->o_lr[p]);
+    CK(timed(d, kStLr, [&] {
+         return launch_lr(static_cast<px_t*>(d->lr_cdef.p), lr_curr, cur, L, lr, maxv, st);
+       }), "loop restoration");
     ++launches;
   }
   if (keep)
-    CK(cudaMemcpyAsync(d->slot_buf[slot].p, cur, pic_bytes, cudaMemcpyDeviceToDevice, st),
-       "reference store");
+    CK(timed(d, kStCopy, [&] {
+         return cudaMemcpyAsync(d->slot_buf[slot].p, cur, pic_bytes, cudaMemcpyDeviceToDevice, st);
+       }), "reference store");
   const px_t* display = cur;
   d->disp_is_cur = true;
   if (P.grain) {
@@ -952,14 +1117,20 @@ int run_frame(av1b_decoder* d, const av1b_frame_syntax& s, int keep, int forced_
     CK(cudaMemcpyAsync(reinterpret_cast<uint8_t*>(gsd) + tail,
                        reinterpret_cast<const uint8_t*>(&P.gs_tail) + tail, sizeof(GrainState) - tail,
                        cudaMemcpyHostToDevice, st), "grain constants");
-    CK(launch_grain(cur, static_cast<px_t*>(d->disp.p), L, gsd, P.gp,
-                    static_cast<const uint16_t*>(d->orbit.p), static_cast<const uint16_t*>(d->pos.p),
-                    st), "film grain");
+    CK(timed(d, kStGrainTemplate, [&] {
+         return launch_grain_template(gsd, P.gp, static_cast<const uint16_t*>(d->orbit.p),
+                                      static_cast<const uint16_t*>(d->pos.p), st);
+       }), "film grain template");
+    CK(timed(d, kStGrainBlend, [&] {
+         return launch_grain_blend(cur, static_cast<px_t*>(d->disp.p), L, gsd,
+                                   static_cast<const uint16_t*>(d->orbit.p),
+                                   static_cast<const uint16_t*>(d->pos.p), st);
+       }), "film grain blend");
     launches += 2;
     display = static_cast<px_t*>(d->disp.p);
     d->disp_is_cur = false;
   }
-  CK(cudaEventRecord(ev[3], st), "event");
+  CK(cudaEventRecord(ev[2], st), "event");
 
   /* ---- read back ---------------------------------------------------------------------------- */
   if (out) {
@@ -973,35 +1144,52 @@ int run_frame(av1b_decoder* d, const av1b_frame_syntax& s, int keep, int forced_
                            cudaMemcpyDeviceToHost, st), "read back");
     }
   }
-  int status = 0;
-  CK(cudaMemcpyAsync(&status, a.status, sizeof(int), cudaMemcpyDeviceToHost, st), "status read");
-  CK(cudaStreamSynchronize(st), "frame sync");
-  if (status & AV1B_STATUS_TIMEOUT)
-    return fail(d, AV1B_ERR_TIMEOUT, "a device-side dependency wait timed out");
-
-  float ms_recon = 0, ms_filter = 0, ms_total = 0;
-  cudaEventElapsedTime(&ms_recon, ev[1], ev[2]);
-  cudaEventElapsedTime(&ms_filter, ev[2], ev[3]);
-  cudaEventElapsedTime(&ms_total, ev[0], ev[3]);
-  d->stats.blocks = static_cast<int>(s.n_blocks);
+  CK(cudaMemcpyAsync(d->status_host, a.status, sizeof(int), cudaMemcpyDeviceToHost, st), "status read");
+  d->stats.blocks = pl->n_blocks;
   d->stats.waves = 0;
   d->stats.kernel_launches = launches;
-  d->stats.reconstruct_ms = ms_recon;
-  d->stats.filter_ms = ms_filter;
-  d->stats.readback_ms = 0;
-  d->stats.total_ms = ms_total;
-
+  d->stats_pending = true;
   if (keep) {
     d->slot_used[slot] = true;
     d->slot_valid[slot] = true;
-    d->slot_width[slot] = s.width;
-    d->slot_height[slot] = s.height;
-    d->slot_bd[slot] = s.bit_depth;
+    d->slot_width[slot] = pl->width;
+    d->slot_height[slot] = pl->height;
+    d->slot_bd[slot] = pl->bit_depth;
   }
   d->last_slot = slot;
   d->have_last = true;
   if (out_slot) *out_slot = slot;
+  if (sync) return finish_frame(d);
   return AV1B_OK;
+}
+
+/* Waits for the frame in flight and checks its status word. */
+int finish_frame(av1b_decoder* d) {
+  CK(cudaStreamSynchronize(d->stream), "frame sync");
+  collect_profile(d);
+  if (d->stats_pending) {
+    float ms_recon = 0, ms_filter = 0;
+    cudaEventElapsedTime(&ms_recon, d->ev[0], d->ev[1]);
+    cudaEventElapsedTime(&ms_filter, d->ev[1], d->ev[2]);
+    d->stats.reconstruct_ms = ms_recon;
+    d->stats.filter_ms = ms_filter;
+    d->stats.readback_ms = 0;
+    d->stats.total_ms = ms_recon + ms_filter;
+    d->stats_pending = false;
+  }
+  if (*d->status_host & AV1B_STATUS_TIMEOUT) {
+    *d->status_host = 0;
+    CK(cudaMemset(static_cast<uint8_t*>(d->status_q.p) + 64, 0, sizeof(int)), "status clear");
+    return fail(d, AV1B_ERR_TIMEOUT, "a device-side dependency wait timed out");
+  }
+  return AV1B_OK;
+}
+
+int run_frame(av1b_decoder* d, const av1b_frame_syntax& s, int keep, int forced_slot,
+              const av1b_planes* out, int* out_slot) {
+  int rc = plan_frame(d, s, d->own_plan);
+  if (rc) return rc;
+  return execute_plan(d, d->own_plan, keep, forced_slot, out, out_slot, true);
 }
 
 /* The picture an output call of `slot` reads: the display picture of the
@@ -1041,11 +1229,17 @@ int av1b_decoder_create(int device, size_t hbm_budget_bytes, av1b_decoder** out)
   d->budget = hbm_budget_bytes;
   cudaDeviceProp prop;
   if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) d->n_sm = prop.multiProcessorCount;
-  if (cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      set_kernel_attributes() != cudaSuccess) {
-    delete d;
+  bool ok = cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking) == cudaSuccess &&
+            set_kernel_attributes() == cudaSuccess &&
+            cudaHostAlloc(reinterpret_cast<void**>(&d->status_host), 64, cudaHostAllocDefault) == cudaSuccess;
+  for (int i = 0; ok && i < 3; ++i) ok = cudaEventCreate(&d->ev[i]) == cudaSuccess;
+  if (!ok) {
+    av1b_decoder_destroy(d);
     return AV1B_ERR_CUDA;
   }
+  *d->status_host = 0;
+  d->own_plan = new av1b_plan;
+  d->own_plan->owned_by_decoder = true;
   *out = d;
   return AV1B_OK;
 }
@@ -1053,7 +1247,16 @@ int av1b_decoder_create(int device, size_t hbm_budget_bytes, av1b_decoder** out)
 int av1b_decoder_destroy(av1b_decoder* d) {
   if (!d) return AV1B_ERR_ARG;
   cudaSetDevice(d->device);
-  cudaStreamSynchronize(d->stream);
+  if (d->stream) cudaStreamSynchronize(d->stream);
+  if (d->own_plan) {
+    dev_release(d, d->own_plan->arena);
+    dev_release(d, d->own_plan->coef);
+    dev_release(d, d->own_plan->residual);
+    delete d->own_plan;
+  }
+  for (int i = 0; i < 3; ++i)
+    if (d->ev[i]) cudaEventDestroy(d->ev[i]);
+  if (d->status_host) cudaFreeHost(d->status_host);
   DevBuf* bufs[] = {&d->cur, &d->snap, &d->lr_pre, &d->lr_pre_up, &d->lr_cdef, &d->disp,
                     &d->slot_ptr_dev, &d->arena, &d->coef, &d->residual, &d->owner[0],
                     &d->owner[1], &d->owner[2], &d->done, &d->status_q, &d->nv12, &d->rgb,
@@ -1061,7 +1264,7 @@ int av1b_decoder_destroy(av1b_decoder* d) {
   for (DevBuf* b : bufs) dev_release(d, *b);
   for (int i = 0; i < kSlots; ++i) dev_release(d, d->slot_buf[i]);
   if (d->stage.p) cudaFreeHost(d->stage.p);
-  cudaStreamDestroy(d->stream);
+  if (d->stream) cudaStreamDestroy(d->stream);
   delete d;
   return AV1B_OK;
 }
@@ -1101,6 +1304,55 @@ int av1b_decode_blob(av1b_decoder* d, const uint8_t* blob, size_t len, int keep_
     return AV1B_ERR_ARG;
   }
   return av1b_decode(d, &v, keep_reference, out, out_slot, error, error_len);
+}
+
+int av1b_plan_frame(av1b_decoder* d, const av1b_frame_syntax* syntax, av1b_plan** out) {
+  if (!d || !syntax || !out) return AV1B_ERR_ARG;
+  std::lock_guard<std::mutex> lk(d->mu);
+  cudaSetDevice(d->device);
+  d->err.clear();
+  *out = nullptr;
+  auto* pl = new av1b_plan;
+  const int rc = plan_frame(d, *syntax, pl);
+  if (rc) {
+    dev_release(d, pl->arena);
+    dev_release(d, pl->coef);
+    dev_release(d, pl->residual);
+    delete pl;
+    return rc;
+  }
+  *out = pl;
+  return AV1B_OK;
+}
+
+int av1b_plan_free(av1b_decoder* d, av1b_plan* pl) {
+  if (!d) return AV1B_ERR_ARG;
+  if (!pl) return AV1B_OK;
+  std::lock_guard<std::mutex> lk(d->mu);
+  cudaSetDevice(d->device);
+  cudaStreamSynchronize(d->stream);
+  dev_release(d, pl->arena);
+  dev_release(d, pl->coef);
+  dev_release(d, pl->residual);
+  delete pl;
+  return AV1B_OK;
+}
+
+int av1b_decode_planned(av1b_decoder* d, av1b_plan* pl, int slot, int keep_reference,
+                        const av1b_planes* out, int* out_slot, int wait) {
+  if (!d || !pl) return AV1B_ERR_ARG;
+  std::lock_guard<std::mutex> lk(d->mu);
+  cudaSetDevice(d->device);
+  d->err.clear();
+  if (out_slot) *out_slot = -1;
+  return execute_plan(d, pl, keep_reference ? 1 : 0, slot, out, out_slot, wait != 0);
+}
+
+int av1b_sync(av1b_decoder* d) {
+  if (!d) return AV1B_ERR_ARG;
+  std::lock_guard<std::mutex> lk(d->mu);
+  cudaSetDevice(d->device);
+  return finish_frame(d);
 }
 
 int av1b_reserve_reference(av1b_decoder* d, int* out_slot) {
@@ -1160,10 +1412,14 @@ static int to_nv12_impl(av1b_decoder* d, int slot, size_t pitch, uint8_t* dst, s
     if ((rc = dev_ensure(d, d->nv12, bytes))) return rc;
     target = static_cast<uint8_t*>(d->nv12.p);
   }
-  CK(launch_nv12(pic, target, d->L, static_cast<int>(pitch), d->stream), "NV12 pack");
-  if (!device_dst)
+  CK(timed(d, kStNv12, [&] { return launch_nv12(pic, target, d->L, static_cast<int>(pitch), d->stream); }),
+     "NV12 pack");
+  if (!device_dst) {
     CK(cudaMemcpyAsync(dst, target, bytes, cudaMemcpyDeviceToHost, d->stream), "NV12 read back");
-  CK(cudaStreamSynchronize(d->stream), "NV12 sync");
+    CK(cudaStreamSynchronize(d->stream), "NV12 sync");
+    collect_profile(d);
+  }
+  /* the device variant stays queued on the decoder's stream */
   return AV1B_OK;
 }
 
@@ -1187,9 +1443,11 @@ int av1b_to_rgb(av1b_decoder* d, int slot, int matrix, int range, uint8_t* dst, 
   if ((rc = dev_ensure(d, d->rgb, bytes))) return rc;
   RgbArgs m{};
   color_matrix(matrix, range, d->bit_depth, m.m, m.o);
-  CK(launch_rgb(pic, static_cast<uint8_t*>(d->rgb.p), d->L, m, d->stream), "RGB pack");
+  CK(timed(d, kStRgb, [&] { return launch_rgb(pic, static_cast<uint8_t*>(d->rgb.p), d->L, m, d->stream); }),
+     "RGB pack");
   CK(cudaMemcpyAsync(dst, d->rgb.p, bytes, cudaMemcpyDeviceToHost, d->stream), "RGB read back");
   CK(cudaStreamSynchronize(d->stream), "RGB sync");
+  collect_profile(d);
   return AV1B_OK;
 }
 
@@ -1219,6 +1477,57 @@ int av1b_slot_planes_device(av1b_decoder* d, int slot, uint16_t* plane_ptr[3], i
 }
 
 void* av1b_decoder_stream(av1b_decoder* d) { return d ? d->stream : nullptr; }
+
+int av1b_set_wait_limit(av1b_decoder* d, long long limit_ns) {
+  if (!d || limit_ns <= 0) return AV1B_ERR_ARG;
+  d->wait_ns = static_cast<unsigned long long>(limit_ns);
+  return AV1B_OK;
+}
+
+int av1b_selftest_wait(av1b_decoder* d, long long limit_ns, int* status, double* elapsed_ms) {
+  if (!d || !status || limit_ns <= 0 || limit_ns > 10000000000LL) return AV1B_ERR_ARG;
+  std::lock_guard<std::mutex> lk(d->mu);
+  cudaSetDevice(d->device);
+  DevBuf mem;
+  int rc = dev_ensure(d, mem, 256);
+  if (rc) return rc;
+  CK(cudaMemsetAsync(mem.p, 0, 256, d->stream), "selftest reset");
+  CK(cudaEventRecord(d->ev[0], d->stream), "event");
+  CK(launch_selftest_wait(static_cast<const unsigned*>(mem.p),
+                          reinterpret_cast<int*>(static_cast<uint8_t*>(mem.p) + 64),
+                          static_cast<unsigned long long>(limit_ns), d->stream), "selftest launch");
+  CK(cudaEventRecord(d->ev[1], d->stream), "event");
+  int st = 0;
+  CK(cudaMemcpyAsync(&st, static_cast<uint8_t*>(mem.p) + 64, sizeof(int), cudaMemcpyDeviceToHost,
+                     d->stream), "selftest status");
+  CK(cudaStreamSynchronize(d->stream), "selftest sync");
+  float ms = 0;
+  cudaEventElapsedTime(&ms, d->ev[0], d->ev[1]);
+  dev_release(d, mem);
+  *status = st;
+  if (elapsed_ms) *elapsed_ms = ms;
+  return AV1B_OK;
+}
+
+int av1b_set_profiling(av1b_decoder* d, int on) {
+  if (!d) return AV1B_ERR_ARG;
+  std::lock_guard<std::mutex> lk(d->mu);
+  d->profiling = on != 0;
+  for (int i = 0; i < 16; ++i) {
+    d->prof_ms[i] = 0;
+    d->prof_n[i] = 0;
+  }
+  return AV1B_OK;
+}
+
+int av1b_profile(av1b_decoder* d, int stage, const char** name, double* total_ms, long long* count) {
+  if (!d || stage < 0) return AV1B_ERR_ARG;
+  if (stage >= kStageCount) return 0;
+  if (name) *name = kStageNames[stage];
+  if (total_ms) *total_ms = d->prof_ms[stage];
+  if (count) *count = d->prof_n[stage];
+  return 1;
+}
 
 const char* av1b_last_error(av1b_decoder* d) { return d ? d->err.c_str() : ""; }
 

@@ -209,21 +209,38 @@ __global__ void k_itx(FrameArgs a) {
 
 /* ---- phase B -------------------------------------------------------------------------- */
 
-/* Waits until block `o` is reconstructed. Returns false on timeout. */
-__device__ bool wait_block(const FrameArgs& a, int o) {
-  if (ld_acquire(a.done + o) == a.epoch) return true;
+/* Waits until *flag == want, for at most limit_ns of globaltimer. Once any
+ * wait has given up (AV1B_STATUS_TIMEOUT in *status), nothing waits any more:
+ * the frame has failed and the kernel only has to run to its end. */
+__device__ bool bounded_wait(const unsigned* flag, unsigned want, int* status,
+                             unsigned long long limit_ns) {
+  if (ld_acquire(flag) == want) return true;
   const unsigned long long t0 = global_ns();
-  while (ld_acquire(a.done + o) != a.epoch) {
-    /* once any wait of this frame has given up, nothing waits any more: the
-     * frame has failed and the kernel only has to run to its end */
-    if (ld_acquire(reinterpret_cast<const unsigned*>(a.status)) & AV1B_STATUS_TIMEOUT) return false;
+  while (ld_acquire(flag) != want) {
+    if (ld_acquire(reinterpret_cast<const unsigned*>(status)) & AV1B_STATUS_TIMEOUT) return false;
     __nanosleep(100);
-    if (global_ns() - t0 > 1000000000ull) {
-      atomicOr(a.status, AV1B_STATUS_TIMEOUT);
+    if (global_ns() - t0 > limit_ns) {
+      atomicOr(status, AV1B_STATUS_TIMEOUT);
       return false;
     }
   }
   return true;
+}
+
+/* Waits until block `o` is reconstructed. Returns false on timeout. */
+__device__ bool wait_block(const FrameArgs& a, int o) {
+  return bounded_wait(a.done + o, a.epoch, a.status, a.wait_ns);
+}
+
+/* A wait on a flag nothing sets: the failure-detection self test. */
+__global__ void k_selftest_wait(const unsigned* flag, int* status, unsigned long long limit_ns) {
+  if (threadIdx.x == 0) bounded_wait(flag, 1u, status, limit_ns);
+}
+
+cudaError_t launch_selftest_wait(const unsigned* flag, int* status, unsigned long long limit_ns,
+                                 cudaStream_t s) {
+  k_selftest_wait<<<1, 32, 0, s>>>(flag, status, limit_ns);
+  return cudaGetLastError();
 }
 
 /* True when every owner of the cells of [x0, x1] x [y0, y1] precedes `bi` in
@@ -770,26 +787,25 @@ __global__ void k_rgb(const px_t* __restrict__ pic, uint8_t* out, Layout L, RgbA
 /* ---- launchers ------------------------------------------------------------------------------------ */
 static inline unsigned cdiv(long long a, long long b) { return (unsigned)((a + b - 1) / b); }
 
-cudaError_t launch_recon(const FrameArgs& a, int n_sm, cudaStream_t s, int* launches) {
-  int n = 0;
-  if (a.n_blocks > 0) {
-    k_owner<<<cdiv((long long)a.n_blocks * 32, 256), 256, 0, s>>>(a);
-    ++n;
+cudaError_t launch_recon_stage(int stage, const FrameArgs& a, int n_sm, cudaStream_t s) {
+  switch (stage) {
+    case 0:
+      if (a.n_blocks > 0) k_owner<<<cdiv((long long)a.n_blocks * 32, 256), 256, 0, s>>>(a);
+      break;
+    case 1:
+      if (a.n_inter_tiles > 0)
+        k_inter<<<cdiv((long long)a.n_inter_tiles * 32, 256), 256, 0, s>>>(a);
+      break;
+    case 2:
+      if (a.n_itx > 0) k_itx<<<cdiv(a.n_itx, 4), 128, 4 * 4096 * sizeof(int), s>>>(a);
+      break;
+    default:
+      if (a.n_units > 0) {
+        const size_t smem = 4 * (3 * AV1B_EDGE_LEN + 4096) * sizeof(int);
+        k_units<<<2 * n_sm, 128, smem, s>>>(a);
+      }
+      break;
   }
-  if (a.n_inter_tiles > 0) {
-    k_inter<<<cdiv((long long)a.n_inter_tiles * 32, 256), 256, 0, s>>>(a);
-    ++n;
-  }
-  if (a.n_itx > 0) {
-    k_itx<<<cdiv(a.n_itx, 4), 128, 4 * 4096 * sizeof(int), s>>>(a);
-    ++n;
-  }
-  if (a.n_units > 0) {
-    const size_t smem = 4 * (3 * AV1B_EDGE_LEN + 4096) * sizeof(int);
-    k_units<<<2 * n_sm, 128, smem, s>>>(a);
-    ++n;
-  }
-  if (launches) *launches += n;
   return cudaGetLastError();
 }
 
@@ -819,10 +835,14 @@ cudaError_t launch_lr(const px_t* cdef, const px_t* curr, px_t* dst, const Layou
   return cudaGetLastError();
 }
 
-cudaError_t launch_grain(const px_t* src, px_t* dst, const Layout& L, GrainState* gs,
-                         const GrainParamsDev& prm, const uint16_t* orbit, const uint16_t* pos,
-                         cudaStream_t s) {
+cudaError_t launch_grain_template(GrainState* gs, const GrainParamsDev& prm, const uint16_t* orbit,
+                                  const uint16_t* pos, cudaStream_t s) {
   k_grain_template<<<1, 256, 0, s>>>(gs, prm, orbit, pos);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_grain_blend(const px_t* src, px_t* dst, const Layout& L, const GrainState* gs,
+                               const uint16_t* orbit, const uint16_t* pos, cudaStream_t s) {
   k_grain_blend<<<dim3(cdiv(L.p[0].out_w, 128), L.p[0].out_h, 3), 128, 0, s>>>(src, dst, L, gs,
                                                                                  orbit, pos);
   return cudaGetLastError();

@@ -42,6 +42,7 @@ struct FrameArgs {
   int* status;
   int maxv;
   int scale_x, scale_y;
+  unsigned long long wait_ns;   /* limit of one dependency wait */
 };
 
 struct LrArgs {
@@ -64,7 +65,11 @@ struct RgbArgs {
 };
 
 cudaError_t set_kernel_attributes();
-cudaError_t launch_recon(const FrameArgs& a, int n_sm, cudaStream_t s, int* launches);
+cudaError_t launch_selftest_wait(const unsigned* flag, int* status, unsigned long long limit_ns,
+                                 cudaStream_t s);
+/* stage 0: owner grid and done flags; 1: phase A prediction; 2: phase A
+ * residual; 3: the dependency-scheduled phase B. */
+cudaError_t launch_recon_stage(int stage, const FrameArgs& a, int n_sm, cudaStream_t s);
 cudaError_t launch_deblock(px_t* pic, const DeblockRec* recs, int n, int sharpness, int bd,
                            int maxv, cudaStream_t s);
 cudaError_t launch_cdef(const px_t* src, px_t* dst, const CdefRec* recs, int n, const Layout& L,
@@ -72,9 +77,10 @@ cudaError_t launch_cdef(const px_t* src, px_t* dst, const CdefRec* recs, int n, 
 cudaError_t launch_upscale(const px_t* src, px_t* dst, const Layout& L, int maxv, cudaStream_t s);
 cudaError_t launch_lr(const px_t* cdef, const px_t* curr, px_t* dst, const Layout& L,
                       const LrArgs& r, int maxv, cudaStream_t s);
-cudaError_t launch_grain(const px_t* src, px_t* dst, const Layout& L, GrainState* gs,
-                         const GrainParamsDev& prm, const uint16_t* orbit, const uint16_t* pos,
-                         cudaStream_t s);
+cudaError_t launch_grain_template(GrainState* gs, const GrainParamsDev& prm, const uint16_t* orbit,
+                                  const uint16_t* pos, cudaStream_t s);
+cudaError_t launch_grain_blend(const px_t* src, px_t* dst, const Layout& L, const GrainState* gs,
+                               const uint16_t* orbit, const uint16_t* pos, cudaStream_t s);
 cudaError_t launch_nv12(const px_t* pic, uint8_t* out, const Layout& L, int pitch, cudaStream_t s);
 cudaError_t launch_rgb(const px_t* pic, uint8_t* out, const Layout& L, const RgbArgs& m,
                        cudaStream_t s);

@@ -191,6 +191,24 @@ AV1B_API int av1b_decode(av1b_decoder* dec, const av1b_frame_syntax* syntax, int
 AV1B_API int av1b_decode_blob(av1b_decoder* dec, const uint8_t* blob, size_t len, int keep_reference,
                      const av1b_planes* out, int* out_slot, char* error, size_t error_len);
 
+/* --- pipelined form: Decoder::plan_frame / decode_reference_planned /
+ * discard_frame_plan (av1gpu.hpp:670-712). A plan holds one frame's validated
+ * device records and coefficient pools, already uploaded into device memory it
+ * owns, so a pipeline can plan frame N+1 while frame N runs and the decode
+ * itself is device work only. The reference slots a plan reads must be held
+ * (decoded, or reserved and decoded before the plan is decoded). */
+typedef struct av1b_plan av1b_plan;
+AV1B_API int av1b_plan_frame(av1b_decoder* dec, const av1b_frame_syntax* syntax, av1b_plan** out);
+/* Decodes a plan into `slot` (a reserved or held slot; -1: the lowest free
+ * slot when `keep_reference`, none otherwise). `wait` == 0 returns once the
+ * work is queued on the decoder's stream: call av1b_sync before reading
+ * anything the frame produced on the host. The plan can be decoded again. */
+AV1B_API int av1b_decode_planned(av1b_decoder* dec, av1b_plan* plan, int slot, int keep_reference,
+                                 const av1b_planes* out, int* out_slot, int wait);
+AV1B_API int av1b_plan_free(av1b_decoder* dec, av1b_plan* plan);
+/* Waits for queued work and reports a device-side failure of the last frame. */
+AV1B_API int av1b_sync(av1b_decoder* dec);
+
 /* Decoder::reserve_reference / decode_reference_reserved (av1gpu.hpp:645-661). */
 AV1B_API int av1b_reserve_reference(av1b_decoder* dec, int* out_slot);
 AV1B_API int av1b_decode_reserved(av1b_decoder* dec, const av1b_frame_syntax* syntax, int slot,
@@ -231,6 +249,26 @@ AV1B_API int av1b_slot_planes_device(av1b_decoder* dec, int slot, uint16_t* plan
 /* The message of the last failed call on this decoder (empty if none). The
  * pointer stays valid until the next call on the decoder. */
 AV1B_API const char* av1b_last_error(av1b_decoder* dec);
+
+/* The limit of one device-side dependency wait (default 1 s). A wait that runs
+ * out sets the status word; the frame then fails with AV1B_ERR_TIMEOUT and
+ * every later wait of the frame gives up at once, so a broken frame ends in
+ * about one limit instead of hanging the device. */
+AV1B_API int av1b_set_wait_limit(av1b_decoder* dec, long long limit_ns);
+/* Failure-detection self test: one device wait on a flag nothing ever sets,
+ * bounded by `limit_ns`. Fills the resulting status word (1: the wait gave up)
+ * and the elapsed device time. */
+AV1B_API int av1b_selftest_wait(av1b_decoder* dec, long long limit_ns, int* status,
+                                double* elapsed_ms);
+
+/* Per-stage device timing: with profiling on, every launch (and device copy)
+ * is bracketed by CUDA events on the decoder's stream, and the elapsed times
+ * are summed per stage at each synchronisation. av1b_profile returns 1 and
+ * fills the stage's name, total milliseconds and launch count, 0 past the last
+ * stage. Switching profiling on or off clears the totals. */
+AV1B_API int av1b_set_profiling(av1b_decoder* dec, int on);
+AV1B_API int av1b_profile(av1b_decoder* dec, int stage, const char** name, double* total_ms,
+                          long long* count);
 
 /* CUDA stream the decoder runs on (a cudaStream_t), so a caller can order its
  * own work after a decode without a host synchronisation. */

@@ -1,15 +1,21 @@
-"""The oracle, for the tests: the reference's own CPU backend (built by
+"""The oracle (TEST INFRASTRUCTURE ONLY; used by tests/, the smoke check and
+bench.py's CPU-baseline leg): the reference's own CPU backend (built by
 oracle/Makefile into oracle/_ref/libav1ref.so) behind a small Python class
 that mirrors av1ongpu_b200.Decoder. Test infrastructure only."""
 import ctypes
+import sys
 import os
 
 import numpy as np
 
-import av1ongpu_b200 as av1b
+
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 REF_LIB = os.path.join(ROOT, 'oracle', '_ref', 'libav1ref.so')
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+import av1ongpu_b200 as av1b  # noqa: E402  (plane_shapes, nv12_size)
+
 _ref = None
 
 

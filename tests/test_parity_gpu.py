@@ -1,0 +1,215 @@
+"""GPU parity: the CUDA path against the oracle (the reference's own CPU
+backend) on the same seeded FrameSyntax, sample for sample, and against the
+committed golden hashes. Every comparison is exact: the path is integer."""
+import numpy as np
+import pytest
+
+import golden_util
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope='module')
+def dec(av1b):
+    if not av1b.cuda_available():
+        pytest.skip('no CUDA device')
+    d = av1b.Decoder(0)
+    yield d
+    d.close()
+
+
+def first_mismatch(a, b):
+    d = np.argwhere(a != b)
+    if not len(d):
+        return None
+    y, x = d[0]
+    return 'n=%d first (y=%d, x=%d) gpu=%d oracle=%d' % (len(d), y, x, a[y, x], b[y, x])
+
+
+def run_pair(av1b, refdec, dec, params, n, seed=4242, check_outputs=True):
+    """Decodes n frames of a generated stream with both decoders and compares
+    the planes of every frame; the NV12 and RGB packs of the newest and an
+    older slot at the end."""
+    ref = refdec.RefDecoder()
+    sg, sr = refdec.Stream(dec), refdec.Stream(ref)
+    w, h = params[0], params[1]
+    for k in range(n):
+        b = av1b.synth_frame_ex(*params[:6], seed, k, params[6])
+        _, pg = sg.decode(k, b)
+        _, pr = sr.decode(k, b)
+        for p in range(3):
+            mm = first_mismatch(pg[p], pr[p])
+            assert mm is None, 'frame %d plane %d: %s' % (k, p, mm)
+    if check_outputs:
+        pitch = (w + 63) & ~63
+        for k in (n - 1, max(0, n - 2)):
+            a = dec.to_nv12(sg.slots[k], pitch, w, h)
+            b = ref.to_nv12(sr.slots[k], pitch, w, h)
+            assert np.array_equal(a, b), 'NV12 of frame %d' % k
+        a = dec.to_rgb(sg.slots[n - 1], 1, 0, w, h)
+        b = ref.to_rgb(sr.slots[n - 1], 1, 0, w, h)
+        assert np.array_equal(a, b), 'RGB'
+    for s in list(sg.slots.values()):
+        dec.release_reference(s)
+
+
+def stage_cases(av1b):
+    A = av1b
+    nodb = A.TOOL_NO_DEBLOCK | A.TOOL_NO_CDEF
+    intra = A.TOOL_TX64 | A.TOOL_ALLTYPES | A.TOOL_CFL | A.TOOL_PALETTE | A.TOOL_FILTER_INTRA | \
+        A.TOOL_EDGE_VARIANTS
+    inter = A.TOOL_TX64 | A.TOOL_ALLTYPES | A.TOOL_COMPOUND | A.TOOL_MASKS | A.TOOL_OBMC | A.TOOL_WARP
+    return {
+        'intra_itx_8bit': ((160, 96, 0, 8, 64, nodb, 0), 1),
+        'inter_8bit': ((160, 96, 0, 8, 64, nodb, 0), 3),
+        'deblock_8bit': ((160, 96, 0, 8, 64, A.TOOL_NO_CDEF, 0), 3),
+        'config1_small': ((160, 96, 0, 8, 64, 0, 0), 4),
+        'odd_size': ((150, 90, 0, 8, 64, 0, 0), 3),
+        'intra_tools_10bit': ((240, 136, 0, 10, 64, intra | nodb, 30), 1),
+        'inter_tools_10bit': ((240, 136, 0, 10, 64, inter | nodb, 30), 4),
+        'all_no_lr_grain': ((240, 136, 0, 10, 64, A.TOOLS_ALL & ~(A.TOOL_LR | A.TOOL_GRAIN), 30), 4),
+        'loop_restoration': ((240, 136, 0, 10, 64, A.TOOLS_ALL & ~A.TOOL_GRAIN, 30), 3),
+        'film_grain': ((240, 136, 0, 10, 64, A.TOOLS_ALL, 30), 3),
+        'superres_128sb': ((480, 270, 360, 10, 128, A.TOOLS_ALL, 30), 3),
+        'interintra_intrabc_residual': ((240, 136, 0, 10, 64, A.TOOLS_ALL | A.TOOL_INTERINTRA |
+                                         A.TOOL_INTRABC | A.TOOL_RESIDUAL, 30), 4),
+        'lossless': ((160, 96, 0, 8, 64, A.TOOL_LOSSLESS, 0), 2),
+        'bitdepth_12': ((192, 128, 0, 12, 64, A.TOOLS_ALL, 30), 2),
+        'tiny_16x16': ((16, 16, 0, 8, 64, A.TOOLS_ALL, 30), 3),
+        'key_interval_2': ((128, 72, 0, 10, 64, A.TOOLS_ALL, 2), 5),
+    }
+
+
+CASES = ['intra_itx_8bit', 'inter_8bit', 'deblock_8bit', 'config1_small', 'odd_size',
+         'intra_tools_10bit', 'inter_tools_10bit', 'all_no_lr_grain', 'loop_restoration',
+         'film_grain', 'superres_128sb', 'interintra_intrabc_residual', 'lossless', 'bitdepth_12',
+         'tiny_16x16', 'key_interval_2']
+
+
+@pytest.mark.parametrize('name', CASES)
+def test_stage_parity(av1b, oracle, dec, name):
+    params, n = stage_cases(av1b)[name]
+    run_pair(av1b, oracle, dec, params, n)
+
+
+@pytest.mark.parametrize('config,scale,frames', [(1, 2, 3), (2, 2, 3), (3, 4, 3)])
+def test_config_parity_reduced(av1b, oracle, dec, config, scale, frames):
+    """The three workloads at a reduced size, through av1b_synth_frame."""
+    ref = oracle.RefDecoder()
+    sg, sr = oracle.Stream(dec), oracle.Stream(ref)
+    for k in range(frames):
+        b = av1b.synth_frame(config, scale, 99, k)
+        _, pg = sg.decode(k, b)
+        _, pr = sr.decode(k, b)
+        for p in range(3):
+            assert first_mismatch(pg[p], pr[p]) is None, (k, p)
+    for s in list(sg.slots.values()):
+        dec.release_reference(s)
+
+
+def test_golden_hashes(av1b, dec):
+    """Against the committed fixtures: works without the oracle build."""
+    for case in golden_util.load():
+        got = golden_util.run_case(dec, case, av1b)
+        assert got == case['frames'], case['name']
+        dec.reset()
+
+
+def test_full_size_4k_superres_parity(av1b, oracle, dec):
+    """Config 3 at its full size (coded 2880x2160 -> 3840x2160, 10-bit), the key
+    frame and two inter frames, against the oracle."""
+    ref = oracle.RefDecoder()
+    sg, sr = oracle.Stream(dec), oracle.Stream(ref)
+    for k in range(3):
+        b = av1b.synth_frame(3, 1, 5, k)
+        _, pg = sg.decode(k, b)
+        _, pr = sr.decode(k, b)
+        for p in range(3):
+            assert first_mismatch(pg[p], pr[p]) is None, (k, p)
+    a = dec.to_nv12(sg.slots[2], 4096, 3840, 2160)
+    b = ref.to_nv12(sr.slots[2], 4096, 3840, 2160)
+    assert np.array_equal(a, b)
+    for s in list(sg.slots.values()):
+        dec.release_reference(s)
+
+
+def test_planned_decode_matches_direct(av1b, dec):
+    """plan_frame + decode_reference_planned gives the direct decode's pixels,
+    also when the frames are queued without waiting."""
+    blobs = [av1b.synth_frame(2, 8, 31, k) for k in range(4)]
+    w, _, h, _, sx, sy = blobs[0].header
+    shapes = av1b.plane_shapes(w, h, sx, sy)
+    import refdec
+    direct = refdec.Stream(dec)
+    want = [direct.decode(k, b)[1] for k, b in enumerate(blobs)]
+    for s in list(direct.slots.values()):
+        dec.release_reference(s)
+    ring = [dec.reserve_reference() for _ in range(4)]
+    plans = []
+    for k, b in enumerate(blobs):
+        d = b.get_refs()
+        b.set_refs([ring[(k - x) % 4] for x in d])
+        plans.append(dec.plan(b))
+        b.set_refs(d)
+    got = []
+    for k, pl in enumerate(plans):
+        planes = [np.empty(s, dtype=np.uint16) for s in shapes]
+        dec.decode_planned(pl, slot=ring[k % 4], keep=True, wait=False, planes=planes)
+        got.append(planes)
+    dec.sync()
+    for k in range(4):
+        for p in range(3):
+            assert np.array_equal(got[k][p], want[k][p]), (k, p)
+    for pl in plans:
+        dec.free_plan(pl)
+    for s in ring:
+        dec.release_reference(s)
+
+
+def test_decode_drop_and_slot_semantics(av1b, oracle, dec):
+    """decode (keep = False) holds no slot; to_nv12 of an older slot packs its
+    stored picture (before film grain), of the newest the output picture."""
+    b0 = av1b.synth_frame(2, 8, 8, 0)
+    b1 = av1b.synth_frame(2, 8, 8, 1)
+    w, _, h, _, _, _ = b0.header
+    ref = oracle.RefDecoder()
+    s0g, _ = dec.decode(b0)
+    s0r, _ = ref.decode(b0)
+    b1.set_refs([s0g])
+    dec.decode(b1, keep=False)
+    b1.set_refs([s0r])
+    ref.decode(b1, keep=False)
+    pitch = (w + 63) & ~63
+    assert np.array_equal(dec.to_nv12(s0g, pitch, w, h), ref.to_nv12(s0r, pitch, w, h))
+    assert np.array_equal(dec.to_nv12(-1, pitch, w, h), ref.to_nv12(-1, pitch, w, h))
+    dec.release_reference(s0g)
+
+
+def test_errors_are_reported_not_faulted(av1b, dec):
+    b = av1b.synth_frame(1, 8, 3, 1)
+    b.set_refs([31])  # a slot that holds nothing
+    with pytest.raises(av1b.Av1bError) as e:
+        dec.decode(b)
+    assert e.value.code == -4
+    with pytest.raises(av1b.Av1bError):
+        dec.to_nv12(0, 63, 160, 90)
+    # the decoder is still usable
+    slot, planes = dec.decode(av1b.synth_frame(1, 8, 3, 0))
+    assert slot >= 0 and planes[0].shape == (90, 160)
+    dec.release_reference(slot)
+
+
+def test_bounded_wait_gives_up(dec):
+    """A device wait on a flag nothing sets returns an error status after its
+    limit instead of hanging (no fault, no trap)."""
+    status, ms = dec.selftest_wait(2_000_000)  # 2 ms
+    assert status == 1
+    assert 1.0 < ms < 1000.0
+
+
+def test_hbm_budget_is_enforced(av1b):
+    d = av1b.Decoder(0, hbm_budget=1 << 20)
+    with pytest.raises(av1b.Av1bError) as e:
+        d.decode(av1b.synth_frame(1, 8, 1, 0))
+    assert e.value.code == -3
+    d.close()
