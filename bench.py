@@ -55,6 +55,7 @@ def parse():
     ap.add_argument('--scale', type=int, default=1, help='divide the picture size (tests only)')
     ap.add_argument('--frames', type=int, default=GOP, help='frames per step')
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--no-e2e', action='store_true', help='skip the end-to-end leg (profiling runs)')
     return ap.parse_args()
 
 
@@ -350,13 +351,15 @@ def run_ours(args):
             if rc:
                 raise av1b.Av1bError(rc, 'to_nv12')
 
-    e2e_step()  # warm-up
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        e2e_step()
-    torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
+    e2e_s = float('inf')
+    if not args.no_e2e:
+        e2e_step()  # warm-up
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            e2e_step()
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t0
     if dist is not None:
         t = torch.tensor([e2e_s], device='cuda:%d' % local)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
