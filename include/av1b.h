@@ -274,6 +274,32 @@ AV1B_API int av1b_profile(av1b_decoder* dec, int stage, const char** name, doubl
  * own work after a decode without a host synchronisation. */
 AV1B_API void* av1b_decoder_stream(av1b_decoder* dec);
 
+/* --- film grain without allocation -----------------------------------------
+ * No counterpart in the reference: its film grain runs inside decode only.
+ * For callers that cannot allocate device memory where they need a frame's
+ * grain - a display callback re-showing a reference slot (which holds the
+ * picture before grain) under a real-time deadline, where cudaMalloc/cudaFree
+ * may synchronize the device, or a host that fixes its device memory at
+ * start-up. It applies `syntax`'s film grain (syntax->grain, its size, bit
+ * depth, subsampling and colour matrix; nothing else of the syntax is read) to
+ * the picture in `src` and writes the output picture to `dst`: three device
+ * planes each, strides in samples, queued on `stream` (a cudaStream_t, 0 for
+ * the default stream). Without grain (apply == 0) it copies src to dst.
+ *
+ * It allocates nothing. Its scratch is a file-scope device array of
+ * AV1B_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until
+ * exit; pictures above AV1B_NOALLOC_MAX_DIM samples on a side are refused
+ * (AV1B_ERR_ARG). The first call on a device sets the scratch up (resolves its
+ * address, builds the grain LFSR tables, and waits for that): make it before
+ * any stream capture. Calls share the scratch, so calls that overlap on the
+ * GPU race; serialize them. */
+#define AV1B_NOALLOC_SCRATCH_BYTES 301312
+#define AV1B_NOALLOC_MAX_DIM 16384
+AV1B_API int av1b_apply_film_grain_noalloc(const av1b_frame_syntax* syntax,
+                                           const uint16_t* const src[3], const int32_t src_stride[3],
+                                           uint16_t* const dst[3], const int32_t dst_stride[3],
+                                           void* stream);
+
 /* --- synthetic input -------------------------------------------------------
  * The seeded synthetic FrameSyntax the benchmarks and tests decode. `config`
  * selects a workload (1..3, see av1ongpu_b200/csrc/synth.cpp), `scale` divides
