@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -74,6 +75,8 @@ struct av1b_decoder {
 
   /* pictures */
   DevBuf cur, snap, lr_pre, lr_pre_up, lr_cdef, disp;
+  DevBuf cdef_search;             /* CDEF direction search results */
+  std::vector<int> cdef_search_at; /* planner scratch: search index per 8x8 luma block */
   bool disp_is_cur = true;
   DevBuf slot_buf[kSlots];
   bool slot_used[kSlots] = {false};
@@ -96,6 +99,10 @@ struct av1b_decoder {
   bool stats_pending = false;
   std::string err;
   cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  /* a side stream for work that depends only on the frame's parameters (the
+   * film grain templates), joined before its consumer */
+  cudaStream_t aux = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   int* status_host = nullptr;          /* pinned */
   void* slot_ptr_host[32] = {nullptr};
   struct av1b_plan* own_plan = nullptr;
@@ -267,6 +274,7 @@ struct Plan {
   std::vector<int2> itx_jobs;
   std::vector<DeblockRec> deblock_v, deblock_h;
   std::vector<CdefRec> cdef;
+  std::vector<unsigned> cdef_search;  /* luma positions to search, x | y << 16 */
   std::vector<LrUnitRec> lr_units[3];
   LrArgs lr{};
   bool use_lr = false;
@@ -544,6 +552,53 @@ int build_plan(av1b_decoder* d, const av1b_frame_syntax& s, Plan* P) {
           P->inter_tiles.push_back(make_int2(static_cast<int>(bi), x0 | (y0 << 16)));
     }
   }
+  /* The claim order of the dependency-scheduled blocks. Coding order is a
+   * valid order but serializes the picture: the blocks in flight all sit in
+   * one superblock row, each waiting for its left neighbour. Ordering by the
+   * anti-diagonal of the superblock a block lies in (2 * row + column), coding
+   * order inside a superblock, keeps every dependency earlier in the order -
+   * left (t - 1), above (t - 2), above-right (t - 1, and only when it was
+   * decoded before the block), corner (t - 3), co-located luma (same
+   * superblock); below-left in another superblock is never decoded before -
+   * while the superblocks of a diagonal run together. The key has to use the
+   * stream's superblock size (64 or 128): it is read from the coding order,
+   * where 128x128 superblocks visit the 64x64 region (1, 0) before (0, 2). An
+   * intra block copy may read further right in the rows above (a larger key),
+   * so a frame with one keeps coding order. */
+  {
+    bool intrabc = false;
+    for (int bi : P->units)
+      if (P->blocks[bi].kind == AV1B_U_INTRABC) intrabc = true;
+    if (!intrabc && P->units.size() > 1) {
+      size_t first_row1 = SIZE_MAX, first_col2 = SIZE_MAX;
+      for (size_t bi = 0; bi < P->blocks.size(); ++bi) {
+        const BlockRec& b = P->blocks[bi];
+        if (b.plane != 0) continue;
+        if ((b.y >> 6) == 1 && first_row1 == SIZE_MAX) first_row1 = bi;
+        if ((b.y >> 6) == 0 && (b.x >> 6) >= 2 && first_col2 == SIZE_MAX) first_col2 = bi;
+        if (first_row1 != SIZE_MAX && first_col2 != SIZE_MAX) break;
+      }
+      const int sb_log2 = first_row1 < first_col2 ? 7 : 6;
+      const int cols = ((L.p[0].grid_w + kPadLuma) >> sb_log2) + 2;
+      const int rows = ((L.p[0].grid_h + kPadLuma) >> sb_log2) + 2;
+      const int nkeys = 2 * rows + cols + 2;
+      std::vector<int> key(P->units.size());
+      std::vector<int> count(nkeys + 1, 0);
+      for (size_t i = 0; i < P->units.size(); ++i) {
+        const BlockRec& b = P->blocks[P->units[i]];
+        const int sx = b.plane ? L.ss_x : 0, sy = b.plane ? L.ss_y : 0;
+        const int c = std::min((b.x << sx) >> sb_log2, cols - 1);
+        const int r = std::min((b.y << sy) >> sb_log2, rows - 1);
+        key[i] = 2 * r + c;
+        ++count[key[i] + 1];
+      }
+      for (int k = 0; k < nkeys; ++k) count[k + 1] += count[k];
+      std::vector<int> sorted(P->units.size());
+      for (size_t i = 0; i < P->units.size(); ++i) sorted[count[key[i]]++] = P->units[i];
+      P->units.swap(sorted);
+    }
+  }
+
   /* the pools read past the caller's arrays as zeros, like the reference's
    * padded plan pools (engine.cpp:665-674) */
   P->coef_pool = std::max(coef_end + 64, s.n_coefficients);
@@ -586,8 +641,13 @@ int build_plan(av1b_decoder* d, const av1b_frame_syntax& s, Plan* P) {
     }
   }
 
-  /* CDEF */
+  /* CDEF: each luma block whose direction is searched is searched once, for
+   * its own record and those of the chroma blocks it covers */
   P->cdef.resize(s.n_cdef);
+  P->cdef_search.clear();
+  const int sgw = L.p[0].stride >> 3;
+  std::vector<int>& search_at = d->cdef_search_at;
+  search_at.assign(static_cast<size_t>(sgw) * (plane_rows(L, 0) >> 3), -1);
   for (size_t i = 0; i < s.n_cdef; ++i) {
     const av1b_cdef_block& c = s.cdef[i];
     if (c.plane < 0 || c.plane > 2) return fail(d, AV1B_ERR_SYNTAX, "CDEF plane out of range");
@@ -608,6 +668,18 @@ int build_plan(av1b_decoder* d, const av1b_frame_syntax& s, Plan* P) {
     r.sec = static_cast<unsigned char>(c.sec_strength);
     r.damping = static_cast<unsigned char>(c.damping);
     r.dir = static_cast<signed char>(c.dir);
+    r.search = -1;
+    if (c.dir < 0) {
+      const int lx = c.x << sx, ly = c.y << sy;
+      int* at = ((lx | ly) & 7) ? nullptr : &search_at[static_cast<size_t>(ly >> 3) * sgw + (lx >> 3)];
+      if (at && *at >= 0) {
+        r.search = *at;
+      } else {
+        r.search = static_cast<int>(P->cdef_search.size());
+        P->cdef_search.push_back(static_cast<unsigned>(lx) | (static_cast<unsigned>(ly) << 16));
+        if (at) *at = r.search;
+      }
+    }
   }
 
   /* loop restoration */
@@ -761,15 +833,16 @@ cudaEvent_t pool_event(av1b_decoder* d) {
 
 /* Runs `launch`; with profiling on, brackets it with two events. */
 template <class F>
-cudaError_t timed(av1b_decoder* d, int stage, F launch) {
+cudaError_t timed(av1b_decoder* d, int stage, F launch, cudaStream_t on = nullptr) {
   if (!d->profiling) return launch();
+  if (!on) on = d->stream;
   const size_t i0 = d->ev_used;
   cudaEvent_t a = pool_event(d);
   cudaEvent_t b = pool_event(d);
   if (!a || !b) return cudaErrorMemoryAllocation;
-  cudaEventRecord(a, d->stream);
+  cudaEventRecord(a, on);
   const cudaError_t e = launch();
-  cudaEventRecord(b, d->stream);
+  cudaEventRecord(b, on);
   d->marks.push_back(std::make_pair(stage, i0));
   return e;
 }
@@ -810,7 +883,7 @@ struct av1b_plan {
   av1b::DevBuf arena, coef, residual;
   size_t o_blocks = 0, o_txs = 0, o_obmc = 0, o_warps = 0, o_pal = 0, o_units = 0;
   size_t o_tiles = 0, o_itx = 0, o_dbv = 0, o_dbh = 0, o_cdef = 0, o_lr[3] = {0, 0, 0};
-  size_t o_map = 0;
+  size_t o_map = 0, o_cdef_search = 0;
   int slots_read[kSlots + 1];     /* the reference slots the frame reads, -1 ended */
   int n_blocks = 0;
   bool owned_by_decoder = false;
@@ -862,6 +935,7 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
   pl->o_dbv = stage_put(&off, P.deblock_v);
   pl->o_dbh = stage_put(&off, P.deblock_h);
   pl->o_cdef = stage_put(&off, P.cdef);
+  pl->o_cdef_search = stage_put(&off, P.cdef_search);
   for (int p = 0; p < 3; ++p) pl->o_lr[p] = stage_put(&off, P.lr_units[p]);
   pl->o_map = off;
   off = align_up(off + s.n_palette_map + 64, 256);
@@ -884,6 +958,7 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
   put(pl->o_dbv, P.deblock_v.data(), P.deblock_v.size() * sizeof(DeblockRec));
   put(pl->o_dbh, P.deblock_h.data(), P.deblock_h.size() * sizeof(DeblockRec));
   put(pl->o_cdef, P.cdef.data(), P.cdef.size() * sizeof(CdefRec));
+  put(pl->o_cdef_search, P.cdef_search.data(), P.cdef_search.size() * sizeof(unsigned));
   for (int p = 0; p < 3; ++p)
     put(pl->o_lr[p], P.lr_units[p].data(), P.lr_units[p].size() * sizeof(LrUnitRec));
   put(pl->o_map, s.palette_map, s.n_palette_map);
@@ -956,6 +1031,9 @@ int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, cons
     if ((rc = dev_ensure(d, d->slot_buf[slot], static_cast<size_t>(L.size) * sizeof(px_t)))) return rc;
   }
   const size_t pic_bytes = static_cast<size_t>(L.size) * sizeof(px_t);
+  if (!P.cdef_search.empty() &&
+      (rc = dev_ensure(d, d->cdef_search, P.cdef_search.size() * sizeof(int))))
+    return rc;
   if (P.use_lr) {
     if ((rc = dev_ensure(d, d->lr_pre, pic_bytes)) || (rc = dev_ensure(d, d->lr_cdef, pic_bytes)) ||
         (P.upscaled && (rc = dev_ensure(d, d->lr_pre_up, pic_bytes))))
@@ -1037,6 +1115,24 @@ int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, cons
   a.wait_ns = d->wait_ns;
 
   int launches = 0;
+  if (P.grain) {
+    /* the grain templates depend only on the parameters: build them on the
+     * side stream while the picture is reconstructed. The fork point orders
+     * them after the previous frame's blend, which read the same state. */
+    GrainState* gsd = static_cast<GrainState*>(d->grain_state.p);
+    const size_t tail = offsetof(GrainState, lut);
+    CK(cudaEventRecord(d->ev_fork, st), "fork");
+    CK(cudaStreamWaitEvent(d->aux, d->ev_fork, 0), "fork wait");
+    CK(cudaMemcpyAsync(reinterpret_cast<uint8_t*>(gsd) + tail,
+                       reinterpret_cast<const uint8_t*>(&P.gs_tail) + tail, sizeof(GrainState) - tail,
+                       cudaMemcpyHostToDevice, d->aux), "grain constants");
+    CK(timed(d, kStGrainTemplate, [&] {
+         return launch_grain_template(gsd, P.gp, static_cast<const uint16_t*>(d->orbit.p),
+                                      static_cast<const uint16_t*>(d->pos.p), d->aux);
+       }, d->aux), "film grain template");
+    CK(cudaEventRecord(d->ev_join, d->aux), "join");
+    ++launches;
+  }
   CK(cudaEventRecord(ev[0], st), "event");
   for (int stage = 0; stage < 4; ++stage) {
     const bool any = stage == 0 ? a.n_blocks > 0
@@ -1074,7 +1170,10 @@ int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, cons
        }), "CDEF snapshot");
     CK(timed(d, kStCdef, [&] {
          return launch_cdef(snap, cur, reinterpret_cast<const CdefRec*>(ar + pl->o_cdef),
-                            static_cast<int>(P.cdef.size()), L, st);
+                            static_cast<int>(P.cdef.size()),
+                            reinterpret_cast<const unsigned*>(ar + pl->o_cdef_search),
+                            static_cast<int>(P.cdef_search.size()),
+                            static_cast<int*>(d->cdef_search.p), L, st);
        }), "CDEF");
     ++launches;
   }
@@ -1083,12 +1182,12 @@ int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, cons
     CK(timed(d, kStCopy, [&] {
          return cudaMemcpyAsync(snap, cur, pic_bytes, cudaMemcpyDeviceToDevice, st);
        }), "superres snapshot");
-    CK(timed(d, kStUpscale, [&] { return launch_upscale(snap, cur, L, maxv, st); }), "superres");
+    CK(timed(d, kStUpscale, [&] { return launch_upscale(snap, cur, L, maxv, false, st); }), "superres");
     ++launches;
     if (P.use_lr) {
       CK(timed(d, kStUpscale, [&] {
            return launch_upscale(static_cast<px_t*>(d->lr_pre.p), static_cast<px_t*>(d->lr_pre_up.p),
-                                 L, maxv, st);
+                                 L, maxv, true, st);
          }), "superres (pre-CDEF)");
       ++launches;
       lr_curr = static_cast<px_t*>(d->lr_pre_up.p);
@@ -1113,20 +1212,13 @@ int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, cons
   d->disp_is_cur = true;
   if (P.grain) {
     GrainState* gsd = static_cast<GrainState*>(d->grain_state.p);
-    const size_t tail = offsetof(GrainState, lut);
-    CK(cudaMemcpyAsync(reinterpret_cast<uint8_t*>(gsd) + tail,
-                       reinterpret_cast<const uint8_t*>(&P.gs_tail) + tail, sizeof(GrainState) - tail,
-                       cudaMemcpyHostToDevice, st), "grain constants");
-    CK(timed(d, kStGrainTemplate, [&] {
-         return launch_grain_template(gsd, P.gp, static_cast<const uint16_t*>(d->orbit.p),
-                                      static_cast<const uint16_t*>(d->pos.p), st);
-       }), "film grain template");
+    CK(cudaStreamWaitEvent(st, d->ev_join, 0), "join wait");
     CK(timed(d, kStGrainBlend, [&] {
          return launch_grain_blend(cur, static_cast<px_t*>(d->disp.p), L, gsd,
                                    static_cast<const uint16_t*>(d->orbit.p),
                                    static_cast<const uint16_t*>(d->pos.p), st);
        }), "film grain blend");
-    launches += 2;
+    launches += 1;
     display = static_cast<px_t*>(d->disp.p);
     d->disp_is_cur = false;
   }
@@ -1233,6 +1325,9 @@ int av1b_decoder_create(int device, size_t hbm_budget_bytes, av1b_decoder** out)
             set_kernel_attributes() == cudaSuccess &&
             cudaHostAlloc(reinterpret_cast<void**>(&d->status_host), 64, cudaHostAllocDefault) == cudaSuccess;
   for (int i = 0; ok && i < 3; ++i) ok = cudaEventCreate(&d->ev[i]) == cudaSuccess;
+  ok = ok && cudaStreamCreateWithFlags(&d->aux, cudaStreamNonBlocking) == cudaSuccess &&
+       cudaEventCreateWithFlags(&d->ev_fork, cudaEventDisableTiming) == cudaSuccess &&
+       cudaEventCreateWithFlags(&d->ev_join, cudaEventDisableTiming) == cudaSuccess;
   if (!ok) {
     av1b_decoder_destroy(d);
     return AV1B_ERR_CUDA;
@@ -1256,11 +1351,17 @@ int av1b_decoder_destroy(av1b_decoder* d) {
   }
   for (int i = 0; i < 3; ++i)
     if (d->ev[i]) cudaEventDestroy(d->ev[i]);
+  if (d->aux) {
+    cudaStreamSynchronize(d->aux);
+    cudaStreamDestroy(d->aux);
+  }
+  if (d->ev_fork) cudaEventDestroy(d->ev_fork);
+  if (d->ev_join) cudaEventDestroy(d->ev_join);
   if (d->status_host) cudaFreeHost(d->status_host);
   DevBuf* bufs[] = {&d->cur, &d->snap, &d->lr_pre, &d->lr_pre_up, &d->lr_cdef, &d->disp,
                     &d->slot_ptr_dev, &d->arena, &d->coef, &d->residual, &d->owner[0],
                     &d->owner[1], &d->owner[2], &d->done, &d->status_q, &d->nv12, &d->rgb,
-                    &d->grain_state, &d->orbit, &d->pos};
+                    &d->grain_state, &d->orbit, &d->pos, &d->cdef_search};
   for (DevBuf* b : bufs) dev_release(d, *b);
   for (int i = 0; i < kSlots; ++i) dev_release(d, d->slot_buf[i]);
   if (d->stage.p) cudaFreeHost(d->stage.p);

@@ -108,57 +108,8 @@ struct CdefRec {
   short x, y;                 /* plane samples */
   unsigned char plane, pri, sec, damping;
   signed char dir, pad0, pad1, pad2;
+  int search;                 /* direction search result to use when dir < 0 */
 };
-
-AV1B_DEV void cdef_direction(const px_t* luma, int stride, int bd, int* dir_out, int* var_out) {
-  int partial[8][15];
-  int cost[8];
-  for (int i = 0; i < 8; ++i) {
-    cost[i] = 0;
-    for (int j = 0; j < 15; ++j) partial[i][j] = 0;
-  }
-  const int shift = bd - 8;
-  for (int i = 0; i < 8; ++i)
-    for (int j = 0; j < 8; ++j) {
-      const int x = ((int)luma[i * stride + j] >> shift) - 128;
-      partial[0][i + j] += x;
-      partial[1][i + j / 2] += x;
-      partial[2][i] += x;
-      partial[3][3 + i - j / 2] += x;
-      partial[4][7 + i - j] += x;
-      partial[5][3 - i / 2 + j] += x;
-      partial[6][j] += x;
-      partial[7][i / 2 + j] += x;
-    }
-  const int div[9] = {0, 840, 420, 280, 210, 168, 140, 120, 105};
-  for (int i = 0; i < 8; ++i) {
-    cost[2] += partial[2][i] * partial[2][i];
-    cost[6] += partial[6][i] * partial[6][i];
-  }
-  cost[2] *= div[8];
-  cost[6] *= div[8];
-  for (int i = 0; i < 7; ++i) {
-    cost[0] += (partial[0][i] * partial[0][i] + partial[0][14 - i] * partial[0][14 - i]) * div[i + 1];
-    cost[4] += (partial[4][i] * partial[4][i] + partial[4][14 - i] * partial[4][14 - i]) * div[i + 1];
-  }
-  cost[0] += partial[0][7] * partial[0][7] * div[8];
-  cost[4] += partial[4][7] * partial[4][7] * div[8];
-  for (int i = 1; i < 8; i += 2) {
-    for (int j = 0; j < 5; ++j) cost[i] += partial[i][3 + j] * partial[i][3 + j];
-    cost[i] *= div[8];
-    for (int j = 0; j < 3; ++j)
-      cost[i] += (partial[i][j] * partial[i][j] + partial[i][10 - j] * partial[i][10 - j]) *
-                 div[2 * j + 2];
-  }
-  int best = 0, d = 0;
-  for (int i = 0; i < 8; ++i)
-    if (cost[i] > best) {
-      best = cost[i];
-      d = i;
-    }
-  *dir_out = d;
-  *var_out = (best - cost[(d + 4) & 7]) >> 10;
-}
 
 AV1B_DEV int cdef_constrain(int diff, int threshold, int damping) {
   if (!threshold) return 0;
@@ -166,17 +117,6 @@ AV1B_DEV int cdef_constrain(int diff, int threshold, int damping) {
   const int mag = absi(diff);
   const int m = clampi(threshold - (mag >> adj), 0, mag);
   return diff < 0 ? -m : m;
-}
-
-/* Cdef_Directions: (dy, dx) of the first and second tap along each of the
- * eight directions. */
-AV1B_DEV void cdef_dir_offsets(int dir, int k, int* dy, int* dx) {
-  const signed char t[8][2][2] = {
-      {{-1, 1}, {-2, 2}}, {{0, 1}, {-1, 2}}, {{0, 1}, {0, 2}}, {{0, 1}, {1, 2}},
-      {{1, 1}, {2, 2}},   {{1, 0}, {2, 1}},  {{1, 0}, {2, 0}}, {{1, 0}, {2, -1}},
-  };
-  *dy = t[dir][k][0];
-  *dx = t[dir][k][1];
 }
 
 /* ---- superres ------------------------------------------------------------------- */
@@ -194,102 +134,6 @@ struct LrUnitRec {
   int vf[3], hf[3];             /* Wiener coded coefficients */
   int r[2], e[2], xqd[2];       /* self guided */
 };
-
-struct LrSrc {
-  const px_t* cdef;   /* plane origin of the CDEF (and superres) output */
-  const px_t* curr;   /* plane origin of the deblocked picture (upscaled) */
-  int stride;
-  int w, h;           /* visible plane size */
-  int s0, s1;         /* stripe rows, inclusive */
-};
-
-AV1B_DEV int lr_src(const LrSrc& s, int x, int y) {
-  x = clampi(x, 0, s.w - 1);
-  y = clampi(y, 0, s.h - 1);
-  if (y < s.s0) return s.curr[maxi(y, s.s0 - 2) * s.stride + x];
-  if (y > s.s1) return s.curr[mini(y, s.s1 + 2) * s.stride + x];
-  return s.cdef[y * s.stride + x];
-}
-
-AV1B_DEV int lr_wiener(const LrSrc& s, const LrUnitRec& u, int bd, int x, int y) {
-  const int r0 = bd == 12 ? 5 : 3, r1 = bd == 12 ? 9 : 11;
-  const int offset = 1 << (bd + 7 - r0 - 1);
-  const int limit = (1 << (bd + 1 + 7 - r0)) - 1;
-  int vt[7], ht[7];
-  for (int t = 0; t < 3; ++t) {
-    vt[t] = vt[6 - t] = u.vf[t];
-    ht[t] = ht[6 - t] = u.hf[t];
-  }
-  vt[3] = 128 - 2 * (u.vf[0] + u.vf[1] + u.vf[2]);
-  ht[3] = 128 - 2 * (u.hf[0] + u.hf[1] + u.hf[2]);
-  int sum = 0;
-  for (int t = 0; t < 7; ++t) {
-    int acc = 0;
-    for (int k = 0; k < 7; ++k) acc += ht[k] * lr_src(s, x + k - 3, y + t - 3);
-    sum += vt[t] * clampi(rnd2(acc, r0), -offset, limit - offset);
-  }
-  return rnd2(sum, r1);
-}
-
-/* A and B of the box filter centred on (x, y) (7.17.3). */
-AV1B_DEV void sgr_ab(const LrSrc& s, int bd, int x, int y, int r, int eps, int* a_out, int* b_out) {
-  const int n = (2 * r + 1) * (2 * r + 1);
-  const long long n2e = (long long)n * n * eps;
-  const long long mtable = ((1LL << 20) + n2e / 2) / n2e;
-  long long sa = 0, sb = 0;
-  for (int dy = -r; dy <= r; ++dy)
-    for (int dx = -r; dx <= r; ++dx) {
-      const int c = lr_src(s, x + dx, y + dy);
-      sa += (long long)c * c;
-      sb += c;
-    }
-  const long long b_sum = sb;
-  sa = rnd2llz(sa, 2 * (bd - 8));
-  sb = rnd2llz(sb, bd - 8);
-  long long p = sa * n - sb * sb;
-  if (p < 0) p = 0;
-  const int z = rnd2ll(p * mtable, 20);
-  int a2;
-  if (z >= 255) a2 = 256;
-  else if (z == 0) a2 = 1;
-  else a2 = ((z << 8) + (z / 2)) / (z + 1);
-  const int one_over_n = ((1 << 12) + (n / 2)) / n;
-  const long long b2 = (long long)(256 - a2) * b_sum * one_over_n;
-  *a_out = a2;
-  *b_out = rnd2ll(b2, 12);
-}
-
-AV1B_DEV int lr_sgr(const LrSrc& s, const LrUnitRec& u, int bd, int x, int y) {
-  const int v = lr_src(s, x, y);
-  const int w0 = u.xqd[0], w1 = u.xqd[1], w2 = 128 - w0 - w1;
-  int flt[2];
-  for (int pass = 0; pass < 2; ++pass) {
-    const int r = u.r[pass];
-    if (r == 0) {
-      flt[pass] = 0;
-      continue;
-    }
-    int a = 0, b = 0;
-    for (int dy = -1; dy <= 1; ++dy)
-      for (int dx = -1; dx <= 1; ++dx) {
-        int wgt;
-        if (pass == 0) wgt = ((y + dy) & 1) ? (dx == 0 ? 6 : 5) : 0;
-        else wgt = (dx == 0 || dy == 0) ? 4 : 3;
-        if (!wgt) continue;
-        int a2, b2;
-        sgr_ab(s, bd, x + dx, y + dy, r, u.e[pass], &a2, &b2);
-        a += wgt * a2;
-        b += wgt * b2;
-      }
-    const int shift = (pass == 0 && (y & 1)) ? 4 : 5;
-    flt[pass] = rnd2ll((long long)a * v + b, 8 + shift - 4);
-  }
-  const int us = v << 4;
-  long long t = (long long)w1 * us;
-  t += (long long)w0 * (u.r[0] ? flt[0] : us);
-  t += (long long)w2 * (u.r[1] ? flt[1] : us);
-  return rnd2ll(t, 4 + 7);
-}
 
 /* ---- film grain ------------------------------------------------------------------ */
 

@@ -13,9 +13,9 @@
  *     (2076-2100), inter-intra taper and edges (2120-2205);
  *   - the composition order: references, compound / mask blend, clip,
  *     inter-intra, OBMC strips in order (2207-2326).
- * The kernels in recon.cu stage reference tiles in shared memory for the
- * common translation case and fall back to these per-sample forms for the
- * rest.
+ * mc_rect is the separable form of the translation cases for a warp's tile,
+ * with the reference window in shared memory; the per-sample forms serve the
+ * warped references and the blocks of the dependency-scheduled phase.
  */
 #ifndef AV1B_DEV_INTER_CUH
 #define AV1B_DEV_INTER_CUH
@@ -128,6 +128,89 @@ AV1B_DEV int mc_tap(const InterCtx& c, const px_t* ref, int stride, int base_x, 
     return mc_unscaled<CG>(c, ref, stride, base_x, base_y, ew, eh, mvx, mvy, filt, filt_v, x, y,
                            compound);
   return mc_scaled<CG>(c, ref, stride, base_x, base_y, ew, eh, mvx, mvy, filt, filt_v, x, y, compound);
+}
+
+/* Separable motion compensation of a rectangle of a patch, for one warp.
+ * Every output sample of a translation (unscaled or scaled) prediction is
+ * the vertical 8-tap filter over intermediate rows, each the horizontal
+ * 8-tap filter of one reference row rounded by InterRound0; the intermediate
+ * at (reference row, output column) is the same for every output sample that
+ * reads it. So the reference window is staged in shared memory once, the
+ * intermediate rows computed once, then the vertical pass - the same integers
+ * as the per-sample form above (mc_unscaled / mc_scaled), 16 multiplies a
+ * sample instead of 64.
+ * The rectangle is (rx, ry) .. + (rw <= 16, rh <= 8) in patch coordinates;
+ * `out` receives rh rows of 16. Returns false, with nothing written, when the
+ * window does not fit the scratch (a reference scaled by more than 2:1). */
+#define AV1B_MC_WR 24
+#define AV1B_MC_WC 40
+struct McScratch {
+  int win[AV1B_MC_WR * AV1B_MC_WC];
+  int mid[AV1B_MC_WR * 16];
+  int cx[16], xf[16], cy[8], yf[8];
+};
+
+template <bool CG = false>
+AV1B_DEV bool mc_rect(const InterCtx& c, const px_t* ref, int stride, int base_x, int base_y,
+                      int ew, int eh, int mvx, int mvy, int filt, int filt_v, int compound, int rx,
+                      int ry, int rw, int rh, McScratch& s, int* out, int lane) {
+  const bool unscaled = c.scale_x == AV1B_SCALE_ONE && c.scale_y == AV1B_SCALE_ONE;
+  if (lane < rw || (lane >= 16 && lane - 16 < rh)) {
+    const int k = lane & 15;
+    int px, py, fx, fy;
+    if (unscaled) {
+      const int mx = mvx * 2, my = mvy * 2;
+      px = base_x + rx + k + (mx >> (4 + c.sub_x));
+      fx = (mx >> c.sub_x) & 15;
+      py = base_y + ry + k + (my >> (4 + c.sub_y));
+      fy = (my >> c.sub_y) & 15;
+    } else {
+      scaled_pos(c, base_x, base_y, mvx, mvy, rx + k, ry + k, &px, &py, &fx, &fy);
+    }
+    if (lane < 16) {
+      s.cx[k] = px;
+      s.xf[k] = fx;
+    } else {
+      s.cy[k] = py;
+      s.yf[k] = fy;
+    }
+  }
+  __syncwarp();
+  const int cbase = s.cx[0] - 3, rbase = s.cy[0] - 3;
+  const int ncols = s.cx[rw - 1] + 5 - cbase, nrows = s.cy[rh - 1] + 5 - rbase;
+  if (ncols > AV1B_MC_WC || nrows > AV1B_MC_WR) {
+    __syncwarp();
+    return false;
+  }
+  for (int k = lane; k < nrows * ncols; k += 32) {
+    const int r = k / ncols, q = k - r * ncols;
+    s.win[r * AV1B_MC_WC + q] = fetch<CG>(ref, stride, cbase + q, rbase + r, c.ref_w - 1, c.ref_h - 1);
+  }
+  __syncwarp();
+  const int fh = filt_row(filt, ew), fv = filt_row(filt_v, eh);
+  int r0, r1;
+  rounds(c.bitdepth, compound, &r0, &r1);
+  for (int k = lane; k < nrows * rw; k += 32) {
+    const int r = k / rw, x = k - r * rw;
+    const int* w = s.win + r * AV1B_MC_WC + s.cx[x] - 3 - cbase;
+    const short* f = kSubpelFilters + (fh * 16 + s.xf[x]) * 8;
+    int sum = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) sum += w[i] * f[i];
+    s.mid[r * 16 + x] = (sum + (1 << (r0 - 1))) >> r0;
+  }
+  __syncwarp();
+  for (int k = lane; k < rh * rw; k += 32) {
+    const int y = k / rw, x = k - y * rw;
+    const int* m = s.mid + (s.cy[y] - 3 - rbase) * 16 + x;
+    const short* f = kSubpelFilters + (fv * 16 + s.yf[y]) * 8;
+    int acc = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc += m[j * 16] * f[j];
+    out[y * 16 + x] = (acc + (1 << (r1 - 1))) >> r1;
+  }
+  __syncwarp();
+  return true;
 }
 
 AV1B_DEV int warp_offs(int v) {
@@ -317,19 +400,12 @@ AV1B_DEV int ii_mask(const InterJob& b, int x, int y) {
   return kIiWeights[mini(k, 127)];
 }
 
-/* The block's prediction before inter-intra and OBMC, clipped. */
+/* The composition of the block's two predictions `v0`, `v1` (or one) at
+ * (x, y): average, distance weights or a mask, then the clip. */
 template <bool CG = false>
-AV1B_DEV int inter_core(const InterJob& b, int x, int y) {
-  const int compound = b.compound != 0;
-  int v[2] = {0, 0};
-  const int nref = compound ? 2 : 1;
-  for (int r = 0; r < nref; ++r)
-    v[r] = b.warp[r] ? warp_tap<CG>(b.ctx.sub_x, b.ctx.sub_y, b.ctx.ref_w, b.ctx.ref_h, *b.model[r],
-                                b.ref[r], b.ref_stride, b.x, b.y, x, y, b.ctx.bitdepth, compound)
-                     : mc_tap<CG>(b.ctx, b.ref[r], b.ref_stride, b.x, b.y, b.w, b.h, b.mv[r][0],
-                              b.mv[r][1], b.filt, b.filt_v, x, y, compound);
-  int out = v[0];
-  if (compound) {
+AV1B_DEV int inter_compose(const InterJob& b, int x, int y, int v0, int v1) {
+  int out = v0;
+  if (b.compound) {
     const int round0 = b.ctx.bitdepth >= 12 ? 5 : 3;
     const int post = 7 - round0;
     if (b.mask_kind != 0) {
@@ -344,7 +420,7 @@ AV1B_DEV int inter_core(const InterJob& b, int x, int y) {
             m = wedge_px(b.wedge_dir, b.wedge_xoff, b.wedge_yoff, b.wedge_flip, ly, lx);
             if (b.mask_sign) m = 64 - m;
           } else if (b.plane == 0) {
-            m = diffwtd_m(absi(v[0] - v[1]), sh, b.mask_sign);
+            m = diffwtd_m(absi(v0 - v1), sh, b.mask_sign);
           } else {
             m = diffwtd_m(absi(mask_luma_diff<CG>(b, lx, ly, b.w << b.ctx.sub_x, b.h << b.ctx.sub_y)),
                           sh, b.mask_sign);
@@ -353,14 +429,38 @@ AV1B_DEV int inter_core(const InterJob& b, int x, int y) {
         }
       const int n = nx * ny;
       const int m = n == 1 ? sum : (n == 2 ? (sum + 1) >> 1 : (sum + 2) >> 2);
-      out = (m * v[0] + (64 - m) * v[1] + (1 << (5 + post))) >> (6 + post);
+      out = (m * v0 + (64 - m) * v1 + (1 << (5 + post))) >> (6 + post);
     } else if (b.compound == 1) {
-      out = (v[0] + v[1] + (1 << post)) >> (1 + post);
+      out = (v0 + v1 + (1 << post)) >> (1 + post);
     } else {
-      out = (b.w0 * v[0] + b.w1 * v[1] + (1 << (3 + post))) >> (4 + post);
+      out = (b.w0 * v0 + b.w1 * v1 + (1 << (3 + post))) >> (4 + post);
     }
   }
   return clampi(out, 0, b.maxv);
+}
+
+/* One reference's prediction of sample (x, y), per sample. */
+template <bool CG = false>
+AV1B_DEV int inter_ref(const InterJob& b, int r, int x, int y) {
+  const int compound = b.compound != 0;
+  return b.warp[r] ? warp_tap<CG>(b.ctx.sub_x, b.ctx.sub_y, b.ctx.ref_w, b.ctx.ref_h, *b.model[r],
+                                  b.ref[r], b.ref_stride, b.x, b.y, x, y, b.ctx.bitdepth, compound)
+                   : mc_tap<CG>(b.ctx, b.ref[r], b.ref_stride, b.x, b.y, b.w, b.h, b.mv[r][0],
+                                b.mv[r][1], b.filt, b.filt_v, x, y, compound);
+}
+
+/* The block's prediction before inter-intra and OBMC, clipped. */
+template <bool CG = false>
+AV1B_DEV int inter_core(const InterJob& b, int x, int y) {
+  const int v0 = inter_ref<CG>(b, 0, x, y);
+  const int v1 = b.compound ? inter_ref<CG>(b, 1, x, y) : 0;
+  return inter_compose<CG>(b, x, y, v0, v1);
+}
+
+AV1B_DEV int obmc_blend(const ObmcRec& c, int j, int i, int out, int pred, int maxv) {
+  const int m = c.pass == 0 ? obmc_mask(c.h, i) : obmc_mask(c.w, j);
+  pred = clampi(pred, 0, maxv);
+  return (m * out + (64 - m) * pred + 32) >> 6;
 }
 
 /* Inter-intra and OBMC on top of a clipped prediction `out`. */
@@ -374,11 +474,9 @@ AV1B_DEV int inter_finish(const InterJob& b, int x, int y, int out, int ii_dc_va
     const ObmcRec& c = b.obmc[k];
     if (x < c.x || x >= c.x + c.w || y < c.y || y >= c.y + c.h) continue;
     const int j = x - c.x, i = y - c.y;
-    const int m = c.pass == 0 ? obmc_mask(c.h, i) : obmc_mask(c.w, j);
-    int pred = mc_tap(b.ctx, b.obmc_ref[k], b.ref_stride, b.x + c.x, b.y + c.y, c.w, c.h, c.mv_x,
-                      c.mv_y, c.filt, c.filt_v, j, i, 0);
-    pred = clampi(pred, 0, b.maxv);
-    out = (m * out + (64 - m) * pred + 32) >> 6;
+    const int pred = mc_tap(b.ctx, b.obmc_ref[k], b.ref_stride, b.x + c.x, b.y + c.y, c.w, c.h,
+                            c.mv_x, c.mv_y, c.filt, c.filt_v, j, i, 0);
+    out = obmc_blend(c, j, i, out, pred, b.maxv);
   }
   return out;
 }

@@ -130,7 +130,7 @@ __device__ void make_inter_job(const FrameArgs& a, const BlockRec& b, InterJob* 
 /* ---- phase A ------------------------------------------------------------------------ */
 
 /* Owner grid and done flags: one warp per block. */
-__global__ void k_owner(FrameArgs a) {
+__global__ void k_owner(const __grid_constant__ FrameArgs a) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= a.n_blocks) return;
@@ -147,10 +147,14 @@ __global__ void k_owner(FrameArgs a) {
   if (lane == 0 && !b.phase_b) a.done[warp] = a.epoch;
 }
 
-/* Inter prediction of phase A blocks: one warp per 16x8 tile. */
-__global__ void k_inter(FrameArgs a) {
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
+/* Inter prediction of phase A blocks: one warp per 16x8 tile. Translation
+ * predictions (and OBMC strips) go through mc_rect, warped ones per sample;
+ * the composition and the OBMC blends run per sample on registers. */
+__global__ void __launch_bounds__(128) k_inter(const __grid_constant__ FrameArgs a) {
+  __shared__ McScratch scr[4];
+  __shared__ int pred[4][2][8 * 16];
+  const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int warp = blockIdx.x * 4 + wib;
   if (warp >= a.n_inter_tiles) return;
   const int2 t = a.inter_tiles[warp];
   const BlockRec& b = a.blocks[t.x];
@@ -160,11 +164,72 @@ __global__ void k_inter(FrameArgs a) {
   const int tw = mini(16, b.w - x0), th = mini(8, b.h - y0);
   const PlaneGeom& g = a.L.p[b.plane];
   px_t* dst = a.cur + g.off + (b.y + y0) * g.stride + b.x + x0;
-  for (int k = lane; k < tw * th; k += 32) {
-    const int yy = k / tw, xx = k - yy * tw;
-    int v = inter_core(j, x0 + xx, y0 + yy);
-    v = inter_finish(j, x0 + xx, y0 + yy, v, 0);
-    dst[yy * g.stride + xx] = (px_t)v;
+  if (j.interintra) {
+    /* inter-intra reads this frame: scheduled with the dependency phase */
+    for (int k = lane; k < tw * th; k += 32) {
+      const int yy = k / tw, xx = k - yy * tw;
+      int v = inter_core(j, x0 + xx, y0 + yy);
+      v = inter_finish(j, x0 + xx, y0 + yy, v, 0);
+      dst[yy * g.stride + xx] = (px_t)v;
+    }
+    return;
+  }
+  const int nref = j.compound ? 2 : 1;
+  for (int r = 0; r < nref; ++r) {
+    int* pr = pred[wib][r];
+    const bool ok = !j.warp[r] &&
+                    mc_rect(j.ctx, j.ref[r], j.ref_stride, j.x, j.y, j.w, j.h, j.mv[r][0],
+                            j.mv[r][1], j.filt, j.filt_v, j.compound != 0, x0, y0, tw, th, scr[wib],
+                            pr, lane);
+    if (!ok) {
+      for (int k = lane; k < tw * th; k += 32) {
+        const int yy = k / tw, xx = k - yy * tw;
+        pr[yy * 16 + xx] = inter_ref(j, r, x0 + xx, y0 + yy);
+      }
+      __syncwarp();
+    }
+  }
+  int acc[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int k = lane + 32 * q;
+    if (k < tw * th) {
+      const int yy = k / tw, xx = k - yy * tw;
+      acc[q] = inter_compose(j, x0 + xx, y0 + yy, pred[wib][0][yy * 16 + xx],
+                             nref > 1 ? pred[wib][1][yy * 16 + xx] : 0);
+    }
+  }
+  __syncwarp();
+  for (int kk = 0; kk < j.obmc_count; ++kk) {
+    const ObmcRec& c = j.obmc[kk];
+    const int ix0 = maxi(c.x, x0), ix1 = mini(c.x + c.w, x0 + tw);
+    const int iy0 = maxi(c.y, y0), iy1 = mini(c.y + c.h, y0 + th);
+    if (ix0 >= ix1 || iy0 >= iy1) continue;
+    int* tmp = pred[wib][0];
+    const bool ok = mc_rect(j.ctx, j.obmc_ref[kk], j.ref_stride, j.x + c.x, j.y + c.y, c.w, c.h,
+                            c.mv_x, c.mv_y, c.filt, c.filt_v, 0, ix0 - c.x, iy0 - c.y, ix1 - ix0,
+                            iy1 - iy0, scr[wib], tmp, lane);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int k = lane + 32 * q;
+      if (k >= tw * th) continue;
+      const int yy = k / tw, xx = k - yy * tw;
+      const int x = x0 + xx, y = y0 + yy;
+      if (x < ix0 || x >= ix1 || y < iy0 || y >= iy1) continue;
+      const int pv = ok ? tmp[(y - iy0) * 16 + x - ix0]
+                        : mc_tap(j.ctx, j.obmc_ref[kk], j.ref_stride, j.x + c.x, j.y + c.y, c.w,
+                                 c.h, c.mv_x, c.mv_y, c.filt, c.filt_v, x - c.x, y - c.y, 0);
+      acc[q] = obmc_blend(c, x - c.x, y - c.y, acc[q], pv, j.maxv);
+    }
+    __syncwarp();
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int k = lane + 32 * q;
+    if (k < tw * th) {
+      const int yy = k / tw, xx = k - yy * tw;
+      dst[yy * g.stride + xx] = (px_t)acc[q];
+    }
   }
 }
 
@@ -196,7 +261,7 @@ __device__ void apply_tx(const FrameArgs& a, const BlockRec& b, const TxRec& tx,
 }
 
 /* Residual of phase A blocks: one warp per transform. */
-__global__ void k_itx(FrameArgs a) {
+__global__ void k_itx(const __grid_constant__ FrameArgs a) {
   extern __shared__ int smem[];
   const int wib = threadIdx.x >> 5;
   const int warp = blockIdx.x * (blockDim.x >> 5) + wib;
@@ -260,7 +325,9 @@ __device__ bool decoded_before(const FrameArgs& a, int p, int x0, int x1, int y0
 }
 
 /* Waits for the owners of the cells of [x0, x1] x [y0, y1] of plane p that
- * precede `bi`. Warp-collective. */
+ * precede `bi` in coding order. The claim order (see the planner) puts every
+ * such owner before this block, so each one has been claimed by a running
+ * warp. Warp-collective. */
 __device__ void wait_rect(const FrameArgs& a, int p, int x0, int x1, int y0, int y1, int bi,
                           int lane) {
   const int oc = 1 << a.cell_shift[p];
@@ -275,7 +342,7 @@ __device__ void wait_rect(const FrameArgs& a, int p, int x0, int x1, int y0, int
 
 /* The persistent dependency-scheduled kernel. Shared memory per warp: three
  * edge buffers and a 64x64 transform scratch. */
-__global__ void __launch_bounds__(128) k_units(FrameArgs a) {
+__global__ void __launch_bounds__(128) k_units(const __grid_constant__ FrameArgs a) {
   extern __shared__ int smem[];
   const int wib = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
@@ -402,133 +469,378 @@ __global__ void k_deblock(px_t* pic, const DeblockRec* recs, int n, int sharpnes
 }
 
 /* ---- CDEF ------------------------------------------------------------------------------ */
-__global__ void k_cdef(const px_t* __restrict__ src, px_t* dst, const CdefRec* recs, int n,
-                       Layout L) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const CdefRec r = recs[i];
+/* CDEF direction search (av1gpu_kernels.h:2601-2660), one thread per 8x8 luma
+ * block: the 90 partial sums of the eight directions stay in registers (the
+ * loops unroll, so every bin index is a constant). The result packs
+ * (variance << 3) | direction. Chroma blocks read the search of their luma
+ * block, so each luma block is searched once. */
+__global__ void __launch_bounds__(128) k_cdef_search(const px_t* __restrict__ src,
+                                                     const unsigned* __restrict__ pos, int n,
+                                                     int* out, const __grid_constant__ Layout L) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const unsigned q = pos[t];
+  const int x = q & 0xffff, y = q >> 16;
+  const int stride = L.p[0].stride, cs = L.bit_depth - 8;
+  const px_t* b = src + L.p[0].off + y * stride + x;
+  int p0[15] = {}, p1[11] = {}, p2[8] = {}, p3[11] = {}, p4[15] = {}, p5[11] = {}, p6[8] = {},
+      p7[11] = {};
+  const bool vec = ((L.p[0].off + y * stride + x) & 7) == 0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    int v[8];
+    if (vec) {
+      const uint4 w = __ldg(reinterpret_cast<const uint4*>(b + i * stride));
+      const unsigned u[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        v[2 * k] = u[k] & 0xffff;
+        v[2 * k + 1] = u[k] >> 16;
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) v[j] = b[i * stride + j];
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int s = (v[j] >> cs) - 128;
+      p0[i + j] += s;
+      p1[i + j / 2] += s;
+      p2[i] += s;
+      p3[3 + i - j / 2] += s;
+      p4[7 + i - j] += s;
+      p5[3 - i / 2 + j] += s;
+      p6[j] += s;
+      p7[i / 2 + j] += s;
+    }
+  }
+  const int div[9] = {0, 840, 420, 280, 210, 168, 140, 120, 105};
+  int cost[8];
+  cost[2] = cost[6] = 0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    cost[2] += p2[i] * p2[i];
+    cost[6] += p6[i] * p6[i];
+  }
+  cost[2] *= div[8];
+  cost[6] *= div[8];
+  cost[0] = p0[7] * p0[7] * div[8];
+  cost[4] = p4[7] * p4[7] * div[8];
+#pragma unroll
+  for (int i = 0; i < 7; ++i) {
+    cost[0] += (p0[i] * p0[i] + p0[14 - i] * p0[14 - i]) * div[i + 1];
+    cost[4] += (p4[i] * p4[i] + p4[14 - i] * p4[14 - i]) * div[i + 1];
+  }
+  int* odd[4] = {p1, p3, p5, p7};
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int* pt = odd[k];
+    int c = 0;
+#pragma unroll
+    for (int j = 0; j < 5; ++j) c += pt[3 + j] * pt[3 + j];
+    c *= div[8];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) c += (pt[j] * pt[j] + pt[10 - j] * pt[10 - j]) * div[2 * j + 2];
+    cost[2 * k + 1] = c;
+  }
+  int best = 0, d = 0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+    if (cost[i] > best) {
+      best = cost[i];
+      d = i;
+    }
+  int opp = 0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+    if (i == ((d + 4) & 7)) opp = cost[i];
+  out[t] = (((best - opp) >> 10) << 3) | d;
+}
+
+__constant__ signed char kCdefDirs[8][2][2] = {
+    {{-1, 1}, {-2, 2}}, {{0, 1}, {-1, 2}}, {{0, 1}, {0, 2}}, {{0, 1}, {1, 2}},
+    {{1, 1}, {2, 2}},   {{1, 0}, {2, 1}},  {{1, 0}, {2, 0}}, {{1, 0}, {2, -1}},
+};
+__constant__ unsigned char kCdefUvDir[2][2][8] = {{{0, 1, 2, 3, 4, 5, 6, 7}, {1, 2, 2, 2, 3, 4, 6, 0}},
+                                                  {{7, 0, 2, 4, 5, 6, 6, 6}, {0, 1, 2, 3, 4, 5, 6, 7}}};
+
+/* CDEF filter (av1gpu_kernels.h:2662-2775), one warp per block: the block and
+ * its 2-sample halo staged in shared memory, one or two samples per lane. */
+__global__ void __launch_bounds__(128) k_cdef_warp(const px_t* __restrict__ src, px_t* dst,
+                                                   const CdefRec* recs, int n,
+                                                   const int* __restrict__ search,
+                                                   const __grid_constant__ Layout L) {
+  __shared__ int sw[4][12 * 12];
+  const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ri = blockIdx.x * 4 + wib;
+  if (ri >= n) return;
+  const CdefRec r = recs[ri];
   const int p = r.plane;
   const bool uv = p > 0;
   const PlaneGeom& g = L.p[p];
-  const int bd = L.bit_depth, maxv = (1 << bd) - 1;
-  const int cs = bd - 8;
+  const int bd = L.bit_depth, maxv = (1 << bd) - 1, cs = bd - 8;
   const int w = uv ? (8 >> L.ss_x) : 8, h = uv ? (8 >> L.ss_y) : 8;
+  const int pw = g.grid_w, ph = g.grid_h;
+  int* win = sw[wib];
+  /* the block and its halo; rows and columns above or left of the buffer
+   * clamp into it (taps outside the plane are never used) */
+  for (int k = lane; k < (h + 4) * (w + 4); k += 32) {
+    const int i = k / (w + 4), j = k - i * (w + 4);
+    const int y = maxi(r.y - 2 + i, 0), x = maxi(r.x - 2 + j, 0);
+    win[i * 12 + j] = src[g.off + y * g.stride + x];
+  }
   int pri = r.pri << cs, sec = r.sec << cs;
   const int damping = r.damping + cs - (uv ? 1 : 0);
   int dir = r.dir;
   if (dir < 0) {
-    const int lx = uv ? r.x << L.ss_x : r.x, ly = uv ? r.y << L.ss_y : r.y;
-    int ydir = 0, var = 0;
-    cdef_direction(src + L.p[0].off + ly * L.p[0].stride + lx, L.p[0].stride, bd, &ydir, &var);
+    const int sr = search[r.search];
+    const int ydir = sr & 7, var = sr >> 3;
     if (uv) {
-      const unsigned char uvd[2][2][8] = {{{0, 1, 2, 3, 4, 5, 6, 7}, {1, 2, 2, 2, 3, 4, 6, 0}},
-                                          {{7, 0, 2, 4, 5, 6, 6, 6}, {0, 1, 2, 3, 4, 5, 6, 7}}};
-      dir = pri == 0 ? 0 : uvd[L.ss_x][L.ss_y][ydir];
+      dir = pri == 0 ? 0 : kCdefUvDir[L.ss_x][L.ss_y][ydir];
     } else {
       const int vs = (var >> 6) ? mini(floor_log2(var >> 6), 12) : 0;
       dir = pri == 0 ? 0 : ydir;
       pri = var ? ((pri * (4 + vs) + 8) >> 4) : 0;
     }
   }
-  const px_t* s = src + g.off + r.y * g.stride + r.x;
+  __syncwarp();
   px_t* d = dst + g.off + r.y * g.stride + r.x;
-  const int pw = g.grid_w, ph = g.grid_h;
   if (pri == 0 && sec == 0) {
-    for (int i2 = 0; i2 < h && r.y + i2 < ph; ++i2)
-      for (int j = 0; j < w && r.x + j < pw; ++j) d[i2 * g.stride + j] = s[i2 * g.stride + j];
+    for (int k = lane; k < w * h; k += 32) {
+      const int i = k / w, j = k - i * w;
+      if (r.y + i < ph && r.x + j < pw) d[i * g.stride + j] = (px_t)win[(i + 2) * 12 + j + 2];
+    }
     return;
   }
-  const int pri_taps[2][2] = {{4, 2}, {3, 3}};
-  const int sec_taps[2] = {2, 1};
   const int ts = (pri >> cs) & 1;
-  for (int i2 = 0; i2 < h; ++i2)
-    for (int j = 0; j < w; ++j) {
-      const int x = s[i2 * g.stride + j];
-      int sum = 0, lo = x, hi = x;
-      for (int k = 0; k < 2; ++k)
+  const int pt0 = ts ? 3 : 4, pt1 = ts ? 3 : 2;
+  for (int k = lane; k < w * h; k += 32) {
+    const int i = k / w, j = k - i * w;
+    if (r.y + i >= ph || r.x + j >= pw) continue;
+    const int x = win[(i + 2) * 12 + j + 2];
+    int sum = 0, lo = x, hi = x;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      const int dd = q == 0 ? dir : (q == 1 ? (dir + 6) & 7 : (dir + 2) & 7);
+      const int th = q == 0 ? pri : sec;
+#pragma unroll
+      for (int t = 0; t < 2; ++t) {
+        const int oy = kCdefDirs[dd][t][0], ox = kCdefDirs[dd][t][1];
+        const int tap = q == 0 ? (t == 0 ? pt0 : pt1) : (t == 0 ? 2 : 1);
+#pragma unroll
         for (int sg = -1; sg <= 1; sg += 2) {
-          int dy, dx;
-          cdef_dir_offsets(dir, k, &dy, &dx);
-          dy *= sg;
-          dx *= sg;
-          int px = r.x + j + dx, py = r.y + i2 + dy;
-          if (px >= 0 && px < pw && py >= 0 && py < ph) {
-            const int v = s[(i2 + dy) * g.stride + j + dx];
-            sum += pri_taps[ts][k] * cdef_constrain(v - x, pri, damping);
-            lo = mini(lo, v);
-            hi = maxi(hi, v);
-          }
-          for (int off = -2; off <= 2; off += 4) {
-            cdef_dir_offsets((dir + off) & 7, k, &dy, &dx);
-            dy *= sg;
-            dx *= sg;
-            px = r.x + j + dx;
-            py = r.y + i2 + dy;
-            if (px >= 0 && px < pw && py >= 0 && py < ph) {
-              const int v = s[(i2 + dy) * g.stride + j + dx];
-              sum += sec_taps[k] * cdef_constrain(v - x, sec, damping);
-              lo = mini(lo, v);
-              hi = maxi(hi, v);
-            }
-          }
+          const int dy = sg * oy, dx = sg * ox;
+          const int px = r.x + j + dx, py = r.y + i + dy;
+          if (px < 0 || px >= pw || py < 0 || py >= ph) continue;
+          const int v = win[(i + 2 + dy) * 12 + j + 2 + dx];
+          sum += tap * cdef_constrain(v - x, th, damping);
+          lo = mini(lo, v);
+          hi = maxi(hi, v);
         }
-      if (r.x + j >= pw || r.y + i2 >= ph) continue;
-      d[i2 * g.stride + j] =
-          (px_t)clampi(clampi(x + ((8 + sum - (sum < 0)) >> 4), lo, hi), 0, maxv);
+      }
     }
+    d[i * g.stride + j] = (px_t)clampi(clampi(x + ((8 + sum - (sum < 0)) >> 4), lo, hi), 0, maxv);
+  }
 }
 
 /* ---- superres ------------------------------------------------------------------------- */
-__global__ void k_upscale(const px_t* __restrict__ src, px_t* dst, Layout L, int maxv) {
+/* One thread per 4 output samples of a row. `border_rows`: only the rows
+ * within two of a loop restoration stripe boundary (the rows the restoration
+ * reads from the pre-CDEF picture, av1gpu_kernels.h:2832-2845); the reference
+ * upscales the whole pre-CDEF picture and reads only these. */
+__global__ void k_upscale(const px_t* __restrict__ src, px_t* dst,
+                          const __grid_constant__ Layout L,
+                          const __grid_constant__ UpscaleArgs u,
+                          int maxv, int border_rows) {
   const int p = blockIdx.z;
   const PlaneGeom& g = L.p[p];
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y;
-  if (x >= g.out_w || y >= g.out_h) return;
-  int step, initial;
-  superres_params(g.coded_w, g.out_w, &step, &initial);
-  const int sx = -(1 << 14) + initial + x * step;
-  const int px = sx >> 14;
-  const int ph = (sx & ((1 << 14) - 1)) >> 8;
+  int y = blockIdx.y;
+  if (border_rows) {
+    const int sub_y = p > 0 ? L.ss_y : 0;
+    const int b = (64 * (y / 4 + 1) - 8) >> sub_y;
+    y = b - 2 + (y & 3);
+    if (y < 0) return;
+  }
+  if (y >= g.out_h) return;
+  const int x0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
+  if (x0 >= g.out_w) return;
   const px_t* row = src + g.off + y * g.stride;
-  int sum = 0;
+  px_t* out = dst + g.off + y * g.stride;
+  const int last = g.coded_w - 1;
 #pragma unroll
-  for (int k = 0; k < 8; ++k)
-    sum += (int)row[clampi(px + k - 3, 0, g.coded_w - 1)] * kUpscaleFilter[ph * 8 + k];
-  dst[g.off + y * g.stride + x] = (px_t)clampi(rnd2(sum, 7), 0, maxv);
+  for (int q = 0; q < 4; ++q) {
+    const int x = x0 + q;
+    if (x >= g.out_w) break;
+    const int sx = -(1 << 14) + u.initial[p] + x * u.step[p];
+    const int px = sx >> 14;
+    const short* f = kUpscaleFilter + ((sx & ((1 << 14) - 1)) >> 8) * 8;
+    int sum = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) sum += (int)row[clampi(px + k - 3, 0, last)] * f[k];
+    out[x] = (px_t)clampi(rnd2(sum, 7), 0, maxv);
+  }
 }
 
 /* ---- loop restoration --------------------------------------------------------------------- */
-__global__ void k_lr(const px_t* __restrict__ cdef, const px_t* __restrict__ curr, px_t* dst,
-                     Layout L, LrArgs r, int maxv) {
+/* Loop restoration by tiles: one CTA per (plane, stripe piece, 32 columns).
+ * A stripe piece is the rows of one 64-row luma stripe (offset by 8), so every
+ * sample of the tile reads through the same stripe mapping (get_source_sample,
+ * av1gpu_kernels.h:2832-2845), and a 32-column tile lies in one restoration
+ * unit (units are 32..256 wide; the last one of a row extends to the edge).
+ * The source window (3 samples of margin) is staged in shared memory once.
+ * Wiener runs as a horizontal pass into an intermediate (rounded and clipped
+ * like the reference's) and a vertical pass. Self-guided computes A and B of
+ * every box position the tile needs once - the reference recomputes them nine
+ * times per output sample (av1gpu_kernels.h:2928-2970) - then projects. */
+#define AV1B_LR_TW 32
+#define AV1B_LR_MAXR 64
+#define AV1B_LR_WR (AV1B_LR_MAXR + 6)
+#define AV1B_LR_WC (AV1B_LR_TW + 6)
+#define AV1B_LR_AR (AV1B_LR_MAXR + 2)
+#define AV1B_LR_AC (AV1B_LR_TW + 2)
+
+__global__ void __launch_bounds__(256) k_lr_tile(const px_t* __restrict__ cdef,
+                                                 const px_t* __restrict__ curr, px_t* dst,
+                                                 const __grid_constant__ Layout L,
+                                                 const __grid_constant__ LrArgs r, int maxv) {
+  __shared__ int win[AV1B_LR_WR * AV1B_LR_WC];
+  __shared__ int aux[2][2][AV1B_LR_AR * AV1B_LR_AC];  /* Wiener: aux[0][0] = intermediate */
   const int p = blockIdx.z;
   if (!r.type[p]) return;
   const PlaneGeom& g = L.p[p];
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y;
-  if (x >= g.out_w || y >= g.out_h) return;
   const int sub_y = p > 0 ? L.ss_y : 0;
-  const int us = r.unit_size[p];
-  const int stripe = ((y << sub_y) + 8) / 64;
+  const int x0 = blockIdx.x * AV1B_LR_TW;
+  if (x0 >= g.out_w) return;
+  /* the stripe piece */
+  const int stripe = blockIdx.y;
   const int s0 = (-8 + stripe * 64) >> sub_y;
   const int s1 = s0 + (64 >> sub_y) - 1;
-  const int ystart = maxi(s0, 0);
-  const int urow = mini(r.unit_rows[p] - 1, ((((ystart << sub_y) + 8) >> sub_y) / us));
-  const int ucol = mini(r.unit_cols[p] - 1, x / us);
+  const int y0 = maxi(s0, 0), y1 = mini(g.out_h, s1 + 1);
+  if (y0 >= y1) return;
+  const int us = r.unit_size[p];
+  const int urow = mini(r.unit_rows[p] - 1, ((((y0 << sub_y) + 8) >> sub_y) / us));
+  const int ucol = mini(r.unit_cols[p] - 1, x0 / us);
   const int idx = urow * r.unit_cols[p] + ucol;
   if (idx >= r.n_units[p]) return;
   const LrUnitRec u = r.units[p][idx];
   if (u.type != 1 && u.type != 2) return;
-  LrSrc s;
-  s.cdef = cdef + g.off;
-  s.curr = curr + g.off;
-  s.stride = g.stride;
-  s.w = g.out_w;
-  s.h = g.out_h;
-  s.s0 = s0;
-  s.s1 = s1;
-  const int v = u.type == 1 ? lr_wiener(s, u, L.bit_depth, x, y) : lr_sgr(s, u, L.bit_depth, x, y);
-  dst[g.off + y * g.stride + x] = (px_t)clampi(v, 0, maxv);
+  const int tw = mini(AV1B_LR_TW, g.out_w - x0), th = y1 - y0;
+  const int wr = th + 6, wc = tw + 6;
+  const px_t* pc = cdef + g.off;
+  const px_t* pp = curr + g.off;
+  /* source window: rows y0-3 .., columns x0-3 .. */
+  for (int k = threadIdx.x; k < wr * wc; k += blockDim.x) {
+    const int i = k / wc, j = k - i * wc;
+    const int x = clampi(x0 - 3 + j, 0, g.out_w - 1);
+    const int y = clampi(y0 - 3 + i, 0, g.out_h - 1);
+    int v;
+    if (y < s0) v = pp[maxi(y, s0 - 2) * g.stride + x];
+    else if (y > s1) v = pp[mini(y, s1 + 2) * g.stride + x];
+    else v = pc[y * g.stride + x];
+    win[i * AV1B_LR_WC + j] = v;
+  }
+  __syncthreads();
+  const int bd = L.bit_depth;
+  px_t* out = dst + g.off + y0 * g.stride + x0;
+  if (u.type == 1) {
+    const int r0 = bd == 12 ? 5 : 3, r1 = bd == 12 ? 9 : 11;
+    const int offset = 1 << (bd + 7 - r0 - 1);
+    const int limit = (1 << (bd + 1 + 7 - r0)) - 1;
+    int ht[7], vt[7];
+    for (int t = 0; t < 3; ++t) {
+      ht[t] = ht[6 - t] = u.hf[t];
+      vt[t] = vt[6 - t] = u.vf[t];
+    }
+    ht[3] = 128 - 2 * (u.hf[0] + u.hf[1] + u.hf[2]);
+    vt[3] = 128 - 2 * (u.vf[0] + u.vf[1] + u.vf[2]);
+    /* the intermediate has up to 70 rows: it spans aux[0][0] and aux[0][1] */
+    static_assert(AV1B_LR_WR * AV1B_LR_AC <= 2 * AV1B_LR_AR * AV1B_LR_AC, "Wiener intermediate");
+    int* mid = &aux[0][0][0];
+    for (int k = threadIdx.x; k < wr * tw; k += blockDim.x) {
+      const int i = k / tw, j = k - i * tw;
+      const int* w = win + i * AV1B_LR_WC + j;
+      int acc = 0;
+#pragma unroll
+      for (int t = 0; t < 7; ++t) acc += ht[t] * w[t];
+      mid[i * AV1B_LR_AC + j] = clampi(rnd2(acc, r0), -offset, limit - offset);
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < th * tw; k += blockDim.x) {
+      const int i = k / tw, j = k - i * tw;
+      int acc = 0;
+#pragma unroll
+      for (int t = 0; t < 7; ++t) acc += vt[t] * mid[(i + t) * AV1B_LR_AC + j];
+      out[i * g.stride + j] = (px_t)clampi(rnd2(acc, r1), 0, maxv);
+    }
+    return;
+  }
+  /* self-guided: A and B of both passes on rows y0-1 .. y1, columns x0-1 .. */
+  const int ar = th + 2, ac = tw + 2;
+  for (int pass = 0; pass < 2; ++pass) {
+    const int rad = u.r[pass];
+    if (rad == 0) continue;
+    const int n = (2 * rad + 1) * (2 * rad + 1);
+    const long long n2e = (long long)n * n * u.e[pass];
+    const long long mtable = ((1LL << 20) + n2e / 2) / n2e;
+    const int one_over_n = ((1 << 12) + (n / 2)) / n;
+    for (int k = threadIdx.x; k < ar * ac; k += blockDim.x) {
+      const int i = k / ac, j = k - i * ac;
+      /* the first pass reads odd rows only */
+      if (pass == 0 && !((y0 - 1 + i) & 1)) continue;
+      long long sa = 0;
+      int sb = 0;
+      for (int dy = -rad; dy <= rad; ++dy) {
+        const int* w = win + (i + 2 + dy) * AV1B_LR_WC + j + 2;
+        for (int dx = -rad; dx <= rad; ++dx) {
+          const int c = w[dx];
+          sa += c * c;
+          sb += c;
+        }
+      }
+      const int b_sum = sb;
+      sa = rnd2llz(sa, 2 * (bd - 8));
+      const long long sbs = rnd2z(sb, bd - 8);
+      long long pv = sa * n - sbs * sbs;
+      if (pv < 0) pv = 0;
+      const int z = rnd2ll(pv * mtable, 20);
+      int a2;
+      if (z >= 255) a2 = 256;
+      else if (z == 0) a2 = 1;
+      else a2 = ((z << 8) + (z / 2)) / (z + 1);
+      const long long b2 = (long long)(256 - a2) * b_sum * one_over_n;
+      aux[pass][0][i * AV1B_LR_AC + j] = a2;
+      aux[pass][1][i * AV1B_LR_AC + j] = rnd2ll(b2, 12);
+    }
+  }
+  __syncthreads();
+  const int w0 = u.xqd[0], w1 = u.xqd[1], w2 = 128 - w0 - w1;
+  for (int k = threadIdx.x; k < th * tw; k += blockDim.x) {
+    const int i = k / tw, j = k - i * tw;
+    const int y = y0 + i;
+    const int v = win[(i + 3) * AV1B_LR_WC + j + 3];
+    int flt[2] = {0, 0};
+    for (int pass = 0; pass < 2; ++pass) {
+      if (u.r[pass] == 0) continue;
+      int a = 0, b = 0;
+      for (int dy = -1; dy <= 1; ++dy)
+        for (int dx = -1; dx <= 1; ++dx) {
+          int wgt;
+          if (pass == 0) wgt = ((y + dy) & 1) ? (dx == 0 ? 6 : 5) : 0;
+          else wgt = (dx == 0 || dy == 0) ? 4 : 3;
+          if (!wgt) continue;
+          const int o = (i + 1 + dy) * AV1B_LR_AC + j + 1 + dx;
+          a += wgt * aux[pass][0][o];
+          b += wgt * aux[pass][1][o];
+        }
+      const int shift = (pass == 0 && (y & 1)) ? 4 : 5;
+      flt[pass] = rnd2ll((long long)a * v + b, 8 + shift - 4);
+    }
+    const int vs = v << 4;
+    long long t = (long long)w1 * vs;
+    t += (long long)w0 * (u.r[0] ? flt[0] : vs);
+    t += (long long)w2 * (u.r[1] ? flt[1] : vs);
+    out[i * g.stride + j] = (px_t)clampi(rnd2ll(t, 11), 0, maxv);
+  }
 }
 
 /* ---- film grain ------------------------------------------------------------------------------- */
@@ -663,7 +975,8 @@ __device__ int grain_stripe(const GrainState* gs, const short* grain, int src_w,
 
 /* Film grain blend, out of place: `src` is the decoded picture (luma read
  * before any grain), `dst` gets the output picture. One thread per sample. */
-__global__ void k_grain_blend(const px_t* __restrict__ src, px_t* dst, Layout L,
+__global__ void k_grain_blend(const px_t* __restrict__ src, px_t* dst,
+                              const __grid_constant__ Layout L,
                               const GrainState* gs, const uint16_t* orbit, const uint16_t* pos) {
   const int p = blockIdx.z;
   const PlaneGeom& g = L.p[p];
@@ -729,7 +1042,8 @@ __global__ void k_grain_blend(const px_t* __restrict__ src, px_t* dst, Layout L,
  * *coded* width into a display-sized frame that starts out zero
  * (cpu_backend.cpp:576-584), so for a superres frame every sample right of the
  * coded width packs as 0. This kernel reproduces that byte for byte. */
-__global__ void k_nv12(const px_t* __restrict__ pic, uint8_t* out, Layout L, int pitch) {
+__global__ void k_nv12(const px_t* __restrict__ pic, uint8_t* out, const __grid_constant__ Layout L,
+                       int pitch) {
   const int row = blockIdx.y;
   const int x0 = (blockIdx.x * blockDim.x + threadIdx.x) * 8;
   if (x0 >= pitch) return;
@@ -764,7 +1078,8 @@ __global__ void k_nv12(const px_t* __restrict__ pic, uint8_t* out, Layout L, int
   }
 }
 
-__global__ void k_rgb(const px_t* __restrict__ pic, uint8_t* out, Layout L, RgbArgs m) {
+__global__ void k_rgb(const px_t* __restrict__ pic, uint8_t* out, const __grid_constant__ Layout L,
+                      const __grid_constant__ RgbArgs m) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y;
   const int w = L.p[0].out_w;
@@ -794,7 +1109,7 @@ cudaError_t launch_recon_stage(int stage, const FrameArgs& a, int n_sm, cudaStre
       break;
     case 1:
       if (a.n_inter_tiles > 0)
-        k_inter<<<cdiv((long long)a.n_inter_tiles * 32, 256), 256, 0, s>>>(a);
+        k_inter<<<cdiv(a.n_inter_tiles, 4), 128, 0, s>>>(a);
       break;
     case 2:
       if (a.n_itx > 0) k_itx<<<cdiv(a.n_itx, 4), 128, 4 * 4096 * sizeof(int), s>>>(a);
@@ -816,22 +1131,31 @@ cudaError_t launch_deblock(px_t* pic, const DeblockRec* recs, int n, int sharpne
   return cudaGetLastError();
 }
 
-cudaError_t launch_cdef(const px_t* src, px_t* dst, const CdefRec* recs, int n, const Layout& L,
+cudaError_t launch_cdef(const px_t* src, px_t* dst, const CdefRec* recs, int n,
+                        const unsigned* search_pos, int n_search, int* search, const Layout& L,
                         cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
-  k_cdef<<<cdiv(n, 128), 128, 0, s>>>(src, dst, recs, n, L);
+  if (n_search > 0)
+    k_cdef_search<<<cdiv(n_search, 128), 128, 0, s>>>(src, search_pos, n_search, search, L);
+  k_cdef_warp<<<cdiv(n, 4), 128, 0, s>>>(src, dst, recs, n, search, L);
   return cudaGetLastError();
 }
 
-cudaError_t launch_upscale(const px_t* src, px_t* dst, const Layout& L, int maxv, cudaStream_t s) {
-  const int wmax = L.p[0].out_w, hmax = L.p[0].out_h;
-  k_upscale<<<dim3(cdiv(wmax, 128), hmax, 3), 128, 0, s>>>(src, dst, L, maxv);
+cudaError_t launch_upscale(const px_t* src, px_t* dst, const Layout& L, int maxv, bool border_rows,
+                           cudaStream_t s) {
+  UpscaleArgs u;
+  for (int p = 0; p < 3; ++p) superres_params(L.p[p].coded_w, L.p[p].out_w, &u.step[p], &u.initial[p]);
+  const int rows = border_rows ? 4 * ((L.p[0].out_h + 8) / 64 + 1) : L.p[0].out_h;
+  k_upscale<<<dim3(cdiv(cdiv(L.p[0].out_w, 4), 64), rows, 3), 64, 0, s>>>(src, dst, L, u, maxv,
+                                                                         border_rows ? 1 : 0);
   return cudaGetLastError();
 }
 
 cudaError_t launch_lr(const px_t* cdef, const px_t* curr, px_t* dst, const Layout& L,
                       const LrArgs& r, int maxv, cudaStream_t s) {
-  k_lr<<<dim3(cdiv(L.p[0].out_w, 128), L.p[0].out_h, 3), 128, 0, s>>>(cdef, curr, dst, L, r, maxv);
+  const int stripes = (L.p[0].out_h + 8 + 63) / 64;
+  k_lr_tile<<<dim3(cdiv(L.p[0].out_w, AV1B_LR_TW), stripes, 3), 256, 0, s>>>(cdef, curr, dst, L, r,
+                                                                            maxv);
   return cudaGetLastError();
 }
 

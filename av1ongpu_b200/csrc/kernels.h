@@ -59,6 +59,11 @@ struct GrainParamsDev {
   int ar_y[24], ar_cb[25], ar_cr[25];
 };
 
+/* superres: per plane, the Q14 step and the phase of the first column */
+struct UpscaleArgs {
+  int step[3], initial[3];
+};
+
 struct RgbArgs {
   int m[8];
   int o[3];
@@ -72,9 +77,15 @@ cudaError_t launch_selftest_wait(const unsigned* flag, int* status, unsigned lon
 cudaError_t launch_recon_stage(int stage, const FrameArgs& a, int n_sm, cudaStream_t s);
 cudaError_t launch_deblock(px_t* pic, const DeblockRec* recs, int n, int sharpness, int bd,
                            int maxv, cudaStream_t s);
-cudaError_t launch_cdef(const px_t* src, px_t* dst, const CdefRec* recs, int n, const Layout& L,
+/* CDEF: the direction searches (luma positions packed x | y << 16, results
+ * into `search`), then the filter of every record. */
+cudaError_t launch_cdef(const px_t* src, px_t* dst, const CdefRec* recs, int n,
+                        const unsigned* search_pos, int n_search, int* search, const Layout& L,
                         cudaStream_t s);
-cudaError_t launch_upscale(const px_t* src, px_t* dst, const Layout& L, int maxv, cudaStream_t s);
+/* border_rows: only the rows within two of a loop restoration stripe
+ * boundary (for the pre-CDEF picture loop restoration reads). */
+cudaError_t launch_upscale(const px_t* src, px_t* dst, const Layout& L, int maxv, bool border_rows,
+                           cudaStream_t s);
 cudaError_t launch_lr(const px_t* cdef, const px_t* curr, px_t* dst, const Layout& L,
                       const LrArgs& r, int maxv, cudaStream_t s);
 cudaError_t launch_grain_template(GrainState* gs, const GrainParamsDev& prm, const uint16_t* orbit,
