@@ -27,7 +27,9 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <chrono>
 #include <mutex>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -36,6 +38,7 @@
 #include "dev_inter.cuh"
 #include "dev_itx.cuh"
 #include "kernels.h"
+#include "work_pool.hpp"
 #include "plan_host.h"
 
 namespace av1b {
@@ -61,12 +64,29 @@ struct HostBuf {
 
 using namespace av1b;
 
+namespace av1b {
+namespace {
+struct PlanScratch;
+}
+}  // namespace av1b
+
 struct av1b_decoder {
   int device = 0;
   cudaStream_t stream = nullptr;
   int n_sm = 148;
   size_t budget = 0, allocated = 0;
-  std::mutex mu;
+  std::mutex mu;                 /* one decode, output or slot call at a time */
+  /* Planning runs outside `mu` (a pipeline plans frame N+1 on its own thread
+   * while frame N runs): plan_mu serializes planners, slot_mu guards the slot
+   * table planners read, err_mu the error text, alloc_mu the HBM account.
+   * Lock order: mu, plan_mu, slot_mu / alloc_mu / err_mu. */
+  std::mutex plan_mu, slot_mu, err_mu, alloc_mu;
+  av1b::WorkPool* pool = nullptr;
+  av1b::PlanScratch* scratch = nullptr;
+  cudaStream_t upload = nullptr;  /* plan uploads, overlapping the frame in flight */
+  /* freed plans kept with their buffers for the next av1b_plan_frame */
+  std::mutex plan_pool_mu;
+  std::vector<struct av1b_plan*> plan_pool;
 
   /* geometry of the pictures currently allocated */
   bool have_geom = false;
@@ -76,7 +96,7 @@ struct av1b_decoder {
   /* pictures */
   DevBuf cur, snap, lr_pre, lr_pre_up, lr_cdef, disp;
   DevBuf cdef_search;             /* CDEF direction search results */
-  std::vector<int> cdef_search_at; /* planner scratch: search index per 8x8 luma block */
+  DevBuf pre_res;                 /* phase B residuals computed ahead */
   bool disp_is_cur = true;
   DevBuf slot_buf[kSlots];
   bool slot_used[kSlots] = {false};
@@ -87,7 +107,6 @@ struct av1b_decoder {
   bool have_last = false;
 
   /* per-frame buffers */
-  HostBuf stage;
   DevBuf arena, coef, residual, owner[3], done, status_q, nv12, rgb;
   unsigned epoch = 0;
 
@@ -113,21 +132,28 @@ struct av1b_decoder {
   std::vector<cudaEvent_t> ev_pool;
   size_t ev_used = 0;
   std::vector<std::pair<int, size_t>> marks;   /* (stage, index of its start event) */
-  double prof_ms[16] = {0};
-  long long prof_n[16] = {0};
+  double prof_ms[24] = {0};
+  long long prof_n[24] = {0};
 };
 
 namespace av1b {
 namespace {
 
 int fail(av1b_decoder* d, int code, const std::string& msg) {
+  std::lock_guard<std::mutex> lk(d->err_mu);
   d->err = msg;
   return code;
 }
 
 int cuda_fail(av1b_decoder* d, cudaError_t e, const char* what) {
+  std::lock_guard<std::mutex> lk(d->err_mu);
   d->err = std::string(what) + ": " + cudaGetErrorString(e);
   return AV1B_ERR_CUDA;
+}
+
+void clear_err(av1b_decoder* d) {
+  std::lock_guard<std::mutex> lk(d->err_mu);
+  d->err.clear();
 }
 
 #define CK(call, what)                                     \
@@ -140,11 +166,14 @@ int dev_ensure(av1b_decoder* d, DevBuf& b, size_t bytes) {
   if (bytes == 0) bytes = 256;
   if (b.cap >= bytes) return AV1B_OK;
   const size_t want = align_up(bytes + bytes / 8, 1 << 16);
-  if (d->budget && d->allocated - b.cap + want > d->budget)
-    return fail(d, AV1B_ERR_NOMEM, "decoder HBM budget exhausted");
+  {
+    std::lock_guard<std::mutex> lk(d->alloc_mu);
+    if (d->budget && d->allocated - b.cap + want > d->budget)
+      return fail(d, AV1B_ERR_NOMEM, "decoder HBM budget exhausted");
+    d->allocated -= b.cap;
+  }
   if (b.p) {
     cudaFree(b.p);
-    d->allocated -= b.cap;
     b.p = nullptr;
     b.cap = 0;
   }
@@ -153,6 +182,7 @@ int dev_ensure(av1b_decoder* d, DevBuf& b, size_t bytes) {
   if (e != cudaSuccess) return cuda_fail(d, e, "cudaMalloc");
   b.p = p;
   b.cap = want;
+  std::lock_guard<std::mutex> lk(d->alloc_mu);
   d->allocated += want;
   return AV1B_OK;
 }
@@ -160,6 +190,7 @@ int dev_ensure(av1b_decoder* d, DevBuf& b, size_t bytes) {
 void dev_release(av1b_decoder* d, DevBuf& b) {
   if (b.p) {
     cudaFree(b.p);
+    std::lock_guard<std::mutex> lk(d->alloc_mu);
     d->allocated -= b.cap;
   }
   b.p = nullptr;
@@ -227,6 +258,7 @@ int ensure_geometry(av1b_decoder* d, const av1b_frame_syntax& s, int coded_width
     return rc;
   if (!same_pictures) {
     /* a different display geometry: the slots' pictures are unusable */
+    std::lock_guard<std::mutex> lk(d->slot_mu);
     for (int i = 0; i < kSlots; ++i) d->slot_valid[i] = false;
   }
   d->L = L;
@@ -274,11 +306,14 @@ struct Plan {
   std::vector<int2> itx_jobs;
   std::vector<DeblockRec> deblock_v, deblock_h;
   std::vector<CdefRec> cdef;
-  std::vector<unsigned> cdef_search;  /* luma positions to search, x | y << 16 */
+  std::vector<unsigned> cdef_search;  /* searches off the 8x8 grid: x | y << 16 */
+  int cdef_grid_w = 0, cdef_grid_n = 0;  /* the grid of 8x8 luma searches */
+  bool cdef_search_any = false;          /* some record reads the grid */
   std::vector<LrUnitRec> lr_units[3];
   LrArgs lr{};
   bool use_lr = false;
   size_t coef_pool = 0, residual_pool = 0;
+  size_t pre_res_pool = 0;        /* ints of residual computed ahead (phase B) */
   int scale_x = AV1B_SCALE_ONE, scale_y = AV1B_SCALE_ONE;
   bool upscaled = false;
   bool grain = false;
@@ -286,38 +321,414 @@ struct Plan {
   GrainState gs_tail;   /* only the constants after the templates are used */
 };
 
+/* What the planner reads of the decoder: the frame's layout and the state of
+ * the reference slots, copied under the slot lock when planning starts, so a
+ * frame can be planned on another thread while earlier frames run. */
+struct PlanCtx {
+  Layout L;
+  bool slot_used[kSlots], slot_valid[kSlots];
+  int slot_width[kSlots], slot_height[kSlots];
+  WorkPool* pool = nullptr;
+  struct PlanScratch* scratch = nullptr;
+};
+
+/* The first error one piece of the planner met. */
+struct PlanErr {
+  int code = AV1B_OK;
+  std::string msg;
+  int set(int c, const char* m) {
+    if (code == AV1B_OK) {
+      code = c;
+      msg = m;
+    }
+    return c;
+  }
+};
+
 /* Maps a block's reference index to a device slot. At planning time a slot
  * only has to be held or reserved (a pipeline plans a frame before the frame
  * it references has been decoded); execute_plan checks that it holds a
  * picture of this size by the time the plan runs. */
-int resolve_slot(av1b_decoder* d, const av1b_frame_syntax& s, int ref, int* slot) {
+int resolve_slot(const PlanCtx& c, PlanErr& e, const av1b_frame_syntax& s, int ref, int* slot) {
   *slot = -1;
   if (ref < 0 || ref >= static_cast<int>(s.n_reference_slots)) return AV1B_OK;
   const int sl = s.reference_slots[ref];
   if (sl < 0 || sl >= kSlots) return AV1B_OK;
-  if (!d->slot_used[sl])
-    return fail(d, AV1B_ERR_SYNTAX, "a block references a slot that is neither held nor reserved");
-  if (d->slot_valid[sl] && (d->slot_width[sl] != s.width || d->slot_height[sl] != s.height))
-    return fail(d, AV1B_ERR_SYNTAX,
-                "engine: reference scaling between pictures of different sizes is not supported");
+  if (!c.slot_used[sl])
+    return e.set(AV1B_ERR_SYNTAX, "a block references a slot that is neither held nor reserved");
+  if (c.slot_valid[sl] && (c.slot_width[sl] != s.width || c.slot_height[sl] != s.height))
+    return e.set(AV1B_ERR_SYNTAX,
+                 "engine: reference scaling between pictures of different sizes is not supported");
   *slot = sl;
   return AV1B_OK;
 }
 
 bool pow2_in(int v, int lo, int hi) { return v >= lo && v <= hi && (v & (v - 1)) == 0; }
 
-int build_plan(av1b_decoder* d, const av1b_frame_syntax& s, Plan* P) {
-  const Layout& L = d->L;
+/* The records of the blocks of one piece of the frame. List indices in the
+ * block records (tx_first, obmc_first, palette_color_idx, warp_idx - 1 based
+ * - and pre_off) are local to the piece until build_plan adds the piece's
+ * offsets. */
+struct BlockOut {
+  std::vector<TxRec> txs;
+  std::vector<ObmcRec> obmc;
+  std::vector<WarpRec> warps;
+  std::vector<int> palette_colors;
+  std::vector<int> units;
+  std::vector<int2> inter_tiles;
+  std::vector<int2> itx_jobs;
+  size_t pre_res_pool = 0, coef_end = 0, res_end = 0;
+  PlanErr err;
+  void clear() {
+    txs.clear();
+    obmc.clear();
+    warps.clear();
+    palette_colors.clear();
+    units.clear();
+    inter_tiles.clear();
+    itx_jobs.clear();
+    pre_res_pool = coef_end = res_end = 0;
+    err = PlanErr();
+  }
+};
+
+int plan_block(const PlanCtx& ctx, const av1b_frame_syntax& s, size_t bi, BlockRec& r, BlockOut* O) {
+  const Layout& L = ctx.L;
+  const av1b_block& b = s.blocks[bi];
+  std::memset(&r, 0, sizeof(r));
+  if (b.plane < 0 || b.plane > 2) return O->err.set(AV1B_ERR_SYNTAX, "block plane out of range");
+  const PlaneGeom& g = L.p[b.plane];
+  const int rows = plane_rows(L, b.plane);
+  if (b.x < 0 || b.y < 0 || b.w < 1 || b.h < 1 || b.w > 128 || b.h > 128 ||
+      b.x + b.w > g.stride || b.y + b.h > rows)
+    return O->err.set(AV1B_ERR_SYNTAX, "block outside the picture and its border");
+  r.x = static_cast<short>(b.x);
+  r.y = static_cast<short>(b.y);
+  r.w = static_cast<short>(b.w);
+  r.h = static_cast<short>(b.h);
+  r.plane = static_cast<unsigned char>(b.plane);
+  r.have_left = b.have_left && b.x > 0;
+  r.have_above = b.have_above && b.y > 0;
+  r.lossless = b.lossless ? 1 : 0;
+  r.residual_provided = b.residual_provided ? 1 : 0;
+  r.warp_idx[0] = r.warp_idx[1] = 0;
+  r.ref_slot[0] = r.ref_slot[1] = -1;
+  if (b.is_intra) {
+    if (!pow2_in(b.w, 2, 64) || !pow2_in(b.h, 2, 64))
+      return O->err.set(AV1B_ERR_SYNTAX, "an intra block must be 2..64 samples per side");
+    if (b.mode < 0 || b.mode > 13) return O->err.set(AV1B_ERR_SYNTAX, "intra mode out of range");
+    if (b.angle_delta < -3 || b.angle_delta > 3)
+      return O->err.set(AV1B_ERR_SYNTAX, "angle delta out of range");
+    r.kind = AV1B_U_INTRA;
+    r.is_inter = 0;
+    r.phase_b = 1;
+    r.mode = static_cast<unsigned char>(b.mode);
+    r.angle_delta = static_cast<signed char>(b.angle_delta);
+    /* negative: no edge filtering at all; any other non-zero value selects
+     * the second strength table (av1gpu_kernels.h:1195-1239, 1459) */
+    r.filter_type = static_cast<signed char>(
+        !s.enable_intra_edge_filter || b.filter_type < 0 ? -1 : (b.filter_type ? 1 : 0));
+    const bool fi = b.use_filter_intra && b.plane == 0;
+    if (fi && (b.filter_intra_mode < 0 || b.filter_intra_mode > 4))
+      return O->err.set(AV1B_ERR_SYNTAX, "filter intra mode out of range");
+    r.fi_mode = static_cast<signed char>(fi ? b.filter_intra_mode : -1);
+    r.cfl_alpha = static_cast<signed char>(std::max(-128, std::min(127, b.cfl_alpha)));
+    r.have_ar = b.have_above_right >= 0 ? (b.have_above_right != 0) : 2;
+    r.have_bl = b.have_below_left >= 0 ? (b.have_below_left != 0) : 2;
+    if (b.use_palette) {
+      if (b.palette_off < 0 || b.palette_stride < b.w ||
+          static_cast<size_t>(b.palette_off) + static_cast<size_t>(b.h - 1) * b.palette_stride + b.w >
+              s.n_palette_map)
+        return O->err.set(AV1B_ERR_SYNTAX, "palette map outside the frame's pool");
+      for (int i = 0; i < b.h; ++i)
+        for (int j = 0; j < b.w; ++j)
+          if (s.palette_map[b.palette_off + i * b.palette_stride + j] > 7)
+            return O->err.set(AV1B_ERR_SYNTAX, "palette index above 7");
+      r.palette = 1;
+      r.palette_off = b.palette_off;
+      r.palette_stride = b.palette_stride;
+      r.palette_color_idx = static_cast<int>(O->palette_colors.size() / 8);
+      for (int k = 0; k < 8; ++k) O->palette_colors.push_back(b.palette[k]);
+    }
+  } else {
+    r.kind = b.intrabc ? AV1B_U_INTRABC : (b.interintra ? AV1B_U_INTERINTRA : 0);
+    r.is_inter = 1;
+    r.phase_b = (b.intrabc || b.interintra) ? 1 : 0;
+    if (b.filter < 0 || b.filter > 3 || b.filter_v < 0 || b.filter_v > 3)
+      return O->err.set(AV1B_ERR_SYNTAX, "interpolation filter out of range");
+    if (b.compound < 0 || b.compound > 4) return O->err.set(AV1B_ERR_SYNTAX, "compound type out of range");
+    int rc;
+    if (b.intrabc) {
+      r.ref_slot[0] = r.ref_slot[1] = -1;
+    } else {
+      if ((rc = resolve_slot(ctx, O->err, s, b.ref[0], &r.ref_slot[0]))) return rc;
+      if (r.ref_slot[0] < 0) return O->err.set(AV1B_ERR_SYNTAX, "an inter block without a reference");
+      if (b.compound) {
+        if ((rc = resolve_slot(ctx, O->err, s, b.ref[1], &r.ref_slot[1]))) return rc;
+        if (r.ref_slot[1] < 0)
+          return O->err.set(AV1B_ERR_SYNTAX, "a compound block without a second reference");
+      }
+    }
+    for (int k = 0; k < 2; ++k) {
+      r.mv[k][0] = b.mv[k][0];
+      r.mv[k][1] = b.mv[k][1];
+    }
+    r.filt = static_cast<unsigned char>(b.filter);
+    r.filt_v = static_cast<unsigned char>(b.filter_v);
+    r.compound = static_cast<unsigned char>(b.compound);
+    r.w0 = static_cast<unsigned char>(b.blend[0]);
+    r.w1 = static_cast<unsigned char>(b.blend[1]);
+    const int lw = b.w << (b.plane > 0 ? s.ss_x : 0), lh = b.h << (b.plane > 0 ? s.ss_y : 0);
+    if (b.compound == 3 || b.compound == 4) {
+      r.mask_kind = b.compound == 3 ? 1 : 2;
+      r.mask_sign = b.mask_sign ? 1 : 0;
+      if (b.compound == 3) {
+        int dir, xo, yo, fl;
+        if (!wedge_entry(lw, lh, b.wedge_index, &dir, &xo, &yo, &fl))
+          return O->err.set(AV1B_ERR_SYNTAX, "engine: a wedge on a block size that has none");
+        r.wedge_dir = static_cast<unsigned char>(dir);
+        r.wedge_xoff = static_cast<signed char>(xo);
+        r.wedge_yoff = static_cast<signed char>(yo);
+        r.wedge_flip = static_cast<unsigned char>(fl);
+      }
+    }
+    if (b.interintra) {
+      if (!pow2_in(b.w, 2, 64) || !pow2_in(b.h, 2, 64) || b.interintra_mode < 0 ||
+          b.interintra_mode > 3)
+        return O->err.set(AV1B_ERR_SYNTAX, "inter-intra block shape or mode out of range");
+      r.interintra = 1;
+      r.ii_mode = static_cast<unsigned char>(b.interintra_mode);
+      if (b.interintra_wedge) {
+        int dir, xo, yo, fl;
+        if (!wedge_entry(lw, lh, b.wedge_index, &dir, &xo, &yo, &fl))
+          return O->err.set(AV1B_ERR_SYNTAX, "engine: an inter/intra wedge on a block size that has none");
+        r.ii_wedge = 1;
+        r.wedge_dir = static_cast<unsigned char>(dir);
+        r.wedge_xoff = static_cast<signed char>(xo);
+        r.wedge_yoff = static_cast<signed char>(yo);
+        r.wedge_flip = static_cast<unsigned char>(fl);
+      }
+    }
+    /* global warp: a model whose shear is invalid keeps the warp flag with
+     * an all-zero model, exactly as the reference engine leaves its job
+     * (engine.cpp:1172-1193) */
+    for (int k = 0; k < 2; ++k) {
+      const bool w = b.warp[k] != 0, mw = b.mask_warp[k] != 0;
+      if (k == 0) {
+        r.warp0 = w;
+        r.mask_warp0 = mw;
+      } else {
+        r.warp1 = w;
+        r.mask_warp1 = mw;
+      }
+      if (!w && !mw) continue;
+      WarpRec m{};
+      int al, be, ga, de;
+      if (gm_setup_shear(b.warp_params[k], &al, &be, &ga, &de)) {
+        for (int j = 0; j < 6; ++j) m.params[j] = b.warp_params[k][j];
+        m.abcd[0] = al;
+        m.abcd[1] = be;
+        m.abcd[2] = ga;
+        m.abcd[3] = de;
+      }
+      r.warp_idx[k] = static_cast<int>(O->warps.size()) + 1;
+      O->warps.push_back(m);
+    }
+    r.obmc_first = static_cast<int>(O->obmc.size());
+    r.obmc_count = 0;
+    if (b.obmc_count > 0) {
+      if (b.obmc_first < 0 || static_cast<size_t>(b.obmc_first) + b.obmc_count > s.n_obmc)
+        return O->err.set(AV1B_ERR_SYNTAX, "OBMC range outside the frame's list");
+      for (int k = 0; k < b.obmc_count && k < 8; ++k) {
+        const av1b_obmc& c = s.obmc[b.obmc_first + k];
+        ObmcRec o{};
+        o.pass = static_cast<short>(c.pass);
+        o.x = static_cast<short>(c.x);
+        o.y = static_cast<short>(c.y);
+        o.w = static_cast<short>(c.w);
+        o.h = static_cast<short>(c.h);
+        const int len = c.pass == 0 ? c.h : c.w;
+        if (c.w < 1 || c.h < 1 || c.x < 0 || c.y < 0 || !(len == 2 || len == 4 || len == 8 ||
+                                                          len == 16 || len == 32))
+          return O->err.set(AV1B_ERR_SYNTAX, "OBMC strip shape out of range");
+        if (c.filter < 0 || c.filter > 3 || c.filter_v < 0 || c.filter_v > 3)
+          return O->err.set(AV1B_ERR_SYNTAX, "OBMC filter out of range");
+        o.filt = static_cast<short>(c.filter);
+        o.filt_v = static_cast<short>(c.filter_v);
+        o.mv_x = c.mv[0];
+        o.mv_y = c.mv[1];
+        if ((rc = resolve_slot(ctx, O->err, s, c.ref, &o.ref_slot))) return rc;
+        if (o.ref_slot < 0) return O->err.set(AV1B_ERR_SYNTAX, "an OBMC strip without a reference");
+        O->obmc.push_back(o);
+        ++r.obmc_count;
+      }
+    }
+  }
+  /* transforms */
+  r.tx_first = static_cast<int>(O->txs.size());
+  r.tx_count = 0;
+  if (b.tx_count > 0) {
+    if (b.tx_first < 0 || static_cast<size_t>(b.tx_first) + b.tx_count > s.n_transforms)
+      return O->err.set(AV1B_ERR_SYNTAX, "transform range outside the frame's list");
+    for (int k = 0; k < b.tx_count; ++k) {
+      const av1b_transform& t = s.transforms[b.tx_first + k];
+      if (t.eob <= 0) continue;
+      if (t.coef_offset < 0 || t.x < 0 || t.y < 0 || b.x + t.x + t.w > g.stride ||
+          b.y + t.y + t.h > rows)
+        return O->err.set(AV1B_ERR_SYNTAX, "transform outside the picture and its border");
+      TxRec x{};
+      x.coef_off = t.coef_offset;
+      x.x = static_cast<short>(t.x);
+      x.y = static_cast<short>(t.y);
+      x.w = static_cast<short>(t.w);
+      x.h = static_cast<short>(t.h);
+      if (b.residual_provided) {
+        if (t.w < 1 || t.h < 1 || t.w > 128 || t.h > 128)
+          return O->err.set(AV1B_ERR_SYNTAX, "residual block size out of range");
+        O->res_end = std::max(O->res_end, static_cast<size_t>(t.coef_offset) + static_cast<size_t>(t.w) * t.h);
+      } else {
+        if (!pow2_in(t.w, 4, 64) || !pow2_in(t.h, 4, 64) || t.tx_type < 0 || t.tx_type > 15)
+          return O->err.set(AV1B_ERR_SYNTAX, "transform size or type out of range");
+        if (b.lossless && (t.w != 4 || t.h != 4))
+          return O->err.set(AV1B_ERR_SYNTAX, "a lossless transform must be 4x4");
+        x.log2w = static_cast<unsigned char>(__builtin_ctz(t.w));
+        x.log2h = static_cast<unsigned char>(__builtin_ctz(t.h));
+        x.type = static_cast<unsigned char>(t.tx_type);
+        x.row_shift = static_cast<unsigned char>(b.lossless ? 0 : tx_row_shift(x.log2w, x.log2h));
+        O->coef_end = std::max(O->coef_end, static_cast<size_t>(t.coef_offset) + static_cast<size_t>(t.w) * t.h);
+      }
+      x.pre_off = -1;
+      if (r.phase_b && !b.residual_provided) {
+        x.pre_off = static_cast<int>(O->pre_res_pool);
+        O->pre_res_pool += static_cast<size_t>(t.w) * t.h;
+      }
+      if (!r.phase_b || x.pre_off >= 0)
+        O->itx_jobs.push_back(make_int2(static_cast<int>(bi), static_cast<int>(O->txs.size())));
+      O->txs.push_back(x);
+      ++r.tx_count;
+    }
+  }
+  if (r.phase_b) {
+    O->units.push_back(static_cast<int>(bi));
+  } else {
+    for (int y0 = 0; y0 < b.h; y0 += 8)
+      for (int x0 = 0; x0 < b.w; x0 += 16)
+        O->inter_tiles.push_back(make_int2(static_cast<int>(bi), x0 | (y0 << 16)));
+  }
+  return AV1B_OK;
+}
+
+
+/* The deblocking edges of one piece of the frame, vertical and horizontal. */
+struct EdgeOut {
+  std::vector<DeblockRec> v, h;
+  PlanErr err;
+};
+
+int plan_edge(const PlanCtx& c, const av1b_frame_syntax& s, size_t i, EdgeOut* O) {
+  const Layout& L = c.L;
+  const av1b_deblock_edge& e = s.deblock[i];
+  if (e.plane < 0 || e.plane > 2) return O->err.set(AV1B_ERR_SYNTAX, "deblock plane out of range");
+  if (e.length <= 0 || e.level == 0) return AV1B_OK;
+  if (e.level < 0 || e.level > 63) return O->err.set(AV1B_ERR_SYNTAX, "deblock level out of range");
+  if (e.filter_size != 4 && e.filter_size != 8 && e.filter_size != 16)
+    return O->err.set(AV1B_ERR_SYNTAX, "deblock filter size must be 4, 8 or 16");
+  const PlaneGeom& g = L.p[e.plane];
+  const int rows = plane_rows(L, e.plane);
+  /* how far the filter reaches across the edge: p6..q6 at most */
+  const int reach = e.filter_size == 16 ? 7 : (e.filter_size == 4 ? 2 : 4);
+  DeblockRec r{};
+  r.len = static_cast<short>(e.length);
+  r.level = static_cast<short>(e.level);
+  r.filter_size = static_cast<unsigned char>(e.filter_size);
+  r.chroma = e.plane != 0;
+  if (e.vertical) {
+    if (e.x - reach < 0 || e.x + reach > g.stride || e.y < 0 || e.y + e.length > rows)
+      return O->err.set(AV1B_ERR_SYNTAX, "deblock edge reaches outside the picture");
+    r.p_off = g.off + e.y * g.stride + e.x - 2;
+    r.across = 1;
+    r.along = g.stride;
+    O->v.push_back(r);
+  } else {
+    if (e.y - reach < 0 || e.y + reach > rows || e.x < 0 || e.x + e.length > g.stride)
+      return O->err.set(AV1B_ERR_SYNTAX, "deblock edge reaches outside the picture");
+    r.p_off = g.off + (e.y - 2) * g.stride + e.x;
+    r.across = g.stride;
+    r.along = 1;
+    O->h.push_back(r);
+  }
+  return AV1B_OK;
+}
+
+/* The CDEF records of one piece of the frame. A block whose direction is
+ * searched reads the search of its 8x8 luma block from a grid the device
+ * fills (every cell searched once); a luma position off the 8x8 grid gets a
+ * search of its own, listed after the grid. */
+struct CdefOut {
+  std::vector<size_t> unaligned;
+  bool any = false;
+  PlanErr err;
+};
+
+int plan_cdef(const PlanCtx& ctx, const av1b_frame_syntax& s, size_t i, int grid_w, CdefRec* out,
+              CdefOut* O) {
+  const Layout& L = ctx.L;
+  const av1b_cdef_block& c = s.cdef[i];
+  if (c.plane < 0 || c.plane > 2) return O->err.set(AV1B_ERR_SYNTAX, "CDEF plane out of range");
+  const int sx = c.plane ? L.ss_x : 0, sy = c.plane ? L.ss_y : 0;
+  const int bw = 8 >> sx, bh = 8 >> sy;
+  const PlaneGeom& g = L.p[c.plane];
+  if (c.x < 0 || c.y < 0 || c.x + bw + 2 > g.stride || c.y + bh + 2 > plane_rows(L, c.plane) ||
+      (c.x << sx) + 8 > L.p[0].stride || (c.y << sy) + 8 > plane_rows(L, 0))
+    return O->err.set(AV1B_ERR_SYNTAX, "CDEF block outside the picture");
+  if (c.dir < -1 || c.dir > 7 || c.pri_strength < 0 || c.pri_strength > 255 ||
+      c.sec_strength < 0 || c.sec_strength > 255 || c.damping < 0 || c.damping > 63)
+    return O->err.set(AV1B_ERR_SYNTAX, "CDEF parameters out of range");
+  CdefRec& r = out[i];
+  r.x = static_cast<short>(c.x);
+  r.y = static_cast<short>(c.y);
+  r.plane = static_cast<unsigned char>(c.plane);
+  r.pri = static_cast<unsigned char>(c.pri_strength);
+  r.sec = static_cast<unsigned char>(c.sec_strength);
+  r.damping = static_cast<unsigned char>(c.damping);
+  r.dir = static_cast<signed char>(c.dir);
+  r.search = -1;
+  if (c.dir < 0) {
+    const int lx = c.x << sx, ly = c.y << sy;
+    if ((lx | ly) & 7) {
+      O->unaligned.push_back(i);
+    } else {
+      r.search = (ly >> 3) * grid_w + (lx >> 3);
+      O->any = true;
+    }
+  }
+  return AV1B_OK;
+}
+
+/* The planner's per-piece outputs, kept between frames for their capacity. */
+struct PlanScratch {
+  std::vector<BlockOut> blocks;
+  std::vector<EdgeOut> edges;
+  std::vector<CdefOut> cdef;
+};
+
+/* Splits [0, n) into pieces of at least `min_piece` for the pool. */
+int pieces_for(size_t n, const PlanCtx& c, size_t min_piece) {
+  if (n == 0) return 0;
+  const size_t most = static_cast<size_t>(c.pool ? 4 * c.pool->threads() : 1);
+  return static_cast<int>(std::max<size_t>(1, std::min(most, n / min_piece)));
+}
+inline size_t piece_begin(size_t n, int pieces, int i) { return n * i / pieces; }
+
+/* Validates a frame and builds its device records. The blocks, deblocking
+ * edges and CDEF blocks are converted in pieces on the pool; each piece stops
+ * at its first invalid record and the error of the earliest piece is the one
+ * reported, so the result - records and error alike - is the one a single
+ * pass in order gives. */
+int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Plan* P) {
+  const Layout& L = c.L;
   const int bd = s.bit_depth;
   P->blocks.resize(s.n_blocks);
-  P->txs.clear();
-  P->obmc.clear();
-  P->warps.clear();
-  P->warps.push_back(WarpRec{});
-  P->palette_colors.clear();
-  P->units.clear();
-  P->inter_tiles.clear();
-  P->itx_jobs.clear();
   for (int i = 0; i < 7; ++i) {
     const int rw = s.reference_width[i] > 0 ? s.reference_width[i] : s.width;
     const int rh = s.reference_height[i] > 0 ? s.reference_height[i] : s.height;
@@ -333,224 +744,76 @@ int build_plan(av1b_decoder* d, const av1b_frame_syntax& s, Plan* P) {
     P->scale_y = ((s.height << 14) + (fh / 2)) / fh;
   }
   size_t coef_end = 0, res_end = 0;
-  for (size_t bi = 0; bi < s.n_blocks; ++bi) {
-    const av1b_block& b = s.blocks[bi];
-    BlockRec& r = P->blocks[bi];
-    std::memset(&r, 0, sizeof(r));
-    if (b.plane < 0 || b.plane > 2) return fail(d, AV1B_ERR_SYNTAX, "block plane out of range");
-    const PlaneGeom& g = L.p[b.plane];
-    const int rows = plane_rows(L, b.plane);
-    if (b.x < 0 || b.y < 0 || b.w < 1 || b.h < 1 || b.w > 128 || b.h > 128 ||
-        b.x + b.w > g.stride || b.y + b.h > rows)
-      return fail(d, AV1B_ERR_SYNTAX, "block outside the picture and its border");
-    r.x = static_cast<short>(b.x);
-    r.y = static_cast<short>(b.y);
-    r.w = static_cast<short>(b.w);
-    r.h = static_cast<short>(b.h);
-    r.plane = static_cast<unsigned char>(b.plane);
-    r.have_left = b.have_left && b.x > 0;
-    r.have_above = b.have_above && b.y > 0;
-    r.lossless = b.lossless ? 1 : 0;
-    r.residual_provided = b.residual_provided ? 1 : 0;
-    r.warp_idx[0] = r.warp_idx[1] = 0;
-    r.ref_slot[0] = r.ref_slot[1] = -1;
-    if (b.is_intra) {
-      if (!pow2_in(b.w, 2, 64) || !pow2_in(b.h, 2, 64))
-        return fail(d, AV1B_ERR_SYNTAX, "an intra block must be 2..64 samples per side");
-      if (b.mode < 0 || b.mode > 13) return fail(d, AV1B_ERR_SYNTAX, "intra mode out of range");
-      if (b.angle_delta < -3 || b.angle_delta > 3)
-        return fail(d, AV1B_ERR_SYNTAX, "angle delta out of range");
-      r.kind = AV1B_U_INTRA;
-      r.is_inter = 0;
-      r.phase_b = 1;
-      r.mode = static_cast<unsigned char>(b.mode);
-      r.angle_delta = static_cast<signed char>(b.angle_delta);
-      /* negative: no edge filtering at all; any other non-zero value selects
-       * the second strength table (av1gpu_kernels.h:1195-1239, 1459) */
-      r.filter_type = static_cast<signed char>(
-          !s.enable_intra_edge_filter || b.filter_type < 0 ? -1 : (b.filter_type ? 1 : 0));
-      const bool fi = b.use_filter_intra && b.plane == 0;
-      if (fi && (b.filter_intra_mode < 0 || b.filter_intra_mode > 4))
-        return fail(d, AV1B_ERR_SYNTAX, "filter intra mode out of range");
-      r.fi_mode = static_cast<signed char>(fi ? b.filter_intra_mode : -1);
-      r.cfl_alpha = static_cast<signed char>(std::max(-128, std::min(127, b.cfl_alpha)));
-      r.have_ar = b.have_above_right >= 0 ? (b.have_above_right != 0) : 2;
-      r.have_bl = b.have_below_left >= 0 ? (b.have_below_left != 0) : 2;
-      if (b.use_palette) {
-        if (b.palette_off < 0 || b.palette_stride < b.w ||
-            static_cast<size_t>(b.palette_off) + static_cast<size_t>(b.h - 1) * b.palette_stride + b.w >
-                s.n_palette_map)
-          return fail(d, AV1B_ERR_SYNTAX, "palette map outside the frame's pool");
-        for (int i = 0; i < b.h; ++i)
-          for (int j = 0; j < b.w; ++j)
-            if (s.palette_map[b.palette_off + i * b.palette_stride + j] > 7)
-              return fail(d, AV1B_ERR_SYNTAX, "palette index above 7");
-        r.palette = 1;
-        r.palette_off = b.palette_off;
-        r.palette_stride = b.palette_stride;
-        r.palette_color_idx = static_cast<int>(P->palette_colors.size() / 8);
-        for (int k = 0; k < 8; ++k) P->palette_colors.push_back(b.palette[k]);
-      }
-    } else {
-      r.kind = b.intrabc ? AV1B_U_INTRABC : (b.interintra ? AV1B_U_INTERINTRA : 0);
-      r.is_inter = 1;
-      r.phase_b = (b.intrabc || b.interintra) ? 1 : 0;
-      if (b.filter < 0 || b.filter > 3 || b.filter_v < 0 || b.filter_v > 3)
-        return fail(d, AV1B_ERR_SYNTAX, "interpolation filter out of range");
-      if (b.compound < 0 || b.compound > 4) return fail(d, AV1B_ERR_SYNTAX, "compound type out of range");
-      int rc;
-      if (b.intrabc) {
-        r.ref_slot[0] = r.ref_slot[1] = -1;
-      } else {
-        if ((rc = resolve_slot(d, s, b.ref[0], &r.ref_slot[0]))) return rc;
-        if (r.ref_slot[0] < 0) return fail(d, AV1B_ERR_SYNTAX, "an inter block without a reference");
-        if (b.compound) {
-          if ((rc = resolve_slot(d, s, b.ref[1], &r.ref_slot[1]))) return rc;
-          if (r.ref_slot[1] < 0)
-            return fail(d, AV1B_ERR_SYNTAX, "a compound block without a second reference");
-        }
-      }
-      for (int k = 0; k < 2; ++k) {
-        r.mv[k][0] = b.mv[k][0];
-        r.mv[k][1] = b.mv[k][1];
-      }
-      r.filt = static_cast<unsigned char>(b.filter);
-      r.filt_v = static_cast<unsigned char>(b.filter_v);
-      r.compound = static_cast<unsigned char>(b.compound);
-      r.w0 = static_cast<unsigned char>(b.blend[0]);
-      r.w1 = static_cast<unsigned char>(b.blend[1]);
-      const int lw = b.w << (b.plane > 0 ? s.ss_x : 0), lh = b.h << (b.plane > 0 ? s.ss_y : 0);
-      if (b.compound == 3 || b.compound == 4) {
-        r.mask_kind = b.compound == 3 ? 1 : 2;
-        r.mask_sign = b.mask_sign ? 1 : 0;
-        if (b.compound == 3) {
-          int dir, xo, yo, fl;
-          if (!wedge_entry(lw, lh, b.wedge_index, &dir, &xo, &yo, &fl))
-            return fail(d, AV1B_ERR_SYNTAX, "engine: a wedge on a block size that has none");
-          r.wedge_dir = static_cast<unsigned char>(dir);
-          r.wedge_xoff = static_cast<signed char>(xo);
-          r.wedge_yoff = static_cast<signed char>(yo);
-          r.wedge_flip = static_cast<unsigned char>(fl);
-        }
-      }
-      if (b.interintra) {
-        if (!pow2_in(b.w, 2, 64) || !pow2_in(b.h, 2, 64) || b.interintra_mode < 0 ||
-            b.interintra_mode > 3)
-          return fail(d, AV1B_ERR_SYNTAX, "inter-intra block shape or mode out of range");
-        r.interintra = 1;
-        r.ii_mode = static_cast<unsigned char>(b.interintra_mode);
-        if (b.interintra_wedge) {
-          int dir, xo, yo, fl;
-          if (!wedge_entry(lw, lh, b.wedge_index, &dir, &xo, &yo, &fl))
-            return fail(d, AV1B_ERR_SYNTAX, "engine: an inter/intra wedge on a block size that has none");
-          r.ii_wedge = 1;
-          r.wedge_dir = static_cast<unsigned char>(dir);
-          r.wedge_xoff = static_cast<signed char>(xo);
-          r.wedge_yoff = static_cast<signed char>(yo);
-          r.wedge_flip = static_cast<unsigned char>(fl);
-        }
-      }
-      /* global warp: a model whose shear is invalid keeps the warp flag with
-       * an all-zero model, exactly as the reference engine leaves its job
-       * (engine.cpp:1172-1193) */
-      for (int k = 0; k < 2; ++k) {
-        const bool w = b.warp[k] != 0, mw = b.mask_warp[k] != 0;
-        if (k == 0) {
-          r.warp0 = w;
-          r.mask_warp0 = mw;
-        } else {
-          r.warp1 = w;
-          r.mask_warp1 = mw;
-        }
-        if (!w && !mw) continue;
-        WarpRec m{};
-        int al, be, ga, de;
-        if (gm_setup_shear(b.warp_params[k], &al, &be, &ga, &de)) {
-          for (int j = 0; j < 6; ++j) m.params[j] = b.warp_params[k][j];
-          m.abcd[0] = al;
-          m.abcd[1] = be;
-          m.abcd[2] = ga;
-          m.abcd[3] = de;
-        }
-        r.warp_idx[k] = static_cast<int>(P->warps.size());
-        P->warps.push_back(m);
-      }
-      r.obmc_first = static_cast<int>(P->obmc.size());
-      r.obmc_count = 0;
-      if (b.obmc_count > 0) {
-        if (b.obmc_first < 0 || static_cast<size_t>(b.obmc_first) + b.obmc_count > s.n_obmc)
-          return fail(d, AV1B_ERR_SYNTAX, "OBMC range outside the frame's list");
-        for (int k = 0; k < b.obmc_count && k < 8; ++k) {
-          const av1b_obmc& c = s.obmc[b.obmc_first + k];
-          ObmcRec o{};
-          o.pass = static_cast<short>(c.pass);
-          o.x = static_cast<short>(c.x);
-          o.y = static_cast<short>(c.y);
-          o.w = static_cast<short>(c.w);
-          o.h = static_cast<short>(c.h);
-          const int len = c.pass == 0 ? c.h : c.w;
-          if (c.w < 1 || c.h < 1 || c.x < 0 || c.y < 0 || !(len == 2 || len == 4 || len == 8 ||
-                                                            len == 16 || len == 32))
-            return fail(d, AV1B_ERR_SYNTAX, "OBMC strip shape out of range");
-          if (c.filter < 0 || c.filter > 3 || c.filter_v < 0 || c.filter_v > 3)
-            return fail(d, AV1B_ERR_SYNTAX, "OBMC filter out of range");
-          o.filt = static_cast<short>(c.filter);
-          o.filt_v = static_cast<short>(c.filter_v);
-          o.mv_x = c.mv[0];
-          o.mv_y = c.mv[1];
-          if ((rc = resolve_slot(d, s, c.ref, &o.ref_slot))) return rc;
-          if (o.ref_slot < 0) return fail(d, AV1B_ERR_SYNTAX, "an OBMC strip without a reference");
-          P->obmc.push_back(o);
-          ++r.obmc_count;
-        }
-      }
+  {
+    const size_t nb = s.n_blocks;
+    const int pieces = pieces_for(nb, c, 512);
+    std::vector<BlockOut>& outs = c.scratch->blocks;
+    if (outs.size() < static_cast<size_t>(pieces)) outs.resize(pieces);
+    c.pool->run(pieces, [&](int i) {
+      BlockOut* O = &outs[i];
+      O->clear();
+      for (size_t bi = piece_begin(nb, pieces, i); bi < piece_begin(nb, pieces, i + 1); ++bi)
+        if (plan_block(c, s, bi, P->blocks[bi], O)) break;
+    });
+    for (int i = 0; i < pieces; ++i)
+      if (outs[i].err.code) return fail(d, outs[i].err.code, outs[i].err.msg);
+    /* piece offsets into the frame's lists */
+    std::vector<size_t> o_tx(pieces + 1, 0), o_obmc(pieces + 1, 0), o_warp(pieces + 1, 0),
+        o_pal(pieces + 1, 0), o_unit(pieces + 1, 0), o_tile(pieces + 1, 0), o_itx(pieces + 1, 0),
+        o_pre(pieces + 1, 0);
+    for (int i = 0; i < pieces; ++i) {
+      const BlockOut& O = outs[i];
+      o_tx[i + 1] = o_tx[i] + O.txs.size();
+      o_obmc[i + 1] = o_obmc[i] + O.obmc.size();
+      o_warp[i + 1] = o_warp[i] + O.warps.size();
+      o_pal[i + 1] = o_pal[i] + O.palette_colors.size();
+      o_unit[i + 1] = o_unit[i] + O.units.size();
+      o_tile[i + 1] = o_tile[i] + O.inter_tiles.size();
+      o_itx[i + 1] = o_itx[i] + O.itx_jobs.size();
+      o_pre[i + 1] = o_pre[i] + O.pre_res_pool;
+      coef_end = std::max(coef_end, O.coef_end);
+      res_end = std::max(res_end, O.res_end);
     }
-    /* transforms */
-    r.tx_first = static_cast<int>(P->txs.size());
-    r.tx_count = 0;
-    if (b.tx_count > 0) {
-      if (b.tx_first < 0 || static_cast<size_t>(b.tx_first) + b.tx_count > s.n_transforms)
-        return fail(d, AV1B_ERR_SYNTAX, "transform range outside the frame's list");
-      for (int k = 0; k < b.tx_count; ++k) {
-        const av1b_transform& t = s.transforms[b.tx_first + k];
-        if (t.eob <= 0) continue;
-        if (t.coef_offset < 0 || t.x < 0 || t.y < 0 || b.x + t.x + t.w > g.stride ||
-            b.y + t.y + t.h > rows)
-          return fail(d, AV1B_ERR_SYNTAX, "transform outside the picture and its border");
-        TxRec x{};
-        x.coef_off = t.coef_offset;
-        x.x = static_cast<short>(t.x);
-        x.y = static_cast<short>(t.y);
-        x.w = static_cast<short>(t.w);
-        x.h = static_cast<short>(t.h);
-        if (b.residual_provided) {
-          if (t.w < 1 || t.h < 1 || t.w > 128 || t.h > 128)
-            return fail(d, AV1B_ERR_SYNTAX, "residual block size out of range");
-          res_end = std::max(res_end, static_cast<size_t>(t.coef_offset) + static_cast<size_t>(t.w) * t.h);
-        } else {
-          if (!pow2_in(t.w, 4, 64) || !pow2_in(t.h, 4, 64) || t.tx_type < 0 || t.tx_type > 15)
-            return fail(d, AV1B_ERR_SYNTAX, "transform size or type out of range");
-          if (b.lossless && (t.w != 4 || t.h != 4))
-            return fail(d, AV1B_ERR_SYNTAX, "a lossless transform must be 4x4");
-          x.log2w = static_cast<unsigned char>(__builtin_ctz(t.w));
-          x.log2h = static_cast<unsigned char>(__builtin_ctz(t.h));
-          x.type = static_cast<unsigned char>(t.tx_type);
-          x.row_shift = static_cast<unsigned char>(b.lossless ? 0 : tx_row_shift(x.log2w, x.log2h));
-          coef_end = std::max(coef_end, static_cast<size_t>(t.coef_offset) + static_cast<size_t>(t.w) * t.h);
-        }
-        if (!r.phase_b)
-          P->itx_jobs.push_back(make_int2(static_cast<int>(bi), static_cast<int>(P->txs.size())));
-        P->txs.push_back(x);
-        ++r.tx_count;
+    if (o_pre[pieces] > static_cast<size_t>(INT32_MAX) || o_tx[pieces] > static_cast<size_t>(INT32_MAX))
+      return fail(d, AV1B_ERR_SYNTAX, "frame too large");
+    P->txs.resize(o_tx[pieces]);
+    P->obmc.resize(o_obmc[pieces]);
+    P->warps.resize(1 + o_warp[pieces]);
+    P->warps[0] = WarpRec{};
+    P->palette_colors.resize(o_pal[pieces]);
+    P->units.resize(o_unit[pieces]);
+    P->inter_tiles.resize(o_tile[pieces]);
+    P->itx_jobs.resize(o_itx[pieces]);
+    P->pre_res_pool = o_pre[pieces];
+    c.pool->run(pieces, [&](int i) {
+      const BlockOut& O = outs[i];
+      const int dtx = static_cast<int>(o_tx[i]), dob = static_cast<int>(o_obmc[i]);
+      const int dwp = static_cast<int>(o_warp[i]), dpal = static_cast<int>(o_pal[i] / 8);
+      const int dpre = static_cast<int>(o_pre[i]);
+      for (size_t bi = piece_begin(nb, pieces, i); bi < piece_begin(nb, pieces, i + 1); ++bi) {
+        BlockRec& r = P->blocks[bi];
+        r.tx_first += dtx;
+        if (r.is_inter) r.obmc_first += dob;
+        if (r.palette) r.palette_color_idx += dpal;
+        for (int k = 0; k < 2; ++k)
+          if (r.warp_idx[k] > 0) r.warp_idx[k] += dwp;
       }
-    }
-    if (r.phase_b) {
-      P->units.push_back(static_cast<int>(bi));
-    } else {
-      for (int y0 = 0; y0 < b.h; y0 += 8)
-        for (int x0 = 0; x0 < b.w; x0 += 16)
-          P->inter_tiles.push_back(make_int2(static_cast<int>(bi), x0 | (y0 << 16)));
-    }
+      for (size_t k = 0; k < O.txs.size(); ++k) {
+        TxRec x = O.txs[k];
+        if (x.pre_off >= 0) x.pre_off += dpre;
+        P->txs[o_tx[i] + k] = x;
+      }
+      std::copy(O.obmc.begin(), O.obmc.end(), P->obmc.begin() + o_obmc[i]);
+      std::copy(O.warps.begin(), O.warps.end(), P->warps.begin() + 1 + o_warp[i]);
+      std::copy(O.palette_colors.begin(), O.palette_colors.end(), P->palette_colors.begin() + o_pal[i]);
+      std::copy(O.units.begin(), O.units.end(), P->units.begin() + o_unit[i]);
+      std::copy(O.inter_tiles.begin(), O.inter_tiles.end(), P->inter_tiles.begin() + o_tile[i]);
+      for (size_t k = 0; k < O.itx_jobs.size(); ++k) {
+        int2 j = O.itx_jobs[k];
+        j.y += dtx;
+        P->itx_jobs[o_itx[i] + k] = j;
+      }
+    });
   }
   /* The claim order of the dependency-scheduled blocks. Coding order is a
    * valid order but serializes the picture: the blocks in flight all sit in
@@ -608,76 +871,63 @@ int build_plan(av1b_decoder* d, const av1b_frame_syntax& s, Plan* P) {
   P->deblock_v.clear();
   P->deblock_h.clear();
   if (s.sharpness < 0 || s.sharpness > 7) return fail(d, AV1B_ERR_SYNTAX, "sharpness out of range");
-  for (size_t i = 0; i < s.n_deblock; ++i) {
-    const av1b_deblock_edge& e = s.deblock[i];
-    if (e.plane < 0 || e.plane > 2) return fail(d, AV1B_ERR_SYNTAX, "deblock plane out of range");
-    if (e.length <= 0 || e.level == 0) continue;
-    if (e.level < 0 || e.level > 63) return fail(d, AV1B_ERR_SYNTAX, "deblock level out of range");
-    if (e.filter_size != 4 && e.filter_size != 8 && e.filter_size != 16)
-      return fail(d, AV1B_ERR_SYNTAX, "deblock filter size must be 4, 8 or 16");
-    const PlaneGeom& g = L.p[e.plane];
-    const int rows = plane_rows(L, e.plane);
-    /* how far the filter reaches across the edge: p6..q6 at most */
-    const int reach = e.filter_size == 16 ? 7 : (e.filter_size == 4 ? 2 : 4);
-    DeblockRec r{};
-    r.len = static_cast<short>(e.length);
-    r.level = static_cast<short>(e.level);
-    r.filter_size = static_cast<unsigned char>(e.filter_size);
-    r.chroma = e.plane != 0;
-    if (e.vertical) {
-      if (e.x - reach < 0 || e.x + reach > g.stride || e.y < 0 || e.y + e.length > rows)
-        return fail(d, AV1B_ERR_SYNTAX, "deblock edge reaches outside the picture");
-      r.p_off = g.off + e.y * g.stride + e.x - 2;
-      r.across = 1;
-      r.along = g.stride;
-      P->deblock_v.push_back(r);
-    } else {
-      if (e.y - reach < 0 || e.y + reach > rows || e.x < 0 || e.x + e.length > g.stride)
-        return fail(d, AV1B_ERR_SYNTAX, "deblock edge reaches outside the picture");
-      r.p_off = g.off + (e.y - 2) * g.stride + e.x;
-      r.across = g.stride;
-      r.along = 1;
-      P->deblock_h.push_back(r);
+  {
+    const size_t ne = s.n_deblock;
+    const int pieces = pieces_for(ne, c, 4096);
+    std::vector<EdgeOut>& outs = c.scratch->edges;
+    if (outs.size() < static_cast<size_t>(pieces)) outs.resize(pieces);
+    c.pool->run(pieces, [&](int i) {
+      EdgeOut* O = &outs[i];
+      O->v.clear();
+      O->h.clear();
+      O->err = PlanErr();
+      for (size_t k = piece_begin(ne, pieces, i); k < piece_begin(ne, pieces, i + 1); ++k)
+        if (plan_edge(c, s, k, O)) break;
+    });
+    size_t nv = 0, nh = 0;
+    std::vector<size_t> ov(pieces), oh(pieces);
+    for (int i = 0; i < pieces; ++i) {
+      if (outs[i].err.code) return fail(d, outs[i].err.code, outs[i].err.msg);
+      ov[i] = nv;
+      oh[i] = nh;
+      nv += outs[i].v.size();
+      nh += outs[i].h.size();
     }
+    P->deblock_v.resize(nv);
+    P->deblock_h.resize(nh);
+    c.pool->run(pieces, [&](int i) {
+      std::copy(outs[i].v.begin(), outs[i].v.end(), P->deblock_v.begin() + ov[i]);
+      std::copy(outs[i].h.begin(), outs[i].h.end(), P->deblock_h.begin() + oh[i]);
+    });
   }
 
-  /* CDEF: each luma block whose direction is searched is searched once, for
-   * its own record and those of the chroma blocks it covers */
-  P->cdef.resize(s.n_cdef);
-  P->cdef_search.clear();
-  const int sgw = L.p[0].stride >> 3;
-  std::vector<int>& search_at = d->cdef_search_at;
-  search_at.assign(static_cast<size_t>(sgw) * (plane_rows(L, 0) >> 3), -1);
-  for (size_t i = 0; i < s.n_cdef; ++i) {
-    const av1b_cdef_block& c = s.cdef[i];
-    if (c.plane < 0 || c.plane > 2) return fail(d, AV1B_ERR_SYNTAX, "CDEF plane out of range");
-    const int sx = c.plane ? L.ss_x : 0, sy = c.plane ? L.ss_y : 0;
-    const int bw = 8 >> sx, bh = 8 >> sy;
-    const PlaneGeom& g = L.p[c.plane];
-    if (c.x < 0 || c.y < 0 || c.x + bw + 2 > g.stride || c.y + bh + 2 > plane_rows(L, c.plane) ||
-        (c.x << sx) + 8 > L.p[0].stride || (c.y << sy) + 8 > plane_rows(L, 0))
-      return fail(d, AV1B_ERR_SYNTAX, "CDEF block outside the picture");
-    if (c.dir < -1 || c.dir > 7 || c.pri_strength < 0 || c.pri_strength > 255 ||
-        c.sec_strength < 0 || c.sec_strength > 255 || c.damping < 0 || c.damping > 63)
-      return fail(d, AV1B_ERR_SYNTAX, "CDEF parameters out of range");
-    CdefRec& r = P->cdef[i];
-    r.x = static_cast<short>(c.x);
-    r.y = static_cast<short>(c.y);
-    r.plane = static_cast<unsigned char>(c.plane);
-    r.pri = static_cast<unsigned char>(c.pri_strength);
-    r.sec = static_cast<unsigned char>(c.sec_strength);
-    r.damping = static_cast<unsigned char>(c.damping);
-    r.dir = static_cast<signed char>(c.dir);
-    r.search = -1;
-    if (c.dir < 0) {
-      const int lx = c.x << sx, ly = c.y << sy;
-      int* at = ((lx | ly) & 7) ? nullptr : &search_at[static_cast<size_t>(ly >> 3) * sgw + (lx >> 3)];
-      if (at && *at >= 0) {
-        r.search = *at;
-      } else {
-        r.search = static_cast<int>(P->cdef_search.size());
-        P->cdef_search.push_back(static_cast<unsigned>(lx) | (static_cast<unsigned>(ly) << 16));
-        if (at) *at = r.search;
+  /* CDEF */
+  {
+    const size_t nc = s.n_cdef;
+    P->cdef.resize(nc);
+    P->cdef_search.clear();
+    P->cdef_grid_w = L.p[0].stride >> 3;
+    P->cdef_grid_n = P->cdef_grid_w * (plane_rows(L, 0) >> 3);
+    const int pieces = pieces_for(nc, c, 4096);
+    std::vector<CdefOut>& outs = c.scratch->cdef;
+    if (outs.size() < static_cast<size_t>(pieces)) outs.resize(pieces);
+    c.pool->run(pieces, [&](int i) {
+      CdefOut* O = &outs[i];
+      O->unaligned.clear();
+      O->any = false;
+      O->err = PlanErr();
+      for (size_t k = piece_begin(nc, pieces, i); k < piece_begin(nc, pieces, i + 1); ++k)
+        if (plan_cdef(c, s, k, P->cdef_grid_w, P->cdef.data(), O)) break;
+    });
+    P->cdef_search_any = false;
+    for (int i = 0; i < pieces; ++i) {
+      if (outs[i].err.code) return fail(d, outs[i].err.code, outs[i].err.msg);
+      P->cdef_search_any |= outs[i].any;
+      for (size_t k : outs[i].unaligned) {
+        const av1b_cdef_block& b = s.cdef[k];
+        const int sx = b.plane ? L.ss_x : 0, sy = b.plane ? L.ss_y : 0;
+        P->cdef[k].search = P->cdef_grid_n + static_cast<int>(P->cdef_search.size());
+        P->cdef_search.push_back(static_cast<unsigned>(b.x << sx) | (static_cast<unsigned>(b.y << sy) << 16));
       }
     }
   }
@@ -816,11 +1066,15 @@ size_t stage_put(size_t* off, const std::vector<T>& v) {
 /* Stages the profiler reports (av1b_profile). */
 enum Stage {
   kStOwner, kStInter, kStItx, kStUnits, kStDeblockV, kStDeblockH, kStCdef, kStUpscale, kStLr,
-  kStGrainTemplate, kStGrainBlend, kStNv12, kStRgb, kStCopy, kStageCount
+  kStGrainTemplate, kStGrainBlend, kStNv12, kStRgb, kStCopy,
+  /* host time of plan_frame: records, the wait for the staging buffer, the
+   * copy into it */
+  kStPlanHost, kStWaitHost, kStStageHost, kStageCount
 };
+static_assert(kStageCount <= 24, "profile table");
 const char* const kStageNames[kStageCount] = {
     "owner", "inter", "itx", "units", "deblock_v", "deblock_h", "cdef", "upscale", "lr",
-    "grain_template", "grain_blend", "nv12", "rgb", "copy"};
+    "grain_template", "grain_blend", "nv12", "rgb", "copy", "plan_host", "wait_host", "stage_host"};
 
 cudaEvent_t pool_event(av1b_decoder* d) {
   if (d->ev_used == d->ev_pool.size()) {
@@ -845,6 +1099,14 @@ cudaError_t timed(av1b_decoder* d, int stage, F launch, cudaStream_t on = nullpt
   cudaEventRecord(b, on);
   d->marks.push_back(std::make_pair(stage, i0));
   return e;
+}
+
+/* Host time since `t0` into a host stage, when profiling. */
+void host_mark(av1b_decoder* d, int stage, std::chrono::steady_clock::time_point t0) {
+  if (!d->profiling) return;
+  d->prof_ms[stage] +=
+      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  d->prof_n[stage] += 1;
 }
 
 /* After a synchronisation: folds the recorded stage times into the totals. */
@@ -879,8 +1141,14 @@ int check_header(av1b_decoder* d, const av1b_frame_syntax& s) {
 struct av1b_plan {
   int width = 0, height = 0, coded_width = 0, bit_depth = 8, ss_x = 1, ss_y = 1;
   int sharpness = 0, color_matrix = 1;
+  av1b::Layout L{};
   av1b::Plan P;                   /* host copy of the counts and constants */
   av1b::DevBuf arena, coef, residual;
+  av1b::HostBuf stage;            /* pinned staging of the records */
+  /* ready: the uploads are done; done: the last frame that read this plan has
+   * finished on the device (a plan is re-planned only after that) */
+  cudaEvent_t ready = nullptr, done = nullptr;
+  bool in_flight = false;
   size_t o_blocks = 0, o_txs = 0, o_obmc = 0, o_warps = 0, o_pal = 0, o_units = 0;
   size_t o_tiles = 0, o_itx = 0, o_dbv = 0, o_dbh = 0, o_cdef = 0, o_lr[3] = {0, 0, 0};
   size_t o_map = 0, o_cdef_search = 0;
@@ -892,15 +1160,57 @@ struct av1b_plan {
 namespace av1b {
 namespace {
 
+/* Copies `bytes` from `src` to `dst` in pieces on the pool. */
+void pool_copy(const PlanCtx& c, void* dst, const void* src, size_t bytes) {
+  const size_t piece = 1 << 20;
+  const int n = static_cast<int>((bytes + piece - 1) / piece);
+  if (n <= 1) {
+    if (bytes) std::memcpy(dst, src, bytes);
+    return;
+  }
+  c.pool->run(n, [&](int i) {
+    const size_t o = static_cast<size_t>(i) * piece;
+    std::memcpy(static_cast<uint8_t*>(dst) + o, static_cast<const uint8_t*>(src) + o,
+                std::min(piece, bytes - o));
+  });
+}
+
 /* Plans `s` into `pl`: validation, records, and the upload of records and
- * coefficient pools (stream ordered, so a decode that follows sees them). */
+ * coefficient pools into the plan's device memory, on the upload stream. It
+ * takes neither the decoder's lock nor its stream, so a pipeline plans frame
+ * N+1 while frame N runs. It returns once the uploads are done: the caller's
+ * arrays are free again. */
 int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
+  std::lock_guard<std::mutex> plk(d->plan_mu);
   int rc;
   if ((rc = check_header(d, s))) return rc;
   const int coded_width = (s.coded_width <= 0 || s.coded_width > s.width) ? s.width : s.coded_width;
-  if ((rc = ensure_geometry(d, s, coded_width))) return rc;
+  PlanCtx c;
+  c.L = make_layout(s.width, s.height, coded_width, s.bit_depth, s.ss_x, s.ss_y);
+  {
+    std::lock_guard<std::mutex> lk(d->slot_mu);
+    for (int i = 0; i < kSlots; ++i) {
+      c.slot_used[i] = d->slot_used[i];
+      c.slot_valid[i] = d->slot_valid[i];
+      c.slot_width[i] = d->slot_width[i];
+      c.slot_height[i] = d->slot_height[i];
+    }
+  }
+  c.pool = d->pool;
+  c.scratch = d->scratch;
+  if (!pl->ready) {
+    CK(cudaEventCreateWithFlags(&pl->ready, cudaEventDisableTiming), "event");
+    CK(cudaEventCreateWithFlags(&pl->done, cudaEventDisableTiming), "event");
+  }
+  if (pl->in_flight) {
+    CK(cudaEventSynchronize(pl->done), "plan reuse wait");
+    pl->in_flight = false;
+  }
   Plan& P = pl->P;
-  if ((rc = build_plan(d, s, &P))) return rc;
+  auto t0 = std::chrono::steady_clock::now();
+  if ((rc = build_plan(d, c, s, &P))) return rc;
+  host_mark(d, kStPlanHost, t0);
+  pl->L = c.L;
   pl->width = s.width;
   pl->height = s.height;
   pl->coded_width = coded_width;
@@ -922,7 +1232,7 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
       if (used[i]) pl->slots_read[n++] = i;
     pl->slots_read[n] = -1;
   }
-  cudaStream_t st = d->stream;
+  cudaStream_t st = d->upload;
   size_t off = 0;
   pl->o_blocks = stage_put(&off, P.blocks);
   pl->o_txs = stage_put(&off, P.txs);
@@ -940,13 +1250,10 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
   pl->o_map = off;
   off = align_up(off + s.n_palette_map + 64, 256);
   const size_t total = off;
-  if ((rc = host_ensure(d, d->stage, total)) || (rc = dev_ensure(d, pl->arena, total))) return rc;
-  /* the staging buffer may still feed an earlier upload */
-  CK(cudaStreamSynchronize(st), "stream sync");
-  uint8_t* hs = static_cast<uint8_t*>(d->stage.p);
-  auto put = [&](size_t o, const void* src, size_t bytes) {
-    if (bytes) std::memcpy(hs + o, src, bytes);
-  };
+  if ((rc = host_ensure(d, pl->stage, total)) || (rc = dev_ensure(d, pl->arena, total))) return rc;
+  t0 = std::chrono::steady_clock::now();
+  uint8_t* hs = static_cast<uint8_t*>(pl->stage.p);
+  auto put = [&](size_t o, const void* src, size_t bytes) { pool_copy(c, hs + o, src, bytes); };
   put(pl->o_blocks, P.blocks.data(), P.blocks.size() * sizeof(BlockRec));
   put(pl->o_txs, P.txs.data(), P.txs.size() * sizeof(TxRec));
   put(pl->o_obmc, P.obmc.data(), P.obmc.size() * sizeof(ObmcRec));
@@ -963,6 +1270,7 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
     put(pl->o_lr[p], P.lr_units[p].data(), P.lr_units[p].size() * sizeof(LrUnitRec));
   put(pl->o_map, s.palette_map, s.n_palette_map);
   std::memset(hs + pl->o_map + s.n_palette_map, 0, 64);
+  host_mark(d, kStStageHost, t0);
   CK(cudaMemcpyAsync(pl->arena.p, hs, total, cudaMemcpyHostToDevice, st), "arena upload");
 
   /* coefficient and residual pools, zero past the caller's arrays */
@@ -983,6 +1291,10 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
       CK(cudaMemsetAsync(static_cast<int*>(pl->residual.p) + s.n_residual, 0,
                          (P.residual_pool - s.n_residual) * sizeof(int), st), "residual pad");
   }
+  CK(cudaEventRecord(pl->ready, st), "event");
+  t0 = std::chrono::steady_clock::now();
+  CK(cudaEventSynchronize(pl->ready), "upload wait");
+  host_mark(d, kStWaitHost, t0);
   return AV1B_OK;
 }
 
@@ -1001,6 +1313,8 @@ int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, cons
   hdr.ss_x = pl->ss_x;
   hdr.ss_y = pl->ss_y;
   if ((rc = ensure_geometry(d, hdr, pl->coded_width))) return rc;
+  if (std::memcmp(&d->L, &pl->L, sizeof(Layout)) != 0)
+    return fail(d, AV1B_ERR_ARG, "a plan of another picture layout");
   for (int i = 0; pl->slots_read[i] >= 0; ++i) {
     const int sl = pl->slots_read[i];
     if (!d->slot_used[sl] || !d->slot_valid[sl] || d->slot_width[sl] != pl->width ||
@@ -1031,8 +1345,9 @@ int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, cons
     if ((rc = dev_ensure(d, d->slot_buf[slot], static_cast<size_t>(L.size) * sizeof(px_t)))) return rc;
   }
   const size_t pic_bytes = static_cast<size_t>(L.size) * sizeof(px_t);
-  if (!P.cdef_search.empty() &&
-      (rc = dev_ensure(d, d->cdef_search, P.cdef_search.size() * sizeof(int))))
+  if (P.pre_res_pool && (rc = dev_ensure(d, d->pre_res, P.pre_res_pool * sizeof(int)))) return rc;
+  if ((P.cdef_search_any || !P.cdef_search.empty()) &&
+      (rc = dev_ensure(d, d->cdef_search, (P.cdef_grid_n + P.cdef_search.size()) * sizeof(int))))
     return rc;
   if (P.use_lr) {
     if ((rc = dev_ensure(d, d->lr_pre, pic_bytes)) || (rc = dev_ensure(d, d->lr_cdef, pic_bytes)) ||
@@ -1040,6 +1355,10 @@ int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, cons
       return rc;
   }
   if (P.grain && (rc = init_grain_tables(d))) return rc;
+
+  /* the plan's uploads (done when plan_frame returned; the wait orders them
+   * on this stream) */
+  CK(cudaStreamWaitEvent(st, pl->ready, 0), "upload order");
 
   /* slot pointer table, uploaded when a slot buffer moved */
   {
@@ -1109,6 +1428,7 @@ int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, cons
   a.n_inter_tiles = static_cast<int>(P.inter_tiles.size());
   a.itx_jobs = reinterpret_cast<const int2*>(ar + pl->o_itx);
   a.n_itx = static_cast<int>(P.itx_jobs.size());
+  a.pre_res = static_cast<int*>(d->pre_res.p);
   a.maxv = maxv;
   a.scale_x = P.scale_x;
   a.scale_y = P.scale_y;
@@ -1170,7 +1490,8 @@ int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, cons
        }), "CDEF snapshot");
     CK(timed(d, kStCdef, [&] {
          return launch_cdef(snap, cur, reinterpret_cast<const CdefRec*>(ar + pl->o_cdef),
-                            static_cast<int>(P.cdef.size()),
+                            static_cast<int>(P.cdef.size()), P.cdef_grid_w, P.cdef_grid_n,
+                            P.cdef_search_any,
                             reinterpret_cast<const unsigned*>(ar + pl->o_cdef_search),
                             static_cast<int>(P.cdef_search.size()),
                             static_cast<int*>(d->cdef_search.p), L, st);
@@ -1241,7 +1562,10 @@ int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, cons
   d->stats.waves = 0;
   d->stats.kernel_launches = launches;
   d->stats_pending = true;
+  CK(cudaEventRecord(pl->done, st), "event");
+  pl->in_flight = true;
   if (keep) {
+    std::lock_guard<std::mutex> lk(d->slot_mu);
     d->slot_used[slot] = true;
     d->slot_valid[slot] = true;
     d->slot_width[slot] = pl->width;
@@ -1253,6 +1577,32 @@ int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, cons
   if (out_slot) *out_slot = slot;
   if (sync) return finish_frame(d);
   return AV1B_OK;
+}
+
+/* Frees a plan's buffers and events once no frame reads it any more. */
+void release_plan(av1b_decoder* d, av1b_plan* pl) {
+  if (pl->in_flight) cudaEventSynchronize(pl->done);
+  dev_release(d, pl->arena);
+  dev_release(d, pl->coef);
+  dev_release(d, pl->residual);
+  if (pl->stage.p) cudaFreeHost(pl->stage.p);
+  pl->stage.p = nullptr;
+  if (pl->ready) cudaEventDestroy(pl->ready);
+  if (pl->done) cudaEventDestroy(pl->done);
+  delete pl;
+}
+
+/* Returns a plan to the decoder's pool (its buffers stay allocated for the
+ * next plan), or frees it when the pool is full. */
+void recycle_plan(av1b_decoder* d, av1b_plan* pl) {
+  {
+    std::lock_guard<std::mutex> lk(d->plan_pool_mu);
+    if (d->plan_pool.size() < 4) {
+      d->plan_pool.push_back(pl);
+      return;
+    }
+  }
+  release_plan(d, pl);
 }
 
 /* Waits for the frame in flight and checks its status word. */
@@ -1300,6 +1650,7 @@ int picture_of(av1b_decoder* d, int slot, const px_t** pic) {
 
 void copy_error(const av1b_decoder* d, char* error, size_t len) {
   if (!error || !len) return;
+  std::lock_guard<std::mutex> lk(const_cast<av1b_decoder*>(d)->err_mu);
   std::snprintf(error, len, "%s", d->err.c_str());
 }
 
@@ -1326,6 +1677,7 @@ int av1b_decoder_create(int device, size_t hbm_budget_bytes, av1b_decoder** out)
             cudaHostAlloc(reinterpret_cast<void**>(&d->status_host), 64, cudaHostAllocDefault) == cudaSuccess;
   for (int i = 0; ok && i < 3; ++i) ok = cudaEventCreate(&d->ev[i]) == cudaSuccess;
   ok = ok && cudaStreamCreateWithFlags(&d->aux, cudaStreamNonBlocking) == cudaSuccess &&
+       cudaStreamCreateWithFlags(&d->upload, cudaStreamNonBlocking) == cudaSuccess &&
        cudaEventCreateWithFlags(&d->ev_fork, cudaEventDisableTiming) == cudaSuccess &&
        cudaEventCreateWithFlags(&d->ev_join, cudaEventDisableTiming) == cudaSuccess;
   if (!ok) {
@@ -1333,6 +1685,11 @@ int av1b_decoder_create(int device, size_t hbm_budget_bytes, av1b_decoder** out)
     return AV1B_ERR_CUDA;
   }
   *d->status_host = 0;
+  {
+    const unsigned hc = std::thread::hardware_concurrency();
+    d->pool = new WorkPool(static_cast<int>(std::min(16u, std::max(1u, hc))));
+    d->scratch = new PlanScratch;
+  }
   d->own_plan = new av1b_plan;
   d->own_plan->owned_by_decoder = true;
   *out = d;
@@ -1343,12 +1700,15 @@ int av1b_decoder_destroy(av1b_decoder* d) {
   if (!d) return AV1B_ERR_ARG;
   cudaSetDevice(d->device);
   if (d->stream) cudaStreamSynchronize(d->stream);
-  if (d->own_plan) {
-    dev_release(d, d->own_plan->arena);
-    dev_release(d, d->own_plan->coef);
-    dev_release(d, d->own_plan->residual);
-    delete d->own_plan;
+  if (d->own_plan) release_plan(d, d->own_plan);
+  for (av1b_plan* pl : d->plan_pool) release_plan(d, pl);
+  d->plan_pool.clear();
+  if (d->upload) {
+    cudaStreamSynchronize(d->upload);
+    cudaStreamDestroy(d->upload);
   }
+  delete d->pool;
+  delete d->scratch;
   for (int i = 0; i < 3; ++i)
     if (d->ev[i]) cudaEventDestroy(d->ev[i]);
   if (d->aux) {
@@ -1361,10 +1721,9 @@ int av1b_decoder_destroy(av1b_decoder* d) {
   DevBuf* bufs[] = {&d->cur, &d->snap, &d->lr_pre, &d->lr_pre_up, &d->lr_cdef, &d->disp,
                     &d->slot_ptr_dev, &d->arena, &d->coef, &d->residual, &d->owner[0],
                     &d->owner[1], &d->owner[2], &d->done, &d->status_q, &d->nv12, &d->rgb,
-                    &d->grain_state, &d->orbit, &d->pos, &d->cdef_search};
+                    &d->grain_state, &d->orbit, &d->pos, &d->cdef_search, &d->pre_res};
   for (DevBuf* b : bufs) dev_release(d, *b);
   for (int i = 0; i < kSlots; ++i) dev_release(d, d->slot_buf[i]);
-  if (d->stage.p) cudaFreeHost(d->stage.p);
   if (d->stream) cudaStreamDestroy(d->stream);
   delete d;
   return AV1B_OK;
@@ -1373,6 +1732,7 @@ int av1b_decoder_destroy(av1b_decoder* d) {
 int av1b_decoder_reset(av1b_decoder* d) {
   if (!d) return AV1B_ERR_ARG;
   std::lock_guard<std::mutex> lk(d->mu);
+  std::lock_guard<std::mutex> slk(d->slot_mu);
   for (int i = 0; i < kSlots; ++i) {
     d->slot_used[i] = false;
     d->slot_valid[i] = false;
@@ -1389,7 +1749,7 @@ int av1b_decode(av1b_decoder* d, const av1b_frame_syntax* syntax, int keep_refer
   std::lock_guard<std::mutex> lk(d->mu);
   cudaSetDevice(d->device);
   if (out_slot) *out_slot = -1;
-  d->err.clear();
+  clear_err(d);
   const int rc = run_frame(d, *syntax, keep_reference ? 1 : 0, -1, out, out_slot);
   if (rc) copy_error(d, error, error_len);
   return rc;
@@ -1400,26 +1760,31 @@ int av1b_decode_blob(av1b_decoder* d, const uint8_t* blob, size_t len, int keep_
   av1b_frame_syntax v;
   if (!d) return AV1B_ERR_ARG;
   if (!view_blob(blob, len, &v)) {
-    d->err = "malformed serialized frame";
+    fail(d, AV1B_ERR_ARG, "malformed serialized frame");
     copy_error(d, error, error_len);
     return AV1B_ERR_ARG;
   }
   return av1b_decode(d, &v, keep_reference, out, out_slot, error, error_len);
 }
 
+/* Planning takes no decoder lock: it may run on its own thread while frames
+ * decode (see plan_frame). */
 int av1b_plan_frame(av1b_decoder* d, const av1b_frame_syntax* syntax, av1b_plan** out) {
   if (!d || !syntax || !out) return AV1B_ERR_ARG;
-  std::lock_guard<std::mutex> lk(d->mu);
   cudaSetDevice(d->device);
-  d->err.clear();
   *out = nullptr;
-  auto* pl = new av1b_plan;
+  av1b_plan* pl = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(d->plan_pool_mu);
+    if (!d->plan_pool.empty()) {
+      pl = d->plan_pool.back();
+      d->plan_pool.pop_back();
+    }
+  }
+  if (!pl) pl = new av1b_plan;
   const int rc = plan_frame(d, *syntax, pl);
   if (rc) {
-    dev_release(d, pl->arena);
-    dev_release(d, pl->coef);
-    dev_release(d, pl->residual);
-    delete pl;
+    recycle_plan(d, pl);
     return rc;
   }
   *out = pl;
@@ -1429,13 +1794,8 @@ int av1b_plan_frame(av1b_decoder* d, const av1b_frame_syntax* syntax, av1b_plan*
 int av1b_plan_free(av1b_decoder* d, av1b_plan* pl) {
   if (!d) return AV1B_ERR_ARG;
   if (!pl) return AV1B_OK;
-  std::lock_guard<std::mutex> lk(d->mu);
   cudaSetDevice(d->device);
-  cudaStreamSynchronize(d->stream);
-  dev_release(d, pl->arena);
-  dev_release(d, pl->coef);
-  dev_release(d, pl->residual);
-  delete pl;
+  recycle_plan(d, pl);
   return AV1B_OK;
 }
 
@@ -1444,7 +1804,7 @@ int av1b_decode_planned(av1b_decoder* d, av1b_plan* pl, int slot, int keep_refer
   if (!d || !pl) return AV1B_ERR_ARG;
   std::lock_guard<std::mutex> lk(d->mu);
   cudaSetDevice(d->device);
-  d->err.clear();
+  clear_err(d);
   if (out_slot) *out_slot = -1;
   return execute_plan(d, pl, keep_reference ? 1 : 0, slot, out, out_slot, wait != 0);
 }
@@ -1460,6 +1820,7 @@ int av1b_reserve_reference(av1b_decoder* d, int* out_slot) {
   if (!d || !out_slot) return AV1B_ERR_ARG;
   std::lock_guard<std::mutex> lk(d->mu);
   *out_slot = -1;
+  std::lock_guard<std::mutex> slk(d->slot_mu);
   for (int i = 0; i < kSlots; ++i)
     if (!d->slot_used[i]) {
       d->slot_used[i] = true;
@@ -1475,7 +1836,7 @@ int av1b_decode_reserved(av1b_decoder* d, const av1b_frame_syntax* syntax, int s
   if (!d || !syntax) return AV1B_ERR_ARG;
   std::lock_guard<std::mutex> lk(d->mu);
   cudaSetDevice(d->device);
-  d->err.clear();
+  clear_err(d);
   int got = -1;
   const int rc = run_frame(d, *syntax, slot >= 0 ? 1 : 0, slot, out, &got);
   if (rc) copy_error(d, error, error_len);
@@ -1485,6 +1846,7 @@ int av1b_decode_reserved(av1b_decoder* d, const av1b_frame_syntax* syntax, int s
 int av1b_release_reference(av1b_decoder* d, int slot) {
   if (!d) return AV1B_ERR_ARG;
   std::lock_guard<std::mutex> lk(d->mu);
+  std::lock_guard<std::mutex> slk(d->slot_mu);
   if (slot >= 0 && slot < kSlots) {
     d->slot_used[slot] = false;
     d->slot_valid[slot] = false;

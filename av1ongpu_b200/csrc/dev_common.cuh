@@ -123,6 +123,8 @@ struct TxRec {
   short x, y;
   short w, h;                 /* 4..64 for a transform; any size for raw residual */
   unsigned char log2w, log2h, type, row_shift;
+  int pre_off;                /* >= 0: the residual is computed ahead, here in the
+                                 precomputed residual buffer (w * h, row-major) */
 };
 
 /* One OBMC strip. */

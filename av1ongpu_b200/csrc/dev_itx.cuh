@@ -438,7 +438,7 @@ AV1B_DEV void itx_row(const ItxParams& p, const int* __restrict__ coef, int y, i
 /* Pass 2 for column `x`: tmp -> residual, added to dst with the flips. */
 template <int LH, bool CG>
 AV1B_DEV void itx_col_add(const ItxParams& p, const int* tmp, int x, px_t* dst, int stride,
-                          int maxv) {
+                          int maxv, int* res = nullptr) {
   constexpr int H = 1 << LH;
   const int W = 1 << p.lw;
   int t[H];
@@ -456,6 +456,10 @@ AV1B_DEV void itx_col_add(const ItxParams& p, const int* tmp, int x, px_t* dst, 
   for (int i = 0; i < H; ++i) {
     const int r = p.lossless ? t[i] : rnd2(t[i], 4);
     const int yy = fud ? H - 1 - i : i;
+    if (res) {
+      res[yy * W + xx] = r;
+      continue;
+    }
     px_t* q = dst + yy * stride + xx;
     const int old = CG ? (int)__ldcg(q) : (int)*q;
     *q = (px_t)clampi(old + r, 0, maxv);
@@ -474,13 +478,13 @@ AV1B_DEV void itx_row_dispatch(const ItxParams& p, const int* coef, int y, int* 
 
 template <bool CG>
 AV1B_DEV void itx_col_dispatch(const ItxParams& p, const int* tmp, int x, px_t* dst, int stride,
-                               int maxv) {
+                               int maxv, int* res = nullptr) {
   switch (p.lh) {
-    case 2: itx_col_add<2, CG>(p, tmp, x, dst, stride, maxv); break;
-    case 3: itx_col_add<3, CG>(p, tmp, x, dst, stride, maxv); break;
-    case 4: itx_col_add<4, CG>(p, tmp, x, dst, stride, maxv); break;
-    case 5: itx_col_add<5, CG>(p, tmp, x, dst, stride, maxv); break;
-    default: itx_col_add<6, CG>(p, tmp, x, dst, stride, maxv); break;
+    case 2: itx_col_add<2, CG>(p, tmp, x, dst, stride, maxv, res); break;
+    case 3: itx_col_add<3, CG>(p, tmp, x, dst, stride, maxv, res); break;
+    case 4: itx_col_add<4, CG>(p, tmp, x, dst, stride, maxv, res); break;
+    case 5: itx_col_add<5, CG>(p, tmp, x, dst, stride, maxv, res); break;
+    default: itx_col_add<6, CG>(p, tmp, x, dst, stride, maxv, res); break;
   }
 }
 
@@ -495,6 +499,17 @@ AV1B_DEV void itx_warp(const ItxParams& p, const int* __restrict__ coef, int* tm
   for (int y = lane; y < h; y += 32) itx_row_dispatch(p, coef, y, tmp);
   __syncwarp();
   for (int x = lane; x < w; x += 32) itx_col_dispatch<CG>(p, tmp, x, dst, stride, maxv);
+  __syncwarp();
+}
+
+/* The 2-D transform alone: the residual (before the add and the clip) into
+ * `res`, w * h row-major. */
+AV1B_DEV void itx_warp_residual(const ItxParams& p, const int* __restrict__ coef, int* tmp, int* res,
+                                int lane) {
+  const int w = 1 << p.lw, h = 1 << p.lh;
+  for (int y = lane; y < h; y += 32) itx_row_dispatch(p, coef, y, tmp);
+  __syncwarp();
+  for (int x = lane; x < w; x += 32) itx_col_dispatch<false>(p, tmp, x, nullptr, 0, 0, res);
   __syncwarp();
 }
 

@@ -239,8 +239,8 @@ __device__ void apply_tx(const FrameArgs& a, const BlockRec& b, const TxRec& tx,
                          int lane) {
   const PlaneGeom& g = a.L.p[b.plane];
   px_t* dst = a.cur + g.off + (b.y + tx.y) * g.stride + b.x + tx.x;
-  if (b.residual_provided) {
-    const int* res = a.residual + tx.coef_off;
+  if (b.residual_provided || tx.pre_off >= 0) {
+    const int* res = b.residual_provided ? a.residual + tx.coef_off : a.pre_res + tx.pre_off;
     for (int k = lane; k < tx.w * tx.h; k += 32) {
       const int yy = k / tx.w, xx = k - yy * tx.w;
       px_t* q = dst + yy * g.stride + xx;
@@ -260,7 +260,10 @@ __device__ void apply_tx(const FrameArgs& a, const BlockRec& b, const TxRec& tx,
   itx_warp<CG>(p, a.coef + tx.coef_off, tmp, dst, g.stride, a.maxv, lane);
 }
 
-/* Residual of phase A blocks: one warp per transform. */
+/* Inverse transforms, one warp per transform: those of phase A blocks add
+ * into the picture; those of phase B blocks leave their residual in the
+ * precomputed buffer, so the dependency-scheduled kernel only predicts and
+ * adds (the residual does not depend on the prediction). */
 __global__ void k_itx(const __grid_constant__ FrameArgs a) {
   extern __shared__ int smem[];
   const int wib = threadIdx.x >> 5;
@@ -269,7 +272,19 @@ __global__ void k_itx(const __grid_constant__ FrameArgs a) {
   if (warp >= a.n_itx) return;
   const int2 t = a.itx_jobs[warp];
   const BlockRec& b = a.blocks[t.x];
-  apply_tx<false>(a, b, a.txs[t.y], smem + wib * 4096, lane);
+  const TxRec& tx = a.txs[t.y];
+  if (tx.pre_off >= 0) {
+    ItxParams p;
+    p.lw = tx.log2w;
+    p.lh = tx.log2h;
+    p.type = tx.type;
+    p.lossless = b.lossless;
+    p.row_shift = tx.row_shift;
+    p.bitdepth = a.L.bit_depth;
+    itx_warp_residual(p, a.coef + tx.coef_off, smem + wib * 4096, a.pre_res + tx.pre_off, lane);
+    return;
+  }
+  apply_tx<false>(a, b, tx, smem + wib * 4096, lane);
 }
 
 /* ---- phase B -------------------------------------------------------------------------- */
@@ -472,15 +487,27 @@ __global__ void k_deblock(px_t* pic, const DeblockRec* recs, int n, int sharpnes
 /* CDEF direction search (av1gpu_kernels.h:2601-2660), one thread per 8x8 luma
  * block: the 90 partial sums of the eight directions stay in registers (the
  * loops unroll, so every bin index is a constant). The result packs
- * (variance << 3) | direction. Chroma blocks read the search of their luma
+ * (variance << 3) | direction. Threads [0, n_grid) search the cells of the
+ * 8x8 grid (result index = cell), the rest the listed positions off the grid
+ * (result index grid_n + k). Chroma blocks read the search of their luma
  * block, so each luma block is searched once. */
-__global__ void __launch_bounds__(128) k_cdef_search(const px_t* __restrict__ src,
-                                                     const unsigned* __restrict__ pos, int n,
+__global__ void __launch_bounds__(128) k_cdef_search(const px_t* __restrict__ src, int grid_w,
+                                                     int grid_n, int n_grid,
+                                                     const unsigned* __restrict__ pos, int n_extra,
                                                      int* out, const __grid_constant__ Layout L) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n) return;
-  const unsigned q = pos[t];
-  const int x = q & 0xffff, y = q >> 16;
+  if (t >= n_grid + n_extra) return;
+  int x, y, o;
+  if (t < n_grid) {
+    y = (t / grid_w) << 3;
+    x = (t - (t / grid_w) * grid_w) << 3;
+    o = t;
+  } else {
+    const unsigned q = pos[t - n_grid];
+    x = q & 0xffff;
+    y = q >> 16;
+    o = grid_n + (t - n_grid);
+  }
   const int stride = L.p[0].stride, cs = L.bit_depth - 8;
   const px_t* b = src + L.p[0].off + y * stride + x;
   int p0[15] = {}, p1[11] = {}, p2[8] = {}, p3[11] = {}, p4[15] = {}, p5[11] = {}, p6[8] = {},
@@ -554,7 +581,7 @@ __global__ void __launch_bounds__(128) k_cdef_search(const px_t* __restrict__ sr
 #pragma unroll
   for (int i = 0; i < 8; ++i)
     if (i == ((d + 4) & 7)) opp = cost[i];
-  out[t] = (((best - opp) >> 10) << 3) | d;
+  out[o] = (((best - opp) >> 10) << 3) | d;
 }
 
 __constant__ signed char kCdefDirs[8][2][2] = {
@@ -1131,12 +1158,14 @@ cudaError_t launch_deblock(px_t* pic, const DeblockRec* recs, int n, int sharpne
   return cudaGetLastError();
 }
 
-cudaError_t launch_cdef(const px_t* src, px_t* dst, const CdefRec* recs, int n,
-                        const unsigned* search_pos, int n_search, int* search, const Layout& L,
-                        cudaStream_t s) {
+cudaError_t launch_cdef(const px_t* src, px_t* dst, const CdefRec* recs, int n, int grid_w,
+                        int grid_n, bool grid, const unsigned* extra_pos, int n_extra, int* search,
+                        const Layout& L, cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
-  if (n_search > 0)
-    k_cdef_search<<<cdiv(n_search, 128), 128, 0, s>>>(src, search_pos, n_search, search, L);
+  const int n_grid = grid ? grid_n : 0;
+  if (n_grid + n_extra > 0)
+    k_cdef_search<<<cdiv(n_grid + n_extra, 128), 128, 0, s>>>(src, grid_w, grid_n, n_grid, extra_pos,
+                                                               n_extra, search, L);
   k_cdef_warp<<<cdiv(n, 4), 128, 0, s>>>(src, dst, recs, n, search, L);
   return cudaGetLastError();
 }

@@ -37,8 +37,10 @@ struct FrameArgs {
   unsigned* queue;
   const int2* inter_tiles;      /* phase A: (block, x0 | y0 << 16) */
   int n_inter_tiles;
-  const int2* itx_jobs;         /* phase A: (block, transform) */
+  const int2* itx_jobs;         /* phase A: (block, transform); the transforms of
+                                   phase B blocks compute their residual ahead */
   int n_itx;
+  int* pre_res;                 /* residuals computed ahead (TxRec::pre_off) */
   int* status;
   int maxv;
   int scale_x, scale_y;
@@ -77,11 +79,12 @@ cudaError_t launch_selftest_wait(const unsigned* flag, int* status, unsigned lon
 cudaError_t launch_recon_stage(int stage, const FrameArgs& a, int n_sm, cudaStream_t s);
 cudaError_t launch_deblock(px_t* pic, const DeblockRec* recs, int n, int sharpness, int bd,
                            int maxv, cudaStream_t s);
-/* CDEF: the direction searches (luma positions packed x | y << 16, results
- * into `search`), then the filter of every record. */
-cudaError_t launch_cdef(const px_t* src, px_t* dst, const CdefRec* recs, int n,
-                        const unsigned* search_pos, int n_search, int* search, const Layout& L,
-                        cudaStream_t s);
+/* CDEF: the direction searches - every 8x8 luma block of a grid_w-wide grid
+ * (grid_n cells) when `grid`, then the n_extra positions off the grid (x | y
+ * << 16, results after the grid's) - then the filter of every record. */
+cudaError_t launch_cdef(const px_t* src, px_t* dst, const CdefRec* recs, int n, int grid_w,
+                        int grid_n, bool grid, const unsigned* extra_pos, int n_extra, int* search,
+                        const Layout& L, cudaStream_t s);
 /* border_rows: only the rows within two of a loop restoration stripe
  * boundary (for the pre-CDEF picture loop restoration reads). */
 cudaError_t launch_upscale(const px_t* src, px_t* dst, const Layout& L, int maxv, bool border_rows,

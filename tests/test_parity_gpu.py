@@ -166,6 +166,50 @@ def test_planned_decode_matches_direct(av1b, dec):
         dec.release_reference(s)
 
 
+def test_planning_on_another_thread(av1b, dec):
+    """A planner thread plans frame k + 1 (validation, records, uploads) while
+    frame k decodes and packs NV12 on the calling thread - the pipelined use
+    of plan_frame / decode_reference_planned - and every frame's NV12 equals
+    the one-call decode's. Plans are recycled through the decoder's pool."""
+    import queue
+    import threading
+    blobs = [av1b.synth_frame(2, 4, 77, k) for k in range(8)]
+    w, _, h, _, sx, sy = blobs[0].header
+    pitch = (w + 63) // 64 * 64
+    import refdec
+    direct = refdec.Stream(dec)
+    want = []
+    for k, b in enumerate(blobs):
+        slot, _ = direct.decode(k, b, read_back=False)
+        want.append(dec.to_nv12(slot, pitch, w, h))
+    for s in list(direct.slots.values()):
+        dec.release_reference(s)
+    ring = [dec.reserve_reference() for _ in range(4)]
+    plans = queue.Queue(maxsize=2)
+
+    def planner():
+        for k, b in enumerate(blobs):
+            d = b.get_refs()
+            b.set_refs([ring[(k - x) % 4] for x in d])
+            plans.put(dec.plan(b))
+            b.set_refs(d)
+
+    th = threading.Thread(target=planner)
+    th.start()
+    try:
+        for k in range(len(blobs)):
+            pl = plans.get(timeout=120)
+            dec.decode_planned(pl, slot=ring[k % 4], keep=True, wait=False)
+            got = dec.to_nv12(ring[k % 4], pitch, w, h)
+            dec.free_plan(pl)
+            assert np.array_equal(got, want[k]), k
+        dec.sync()
+    finally:
+        th.join()
+    for s in ring:
+        dec.release_reference(s)
+
+
 def test_decode_drop_and_slot_semantics(av1b, oracle, dec):
     """decode (keep = False) holds no slot; to_nv12 of an older slot packs its
     stored picture (before film grain), of the newest the output picture."""
