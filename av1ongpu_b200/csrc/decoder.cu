@@ -54,11 +54,6 @@ struct DevBuf {
   size_t cap = 0;
 };
 
-struct HostBuf {
-  void* p = nullptr;
-  size_t cap = 0;
-};
-
 }  // namespace
 }  // namespace av1b
 
@@ -107,7 +102,7 @@ struct av1b_decoder {
   bool have_last = false;
 
   /* per-frame buffers */
-  DevBuf arena, coef, residual, owner[3], done, status_q, nv12, rgb;
+  DevBuf arena, coef, residual, done, status_q, nv12, rgb;
   unsigned epoch = 0;
 
   /* film grain */
@@ -197,20 +192,6 @@ void dev_release(av1b_decoder* d, DevBuf& b) {
   b.cap = 0;
 }
 
-int host_ensure(av1b_decoder* d, HostBuf& b, size_t bytes) {
-  if (b.cap >= bytes) return AV1B_OK;
-  if (b.p) cudaFreeHost(b.p);
-  b.p = nullptr;
-  b.cap = 0;
-  const size_t want = align_up(bytes + bytes / 4, 1 << 20);
-  void* p = nullptr;
-  cudaError_t e = cudaHostAlloc(&p, want, cudaHostAllocDefault);
-  if (e != cudaSuccess) return cuda_fail(d, e, "cudaHostAlloc");
-  b.p = p;
-  b.cap = want;
-  return AV1B_OK;
-}
-
 Layout make_layout(int width, int height, int coded_width, int bd, int ss_x, int ss_y) {
   Layout L{};
   L.ss_x = ss_x;
@@ -295,21 +276,48 @@ int init_grain_tables(av1b_decoder* d) {
 
 /* ---- the planner ------------------------------------------------------------------------- */
 
+/* Page-locked host memory for the plan's record lists, so they upload
+ * straight from where the planner wrote them (no staging copy). A plan keeps
+ * its lists between frames, so allocations stop once the sizes settle. */
+template <class T>
+struct PinnedAlloc {
+  using value_type = T;
+  PinnedAlloc() = default;
+  template <class U>
+  PinnedAlloc(const PinnedAlloc<U>&) {}
+  T* allocate(size_t n) {
+    void* p = nullptr;
+    if (cudaHostAlloc(&p, std::max<size_t>(n, 1) * sizeof(T), cudaHostAllocDefault) != cudaSuccess)
+      throw std::bad_alloc();
+    return static_cast<T*>(p);
+  }
+  void deallocate(T* p, size_t) { cudaFreeHost(p); }
+  template <class U>
+  bool operator==(const PinnedAlloc<U>&) const { return true; }
+  template <class U>
+  bool operator!=(const PinnedAlloc<U>&) const { return false; }
+};
+template <class T>
+using pvec = std::vector<T, PinnedAlloc<T>>;
+
 struct Plan {
-  std::vector<BlockRec> blocks;
-  std::vector<TxRec> txs;
-  std::vector<ObmcRec> obmc;
-  std::vector<WarpRec> warps;
-  std::vector<int> palette_colors;
-  std::vector<int> units;
-  std::vector<int2> inter_tiles;
-  std::vector<int2> itx_jobs;
-  std::vector<DeblockRec> deblock_v, deblock_h;
-  std::vector<CdefRec> cdef;
-  std::vector<unsigned> cdef_search;  /* searches off the 8x8 grid: x | y << 16 */
+  pvec<BlockRec> blocks;
+  pvec<TxRec> txs;
+  pvec<ObmcRec> obmc;
+  pvec<WarpRec> warps;
+  pvec<int> palette_colors;
+  pvec<int> units;                /* phase B blocks in claim order */
+  pvec<int> deps;                 /* per phase B block (dep_first, dep_count): the
+                                     phase B blocks it waits for */
+  int unit_depth = 0;             /* dependency depth of the frame */
+  pvec<int2> inter_tiles;
+  pvec<int2> itx_jobs;
+  pvec<DeblockRec> deblock_v, deblock_h;
+  pvec<CdefRec> cdef;
+  pvec<unsigned> cdef_search;     /* searches off the 8x8 grid: x | y << 16 */
   int cdef_grid_w = 0, cdef_grid_n = 0;  /* the grid of 8x8 luma searches */
   bool cdef_search_any = false;          /* some record reads the grid */
-  std::vector<LrUnitRec> lr_units[3];
+  pvec<LrUnitRec> lr_units[3];
   LrArgs lr{};
   bool use_lr = false;
   size_t coef_pool = 0, residual_pool = 0;
@@ -710,6 +718,10 @@ struct PlanScratch {
   std::vector<BlockOut> blocks;
   std::vector<EdgeOut> edges;
   std::vector<CdefOut> cdef;
+  std::vector<int> owner[3];
+  std::vector<std::vector<int>> unit_deps;
+  std::vector<int> dep_count, depth, sorted;
+  std::vector<uint8_t> is_b;
 };
 
 /* Splits [0, n) into pieces of at least `min_piece` for the pool. */
@@ -720,6 +732,231 @@ int pieces_for(size_t n, const PlanCtx& c, size_t min_piece) {
 }
 inline size_t piece_begin(size_t n, int pieces, int i) { return n * i / pieces; }
 
+/* The dependency-scheduled (phase B) blocks: what each waits for, and the
+ * order the device claims them in.
+ *
+ * A block waits for the blocks that own the samples it reads from this
+ * picture - its left column and above row (extended below-left / above-right
+ * when a directional mode reads there and that part was decoded before it),
+ * the corner, an intra block copy's source, CFL's co-located luma - as the
+ * reference's owner grids (square cells of 4 luma samples, 2 for a chroma
+ * plane whose axis is subsampled; plane 1 keyed on ss_x and plane 2 on ss_y,
+ * engine.cpp:737-741) and already_decoded (engine.cpp:784-793) define them.
+ * Blocks of the parallel phase are complete before any of these run, so only
+ * phase B owners are kept: a short deduplicated list per block, resolved here
+ * once instead of by owner lookups on the device's critical path. The
+ * above-right / below-left availability the reference derives the same way is
+ * resolved here too.
+ *
+ * The claim order is by dependency depth (1 + the deepest block waited for),
+ * coding order within a depth. Every block a block waits for is shallower, so
+ * it is claimed earlier - by a warp that is running it or will - and every
+ * depth runs as one wide wave. */
+int plan_units(av1b_decoder* d, const PlanCtx& c, Plan* P) {
+  const Layout& L = c.L;
+  P->deps.clear();
+  if (P->units.empty()) return AV1B_OK;
+  PlanScratch& S = *c.scratch;
+  int sh[3], cw[3], ch[3];
+  for (int p = 0; p < 3; ++p) {
+    sh[p] = p == 0 ? 2 : (p == 1 ? (L.ss_x ? 1 : 2) : (L.ss_y ? 1 : 2));
+    cw[p] = (L.p[p].grid_w + (1 << sh[p]) - 1) >> sh[p];
+    ch[p] = (L.p[p].grid_h + (1 << sh[p]) - 1) >> sh[p];
+    S.owner[p].resize(static_cast<size_t>(cw[p]) * ch[p]);
+  }
+  c.pool->run(3 * 8, [&](int i) {
+    std::vector<int>& o = S.owner[i / 8];
+    std::fill(o.begin() + piece_begin(o.size(), 8, i % 8), o.begin() + piece_begin(o.size(), 8, i % 8 + 1), -1);
+  });
+  /* owner grids: later blocks overwrite earlier ones where cells overlap, so
+   * a plane whose blocks are not all cell aligned is filled in order */
+  const size_t nb = P->blocks.size();
+  std::vector<uint8_t>& is_b = S.is_b;
+  is_b.resize(nb);
+  bool aligned[3] = {true, true, true};
+  for (size_t bi = 0; bi < nb; ++bi) {
+    const BlockRec& b = P->blocks[bi];
+    const int m = (1 << sh[b.plane]) - 1;
+    if ((b.x | b.y | b.w | b.h) & m) aligned[b.plane] = false;
+    is_b[bi] = b.phase_b;
+  }
+  auto fill = [&](size_t bi) {
+    const BlockRec& b = P->blocks[bi];
+    const int p = b.plane, oc = 1 << sh[p];
+    const int cx0 = std::max<int>(b.x, 0) >> sh[p], cy0 = std::max<int>(b.y, 0) >> sh[p];
+    const int cx1 = std::min((b.x + b.w + oc - 1) >> sh[p], cw[p]);
+    const int cy1 = std::min((b.y + b.h + oc - 1) >> sh[p], ch[p]);
+    int* o = S.owner[p].data();
+    for (int y = cy0; y < cy1; ++y)
+      for (int x = cx0; x < cx1; ++x) o[static_cast<size_t>(y) * cw[p] + x] = static_cast<int>(bi);
+  };
+  {
+    const int pieces = pieces_for(nb, c, 2048);
+    c.pool->run(pieces, [&](int i) {
+      for (size_t bi = piece_begin(nb, pieces, i); bi < piece_begin(nb, pieces, i + 1); ++bi)
+        if (aligned[P->blocks[bi].plane]) fill(bi);
+    });
+    if (!aligned[0] || !aligned[1] || !aligned[2])
+      for (size_t bi = 0; bi < nb; ++bi)
+        if (!aligned[P->blocks[bi].plane]) fill(bi);
+  }
+  auto owner_at = [&](int p, int x, int y) -> int {
+    if (x < 0 || y < 0 || x >= L.p[p].grid_w || y >= L.p[p].grid_h) return -1;
+    return S.owner[p][static_cast<size_t>(y >> sh[p]) * cw[p] + (x >> sh[p])];
+  };
+  /* the cells of [x0, x1] x [y0, y1]: `f(owner)` for each, from the cell
+   * holding (x0, y0) on (the device's wait_rect / decoded_before walk) */
+  auto each_cell = [&](int p, int x0, int x1, int y0, int y1, auto&& f) {
+    const int oc = 1 << sh[p];
+    const int xs = x0 & ~(oc - 1), ys = y0 & ~(oc - 1);
+    for (int y = ys; y <= y1; y += oc)
+      for (int x = xs; x <= x1; x += oc) f(owner_at(p, x, y));
+  };
+  static const int kAngle[9] = {0, 90, 180, 45, 135, 113, 157, 203, 67};
+  const size_t nu = P->units.size();
+  const int pieces = pieces_for(nu, c, 256);
+  std::vector<std::vector<int>>& pdeps = S.unit_deps;
+  if (pdeps.size() < static_cast<size_t>(pieces)) pdeps.resize(pieces);
+  std::vector<int>& dep_count = S.dep_count;
+  dep_count.assign(nu, 0);
+  c.pool->run(pieces, [&](int pi) {
+    std::vector<int>& out = pdeps[pi];
+    out.clear();
+    std::vector<int> mine;
+    for (size_t ui = piece_begin(nu, pieces, pi); ui < piece_begin(nu, pieces, pi + 1); ++ui) {
+      const int bi = P->units[ui];
+      BlockRec& b = P->blocks[bi];
+      const int p = b.plane, oc = 1 << sh[p];
+      mine.clear();
+      auto wait_on = [&](int o) {
+        if (o >= 0 && o < bi && is_b[o]) mine.push_back(o);
+      };
+      int har = b.have_ar, hbl = b.have_bl;
+      if (b.kind == AV1B_U_INTRA) {
+        if (har == 2) {
+          bool ok = true;
+          each_cell(p, b.x + b.w, b.x + 2 * b.w - 1, b.y - 1, b.y - 1,
+                    [&](int o) { if (o >= 0 && o >= bi) ok = false; });
+          har = b.y > 0 && ok;
+        }
+        if (hbl == 2) {
+          bool ok = true;
+          each_cell(p, b.x - 1, b.x - 1, b.y + b.h, b.y + 2 * b.h - 1,
+                    [&](int o) { if (o >= 0 && o >= bi) ok = false; });
+          hbl = b.x > 0 && ok;
+        }
+      } else {
+        har = hbl = 0;
+      }
+      b.have_ar = static_cast<unsigned char>(har);
+      b.have_bl = static_cast<unsigned char>(hbl);
+      if (b.kind == AV1B_U_INTRA || b.interintra) {
+        int left_y1 = b.y + b.h - 1, above_x1 = b.x + b.w - 1;
+        if (b.kind == AV1B_U_INTRA && !b.palette) {
+          if (b.mode >= 1 && b.mode <= 8) {
+            const int pangle = kAngle[b.mode] + 3 * b.angle_delta;
+            if (pangle < 90 && har) above_x1 = b.x + 2 * b.w - 1;
+            if (pangle > 180 && hbl) left_y1 = b.y + 2 * b.h - 1;
+          }
+        } else if (b.kind == AV1B_U_INTRA) {
+          above_x1 = b.x - 1;
+          left_y1 = b.y - 1;
+        }
+        if (left_y1 >= (b.y & ~(oc - 1))) each_cell(p, b.x - 1, b.x - 1, b.y, left_y1, wait_on);
+        if (above_x1 >= (b.x & ~(oc - 1))) each_cell(p, b.x, above_x1, b.y - 1, b.y - 1, wait_on);
+        if (above_x1 >= b.x || left_y1 >= b.y) each_cell(p, b.x - 1, b.x - 1, b.y - 1, b.y - 1, wait_on);
+      }
+      if (b.kind == AV1B_U_INTRABC) {
+        const int sx_ = p > 0 ? L.ss_x : 0, sy_ = p > 0 ? L.ss_y : 0;
+        const int sx = b.x + (b.mv[0][0] >> (3 + sx_));
+        const int sy = b.y + (b.mv[0][1] >> (3 + sy_));
+        const int x1 = std::min(sx + b.w, L.p[p].grid_w), y1 = std::min(sy + b.h, L.p[p].grid_h);
+        if (x1 > std::max(sx, 0) && y1 > std::max(sy, 0))
+          each_cell(p, std::max(sx, 0), x1 - 1, std::max(sy, 0), y1 - 1, wait_on);
+      }
+      if (b.kind == AV1B_U_INTRA && b.mode == 13 && !b.palette)
+        each_cell(0, b.x << L.ss_x, (b.x + b.w - 1) << L.ss_x, b.y << L.ss_y,
+                  (b.y + b.h - 1) << L.ss_y, wait_on);
+      for (size_t x = 1; x < mine.size(); ++x)  /* short lists: insertion sort */
+        for (size_t y = x; y > 0 && mine[y - 1] > mine[y]; --y) std::swap(mine[y - 1], mine[y]);
+      mine.erase(std::unique(mine.begin(), mine.end()), mine.end());
+      /* prediction and residual fuse when the transforms cover disjoint parts
+       * of the block (each sample then gets at most one residual) */
+      b.fuse_res = 0;
+      if (b.kind == AV1B_U_INTRA && b.w * b.h <= 4096) {
+        bool ok = true, grid4 = true;
+        for (int t = 0; t < b.tx_count && ok; ++t) {
+          const TxRec& x = P->txs[b.tx_first + t];
+          if (x.x < 0 || x.y < 0 || x.x + x.w > b.w || x.y + x.h > b.h) ok = false;
+          if ((x.x | x.y | x.w | x.h) & 3) grid4 = false;
+        }
+        if (ok && grid4) {
+          /* 4x4 cells of the block (at most 16 x 16) */
+          uint64_t cov[4] = {0, 0, 0, 0};
+          for (int t = 0; t < b.tx_count && ok; ++t) {
+            const TxRec& x = P->txs[b.tx_first + t];
+            for (int cy = x.y >> 2; cy < (x.y + x.h) >> 2 && ok; ++cy)
+              for (int cx = x.x >> 2; cx < (x.x + x.w) >> 2; ++cx) {
+                const int bit = cy * 16 + cx;
+                if (cov[bit >> 6] >> (bit & 63) & 1) {
+                  ok = false;
+                  break;
+                }
+                cov[bit >> 6] |= 1ull << (bit & 63);
+              }
+          }
+        } else if (ok) {
+          for (int t = 0; t < b.tx_count && ok; ++t) {
+            const TxRec& x = P->txs[b.tx_first + t];
+            for (int u = 0; u < t && ok; ++u) {
+              const TxRec& y = P->txs[b.tx_first + u];
+              if (x.x < y.x + y.w && y.x < x.x + x.w && x.y < y.y + y.h && y.y < x.y + x.h) ok = false;
+            }
+            if (t > 64) ok = false;
+          }
+        }
+        b.fuse_res = ok ? 1 : 0;
+      }
+      dep_count[ui] = static_cast<int>(mine.size());
+      out.insert(out.end(), mine.begin(), mine.end());
+    }
+  });
+  /* depths, in coding order (every dependency precedes its dependant) */
+  std::vector<int>& depth = S.depth;
+  depth.assign(nb, 0);
+  std::vector<size_t> first(nu + 1, 0);
+  for (size_t ui = 0; ui < nu; ++ui) first[ui + 1] = first[ui] + dep_count[ui];
+  if (first[nu] > static_cast<size_t>(INT32_MAX)) return fail(d, AV1B_ERR_SYNTAX, "frame too large");
+  P->deps.resize(first[nu]);
+  c.pool->run(pieces, [&](int pi) {
+    std::copy(pdeps[pi].begin(), pdeps[pi].end(),
+              P->deps.begin() + first[piece_begin(nu, pieces, pi)]);
+    for (size_t ui = piece_begin(nu, pieces, pi); ui < piece_begin(nu, pieces, pi + 1); ++ui) {
+      BlockRec& b = P->blocks[P->units[ui]];
+      b.dep_first = static_cast<int>(first[ui]);
+      b.dep_count = dep_count[ui];
+    }
+  });
+  int max_depth = 0;
+  const int* dl = P->deps.data();
+  for (size_t ui = 0; ui < nu; ++ui) {
+    int dd = 0;
+    for (size_t k = first[ui]; k < first[ui + 1]; ++k) dd = std::max(dd, depth[dl[k]]);
+    depth[P->units[ui]] = dd + 1;
+    max_depth = std::max(max_depth, dd + 1);
+  }
+  /* claim order: by depth, coding order within one */
+  std::vector<int> count(max_depth + 2, 0);
+  for (size_t ui = 0; ui < nu; ++ui) ++count[depth[P->units[ui]] + 1];
+  for (int k = 0; k <= max_depth; ++k) count[k + 1] += count[k];
+  std::vector<int>& sorted = S.sorted;
+  sorted.resize(nu);
+  for (size_t ui = 0; ui < nu; ++ui) sorted[count[depth[P->units[ui]]]++] = P->units[ui];
+  std::copy(sorted.begin(), sorted.end(), P->units.begin());
+  P->unit_depth = max_depth;
+  return AV1B_OK;
+}
+
 /* Validates a frame and builds its device records. The blocks, deblocking
  * edges and CDEF blocks are converted in pieces on the pool; each piece stops
  * at its first invalid record and the error of the earliest piece is the one
@@ -728,6 +965,7 @@ inline size_t piece_begin(size_t n, int pieces, int i) { return n * i / pieces; 
 int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Plan* P) {
   const Layout& L = c.L;
   const int bd = s.bit_depth;
+  int rc_units;
   P->blocks.resize(s.n_blocks);
   for (int i = 0; i < 7; ++i) {
     const int rw = s.reference_width[i] > 0 ? s.reference_width[i] : s.width;
@@ -815,52 +1053,7 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
       }
     });
   }
-  /* The claim order of the dependency-scheduled blocks. Coding order is a
-   * valid order but serializes the picture: the blocks in flight all sit in
-   * one superblock row, each waiting for its left neighbour. Ordering by the
-   * anti-diagonal of the superblock a block lies in (2 * row + column), coding
-   * order inside a superblock, keeps every dependency earlier in the order -
-   * left (t - 1), above (t - 2), above-right (t - 1, and only when it was
-   * decoded before the block), corner (t - 3), co-located luma (same
-   * superblock); below-left in another superblock is never decoded before -
-   * while the superblocks of a diagonal run together. The key has to use the
-   * stream's superblock size (64 or 128): it is read from the coding order,
-   * where 128x128 superblocks visit the 64x64 region (1, 0) before (0, 2). An
-   * intra block copy may read further right in the rows above (a larger key),
-   * so a frame with one keeps coding order. */
-  {
-    bool intrabc = false;
-    for (int bi : P->units)
-      if (P->blocks[bi].kind == AV1B_U_INTRABC) intrabc = true;
-    if (!intrabc && P->units.size() > 1) {
-      size_t first_row1 = SIZE_MAX, first_col2 = SIZE_MAX;
-      for (size_t bi = 0; bi < P->blocks.size(); ++bi) {
-        const BlockRec& b = P->blocks[bi];
-        if (b.plane != 0) continue;
-        if ((b.y >> 6) == 1 && first_row1 == SIZE_MAX) first_row1 = bi;
-        if ((b.y >> 6) == 0 && (b.x >> 6) >= 2 && first_col2 == SIZE_MAX) first_col2 = bi;
-        if (first_row1 != SIZE_MAX && first_col2 != SIZE_MAX) break;
-      }
-      const int sb_log2 = first_row1 < first_col2 ? 7 : 6;
-      const int cols = ((L.p[0].grid_w + kPadLuma) >> sb_log2) + 2;
-      const int rows = ((L.p[0].grid_h + kPadLuma) >> sb_log2) + 2;
-      const int nkeys = 2 * rows + cols + 2;
-      std::vector<int> key(P->units.size());
-      std::vector<int> count(nkeys + 1, 0);
-      for (size_t i = 0; i < P->units.size(); ++i) {
-        const BlockRec& b = P->blocks[P->units[i]];
-        const int sx = b.plane ? L.ss_x : 0, sy = b.plane ? L.ss_y : 0;
-        const int c = std::min((b.x << sx) >> sb_log2, cols - 1);
-        const int r = std::min((b.y << sy) >> sb_log2, rows - 1);
-        key[i] = 2 * r + c;
-        ++count[key[i] + 1];
-      }
-      for (int k = 0; k < nkeys; ++k) count[k + 1] += count[k];
-      std::vector<int> sorted(P->units.size());
-      for (size_t i = 0; i < P->units.size(); ++i) sorted[count[key[i]]++] = P->units[i];
-      P->units.swap(sorted);
-    }
-  }
+  if ((rc_units = plan_units(d, c, P))) return rc_units;
 
   /* the pools read past the caller's arrays as zeros, like the reference's
    * padded plan pools (engine.cpp:665-674) */
@@ -1056,10 +1249,10 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
 /* ---- the frame step ------------------------------------------------------------------------ */
 
 /* Reserves room for `v` in the staging arena; returns its offset. */
-template <class T>
-size_t stage_put(size_t* off, const std::vector<T>& v) {
+template <class V>
+size_t stage_put(size_t* off, const V& v) {
   const size_t o = *off;
-  *off = align_up(o + v.size() * sizeof(T), 256);
+  *off = align_up(o + v.size() * sizeof(typename V::value_type), 256);
   return o;
 }
 
@@ -1144,12 +1337,11 @@ struct av1b_plan {
   av1b::Layout L{};
   av1b::Plan P;                   /* host copy of the counts and constants */
   av1b::DevBuf arena, coef, residual;
-  av1b::HostBuf stage;            /* pinned staging of the records */
   /* ready: the uploads are done; done: the last frame that read this plan has
    * finished on the device (a plan is re-planned only after that) */
   cudaEvent_t ready = nullptr, done = nullptr;
   bool in_flight = false;
-  size_t o_blocks = 0, o_txs = 0, o_obmc = 0, o_warps = 0, o_pal = 0, o_units = 0;
+  size_t o_blocks = 0, o_txs = 0, o_obmc = 0, o_warps = 0, o_pal = 0, o_units = 0, o_deps = 0;
   size_t o_tiles = 0, o_itx = 0, o_dbv = 0, o_dbh = 0, o_cdef = 0, o_lr[3] = {0, 0, 0};
   size_t o_map = 0, o_cdef_search = 0;
   int slots_read[kSlots + 1];     /* the reference slots the frame reads, -1 ended */
@@ -1159,21 +1351,6 @@ struct av1b_plan {
 
 namespace av1b {
 namespace {
-
-/* Copies `bytes` from `src` to `dst` in pieces on the pool. */
-void pool_copy(const PlanCtx& c, void* dst, const void* src, size_t bytes) {
-  const size_t piece = 1 << 20;
-  const int n = static_cast<int>((bytes + piece - 1) / piece);
-  if (n <= 1) {
-    if (bytes) std::memcpy(dst, src, bytes);
-    return;
-  }
-  c.pool->run(n, [&](int i) {
-    const size_t o = static_cast<size_t>(i) * piece;
-    std::memcpy(static_cast<uint8_t*>(dst) + o, static_cast<const uint8_t*>(src) + o,
-                std::min(piece, bytes - o));
-  });
-}
 
 /* Plans `s` into `pl`: validation, records, and the upload of records and
  * coefficient pools into the plan's device memory, on the upload stream. It
@@ -1207,8 +1384,28 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
     pl->in_flight = false;
   }
   Plan& P = pl->P;
+  cudaStream_t st = d->upload;
+  /* the caller's coefficients and raw residuals go up first, while the
+   * records are built */
+  if ((rc = dev_ensure(d, pl->coef, (s.n_coefficients + 64) * sizeof(int))) ||
+      (rc = dev_ensure(d, pl->residual, (s.n_residual + 64) * sizeof(int))))
+    return rc;
+  if (s.n_coefficients)
+    CK(cudaMemcpyAsync(pl->coef.p, s.coefficients, s.n_coefficients * sizeof(int),
+                       cudaMemcpyHostToDevice, st), "coefficient upload");
+  if (s.n_residual)
+    CK(cudaMemcpyAsync(pl->residual.p, s.residual, s.n_residual * sizeof(int),
+                       cudaMemcpyHostToDevice, st), "residual upload");
   auto t0 = std::chrono::steady_clock::now();
-  if ((rc = build_plan(d, c, s, &P))) return rc;
+  try {
+    rc = build_plan(d, c, s, &P);
+  } catch (const std::bad_alloc&) {
+    rc = fail(d, AV1B_ERR_NOMEM, "host memory exhausted while planning");
+  }
+  if (rc) {
+    cudaStreamSynchronize(st);  /* nothing in flight reads the caller's arrays */
+    return rc;
+  }
   host_mark(d, kStPlanHost, t0);
   pl->L = c.L;
   pl->width = s.width;
@@ -1232,7 +1429,6 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
       if (used[i]) pl->slots_read[n++] = i;
     pl->slots_read[n] = -1;
   }
-  cudaStream_t st = d->upload;
   size_t off = 0;
   pl->o_blocks = stage_put(&off, P.blocks);
   pl->o_txs = stage_put(&off, P.txs);
@@ -1240,6 +1436,7 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
   pl->o_warps = stage_put(&off, P.warps);
   pl->o_pal = stage_put(&off, P.palette_colors);
   pl->o_units = stage_put(&off, P.units);
+  pl->o_deps = stage_put(&off, P.deps);
   pl->o_tiles = stage_put(&off, P.inter_tiles);
   pl->o_itx = stage_put(&off, P.itx_jobs);
   pl->o_dbv = stage_put(&off, P.deblock_v);
@@ -1250,47 +1447,58 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
   pl->o_map = off;
   off = align_up(off + s.n_palette_map + 64, 256);
   const size_t total = off;
-  if ((rc = host_ensure(d, pl->stage, total)) || (rc = dev_ensure(d, pl->arena, total))) return rc;
-  t0 = std::chrono::steady_clock::now();
-  uint8_t* hs = static_cast<uint8_t*>(pl->stage.p);
-  auto put = [&](size_t o, const void* src, size_t bytes) { pool_copy(c, hs + o, src, bytes); };
-  put(pl->o_blocks, P.blocks.data(), P.blocks.size() * sizeof(BlockRec));
-  put(pl->o_txs, P.txs.data(), P.txs.size() * sizeof(TxRec));
-  put(pl->o_obmc, P.obmc.data(), P.obmc.size() * sizeof(ObmcRec));
-  put(pl->o_warps, P.warps.data(), P.warps.size() * sizeof(WarpRec));
-  put(pl->o_pal, P.palette_colors.data(), P.palette_colors.size() * sizeof(int));
-  put(pl->o_units, P.units.data(), P.units.size() * sizeof(int));
-  put(pl->o_tiles, P.inter_tiles.data(), P.inter_tiles.size() * sizeof(int2));
-  put(pl->o_itx, P.itx_jobs.data(), P.itx_jobs.size() * sizeof(int2));
-  put(pl->o_dbv, P.deblock_v.data(), P.deblock_v.size() * sizeof(DeblockRec));
-  put(pl->o_dbh, P.deblock_h.data(), P.deblock_h.size() * sizeof(DeblockRec));
-  put(pl->o_cdef, P.cdef.data(), P.cdef.size() * sizeof(CdefRec));
-  put(pl->o_cdef_search, P.cdef_search.data(), P.cdef_search.size() * sizeof(unsigned));
-  for (int p = 0; p < 3; ++p)
-    put(pl->o_lr[p], P.lr_units[p].data(), P.lr_units[p].size() * sizeof(LrUnitRec));
-  put(pl->o_map, s.palette_map, s.n_palette_map);
-  std::memset(hs + pl->o_map + s.n_palette_map, 0, 64);
-  host_mark(d, kStStageHost, t0);
-  CK(cudaMemcpyAsync(pl->arena.p, hs, total, cudaMemcpyHostToDevice, st), "arena upload");
-
-  /* coefficient and residual pools, zero past the caller's arrays */
-  if ((rc = dev_ensure(d, pl->coef, P.coef_pool * sizeof(int))) ||
-      (rc = dev_ensure(d, pl->residual, P.residual_pool * sizeof(int))))
+  if ((rc = dev_ensure(d, pl->arena, total))) {
+    cudaStreamSynchronize(st);
     return rc;
-  if (!P.itx_jobs.empty() || !P.units.empty()) {
+  }
+  /* the record lists upload from where the planner wrote them (page-locked) */
+  t0 = std::chrono::steady_clock::now();
+  uint8_t* ar = static_cast<uint8_t*>(pl->arena.p);
+  auto put = [&](size_t o, const auto& v) -> cudaError_t {
+    const size_t bytes = v.size() * sizeof(v[0]);
+    return bytes ? cudaMemcpyAsync(ar + o, v.data(), bytes, cudaMemcpyHostToDevice, st) : cudaSuccess;
+  };
+  CK(put(pl->o_blocks, P.blocks), "record upload");
+  CK(put(pl->o_txs, P.txs), "record upload");
+  CK(put(pl->o_obmc, P.obmc), "record upload");
+  CK(put(pl->o_warps, P.warps), "record upload");
+  CK(put(pl->o_pal, P.palette_colors), "record upload");
+  CK(put(pl->o_units, P.units), "record upload");
+  CK(put(pl->o_deps, P.deps), "record upload");
+  CK(put(pl->o_tiles, P.inter_tiles), "record upload");
+  CK(put(pl->o_itx, P.itx_jobs), "record upload");
+  CK(put(pl->o_dbv, P.deblock_v), "record upload");
+  CK(put(pl->o_dbh, P.deblock_h), "record upload");
+  CK(put(pl->o_cdef, P.cdef), "record upload");
+  CK(put(pl->o_cdef_search, P.cdef_search), "record upload");
+  for (int p = 0; p < 3; ++p) CK(put(pl->o_lr[p], P.lr_units[p]), "record upload");
+  if (s.n_palette_map)
+    CK(cudaMemcpyAsync(ar + pl->o_map, s.palette_map, s.n_palette_map, cudaMemcpyHostToDevice, st),
+       "palette map upload");
+  CK(cudaMemsetAsync(ar + pl->o_map + s.n_palette_map, 0, 64, st), "palette map pad");
+  host_mark(d, kStStageHost, t0);
+
+  /* the pools read past the caller's arrays as zeros; a pool longer than the
+   * early copy's buffer is copied again into a larger one */
+  const size_t coef_cap = pl->coef.cap / sizeof(int), res_cap = pl->residual.cap / sizeof(int);
+  if (P.coef_pool > coef_cap || P.residual_pool > res_cap) {
+    CK(cudaStreamSynchronize(st), "upload sync");
+    if ((rc = dev_ensure(d, pl->coef, P.coef_pool * sizeof(int))) ||
+        (rc = dev_ensure(d, pl->residual, P.residual_pool * sizeof(int))))
+      return rc;
     if (s.n_coefficients)
       CK(cudaMemcpyAsync(pl->coef.p, s.coefficients, s.n_coefficients * sizeof(int),
                          cudaMemcpyHostToDevice, st), "coefficient upload");
-    if (P.coef_pool > s.n_coefficients)
-      CK(cudaMemsetAsync(static_cast<int*>(pl->coef.p) + s.n_coefficients, 0,
-                         (P.coef_pool - s.n_coefficients) * sizeof(int), st), "coefficient pad");
     if (s.n_residual)
       CK(cudaMemcpyAsync(pl->residual.p, s.residual, s.n_residual * sizeof(int),
                          cudaMemcpyHostToDevice, st), "residual upload");
-    if (P.residual_pool > s.n_residual)
-      CK(cudaMemsetAsync(static_cast<int*>(pl->residual.p) + s.n_residual, 0,
-                         (P.residual_pool - s.n_residual) * sizeof(int), st), "residual pad");
   }
+  if (P.coef_pool > s.n_coefficients)
+    CK(cudaMemsetAsync(static_cast<int*>(pl->coef.p) + s.n_coefficients, 0,
+                       (P.coef_pool - s.n_coefficients) * sizeof(int), st), "coefficient pad");
+  if (P.residual_pool > s.n_residual)
+    CK(cudaMemsetAsync(static_cast<int*>(pl->residual.p) + s.n_residual, 0,
+                       (P.residual_pool - s.n_residual) * sizeof(int), st), "residual pad");
   CK(cudaEventRecord(pl->ready, st), "event");
   t0 = std::chrono::steady_clock::now();
   CK(cudaEventSynchronize(pl->ready), "upload wait");
@@ -1373,22 +1581,9 @@ int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, cons
   }
   uint8_t* ar = static_cast<uint8_t*>(pl->arena.p);
 
-  /* owner grids, done flags, queue and status */
+  /* done flags, queue and status */
   FrameArgs a{};
   a.L = L;
-  for (int p = 0; p < 3; ++p) {
-    /* square cells: 4 luma samples; 2 for a chroma plane whose axis is
-     * subsampled - the reference keys plane 1 on ss_x and plane 2 on ss_y
-     * (engine.cpp:737-741), which this mirrors */
-    const int shift = p == 0 ? 2 : (p == 1 ? (L.ss_x ? 1 : 2) : (L.ss_y ? 1 : 2));
-    a.cell_shift[p] = shift;
-    a.cell_w[p] = (L.p[p].grid_w + (1 << shift) - 1) >> shift;
-    a.cell_h[p] = (L.p[p].grid_h + (1 << shift) - 1) >> shift;
-    const size_t cells = static_cast<size_t>(a.cell_w[p]) * a.cell_h[p];
-    if ((rc = dev_ensure(d, d->owner[p], cells * sizeof(int)))) return rc;
-    a.owner[p] = static_cast<int*>(d->owner[p].p);
-    if (!P.units.empty()) CK(cudaMemsetAsync(a.owner[p], 0xff, cells * sizeof(int), st), "owner reset");
-  }
   const size_t done_bytes = static_cast<size_t>(pl->n_blocks) * sizeof(unsigned) + 256;
   if (d->done.cap < done_bytes) {
     if ((rc = dev_ensure(d, d->done, done_bytes))) return rc;
@@ -1422,6 +1617,7 @@ int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, cons
   a.epoch = d->epoch;
   a.units = reinterpret_cast<const int*>(ar + pl->o_units);
   a.n_units = static_cast<int>(P.units.size());
+  a.deps = reinterpret_cast<const int*>(ar + pl->o_deps);
   a.queue = static_cast<unsigned*>(d->status_q.p);
   a.status = reinterpret_cast<int*>(static_cast<uint8_t*>(d->status_q.p) + 64);
   a.inter_tiles = reinterpret_cast<const int2*>(ar + pl->o_tiles);
@@ -1454,9 +1650,8 @@ int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, cons
     ++launches;
   }
   CK(cudaEventRecord(ev[0], st), "event");
-  for (int stage = 0; stage < 4; ++stage) {
-    const bool any = stage == 0 ? a.n_blocks > 0
-                                : (stage == 1 ? a.n_inter_tiles > 0 : (stage == 2 ? a.n_itx > 0 : a.n_units > 0));
+  for (int stage = 1; stage < 4; ++stage) {
+    const bool any = stage == 1 ? a.n_inter_tiles > 0 : (stage == 2 ? a.n_itx > 0 : a.n_units > 0);
     if (!any) continue;
     CK(timed(d, kStOwner + stage, [&] { return launch_recon_stage(stage, a, d->n_sm, st); }),
        "reconstruction launch");
@@ -1585,8 +1780,6 @@ void release_plan(av1b_decoder* d, av1b_plan* pl) {
   dev_release(d, pl->arena);
   dev_release(d, pl->coef);
   dev_release(d, pl->residual);
-  if (pl->stage.p) cudaFreeHost(pl->stage.p);
-  pl->stage.p = nullptr;
   if (pl->ready) cudaEventDestroy(pl->ready);
   if (pl->done) cudaEventDestroy(pl->done);
   delete pl;
@@ -1719,8 +1912,8 @@ int av1b_decoder_destroy(av1b_decoder* d) {
   if (d->ev_join) cudaEventDestroy(d->ev_join);
   if (d->status_host) cudaFreeHost(d->status_host);
   DevBuf* bufs[] = {&d->cur, &d->snap, &d->lr_pre, &d->lr_pre_up, &d->lr_cdef, &d->disp,
-                    &d->slot_ptr_dev, &d->arena, &d->coef, &d->residual, &d->owner[0],
-                    &d->owner[1], &d->owner[2], &d->done, &d->status_q, &d->nv12, &d->rgb,
+                    &d->slot_ptr_dev, &d->arena, &d->coef, &d->residual, &d->done,
+                    &d->status_q, &d->nv12, &d->rgb,
                     &d->grain_state, &d->orbit, &d->pos, &d->cdef_search, &d->pre_res};
   for (DevBuf* b : bufs) dev_release(d, *b);
   for (int i = 0; i < kSlots; ++i) dev_release(d, d->slot_buf[i]);

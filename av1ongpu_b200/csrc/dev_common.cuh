@@ -111,10 +111,13 @@ struct BlockRec {
   unsigned char w0, w1, mask_sign, ii_mode;
   unsigned char interintra, ii_wedge, wedge_dir, wedge_flip;
   signed char wedge_xoff, wedge_yoff, warp0, warp1;
-  unsigned char mask_warp0, mask_warp1, phase_b, pad1;   /* phase_b: dependency scheduled */
+  unsigned char mask_warp0, mask_warp1, phase_b;   /* phase_b: dependency scheduled */
+  unsigned char fuse_res;     /* phase B: the transforms tile disjoint parts of the
+                                 block, so prediction and residual add fuse */
   int warp_idx[2];            /* into the frame's warp model table, -1 none */
   int obmc_first, obmc_count;
   int palette_color_idx;      /* into the palette colour table */
+  int dep_first, dep_count;   /* phase B: the blocks it waits for (frame's dep list) */
 };
 
 /* One transform of a block: position relative to the block. 16 bytes. */

@@ -210,14 +210,22 @@ AV1B_DEV int dir_sample(const int* above, const int* left, int w, int h, int pan
  * 3 * AV1B_EDGE_LEN ints. */
 AV1B_DEV void intra_predict(const IntraJob& j, px_t* dst, int stride, const px_t* luma,
                             int luma_stride, const uint8_t* palette_map,
-                            const int* palette_colors, int* scratch, int lane) {
+                            const int* palette_colors, int* scratch, int lane,
+                            const int* res = nullptr) {
   const int w = j.w, h = j.h, n = w * h;
   const int lw = ilog2(w);
+  /* the reconstructed sample: the prediction plus, when the caller fused the
+   * residual in (`res`, the block's residual, w x h row-major), that residual,
+   * clipped - what adding the transforms afterwards gives */
+  auto put = [&](int i, int jj, int v) {
+    if (res) v = clampi(v + res[i * w + jj], 0, j.maxv);
+    dst[i * stride + jj] = (px_t)v;
+  };
   if (j.palette) {
     const uint8_t* map = palette_map + j.palette_off;
     for (int k = lane; k < n; k += 32) {
       const int i = k >> lw, jj = k & (w - 1);
-      dst[i * stride + jj] = (px_t)palette_colors[map[i * j.palette_stride + jj]];
+      put(i, jj, palette_colors[map[i * j.palette_stride + jj]]);
     }
     return;
   }
@@ -250,14 +258,16 @@ AV1B_DEV void intra_predict(const IntraJob& j, px_t* dst, int stride, const px_t
       for (int a = 0; a <= sy; ++a)
         for (int b = 0; b <= sx; ++b) t += ldpx(luma + (ly + a) * luma_stride + lx + b);
       const int v = t << (3 - sx - sy);
-      dst[i * stride + jj] = (px_t)clampi(dc + rnd2s(j.cfl_alpha * (v - avg), 6), 0, j.maxv);
+      put(i, jj, clampi(dc + rnd2s(j.cfl_alpha * (v - avg), 6), 0, j.maxv));
     }
     return;
   }
 
   if (j.filter_intra && w >= 4 && h >= 2) {
     /* recursive filter: 4x2 cells along anti-diagonals; a cell reads the row
-     * above it (cells up-left and up) and the column left of it */
+     * above it (cells up-left and up) and the column left of it - the
+     * predictions of this block, so the residual is never fused here (the
+     * caller adds the transforms afterwards) */
     const int cw = w >> 2, ch = h >> 1;
     const signed char* taps = kFilterIntraTaps + j.fi_mode * 56;
     for (int d = 0; d < cw + ch - 1; ++d) {
@@ -321,7 +331,7 @@ AV1B_DEV void intra_predict(const IntraJob& j, px_t* dst, int stride, const px_t
     for (int k = lane; k < n; k += 32) {
       const int i = k >> lw, jj = k & (w - 1);
       const int v = dir_sample(above, left, w, h, pangle, dx, dy, ua, ul, i, jj);
-      dst[i * stride + jj] = (px_t)clampi(v, 0, j.maxv);
+      put(i, jj, clampi(v, 0, j.maxv));
     }
     return;
   }
@@ -340,7 +350,7 @@ AV1B_DEV void intra_predict(const IntraJob& j, px_t* dst, int stride, const px_t
         const int wx = sm_weight(w, jj);
         pred = rnd2(wx * left[i] + (256 - wx) * above[w - 1], 8);
       }
-      dst[i * stride + jj] = (px_t)clampi(pred, 0, j.maxv);
+      put(i, jj, clampi(pred, 0, j.maxv));
     }
     return;
   }
@@ -351,14 +361,14 @@ AV1B_DEV void intra_predict(const IntraJob& j, px_t* dst, int stride, const px_t
       const int base = above[jj] + left[i] - tl;
       const int pl = absi(base - left[i]), pt = absi(base - above[jj]), ptl = absi(base - tl);
       const int v = (pl <= pt && pl <= ptl) ? left[i] : (pt <= ptl ? above[jj] : tl);
-      dst[i * stride + jj] = (px_t)clampi(v, 0, j.maxv);
+      put(i, jj, clampi(v, 0, j.maxv));
     }
     return;
   }
   const int dc = clampi(intra_dc(j, above, left, lane), 0, j.maxv);
   for (int k = lane; k < n; k += 32) {
     const int i = k >> lw, jj = k & (w - 1);
-    dst[i * stride + jj] = (px_t)dc;
+    put(i, jj, dc);
   }
 }
 

@@ -3,20 +3,22 @@
  *
  * Reconstruction runs in two phases. Phase A is everything that reads only
  * reference pictures: the inter prediction of every inter block (one warp per
- * 16x8 tile) and then its residual (one warp per transform). Phase B is the
- * dependency-scheduled rest: intra blocks, inter-intra blocks and intra block
- * copies, in coding order, by a persistent kernel whose warps claim blocks
- * from a device queue and wait on the blocks that own the samples they read.
- * The dependency tracking is the reference planner's owner grid and edge scans
- * (engine.cpp:719-924), done here on the device: the host never computes a
- * wave and launches nothing per wave.
+ * 16x8 tile), then every inverse transform (one warp per transform) - added
+ * to the picture for inter blocks, left in a buffer for the rest. Phase B is
+ * the dependency-scheduled rest: intra blocks, inter-intra blocks and intra
+ * block copies, by a persistent kernel whose warps claim blocks from a device
+ * queue, wait for the blocks whose samples they read and add the residual
+ * computed ahead. What each block waits for comes from the planner, which
+ * resolves the reference's owner grids and edge scans (engine.cpp:719-924)
+ * into a short list per block and orders the claims by dependency depth: the
+ * host launches nothing per wave.
  *
- * Waiting is safe without a cooperative launch: blocks are claimed in index
- * order and a block only ever waits on lower indices, each of which was
- * claimed by a warp that is already running; the lowest unfinished block
- * therefore always has everything it needs. Every wait is bounded (one second
- * of globaltimer); on expiry the kernel records AV1B_STATUS_TIMEOUT in the
- * status word and carries on, and the host fails the frame.
+ * Waiting is safe without a cooperative launch: a block only ever waits on
+ * blocks claimed before it, each by a warp that is already running (or has
+ * finished it), so the first unfinished block in claim order always has
+ * everything it needs. Every wait is bounded (one second of globaltimer); on
+ * expiry the kernel records AV1B_STATUS_TIMEOUT in the status word and
+ * carries on, and the host fails the frame.
  */
 #include <cuda_runtime.h>
 
@@ -47,13 +49,6 @@ __device__ __forceinline__ unsigned long long global_ns() {
 __device__ __forceinline__ const px_t* ref_plane(const FrameArgs& a, int slot, int plane) {
   const px_t* base = slot >= 0 ? a.slot_ptr[slot] : a.cur;
   return base + a.L.p[plane].off;
-}
-
-/* Owner of the 4x4 (luma) / 2x2 (subsampled chroma) cell holding (x, y). */
-__device__ __forceinline__ int owner_at(const FrameArgs& a, int p, int x, int y) {
-  if (x < 0 || y < 0 || x >= a.L.p[p].grid_w || y >= a.L.p[p].grid_h) return -1;
-  const int sh = a.cell_shift[p];
-  return __ldcg(a.owner[p] + (y >> sh) * a.cell_w[p] + (x >> sh));
 }
 
 /* Builds the resolved inter job of a block. */
@@ -128,24 +123,6 @@ __device__ void make_inter_job(const FrameArgs& a, const BlockRec& b, InterJob* 
 }
 
 /* ---- phase A ------------------------------------------------------------------------ */
-
-/* Owner grid and done flags: one warp per block. */
-__global__ void k_owner(const __grid_constant__ FrameArgs a) {
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (warp >= a.n_blocks) return;
-  const BlockRec b = a.blocks[warp];
-  const int p = b.plane;
-  const int sh = a.cell_shift[p], oc = 1 << sh;
-  const int cx0 = maxi(b.x, 0) >> sh, cy0 = maxi(b.y, 0) >> sh;
-  const int cx1 = mini((b.x + b.w + oc - 1) >> sh, a.cell_w[p]);
-  const int cy1 = mini((b.y + b.h + oc - 1) >> sh, a.cell_h[p]);
-  const int cw = cx1 - cx0;
-  if (cw > 0)
-    for (int k = lane; k < cw * (cy1 - cy0); k += 32)
-      a.owner[p][(cy0 + k / cw) * a.cell_w[p] + cx0 + k % cw] = warp;
-  if (lane == 0 && !b.phase_b) a.done[warp] = a.epoch;
-}
 
 /* Inter prediction of phase A blocks: one warp per 16x8 tile. Translation
  * predictions (and OBMC strips) go through mc_rect, warped ones per sample;
@@ -323,40 +300,12 @@ cudaError_t launch_selftest_wait(const unsigned* flag, int* status, unsigned lon
   return cudaGetLastError();
 }
 
-/* True when every owner of the cells of [x0, x1] x [y0, y1] precedes `bi` in
- * coding order (or lies outside the grid): the reference's already_decoded
- * (engine.cpp:784-793). Warp-collective. */
-__device__ bool decoded_before(const FrameArgs& a, int p, int x0, int x1, int y0, int y1, int bi,
-                               int lane) {
-  const int oc = 1 << a.cell_shift[p];
-  const int xs = x0 & ~(oc - 1), ys = y0 & ~(oc - 1);
-  const int nx = x1 >= xs ? (x1 - xs) / oc + 1 : 0, ny = y1 >= ys ? (y1 - ys) / oc + 1 : 0;
-  bool ok = true;
-  for (int k = lane; k < nx * ny; k += 32) {
-    const int o = owner_at(a, p, xs + (k % nx) * oc, ys + (k / nx) * oc);
-    if (o >= 0 && o >= bi) ok = false;
-  }
-  return __all_sync(0xffffffffu, ok);
-}
-
-/* Waits for the owners of the cells of [x0, x1] x [y0, y1] of plane p that
- * precede `bi` in coding order. The claim order (see the planner) puts every
- * such owner before this block, so each one has been claimed by a running
- * warp. Warp-collective. */
-__device__ void wait_rect(const FrameArgs& a, int p, int x0, int x1, int y0, int y1, int bi,
-                          int lane) {
-  const int oc = 1 << a.cell_shift[p];
-  const int xs = x0 & ~(oc - 1), ys = y0 & ~(oc - 1);
-  const int nx = x1 >= xs ? (x1 - xs) / oc + 1 : 0, ny = y1 >= ys ? (y1 - ys) / oc + 1 : 0;
-  for (int k = lane; k < nx * ny; k += 32) {
-    const int o = owner_at(a, p, xs + (k % nx) * oc, ys + (k / nx) * oc);
-    if (o >= 0 && o < bi) wait_block(a, o);
-  }
-  __syncwarp();
-}
-
-/* The persistent dependency-scheduled kernel. Shared memory per warp: three
- * edge buffers and a 64x64 transform scratch. */
+/* The persistent dependency-scheduled kernel: each warp claims blocks in the
+ * planner's order (by dependency depth), waits for the blocks its list names
+ * and reconstructs. Everything that does not depend on other blocks - the
+ * block record, its dependency list, its residual - is loaded before the
+ * wait. Shared memory per warp: three edge buffers and a 64x64 scratch (the
+ * block's residual image, or the transform scratch). */
 __global__ void __launch_bounds__(128) k_units(const __grid_constant__ FrameArgs a) {
   extern __shared__ int smem[];
   const int wib = threadIdx.x >> 5;
@@ -372,52 +321,26 @@ __global__ void __launch_bounds__(128) k_units(const __grid_constant__ FrameArgs
     const BlockRec b = a.blocks[bi];
     const int p = b.plane;
     const PlaneGeom& g = a.L.p[p];
+    const bool fused = b.kind == AV1B_U_INTRA && b.fuse_res &&
+                       !(b.fi_mode >= 0 && b.w >= 4 && b.h >= 2);
 
-    /* availability of the above-right / below-left extensions */
-    int have_ar = b.have_ar, have_bl = b.have_bl;
-    if (b.kind == AV1B_U_INTRA) {
-      if (have_ar == 2)
-        have_ar = b.y > 0 && decoded_before(a, p, b.x + b.w, b.x + 2 * b.w - 1, b.y - 1, b.y - 1,
-                                            bi, lane);
-      if (have_bl == 2)
-        have_bl = b.x > 0 && decoded_before(a, p, b.x - 1, b.x - 1, b.y + b.h, b.y + 2 * b.h - 1,
-                                            bi, lane);
-    } else {
-      have_ar = have_bl = 0;
-    }
-
-    /* dependencies: the edge samples (intra, inter-intra), the source
-     * rectangle (intra block copy) and the co-located luma (CFL) */
-    if (b.kind == AV1B_U_INTRA || b.interintra) {
-      int left_y1 = b.y + b.h - 1, above_x1 = b.x + b.w - 1;
-      if (b.kind == AV1B_U_INTRA && !b.palette) {
-        if (b.mode >= 1 && b.mode <= 8) {
-          const int pangle = kModeAngle[b.mode] + 3 * b.angle_delta;
-          if (pangle < 90 && have_ar) above_x1 = b.x + 2 * b.w - 1;
-          if (pangle > 180 && have_bl) left_y1 = b.y + 2 * b.h - 1;
+    /* the residual image, before the wait */
+    if (fused) {
+      const int n = b.w * b.h;
+      for (int k = lane; k < n; k += 32) tmp[k] = 0;
+      __syncwarp();
+      for (int t = 0; t < b.tx_count; ++t) {
+        const TxRec tx = a.txs[b.tx_first + t];
+        const int* src = b.residual_provided ? a.residual + tx.coef_off : a.pre_res + tx.pre_off;
+        for (int k = lane; k < tx.w * tx.h; k += 32) {
+          const int yy = k / tx.w, xx = k - yy * tx.w;
+          tmp[(tx.y + yy) * b.w + tx.x + xx] = src[k];
         }
-      } else if (b.kind == AV1B_U_INTRA) {
-        above_x1 = b.x - 1;
-        left_y1 = b.y - 1;
       }
-      const int oc = 1 << a.cell_shift[p];
-      if (left_y1 >= (b.y & ~(oc - 1))) wait_rect(a, p, b.x - 1, b.x - 1, b.y, left_y1, bi, lane);
-      if (above_x1 >= (b.x & ~(oc - 1))) wait_rect(a, p, b.x, above_x1, b.y - 1, b.y - 1, bi, lane);
-      if (above_x1 >= b.x || left_y1 >= b.y)
-        wait_rect(a, p, b.x - 1, b.x - 1, b.y - 1, b.y - 1, bi, lane);
     }
-    if (b.kind == AV1B_U_INTRABC) {
-      const int sx_ = p > 0 ? a.L.ss_x : 0, sy_ = p > 0 ? a.L.ss_y : 0;
-      const int sx = b.x + (b.mv[0][0] >> (3 + sx_));
-      const int sy = b.y + (b.mv[0][1] >> (3 + sy_));
-      const int x1 = mini(sx + b.w, g.grid_w), y1 = mini(sy + b.h, g.grid_h);
-      if (x1 > maxi(sx, 0) && y1 > maxi(sy, 0))
-        wait_rect(a, p, maxi(sx, 0), x1 - 1, maxi(sy, 0), y1 - 1, bi, lane);
-    }
-    if (b.kind == AV1B_U_INTRA && b.mode == 13 && !b.palette) {
-      wait_rect(a, 0, b.x << a.L.ss_x, ((b.x + b.w - 1) << a.L.ss_x), b.y << a.L.ss_y,
-                ((b.y + b.h - 1) << a.L.ss_y), bi, lane);
-    }
+
+    /* the blocks this one reads from */
+    for (int k = lane; k < b.dep_count; k += 32) wait_block(a, a.deps[b.dep_first + k]);
     __threadfence();
     __syncwarp();
 
@@ -434,8 +357,8 @@ __global__ void __launch_bounds__(128) k_units(const __grid_constant__ FrameArgs
       j.maxv = a.maxv;
       j.have_left = b.have_left;
       j.have_above = b.have_above;
-      j.have_ar = have_ar;
-      j.have_bl = have_bl;
+      j.have_ar = b.have_ar;
+      j.have_bl = b.have_bl;
       j.filter_type = b.filter_type;
       j.filter_intra = b.fi_mode >= 0;
       j.fi_mode = b.fi_mode >= 0 ? b.fi_mode : 0;
@@ -448,7 +371,8 @@ __global__ void __launch_bounds__(128) k_units(const __grid_constant__ FrameArgs
       j.palette_off = b.palette_off;
       j.palette_stride = b.palette_stride;
       intra_predict(j, dst, g.stride, a.cur + a.L.p[0].off, a.L.p[0].stride, a.palette_map,
-                    a.palette_colors + 8 * b.palette_color_idx, edges, lane);
+                    a.palette_colors + 8 * b.palette_color_idx, edges, lane,
+                    fused ? tmp : nullptr);
     } else {
       InterJob j;
       make_inter_job(a, b, &j);
@@ -462,7 +386,8 @@ __global__ void __launch_bounds__(128) k_units(const __grid_constant__ FrameArgs
       }
     }
     __syncwarp();
-    for (int t = 0; t < b.tx_count; ++t) apply_tx<true>(a, b, a.txs[b.tx_first + t], tmp, lane);
+    if (!fused)
+      for (int t = 0; t < b.tx_count; ++t) apply_tx<true>(a, b, a.txs[b.tx_first + t], tmp, lane);
 
     /* publish */
     __threadfence();
@@ -1131,9 +1056,6 @@ static inline unsigned cdiv(long long a, long long b) { return (unsigned)((a + b
 
 cudaError_t launch_recon_stage(int stage, const FrameArgs& a, int n_sm, cudaStream_t s) {
   switch (stage) {
-    case 0:
-      if (a.n_blocks > 0) k_owner<<<cdiv((long long)a.n_blocks * 32, 256), 256, 0, s>>>(a);
-      break;
     case 1:
       if (a.n_inter_tiles > 0)
         k_inter<<<cdiv(a.n_inter_tiles, 4), 128, 0, s>>>(a);

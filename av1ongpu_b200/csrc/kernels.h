@@ -28,11 +28,10 @@ struct FrameArgs {
   const int* residual;
   const uint8_t* palette_map;
   const int* palette_colors;    /* 8 per palette block */
-  int* owner[3];
-  int cell_w[3], cell_h[3], cell_shift[3];
-  unsigned* done;
+  unsigned* done;               /* per block: == epoch once reconstructed (phase B) */
   unsigned epoch;
-  const int* units;             /* phase B block indices, coding order */
+  const int* units;             /* phase B block indices, claim order */
+  const int* deps;              /* the phase B blocks each phase B block waits for */
   int n_units;
   unsigned* queue;
   const int2* inter_tiles;      /* phase A: (block, x0 | y0 << 16) */
@@ -74,8 +73,9 @@ struct RgbArgs {
 cudaError_t set_kernel_attributes();
 cudaError_t launch_selftest_wait(const unsigned* flag, int* status, unsigned long long limit_ns,
                                  cudaStream_t s);
-/* stage 0: owner grid and done flags; 1: phase A prediction; 2: phase A
- * residual; 3: the dependency-scheduled phase B. */
+/* stage 1: phase A prediction; 2: the inverse transforms (phase A residual
+ * added, phase B residual computed ahead); 3: the dependency-scheduled
+ * phase B. */
 cudaError_t launch_recon_stage(int stage, const FrameArgs& a, int n_sm, cudaStream_t s);
 cudaError_t launch_deblock(px_t* pic, const DeblockRec* recs, int n, int sharpness, int bd,
                            int maxv, cudaStream_t s);
