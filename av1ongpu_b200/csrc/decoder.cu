@@ -28,6 +28,7 @@
 #include <cstdio>
 #include <cstring>
 #include <chrono>
+#include <condition_variable>
 #include <mutex>
 #include <thread>
 #include <string>
@@ -62,6 +63,7 @@ using namespace av1b;
 namespace av1b {
 namespace {
 struct PlanScratch;
+struct PlanLists;
 }
 }  // namespace av1b
 
@@ -71,14 +73,22 @@ struct av1b_decoder {
   int n_sm = 148;
   size_t budget = 0, allocated = 0;
   std::mutex mu;                 /* one decode, output or slot call at a time */
-  /* Planning runs outside `mu` (a pipeline plans frame N+1 on its own thread
-   * while frame N runs): plan_mu serializes planners, slot_mu guards the slot
+  /* Planning runs outside `mu` (a pipeline plans frames N+1, N+2 on their
+   * own threads while frame N runs), on one of a few planners - each a host
+   * thread pool, scratch, record lists and an upload stream - taken one
+   * plan_frame at a time (planner_mu / planner_cv). slot_mu guards the slot
    * table planners read, err_mu the error text, alloc_mu the HBM account.
-   * Lock order: mu, plan_mu, slot_mu / alloc_mu / err_mu. */
-  std::mutex plan_mu, slot_mu, err_mu, alloc_mu;
-  av1b::WorkPool* pool = nullptr;
-  av1b::PlanScratch* scratch = nullptr;
-  cudaStream_t upload = nullptr;  /* plan uploads, overlapping the frame in flight */
+   * Lock order: mu, a planner, slot_mu / alloc_mu / err_mu. */
+  std::mutex planner_mu, slot_mu, err_mu, alloc_mu, prof_mu;
+  std::condition_variable planner_cv;
+  struct Planner {
+    av1b::WorkPool* pool = nullptr;
+    av1b::PlanScratch* scratch = nullptr;
+    av1b::PlanLists* lists = nullptr;  /* the record lists (page-locked) */
+    cudaStream_t upload = nullptr;     /* its uploads, overlapping frames in flight */
+    bool busy = false;
+  };
+  std::vector<Planner> planners;
   /* freed plans kept with their buffers for the next av1b_plan_frame */
   std::mutex plan_pool_mu;
   std::vector<struct av1b_plan*> plan_pool;
@@ -117,6 +127,7 @@ struct av1b_decoder {
    * film grain templates), joined before its consumer */
   cudaStream_t aux = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaEvent_t ev_block = nullptr;  /* blocking-sync event: host waits on the stream */
   int* status_host = nullptr;          /* pinned */
   void* slot_ptr_host[32] = {nullptr};
   struct av1b_plan* own_plan = nullptr;
@@ -149,6 +160,13 @@ int cuda_fail(av1b_decoder* d, cudaError_t e, const char* what) {
 void clear_err(av1b_decoder* d) {
   std::lock_guard<std::mutex> lk(d->err_mu);
   d->err.clear();
+}
+
+/* Waits for the decoder's stream without spinning a core (the planner pool
+ * and a planning thread share the host). Called with the decoder lock. */
+cudaError_t wait_stream(av1b_decoder* d) {
+  const cudaError_t e = cudaEventRecord(d->ev_block, d->stream);
+  return e != cudaSuccess ? e : cudaEventSynchronize(d->ev_block);
 }
 
 #define CK(call, what)                                     \
@@ -300,7 +318,13 @@ struct PinnedAlloc {
 template <class T>
 using pvec = std::vector<T, PinnedAlloc<T>>;
 
-struct Plan {
+/* The record lists a plan builds, in page-locked host memory so they upload
+ * from where the planner wrote them. One set serves every plan of a decoder:
+ * planning is serialized and a plan's uploads finish before the next starts,
+ * so the lists are free again once plan_frame returns (and their capacity,
+ * grown to the largest frame, is kept - no page-locked allocation, which
+ * stalls every CUDA call of the process, in the steady state). */
+struct PlanLists {
   pvec<BlockRec> blocks;
   pvec<TxRec> txs;
   pvec<ObmcRec> obmc;
@@ -309,6 +333,22 @@ struct Plan {
   pvec<int> units;                /* phase B blocks in claim order */
   pvec<int> deps;                 /* per phase B block (dep_first, dep_count): the
                                      phase B blocks it waits for */
+  pvec<int2> inter_tiles;
+  pvec<int2> itx_jobs;            /* sorted by size class, then shape and type */
+  pvec<int4> itx_batches;         /* (first job, jobs, log2 class or 7 = raw) */
+  pvec<DeblockRec> deblock_v, deblock_h;
+  pvec<CdefRec> cdef;
+  pvec<unsigned> cdef_search;     /* searches off the 8x8 grid: x | y << 16 */
+  pvec<LrUnitRec> lr_units[3];
+};
+
+/* One planned frame's constants and record counts (its records live in
+ * device memory, uploaded from the PlanLists). */
+struct Plan {
+  PlanLists* R = nullptr;         /* while planning: the lists being built */
+  size_t n_blocks = 0, n_units = 0, n_tiles = 0, n_itx = 0, n_itxb = 0, n_dbv = 0, n_dbh = 0,
+         n_cdef = 0,
+         n_cdef_search = 0;
   int unit_depth = 0;             /* dependency depth of the frame */
   pvec<int2> inter_tiles;
   pvec<int2> itx_jobs;
@@ -317,7 +357,6 @@ struct Plan {
   pvec<unsigned> cdef_search;     /* searches off the 8x8 grid: x | y << 16 */
   int cdef_grid_w = 0, cdef_grid_n = 0;  /* the grid of 8x8 luma searches */
   bool cdef_search_any = false;          /* some record reads the grid */
-  pvec<LrUnitRec> lr_units[3];
   LrArgs lr{};
   bool use_lr = false;
   size_t coef_pool = 0, residual_pool = 0;
@@ -439,6 +478,8 @@ int plan_block(const PlanCtx& ctx, const av1b_frame_syntax& s, size_t bi, BlockR
     const bool fi = b.use_filter_intra && b.plane == 0;
     if (fi && (b.filter_intra_mode < 0 || b.filter_intra_mode > 4))
       return O->err.set(AV1B_ERR_SYNTAX, "filter intra mode out of range");
+    if (fi && (b.w > 32 || b.h > 32))
+      return O->err.set(AV1B_ERR_SYNTAX, "filter intra on a block larger than 32x32");
     r.fi_mode = static_cast<signed char>(fi ? b.filter_intra_mode : -1);
     r.cfl_alpha = static_cast<signed char>(std::max(-128, std::min(127, b.cfl_alpha)));
     r.have_ar = b.have_above_right >= 0 ? (b.have_above_right != 0) : 2;
@@ -722,6 +763,10 @@ struct PlanScratch {
   std::vector<std::vector<int>> unit_deps;
   std::vector<int> dep_count, depth, sorted;
   std::vector<uint8_t> is_b;
+  std::vector<uint16_t> itx_key;
+  std::vector<int> itx_hist;
+  std::vector<int2> itx_sorted;
+  std::vector<uint8_t> itx_scls;
 };
 
 /* Splits [0, n) into pieces of at least `min_piece` for the pool. */
@@ -754,8 +799,8 @@ inline size_t piece_begin(size_t n, int pieces, int i) { return n * i / pieces; 
  * depth runs as one wide wave. */
 int plan_units(av1b_decoder* d, const PlanCtx& c, Plan* P) {
   const Layout& L = c.L;
-  P->deps.clear();
-  if (P->units.empty()) return AV1B_OK;
+  P->R->deps.clear();
+  if (P->R->units.empty()) return AV1B_OK;
   PlanScratch& S = *c.scratch;
   int sh[3], cw[3], ch[3];
   for (int p = 0; p < 3; ++p) {
@@ -770,18 +815,18 @@ int plan_units(av1b_decoder* d, const PlanCtx& c, Plan* P) {
   });
   /* owner grids: later blocks overwrite earlier ones where cells overlap, so
    * a plane whose blocks are not all cell aligned is filled in order */
-  const size_t nb = P->blocks.size();
+  const size_t nb = P->R->blocks.size();
   std::vector<uint8_t>& is_b = S.is_b;
   is_b.resize(nb);
   bool aligned[3] = {true, true, true};
   for (size_t bi = 0; bi < nb; ++bi) {
-    const BlockRec& b = P->blocks[bi];
+    const BlockRec& b = P->R->blocks[bi];
     const int m = (1 << sh[b.plane]) - 1;
     if ((b.x | b.y | b.w | b.h) & m) aligned[b.plane] = false;
     is_b[bi] = b.phase_b;
   }
   auto fill = [&](size_t bi) {
-    const BlockRec& b = P->blocks[bi];
+    const BlockRec& b = P->R->blocks[bi];
     const int p = b.plane, oc = 1 << sh[p];
     const int cx0 = std::max<int>(b.x, 0) >> sh[p], cy0 = std::max<int>(b.y, 0) >> sh[p];
     const int cx1 = std::min((b.x + b.w + oc - 1) >> sh[p], cw[p]);
@@ -794,11 +839,11 @@ int plan_units(av1b_decoder* d, const PlanCtx& c, Plan* P) {
     const int pieces = pieces_for(nb, c, 2048);
     c.pool->run(pieces, [&](int i) {
       for (size_t bi = piece_begin(nb, pieces, i); bi < piece_begin(nb, pieces, i + 1); ++bi)
-        if (aligned[P->blocks[bi].plane]) fill(bi);
+        if (aligned[P->R->blocks[bi].plane]) fill(bi);
     });
     if (!aligned[0] || !aligned[1] || !aligned[2])
       for (size_t bi = 0; bi < nb; ++bi)
-        if (!aligned[P->blocks[bi].plane]) fill(bi);
+        if (!aligned[P->R->blocks[bi].plane]) fill(bi);
   }
   auto owner_at = [&](int p, int x, int y) -> int {
     if (x < 0 || y < 0 || x >= L.p[p].grid_w || y >= L.p[p].grid_h) return -1;
@@ -813,7 +858,7 @@ int plan_units(av1b_decoder* d, const PlanCtx& c, Plan* P) {
       for (int x = xs; x <= x1; x += oc) f(owner_at(p, x, y));
   };
   static const int kAngle[9] = {0, 90, 180, 45, 135, 113, 157, 203, 67};
-  const size_t nu = P->units.size();
+  const size_t nu = P->R->units.size();
   const int pieces = pieces_for(nu, c, 256);
   std::vector<std::vector<int>>& pdeps = S.unit_deps;
   if (pdeps.size() < static_cast<size_t>(pieces)) pdeps.resize(pieces);
@@ -824,8 +869,8 @@ int plan_units(av1b_decoder* d, const PlanCtx& c, Plan* P) {
     out.clear();
     std::vector<int> mine;
     for (size_t ui = piece_begin(nu, pieces, pi); ui < piece_begin(nu, pieces, pi + 1); ++ui) {
-      const int bi = P->units[ui];
-      BlockRec& b = P->blocks[bi];
+      const int bi = P->R->units[ui];
+      BlockRec& b = P->R->blocks[bi];
       const int p = b.plane, oc = 1 << sh[p];
       mine.clear();
       auto wait_on = [&](int o) {
@@ -886,7 +931,7 @@ int plan_units(av1b_decoder* d, const PlanCtx& c, Plan* P) {
       if (b.kind == AV1B_U_INTRA && b.w * b.h <= 4096) {
         bool ok = true, grid4 = true;
         for (int t = 0; t < b.tx_count && ok; ++t) {
-          const TxRec& x = P->txs[b.tx_first + t];
+          const TxRec& x = P->R->txs[b.tx_first + t];
           if (x.x < 0 || x.y < 0 || x.x + x.w > b.w || x.y + x.h > b.h) ok = false;
           if ((x.x | x.y | x.w | x.h) & 3) grid4 = false;
         }
@@ -894,7 +939,7 @@ int plan_units(av1b_decoder* d, const PlanCtx& c, Plan* P) {
           /* 4x4 cells of the block (at most 16 x 16) */
           uint64_t cov[4] = {0, 0, 0, 0};
           for (int t = 0; t < b.tx_count && ok; ++t) {
-            const TxRec& x = P->txs[b.tx_first + t];
+            const TxRec& x = P->R->txs[b.tx_first + t];
             for (int cy = x.y >> 2; cy < (x.y + x.h) >> 2 && ok; ++cy)
               for (int cx = x.x >> 2; cx < (x.x + x.w) >> 2; ++cx) {
                 const int bit = cy * 16 + cx;
@@ -907,9 +952,9 @@ int plan_units(av1b_decoder* d, const PlanCtx& c, Plan* P) {
           }
         } else if (ok) {
           for (int t = 0; t < b.tx_count && ok; ++t) {
-            const TxRec& x = P->txs[b.tx_first + t];
+            const TxRec& x = P->R->txs[b.tx_first + t];
             for (int u = 0; u < t && ok; ++u) {
-              const TxRec& y = P->txs[b.tx_first + u];
+              const TxRec& y = P->R->txs[b.tx_first + u];
               if (x.x < y.x + y.w && y.x < x.x + x.w && x.y < y.y + y.h && y.y < x.y + x.h) ok = false;
             }
             if (t > 64) ok = false;
@@ -927,34 +972,95 @@ int plan_units(av1b_decoder* d, const PlanCtx& c, Plan* P) {
   std::vector<size_t> first(nu + 1, 0);
   for (size_t ui = 0; ui < nu; ++ui) first[ui + 1] = first[ui] + dep_count[ui];
   if (first[nu] > static_cast<size_t>(INT32_MAX)) return fail(d, AV1B_ERR_SYNTAX, "frame too large");
-  P->deps.resize(first[nu]);
+  P->R->deps.resize(first[nu]);
   c.pool->run(pieces, [&](int pi) {
     std::copy(pdeps[pi].begin(), pdeps[pi].end(),
-              P->deps.begin() + first[piece_begin(nu, pieces, pi)]);
+              P->R->deps.begin() + first[piece_begin(nu, pieces, pi)]);
     for (size_t ui = piece_begin(nu, pieces, pi); ui < piece_begin(nu, pieces, pi + 1); ++ui) {
-      BlockRec& b = P->blocks[P->units[ui]];
+      BlockRec& b = P->R->blocks[P->R->units[ui]];
       b.dep_first = static_cast<int>(first[ui]);
       b.dep_count = dep_count[ui];
     }
   });
   int max_depth = 0;
-  const int* dl = P->deps.data();
+  const int* dl = P->R->deps.data();
   for (size_t ui = 0; ui < nu; ++ui) {
     int dd = 0;
     for (size_t k = first[ui]; k < first[ui + 1]; ++k) dd = std::max(dd, depth[dl[k]]);
-    depth[P->units[ui]] = dd + 1;
+    depth[P->R->units[ui]] = dd + 1;
     max_depth = std::max(max_depth, dd + 1);
   }
   /* claim order: by depth, coding order within one */
   std::vector<int> count(max_depth + 2, 0);
-  for (size_t ui = 0; ui < nu; ++ui) ++count[depth[P->units[ui]] + 1];
+  for (size_t ui = 0; ui < nu; ++ui) ++count[depth[P->R->units[ui]] + 1];
   for (int k = 0; k <= max_depth; ++k) count[k + 1] += count[k];
   std::vector<int>& sorted = S.sorted;
   sorted.resize(nu);
-  for (size_t ui = 0; ui < nu; ++ui) sorted[count[depth[P->units[ui]]]++] = P->units[ui];
-  std::copy(sorted.begin(), sorted.end(), P->units.begin());
+  for (size_t ui = 0; ui < nu; ++ui) sorted[count[depth[P->R->units[ui]]]++] = P->R->units[ui];
+  std::copy(sorted.begin(), sorted.end(), P->R->units.begin());
   P->unit_depth = max_depth;
   return AV1B_OK;
+}
+
+/* Orders the inverse transforms for the batched kernel: by size class (the
+ * longer side, 4 .. 64; raw residual blocks last), then shape and type, so
+ * the lane groups of a warp mostly run the same code; then cuts each class
+ * into batches of 32 / class transforms (one for 64 and raw). */
+void plan_itx(const PlanCtx& c, Plan* P) {
+  PlanLists& R = *P->R;
+  const size_t n = R.itx_jobs.size();
+  R.itx_batches.clear();
+  if (n == 0) return;
+  PlanScratch& S = *c.scratch;
+  constexpr int kKeys = 8 * 7 * 7 * 16;
+  std::vector<uint16_t>& key = S.itx_key;
+  key.resize(n);
+  /* a parallel counting sort: keys and per-piece histograms, offsets per
+   * (key, piece), then every piece scatters its own jobs */
+  const int pieces = pieces_for(n, c, 4096);
+  std::vector<int>& hist = S.itx_hist;
+  hist.assign(static_cast<size_t>(kKeys) * pieces, 0);
+  c.pool->run(pieces, [&](int pi) {
+    int* h = hist.data() + static_cast<size_t>(pi) * kKeys;
+    for (size_t i = piece_begin(n, pieces, pi); i < piece_begin(n, pieces, pi + 1); ++i) {
+      const int2 j = R.itx_jobs[i];
+      const TxRec& t = R.txs[j.y];
+      int k = 7 * 7 * 7 * 16;
+      if (!R.blocks[j.x].residual_provided)
+        k = ((std::max(t.log2w, t.log2h) * 7 + t.log2w) * 7 + t.log2h) * 16 + t.type;
+      key[i] = static_cast<uint16_t>(k);
+      ++h[k];
+    }
+  });
+  int run = 0;
+  for (int k = 0; k < kKeys; ++k)
+    for (int pi = 0; pi < pieces; ++pi) {
+      int& h = hist[static_cast<size_t>(pi) * kKeys + k];
+      const int c0 = h;
+      h = run;
+      run += c0;
+    }
+  std::vector<int2>& sorted = S.itx_sorted;
+  std::vector<uint8_t>& scls = S.itx_scls;
+  sorted.resize(n);
+  scls.resize(n);
+  c.pool->run(pieces, [&](int pi) {
+    int* h = hist.data() + static_cast<size_t>(pi) * kKeys;
+    for (size_t i = piece_begin(n, pieces, pi); i < piece_begin(n, pieces, pi + 1); ++i) {
+      const int o = h[key[i]]++;
+      sorted[o] = R.itx_jobs[i];
+      scls[o] = static_cast<uint8_t>(key[i] == 7 * 7 * 7 * 16 ? 7 : key[i] / (7 * 7 * 16));
+    }
+  });
+  std::copy(sorted.begin(), sorted.end(), R.itx_jobs.begin());
+  for (size_t i = 0; i < n;) {
+    const int cl = scls[i];
+    const size_t per = cl >= 6 ? 1 : static_cast<size_t>(32 >> cl);
+    size_t e = i + 1;
+    while (e < n && e - i < per && scls[e] == cl) ++e;
+    R.itx_batches.push_back(make_int4(static_cast<int>(i), static_cast<int>(e - i), cl, 0));
+    i = e;
+  }
 }
 
 /* Validates a frame and builds its device records. The blocks, deblocking
@@ -966,7 +1072,7 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
   const Layout& L = c.L;
   const int bd = s.bit_depth;
   int rc_units;
-  P->blocks.resize(s.n_blocks);
+  P->R->blocks.resize(s.n_blocks);
   for (int i = 0; i < 7; ++i) {
     const int rw = s.reference_width[i] > 0 ? s.reference_width[i] : s.width;
     const int rh = s.reference_height[i] > 0 ? s.reference_height[i] : s.height;
@@ -991,7 +1097,7 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
       BlockOut* O = &outs[i];
       O->clear();
       for (size_t bi = piece_begin(nb, pieces, i); bi < piece_begin(nb, pieces, i + 1); ++bi)
-        if (plan_block(c, s, bi, P->blocks[bi], O)) break;
+        if (plan_block(c, s, bi, P->R->blocks[bi], O)) break;
     });
     for (int i = 0; i < pieces; ++i)
       if (outs[i].err.code) return fail(d, outs[i].err.code, outs[i].err.msg);
@@ -1014,14 +1120,14 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
     }
     if (o_pre[pieces] > static_cast<size_t>(INT32_MAX) || o_tx[pieces] > static_cast<size_t>(INT32_MAX))
       return fail(d, AV1B_ERR_SYNTAX, "frame too large");
-    P->txs.resize(o_tx[pieces]);
-    P->obmc.resize(o_obmc[pieces]);
-    P->warps.resize(1 + o_warp[pieces]);
-    P->warps[0] = WarpRec{};
-    P->palette_colors.resize(o_pal[pieces]);
-    P->units.resize(o_unit[pieces]);
-    P->inter_tiles.resize(o_tile[pieces]);
-    P->itx_jobs.resize(o_itx[pieces]);
+    P->R->txs.resize(o_tx[pieces]);
+    P->R->obmc.resize(o_obmc[pieces]);
+    P->R->warps.resize(1 + o_warp[pieces]);
+    P->R->warps[0] = WarpRec{};
+    P->R->palette_colors.resize(o_pal[pieces]);
+    P->R->units.resize(o_unit[pieces]);
+    P->R->inter_tiles.resize(o_tile[pieces]);
+    P->R->itx_jobs.resize(o_itx[pieces]);
     P->pre_res_pool = o_pre[pieces];
     c.pool->run(pieces, [&](int i) {
       const BlockOut& O = outs[i];
@@ -1029,7 +1135,7 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
       const int dwp = static_cast<int>(o_warp[i]), dpal = static_cast<int>(o_pal[i] / 8);
       const int dpre = static_cast<int>(o_pre[i]);
       for (size_t bi = piece_begin(nb, pieces, i); bi < piece_begin(nb, pieces, i + 1); ++bi) {
-        BlockRec& r = P->blocks[bi];
+        BlockRec& r = P->R->blocks[bi];
         r.tx_first += dtx;
         if (r.is_inter) r.obmc_first += dob;
         if (r.palette) r.palette_color_idx += dpal;
@@ -1039,21 +1145,22 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
       for (size_t k = 0; k < O.txs.size(); ++k) {
         TxRec x = O.txs[k];
         if (x.pre_off >= 0) x.pre_off += dpre;
-        P->txs[o_tx[i] + k] = x;
+        P->R->txs[o_tx[i] + k] = x;
       }
-      std::copy(O.obmc.begin(), O.obmc.end(), P->obmc.begin() + o_obmc[i]);
-      std::copy(O.warps.begin(), O.warps.end(), P->warps.begin() + 1 + o_warp[i]);
-      std::copy(O.palette_colors.begin(), O.palette_colors.end(), P->palette_colors.begin() + o_pal[i]);
-      std::copy(O.units.begin(), O.units.end(), P->units.begin() + o_unit[i]);
-      std::copy(O.inter_tiles.begin(), O.inter_tiles.end(), P->inter_tiles.begin() + o_tile[i]);
+      std::copy(O.obmc.begin(), O.obmc.end(), P->R->obmc.begin() + o_obmc[i]);
+      std::copy(O.warps.begin(), O.warps.end(), P->R->warps.begin() + 1 + o_warp[i]);
+      std::copy(O.palette_colors.begin(), O.palette_colors.end(), P->R->palette_colors.begin() + o_pal[i]);
+      std::copy(O.units.begin(), O.units.end(), P->R->units.begin() + o_unit[i]);
+      std::copy(O.inter_tiles.begin(), O.inter_tiles.end(), P->R->inter_tiles.begin() + o_tile[i]);
       for (size_t k = 0; k < O.itx_jobs.size(); ++k) {
         int2 j = O.itx_jobs[k];
         j.y += dtx;
-        P->itx_jobs[o_itx[i] + k] = j;
+        P->R->itx_jobs[o_itx[i] + k] = j;
       }
     });
   }
   if ((rc_units = plan_units(d, c, P))) return rc_units;
+  plan_itx(c, P);
 
   /* the pools read past the caller's arrays as zeros, like the reference's
    * padded plan pools (engine.cpp:665-674) */
@@ -1061,8 +1168,8 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
   P->residual_pool = std::max(res_end + 64, s.n_residual);
 
   /* deblocking edges: V then H, each a list of independent edges */
-  P->deblock_v.clear();
-  P->deblock_h.clear();
+  P->R->deblock_v.clear();
+  P->R->deblock_h.clear();
   if (s.sharpness < 0 || s.sharpness > 7) return fail(d, AV1B_ERR_SYNTAX, "sharpness out of range");
   {
     const size_t ne = s.n_deblock;
@@ -1086,19 +1193,19 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
       nv += outs[i].v.size();
       nh += outs[i].h.size();
     }
-    P->deblock_v.resize(nv);
-    P->deblock_h.resize(nh);
+    P->R->deblock_v.resize(nv);
+    P->R->deblock_h.resize(nh);
     c.pool->run(pieces, [&](int i) {
-      std::copy(outs[i].v.begin(), outs[i].v.end(), P->deblock_v.begin() + ov[i]);
-      std::copy(outs[i].h.begin(), outs[i].h.end(), P->deblock_h.begin() + oh[i]);
+      std::copy(outs[i].v.begin(), outs[i].v.end(), P->R->deblock_v.begin() + ov[i]);
+      std::copy(outs[i].h.begin(), outs[i].h.end(), P->R->deblock_h.begin() + oh[i]);
     });
   }
 
   /* CDEF */
   {
     const size_t nc = s.n_cdef;
-    P->cdef.resize(nc);
-    P->cdef_search.clear();
+    P->R->cdef.resize(nc);
+    P->R->cdef_search.clear();
     P->cdef_grid_w = L.p[0].stride >> 3;
     P->cdef_grid_n = P->cdef_grid_w * (plane_rows(L, 0) >> 3);
     const int pieces = pieces_for(nc, c, 4096);
@@ -1110,7 +1217,7 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
       O->any = false;
       O->err = PlanErr();
       for (size_t k = piece_begin(nc, pieces, i); k < piece_begin(nc, pieces, i + 1); ++k)
-        if (plan_cdef(c, s, k, P->cdef_grid_w, P->cdef.data(), O)) break;
+        if (plan_cdef(c, s, k, P->cdef_grid_w, P->R->cdef.data(), O)) break;
     });
     P->cdef_search_any = false;
     for (int i = 0; i < pieces; ++i) {
@@ -1119,8 +1226,8 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
       for (size_t k : outs[i].unaligned) {
         const av1b_cdef_block& b = s.cdef[k];
         const int sx = b.plane ? L.ss_x : 0, sy = b.plane ? L.ss_y : 0;
-        P->cdef[k].search = P->cdef_grid_n + static_cast<int>(P->cdef_search.size());
-        P->cdef_search.push_back(static_cast<unsigned>(b.x << sx) | (static_cast<unsigned>(b.y << sy) << 16));
+        P->R->cdef[k].search = P->cdef_grid_n + static_cast<int>(P->R->cdef_search.size());
+        P->R->cdef_search.push_back(static_cast<unsigned>(b.x << sx) | (static_cast<unsigned>(b.y << sy) << 16));
       }
     }
   }
@@ -1129,7 +1236,7 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
   P->use_lr = false;
   std::memset(&P->lr, 0, sizeof(P->lr));
   for (int p = 0; p < 3; ++p) {
-    P->lr_units[p].clear();
+    P->R->lr_units[p].clear();
     if (s.restoration_type[p] == 0) continue;
     const int sub_y = p ? L.ss_y : 0;
     if (s.restoration_unit_log2[p] < 5 || s.restoration_unit_log2[p] > 8)
@@ -1158,7 +1265,7 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
       o.e[1] = sp[3];
       o.xqd[0] = u.sgr_xqd[0];
       o.xqd[1] = u.sgr_xqd[1];
-      P->lr_units[p].push_back(o);
+      P->R->lr_units[p].push_back(o);
     }
     P->use_lr = true;
   }
@@ -1297,6 +1404,7 @@ cudaError_t timed(av1b_decoder* d, int stage, F launch, cudaStream_t on = nullpt
 /* Host time since `t0` into a host stage, when profiling. */
 void host_mark(av1b_decoder* d, int stage, std::chrono::steady_clock::time_point t0) {
   if (!d->profiling) return;
+  std::lock_guard<std::mutex> lk(d->prof_mu);
   d->prof_ms[stage] +=
       std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   d->prof_n[stage] += 1;
@@ -1342,7 +1450,7 @@ struct av1b_plan {
   cudaEvent_t ready = nullptr, done = nullptr;
   bool in_flight = false;
   size_t o_blocks = 0, o_txs = 0, o_obmc = 0, o_warps = 0, o_pal = 0, o_units = 0, o_deps = 0;
-  size_t o_tiles = 0, o_itx = 0, o_dbv = 0, o_dbh = 0, o_cdef = 0, o_lr[3] = {0, 0, 0};
+  size_t o_tiles = 0, o_itx = 0, o_itxb = 0, o_dbv = 0, o_dbh = 0, o_cdef = 0, o_lr[3] = {0, 0, 0};
   size_t o_map = 0, o_cdef_search = 0;
   int slots_read[kSlots + 1];     /* the reference slots the frame reads, -1 ended */
   int n_blocks = 0;
@@ -1358,7 +1466,33 @@ namespace {
  * N+1 while frame N runs. It returns once the uploads are done: the caller's
  * arrays are free again. */
 int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
-  std::lock_guard<std::mutex> plk(d->plan_mu);
+  /* a free planner, held for this call */
+  av1b_decoder::Planner* pn = nullptr;
+  {
+    std::unique_lock<std::mutex> lk(d->planner_mu);
+    d->planner_cv.wait(lk, [&] {
+      for (auto& q : d->planners)
+        if (!q.busy) return true;
+      return false;
+    });
+    for (auto& q : d->planners)
+      if (!q.busy) {
+        pn = &q;
+        break;
+      }
+    pn->busy = true;
+  }
+  struct Release {
+    av1b_decoder* d;
+    av1b_decoder::Planner* pn;
+    ~Release() {
+      {
+        std::lock_guard<std::mutex> lk(d->planner_mu);
+        pn->busy = false;
+      }
+      d->planner_cv.notify_one();
+    }
+  } release{d, pn};
   int rc;
   if ((rc = check_header(d, s))) return rc;
   const int coded_width = (s.coded_width <= 0 || s.coded_width > s.width) ? s.width : s.coded_width;
@@ -1373,18 +1507,21 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
       c.slot_height[i] = d->slot_height[i];
     }
   }
-  c.pool = d->pool;
-  c.scratch = d->scratch;
+  c.pool = pn->pool;
+  c.scratch = pn->scratch;
   if (!pl->ready) {
-    CK(cudaEventCreateWithFlags(&pl->ready, cudaEventDisableTiming), "event");
-    CK(cudaEventCreateWithFlags(&pl->done, cudaEventDisableTiming), "event");
+    /* blocking-sync events: a waiting planner sleeps instead of spinning on
+     * a core the planner pool or the decoding thread could use */
+    CK(cudaEventCreateWithFlags(&pl->ready, cudaEventDisableTiming | cudaEventBlockingSync), "event");
+    CK(cudaEventCreateWithFlags(&pl->done, cudaEventDisableTiming | cudaEventBlockingSync), "event");
   }
   if (pl->in_flight) {
     CK(cudaEventSynchronize(pl->done), "plan reuse wait");
     pl->in_flight = false;
   }
   Plan& P = pl->P;
-  cudaStream_t st = d->upload;
+  P.R = pn->lists;
+  cudaStream_t st = pn->upload;
   /* the caller's coefficients and raw residuals go up first, while the
    * records are built */
   if ((rc = dev_ensure(d, pl->coef, (s.n_coefficients + 64) * sizeof(int))) ||
@@ -1407,6 +1544,15 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
     return rc;
   }
   host_mark(d, kStPlanHost, t0);
+  P.n_blocks = P.R->blocks.size();
+  P.n_units = P.R->units.size();
+  P.n_tiles = P.R->inter_tiles.size();
+  P.n_itx = P.R->itx_jobs.size();
+  P.n_itxb = P.R->itx_batches.size();
+  P.n_dbv = P.R->deblock_v.size();
+  P.n_dbh = P.R->deblock_h.size();
+  P.n_cdef = P.R->cdef.size();
+  P.n_cdef_search = P.R->cdef_search.size();
   pl->L = c.L;
   pl->width = s.width;
   pl->height = s.height;
@@ -1419,10 +1565,10 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
   pl->n_blocks = static_cast<int>(s.n_blocks);
   {
     bool used[kSlots] = {false};
-    for (const BlockRec& b : P.blocks)
+    for (const BlockRec& b : P.R->blocks)
       for (int k = 0; k < 2; ++k)
         if (b.ref_slot[k] >= 0) used[b.ref_slot[k]] = true;
-    for (const ObmcRec& o : P.obmc)
+    for (const ObmcRec& o : P.R->obmc)
       if (o.ref_slot >= 0) used[o.ref_slot] = true;
     int n = 0;
     for (int i = 0; i < kSlots; ++i)
@@ -1430,20 +1576,21 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
     pl->slots_read[n] = -1;
   }
   size_t off = 0;
-  pl->o_blocks = stage_put(&off, P.blocks);
-  pl->o_txs = stage_put(&off, P.txs);
-  pl->o_obmc = stage_put(&off, P.obmc);
-  pl->o_warps = stage_put(&off, P.warps);
-  pl->o_pal = stage_put(&off, P.palette_colors);
-  pl->o_units = stage_put(&off, P.units);
-  pl->o_deps = stage_put(&off, P.deps);
-  pl->o_tiles = stage_put(&off, P.inter_tiles);
-  pl->o_itx = stage_put(&off, P.itx_jobs);
-  pl->o_dbv = stage_put(&off, P.deblock_v);
-  pl->o_dbh = stage_put(&off, P.deblock_h);
-  pl->o_cdef = stage_put(&off, P.cdef);
-  pl->o_cdef_search = stage_put(&off, P.cdef_search);
-  for (int p = 0; p < 3; ++p) pl->o_lr[p] = stage_put(&off, P.lr_units[p]);
+  pl->o_blocks = stage_put(&off, P.R->blocks);
+  pl->o_txs = stage_put(&off, P.R->txs);
+  pl->o_obmc = stage_put(&off, P.R->obmc);
+  pl->o_warps = stage_put(&off, P.R->warps);
+  pl->o_pal = stage_put(&off, P.R->palette_colors);
+  pl->o_units = stage_put(&off, P.R->units);
+  pl->o_deps = stage_put(&off, P.R->deps);
+  pl->o_tiles = stage_put(&off, P.R->inter_tiles);
+  pl->o_itx = stage_put(&off, P.R->itx_jobs);
+  pl->o_itxb = stage_put(&off, P.R->itx_batches);
+  pl->o_dbv = stage_put(&off, P.R->deblock_v);
+  pl->o_dbh = stage_put(&off, P.R->deblock_h);
+  pl->o_cdef = stage_put(&off, P.R->cdef);
+  pl->o_cdef_search = stage_put(&off, P.R->cdef_search);
+  for (int p = 0; p < 3; ++p) pl->o_lr[p] = stage_put(&off, P.R->lr_units[p]);
   pl->o_map = off;
   off = align_up(off + s.n_palette_map + 64, 256);
   const size_t total = off;
@@ -1458,20 +1605,21 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
     const size_t bytes = v.size() * sizeof(v[0]);
     return bytes ? cudaMemcpyAsync(ar + o, v.data(), bytes, cudaMemcpyHostToDevice, st) : cudaSuccess;
   };
-  CK(put(pl->o_blocks, P.blocks), "record upload");
-  CK(put(pl->o_txs, P.txs), "record upload");
-  CK(put(pl->o_obmc, P.obmc), "record upload");
-  CK(put(pl->o_warps, P.warps), "record upload");
-  CK(put(pl->o_pal, P.palette_colors), "record upload");
-  CK(put(pl->o_units, P.units), "record upload");
-  CK(put(pl->o_deps, P.deps), "record upload");
-  CK(put(pl->o_tiles, P.inter_tiles), "record upload");
-  CK(put(pl->o_itx, P.itx_jobs), "record upload");
-  CK(put(pl->o_dbv, P.deblock_v), "record upload");
-  CK(put(pl->o_dbh, P.deblock_h), "record upload");
-  CK(put(pl->o_cdef, P.cdef), "record upload");
-  CK(put(pl->o_cdef_search, P.cdef_search), "record upload");
-  for (int p = 0; p < 3; ++p) CK(put(pl->o_lr[p], P.lr_units[p]), "record upload");
+  CK(put(pl->o_blocks, P.R->blocks), "record upload");
+  CK(put(pl->o_txs, P.R->txs), "record upload");
+  CK(put(pl->o_obmc, P.R->obmc), "record upload");
+  CK(put(pl->o_warps, P.R->warps), "record upload");
+  CK(put(pl->o_pal, P.R->palette_colors), "record upload");
+  CK(put(pl->o_units, P.R->units), "record upload");
+  CK(put(pl->o_deps, P.R->deps), "record upload");
+  CK(put(pl->o_tiles, P.R->inter_tiles), "record upload");
+  CK(put(pl->o_itx, P.R->itx_jobs), "record upload");
+  CK(put(pl->o_itxb, P.R->itx_batches), "record upload");
+  CK(put(pl->o_dbv, P.R->deblock_v), "record upload");
+  CK(put(pl->o_dbh, P.R->deblock_h), "record upload");
+  CK(put(pl->o_cdef, P.R->cdef), "record upload");
+  CK(put(pl->o_cdef_search, P.R->cdef_search), "record upload");
+  for (int p = 0; p < 3; ++p) CK(put(pl->o_lr[p], P.R->lr_units[p]), "record upload");
   if (s.n_palette_map)
     CK(cudaMemcpyAsync(ar + pl->o_map, s.palette_map, s.n_palette_map, cudaMemcpyHostToDevice, st),
        "palette map upload");
@@ -1503,6 +1651,7 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
   t0 = std::chrono::steady_clock::now();
   CK(cudaEventSynchronize(pl->ready), "upload wait");
   host_mark(d, kStWaitHost, t0);
+  P.R = nullptr;
   return AV1B_OK;
 }
 
@@ -1554,8 +1703,8 @@ int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, cons
   }
   const size_t pic_bytes = static_cast<size_t>(L.size) * sizeof(px_t);
   if (P.pre_res_pool && (rc = dev_ensure(d, d->pre_res, P.pre_res_pool * sizeof(int)))) return rc;
-  if ((P.cdef_search_any || !P.cdef_search.empty()) &&
-      (rc = dev_ensure(d, d->cdef_search, (P.cdef_grid_n + P.cdef_search.size()) * sizeof(int))))
+  if ((P.cdef_search_any || (P.n_cdef_search != 0)) &&
+      (rc = dev_ensure(d, d->cdef_search, (P.cdef_grid_n + P.n_cdef_search) * sizeof(int))))
     return rc;
   if (P.use_lr) {
     if ((rc = dev_ensure(d, d->lr_pre, pic_bytes)) || (rc = dev_ensure(d, d->lr_cdef, pic_bytes)) ||
@@ -1584,7 +1733,8 @@ int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, cons
   /* done flags, queue and status */
   FrameArgs a{};
   a.L = L;
-  const size_t done_bytes = static_cast<size_t>(pl->n_blocks) * sizeof(unsigned) + 256;
+  const size_t done_bytes =
+      static_cast<size_t>(pl->n_blocks) * AV1B_FLAG_STRIDE * sizeof(unsigned) + 256;
   if (d->done.cap < done_bytes) {
     if ((rc = dev_ensure(d, d->done, done_bytes))) return rc;
     CK(cudaMemsetAsync(d->done.p, 0, d->done.cap, st), "done reset");
@@ -1605,7 +1755,7 @@ int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, cons
   a.cur = static_cast<px_t*>(d->cur.p);
   a.slot_ptr = static_cast<px_t* const*>(d->slot_ptr_dev.p);
   a.blocks = reinterpret_cast<const BlockRec*>(ar + pl->o_blocks);
-  a.n_blocks = static_cast<int>(P.blocks.size());
+  a.n_blocks = static_cast<int>(P.n_blocks);
   a.txs = reinterpret_cast<const TxRec*>(ar + pl->o_txs);
   a.obmc = reinterpret_cast<const ObmcRec*>(ar + pl->o_obmc);
   a.warps = reinterpret_cast<const WarpRec*>(ar + pl->o_warps);
@@ -1616,14 +1766,16 @@ int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, cons
   a.done = static_cast<unsigned*>(d->done.p);
   a.epoch = d->epoch;
   a.units = reinterpret_cast<const int*>(ar + pl->o_units);
-  a.n_units = static_cast<int>(P.units.size());
+  a.n_units = static_cast<int>(P.n_units);
   a.deps = reinterpret_cast<const int*>(ar + pl->o_deps);
   a.queue = static_cast<unsigned*>(d->status_q.p);
   a.status = reinterpret_cast<int*>(static_cast<uint8_t*>(d->status_q.p) + 64);
   a.inter_tiles = reinterpret_cast<const int2*>(ar + pl->o_tiles);
-  a.n_inter_tiles = static_cast<int>(P.inter_tiles.size());
+  a.n_inter_tiles = static_cast<int>(P.n_tiles);
   a.itx_jobs = reinterpret_cast<const int2*>(ar + pl->o_itx);
-  a.n_itx = static_cast<int>(P.itx_jobs.size());
+  a.n_itx = static_cast<int>(P.n_itx);
+  a.itx_batches = reinterpret_cast<const int4*>(ar + pl->o_itxb);
+  a.n_itx_batches = static_cast<int>(P.n_itxb);
   a.pre_res = static_cast<int*>(d->pre_res.p);
   a.maxv = maxv;
   a.scale_x = P.scale_x;
@@ -1651,7 +1803,8 @@ int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, cons
   }
   CK(cudaEventRecord(ev[0], st), "event");
   for (int stage = 1; stage < 4; ++stage) {
-    const bool any = stage == 1 ? a.n_inter_tiles > 0 : (stage == 2 ? a.n_itx > 0 : a.n_units > 0);
+    const bool any =
+        stage == 1 ? a.n_inter_tiles > 0 : (stage == 2 ? a.n_itx_batches > 0 : a.n_units > 0);
     if (!any) continue;
     CK(timed(d, kStOwner + stage, [&] { return launch_recon_stage(stage, a, d->n_sm, st); }),
        "reconstruction launch");
@@ -1661,34 +1814,34 @@ int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, cons
 
   /* ---- filters --------------------------------------------------------------------------- */
   px_t* cur = a.cur;
-  if (!P.deblock_v.empty())
+  if ((P.n_dbv != 0))
     CK(timed(d, kStDeblockV, [&] {
          return launch_deblock(cur, reinterpret_cast<const DeblockRec*>(ar + pl->o_dbv),
-                               static_cast<int>(P.deblock_v.size()), pl->sharpness, pl->bit_depth,
+                               static_cast<int>(P.n_dbv), pl->sharpness, pl->bit_depth,
                                maxv, st);
        }), "deblock V");
-  if (!P.deblock_h.empty())
+  if ((P.n_dbh != 0))
     CK(timed(d, kStDeblockH, [&] {
          return launch_deblock(cur, reinterpret_cast<const DeblockRec*>(ar + pl->o_dbh),
-                               static_cast<int>(P.deblock_h.size()), pl->sharpness, pl->bit_depth,
+                               static_cast<int>(P.n_dbh), pl->sharpness, pl->bit_depth,
                                maxv, st);
        }), "deblock H");
-  launches += (!P.deblock_v.empty()) + (!P.deblock_h.empty());
+  launches += ((P.n_dbv != 0)) + ((P.n_dbh != 0));
   px_t* snap = static_cast<px_t*>(d->snap.p);
   if (P.use_lr)
     CK(timed(d, kStCopy, [&] {
          return cudaMemcpyAsync(d->lr_pre.p, cur, pic_bytes, cudaMemcpyDeviceToDevice, st);
        }), "pre-CDEF copy");
-  if (!P.cdef.empty()) {
+  if ((P.n_cdef != 0)) {
     CK(timed(d, kStCopy, [&] {
          return cudaMemcpyAsync(snap, cur, pic_bytes, cudaMemcpyDeviceToDevice, st);
        }), "CDEF snapshot");
     CK(timed(d, kStCdef, [&] {
          return launch_cdef(snap, cur, reinterpret_cast<const CdefRec*>(ar + pl->o_cdef),
-                            static_cast<int>(P.cdef.size()), P.cdef_grid_w, P.cdef_grid_n,
+                            static_cast<int>(P.n_cdef), P.cdef_grid_w, P.cdef_grid_n,
                             P.cdef_search_any,
                             reinterpret_cast<const unsigned*>(ar + pl->o_cdef_search),
-                            static_cast<int>(P.cdef_search.size()),
+                            static_cast<int>(P.n_cdef_search),
                             static_cast<int*>(d->cdef_search.p), L, st);
        }), "CDEF");
     ++launches;
@@ -1800,7 +1953,7 @@ void recycle_plan(av1b_decoder* d, av1b_plan* pl) {
 
 /* Waits for the frame in flight and checks its status word. */
 int finish_frame(av1b_decoder* d) {
-  CK(cudaStreamSynchronize(d->stream), "frame sync");
+  CK(wait_stream(d), "frame sync");
   collect_profile(d);
   if (d->stats_pending) {
     float ms_recon = 0, ms_filter = 0;
@@ -1870,18 +2023,30 @@ int av1b_decoder_create(int device, size_t hbm_budget_bytes, av1b_decoder** out)
             cudaHostAlloc(reinterpret_cast<void**>(&d->status_host), 64, cudaHostAllocDefault) == cudaSuccess;
   for (int i = 0; ok && i < 3; ++i) ok = cudaEventCreate(&d->ev[i]) == cudaSuccess;
   ok = ok && cudaStreamCreateWithFlags(&d->aux, cudaStreamNonBlocking) == cudaSuccess &&
-       cudaStreamCreateWithFlags(&d->upload, cudaStreamNonBlocking) == cudaSuccess &&
        cudaEventCreateWithFlags(&d->ev_fork, cudaEventDisableTiming) == cudaSuccess &&
-       cudaEventCreateWithFlags(&d->ev_join, cudaEventDisableTiming) == cudaSuccess;
+       cudaEventCreateWithFlags(&d->ev_join, cudaEventDisableTiming) == cudaSuccess &&
+       cudaEventCreateWithFlags(&d->ev_block, cudaEventDisableTiming | cudaEventBlockingSync) ==
+           cudaSuccess;
   if (!ok) {
     av1b_decoder_destroy(d);
     return AV1B_ERR_CUDA;
   }
   *d->status_host = 0;
   {
+    /* two planners: one plan at a time uses all cores but the one left to
+     * the thread that drives the device; two plans at once share them */
     const unsigned hc = std::thread::hardware_concurrency();
-    d->pool = new WorkPool(static_cast<int>(std::min(16u, std::max(1u, hc))));
-    d->scratch = new PlanScratch;
+    const int threads = static_cast<int>(std::min(16u, std::max(2u, hc) - 1));
+    d->planners.resize(2);
+    for (auto& q : d->planners) {
+      q.pool = new WorkPool(threads);
+      q.scratch = new PlanScratch;
+      q.lists = new PlanLists;
+      if (cudaStreamCreateWithFlags(&q.upload, cudaStreamNonBlocking) != cudaSuccess) {
+        av1b_decoder_destroy(d);
+        return AV1B_ERR_CUDA;
+      }
+    }
   }
   d->own_plan = new av1b_plan;
   d->own_plan->owned_by_decoder = true;
@@ -1896,12 +2061,16 @@ int av1b_decoder_destroy(av1b_decoder* d) {
   if (d->own_plan) release_plan(d, d->own_plan);
   for (av1b_plan* pl : d->plan_pool) release_plan(d, pl);
   d->plan_pool.clear();
-  if (d->upload) {
-    cudaStreamSynchronize(d->upload);
-    cudaStreamDestroy(d->upload);
+  for (auto& q : d->planners) {
+    if (q.upload) {
+      cudaStreamSynchronize(q.upload);
+      cudaStreamDestroy(q.upload);
+    }
+    delete q.pool;
+    delete q.scratch;
+    delete q.lists;
   }
-  delete d->pool;
-  delete d->scratch;
+  d->planners.clear();
   for (int i = 0; i < 3; ++i)
     if (d->ev[i]) cudaEventDestroy(d->ev[i]);
   if (d->aux) {
@@ -1910,6 +2079,7 @@ int av1b_decoder_destroy(av1b_decoder* d) {
   }
   if (d->ev_fork) cudaEventDestroy(d->ev_fork);
   if (d->ev_join) cudaEventDestroy(d->ev_join);
+  if (d->ev_block) cudaEventDestroy(d->ev_block);
   if (d->status_host) cudaFreeHost(d->status_host);
   DevBuf* bufs[] = {&d->cur, &d->snap, &d->lr_pre, &d->lr_pre_up, &d->lr_cdef, &d->disp,
                     &d->slot_ptr_dev, &d->arena, &d->coef, &d->residual, &d->done,
@@ -2072,7 +2242,7 @@ static int to_nv12_impl(av1b_decoder* d, int slot, size_t pitch, uint8_t* dst, s
      "NV12 pack");
   if (!device_dst) {
     CK(cudaMemcpyAsync(dst, target, bytes, cudaMemcpyDeviceToHost, d->stream), "NV12 read back");
-    CK(cudaStreamSynchronize(d->stream), "NV12 sync");
+    CK(wait_stream(d), "NV12 sync");
     collect_profile(d);
   }
   /* the device variant stays queued on the decoder's stream */
@@ -2102,7 +2272,7 @@ int av1b_to_rgb(av1b_decoder* d, int slot, int matrix, int range, uint8_t* dst, 
   CK(timed(d, kStRgb, [&] { return launch_rgb(pic, static_cast<uint8_t*>(d->rgb.p), d->L, m, d->stream); }),
      "RGB pack");
   CK(cudaMemcpyAsync(dst, d->rgb.p, bytes, cudaMemcpyDeviceToHost, d->stream), "RGB read back");
-  CK(cudaStreamSynchronize(d->stream), "RGB sync");
+  CK(wait_stream(d), "RGB sync");
   collect_profile(d);
   return AV1B_OK;
 }
@@ -2169,7 +2339,7 @@ int av1b_set_profiling(av1b_decoder* d, int on) {
   if (!d) return AV1B_ERR_ARG;
   std::lock_guard<std::mutex> lk(d->mu);
   d->profiling = on != 0;
-  for (int i = 0; i < 16; ++i) {
+  for (int i = 0; i < kStageCount; ++i) {
     d->prof_ms[i] = 0;
     d->prof_n[i] = 0;
   }

@@ -90,21 +90,35 @@ AV1B_DEV void intra_edges(const IntraJob& j, const px_t* p, int stride, int* abo
   const int mid = 1 << (j.bitdepth - 1);
   const int alimit = mini(j.max_x, j.x + (j.have_ar ? 2 * j.w : j.w) - 1);
   const int llimit = mini(j.max_y, j.y + (j.have_bl ? 2 * j.h : j.h) - 1);
-  for (int i = lane; i < n; i += 32) {
-    int a, l;
-    if (!j.have_above) a = j.have_left ? ldpx(p - 1) : mid - 1;
-    else a = ldpx(p - stride + (mini(j.x + i, alimit) - j.x));
-    if (!j.have_left) l = j.have_above ? ldpx(p - stride) : mid + 1;
-    else l = ldpx(p + (mini(j.y + i, llimit) - j.y) * stride - 1);
-    above[i] = a;
-    left[i] = l;
+  /* every load of the edges (at most 128 + 128 samples and the corner) is
+   * issued before any is used: one round trip to L2, not one per sample */
+  int a[4], l[4], c = mid;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int i = lane + 32 * q;
+    a[q] = mid - 1;
+    l[q] = mid + 1;
+    if (i < n) {
+      if (!j.have_above) a[q] = j.have_left ? ldpx(p - 1) : mid - 1;
+      else a[q] = ldpx(p - stride + (mini(j.x + i, alimit) - j.x));
+      if (!j.have_left) l[q] = j.have_above ? ldpx(p - stride) : mid + 1;
+      else l[q] = ldpx(p + (mini(j.y + i, llimit) - j.y) * stride - 1);
+    }
   }
   if (lane == 0) {
-    int c;
     if (j.have_above && j.have_left) c = ldpx(p - stride - 1);
     else if (j.have_above) c = ldpx(p - stride);
     else if (j.have_left) c = ldpx(p - 1);
-    else c = mid;
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int i = lane + 32 * q;
+    if (i < n) {
+      above[i] = a[q];
+      left[i] = l[q];
+    }
+  }
+  if (lane == 0) {
     above[-1] = c;
     left[-1] = c;
   }
@@ -211,7 +225,7 @@ AV1B_DEV int dir_sample(const int* above, const int* left, int w, int h, int pan
 AV1B_DEV void intra_predict(const IntraJob& j, px_t* dst, int stride, const px_t* luma,
                             int luma_stride, const uint8_t* palette_map,
                             const int* palette_colors, int* scratch, int lane,
-                            const int* res = nullptr) {
+                            const int* res = nullptr, int* fi_pred = nullptr) {
   const int w = j.w, h = j.h, n = w * h;
   const int lw = ilog2(w);
   /* the reconstructed sample: the prediction plus, when the caller fused the
@@ -266,8 +280,9 @@ AV1B_DEV void intra_predict(const IntraJob& j, px_t* dst, int stride, const px_t
   if (j.filter_intra && w >= 4 && h >= 2) {
     /* recursive filter: 4x2 cells along anti-diagonals; a cell reads the row
      * above it (cells up-left and up) and the column left of it - the
-     * predictions of this block, so the residual is never fused here (the
-     * caller adds the transforms afterwards) */
+     * predictions of this block, kept in `fi_pred` (w x h, shared memory) so
+     * the recursion never round-trips through global memory; the block is
+     * written (with its residual when fused) once every cell is done */
     const int cw = w >> 2, ch = h >> 1;
     const signed char* taps = kFilterIntraTaps + j.fi_mode * 56;
     for (int d = 0; d < cw + ch - 1; ++d) {
@@ -280,17 +295,21 @@ AV1B_DEV void intra_predict(const IntraJob& j, px_t* dst, int stride, const px_t
         for (int t = 0; t < 5; ++t) {
           if (i2 == 0) pv[t] = above[(j4 << 2) + t - 1];
           else if (j4 == 0 && t == 0) pv[t] = left[(i2 << 1) - 1];
-          else pv[t] = ldpx(dst + ((i2 << 1) - 1) * stride + (j4 << 2) + t - 1);
+          else pv[t] = fi_pred[((i2 << 1) - 1) * w + (j4 << 2) + t - 1];
         }
         for (int t = 5; t < 7; ++t) {
           if (j4 == 0) pv[t] = left[(i2 << 1) + t - 5];
-          else pv[t] = ldpx(dst + ((i2 << 1) + t - 5) * stride + (j4 << 2) - 1);
+          else pv[t] = fi_pred[((i2 << 1) + t - 5) * w + (j4 << 2) - 1];
         }
         int pr = 0;
         for (int t = 0; t < 7; ++t) pr += taps[pos * 7 + t] * pv[t];
-        dst[((i2 << 1) + i1) * stride + (j4 << 2) + j1] = (px_t)clampi(rnd2(pr, 4), 0, j.maxv);
+        fi_pred[((i2 << 1) + i1) * w + (j4 << 2) + j1] = clampi(rnd2(pr, 4), 0, j.maxv);
       }
       __syncwarp();
+    }
+    for (int k = lane; k < n; k += 32) {
+      const int i = k >> lw, jj = k & (w - 1);
+      put(i, jj, fi_pred[k]);
     }
     return;
   }

@@ -502,6 +502,23 @@ AV1B_DEV void itx_warp(const ItxParams& p, const int* __restrict__ coef, int* tm
   __syncwarp();
 }
 
+/* One transform by a group of `step` lanes of a warp (`sub`: this lane's
+ * index in the group), several groups - several transforms of one size class
+ * - per warp. Every lane of the warp takes both barriers, active or not.
+ * `res` non-null: the residual goes there (w * h, row-major) instead of into
+ * the picture. */
+template <bool CG>
+AV1B_DEV void itx_group(const ItxParams& p, const int* __restrict__ coef, int* tmp, px_t* dst,
+                        int stride, int maxv, int* res, int sub, int step, bool active) {
+  const int w = 1 << p.lw, h = 1 << p.lh;
+  if (active)
+    for (int y = sub; y < h; y += step) itx_row_dispatch(p, coef, y, tmp);
+  __syncwarp();
+  if (active)
+    for (int x = sub; x < w; x += step) itx_col_dispatch<CG>(p, tmp, x, dst, stride, maxv, res);
+  __syncwarp();
+}
+
 /* The 2-D transform alone: the residual (before the add and the clip) into
  * `res`, w * h row-major. */
 AV1B_DEV void itx_warp_residual(const ItxParams& p, const int* __restrict__ coef, int* tmp, int* res,

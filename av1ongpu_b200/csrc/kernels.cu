@@ -32,11 +32,12 @@
 namespace av1b {
 
 /* ---- helpers --------------------------------------------------------------------- */
-__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+__device__ __forceinline__ unsigned ld_relaxed(const unsigned* p) {
   unsigned v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
+__device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 __device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
   asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
@@ -237,31 +238,45 @@ __device__ void apply_tx(const FrameArgs& a, const BlockRec& b, const TxRec& tx,
   itx_warp<CG>(p, a.coef + tx.coef_off, tmp, dst, g.stride, a.maxv, lane);
 }
 
-/* Inverse transforms, one warp per transform: those of phase A blocks add
- * into the picture; those of phase B blocks leave their residual in the
- * precomputed buffer, so the dependency-scheduled kernel only predicts and
- * adds (the residual does not depend on the prediction). */
-__global__ void k_itx(const __grid_constant__ FrameArgs a) {
+/* Inverse transforms, in batches of one size class: a warp runs 32 / S
+ * transforms whose longer side is S (S = 4, 8, 16, 32; one of 64), one lane
+ * group of S lanes each, so a 4x4 transform no longer leaves 28 lanes idle.
+ * The planner sorts the transforms by class and kind, so the groups of a
+ * warp mostly take the same path. Those of phase A blocks add into the
+ * picture; those of phase B blocks leave their residual in the precomputed
+ * buffer, so the dependency-scheduled kernel only predicts and adds (the
+ * residual does not depend on the prediction). Raw residual blocks (class
+ * 7) add with the whole warp. */
+__global__ void __launch_bounds__(128) k_itx(const __grid_constant__ FrameArgs a) {
   extern __shared__ int smem[];
   const int wib = threadIdx.x >> 5;
   const int warp = blockIdx.x * (blockDim.x >> 5) + wib;
   const int lane = threadIdx.x & 31;
-  if (warp >= a.n_itx) return;
-  const int2 t = a.itx_jobs[warp];
-  const BlockRec& b = a.blocks[t.x];
-  const TxRec& tx = a.txs[t.y];
-  if (tx.pre_off >= 0) {
-    ItxParams p;
-    p.lw = tx.log2w;
-    p.lh = tx.log2h;
-    p.type = tx.type;
-    p.lossless = b.lossless;
-    p.row_shift = tx.row_shift;
-    p.bitdepth = a.L.bit_depth;
-    itx_warp_residual(p, a.coef + tx.coef_off, smem + wib * 4096, a.pre_res + tx.pre_off, lane);
+  if (warp >= a.n_itx_batches) return;
+  const int4 bt = a.itx_batches[warp];   /* first job, jobs, log2 of the class */
+  if (bt.z == 7) {
+    const int2 t = a.itx_jobs[bt.x];
+    apply_tx<false>(a, a.blocks[t.x], a.txs[t.y], smem + wib * 4096, lane);
     return;
   }
-  apply_tx<false>(a, b, tx, smem + wib * 4096, lane);
+  const int S = 1 << bt.z, step = S < 32 ? S : 32;
+  const int g = lane / step, sub = lane - g * step;
+  const bool active = g < bt.y;
+  const int2 t = a.itx_jobs[bt.x + (active ? g : 0)];
+  const BlockRec& b = a.blocks[t.x];
+  const TxRec& tx = a.txs[t.y];
+  ItxParams p;
+  p.lw = tx.log2w;
+  p.lh = tx.log2h;
+  p.type = tx.type;
+  p.lossless = b.lossless;
+  p.row_shift = tx.row_shift;
+  p.bitdepth = a.L.bit_depth;
+  int* tmp = smem + wib * 4096 + (S <= 32 ? g * S * S : 0);
+  const PlaneGeom& gm = a.L.p[b.plane];
+  px_t* dst = a.cur + gm.off + (b.y + tx.y) * gm.stride + b.x + tx.x;
+  int* res = tx.pre_off >= 0 ? a.pre_res + tx.pre_off : nullptr;
+  itx_group<false>(p, a.coef + tx.coef_off, tmp, dst, gm.stride, a.maxv, res, sub, step, active);
 }
 
 /* ---- phase B -------------------------------------------------------------------------- */
@@ -271,22 +286,36 @@ __global__ void k_itx(const __grid_constant__ FrameArgs a) {
  * the frame has failed and the kernel only has to run to its end. */
 __device__ bool bounded_wait(const unsigned* flag, unsigned want, int* status,
                              unsigned long long limit_ns) {
-  if (ld_acquire(flag) == want) return true;
-  const unsigned long long t0 = global_ns();
-  while (ld_acquire(flag) != want) {
-    if (ld_acquire(reinterpret_cast<const unsigned*>(status)) & AV1B_STATUS_TIMEOUT) return false;
-    __nanosleep(100);
-    if (global_ns() - t0 > limit_ns) {
-      atomicOr(status, AV1B_STATUS_TIMEOUT);
-      return false;
-    }
+  /* relaxed polls and one acquire fence once the flag is seen (the acquire
+   * pattern); the status word and the clock are read every 16th poll, and the
+   * pause between polls backs off to 256 ns, so a thousand waiting warps load
+   * the memory system little while the warp whose flag was just set notices
+   * within a poll */
+  if (ld_relaxed(flag) == want) {
+    fence_acq_rel();
+    return true;
   }
+  const unsigned long long t0 = global_ns();
+  unsigned pause = 32;
+  for (unsigned it = 1;; ++it) {
+    if (ld_relaxed(flag) == want) break;
+    if ((it & 15) == 0) {
+      if (ld_relaxed(reinterpret_cast<const unsigned*>(status)) & AV1B_STATUS_TIMEOUT) return false;
+      if (global_ns() - t0 > limit_ns) {
+        atomicOr(status, AV1B_STATUS_TIMEOUT);
+        return false;
+      }
+    }
+    __nanosleep(pause);
+    if (pause < 256) pause <<= 1;
+  }
+  fence_acq_rel();
   return true;
 }
 
 /* Waits until block `o` is reconstructed. Returns false on timeout. */
 __device__ bool wait_block(const FrameArgs& a, int o) {
-  return bounded_wait(a.done + o, a.epoch, a.status, a.wait_ns);
+  return bounded_wait(a.done + (size_t)o * AV1B_FLAG_STRIDE, a.epoch, a.status, a.wait_ns);
 }
 
 /* A wait on a flag nothing sets: the failure-detection self test. */
@@ -321,8 +350,7 @@ __global__ void __launch_bounds__(128) k_units(const __grid_constant__ FrameArgs
     const BlockRec b = a.blocks[bi];
     const int p = b.plane;
     const PlaneGeom& g = a.L.p[p];
-    const bool fused = b.kind == AV1B_U_INTRA && b.fuse_res &&
-                       !(b.fi_mode >= 0 && b.w >= 4 && b.h >= 2);
+    const bool fused = b.kind == AV1B_U_INTRA && b.fuse_res;
 
     /* the residual image, before the wait */
     if (fused) {
@@ -339,9 +367,11 @@ __global__ void __launch_bounds__(128) k_units(const __grid_constant__ FrameArgs
       }
     }
 
-    /* the blocks this one reads from */
+    /* the blocks this one reads from: each lane's acquire load of a done flag
+     * orders the samples that block published before that lane's later
+     * reads, and the warp barrier extends the order to every lane (all
+     * picture reads go through L2, never a stale L1 line) */
     for (int k = lane; k < b.dep_count; k += 32) wait_block(a, a.deps[b.dep_first + k]);
-    __threadfence();
     __syncwarp();
 
     px_t* dst = a.cur + g.off + b.y * g.stride + b.x;
@@ -370,9 +400,11 @@ __global__ void __launch_bounds__(128) k_units(const __grid_constant__ FrameArgs
       j.palette = b.palette;
       j.palette_off = b.palette_off;
       j.palette_stride = b.palette_stride;
+      /* filter intra (at most 32x32) keeps its predictions after the
+       * residual image: tmp[1024 ..] */
       intra_predict(j, dst, g.stride, a.cur + a.L.p[0].off, a.L.p[0].stride, a.palette_map,
                     a.palette_colors + 8 * b.palette_color_idx, edges, lane,
-                    fused ? tmp : nullptr);
+                    fused ? tmp : nullptr, tmp + 1024);
     } else {
       InterJob j;
       make_inter_job(a, b, &j);
@@ -389,10 +421,11 @@ __global__ void __launch_bounds__(128) k_units(const __grid_constant__ FrameArgs
     if (!fused)
       for (int t = 0; t < b.tx_count; ++t) apply_tx<true>(a, b, a.txs[b.tx_first + t], tmp, lane);
 
-    /* publish */
-    __threadfence();
+    /* publish: the barrier orders every lane's stores before lane 0's
+     * release, whose fence (cumulative) makes them visible at GPU scope to
+     * any warp that acquires the flag */
     __syncwarp();
-    if (lane == 0) st_release(a.done + bi, a.epoch);
+    if (lane == 0) st_release(a.done + (size_t)bi * AV1B_FLAG_STRIDE, a.epoch);
   }
 }
 
@@ -1061,7 +1094,8 @@ cudaError_t launch_recon_stage(int stage, const FrameArgs& a, int n_sm, cudaStre
         k_inter<<<cdiv(a.n_inter_tiles, 4), 128, 0, s>>>(a);
       break;
     case 2:
-      if (a.n_itx > 0) k_itx<<<cdiv(a.n_itx, 4), 128, 4 * 4096 * sizeof(int), s>>>(a);
+      if (a.n_itx_batches > 0)
+        k_itx<<<cdiv(a.n_itx_batches, 4), 128, 4 * 4096 * sizeof(int), s>>>(a);
       break;
     default:
       if (a.n_units > 0) {

@@ -15,6 +15,11 @@ namespace av1b {
 #define AV1B_STATUS_TIMEOUT 1   /* a dependency wait gave up */
 
 /* Everything the reconstruction kernels read, by value. */
+/* Done flags sit 128 bytes apart: the blocks in flight are neighbours in
+ * coding order, and flags sharing lines would pile every poll of the frontier
+ * onto a few L2 slices, slowing every other access there. */
+#define AV1B_FLAG_STRIDE 32
+
 struct FrameArgs {
   Layout L;
   px_t* cur;                    /* the picture being reconstructed */
@@ -28,7 +33,8 @@ struct FrameArgs {
   const int* residual;
   const uint8_t* palette_map;
   const int* palette_colors;    /* 8 per palette block */
-  unsigned* done;               /* per block: == epoch once reconstructed (phase B) */
+  unsigned* done;               /* per block, AV1B_FLAG_STRIDE apart: == epoch once
+                                   reconstructed (phase B) */
   unsigned epoch;
   const int* units;             /* phase B block indices, claim order */
   const int* deps;              /* the phase B blocks each phase B block waits for */
@@ -39,6 +45,8 @@ struct FrameArgs {
   const int2* itx_jobs;         /* phase A: (block, transform); the transforms of
                                    phase B blocks compute their residual ahead */
   int n_itx;
+  const int4* itx_batches;      /* (first job, jobs, log2 size class or 7 raw) */
+  int n_itx_batches;
   int* pre_res;                 /* residuals computed ahead (TxRec::pre_off) */
   int* status;
   int maxv;

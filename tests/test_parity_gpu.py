@@ -166,14 +166,14 @@ def test_planned_decode_matches_direct(av1b, dec):
         dec.release_reference(s)
 
 
-def test_planning_on_another_thread(av1b, dec):
-    """A planner thread plans frame k + 1 (validation, records, uploads) while
-    frame k decodes and packs NV12 on the calling thread - the pipelined use
-    of plan_frame / decode_reference_planned - and every frame's NV12 equals
-    the one-call decode's. Plans are recycled through the decoder's pool."""
-    import queue
-    import threading
-    blobs = [av1b.synth_frame(2, 4, 77, k) for k in range(8)]
+def test_planning_on_other_threads(av1b, dec):
+    """Two planner threads plan frames k + 1 .. k + 3 (validation, records,
+    uploads) while frame k decodes and packs NV12 on the calling thread - the
+    pipelined use of plan_frame / decode_reference_planned, with two planners
+    of the decoder busy at once - and every frame's NV12 equals the one-call
+    decode's. Plans are recycled through the decoder's pool."""
+    from concurrent.futures import ThreadPoolExecutor
+    blobs = [av1b.synth_frame(2, 4, 77, k) for k in range(10)]
     w, _, h, _, sx, sy = blobs[0].header
     pitch = (w + 63) // 64 * 64
     import refdec
@@ -185,27 +185,28 @@ def test_planning_on_another_thread(av1b, dec):
     for s in list(direct.slots.values()):
         dec.release_reference(s)
     ring = [dec.reserve_reference() for _ in range(4)]
-    plans = queue.Queue(maxsize=2)
 
-    def planner():
-        for k, b in enumerate(blobs):
-            d = b.get_refs()
-            b.set_refs([ring[(k - x) % 4] for x in d])
-            plans.put(dec.plan(b))
+    def plan(k):
+        b = blobs[k]
+        d = b.get_refs()
+        b.set_refs([ring[(k - x) % 4] for x in d])
+        try:
+            return dec.plan(b)
+        finally:
             b.set_refs(d)
 
-    th = threading.Thread(target=planner)
-    th.start()
-    try:
+    ahead = 3
+    with ThreadPoolExecutor(max_workers=2) as ex:
+        futs = {k: ex.submit(plan, k) for k in range(ahead)}
         for k in range(len(blobs)):
-            pl = plans.get(timeout=120)
+            pl = futs.pop(k).result(timeout=120)
+            if k + ahead < len(blobs):
+                futs[k + ahead] = ex.submit(plan, k + ahead)
             dec.decode_planned(pl, slot=ring[k % 4], keep=True, wait=False)
             got = dec.to_nv12(ring[k % 4], pitch, w, h)
             dec.free_plan(pl)
             assert np.array_equal(got, want[k]), k
         dec.sync()
-    finally:
-        th.join()
     for s in ring:
         dec.release_reference(s)
 
