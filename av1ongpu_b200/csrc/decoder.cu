@@ -355,6 +355,7 @@ struct Plan {
   pvec<DeblockRec> deblock_v, deblock_h;
   pvec<CdefRec> cdef;
   pvec<unsigned> cdef_search;     /* searches off the 8x8 grid: x | y << 16 */
+  int itx_class_first[8] = {0}, itx_class_count[8] = {0};  /* batches per class */
   int cdef_grid_w = 0, cdef_grid_n = 0;  /* the grid of 8x8 luma searches */
   bool cdef_search_any = false;          /* some record reads the grid */
   LrArgs lr{};
@@ -1010,6 +1011,7 @@ void plan_itx(const PlanCtx& c, Plan* P) {
   PlanLists& R = *P->R;
   const size_t n = R.itx_jobs.size();
   R.itx_batches.clear();
+  for (int k = 0; k < 8; ++k) P->itx_class_first[k] = P->itx_class_count[k] = 0;
   if (n == 0) return;
   PlanScratch& S = *c.scratch;
   constexpr int kKeys = 8 * 7 * 7 * 16;
@@ -1060,6 +1062,11 @@ void plan_itx(const PlanCtx& c, Plan* P) {
     while (e < n && e - i < per && scls[e] == cl) ++e;
     R.itx_batches.push_back(make_int4(static_cast<int>(i), static_cast<int>(e - i), cl, 0));
     i = e;
+  }
+  /* the batches of each class, for one launch per class */
+  for (size_t bi = 0; bi < R.itx_batches.size(); ++bi) {
+    const int cl = R.itx_batches[bi].z;
+    if (P->itx_class_count[cl]++ == 0) P->itx_class_first[cl] = static_cast<int>(bi);
   }
 }
 
@@ -1776,6 +1783,10 @@ int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, cons
   a.n_itx = static_cast<int>(P.n_itx);
   a.itx_batches = reinterpret_cast<const int4*>(ar + pl->o_itxb);
   a.n_itx_batches = static_cast<int>(P.n_itxb);
+  for (int k = 0; k < 8; ++k) {
+    a.itx_class_first[k] = P.itx_class_first[k];
+    a.itx_class_count[k] = P.itx_class_count[k];
+  }
   a.pre_res = static_cast<int*>(d->pre_res.p);
   a.maxv = maxv;
   a.scale_x = P.scale_x;

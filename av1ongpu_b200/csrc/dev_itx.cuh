@@ -519,6 +519,50 @@ AV1B_DEV void itx_group(const ItxParams& p, const int* __restrict__ coef, int* t
   __syncwarp();
 }
 
+/* The same for transforms whose longer side is 1 << CLS: only the three
+ * lengths that class holds (CLS - 2 .. CLS, the 4:1 shapes included) are
+ * instantiated, so a kernel for the small classes is not sized for the
+ * 64-point transforms' registers. */
+template <int LO, int HI>
+AV1B_DEV void itx_row_range(const ItxParams& p, const int* coef, int y, int* tmp) {
+  if constexpr (LO < HI) {
+    if (p.lw == LO) {
+      itx_row<LO>(p, coef, y, tmp);
+      return;
+    }
+    itx_row_range<LO + 1, HI>(p, coef, y, tmp);
+  } else {
+    itx_row<HI>(p, coef, y, tmp);
+  }
+}
+
+template <int LO, int HI, bool CG>
+AV1B_DEV void itx_col_range(const ItxParams& p, const int* tmp, int x, px_t* dst, int stride, int maxv,
+                            int* res) {
+  if constexpr (LO < HI) {
+    if (p.lh == LO) {
+      itx_col_add<LO, CG>(p, tmp, x, dst, stride, maxv, res);
+      return;
+    }
+    itx_col_range<LO + 1, HI, CG>(p, tmp, x, dst, stride, maxv, res);
+  } else {
+    itx_col_add<HI, CG>(p, tmp, x, dst, stride, maxv, res);
+  }
+}
+
+template <int CLS, bool CG>
+AV1B_DEV void itx_group_cls(const ItxParams& p, const int* __restrict__ coef, int* tmp, px_t* dst,
+                            int stride, int maxv, int* res, int sub, int step, bool active) {
+  constexpr int LO = CLS - 2 > 2 ? CLS - 2 : 2;
+  const int w = 1 << p.lw, h = 1 << p.lh;
+  if (active)
+    for (int y = sub; y < h; y += step) itx_row_range<LO, CLS>(p, coef, y, tmp);
+  __syncwarp();
+  if (active)
+    for (int x = sub; x < w; x += step) itx_col_range<LO, CLS, CG>(p, tmp, x, dst, stride, maxv, res);
+  __syncwarp();
+}
+
 /* The 2-D transform alone: the residual (before the add and the clip) into
  * `res`, w * h row-major. */
 AV1B_DEV void itx_warp_residual(const ItxParams& p, const int* __restrict__ coef, int* tmp, int* res,

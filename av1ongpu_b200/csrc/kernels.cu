@@ -241,42 +241,58 @@ __device__ void apply_tx(const FrameArgs& a, const BlockRec& b, const TxRec& tx,
 /* Inverse transforms, in batches of one size class: a warp runs 32 / S
  * transforms whose longer side is S (S = 4, 8, 16, 32; one of 64), one lane
  * group of S lanes each, so a 4x4 transform no longer leaves 28 lanes idle.
- * The planner sorts the transforms by class and kind, so the groups of a
- * warp mostly take the same path. Those of phase A blocks add into the
- * picture; those of phase B blocks leave their residual in the precomputed
- * buffer, so the dependency-scheduled kernel only predicts and adds (the
- * residual does not depend on the prediction). Raw residual blocks (class
- * 7) add with the whole warp. */
-__global__ void __launch_bounds__(128) k_itx(const __grid_constant__ FrameArgs a) {
+ * One launch per class (CLS = log2 S), each instantiating only its class's
+ * transform lengths: the small classes, most of the transforms, run with a
+ * fraction of the registers of the 64-point ones and so with many more warps
+ * in flight. The planner sorts the transforms by class, shape and type, so
+ * the groups of a warp mostly take the same path. Those of phase A blocks add
+ * into the picture; those of phase B blocks leave their residual in the
+ * precomputed buffer, so the dependency-scheduled kernel only predicts and
+ * adds (the residual does not depend on the prediction). Raw residual blocks
+ * (class 7) add with the whole warp. */
+template <int CLS>
+__global__ void __launch_bounds__(128) k_itx(const __grid_constant__ FrameArgs a, int first,
+                                             int count) {
   extern __shared__ int smem[];
+  constexpr int S = 1 << (CLS < 7 ? CLS : 5), STEP = S < 32 ? S : 32;
+  constexpr int PER_WARP = CLS >= 6 ? 4096 : 32 * S;   /* scratch ints a warp */
   const int wib = threadIdx.x >> 5;
-  const int warp = blockIdx.x * (blockDim.x >> 5) + wib;
+  const int bi = blockIdx.x * (blockDim.x >> 5) + wib;
   const int lane = threadIdx.x & 31;
-  if (warp >= a.n_itx_batches) return;
-  const int4 bt = a.itx_batches[warp];   /* first job, jobs, log2 of the class */
-  if (bt.z == 7) {
+  if (bi >= count) return;
+  const int4 bt = a.itx_batches[first + bi];   /* first job, jobs, class */
+  if constexpr (CLS == 7) {
     const int2 t = a.itx_jobs[bt.x];
     apply_tx<false>(a, a.blocks[t.x], a.txs[t.y], smem + wib * 4096, lane);
-    return;
+  } else {
+    const int g = lane / STEP, sub = lane - g * STEP;
+    const bool active = g < bt.y;
+    const int2 t = a.itx_jobs[bt.x + (active ? g : 0)];
+    const BlockRec& b = a.blocks[t.x];
+    const TxRec& tx = a.txs[t.y];
+    ItxParams p;
+    p.lw = tx.log2w;
+    p.lh = tx.log2h;
+    p.type = tx.type;
+    p.lossless = b.lossless;
+    p.row_shift = tx.row_shift;
+    p.bitdepth = a.L.bit_depth;
+    int* tmp = smem + wib * PER_WARP + (S <= 32 ? g * S * S : 0);
+    const PlaneGeom& gm = a.L.p[b.plane];
+    px_t* dst = a.cur + gm.off + (b.y + tx.y) * gm.stride + b.x + tx.x;
+    int* res = tx.pre_off >= 0 ? a.pre_res + tx.pre_off : nullptr;
+    itx_group_cls<CLS, false>(p, a.coef + tx.coef_off, tmp, dst, gm.stride, a.maxv, res, sub, STEP,
+                              active);
   }
-  const int S = 1 << bt.z, step = S < 32 ? S : 32;
-  const int g = lane / step, sub = lane - g * step;
-  const bool active = g < bt.y;
-  const int2 t = a.itx_jobs[bt.x + (active ? g : 0)];
-  const BlockRec& b = a.blocks[t.x];
-  const TxRec& tx = a.txs[t.y];
-  ItxParams p;
-  p.lw = tx.log2w;
-  p.lh = tx.log2h;
-  p.type = tx.type;
-  p.lossless = b.lossless;
-  p.row_shift = tx.row_shift;
-  p.bitdepth = a.L.bit_depth;
-  int* tmp = smem + wib * 4096 + (S <= 32 ? g * S * S : 0);
-  const PlaneGeom& gm = a.L.p[b.plane];
-  px_t* dst = a.cur + gm.off + (b.y + tx.y) * gm.stride + b.x + tx.x;
-  int* res = tx.pre_off >= 0 ? a.pre_res + tx.pre_off : nullptr;
-  itx_group<false>(p, a.coef + tx.coef_off, tmp, dst, gm.stride, a.maxv, res, sub, step, active);
+}
+
+template <int CLS>
+static cudaError_t launch_itx_class(const FrameArgs& a, cudaStream_t s) {
+  const int first = a.itx_class_first[CLS], count = a.itx_class_count[CLS];
+  if (count <= 0) return cudaSuccess;
+  constexpr int per_warp = CLS == 7 || CLS >= 6 ? 4096 : 32 * (1 << CLS);
+  k_itx<CLS><<<(count + 3) / 4, 128, 4 * per_warp * sizeof(int), s>>>(a, first, count);
+  return cudaGetLastError();
 }
 
 /* ---- phase B -------------------------------------------------------------------------- */
@@ -549,15 +565,59 @@ __constant__ signed char kCdefDirs[8][2][2] = {
 __constant__ unsigned char kCdefUvDir[2][2][8] = {{{0, 1, 2, 3, 4, 5, 6, 7}, {1, 2, 2, 2, 3, 4, 6, 0}},
                                                   {{7, 0, 2, 4, 5, 6, 6, 6}, {0, 1, 2, 3, 4, 5, 6, 7}}};
 
-/* CDEF filter (av1gpu_kernels.h:2662-2775), one warp per block: the block and
- * its 2-sample halo staged in shared memory, one or two samples per lane. */
-__global__ void __launch_bounds__(128) k_cdef_warp(const px_t* __restrict__ src, px_t* dst,
-                                                   const CdefRec* recs, int n,
-                                                   const int* __restrict__ search,
-                                                   const __grid_constant__ Layout L) {
-  __shared__ int sw[4][12 * 12];
-  const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int ri = blockIdx.x * 4 + wib;
+/* CDEF filter (av1gpu_kernels.h:2662-2775), one half-warp per block: the
+ * block and its 2-sample halo staged in shared memory, then 4 samples a lane
+ * (luma 8x8) or 1 (4:2:0 chroma 4x4), so chroma blocks leave no lane idle.
+ * Everything per block is resolved once before the sample loop: the tap
+ * offsets of the three directions, each strength's damping shift (the
+ * constrain function's floor_log2), and whether every tap of the block lies
+ * inside the plane (then no per-tap bound checks). */
+__device__ __forceinline__ int cdef_cst(int diff, int th, int sh) {
+  const int m = absi(diff);
+  const int v = clampi(th - (m >> sh), 0, m);
+  return diff < 0 ? -v : v;
+}
+
+template <bool EDGE>
+__device__ __forceinline__ void cdef_samples(const int* win, px_t* d, int stride, int w, int h,
+                                             int hl, int x0, int y0, int pw, int ph,
+                                             const int (&oy)[6], const int (&ox)[6], int pri,
+                                             int psh, int sec, int ssh, int pt0, int pt1,
+                                             int maxv) {
+  for (int k = hl; k < w * h; k += 16) {
+    const int i = k >> (w == 8 ? 3 : (w == 4 ? 2 : 1)), j = k & (w - 1);
+    if (EDGE && (y0 + i >= ph || x0 + j >= pw)) continue;
+    const int x = win[(i + 2) * 12 + j + 2];
+    int sum = 0, lo = x, hi = x;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      const int tap = q == 0 ? pt0 : (q == 1 ? pt1 : (q & 1 ? 1 : 2));
+      const int th = q < 2 ? pri : sec, sh = q < 2 ? psh : ssh;
+#pragma unroll
+      for (int sg = -1; sg <= 1; sg += 2) {
+        const int dy = sg * oy[q], dx = sg * ox[q];
+        if (EDGE) {
+          const int px = x0 + j + dx, py = y0 + i + dy;
+          if (px < 0 || px >= pw || py < 0 || py >= ph) continue;
+        }
+        const int v = win[(i + 2 + dy) * 12 + j + 2 + dx];
+        if (th) sum += tap * cdef_cst(v - x, th, sh);
+        lo = mini(lo, v);
+        hi = maxi(hi, v);
+      }
+    }
+    d[i * stride + j] = (px_t)clampi(clampi(x + ((8 + sum - (sum < 0)) >> 4), lo, hi), 0, maxv);
+  }
+}
+
+__global__ void __launch_bounds__(128) k_cdef(const px_t* __restrict__ src, px_t* dst,
+                                              const CdefRec* recs, int n,
+                                              const int* __restrict__ search,
+                                              const __grid_constant__ Layout L) {
+  __shared__ int sw[8][12 * 12];
+  const int hw = threadIdx.x >> 4, hl = threadIdx.x & 15;
+  const unsigned hmask = 0xffffu << (threadIdx.x & 16);
+  const int ri = blockIdx.x * 8 + hw;
   if (ri >= n) return;
   const CdefRec r = recs[ri];
   const int p = r.plane;
@@ -566,10 +626,10 @@ __global__ void __launch_bounds__(128) k_cdef_warp(const px_t* __restrict__ src,
   const int bd = L.bit_depth, maxv = (1 << bd) - 1, cs = bd - 8;
   const int w = uv ? (8 >> L.ss_x) : 8, h = uv ? (8 >> L.ss_y) : 8;
   const int pw = g.grid_w, ph = g.grid_h;
-  int* win = sw[wib];
+  int* win = sw[hw];
   /* the block and its halo; rows and columns above or left of the buffer
    * clamp into it (taps outside the plane are never used) */
-  for (int k = lane; k < (h + 4) * (w + 4); k += 32) {
+  for (int k = hl; k < (h + 4) * (w + 4); k += 16) {
     const int i = k / (w + 4), j = k - i * (w + 4);
     const int y = maxi(r.y - 2 + i, 0), x = maxi(r.x - 2 + j, 0);
     win[i * 12 + j] = src[g.off + y * g.stride + x];
@@ -588,10 +648,10 @@ __global__ void __launch_bounds__(128) k_cdef_warp(const px_t* __restrict__ src,
       pri = var ? ((pri * (4 + vs) + 8) >> 4) : 0;
     }
   }
-  __syncwarp();
+  __syncwarp(hmask);
   px_t* d = dst + g.off + r.y * g.stride + r.x;
   if (pri == 0 && sec == 0) {
-    for (int k = lane; k < w * h; k += 32) {
+    for (int k = hl; k < w * h; k += 16) {
       const int i = k / w, j = k - i * w;
       if (r.y + i < ph && r.x + j < pw) d[i * g.stride + j] = (px_t)win[(i + 2) * 12 + j + 2];
     }
@@ -599,33 +659,24 @@ __global__ void __launch_bounds__(128) k_cdef_warp(const px_t* __restrict__ src,
   }
   const int ts = (pri >> cs) & 1;
   const int pt0 = ts ? 3 : 4, pt1 = ts ? 3 : 2;
-  for (int k = lane; k < w * h; k += 32) {
-    const int i = k / w, j = k - i * w;
-    if (r.y + i >= ph || r.x + j >= pw) continue;
-    const int x = win[(i + 2) * 12 + j + 2];
-    int sum = 0, lo = x, hi = x;
+  const int psh = pri ? maxi(0, damping - floor_log2(pri)) : 0;
+  const int ssh = sec ? maxi(0, damping - floor_log2(sec)) : 0;
+  /* taps: primary (dir) k = 0, 1; secondary (dir - 2, dir + 2) k = 0, 1 */
+  int oy[6], ox[6];
 #pragma unroll
-    for (int q = 0; q < 3; ++q) {
-      const int dd = q == 0 ? dir : (q == 1 ? (dir + 6) & 7 : (dir + 2) & 7);
-      const int th = q == 0 ? pri : sec;
-#pragma unroll
-      for (int t = 0; t < 2; ++t) {
-        const int oy = kCdefDirs[dd][t][0], ox = kCdefDirs[dd][t][1];
-        const int tap = q == 0 ? (t == 0 ? pt0 : pt1) : (t == 0 ? 2 : 1);
-#pragma unroll
-        for (int sg = -1; sg <= 1; sg += 2) {
-          const int dy = sg * oy, dx = sg * ox;
-          const int px = r.x + j + dx, py = r.y + i + dy;
-          if (px < 0 || px >= pw || py < 0 || py >= ph) continue;
-          const int v = win[(i + 2 + dy) * 12 + j + 2 + dx];
-          sum += tap * cdef_constrain(v - x, th, damping);
-          lo = mini(lo, v);
-          hi = maxi(hi, v);
-        }
-      }
-    }
-    d[i * g.stride + j] = (px_t)clampi(clampi(x + ((8 + sum - (sum < 0)) >> 4), lo, hi), 0, maxv);
+  for (int q = 0; q < 6; ++q) {
+    const int dd = q < 2 ? dir : (q < 4 ? (dir + 6) & 7 : (dir + 2) & 7);
+    const int t = q & 1;
+    oy[q] = kCdefDirs[dd][t][0];
+    ox[q] = kCdefDirs[dd][t][1];
   }
+  const bool interior = r.x >= 2 && r.y >= 2 && r.x + w + 2 <= pw && r.y + h + 2 <= ph;
+  if (interior)
+    cdef_samples<false>(win, d, g.stride, w, h, hl, r.x, r.y, pw, ph, oy, ox, pri, psh, sec, ssh,
+                        pt0, pt1, maxv);
+  else
+    cdef_samples<true>(win, d, g.stride, w, h, hl, r.x, r.y, pw, ph, oy, ox, pri, psh, sec, ssh,
+                       pt0, pt1, maxv);
 }
 
 /* ---- superres ------------------------------------------------------------------------- */
@@ -1094,8 +1145,13 @@ cudaError_t launch_recon_stage(int stage, const FrameArgs& a, int n_sm, cudaStre
         k_inter<<<cdiv(a.n_inter_tiles, 4), 128, 0, s>>>(a);
       break;
     case 2:
-      if (a.n_itx_batches > 0)
-        k_itx<<<cdiv(a.n_itx_batches, 4), 128, 4 * 4096 * sizeof(int), s>>>(a);
+      if (a.n_itx_batches > 0) {
+        cudaError_t e;
+        if ((e = launch_itx_class<2>(a, s)) != cudaSuccess || (e = launch_itx_class<3>(a, s)) != cudaSuccess ||
+            (e = launch_itx_class<4>(a, s)) != cudaSuccess || (e = launch_itx_class<5>(a, s)) != cudaSuccess ||
+            (e = launch_itx_class<6>(a, s)) != cudaSuccess || (e = launch_itx_class<7>(a, s)) != cudaSuccess)
+          return e;
+      }
       break;
     default:
       if (a.n_units > 0) {
@@ -1122,7 +1178,7 @@ cudaError_t launch_cdef(const px_t* src, px_t* dst, const CdefRec* recs, int n, 
   if (n_grid + n_extra > 0)
     k_cdef_search<<<cdiv(n_grid + n_extra, 128), 128, 0, s>>>(src, grid_w, grid_n, n_grid, extra_pos,
                                                                n_extra, search, L);
-  k_cdef_warp<<<cdiv(n, 4), 128, 0, s>>>(src, dst, recs, n, search, L);
+  k_cdef<<<cdiv(n, 8), 128, 0, s>>>(src, dst, recs, n, search, L);
   return cudaGetLastError();
 }
 
@@ -1173,7 +1229,11 @@ cudaError_t set_kernel_attributes() {
   cudaError_t e = cudaFuncSetAttribute(k_units, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        4 * (3 * AV1B_EDGE_LEN + 4096) * (int)sizeof(int));
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_itx, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  /* the two classes whose scratch passes the 48 KB default */
+  if ((e = cudaFuncSetAttribute(k_itx<6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                4 * 4096 * (int)sizeof(int))) != cudaSuccess)
+    return e;
+  return cudaFuncSetAttribute(k_itx<7>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               4 * 4096 * (int)sizeof(int));
 }
 

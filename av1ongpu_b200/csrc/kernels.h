@@ -47,6 +47,7 @@ struct FrameArgs {
   int n_itx;
   const int4* itx_batches;      /* (first job, jobs, log2 size class or 7 raw) */
   int n_itx_batches;
+  int itx_class_first[8], itx_class_count[8];   /* the batches of each class */
   int* pre_res;                 /* residuals computed ahead (TxRec::pre_off) */
   int* status;
   int maxv;
