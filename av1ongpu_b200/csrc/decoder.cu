@@ -346,6 +346,7 @@ struct PlanLists {
  * device memory, uploaded from the PlanLists). */
 struct Plan {
   PlanLists* R = nullptr;         /* while planning: the lists being built */
+  size_t n_tiles_simple = 0;      /* inter tiles the lean kernel takes (listed first) */
   size_t n_blocks = 0, n_units = 0, n_tiles = 0, n_itx = 0, n_itxb = 0, n_dbv = 0, n_dbh = 0,
          n_cdef = 0,
          n_cdef_search = 0;
@@ -423,7 +424,7 @@ struct BlockOut {
   std::vector<WarpRec> warps;
   std::vector<int> palette_colors;
   std::vector<int> units;
-  std::vector<int2> inter_tiles;
+  std::vector<int2> inter_tiles, inter_tiles_full;
   std::vector<int2> itx_jobs;
   size_t pre_res_pool = 0, coef_end = 0, res_end = 0;
   PlanErr err;
@@ -434,6 +435,7 @@ struct BlockOut {
     palette_colors.clear();
     units.clear();
     inter_tiles.clear();
+    inter_tiles_full.clear();
     itx_jobs.clear();
     pre_res_pool = coef_end = res_end = 0;
     err = PlanErr();
@@ -661,9 +663,14 @@ int plan_block(const PlanCtx& ctx, const av1b_frame_syntax& s, size_t bi, BlockR
   if (r.phase_b) {
     O->units.push_back(static_cast<int>(bi));
   } else {
+    /* translation-only blocks (no global warp, mask, or OBMC) take the lean
+     * prediction kernel */
+    const bool simple = !r.warp0 && !r.warp1 && !r.mask_warp0 && !r.mask_warp1 &&
+                        r.mask_kind == 0 && r.obmc_count == 0 && !r.interintra;
+    auto& tiles = simple ? O->inter_tiles : O->inter_tiles_full;
     for (int y0 = 0; y0 < b.h; y0 += 8)
       for (int x0 = 0; x0 < b.w; x0 += 16)
-        O->inter_tiles.push_back(make_int2(static_cast<int>(bi), x0 | (y0 << 16)));
+        tiles.push_back(make_int2(static_cast<int>(bi), x0 | (y0 << 16)));
   }
   return AV1B_OK;
 }
@@ -1110,8 +1117,8 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
       if (outs[i].err.code) return fail(d, outs[i].err.code, outs[i].err.msg);
     /* piece offsets into the frame's lists */
     std::vector<size_t> o_tx(pieces + 1, 0), o_obmc(pieces + 1, 0), o_warp(pieces + 1, 0),
-        o_pal(pieces + 1, 0), o_unit(pieces + 1, 0), o_tile(pieces + 1, 0), o_itx(pieces + 1, 0),
-        o_pre(pieces + 1, 0);
+        o_pal(pieces + 1, 0), o_unit(pieces + 1, 0), o_tile(pieces + 1, 0), o_tilef(pieces + 1, 0),
+        o_itx(pieces + 1, 0), o_pre(pieces + 1, 0);
     for (int i = 0; i < pieces; ++i) {
       const BlockOut& O = outs[i];
       o_tx[i + 1] = o_tx[i] + O.txs.size();
@@ -1120,6 +1127,7 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
       o_pal[i + 1] = o_pal[i] + O.palette_colors.size();
       o_unit[i + 1] = o_unit[i] + O.units.size();
       o_tile[i + 1] = o_tile[i] + O.inter_tiles.size();
+      o_tilef[i + 1] = o_tilef[i] + O.inter_tiles_full.size();
       o_itx[i + 1] = o_itx[i] + O.itx_jobs.size();
       o_pre[i + 1] = o_pre[i] + O.pre_res_pool;
       coef_end = std::max(coef_end, O.coef_end);
@@ -1133,7 +1141,9 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
     P->R->warps[0] = WarpRec{};
     P->R->palette_colors.resize(o_pal[pieces]);
     P->R->units.resize(o_unit[pieces]);
-    P->R->inter_tiles.resize(o_tile[pieces]);
+    /* the lean kernel's tiles first, then the rest */
+    P->R->inter_tiles.resize(o_tile[pieces] + o_tilef[pieces]);
+    P->n_tiles_simple = o_tile[pieces];
     P->R->itx_jobs.resize(o_itx[pieces]);
     P->pre_res_pool = o_pre[pieces];
     c.pool->run(pieces, [&](int i) {
@@ -1159,6 +1169,8 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
       std::copy(O.palette_colors.begin(), O.palette_colors.end(), P->R->palette_colors.begin() + o_pal[i]);
       std::copy(O.units.begin(), O.units.end(), P->R->units.begin() + o_unit[i]);
       std::copy(O.inter_tiles.begin(), O.inter_tiles.end(), P->R->inter_tiles.begin() + o_tile[i]);
+      std::copy(O.inter_tiles_full.begin(), O.inter_tiles_full.end(),
+                P->R->inter_tiles.begin() + o_tile[pieces] + o_tilef[i]);
       for (size_t k = 0; k < O.itx_jobs.size(); ++k) {
         int2 j = O.itx_jobs[k];
         j.y += dtx;
@@ -1779,6 +1791,7 @@ int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, cons
   a.status = reinterpret_cast<int*>(static_cast<uint8_t*>(d->status_q.p) + 64);
   a.inter_tiles = reinterpret_cast<const int2*>(ar + pl->o_tiles);
   a.n_inter_tiles = static_cast<int>(P.n_tiles);
+  a.n_inter_simple = static_cast<int>(P.n_tiles_simple);
   a.itx_jobs = reinterpret_cast<const int2*>(ar + pl->o_itx);
   a.n_itx = static_cast<int>(P.n_itx);
   a.itx_batches = reinterpret_cast<const int4*>(ar + pl->o_itxb);

@@ -125,6 +125,60 @@ __device__ void make_inter_job(const FrameArgs& a, const BlockRec& b, InterJob* 
 
 /* ---- phase A ------------------------------------------------------------------------ */
 
+/* Inter prediction of the translation-only blocks of phase A (no global
+ * warp, no mask, no OBMC - most inter blocks): one warp per 16x8 tile,
+ * each reference through mc_rect, then the average or distance-weighted
+ * blend. It carries none of the full kernel's state, so it runs with a
+ * fraction of its registers and many more warps in flight. */
+__global__ void __launch_bounds__(128) k_inter_simple(const __grid_constant__ FrameArgs a) {
+  __shared__ McScratch scr[4];
+  __shared__ int pred[4][2][8 * 16];
+  const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int warp = blockIdx.x * 4 + wib;
+  if (warp >= a.n_inter_simple) return;
+  const int2 t = a.inter_tiles[warp];
+  const BlockRec& b = a.blocks[t.x];
+  const int p = b.plane;
+  const PlaneGeom& g = a.L.p[p];
+  InterCtx c;
+  c.sub_x = p > 0 ? a.L.ss_x : 0;
+  c.sub_y = p > 0 ? a.L.ss_y : 0;
+  c.ref_w = g.out_w;
+  c.ref_h = g.out_h;
+  c.bitdepth = a.L.bit_depth;
+  c.scale_x = a.scale_x;
+  c.scale_y = a.scale_y;
+  const int x0 = t.y & 0xffff, y0 = t.y >> 16;
+  const int tw = mini(16, b.w - x0), th = mini(8, b.h - y0);
+  const int nref = b.compound ? 2 : 1;
+  for (int r = 0; r < nref; ++r) {
+    int* pr = pred[wib][r];
+    const px_t* ref = ref_plane(a, b.ref_slot[r], p);
+    if (!mc_rect(c, ref, g.stride, b.x, b.y, b.w, b.h, b.mv[r][0], b.mv[r][1], b.filt, b.filt_v,
+                 b.compound != 0, x0, y0, tw, th, scr[wib], pr, lane)) {
+      for (int k = lane; k < tw * th; k += 32) {
+        const int yy = k / tw, xx = k - yy * tw;
+        pr[yy * 16 + xx] = mc_tap(c, ref, g.stride, b.x, b.y, b.w, b.h, b.mv[r][0], b.mv[r][1],
+                                  b.filt, b.filt_v, x0 + xx, y0 + yy, b.compound != 0);
+      }
+      __syncwarp();
+    }
+  }
+  px_t* dst = a.cur + g.off + (b.y + y0) * g.stride + b.x + x0;
+  const int post = 7 - (c.bitdepth >= 12 ? 5 : 3);
+  for (int k = lane; k < tw * th; k += 32) {
+    const int yy = k / tw, xx = k - yy * tw;
+    const int v0 = pred[wib][0][yy * 16 + xx];
+    int out = v0;
+    if (b.compound == 1) {
+      out = (v0 + pred[wib][1][yy * 16 + xx] + (1 << post)) >> (1 + post);
+    } else if (b.compound) {
+      out = (b.w0 * v0 + b.w1 * pred[wib][1][yy * 16 + xx] + (1 << (3 + post))) >> (4 + post);
+    }
+    dst[yy * g.stride + xx] = (px_t)clampi(out, 0, a.maxv);
+  }
+}
+
 /* Inter prediction of phase A blocks: one warp per 16x8 tile. Translation
  * predictions (and OBMC strips) go through mc_rect, warped ones per sample;
  * the composition and the OBMC blends run per sample on registers. */
@@ -132,7 +186,7 @@ __global__ void __launch_bounds__(128) k_inter(const __grid_constant__ FrameArgs
   __shared__ McScratch scr[4];
   __shared__ int pred[4][2][8 * 16];
   const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int warp = blockIdx.x * 4 + wib;
+  const int warp = a.n_inter_simple + blockIdx.x * 4 + wib;
   if (warp >= a.n_inter_tiles) return;
   const int2 t = a.inter_tiles[warp];
   const BlockRec& b = a.blocks[t.x];
@@ -1142,7 +1196,11 @@ cudaError_t launch_recon_stage(int stage, const FrameArgs& a, int n_sm, cudaStre
   switch (stage) {
     case 1:
       if (a.n_inter_tiles > 0)
-        k_inter<<<cdiv(a.n_inter_tiles, 4), 128, 0, s>>>(a);
+      {
+        if (a.n_inter_simple > 0) k_inter_simple<<<cdiv(a.n_inter_simple, 4), 128, 0, s>>>(a);
+        const int rest = a.n_inter_tiles - a.n_inter_simple;
+        if (rest > 0) k_inter<<<cdiv(rest, 4), 128, 0, s>>>(a);
+      }
       break;
     case 2:
       if (a.n_itx_batches > 0) {

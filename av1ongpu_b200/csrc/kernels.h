@@ -42,6 +42,7 @@ struct FrameArgs {
   unsigned* queue;
   const int2* inter_tiles;      /* phase A: (block, x0 | y0 << 16) */
   int n_inter_tiles;
+  int n_inter_simple;           /* the first ones: translation-only blocks */
   const int2* itx_jobs;         /* phase A: (block, transform); the transforms of
                                    phase B blocks compute their residual ahead */
   int n_itx;
