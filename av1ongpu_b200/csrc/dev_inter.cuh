@@ -249,6 +249,59 @@ AV1B_DEV int warp_tap(int sub_x, int sub_y, int ref_w, int ref_h, const WarpRec&
   return (acc + (1 << (r1 - 1))) >> r1;
 }
 
+/* One 8x8 block of a globally warped prediction, for one warp, separable
+ * like the reference's per-block warp (av1gpu_kernels.h:1919-1958): the
+ * 15x15 reference window around the block's projected centre staged in
+ * shared memory, the horizontal 8-tap filter (its phase from alpha and beta)
+ * for the 15 rows x 8 columns the block reads, rounded by InterRound0, then
+ * the vertical filter (phase from gamma and delta) - the same integers as
+ * warp_tap, which computes them again for every output sample. (bx, by): the
+ * 8x8 block's offset in the prediction block; out: rows of `out_stride`. */
+template <bool CG = false>
+AV1B_DEV void warp_block8(int sub_x, int sub_y, int ref_w, int ref_h, const WarpRec& m,
+                          const px_t* ref, int stride, int base_x, int base_y, int bx, int by,
+                          int bitdepth, int compound, McScratch& s, int* out, int out_stride,
+                          int ow, int oh, int lane) {
+  const long long src_x = (long long)((base_x + bx + 4) << sub_x);
+  const long long src_y = (long long)((base_y + by + 4) << sub_y);
+  const long long dst_x = (long long)m.params[2] * src_x + (long long)m.params[3] * src_y + m.params[0];
+  const long long dst_y = (long long)m.params[4] * src_x + (long long)m.params[5] * src_y + m.params[1];
+  const long long x4 = dst_x >> sub_x, y4 = dst_y >> sub_y;
+  const int ix4 = (int)(x4 >> 16), sx4 = (int)(x4 & 0xffff);
+  const int iy4 = (int)(y4 >> 16), sy4 = (int)(y4 & 0xffff);
+  int r0, r1;
+  rounds(bitdepth, compound, &r0, &r1);
+  /* window rows iy4 - 7 .. iy4 + 7, columns ix4 - 7 .. ix4 + 7 */
+  for (int k = lane; k < 15 * 15; k += 32) {
+    const int r = k / 15, c = k - r * 15;
+    s.win[r * 16 + c] = fetch<CG>(ref, stride, ix4 - 7 + c, iy4 - 7 + r, ref_w - 1, ref_h - 1);
+  }
+  __syncwarp();
+  /* H[r][c]: row r - 7, column offset i2 = c - 4 */
+  for (int k = lane; k < 15 * 8; k += 32) {
+    const int r = k >> 3, c = k & 7;
+    const int offs_x = warp_offs(sx4 + m.abcd[0] * (c - 4) + m.abcd[1] * (r - 7));
+    const short* f = kWarpedFilters + offs_x * 8;
+    const int* w = s.win + r * 16 + c;
+    int sum = 0;
+#pragma unroll
+    for (int t = 0; t < 8; ++t) sum += f[t] * w[t];
+    s.mid[r * 8 + c] = (sum + (1 << (r0 - 1))) >> r0;
+  }
+  __syncwarp();
+  for (int k = lane; k < 64; k += 32) {
+    const int i = k >> 3, j = k & 7;
+    if (i >= oh || j >= ow) continue;
+    const int offs_y = warp_offs(sy4 + m.abcd[2] * (j - 4) + m.abcd[3] * (i - 4));
+    const short* f = kWarpedFilters + offs_y * 8;
+    int acc = 0;
+#pragma unroll
+    for (int t = 0; t < 8; ++t) acc += f[t] * s.mid[(i + t) * 8 + j];
+    out[i * out_stride + j] = (acc + (1 << (r1 - 1))) >> r1;
+  }
+  __syncwarp();
+}
+
 /* ---- masks ------------------------------------------------------------------- */
 
 AV1B_DEV int wedge_px(int dir, int xoff, int yoff, int flip, int i, int j) {

@@ -209,8 +209,16 @@ __global__ void __launch_bounds__(128) k_inter(const __grid_constant__ FrameArgs
   const int nref = j.compound ? 2 : 1;
   for (int r = 0; r < nref; ++r) {
     int* pr = pred[wib][r];
-    const bool ok = !j.warp[r] &&
-                    mc_rect(j.ctx, j.ref[r], j.ref_stride, j.x, j.y, j.w, j.h, j.mv[r][0],
+    if (j.warp[r]) {
+      /* the tile is one or two whole 8x8 warp blocks (x0 is a multiple of
+       * 16, y0 of 8) */
+      for (int bx = 0; bx < tw; bx += 8)
+        warp_block8(j.ctx.sub_x, j.ctx.sub_y, j.ctx.ref_w, j.ctx.ref_h, *j.model[r], j.ref[r],
+                    j.ref_stride, j.x, j.y, x0 + bx, y0, j.ctx.bitdepth, j.compound != 0, scr[wib],
+                    pr + bx, 16, mini(8, tw - bx), th, lane);
+      continue;
+    }
+    const bool ok = mc_rect(j.ctx, j.ref[r], j.ref_stride, j.x, j.y, j.w, j.h, j.mv[r][0],
                             j.mv[r][1], j.filt, j.filt_v, j.compound != 0, x0, y0, tw, th, scr[wib],
                             pr, lane);
     if (!ok) {
