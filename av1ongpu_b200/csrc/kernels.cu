@@ -182,7 +182,7 @@ __global__ void __launch_bounds__(128) k_inter_simple(const __grid_constant__ Fr
 /* Inter prediction of phase A blocks: one warp per 16x8 tile. Translation
  * predictions (and OBMC strips) go through mc_rect, warped ones per sample;
  * the composition and the OBMC blends run per sample on registers. */
-__global__ void __launch_bounds__(128) k_inter(const __grid_constant__ FrameArgs a) {
+__global__ void __launch_bounds__(128, 4) k_inter(const __grid_constant__ FrameArgs a) {
   __shared__ McScratch scr[4];
   __shared__ int pred[4][2][8 * 16];
   const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
