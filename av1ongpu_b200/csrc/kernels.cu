@@ -951,13 +951,18 @@ __global__ void __launch_bounds__(256) k_lr_tile(const px_t* __restrict__ cdef,
 __global__ void __launch_bounds__(256) k_grain_template(GrainState* gs, GrainParamsDev prm,
                                                         const uint16_t* orbit,
                                                         const uint16_t* pos) {
+  /* the templates live in shared memory while the auto-regressive wavefront
+   * runs (hundreds of dependent steps: every tap a shared-memory read, not a
+   * global one) and are written out at the end */
+  __shared__ short s_luma[82 * 73], s_cb[82 * 73], s_cr[82 * 73];
   const int tid = threadIdx.x;
   const int bd = prm.bitdepth;
   const int shift = 12 - bd + prm.grain_scale_shift;
   const int gmin = -(128 << (bd - 8)), gmax = (256 << (bd - 8)) - 1 - (128 << (bd - 8));
   const int cw = gs->chroma_w, ch = gs->chroma_h;
-  short* cb = gs->cb;
-  short* cr = gs->cr;
+  short* luma = s_luma;
+  short* cb = s_cb;
+  short* cr = s_cr;
   /* Gaussian fill */
   for (int k = tid; k < 82 * 73; k += blockDim.x) {
     int g = 0;
@@ -965,7 +970,7 @@ __global__ void __launch_bounds__(256) k_grain_template(GrainState* gs, GrainPar
       const int st = lfsr_after(orbit, pos, (unsigned)prm.seed & 0xffffu, k + 1);
       g = kGaussianSequence[(st >> 5) & 2047];
     }
-    gs->luma[k] = (short)rnd2z(g, shift);
+    luma[k] = (short)rnd2z(g, shift);
   }
   const bool chroma = prm.chroma_scaling_from_luma || prm.num_cb_points > 0 || prm.num_cr_points > 0;
   if (chroma) {
@@ -994,11 +999,11 @@ __global__ void __launch_bounds__(256) k_grain_template(GrainState* gs, GrainPar
         for (int dr = -lag; dr <= 0; ++dr)
           for (int dc = -lag; dc <= lag; ++dc) {
             if (dr == 0 && dc == 0) goto done_l;
-            sum += gs->luma[(y + dr) * W + x + dc] * prm.ar_y[pos_];
+            sum += luma[(y + dr) * W + x + dc] * prm.ar_y[pos_];
             ++pos_;
           }
       done_l:
-        gs->luma[y * W + x] = (short)clampi(gs->luma[y * W + x] + rnd2z(sum, arshift), gmin, gmax);
+        luma[y * W + x] = (short)clampi(luma[y * W + x] + rnd2z(sum, arshift), gmin, gmax);
       }
       __syncthreads();
     }
@@ -1022,7 +1027,7 @@ __global__ void __launch_bounds__(256) k_grain_template(GrainState* gs, GrainPar
                 const int lx = ((x - 3) << sx) + 3, ly = ((y - 3) << sy) + 3;
                 int acc = 0;
                 for (int i = 0; i <= sy; ++i)
-                  for (int j = 0; j <= sx; ++j) acc += gs->luma[(ly + i) * 82 + lx + j];
+                  for (int j = 0; j <= sx; ++j) acc += luma[(ly + i) * 82 + lx + j];
                 sum += rnd2z(acc, sx + sy) * co[pos_];
               }
               goto done_c;
@@ -1036,6 +1041,13 @@ __global__ void __launch_bounds__(256) k_grain_template(GrainState* gs, GrainPar
       __syncthreads();
     }
   }
+  __syncthreads();
+  for (int k = tid; k < 82 * 73; k += blockDim.x) gs->luma[k] = luma[k];
+  if (chroma)
+    for (int k = tid; k < cw * ch; k += blockDim.x) {
+      gs->cb[k] = cb[k];
+      gs->cr[k] = cr[k];
+    }
 }
 
 /* The stripe value of plane `p` at (row, col) of stripe `s` (7.18.3.5, the
