@@ -351,6 +351,7 @@ struct Plan {
          n_cdef = 0,
          n_cdef_search = 0;
   int unit_depth = 0;             /* dependency depth of the frame */
+  bool units_inter = false;       /* some phase B block is an inter kind */
   pvec<int2> inter_tiles;
   pvec<int2> itx_jobs;
   pvec<DeblockRec> deblock_v, deblock_h;
@@ -1007,6 +1008,12 @@ int plan_units(av1b_decoder* d, const PlanCtx& c, Plan* P) {
   for (size_t ui = 0; ui < nu; ++ui) sorted[count[depth[P->R->units[ui]]]++] = P->R->units[ui];
   std::copy(sorted.begin(), sorted.end(), P->R->units.begin());
   P->unit_depth = max_depth;
+  P->units_inter = false;
+  for (size_t ui = 0; ui < nu; ++ui)
+    if (P->R->blocks[P->R->units[ui]].kind != AV1B_U_INTRA) {
+      P->units_inter = true;
+      break;
+    }
   return AV1B_OK;
 }
 
@@ -1787,6 +1794,7 @@ int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, cons
   a.units = reinterpret_cast<const int*>(ar + pl->o_units);
   a.n_units = static_cast<int>(P.n_units);
   a.deps = reinterpret_cast<const int*>(ar + pl->o_deps);
+  a.units_inter = P.units_inter ? 1 : 0;
   a.queue = static_cast<unsigned*>(d->status_q.p);
   a.status = reinterpret_cast<int*>(static_cast<uint8_t*>(d->status_q.p) + 64);
   a.inter_tiles = reinterpret_cast<const int2*>(ar + pl->o_tiles);

@@ -413,6 +413,25 @@ cudaError_t launch_selftest_wait(const unsigned* flag, int* status, unsigned lon
  * block record, its dependency list, its residual - is loaded before the
  * wait. Shared memory per warp: three edge buffers and a 64x64 scratch (the
  * block's residual image, or the transform scratch). */
+/* Adds a phase B transform's residual - precomputed by k_itx, or the raw
+ * residual of a residual-provided block - to the reconstructed prediction
+ * (read back through L2). No transform code here: the kernel stays small. */
+__device__ void add_residual_cg(const FrameArgs& a, const BlockRec& b, const TxRec& tx, int lane) {
+  const PlaneGeom& g = a.L.p[b.plane];
+  px_t* dst = a.cur + g.off + (b.y + tx.y) * g.stride + b.x + tx.x;
+  const int* res = b.residual_provided ? a.residual + tx.coef_off : a.pre_res + tx.pre_off;
+  for (int k = lane; k < tx.w * tx.h; k += 32) {
+    const int yy = k / tx.w, xx = k - yy * tx.w;
+    px_t* q = dst + yy * g.stride + xx;
+    *q = (px_t)clampi((int)__ldcg(q) + res[yy * tx.w + xx], 0, a.maxv);
+  }
+  __syncwarp();
+}
+
+/* INTER: the frame has phase B inter blocks (inter-intra, intra block copy);
+ * a frame of intra blocks only (every key frame) runs the instantiation
+ * without the inter prediction code, a much smaller kernel. */
+template <bool INTER>
 __global__ void __launch_bounds__(128) k_units(const __grid_constant__ FrameArgs a) {
   extern __shared__ int smem[];
   const int wib = threadIdx.x >> 5;
@@ -483,7 +502,7 @@ __global__ void __launch_bounds__(128) k_units(const __grid_constant__ FrameArgs
       intra_predict(j, dst, g.stride, a.cur + a.L.p[0].off, a.L.p[0].stride, a.palette_map,
                     a.palette_colors + 8 * b.palette_color_idx, edges, lane,
                     fused ? tmp : nullptr, tmp + 1024);
-    } else {
+    } else if constexpr (INTER) {
       InterJob j;
       make_inter_job(a, b, &j);
       int dc = 0;
@@ -497,7 +516,7 @@ __global__ void __launch_bounds__(128) k_units(const __grid_constant__ FrameArgs
     }
     __syncwarp();
     if (!fused)
-      for (int t = 0; t < b.tx_count; ++t) apply_tx<true>(a, b, a.txs[b.tx_first + t], tmp, lane);
+      for (int t = 0; t < b.tx_count; ++t) add_residual_cg(a, b, a.txs[b.tx_first + t], lane);
 
     /* publish: the barrier orders every lane's stores before lane 0's
      * release, whose fence (cumulative) makes them visible at GPU scope to
@@ -1234,7 +1253,8 @@ cudaError_t launch_recon_stage(int stage, const FrameArgs& a, int n_sm, cudaStre
     default:
       if (a.n_units > 0) {
         const size_t smem = 4 * (3 * AV1B_EDGE_LEN + 4096) * sizeof(int);
-        k_units<<<2 * n_sm, 128, smem, s>>>(a);
+        if (a.units_inter) k_units<true><<<2 * n_sm, 128, smem, s>>>(a);
+        else k_units<false><<<2 * n_sm, 128, smem, s>>>(a);
       }
       break;
   }
@@ -1304,9 +1324,12 @@ cudaError_t launch_rgb(const px_t* pic, uint8_t* out, const Layout& L, const Rgb
 }
 
 cudaError_t set_kernel_attributes() {
-  cudaError_t e = cudaFuncSetAttribute(k_units, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(k_units<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        4 * (3 * AV1B_EDGE_LEN + 4096) * (int)sizeof(int));
   if (e != cudaSuccess) return e;
+  if ((e = cudaFuncSetAttribute(k_units<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                4 * (3 * AV1B_EDGE_LEN + 4096) * (int)sizeof(int))) != cudaSuccess)
+    return e;
   /* the two classes whose scratch passes the 48 KB default */
   if ((e = cudaFuncSetAttribute(k_itx<6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 4 * 4096 * (int)sizeof(int))) != cudaSuccess)

@@ -38,6 +38,7 @@ struct FrameArgs {
   unsigned epoch;
   const int* units;             /* phase B block indices, claim order */
   const int* deps;              /* the phase B blocks each phase B block waits for */
+  int units_inter;              /* some phase B block is an inter kind */
   int n_units;
   unsigned* queue;
   const int2* inter_tiles;      /* phase A: (block, x0 | y0 << 16) */
