@@ -1323,7 +1323,37 @@ cudaError_t launch_rgb(const px_t* pic, uint8_t* out, const Layout& L, const Rgb
   return cudaGetLastError();
 }
 
+/* Loads every kernel of this file now. With lazy module loading (the CUDA
+ * 12 default) a kernel's first launch loads its code, and a load waits for
+ * the kernels already running; decoder creation loading them all keeps that
+ * wait out of every frame. */
+template <class K>
+static cudaError_t load_kernel(K k) {
+  cudaFuncAttributes fa;
+  return cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(k));
+}
+
+static cudaError_t load_all_kernels() {
+  cudaError_t e;
+  if ((e = load_kernel(k_inter_simple)) != cudaSuccess || (e = load_kernel(k_inter)) != cudaSuccess ||
+      (e = load_kernel(k_itx<2>)) != cudaSuccess || (e = load_kernel(k_itx<3>)) != cudaSuccess ||
+      (e = load_kernel(k_itx<4>)) != cudaSuccess || (e = load_kernel(k_itx<5>)) != cudaSuccess ||
+      (e = load_kernel(k_itx<6>)) != cudaSuccess || (e = load_kernel(k_itx<7>)) != cudaSuccess ||
+      (e = load_kernel(k_units<true>)) != cudaSuccess || (e = load_kernel(k_units<false>)) != cudaSuccess ||
+      (e = load_kernel(k_selftest_wait)) != cudaSuccess || (e = load_kernel(k_deblock)) != cudaSuccess ||
+      (e = load_kernel(k_cdef_search)) != cudaSuccess || (e = load_kernel(k_cdef)) != cudaSuccess ||
+      (e = load_kernel(k_upscale)) != cudaSuccess || (e = load_kernel(k_lr_tile)) != cudaSuccess ||
+      (e = load_kernel(k_grain_template)) != cudaSuccess || (e = load_kernel(k_grain_blend)) != cudaSuccess ||
+      (e = load_kernel(k_nv12)) != cudaSuccess || (e = load_kernel(k_rgb)) != cudaSuccess)
+    return e;
+  return cudaSuccess;
+}
+
 cudaError_t set_kernel_attributes() {
+  {
+    const cudaError_t e = load_all_kernels();
+    if (e != cudaSuccess) return e;
+  }
   cudaError_t e = cudaFuncSetAttribute(k_units<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        4 * (3 * AV1B_EDGE_LEN + 4096) * (int)sizeof(int));
   if (e != cudaSuccess) return e;
