@@ -664,10 +664,9 @@ int plan_block(const PlanCtx& ctx, const av1b_frame_syntax& s, size_t bi, BlockR
   if (r.phase_b) {
     O->units.push_back(static_cast<int>(bi));
   } else {
-    /* translation-only blocks (no global warp, mask, or OBMC) take the lean
-     * prediction kernel */
-    const bool simple = !r.warp0 && !r.warp1 && !r.mask_warp0 && !r.mask_warp1 &&
-                        r.mask_kind == 0 && r.obmc_count == 0 && !r.interintra;
+    /* blocks without masks (translation or global warp, with or without
+     * OBMC) take the lean prediction kernel */
+    const bool simple = r.mask_kind == 0 && !r.interintra;
     auto& tiles = simple ? O->inter_tiles : O->inter_tiles_full;
     for (int y0 = 0; y0 < b.h; y0 += 8)
       for (int x0 = 0; x0 < b.w; x0 += 16)

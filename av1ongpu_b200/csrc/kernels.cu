@@ -125,11 +125,12 @@ __device__ void make_inter_job(const FrameArgs& a, const BlockRec& b, InterJob* 
 
 /* ---- phase A ------------------------------------------------------------------------ */
 
-/* Inter prediction of the translation-only blocks of phase A (no global
- * warp, no mask, no OBMC - most inter blocks): one warp per 16x8 tile,
- * each reference through mc_rect, then the average or distance-weighted
- * blend. It carries none of the full kernel's state, so it runs with a
- * fraction of its registers and many more warps in flight. */
+/* Inter prediction of the phase A blocks without masks (almost every inter
+ * block): one warp per 16x8 tile, each reference through mc_rect or, for a
+ * globally warped one, warp_block8, then the average or distance-weighted
+ * blend, then the OBMC strips in order, each neighbour's prediction of the
+ * strip through mc_rect. It carries none of the full kernel's state, so it
+ * runs with a fraction of its registers and many more warps in flight. */
 __global__ void __launch_bounds__(128) k_inter_simple(const __grid_constant__ FrameArgs a) {
   __shared__ McScratch scr[4];
   __shared__ int pred[4][2][8 * 16];
@@ -154,6 +155,14 @@ __global__ void __launch_bounds__(128) k_inter_simple(const __grid_constant__ Fr
   for (int r = 0; r < nref; ++r) {
     int* pr = pred[wib][r];
     const px_t* ref = ref_plane(a, b.ref_slot[r], p);
+    if (r == 0 ? b.warp0 : b.warp1) {
+      /* one or two whole 8x8 warp blocks (x0 is a multiple of 16, y0 of 8) */
+      const WarpRec& m = a.warps[b.warp_idx[r] >= 0 ? b.warp_idx[r] : 0];
+      for (int bx = 0; bx < tw; bx += 8)
+        warp_block8(c.sub_x, c.sub_y, c.ref_w, c.ref_h, m, ref, g.stride, b.x, b.y, x0 + bx, y0,
+                    c.bitdepth, b.compound != 0, scr[wib], pr + bx, 16, mini(8, tw - bx), th, lane);
+      continue;
+    }
     if (!mc_rect(c, ref, g.stride, b.x, b.y, b.w, b.h, b.mv[r][0], b.mv[r][1], b.filt, b.filt_v,
                  b.compound != 0, x0, y0, tw, th, scr[wib], pr, lane)) {
       for (int k = lane; k < tw * th; k += 32) {
@@ -166,7 +175,11 @@ __global__ void __launch_bounds__(128) k_inter_simple(const __grid_constant__ Fr
   }
   px_t* dst = a.cur + g.off + (b.y + y0) * g.stride + b.x + x0;
   const int post = 7 - (c.bitdepth >= 12 ? 5 : 3);
-  for (int k = lane; k < tw * th; k += 32) {
+  int acc[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int k = lane + 32 * q;
+    if (k >= tw * th) continue;
     const int yy = k / tw, xx = k - yy * tw;
     const int v0 = pred[wib][0][yy * 16 + xx];
     int out = v0;
@@ -175,7 +188,41 @@ __global__ void __launch_bounds__(128) k_inter_simple(const __grid_constant__ Fr
     } else if (b.compound) {
       out = (b.w0 * v0 + b.w1 * pred[wib][1][yy * 16 + xx] + (1 << (3 + post))) >> (4 + post);
     }
-    dst[yy * g.stride + xx] = (px_t)clampi(out, 0, a.maxv);
+    acc[q] = clampi(out, 0, a.maxv);
+  }
+  __syncwarp();
+  /* OBMC: the strips in order, each blended onto the samples it covers */
+  for (int kk = 0; kk < b.obmc_count; ++kk) {
+    const ObmcRec& o = a.obmc[b.obmc_first + kk];
+    const int ix0 = maxi(o.x, x0), ix1 = mini(o.x + o.w, x0 + tw);
+    const int iy0 = maxi(o.y, y0), iy1 = mini(o.y + o.h, y0 + th);
+    if (ix0 >= ix1 || iy0 >= iy1) continue;
+    int* tmp = pred[wib][0];
+    const px_t* oref = ref_plane(a, o.ref_slot, p);
+    const bool ok = mc_rect(c, oref, g.stride, b.x + o.x, b.y + o.y, o.w, o.h, o.mv_x, o.mv_y, o.filt,
+                            o.filt_v, 0, ix0 - o.x, iy0 - o.y, ix1 - ix0, iy1 - iy0, scr[wib], tmp,
+                            lane);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int k = lane + 32 * q;
+      if (k >= tw * th) continue;
+      const int yy = k / tw, xx = k - yy * tw;
+      const int x = x0 + xx, y = y0 + yy;
+      if (x < ix0 || x >= ix1 || y < iy0 || y >= iy1) continue;
+      const int pv = ok ? tmp[(y - iy0) * 16 + x - ix0]
+                        : mc_tap(c, oref, g.stride, b.x + o.x, b.y + o.y, o.w, o.h, o.mv_x, o.mv_y,
+                                 o.filt, o.filt_v, x - o.x, y - o.y, 0);
+      acc[q] = obmc_blend(o, x - o.x, y - o.y, acc[q], pv, a.maxv);
+    }
+    __syncwarp();
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int k = lane + 32 * q;
+    if (k < tw * th) {
+      const int yy = k / tw, xx = k - yy * tw;
+      dst[yy * g.stride + xx] = (px_t)acc[q];
+    }
   }
 }
 
