@@ -175,12 +175,18 @@ cudaError_t wait_stream(av1b_decoder* d) {
     if (e_ != cudaSuccess) return cuda_fail(d, e_, what);  \
   } while (0)
 
-int dev_ensure(av1b_decoder* d, DevBuf& b, size_t bytes) {
+/* Makes `b` hold at least `bytes`; when it has to grow, it takes `room`
+ * bytes if that is more (and the HBM budget allows), so buffers whose need
+ * varies frame to frame grow once rather than at every larger frame - each
+ * cudaFree waits for the whole device. */
+int dev_ensure(av1b_decoder* d, DevBuf& b, size_t bytes, size_t room = 0) {
   if (bytes == 0) bytes = 256;
   if (b.cap >= bytes) return AV1B_OK;
-  const size_t want = align_up(bytes + bytes / 8, 1 << 16);
+  size_t want = align_up(bytes + bytes / 8, 1 << 16);
   {
     std::lock_guard<std::mutex> lk(d->alloc_mu);
+    const size_t roomy = align_up(room, 1 << 16);
+    if (roomy > want && (!d->budget || d->allocated - b.cap + roomy <= d->budget)) want = roomy;
     if (d->budget && d->allocated - b.cap + want > d->budget)
       return fail(d, AV1B_ERR_NOMEM, "decoder HBM budget exhausted");
     d->allocated -= b.cap;
@@ -344,6 +350,15 @@ struct PlanLists {
 
 /* One planned frame's constants and record counts (its records live in
  * device memory, uploaded from the PlanLists). */
+/* Sizes a page-locked list, growing it with half again as much room: a
+ * page-locked allocation stalls every CUDA call of the process, so lists
+ * grow rarely and early (the key frame's lists are the largest). */
+template <class V>
+void sized(V& v, size_t n) {
+  if (n > v.capacity()) v.reserve(n + n / 2);
+  v.resize(n);
+}
+
 struct Plan {
   PlanLists* R = nullptr;         /* while planning: the lists being built */
   size_t n_tiles_simple = 0;      /* inter tiles the lean kernel takes (listed first) */
@@ -980,7 +995,7 @@ int plan_units(av1b_decoder* d, const PlanCtx& c, Plan* P) {
   std::vector<size_t> first(nu + 1, 0);
   for (size_t ui = 0; ui < nu; ++ui) first[ui + 1] = first[ui] + dep_count[ui];
   if (first[nu] > static_cast<size_t>(INT32_MAX)) return fail(d, AV1B_ERR_SYNTAX, "frame too large");
-  P->R->deps.resize(first[nu]);
+  sized(P->R->deps, first[nu]);
   c.pool->run(pieces, [&](int pi) {
     std::copy(pdeps[pi].begin(), pdeps[pi].end(),
               P->R->deps.begin() + first[piece_begin(nu, pieces, pi)]);
@@ -1092,7 +1107,7 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
   const Layout& L = c.L;
   const int bd = s.bit_depth;
   int rc_units;
-  P->R->blocks.resize(s.n_blocks);
+  sized(P->R->blocks, s.n_blocks);
   for (int i = 0; i < 7; ++i) {
     const int rw = s.reference_width[i] > 0 ? s.reference_width[i] : s.width;
     const int rh = s.reference_height[i] > 0 ? s.reference_height[i] : s.height;
@@ -1141,16 +1156,16 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
     }
     if (o_pre[pieces] > static_cast<size_t>(INT32_MAX) || o_tx[pieces] > static_cast<size_t>(INT32_MAX))
       return fail(d, AV1B_ERR_SYNTAX, "frame too large");
-    P->R->txs.resize(o_tx[pieces]);
-    P->R->obmc.resize(o_obmc[pieces]);
-    P->R->warps.resize(1 + o_warp[pieces]);
+    sized(P->R->txs, o_tx[pieces]);
+    sized(P->R->obmc, o_obmc[pieces]);
+    sized(P->R->warps, 1 + o_warp[pieces]);
     P->R->warps[0] = WarpRec{};
-    P->R->palette_colors.resize(o_pal[pieces]);
-    P->R->units.resize(o_unit[pieces]);
+    sized(P->R->palette_colors, o_pal[pieces]);
+    sized(P->R->units, o_unit[pieces]);
     /* the lean kernel's tiles first, then the rest */
-    P->R->inter_tiles.resize(o_tile[pieces] + o_tilef[pieces]);
+    sized(P->R->inter_tiles, o_tile[pieces] + o_tilef[pieces]);
     P->n_tiles_simple = o_tile[pieces];
-    P->R->itx_jobs.resize(o_itx[pieces]);
+    sized(P->R->itx_jobs, o_itx[pieces]);
     P->pre_res_pool = o_pre[pieces];
     c.pool->run(pieces, [&](int i) {
       const BlockOut& O = outs[i];
@@ -1218,8 +1233,8 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
       nv += outs[i].v.size();
       nh += outs[i].h.size();
     }
-    P->R->deblock_v.resize(nv);
-    P->R->deblock_h.resize(nh);
+    sized(P->R->deblock_v, nv);
+    sized(P->R->deblock_h, nh);
     c.pool->run(pieces, [&](int i) {
       std::copy(outs[i].v.begin(), outs[i].v.end(), P->R->deblock_v.begin() + ov[i]);
       std::copy(outs[i].h.begin(), outs[i].h.end(), P->R->deblock_h.begin() + oh[i]);
@@ -1229,7 +1244,7 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
   /* CDEF */
   {
     const size_t nc = s.n_cdef;
-    P->R->cdef.resize(nc);
+    sized(P->R->cdef, nc);
     P->R->cdef_search.clear();
     P->cdef_grid_w = L.p[0].stride >> 3;
     P->cdef_grid_n = P->cdef_grid_w * (plane_rows(L, 0) >> 3);
@@ -1549,7 +1564,10 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
   cudaStream_t st = pn->upload;
   /* the caller's coefficients and raw residuals go up first, while the
    * records are built */
-  if ((rc = dev_ensure(d, pl->coef, (s.n_coefficients + 64) * sizeof(int))) ||
+  /* a frame's coefficients never outnumber its samples: a plan's pool is
+   * made that large on first use, whatever frame it first holds */
+  if ((rc = dev_ensure(d, pl->coef, (s.n_coefficients + 64) * sizeof(int),
+                       (static_cast<size_t>(c.L.size) + 64) * sizeof(int))) ||
       (rc = dev_ensure(d, pl->residual, (s.n_residual + 64) * sizeof(int))))
     return rc;
   if (s.n_coefficients)
@@ -1619,7 +1637,7 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
   pl->o_map = off;
   off = align_up(off + s.n_palette_map + 64, 256);
   const size_t total = off;
-  if ((rc = dev_ensure(d, pl->arena, total))) {
+  if ((rc = dev_ensure(d, pl->arena, total, total + total / 2))) {
     cudaStreamSynchronize(st);
     return rc;
   }
@@ -1974,7 +1992,7 @@ void release_plan(av1b_decoder* d, av1b_plan* pl) {
 void recycle_plan(av1b_decoder* d, av1b_plan* pl) {
   {
     std::lock_guard<std::mutex> lk(d->plan_pool_mu);
-    if (d->plan_pool.size() < 4) {
+    if (d->plan_pool.size() < 8) {
       d->plan_pool.push_back(pl);
       return;
     }
