@@ -177,4 +177,32 @@ __attribute__((visibility("default"))) void av1ref_itx(int w, int h, int tx_type
   for (int x = 0; x < w; ++x) av1g_itx_col_add(&job, tmp.data(), dst, x, maxv);
 }
 
+/* The array lengths of a serialized frame, in av1b_frame_syntax order: blocks,
+ * transforms, obmc, coefficients, residual, levels, qm_pool, palette_map,
+ * deblock, cdef, and the restoration units of all three planes. Returns 11,
+ * or -1 for a malformed blob. */
+__attribute__((visibility("default"))) int av1ref_blob_counts(const uint8_t* blob, size_t len,
+                                                              uint64_t* out) {
+  av1b_frame_syntax v;
+  if (!av1b::view_blob(blob, len, &v)) return -1;
+  const size_t n[11] = {v.n_blocks,   v.n_transforms,   v.n_obmc,           v.n_coefficients,
+                        v.n_residual, v.n_levels,       v.n_qm_pool,        v.n_palette_map,
+                        v.n_deblock,  v.n_cdef,         v.n_restoration[0] + v.n_restoration[1] +
+                                                            v.n_restoration[2]};
+  for (int i = 0; i < 11; ++i) out[i] = n[i];
+  return 11;
+}
+
+/* FNV-1a 64 over `n` bytes, seeded with `h` (0xcbf29ce484222325 to start): the
+ * frame hash of the reference's stream tests (tools/av1gpu_decode.cpp:131-140),
+ * chainable so a picture can be hashed plane by plane. */
+__attribute__((visibility("default"))) uint64_t av1ref_fnv1a64(uint64_t h, const uint8_t* p,
+                                                               size_t n) {
+  for (size_t i = 0; i < n; ++i) {
+    h ^= p[i];
+    h *= 0x100000001b3ull;
+  }
+  return h;
+}
+
 }  // extern "C"

@@ -43,6 +43,9 @@ def ref_lib():
         L.av1ref_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                    ctypes.POINTER(ctypes.c_int)]
         L.av1ref_itx.argtypes = [ctypes.c_int] * 6 + [ctypes.c_void_p, ctypes.c_void_p]
+        L.av1ref_fnv1a64.argtypes = [ctypes.c_uint64, ctypes.c_void_p, ctypes.c_size_t]
+        L.av1ref_fnv1a64.restype = ctypes.c_uint64
+        L.av1ref_blob_counts.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
         _ref = L
     return _ref
 
@@ -96,15 +99,35 @@ class RefDecoder:
         return out[:got]
 
 
-def fnv1a64(arr):
+def fnv1a64(arr, h=0xcbf29ce484222325):
     """FNV-1a 64 over the bytes of an array (the hash the reference's stream
-    tests use, av1gpu_decode.cpp:133-140)."""
-    data = np.ascontiguousarray(arr).view(np.uint8)
+    tests use, av1gpu_decode.cpp:131-140); `h` chains a previous result."""
+    data = np.ascontiguousarray(arr).view(np.uint8).reshape(-1)
+    return ref_lib().av1ref_fnv1a64(h, data.ctypes.data, data.size)
+
+
+BLOB_ARRAYS = ('blocks', 'transforms', 'obmc', 'coefficients', 'residual', 'levels', 'qm_pool',
+               'palette_map', 'deblock', 'cdef', 'restoration')
+
+
+def blob_counts(blob):
+    """{array name: length} of a serialized frame (an av1ongpu_b200.Blob)."""
+    out = (ctypes.c_uint64 * 11)()
+    if ref_lib().av1ref_blob_counts(blob.ptr, blob.size, out) != 11:
+        raise ValueError('malformed blob')
+    return dict(zip(BLOB_ARRAYS, list(out)))
+
+
+def picture_hash(planes, bit_depth, yuv16):
+    """The stream tests' frame hash of one picture: its planes in order, each
+    sample one byte (shifted down to 8 bits) or two little endian bytes with
+    `yuv16` (factory.cpp:194-233 of the reference)."""
     h = 0xcbf29ce484222325
-    # vectorised in chunks: fold bytes sequentially (exact FNV-1a)
-    for b in data.tobytes():
-        h ^= b
-        h = (h * 0x100000001b3) & 0xFFFFFFFFFFFFFFFF
+    for p in planes:
+        if yuv16:
+            h = fnv1a64(np.ascontiguousarray(p, dtype='<u2'), h)
+        else:
+            h = fnv1a64((np.asarray(p) >> (bit_depth - 8)).astype(np.uint8), h)
     return h
 
 
