@@ -346,6 +346,7 @@ struct PlanLists {
   pvec<CdefRec> cdef;
   pvec<unsigned> cdef_search;     /* searches off the 8x8 grid: x | y << 16 */
   pvec<LrUnitRec> lr_units[3];
+  pvec<DqRec> dq;                 /* coded transforms to dequantise (levels frames) */
 };
 
 /* One planned frame's constants and record counts (its records live in
@@ -379,6 +380,7 @@ struct Plan {
   bool use_lr = false;
   size_t coef_pool = 0, residual_pool = 0;
   size_t pre_res_pool = 0;        /* ints of residual computed ahead (phase B) */
+  size_t n_dq = 0;                /* transforms the device dequantises */
   int scale_x = AV1B_SCALE_ONE, scale_y = AV1B_SCALE_ONE;
   bool upscaled = false;
   bool grain = false;
@@ -395,6 +397,10 @@ struct PlanCtx {
   int slot_width[kSlots], slot_height[kSlots];
   WorkPool* pool = nullptr;
   struct PlanScratch* scratch = nullptr;
+  /* the frame carries coded levels: the device builds the coefficient
+   * rasters from them (and the frame's coefficient array is not read) */
+  bool levels = false;
+  size_t n_levels = 0, n_qm = 0;
 };
 
 /* The first error one piece of the planner met. */
@@ -442,10 +448,12 @@ struct BlockOut {
   std::vector<int> units;
   std::vector<int2> inter_tiles, inter_tiles_full;
   std::vector<int2> itx_jobs;
+  std::vector<DqRec> dq;
   size_t pre_res_pool = 0, coef_end = 0, res_end = 0;
   PlanErr err;
   void clear() {
     txs.clear();
+    dq.clear();
     obmc.clear();
     warps.clear();
     palette_colors.clear();
@@ -457,6 +465,46 @@ struct BlockOut {
     err = PlanErr();
   }
 };
+
+/* The dequantiser of one coded transform of a levels frame, as the reference
+ * front end's dequantise_tile reads it (dequant.hpp:317-345): the raster is
+ * the adjusted size (each side at most 32), the levels are min(eob, area) in
+ * the scan of the transform's class (coef_model.hpp:190-219: vertical 1-D
+ * types the row scan, horizontal ones the column scan, falling back to the
+ * diagonal scan of the size), and the matrix, when there is one, is read
+ * whatever the type. */
+int plan_dequant(const PlanCtx& ctx, const av1b_transform& t, const TxRec& x, BlockOut* O) {
+  DqRec q{};
+  q.alw = static_cast<unsigned char>(std::min<int>(x.log2w, 5));
+  q.alh = static_cast<unsigned char>(std::min<int>(x.log2h, 5));
+  const int area = 1 << (q.alw + q.alh);
+  const int cls = (t.tx_type == 10 || t.tx_type == 12 || t.tx_type == 14)   ? 2
+                  : (t.tx_type == 11 || t.tx_type == 13 || t.tx_type == 15) ? 1
+                                                                            : 0;
+  const int key = (q.alw - 2) * 4 + (q.alh - 2);
+  int so = kScanOffset[cls * 16 + key];
+  if (so < 0) so = kScanOffset[key];
+  if (so < 0) so = 0;
+  q.count = std::min(t.eob, area);
+  if (t.level_offset < 0 || static_cast<size_t>(t.level_offset) + q.count > ctx.n_levels)
+    return O->err.set(AV1B_ERR_SYNTAX, "transform levels outside the frame's level list");
+  if (so + q.count > AV1B_SCAN_ENTRIES)
+    return O->err.set(AV1B_ERR_SYNTAX, "transform size without a coefficient scan");
+  if (t.denominator < 1 || t.denominator > 4 || t.dc_step < 0 || t.dc_step > (1 << 20) ||
+      t.ac_step < 0 || t.ac_step > (1 << 20))
+    return O->err.set(AV1B_ERR_SYNTAX, "dequantiser step or denominator out of range");
+  if (t.qm_off >= 0 && static_cast<size_t>(t.qm_off) + area > ctx.n_qm)
+    return O->err.set(AV1B_ERR_SYNTAX, "quantiser matrix outside the frame's pool");
+  q.coef_off = t.coef_offset;
+  q.level_off = t.level_offset;
+  q.dc_step = t.dc_step;
+  q.ac_step = t.ac_step;
+  q.qm_off = t.qm_off >= 0 ? t.qm_off : -1;
+  q.scan_off = static_cast<unsigned short>(so);
+  q.denom = static_cast<unsigned short>(t.denominator);
+  O->dq.push_back(q);
+  return AV1B_OK;
+}
 
 int plan_block(const PlanCtx& ctx, const av1b_frame_syntax& s, size_t bi, BlockRec& r, BlockOut* O) {
   const Layout& L = ctx.L;
@@ -664,6 +712,10 @@ int plan_block(const PlanCtx& ctx, const av1b_frame_syntax& s, size_t bi, BlockR
         x.type = static_cast<unsigned char>(t.tx_type);
         x.row_shift = static_cast<unsigned char>(b.lossless ? 0 : tx_row_shift(x.log2w, x.log2h));
         O->coef_end = std::max(O->coef_end, static_cast<size_t>(t.coef_offset) + static_cast<size_t>(t.w) * t.h);
+        if (ctx.levels) {
+          int rc;
+          if ((rc = plan_dequant(ctx, t, x, O))) return rc;
+        }
       }
       x.pre_off = -1;
       if (r.phase_b && !b.residual_provided) {
@@ -1139,7 +1191,7 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
     /* piece offsets into the frame's lists */
     std::vector<size_t> o_tx(pieces + 1, 0), o_obmc(pieces + 1, 0), o_warp(pieces + 1, 0),
         o_pal(pieces + 1, 0), o_unit(pieces + 1, 0), o_tile(pieces + 1, 0), o_tilef(pieces + 1, 0),
-        o_itx(pieces + 1, 0), o_pre(pieces + 1, 0);
+        o_itx(pieces + 1, 0), o_pre(pieces + 1, 0), o_dq(pieces + 1, 0);
     for (int i = 0; i < pieces; ++i) {
       const BlockOut& O = outs[i];
       o_tx[i + 1] = o_tx[i] + O.txs.size();
@@ -1151,6 +1203,7 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
       o_tilef[i + 1] = o_tilef[i] + O.inter_tiles_full.size();
       o_itx[i + 1] = o_itx[i] + O.itx_jobs.size();
       o_pre[i + 1] = o_pre[i] + O.pre_res_pool;
+      o_dq[i + 1] = o_dq[i] + O.dq.size();
       coef_end = std::max(coef_end, O.coef_end);
       res_end = std::max(res_end, O.res_end);
     }
@@ -1166,6 +1219,8 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
     sized(P->R->inter_tiles, o_tile[pieces] + o_tilef[pieces]);
     P->n_tiles_simple = o_tile[pieces];
     sized(P->R->itx_jobs, o_itx[pieces]);
+    sized(P->R->dq, o_dq[pieces]);
+    P->n_dq = o_dq[pieces];
     P->pre_res_pool = o_pre[pieces];
     c.pool->run(pieces, [&](int i) {
       const BlockOut& O = outs[i];
@@ -1197,6 +1252,7 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
         j.y += dtx;
         P->R->itx_jobs[o_itx[i] + k] = j;
       }
+      std::copy(O.dq.begin(), O.dq.end(), P->R->dq.begin() + o_dq[i]);
     });
   }
   if ((rc_units = plan_units(d, c, P))) return rc_units;
@@ -1204,7 +1260,7 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
 
   /* the pools read past the caller's arrays as zeros, like the reference's
    * padded plan pools (engine.cpp:665-674) */
-  P->coef_pool = std::max(coef_end + 64, s.n_coefficients);
+  P->coef_pool = c.levels ? coef_end + 64 : std::max(coef_end + 64, s.n_coefficients);
   P->residual_pool = std::max(res_end + 64, s.n_residual);
 
   /* deblocking edges: V then H, each a list of independent edges */
@@ -1470,6 +1526,14 @@ int check_header(av1b_decoder* d, const av1b_frame_syntax& s) {
   if (s.ss_x < 0 || s.ss_x > 1 || s.ss_y < 0 || s.ss_y > 1 || (s.ss_y && !s.ss_x))
     return fail(d, AV1B_ERR_SYNTAX, "unsupported chroma subsampling");
   if (s.width > 16384 || s.height > 16384) return fail(d, AV1B_ERR_SYNTAX, "frame too large");
+  if ((s.n_blocks && !s.blocks) || (s.n_transforms && !s.transforms) || (s.n_obmc && !s.obmc) ||
+      (s.n_coefficients && !s.coefficients) || (s.n_residual && !s.residual) ||
+      (s.n_levels && !s.levels) || (s.n_qm_pool && !s.qm_pool) ||
+      (s.n_palette_map && !s.palette_map) || (s.n_deblock && !s.deblock) || (s.n_cdef && !s.cdef) ||
+      (s.n_reference_slots && !s.reference_slots) ||
+      (s.n_restoration[0] && !s.restoration[0]) || (s.n_restoration[1] && !s.restoration[1]) ||
+      (s.n_restoration[2] && !s.restoration[2]))
+    return fail(d, AV1B_ERR_ARG, "a syntax array with a length but no data");
   return AV1B_OK;
 }
 
@@ -1485,13 +1549,14 @@ struct av1b_plan {
   av1b::Layout L{};
   av1b::Plan P;                   /* host copy of the counts and constants */
   av1b::DevBuf arena, coef, residual;
+  av1b::DevBuf dqsrc;             /* a levels frame's levels, then its QM pool */
   /* ready: the uploads are done; done: the last frame that read this plan has
    * finished on the device (a plan is re-planned only after that) */
   cudaEvent_t ready = nullptr, done = nullptr;
   bool in_flight = false;
   size_t o_blocks = 0, o_txs = 0, o_obmc = 0, o_warps = 0, o_pal = 0, o_units = 0, o_deps = 0;
   size_t o_tiles = 0, o_itx = 0, o_itxb = 0, o_dbv = 0, o_dbh = 0, o_cdef = 0, o_lr[3] = {0, 0, 0};
-  size_t o_map = 0, o_cdef_search = 0;
+  size_t o_map = 0, o_cdef_search = 0, o_dq = 0;
   int slots_read[kSlots + 1];     /* the reference slots the frame reads, -1 ended */
   int n_blocks = 0;
   bool owned_by_decoder = false;
@@ -1549,6 +1614,13 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
   }
   c.pool = pn->pool;
   c.scratch = pn->scratch;
+  /* a frame that carries its coded levels is dequantised on the device, the
+   * reference engine's device-dequantiser path (engine.cpp:386, 655-670):
+   * its coefficient array, if it has one too, is not uploaded */
+  c.levels = s.n_levels > 0;
+  c.n_levels = s.n_levels;
+  c.n_qm = s.n_qm_pool;
+  const size_t n_coef = c.levels ? 0 : s.n_coefficients;
   if (!pl->ready) {
     /* blocking-sync events: a waiting planner sleeps instead of spinning on
      * a core the planner pool or the decoding thread could use */
@@ -1566,13 +1638,23 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
    * records are built */
   /* a frame's coefficients never outnumber its samples: a plan's pool is
    * made that large on first use, whatever frame it first holds */
-  if ((rc = dev_ensure(d, pl->coef, (s.n_coefficients + 64) * sizeof(int),
+  if ((rc = dev_ensure(d, pl->coef, (n_coef + 64) * sizeof(int),
                        (static_cast<size_t>(c.L.size) + 64) * sizeof(int))) ||
       (rc = dev_ensure(d, pl->residual, (s.n_residual + 64) * sizeof(int))))
     return rc;
-  if (s.n_coefficients)
-    CK(cudaMemcpyAsync(pl->coef.p, s.coefficients, s.n_coefficients * sizeof(int),
+  if (n_coef)
+    CK(cudaMemcpyAsync(pl->coef.p, s.coefficients, n_coef * sizeof(int),
                        cudaMemcpyHostToDevice, st), "coefficient upload");
+  const size_t qm_at = align_up(s.n_levels * sizeof(int16_t), 256);
+  if (c.levels) {
+    const size_t bytes = qm_at + s.n_qm_pool + 64;
+    if ((rc = dev_ensure(d, pl->dqsrc, bytes, bytes + bytes / 2))) return rc;
+    CK(cudaMemcpyAsync(pl->dqsrc.p, s.levels, s.n_levels * sizeof(int16_t), cudaMemcpyHostToDevice,
+                       st), "level upload");
+    if (s.n_qm_pool)
+      CK(cudaMemcpyAsync(static_cast<uint8_t*>(pl->dqsrc.p) + qm_at, s.qm_pool, s.n_qm_pool,
+                         cudaMemcpyHostToDevice, st), "quantiser matrix upload");
+  }
   if (s.n_residual)
     CK(cudaMemcpyAsync(pl->residual.p, s.residual, s.n_residual * sizeof(int),
                        cudaMemcpyHostToDevice, st), "residual upload");
@@ -1634,6 +1716,7 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
   pl->o_cdef = stage_put(&off, P.R->cdef);
   pl->o_cdef_search = stage_put(&off, P.R->cdef_search);
   for (int p = 0; p < 3; ++p) pl->o_lr[p] = stage_put(&off, P.R->lr_units[p]);
+  pl->o_dq = stage_put(&off, P.R->dq);
   pl->o_map = off;
   off = align_up(off + s.n_palette_map + 64, 256);
   const size_t total = off;
@@ -1663,6 +1746,7 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
   CK(put(pl->o_cdef, P.R->cdef), "record upload");
   CK(put(pl->o_cdef_search, P.R->cdef_search), "record upload");
   for (int p = 0; p < 3; ++p) CK(put(pl->o_lr[p], P.R->lr_units[p]), "record upload");
+  CK(put(pl->o_dq, P.R->dq), "record upload");
   if (s.n_palette_map)
     CK(cudaMemcpyAsync(ar + pl->o_map, s.palette_map, s.n_palette_map, cudaMemcpyHostToDevice, st),
        "palette map upload");
@@ -1677,16 +1761,24 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
     if ((rc = dev_ensure(d, pl->coef, P.coef_pool * sizeof(int))) ||
         (rc = dev_ensure(d, pl->residual, P.residual_pool * sizeof(int))))
       return rc;
-    if (s.n_coefficients)
-      CK(cudaMemcpyAsync(pl->coef.p, s.coefficients, s.n_coefficients * sizeof(int),
+    if (n_coef)
+      CK(cudaMemcpyAsync(pl->coef.p, s.coefficients, n_coef * sizeof(int),
                          cudaMemcpyHostToDevice, st), "coefficient upload");
     if (s.n_residual)
       CK(cudaMemcpyAsync(pl->residual.p, s.residual, s.n_residual * sizeof(int),
                          cudaMemcpyHostToDevice, st), "residual upload");
   }
-  if (P.coef_pool > s.n_coefficients)
-    CK(cudaMemsetAsync(static_cast<int*>(pl->coef.p) + s.n_coefficients, 0,
-                       (P.coef_pool - s.n_coefficients) * sizeof(int), st), "coefficient pad");
+  if (c.levels) {
+    /* every raster a transform reads is written whole by the dequantiser */
+    const uint8_t* src = static_cast<const uint8_t*>(pl->dqsrc.p);
+    CK(launch_dequant(reinterpret_cast<const DqRec*>(ar + pl->o_dq), static_cast<int>(P.n_dq),
+                      reinterpret_cast<const short*>(src), s.n_qm_pool ? src + qm_at : nullptr,
+                      static_cast<int*>(pl->coef.p), s.bit_depth, st),
+       "dequantiser launch");
+  } else if (P.coef_pool > n_coef) {
+    CK(cudaMemsetAsync(static_cast<int*>(pl->coef.p) + n_coef, 0,
+                       (P.coef_pool - n_coef) * sizeof(int), st), "coefficient pad");
+  }
   if (P.residual_pool > s.n_residual)
     CK(cudaMemsetAsync(static_cast<int*>(pl->residual.p) + s.n_residual, 0,
                        (P.residual_pool - s.n_residual) * sizeof(int), st), "residual pad");
@@ -1982,6 +2074,7 @@ void release_plan(av1b_decoder* d, av1b_plan* pl) {
   dev_release(d, pl->arena);
   dev_release(d, pl->coef);
   dev_release(d, pl->residual);
+  dev_release(d, pl->dqsrc);
   if (pl->ready) cudaEventDestroy(pl->ready);
   if (pl->done) cudaEventDestroy(pl->done);
   delete pl;

@@ -120,6 +120,21 @@ struct BlockRec {
   int dep_first, dep_count;   /* phase B: the blocks it waits for (frame's dep list) */
 };
 
+/* One coded transform of a frame whose coefficients arrive as coded levels:
+ * where its raster goes in the coefficient pool, where its levels start, and
+ * its dequantiser. 32 bytes. */
+struct DqRec {
+  int coef_off;               /* the raster, (1 << alw) x (1 << alh) ints */
+  int level_off;              /* first of `count` levels, in scan order */
+  int count;                  /* min(eob, raster area) */
+  int dc_step, ac_step;
+  int qm_off;                 /* into the frame's QM pool, -1: no matrix */
+  unsigned short scan_off;    /* into the scan table */
+  unsigned short denom;       /* 1, 2 or 4 (the 32 and 64 point families) */
+  unsigned char alw, alh;     /* log2 of the raster's width and height (2..5) */
+  unsigned char pad[2];
+};
+
 /* One transform of a block: position relative to the block. 16 bytes. */
 struct TxRec {
   int coef_off;               /* into the coefficient (or residual) pool */

@@ -18,6 +18,7 @@ import sys
 REF = sys.argv[1] if len(sys.argv) > 1 else '/root/reference'
 tables_h = open(REF + '/kernels/av1gpu_tables.h').read()
 tables_cpp = open(REF + '/src/core/tables.cpp').read()
+coef_h = open(REF + '/src/frontend/coef_tables.hpp').read()
 
 
 def numbers(src, decl_regex, count):
@@ -116,5 +117,36 @@ if len(codes) != 48:
 w('/* Wedge_Codebook[shape][index]: direction (0 horizontal, 1 vertical, 2..5 oblique\n'
   ' * 27/63/117/153), x offset, y offset in eighths; shapes tall, wide, square */')
 w(emit('kWedgeCodebook', 'unsigned char', [48 * 3], [v for c in codes for v in c], per_line=12))
+
+
+def scan_offsets(fn):
+    m = re.search(r'inline int ' + fn + r'\(int lw, int lh\)\s*\{(.*?)\n\}', coef_h, re.S)
+    if not m:
+        raise SystemExit('scan offsets not found: ' + fn)
+    return {int(k, 16): int(v) for k, v in re.findall(r'case (0x[0-9a-f]+): return (-?\d+);', m.group(1))}
+
+
+n2d, nrow, ncol = 3344, 784, 784
+scans = (numbers(coef_h, r'kDefaultScan\[3344\]', n2d) + numbers(coef_h, r'kMrowScan\[784\]', nrow) +
+         numbers(coef_h, r'kMcolScan\[784\]', ncol))
+w('/* The coefficient scans, positions in raster order of the (at most 32x32)\n'
+  ' * coded block: Default_Scan_* (the 2-D classes), then Mrow_Scan_* (vertical\n'
+  ' * 1-D types), then Mcol_Scan_* (horizontal 1-D types), each run of sizes back\n'
+  ' * to back; kScanOffset gives where a size starts */')
+w('#define AV1B_SCAN_ENTRIES %d' % len(scans))
+w(emit('kScans', 'unsigned short', [len(scans)], scans))
+table = []
+for cls, fn, base in ((0, 'default_scan_offset', 0), (1, 'col_scan_offset', n2d + nrow),
+                      (2, 'row_scan_offset', n2d)):
+    offs = scan_offsets(fn)
+    row = [-1] * 16
+    for key, v in offs.items():
+        lw, lh = key >> 4, key & 15
+        row[lw * 4 + lh] = base + v if v >= 0 else -1
+    table += row
+w('/* kScanOffset[class][lw * 4 + lh]: the start in kScans of the scan of a\n'
+  ' * (1 << (lw + 2)) x (1 << (lh + 2)) coded block, lw, lh <= 3; classes 2-D,\n'
+  ' * horizontal (column scan), vertical (row scan); -1: no such scan (host table) */')
+w(emit('kScanOffset', 'short', [48], table, storage='static const'))
 w('#endif /* AV1B_TABLES_H */')
 print('\n'.join(parts))

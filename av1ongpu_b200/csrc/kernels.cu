@@ -347,6 +347,55 @@ __device__ void apply_tx(const FrameArgs& a, const BlockRec& b, const TxRec& tx,
   itx_warp<CG>(p, a.coef + tx.coef_off, tmp, dst, g.stride, a.maxv, lane);
 }
 
+/* Dequantisation on the device: a frame's coded levels, in scan order, into
+ * the raster the inverse transforms read (the reference front end's
+ * dequantise_tile fill, dequant.hpp:317-345, with dequantise_level,
+ * dequant.hpp:94-106). One warp per coded transform: the raster is cleared
+ * with vector stores, then the lanes place the levels through the scan. It
+ * runs on the planner's upload stream right after the levels arrive, so it
+ * overlaps the frames still decoding; the rasters it writes are what the
+ * ITX kernels read next, mostly out of L2. */
+__global__ void __launch_bounds__(256) k_dequant(const DqRec* __restrict__ jobs, int n,
+                                                 const short* __restrict__ levels,
+                                                 const unsigned char* __restrict__ qm,
+                                                 int* __restrict__ coef, int bit_depth) {
+  const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (j >= n) return;
+  const DqRec r = jobs[j];
+  const int area = 1 << (r.alw + r.alh);
+  int* raster = coef + r.coef_off;
+  if ((r.coef_off & 3) == 0) {
+    int4* v = reinterpret_cast<int4*>(raster);
+    for (int k = lane; k < (area >> 2); k += 32) v[k] = make_int4(0, 0, 0, 0);
+  } else {
+    for (int k = lane; k < area; k += 32) raster[k] = 0;
+  }
+  __syncwarp();
+  const short* lv = levels + r.level_off;
+  const unsigned short* scan = kScans + r.scan_off;
+  const unsigned char* m = r.qm_off >= 0 ? qm + r.qm_off : nullptr;
+  const int hi = (1 << (7 + bit_depth)) - 1, lo = -(1 << (7 + bit_depth));
+  for (int i = lane; i < r.count; i += 32) {
+    const int level = lv[i];
+    const int pos = scan[i];
+    if (level == 0 || pos >= area) continue;
+    int step = pos == 0 ? r.dc_step : r.ac_step;
+    if (m) step = (step * m[pos] + 16) >> 5;
+    const long long prod = static_cast<long long>(level) * step;
+    const unsigned mag = static_cast<unsigned>((prod < 0 ? -prod : prod) & 0xFFFFFF);
+    const int scaled = static_cast<int>(mag / r.denom);
+    raster[pos] = clampi(prod < 0 ? -scaled : scaled, lo, hi);
+  }
+}
+
+cudaError_t launch_dequant(const DqRec* jobs, int n, const short* levels, const unsigned char* qm,
+                           int* coef, int bit_depth, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_dequant<<<(n + 7) / 8, 256, 0, s>>>(jobs, n, levels, qm, coef, bit_depth);
+  return cudaGetLastError();
+}
+
 /* Inverse transforms, in batches of one size class: a warp runs 32 / S
  * transforms whose longer side is S (S = 4, 8, 16, 32; one of 64), one lane
  * group of S lanes each, so a 4x4 transform no longer leaves 28 lanes idle.
@@ -1391,7 +1440,8 @@ static cudaError_t load_all_kernels() {
       (e = load_kernel(k_cdef_search)) != cudaSuccess || (e = load_kernel(k_cdef)) != cudaSuccess ||
       (e = load_kernel(k_upscale)) != cudaSuccess || (e = load_kernel(k_lr_tile)) != cudaSuccess ||
       (e = load_kernel(k_grain_template)) != cudaSuccess || (e = load_kernel(k_grain_blend)) != cudaSuccess ||
-      (e = load_kernel(k_nv12)) != cudaSuccess || (e = load_kernel(k_rgb)) != cudaSuccess)
+      (e = load_kernel(k_nv12)) != cudaSuccess || (e = load_kernel(k_rgb)) != cudaSuccess ||
+      (e = load_kernel(k_dequant)) != cudaSuccess)
     return e;
   return cudaSuccess;
 }

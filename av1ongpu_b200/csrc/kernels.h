@@ -88,6 +88,8 @@ cudaError_t launch_selftest_wait(const unsigned* flag, int* status, unsigned lon
  * added, phase B residual computed ahead); 3: the dependency-scheduled
  * phase B. */
 cudaError_t launch_recon_stage(int stage, const FrameArgs& a, int n_sm, cudaStream_t s);
+cudaError_t launch_dequant(const DqRec* jobs, int n, const short* levels, const unsigned char* qm,
+                           int* coef, int bit_depth, cudaStream_t s);
 cudaError_t launch_deblock(px_t* pic, const DeblockRec* recs, int n, int sharpness, int bd,
                            int maxv, cudaStream_t s);
 /* CDEF: the direction searches - every 8x8 luma block of a grid_w-wide grid

@@ -124,7 +124,16 @@ typedef struct av1b_film_grain {
 } av1b_film_grain;
 
 /* FrameSyntax (av1gpu.hpp:476-537): the scalars and one (pointer, count) per
- * vector. Nothing is retained after the call that takes it returns. */
+ * vector. Nothing is retained after the call that takes it returns.
+ *
+ * Coefficients arrive one of two ways. A frame with n_levels == 0 brings its
+ * dequantised rasters in `coefficients` (TransformBlock::coef_offset). A frame
+ * with coded levels (n_levels > 0, as the reference front end leaves them with
+ * its levels_only dequantiser, dequant.hpp:200-210) is dequantised on the
+ * device from `levels` (level_offset, eob), the per-transform dc_step,
+ * ac_step, denominator and qm_off into `qm_pool`; its `coefficients`, if
+ * any, are then not read - the reference engine's device-dequantiser path
+ * (engine.cpp:386, 655-670). */
 typedef struct av1b_frame_syntax {
   int32_t width, coded_width, height, bit_depth, ss_x, ss_y;
   int32_t base_q_idx, sharpness, enable_intra_edge_filter;

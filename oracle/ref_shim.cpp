@@ -15,6 +15,8 @@
  * tests and benchmark use, and are rebuilt into the reference's FrameSyntax
  * field by field (av1ongpu_b200/csrc/flat_syntax.hpp).
  */
+#include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -27,6 +29,8 @@
 #include "av1gpu/av1gpu.hpp"
 #include "av1gpu_kernels.h"
 #include "flat_syntax.hpp"
+#include "frontend/coef_model.hpp"
+#include "frontend/dequant.hpp"
 
 namespace {
 
@@ -192,6 +196,85 @@ __attribute__((visibility("default"))) int av1ref_blob_counts(const uint8_t* blo
   for (int i = 0; i < 11; ++i) out[i] = n[i];
   return 11;
 }
+
+/* Test support for device dequantisation. From a frame that carries coded
+ * levels, two serialized frames: `with_qm` is the frame with a quantiser
+ * matrix pool (4096 bytes of values 1..255 drawn from `seed`; seed 0: all 32,
+ * the identity) and a matrix on every transform that has levels, at a seeded
+ * offset; `expanded` is that
+ * same frame with the coefficient rasters the reference front end's host fill
+ * builds from those levels (dequant.hpp:317-345, through its own coef_scan
+ * and dequantise_level) and no levels. The caller frees both with
+ * av1ref_free. Returns 0, or -1 for a malformed blob. */
+__attribute__((visibility("default"))) int av1ref_dequant_pair(const uint8_t* blob, size_t len,
+                                                               uint32_t seed, uint8_t** with_qm,
+                                                               size_t* with_qm_len,
+                                                               uint8_t** expanded,
+                                                               size_t* expanded_len) {
+  namespace fe = av1gpu::frontend;
+  av1b_frame_syntax v;
+  if (!av1b::view_blob(blob, len, &v)) return -1;
+  std::vector<uint8_t> qm(4096);
+  uint32_t x = seed * 2654435761u + 1;
+  for (uint8_t& b : qm) {
+    x ^= x << 13;
+    x ^= x >> 17;
+    x ^= x << 5;
+    b = seed ? static_cast<uint8_t>(1 + x % 255) : 32;
+  }
+  std::vector<av1b_transform> txs(v.transforms, v.transforms + v.n_transforms);
+  size_t pool = 0;
+  for (av1b_transform& t : txs) {
+    const int aw = t.w < 32 ? t.w : 32, ah = t.h < 32 ? t.h : 32;
+    pool = std::max(pool, static_cast<size_t>(t.coef_offset) + static_cast<size_t>(aw) * ah);
+    if (t.eob <= 0) continue;
+    x ^= x << 13;
+    x ^= x >> 17;
+    x ^= x << 5;
+    t.qm_off = static_cast<int32_t>(x % (4096 - aw * ah + 1));
+  }
+  std::vector<int32_t> coef(pool + 64, 0);
+  for (const av1b_transform& t : txs) {
+    if (t.eob <= 0) continue;
+    fe::TxSize size;
+    for (size.lw = 0; (4 << size.lw) < t.w; ++size.lw) {}
+    for (size.lh = 0; (4 << size.lh) < t.h; ++size.lh) {}
+    const fe::TxSize adjusted = fe::adjusted_tx_size(size);
+    const int area = (4 << adjusted.lw) * (4 << adjusted.lh);
+    const fe::ScanOrder scan = fe::coef_scan(adjusted, t.tx_type);
+    const int count = t.eob < scan.count ? t.eob : scan.count;
+    for (int i = 0; i < count; ++i) {
+      const int pos = scan.at(i);
+      if (pos < 0 || pos >= area) continue;
+      const int level = v.levels[t.level_offset + i];
+      if (level == 0) continue;
+      int step = pos == 0 ? t.dc_step : t.ac_step;
+      step = (step * qm[t.qm_off + pos] + 16) >> 5;
+      coef[t.coef_offset + pos] = fe::dequantise_level(level, step, t.denominator, v.bit_depth);
+    }
+  }
+  av1b_frame_syntax a = v;
+  a.transforms = txs.data();
+  a.qm_pool = qm.data();
+  a.n_qm_pool = qm.size();
+  av1b_frame_syntax b = a;
+  b.levels = nullptr;
+  b.n_levels = 0;
+  b.coefficients = coef.data();
+  b.n_coefficients = coef.size();
+  std::vector<uint8_t> out_a, out_b;
+  av1b::write_blob(a, &out_a);
+  av1b::write_blob(b, &out_b);
+  *with_qm = static_cast<uint8_t*>(std::malloc(out_a.size()));
+  *expanded = static_cast<uint8_t*>(std::malloc(out_b.size()));
+  std::memcpy(*with_qm, out_a.data(), out_a.size());
+  std::memcpy(*expanded, out_b.data(), out_b.size());
+  *with_qm_len = out_a.size();
+  *expanded_len = out_b.size();
+  return 0;
+}
+
+__attribute__((visibility("default"))) void av1ref_free(void* p) { std::free(p); }
 
 /* FNV-1a 64 over `n` bytes, seeded with `h` (0xcbf29ce484222325 to start): the
  * frame hash of the reference's stream tests (tools/av1gpu_decode.cpp:131-140),

@@ -46,6 +46,9 @@ def ref_lib():
         L.av1ref_fnv1a64.argtypes = [ctypes.c_uint64, ctypes.c_void_p, ctypes.c_size_t]
         L.av1ref_fnv1a64.restype = ctypes.c_uint64
         L.av1ref_blob_counts.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
+        L.av1ref_dequant_pair.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint32] + \
+            [ctypes.c_void_p] * 4
+        L.av1ref_free.argtypes = [ctypes.c_void_p]
         _ref = L
     return _ref
 
@@ -116,6 +119,24 @@ def blob_counts(blob):
     if ref_lib().av1ref_blob_counts(blob.ptr, blob.size, out) != 11:
         raise ValueError('malformed blob')
     return dict(zip(BLOB_ARRAYS, list(out)))
+
+
+def dequant_pair(blob_bytes, seed):
+    """(levels frame with seeded quantiser matrices, the same frame expanded
+    into coefficient rasters by the reference front end's host dequantiser),
+    both as serialized bytes, from a serialized levels frame."""
+    src = av1b.Blob.from_bytes(blob_bytes)
+    pa, pb = ctypes.c_void_p(), ctypes.c_void_p()
+    na, nb = ctypes.c_size_t(), ctypes.c_size_t()
+    L = ref_lib()
+    if L.av1ref_dequant_pair(src.ptr, src.size, seed, ctypes.byref(pa), ctypes.byref(na),
+                             ctypes.byref(pb), ctypes.byref(nb)):
+        raise ValueError('malformed blob')
+    try:
+        return ctypes.string_at(pa, na.value), ctypes.string_at(pb, nb.value)
+    finally:
+        L.av1ref_free(pa)
+        L.av1ref_free(pb)
 
 
 def picture_hash(planes, bit_depth, yuv16):

@@ -54,11 +54,12 @@ class Fixture:
         return [e for e in self.events if e[0] == DECODE]
 
 
-def replay(fx, dec, limit=None, keep_pictures=False):
+def replay(fx, dec, limit=None, keep_pictures=False, rewrite=None):
     """Runs the fixture's calls on `dec` (av1ongpu_b200.Decoder or
     refdec.RefDecoder). Returns (hashes of the shown pictures, pictures in
     decode order when keep_pictures else None). Slots are the decoder's own:
-    the recorded ones are mapped as they are returned."""
+    the recorded ones are mapped as they are returned. `rewrite(k, bytes)`,
+    when given, replaces the k-th decode's serialized frame."""
     slot_of = {-1: -1}
     shown_hash = []
     by_decode = []
@@ -67,6 +68,8 @@ def replay(fx, dec, limit=None, keep_pictures=False):
         if limit is not None and len(shown_hash) >= limit:
             break
         if kind == DECODE:
+            if rewrite is not None:
+                payload = rewrite(len(by_decode), payload)
             blob = av1b.Blob.from_bytes(payload)
             blob.set_refs([slot_of[s] for s in blob.get_refs()])
             bit_depth = blob.header[3]

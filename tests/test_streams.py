@@ -53,3 +53,16 @@ def test_levels_fixture_matches_coefficient_fixture(av1b, oracle, name):
             if k not in ('coefficients', 'levels'):
                 assert ca[k] == cb[k], k
     assert levels > 0
+
+
+@pytest.mark.parametrize('name', LEVEL_NAMES or ['none'])
+def test_host_expansion_of_levels_matches_stream_hashes(oracle, name):
+    """The levels fixtures, expanded on the host by the reference front end's
+    own dequantiser (through an identity quantiser matrix on every transform,
+    so the matrix path runs too), decode to the dav1d hashes: the levels,
+    offsets and steps the device dequantiser reads are pinned."""
+    need_fixtures()
+    fx = sr.Fixture(name, levels=True)
+    got, _ = sr.replay(fx, oracle.RefDecoder(),
+                       rewrite=lambda k, p: oracle.dequant_pair(p, 0)[1])
+    assert got == fx.hashes

@@ -50,3 +50,47 @@ def test_stream_matches_recorded_hashes(av1b, dec, oracle, name):
         bad = [i for i, (a, b) in enumerate(zip(got, fx.hashes)) if a != b]
         pytest.fail('%s: shown frames %s differ; %s' % (name, bad[:8],
                                                        first_difference(fx, dec, oracle)))
+
+
+@pytest.mark.parametrize('name', sr.fixture_names(levels=True) or ['none'])
+def test_stream_from_levels_matches_recorded_hashes(av1b, dec, oracle, name):
+    """The same streams as the reference pipeline hands a device dequantiser:
+    coded levels, per-transform steps and QM offsets, no coefficient pool. The
+    rasters are built on the device (k_dequant) and must give the same frames."""
+    if not sr.fixture_names(levels=True):
+        pytest.skip('no stream fixtures (make -C oracle streams)')
+    fx = sr.Fixture(name, levels=True)
+    got, _ = sr.replay(fx, dec)
+    assert len(got) == len(fx.hashes)
+    if got != fx.hashes:
+        bad = [i for i, (a, b) in enumerate(zip(got, fx.hashes)) if a != b]
+        pytest.fail('%s (levels): shown frames %s differ; %s' % (
+            name, bad[:8], first_difference(sr.Fixture(name), dec, oracle)))
+
+
+@pytest.mark.parametrize('name', ['lr_10bit', 'aom_444_10bit_320x240', 'lw_t2', 'tiles_grid'])
+def test_quantiser_matrices_on_device(av1b, dec, oracle, name):
+    """No test stream codes quantiser matrices, so they are planted: every
+    coded transform of a levels stream gets a seeded matrix out of a seeded
+    pool. The CUDA path dequantises the levels on the device; the oracle
+    decodes the same frames expanded by the reference front end's own host
+    dequantiser. Every picture must agree."""
+    if name not in sr.fixture_names(levels=True):
+        pytest.skip('no stream fixtures (make -C oracle streams)')
+    fx = sr.Fixture(name, levels=True)
+    pairs = {}
+
+    def pair(k, payload):
+        if k not in pairs:
+            pairs[k] = oracle.dequant_pair(payload, 1000 + k)
+        return pairs[k]
+
+    _, mine = sr.replay(fx, dec, keep_pictures=True, rewrite=lambda k, p: pair(k, p)[0])
+    _, ref = sr.replay(fx, oracle.RefDecoder(), keep_pictures=True,
+                       rewrite=lambda k, p: pair(k, p)[1])
+    assert len(mine) == len(ref)
+    for k, (a, b) in enumerate(zip(mine, ref)):
+        for p in range(3):
+            d = np.argwhere(a[p] != b[p])
+            assert not len(d), '%s decode %d plane %d: %d samples differ, first %s' % (
+                name, k, p, len(d), tuple(d[0]))
