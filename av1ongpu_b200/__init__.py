@@ -87,6 +87,12 @@ _SIGNATURES = {
                                            ctypes.c_void_p, ctypes.c_size_t]),
     'av1b_nv12_size': (ctypes.c_size_t, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                          ctypes.c_size_t]),
+    'av1b_nv12_pack_begin': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t,
+                                            ctypes.POINTER(ctypes.c_int)]),
+    'av1b_nv12_pack_wait': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                           ctypes.c_size_t, ctypes.c_void_p,
+                                           ctypes.POINTER(ctypes.c_size_t)]),
+    'av1b_nv12_pack_release': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     'av1b_to_rgb': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                    ctypes.c_void_p, ctypes.c_size_t]),
     'av1b_get_stats': (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Stats)]),
@@ -337,6 +343,32 @@ class Decoder:
         out = np.empty(n, dtype=np.uint8)
         self._check(lib().av1b_to_nv12(self.h, slot, pitch, out.ctypes.data, n), 'to_nv12')
         return out
+
+    def nv12_pack_begin(self, slot, pitch):
+        """Starts packing `slot` as NV12 (device pack, read back on a side
+        stream into page-locked memory); returns a handle for nv12_pack_wait."""
+        h = ctypes.c_int(-1)
+        self._check(lib().av1b_nv12_pack_begin(self.h, slot, pitch, ctypes.byref(h)),
+                    'nv12_pack_begin')
+        return h.value
+
+    def nv12_pack_wait(self, handle, out=None):
+        """Waits for a pack. With `out` (a uint8 array) the bytes are copied
+        into it and it is returned; without, a uint8 view of the page-locked
+        bytes is returned, valid until nv12_pack_release."""
+        data = ctypes.c_void_p()
+        n = ctypes.c_size_t(0)
+        if out is not None:
+            self._check(lib().av1b_nv12_pack_wait(self.h, handle, out.ctypes.data, out.nbytes, None,
+                                                  ctypes.byref(n)), 'nv12_pack_wait')
+            return out[:n.value]
+        self._check(lib().av1b_nv12_pack_wait(self.h, handle, None, 0, ctypes.byref(data),
+                                              ctypes.byref(n)), 'nv12_pack_wait')
+        buf = (ctypes.c_uint8 * n.value).from_address(data.value)
+        return np.frombuffer(buf, dtype=np.uint8)
+
+    def nv12_pack_release(self, handle):
+        self._check(lib().av1b_nv12_pack_release(self.h, handle), 'nv12_pack_release')
 
     def to_rgb(self, slot, matrix, rng, width, height):
         out = np.empty(width * height * 3, dtype=np.uint8)

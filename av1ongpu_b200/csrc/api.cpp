@@ -279,7 +279,7 @@ class B200Decoder final : public Decoder {
   }
 
   bool supports_preplanning() const override { return true; }
-  bool dequantises_on_device() const override { return false; }
+  bool dequantises_on_device() const override { return true; }
   bool packs_nv12_on_device() const override { return true; }
 
   void release_reference(int slot) override { av1b_release_reference(h_, slot); }
@@ -311,29 +311,26 @@ class B200Decoder final : public Decoder {
   }
 
   int nv12_pack_begin(int slot, size_t pitch, std::string* error) override {
-    std::vector<uint8_t> bytes;
-    if (!to_nv12(slot, pitch, &bytes, error)) return -1;
-    std::lock_guard<std::mutex> lk(mu_);
-    const int handle = next_handle_++;
-    packs_[handle] = std::move(bytes);
+    int handle = -1;
+    if (av1b_nv12_pack_begin(h_, slot, pitch, &handle) != AV1B_OK) {
+      if (error) *error = av1b_last_error(h_);
+      return -1;
+    }
     return handle;
   }
 
   bool nv12_pack_wait(int handle, std::vector<uint8_t>* nv12, std::string* error) override {
-    std::lock_guard<std::mutex> lk(mu_);
-    auto it = packs_.find(handle);
-    if (it == packs_.end()) {
-      if (error) *error = "unknown NV12 pack handle";
+    const uint8_t* data = nullptr;
+    size_t bytes = 0;
+    if (av1b_nv12_pack_wait(h_, handle, nullptr, 0, &data, &bytes) != AV1B_OK) {
+      if (error) *error = av1b_last_error(h_);
       return false;
     }
-    if (nv12) *nv12 = it->second;
+    if (nv12) nv12->assign(data, data + bytes);
     return true;
   }
 
-  void nv12_pack_release(int handle) override {
-    std::lock_guard<std::mutex> lk(mu_);
-    packs_.erase(handle);
-  }
+  void nv12_pack_release(int handle) override { av1b_nv12_pack_release(h_, handle); }
 
   void hold_output(bool hold) override { hold_.store(hold, std::memory_order_relaxed); }
 
@@ -399,8 +396,6 @@ class B200Decoder final : public Decoder {
   Geom geom_;
   std::mutex mu_;
   std::map<void*, Geom> plan_geom_;
-  std::map<int, std::vector<uint8_t>> packs_;
-  int next_handle_ = 1;
   std::atomic<bool> hold_{false};
 };
 

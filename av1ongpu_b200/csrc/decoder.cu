@@ -132,6 +132,23 @@ struct av1b_decoder {
   void* slot_ptr_host[32] = {nullptr};
   struct av1b_plan* own_plan = nullptr;
 
+  /* split NV12 packs (av1b_nv12_pack_begin / wait / release): each entry a
+   * device buffer the pack kernel writes on the decoder's stream and a
+   * page-locked one the copy stream reads it back into, so the read back
+   * overlaps the next frame's decode. pack_mu guards the table; a wait does
+   * not hold `mu`. */
+  struct Pack {
+    DevBuf dev;
+    uint8_t* host = nullptr;
+    size_t host_cap = 0, bytes = 0;
+    cudaEvent_t packed = nullptr, copied = nullptr;
+    int handle = -1;               /* -1: free */
+  };
+  std::mutex pack_mu;
+  std::vector<Pack> packs;
+  int next_pack = 0;
+  cudaStream_t copy_stream = nullptr;
+
   /* optional per-stage device timing (CUDA events on the decoder's stream) */
   unsigned long long wait_ns = 1000000000ull;   /* one dependency wait: 1 s */
   bool profiling = false;
@@ -2223,6 +2240,15 @@ int av1b_decoder_destroy(av1b_decoder* d) {
   if (d->ev_join) cudaEventDestroy(d->ev_join);
   if (d->ev_block) cudaEventDestroy(d->ev_block);
   if (d->status_host) cudaFreeHost(d->status_host);
+  for (auto& k : d->packs) {
+    if (k.copied) cudaEventSynchronize(k.copied);
+    if (k.host) cudaFreeHost(k.host);
+    if (k.packed) cudaEventDestroy(k.packed);
+    if (k.copied) cudaEventDestroy(k.copied);
+    dev_release(d, k.dev);
+  }
+  d->packs.clear();
+  if (d->copy_stream) cudaStreamDestroy(d->copy_stream);
   DevBuf* bufs[] = {&d->cur, &d->snap, &d->lr_pre, &d->lr_pre_up, &d->lr_cdef, &d->disp,
                     &d->slot_ptr_dev, &d->arena, &d->coef, &d->residual, &d->done,
                     &d->status_q, &d->nv12, &d->rgb,
@@ -2397,6 +2423,101 @@ int av1b_to_nv12(av1b_decoder* d, int slot, size_t pitch, uint8_t* dst, size_t d
 
 int av1b_to_nv12_device(av1b_decoder* d, int slot, size_t pitch, void* dst_device, size_t dst_len) {
   return to_nv12_impl(d, slot, pitch, static_cast<uint8_t*>(dst_device), dst_len, true);
+}
+
+/* The split pack. Up to eight packs are outstanding at once: a caller that
+ * holds more gets AV1B_ERR_NOMEM until it releases one. */
+constexpr int kMaxPacks = 8;
+
+int av1b_nv12_pack_begin(av1b_decoder* d, int slot, size_t pitch, int* out_handle) {
+  if (!d || !out_handle) return AV1B_ERR_ARG;
+  *out_handle = -1;
+  std::lock_guard<std::mutex> lk(d->mu);
+  cudaSetDevice(d->device);
+  const px_t* pic = nullptr;
+  int rc = picture_of(d, slot, &pic);
+  if (rc) return rc;
+  const size_t bytes = nv12_bytes(d->width, d->height, d->ss_x, d->ss_y, pitch);
+  if (bytes == 0 || pitch > (1u << 30))
+    return fail(d, AV1B_ERR_ARG, "NV12 output needs a 4:2:0 frame and an even pitch at least as wide");
+  std::lock_guard<std::mutex> pk(d->pack_mu);
+  if (!d->copy_stream)
+    CK(cudaStreamCreateWithFlags(&d->copy_stream, cudaStreamNonBlocking), "copy stream");
+  av1b_decoder::Pack* e = nullptr;
+  for (auto& k : d->packs)
+    if (k.handle < 0) {
+      e = &k;
+      break;
+    }
+  if (!e) {
+    if (d->packs.size() >= static_cast<size_t>(kMaxPacks))
+      return fail(d, AV1B_ERR_NOMEM, "every NV12 pack entry is in use; release one first");
+    if (d->packs.empty()) d->packs.reserve(kMaxPacks);
+    d->packs.emplace_back();
+    e = &d->packs.back();
+    CK(cudaEventCreateWithFlags(&e->packed, cudaEventDisableTiming), "event");
+    CK(cudaEventCreateWithFlags(&e->copied, cudaEventDisableTiming | cudaEventBlockingSync), "event");
+  }
+  if ((rc = dev_ensure(d, e->dev, bytes))) return rc;
+  if (e->host_cap < bytes) {
+    if (e->host) cudaFreeHost(e->host);
+    e->host = nullptr;
+    e->host_cap = 0;
+    CK(cudaHostAlloc(reinterpret_cast<void**>(&e->host), bytes, cudaHostAllocDefault),
+       "page-locked NV12 buffer");
+    e->host_cap = bytes;
+  }
+  uint8_t* dev = static_cast<uint8_t*>(e->dev.p);
+  CK(timed(d, kStNv12, [&] { return launch_nv12(pic, dev, d->L, static_cast<int>(pitch), d->stream); }),
+     "NV12 pack");
+  CK(cudaEventRecord(e->packed, d->stream), "event");
+  CK(cudaStreamWaitEvent(d->copy_stream, e->packed, 0), "copy stream wait");
+  CK(cudaMemcpyAsync(e->host, dev, bytes, cudaMemcpyDeviceToHost, d->copy_stream), "NV12 read back");
+  CK(cudaEventRecord(e->copied, d->copy_stream), "event");
+  e->bytes = bytes;
+  e->handle = d->next_pack = (d->next_pack + 1) & 0x3fffffff;
+  *out_handle = e->handle;
+  return AV1B_OK;
+}
+
+int av1b_nv12_pack_wait(av1b_decoder* d, int handle, uint8_t* dst, size_t dst_len,
+                        const uint8_t** data, size_t* bytes) {
+  if (!d || handle < 0) return AV1B_ERR_ARG;
+  cudaEvent_t ev = nullptr;
+  const uint8_t* host = nullptr;
+  size_t n = 0;
+  {
+    std::lock_guard<std::mutex> pk(d->pack_mu);
+    for (auto& k : d->packs)
+      if (k.handle == handle) {
+        ev = k.copied;
+        host = k.host;
+        n = k.bytes;
+      }
+  }
+  if (!ev) return fail(d, AV1B_ERR_ARG, "unknown NV12 pack handle");
+  if (dst && dst_len < n) return fail(d, AV1B_ERR_ARG, "NV12 destination too small");
+  cudaSetDevice(d->device);
+  CK(cudaEventSynchronize(ev), "NV12 pack wait");
+  /* the entry stays ours until release: its bytes do not change */
+  if (dst) std::memcpy(dst, host, n);
+  if (data) *data = host;
+  if (bytes) *bytes = n;
+  return AV1B_OK;
+}
+
+int av1b_nv12_pack_release(av1b_decoder* d, int handle) {
+  if (!d || handle < 0) return AV1B_ERR_ARG;
+  std::lock_guard<std::mutex> pk(d->pack_mu);
+  for (auto& k : d->packs)
+    if (k.handle == handle) {
+      /* a pack released unwaited still finishes before its buffers are reused */
+      cudaSetDevice(d->device);
+      cudaEventSynchronize(k.copied);
+      k.handle = -1;
+      return AV1B_OK;
+    }
+  return fail(d, AV1B_ERR_ARG, "unknown NV12 pack handle");
 }
 
 int av1b_to_rgb(av1b_decoder* d, int slot, int matrix, int range, uint8_t* dst, size_t dst_len) {

@@ -340,22 +340,16 @@ def run_ours(args):
     h2d = sum(b.size for b in pinned)
     e2e_dec = av1b.Decoder(local)
     e2e_ring = [e2e_dec.reserve_reference() for _ in range(4)]
-    # NV12 out: packed on the decoder's stream into one of two device
-    # buffers, copied to pinned host memory on a copy stream, so frame k's
-    # read back overlaps frame k + 1's decode
-    nv12_dev = [torch.empty(geo['nv12'], dtype=torch.uint8, device='cuda:%d' % local) for _ in range(2)]
-    nv12_host = [torch.empty(geo['nv12'], dtype=torch.uint8, pin_memory=True) for _ in range(2)]
-    dec_stream = torch.cuda.ExternalStream(e2e_dec.stream(), device='cuda:%d' % local)
-    copy_stream = torch.cuda.Stream(device='cuda:%d' % local)
 
     def e2e_step():
         """One step through the public plan / decode API, pipelined the way the
         API is meant for: two planner threads plan frames k + 1 .. k + 3
         (validation, records, upload from the pinned host blob) while the
-        device decodes frame k; its NV12 is packed on the device
-        (av1b_to_nv12_device) and read back into pinned host memory while
-        frame k + 1 decodes. Frames decode in order; the host holds frame
-        k - 1's NV12 once frame k is queued."""
+        device decodes frame k; its NV12 goes out through the split pack
+        (av1b_nv12_pack_begin / wait / release: packed on the device, read back
+        into the library's page-locked memory on its copy stream while frame
+        k + 1 decodes). Frames decode in order; the host holds frame k - 1's
+        NV12 once frame k is queued."""
         ahead = 3
 
         def plan(k):
@@ -371,7 +365,7 @@ def run_ours(args):
                 raise av1b.Av1bError(rc, 'plan_frame')
             return h
 
-        copied = [None, None]
+        packs = []
         with ThreadPoolExecutor(max_workers=2) as ex:
             futs = {k: ex.submit(plan, k) for k in range(min(ahead, len(pinned)))}
             for k in range(len(pinned)):
@@ -384,23 +378,15 @@ def run_ours(args):
                 if rc:
                     raise av1b.Av1bError(rc, 'decode_planned')
                 av1b.lib().av1b_plan_free(e2e_dec.h, h)
-                i = k & 1
-                if copied[i] is not None:
-                    copied[i].synchronize()  # frame k - 2's copy out of this buffer
-                e2e_dec.to_nv12_device(e2e_ring[k % 4], PITCH, nv12_dev[i].data_ptr(), geo['nv12'])
-                packed = torch.cuda.Event()
-                packed.record(dec_stream)
-                copy_stream.wait_event(packed)
-                with torch.cuda.stream(copy_stream):
-                    nv12_host[i].copy_(nv12_dev[i], non_blocking=True)
-                    copied[i] = torch.cuda.Event()
-                    copied[i].record(copy_stream)
-                if copied[i ^ 1] is not None:
-                    copied[i ^ 1].synchronize()  # frame k - 1's NV12 is on the host
+                packs.append(e2e_dec.nv12_pack_begin(e2e_ring[k % 4], PITCH))
+                if len(packs) > 1:
+                    hd = packs.pop(0)
+                    e2e_dec.nv12_pack_wait(hd)  # frame k - 1's NV12 is on the host
+                    e2e_dec.nv12_pack_release(hd)
             e2e_dec.sync()
-            for c in copied:
-                if c is not None:
-                    c.synchronize()
+            for hd in packs:
+                e2e_dec.nv12_pack_wait(hd)
+                e2e_dec.nv12_pack_release(hd)
 
     e2e_s = float('inf')
     if not args.no_e2e:

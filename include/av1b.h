@@ -235,6 +235,19 @@ AV1B_API int av1b_to_nv12(av1b_decoder* dec, int slot, size_t pitch, uint8_t* ds
 /* Same, but `dst` is device memory: the zero-copy end of the path. */
 AV1B_API int av1b_to_nv12_device(av1b_decoder* dec, int slot, size_t pitch, void* dst_device,
                         size_t dst_len);
+/* Decoder::nv12_pack_begin / nv12_pack_wait / nv12_pack_release
+ * (av1gpu.hpp:748-772): the pack split so the read back leaves the decoding
+ * thread. begin packs `slot` on the device (the picture to_nv12 would give)
+ * and starts its copy into page-locked memory on a side stream, so the next
+ * frame's decode overlaps it; it returns a handle. wait blocks until the
+ * bytes are there and copies them to `dst` (may be null), and/or points
+ * `*data` at the page-locked bytes, valid until release; `*bytes` is their
+ * count. Up to eight packs are outstanding; begin returns AV1B_ERR_NOMEM
+ * while all are held. */
+AV1B_API int av1b_nv12_pack_begin(av1b_decoder* dec, int slot, size_t pitch, int* out_handle);
+AV1B_API int av1b_nv12_pack_wait(av1b_decoder* dec, int handle, uint8_t* dst, size_t dst_len,
+                                 const uint8_t** data, size_t* bytes);
+AV1B_API int av1b_nv12_pack_release(av1b_decoder* dec, int handle);
 /* The byte count to_nv12 produces (factory.cpp:236-244's nv12_buffer_size):
  * 0 for a frame that is not 4:2:0, an odd pitch or a pitch below a chroma row. */
 AV1B_API size_t av1b_nv12_size(int width, int height, int ss_x, int ss_y, size_t pitch);

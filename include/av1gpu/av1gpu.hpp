@@ -11,9 +11,7 @@
  *
  * Differences a caller can observe:
  *   - BackendKind::Cpu and BackendKind::OpenCL are refused by Decoder::create
- *     (there is one backend, CUDA on sm_100a, and no CPU fallback);
- *   - dequantises_on_device() is false: the coefficient pool is uploaded as
- *     given (the levels path is not implemented yet).
+ *     (there is one backend, CUDA on sm_100a, and no CPU fallback).
  */
 #ifndef AV1GPU_AV1GPU_HPP
 #define AV1GPU_AV1GPU_HPP

@@ -1,7 +1,8 @@
 /*
  * api_client.cpp - a client of the av1gpu::Decoder C++ API, written the way a
  * user of the reference library writes one: create, decode_reference into
- * reference slots, release, to_nv12, plan_frame / decode_reference_planned.
+ * reference slots, release, to_nv12 and the split nv12_pack_begin / wait /
+ * release, plan_frame / decode_reference_planned.
  * The frames come from the workload generator as serialized syntax and are
  * rebuilt into av1gpu::FrameSyntax. Output: the decoded planes and NV12 bytes
  * of every frame, appended to a binary file the test compares with the oracle.
@@ -69,9 +70,20 @@ int main(int argc, char** argv) {
                     frame.plane_width(p), out);
     std::vector<uint8_t> nv12;
     const size_t pitch = (w + 63) & ~63;
-    if (!dec->to_nv12(slot, pitch, &nv12, &err)) {
-      std::fprintf(stderr, "to_nv12: %s\n", err.c_str());
-      return 1;
+    if (k % 2 == 0) {
+      if (!dec->to_nv12(slot, pitch, &nv12, &err)) {
+        std::fprintf(stderr, "to_nv12: %s\n", err.c_str());
+        return 1;
+      }
+    } else {
+      /* the split pack, the way a pipeline's output stage uses it */
+      if (!dec->packs_nv12_on_device()) return 1;
+      const int handle = dec->nv12_pack_begin(slot, pitch, &err);
+      if (handle < 0 || !dec->nv12_pack_wait(handle, &nv12, &err)) {
+        std::fprintf(stderr, "nv12_pack: %s\n", err.c_str());
+        return 1;
+      }
+      dec->nv12_pack_release(handle);
     }
     std::fwrite(nv12.data(), 1, nv12.size(), out);
     if (k >= 3) dec->release_reference(slot_of[k - 3]);

@@ -258,3 +258,41 @@ def test_hbm_budget_is_enforced(av1b):
         d.decode(av1b.synth_frame(1, 8, 1, 0))
     assert e.value.code == -3
     d.close()
+
+
+def test_nv12_split_pack(av1b, oracle, dec):
+    """nv12_pack_begin / wait / release (the reference's split pack,
+    av1gpu.hpp:748-772): a pack begun right after a frame carries that frame's
+    picture after film grain even when the next frame is decoded before the
+    wait; a pack of an older slot carries its stored picture; several packs
+    are outstanding at once; a view of the page-locked bytes and a copy agree."""
+    w, h = 240, 136
+    params = (w, h, 0, 10, 64, av1b.TOOLS_ALL, 30)
+    ref = oracle.RefDecoder()
+    sg, sr = oracle.Stream(dec), oracle.Stream(ref)
+    pitch = 256
+    pending = []
+    for k in range(5):
+        b = av1b.synth_frame_ex(*params[:6], 77, k, params[6])
+        sg.decode(k, b, read_back=False)
+        sr.decode(k, b, read_back=False)
+        expect = ref.to_nv12(sr.slots[k], pitch, w, h)
+        pending.append((dec.nv12_pack_begin(sg.slots[k], pitch), expect))
+        if k >= 1:
+            handle, want = pending.pop(0)
+            got = dec.nv12_pack_wait(handle)
+            assert np.array_equal(got, want), 'frame %d (packed before the next decode)' % (k - 1)
+            copy = dec.nv12_pack_wait(handle, np.empty(want.size, dtype=np.uint8))
+            assert np.array_equal(copy, want)
+            dec.nv12_pack_release(handle)
+    handle, want = pending.pop()
+    assert np.array_equal(dec.nv12_pack_wait(handle), want)
+    dec.nv12_pack_release(handle)
+    older = [dec.nv12_pack_begin(sg.slots[k], pitch) for k in (3, 4)]
+    for k, handle in zip((3, 4), older):
+        assert np.array_equal(dec.nv12_pack_wait(handle), ref.to_nv12(sr.slots[k], pitch, w, h))
+        dec.nv12_pack_release(handle)
+    with pytest.raises(av1b.Av1bError):
+        dec.nv12_pack_wait(older[0])
+    for s in list(sg.slots.values()):
+        dec.release_reference(s)
