@@ -276,6 +276,31 @@ __attribute__((visibility("default"))) int av1ref_dequant_pair(const uint8_t* bl
 
 __attribute__((visibility("default"))) void av1ref_free(void* p) { std::free(p); }
 
+/* Test support for stage-by-stage comparisons: a copy of a serialized frame
+ * without some of its in-loop stages. `drop` bit 0: the deblocking edges,
+ * bit 1: the CDEF blocks, bit 2: loop restoration (types and units), bit 3:
+ * film grain. The caller frees the copy with av1ref_free. Returns 0, or -1
+ * for a malformed blob. */
+__attribute__((visibility("default"))) int av1ref_strip(const uint8_t* blob, size_t len, int drop,
+                                                        uint8_t** out, size_t* out_len) {
+  av1b_frame_syntax v;
+  if (!av1b::view_blob(blob, len, &v)) return -1;
+  if (drop & 1) v.n_deblock = 0;
+  if (drop & 2) v.n_cdef = 0;
+  if (drop & 4)
+    for (int p = 0; p < 3; ++p) {
+      v.restoration_type[p] = 0;
+      v.n_restoration[p] = 0;
+    }
+  if (drop & 8) v.grain.apply = 0;
+  std::vector<uint8_t> bytes;
+  av1b::write_blob(v, &bytes);
+  *out = static_cast<uint8_t*>(std::malloc(bytes.size()));
+  std::memcpy(*out, bytes.data(), bytes.size());
+  *out_len = bytes.size();
+  return 0;
+}
+
 /* FNV-1a 64 over `n` bytes, seeded with `h` (0xcbf29ce484222325 to start): the
  * frame hash of the reference's stream tests (tools/av1gpu_decode.cpp:131-140),
  * chainable so a picture can be hashed plane by plane. */

@@ -49,6 +49,8 @@ def ref_lib():
         L.av1ref_dequant_pair.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint32] + \
             [ctypes.c_void_p] * 4
         L.av1ref_free.argtypes = [ctypes.c_void_p]
+        L.av1ref_strip.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_void_p,
+                                   ctypes.c_void_p]
         _ref = L
     return _ref
 
@@ -137,6 +139,23 @@ def dequant_pair(blob_bytes, seed):
     finally:
         L.av1ref_free(pa)
         L.av1ref_free(pb)
+
+
+DROP_DEBLOCK, DROP_CDEF, DROP_LR, DROP_GRAIN = 1, 2, 4, 8
+
+
+def strip_stages(blob_bytes, drop):
+    """A serialized frame without the in-loop stages named by `drop`
+    (DROP_* bits), as bytes."""
+    src = av1b.Blob.from_bytes(blob_bytes)
+    p, n = ctypes.c_void_p(), ctypes.c_size_t()
+    L = ref_lib()
+    if L.av1ref_strip(src.ptr, src.size, drop, ctypes.byref(p), ctypes.byref(n)):
+        raise ValueError('malformed blob')
+    try:
+        return ctypes.string_at(p, n.value)
+    finally:
+        L.av1ref_free(p)
 
 
 def picture_hash(planes, bit_depth, yuv16):

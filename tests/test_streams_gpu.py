@@ -94,3 +94,38 @@ def test_quantiser_matrices_on_device(av1b, dec, oracle, name):
             d = np.argwhere(a[p] != b[p])
             assert not len(d), '%s decode %d plane %d: %d samples differ, first %s' % (
                 name, k, p, len(d), tuple(d[0]))
+
+
+STAGES = {
+    'reconstruction': 15,      # prediction and residual only
+    'deblock': 14,             # + the deblocking filter
+    'cdef': 12,                # + CDEF
+    'restoration': 8,          # + superres upscaling and loop restoration, no grain
+}
+
+
+@pytest.mark.parametrize('stage', list(STAGES))
+def test_streams_stage_by_stage(av1b, dec, oracle, stage):
+    """Every stream with the in-loop stages after `stage` taken out of its
+    frames, through the CUDA path and the oracle: the pictures must agree
+    frame by frame, so a difference is pinned to the first stage that shows
+    it (the job-level isolation the reference gets from replaying its plan
+    files, here on real streams above the API boundary)."""
+    if not NAMES:
+        pytest.skip('no stream fixtures (make -C oracle streams)')
+    drop = STAGES[stage]
+    bad = []
+    for name in NAMES:
+        fx = sr.Fixture(name)
+        strip = {}
+
+        def rewrite(k, p):
+            if k not in strip:
+                strip[k] = oracle.strip_stages(p, drop)
+            return strip[k]
+
+        mine, _ = sr.replay(fx, dec, rewrite=rewrite)
+        ref, _ = sr.replay(fx, oracle.RefDecoder(), rewrite=rewrite)
+        if mine != ref:
+            bad.append((name, [i for i, (a, b) in enumerate(zip(mine, ref)) if a != b][:4]))
+    assert not bad, '%s: %s' % (stage, bad)
