@@ -359,9 +359,6 @@ struct PlanLists {
   pvec<int2> inter_tiles;
   pvec<int2> itx_jobs;            /* sorted by size class, then shape and type */
   pvec<int4> itx_batches;         /* (first job, jobs, log2 class or 7 = raw) */
-  pvec<DeblockRec> deblock_v, deblock_h;
-  pvec<CdefRec> cdef;
-  pvec<unsigned> cdef_search;     /* searches off the 8x8 grid: x | y << 16 */
   pvec<LrUnitRec> lr_units[3];
   pvec<DqRec> dq;                 /* coded transforms to dequantise (levels frames) */
 };
@@ -385,11 +382,6 @@ struct Plan {
          n_cdef_search = 0;
   int unit_depth = 0;             /* dependency depth of the frame */
   bool units_inter = false;       /* some phase B block is an inter kind */
-  pvec<int2> inter_tiles;
-  pvec<int2> itx_jobs;
-  pvec<DeblockRec> deblock_v, deblock_h;
-  pvec<CdefRec> cdef;
-  pvec<unsigned> cdef_search;     /* searches off the 8x8 grid: x | y << 16 */
   int itx_class_first[8] = {0}, itx_class_count[8] = {0};  /* batches per class */
   int cdef_grid_w = 0, cdef_grid_n = 0;  /* the grid of 8x8 luma searches */
   bool cdef_search_any = false;          /* some record reads the grid */
@@ -761,96 +753,9 @@ int plan_block(const PlanCtx& ctx, const av1b_frame_syntax& s, size_t bi, BlockR
 
 
 /* The deblocking edges of one piece of the frame, vertical and horizontal. */
-struct EdgeOut {
-  std::vector<DeblockRec> v, h;
-  PlanErr err;
-};
-
-int plan_edge(const PlanCtx& c, const av1b_frame_syntax& s, size_t i, EdgeOut* O) {
-  const Layout& L = c.L;
-  const av1b_deblock_edge& e = s.deblock[i];
-  if (e.plane < 0 || e.plane > 2) return O->err.set(AV1B_ERR_SYNTAX, "deblock plane out of range");
-  if (e.length <= 0 || e.level == 0) return AV1B_OK;
-  if (e.level < 0 || e.level > 63) return O->err.set(AV1B_ERR_SYNTAX, "deblock level out of range");
-  if (e.filter_size != 4 && e.filter_size != 8 && e.filter_size != 16)
-    return O->err.set(AV1B_ERR_SYNTAX, "deblock filter size must be 4, 8 or 16");
-  const PlaneGeom& g = L.p[e.plane];
-  const int rows = plane_rows(L, e.plane);
-  /* how far the filter reaches across the edge: p6..q6 at most */
-  const int reach = e.filter_size == 16 ? 7 : (e.filter_size == 4 ? 2 : 4);
-  DeblockRec r{};
-  r.len = static_cast<short>(e.length);
-  r.level = static_cast<short>(e.level);
-  r.filter_size = static_cast<unsigned char>(e.filter_size);
-  r.chroma = e.plane != 0;
-  if (e.vertical) {
-    if (e.x - reach < 0 || e.x + reach > g.stride || e.y < 0 || e.y + e.length > rows)
-      return O->err.set(AV1B_ERR_SYNTAX, "deblock edge reaches outside the picture");
-    r.p_off = g.off + e.y * g.stride + e.x - 2;
-    r.across = 1;
-    r.along = g.stride;
-    O->v.push_back(r);
-  } else {
-    if (e.y - reach < 0 || e.y + reach > rows || e.x < 0 || e.x + e.length > g.stride)
-      return O->err.set(AV1B_ERR_SYNTAX, "deblock edge reaches outside the picture");
-    r.p_off = g.off + (e.y - 2) * g.stride + e.x;
-    r.across = g.stride;
-    r.along = 1;
-    O->h.push_back(r);
-  }
-  return AV1B_OK;
-}
-
-/* The CDEF records of one piece of the frame. A block whose direction is
- * searched reads the search of its 8x8 luma block from a grid the device
- * fills (every cell searched once); a luma position off the 8x8 grid gets a
- * search of its own, listed after the grid. */
-struct CdefOut {
-  std::vector<size_t> unaligned;
-  bool any = false;
-  PlanErr err;
-};
-
-int plan_cdef(const PlanCtx& ctx, const av1b_frame_syntax& s, size_t i, int grid_w, CdefRec* out,
-              CdefOut* O) {
-  const Layout& L = ctx.L;
-  const av1b_cdef_block& c = s.cdef[i];
-  if (c.plane < 0 || c.plane > 2) return O->err.set(AV1B_ERR_SYNTAX, "CDEF plane out of range");
-  const int sx = c.plane ? L.ss_x : 0, sy = c.plane ? L.ss_y : 0;
-  const int bw = 8 >> sx, bh = 8 >> sy;
-  const PlaneGeom& g = L.p[c.plane];
-  if (c.x < 0 || c.y < 0 || c.x + bw + 2 > g.stride || c.y + bh + 2 > plane_rows(L, c.plane) ||
-      (c.x << sx) + 8 > L.p[0].stride || (c.y << sy) + 8 > plane_rows(L, 0))
-    return O->err.set(AV1B_ERR_SYNTAX, "CDEF block outside the picture");
-  if (c.dir < -1 || c.dir > 7 || c.pri_strength < 0 || c.pri_strength > 255 ||
-      c.sec_strength < 0 || c.sec_strength > 255 || c.damping < 0 || c.damping > 63)
-    return O->err.set(AV1B_ERR_SYNTAX, "CDEF parameters out of range");
-  CdefRec& r = out[i];
-  r.x = static_cast<short>(c.x);
-  r.y = static_cast<short>(c.y);
-  r.plane = static_cast<unsigned char>(c.plane);
-  r.pri = static_cast<unsigned char>(c.pri_strength);
-  r.sec = static_cast<unsigned char>(c.sec_strength);
-  r.damping = static_cast<unsigned char>(c.damping);
-  r.dir = static_cast<signed char>(c.dir);
-  r.search = -1;
-  if (c.dir < 0) {
-    const int lx = c.x << sx, ly = c.y << sy;
-    if ((lx | ly) & 7) {
-      O->unaligned.push_back(i);
-    } else {
-      r.search = (ly >> 3) * grid_w + (lx >> 3);
-      O->any = true;
-    }
-  }
-  return AV1B_OK;
-}
-
 /* The planner's per-piece outputs, kept between frames for their capacity. */
 struct PlanScratch {
   std::vector<BlockOut> blocks;
-  std::vector<EdgeOut> edges;
-  std::vector<CdefOut> cdef;
   std::vector<int> owner[3];
   std::vector<std::vector<int>> unit_deps;
   std::vector<int> dep_count, depth, sorted;
@@ -911,11 +816,20 @@ int plan_units(av1b_decoder* d, const PlanCtx& c, Plan* P) {
   std::vector<uint8_t>& is_b = S.is_b;
   is_b.resize(nb);
   bool aligned[3] = {true, true, true};
-  for (size_t bi = 0; bi < nb; ++bi) {
-    const BlockRec& b = P->R->blocks[bi];
-    const int m = (1 << sh[b.plane]) - 1;
-    if ((b.x | b.y | b.w | b.h) & m) aligned[b.plane] = false;
-    is_b[bi] = b.phase_b;
+  {
+    const int pieces = pieces_for(nb, c, 4096);
+    std::vector<uint8_t> unaligned(static_cast<size_t>(pieces) * 3, 0);
+    c.pool->run(pieces, [&](int i) {
+      uint8_t* u = &unaligned[static_cast<size_t>(i) * 3];
+      for (size_t bi = piece_begin(nb, pieces, i); bi < piece_begin(nb, pieces, i + 1); ++bi) {
+        const BlockRec& b = P->R->blocks[bi];
+        const int m = (1 << sh[b.plane]) - 1;
+        if ((b.x | b.y | b.w | b.h) & m) u[b.plane] = 1;
+        is_b[bi] = b.phase_b;
+      }
+    });
+    for (size_t k = 0; k < unaligned.size(); ++k)
+      if (unaligned[k]) aligned[k % 3] = false;
   }
   auto fill = [&](size_t bi) {
     const BlockRec& b = P->R->blocks[bi];
@@ -965,8 +879,9 @@ int plan_units(av1b_decoder* d, const PlanCtx& c, Plan* P) {
       BlockRec& b = P->R->blocks[bi];
       const int p = b.plane, oc = 1 << sh[p];
       mine.clear();
+      /* neighbouring cells mostly share an owner: skip the repeat at once */
       auto wait_on = [&](int o) {
-        if (o >= 0 && o < bi && is_b[o]) mine.push_back(o);
+        if (o >= 0 && o < bi && is_b[o] && (mine.empty() || mine.back() != o)) mine.push_back(o);
       };
       int har = b.have_ar, hbl = b.have_bl;
       if (b.kind == AV1B_U_INTRA) {
@@ -1014,8 +929,12 @@ int plan_units(av1b_decoder* d, const PlanCtx& c, Plan* P) {
       if (b.kind == AV1B_U_INTRA && b.mode == 13 && !b.palette)
         each_cell(0, b.x << L.ss_x, (b.x + b.w - 1) << L.ss_x, b.y << L.ss_y,
                   (b.y + b.h - 1) << L.ss_y, wait_on);
-      for (size_t x = 1; x < mine.size(); ++x)  /* short lists: insertion sort */
-        for (size_t y = x; y > 0 && mine[y - 1] > mine[y]; --y) std::swap(mine[y - 1], mine[y]);
+      if (mine.size() > 24) {
+        std::sort(mine.begin(), mine.end());
+      } else {
+        for (size_t x = 1; x < mine.size(); ++x)  /* short lists: insertion sort */
+          for (size_t y = x; y > 0 && mine[y - 1] > mine[y]; --y) std::swap(mine[y - 1], mine[y]);
+      }
       mine.erase(std::unique(mine.begin(), mine.end()), mine.end());
       /* prediction and residual fuse when the transforms cover disjoint parts
        * of the block (each sample then gets at most one residual) */
@@ -1167,6 +1086,70 @@ void plan_itx(const PlanCtx& c, Plan* P) {
   }
 }
 
+/* Stages the profiler reports (av1b_profile). */
+enum Stage {
+  kStOwner, kStInter, kStItx, kStUnits, kStDeblockV, kStDeblockH, kStCdef, kStUpscale, kStLr,
+  kStGrainTemplate, kStGrainBlend, kStNv12, kStRgb, kStCopy,
+  /* host time of plan_frame: records, the wait for the staging buffer, the
+   * copy into it; and the parts of the records: blocks, the dependency
+   * schedule, the transform batches, the filter lists, film grain */
+  kStPlanHost, kStWaitHost, kStStageHost, kStPlanBlocks, kStPlanUnits, kStPlanItx, kStPlanFilters,
+  kStPlanGrain, kStageCount
+};
+static_assert(kStageCount <= 24, "profile table");
+const char* const kStageNames[kStageCount] = {
+    "owner", "inter", "itx", "units", "deblock_v", "deblock_h", "cdef", "upscale", "lr",
+    "grain_template", "grain_blend", "nv12", "rgb", "copy", "plan_host", "wait_host", "stage_host",
+    "blocks_host", "units_host", "itx_host", "filters_host", "grain_host"};
+
+/* Host time since `t0` into a host stage, when profiling. */
+void host_mark(av1b_decoder* d, int stage, std::chrono::steady_clock::time_point t0) {
+  if (!d->profiling) return;
+  std::lock_guard<std::mutex> lk(d->prof_mu);
+  d->prof_ms[stage] +=
+      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  d->prof_n[stage] += 1;
+}
+
+/* The first invalid deblocking edge or CDEF block of a frame, in list order
+ * (edges first): the device conversion only reports that there is one. The
+ * lists are checked in pieces on the pool; the earliest piece's first invalid
+ * record is the one a single pass in order meets. */
+int filter_records_error(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s) {
+  struct List {
+    size_t n;
+    std::function<int(size_t)> check;
+  };
+  const List lists[2] = {
+      {s.n_deblock,
+       [&](size_t i) {
+         DeblockRec r;
+         int vertical;
+         return prep_edge(c.L, s.deblock[i], &r, &vertical);
+       }},
+      {s.n_cdef, [&](size_t i) {
+         CdefRec r;
+         int off_grid;
+         return prep_cdef(c.L, s.cdef[i], c.L.p[0].stride >> 3, &r, &off_grid);
+       }}};
+  for (const List& l : lists) {
+    const int pieces = pieces_for(l.n, c, 4096);
+    std::vector<int> first(pieces, kPrepOk);
+    c.pool->run(pieces, [&](int i) {
+      for (size_t k = piece_begin(l.n, pieces, i); k < piece_begin(l.n, pieces, i + 1); ++k) {
+        const int code = l.check(k);
+        if (code >= kPrepErrFirst) {
+          first[i] = code;
+          break;
+        }
+      }
+    });
+    for (int i = 0; i < pieces; ++i)
+      if (first[i] >= kPrepErrFirst) return fail(d, AV1B_ERR_SYNTAX, kPrepMessages[first[i]]);
+  }
+  return AV1B_OK;
+}
+
 /* Validates a frame and builds its device records. The blocks, deblocking
  * edges and CDEF blocks are converted in pieces on the pool; each piece stops
  * at its first invalid record and the error of the earliest piece is the one
@@ -1176,6 +1159,11 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
   const Layout& L = c.L;
   const int bd = s.bit_depth;
   int rc_units;
+  auto tp = std::chrono::steady_clock::now();
+  auto phase = [&](int stage) {
+    host_mark(d, stage, tp);
+    tp = std::chrono::steady_clock::now();
+  };
   sized(P->R->blocks, s.n_blocks);
   for (int i = 0; i < 7; ++i) {
     const int rw = s.reference_width[i] > 0 ? s.reference_width[i] : s.width;
@@ -1272,78 +1260,28 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
       std::copy(O.dq.begin(), O.dq.end(), P->R->dq.begin() + o_dq[i]);
     });
   }
+  phase(kStPlanBlocks);
   if ((rc_units = plan_units(d, c, P))) return rc_units;
+  phase(kStPlanUnits);
   plan_itx(c, P);
+  phase(kStPlanItx);
 
   /* the pools read past the caller's arrays as zeros, like the reference's
    * padded plan pools (engine.cpp:665-674) */
   P->coef_pool = c.levels ? coef_end + 64 : std::max(coef_end + 64, s.n_coefficients);
   P->residual_pool = std::max(res_end + 64, s.n_residual);
 
-  /* deblocking edges: V then H, each a list of independent edges */
-  P->R->deblock_v.clear();
-  P->R->deblock_h.clear();
+  /* deblocking edges and CDEF blocks: converted on the device where they
+   * are uploaded (plan_frame, k_prep_filters) */
   if (s.sharpness < 0 || s.sharpness > 7) return fail(d, AV1B_ERR_SYNTAX, "sharpness out of range");
-  {
-    const size_t ne = s.n_deblock;
-    const int pieces = pieces_for(ne, c, 4096);
-    std::vector<EdgeOut>& outs = c.scratch->edges;
-    if (outs.size() < static_cast<size_t>(pieces)) outs.resize(pieces);
-    c.pool->run(pieces, [&](int i) {
-      EdgeOut* O = &outs[i];
-      O->v.clear();
-      O->h.clear();
-      O->err = PlanErr();
-      for (size_t k = piece_begin(ne, pieces, i); k < piece_begin(ne, pieces, i + 1); ++k)
-        if (plan_edge(c, s, k, O)) break;
-    });
-    size_t nv = 0, nh = 0;
-    std::vector<size_t> ov(pieces), oh(pieces);
-    for (int i = 0; i < pieces; ++i) {
-      if (outs[i].err.code) return fail(d, outs[i].err.code, outs[i].err.msg);
-      ov[i] = nv;
-      oh[i] = nh;
-      nv += outs[i].v.size();
-      nh += outs[i].h.size();
-    }
-    sized(P->R->deblock_v, nv);
-    sized(P->R->deblock_h, nh);
-    c.pool->run(pieces, [&](int i) {
-      std::copy(outs[i].v.begin(), outs[i].v.end(), P->R->deblock_v.begin() + ov[i]);
-      std::copy(outs[i].h.begin(), outs[i].h.end(), P->R->deblock_h.begin() + oh[i]);
-    });
-  }
-
-  /* CDEF */
-  {
-    const size_t nc = s.n_cdef;
-    sized(P->R->cdef, nc);
-    P->R->cdef_search.clear();
-    P->cdef_grid_w = L.p[0].stride >> 3;
-    P->cdef_grid_n = P->cdef_grid_w * (plane_rows(L, 0) >> 3);
-    const int pieces = pieces_for(nc, c, 4096);
-    std::vector<CdefOut>& outs = c.scratch->cdef;
-    if (outs.size() < static_cast<size_t>(pieces)) outs.resize(pieces);
-    c.pool->run(pieces, [&](int i) {
-      CdefOut* O = &outs[i];
-      O->unaligned.clear();
-      O->any = false;
-      O->err = PlanErr();
-      for (size_t k = piece_begin(nc, pieces, i); k < piece_begin(nc, pieces, i + 1); ++k)
-        if (plan_cdef(c, s, k, P->cdef_grid_w, P->R->cdef.data(), O)) break;
-    });
-    P->cdef_search_any = false;
-    for (int i = 0; i < pieces; ++i) {
-      if (outs[i].err.code) return fail(d, outs[i].err.code, outs[i].err.msg);
-      P->cdef_search_any |= outs[i].any;
-      for (size_t k : outs[i].unaligned) {
-        const av1b_cdef_block& b = s.cdef[k];
-        const int sx = b.plane ? L.ss_x : 0, sy = b.plane ? L.ss_y : 0;
-        P->R->cdef[k].search = P->cdef_grid_n + static_cast<int>(P->R->cdef_search.size());
-        P->R->cdef_search.push_back(static_cast<unsigned>(b.x << sx) | (static_cast<unsigned>(b.y << sy) << 16));
-      }
-    }
-  }
+  P->cdef_grid_w = L.p[0].stride >> 3;
+  P->cdef_grid_n = P->cdef_grid_w * (plane_rows(L, 0) >> 3);
+  /* an error found after them still reports an invalid filter record first,
+   * as it comes earlier in the frame's validation order */
+  auto fail_late = [&](int code, const char* msg) {
+    const int rc = filter_records_error(d, c, s);
+    return rc ? rc : fail(d, code, msg);
+  };
 
   /* loop restoration */
   P->use_lr = false;
@@ -1353,7 +1291,7 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
     if (s.restoration_type[p] == 0) continue;
     const int sub_y = p ? L.ss_y : 0;
     if (s.restoration_unit_log2[p] < 5 || s.restoration_unit_log2[p] > 8)
-      return fail(d, AV1B_ERR_SYNTAX, "restoration unit size out of range");
+      return fail_late(AV1B_ERR_SYNTAX, "restoration unit size out of range");
     const int us = 1 << s.restoration_unit_log2[p];
     const int fh = (s.height + (sub_y ? 1 << (sub_y - 1) : 0)) >> sub_y;
     P->lr.type[p] = 1;
@@ -1383,6 +1321,8 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
     P->use_lr = true;
   }
 
+  phase(kStPlanFilters);
+
   /* film grain */
   P->grain = s.grain.apply != 0;
   if (P->grain) {
@@ -1392,7 +1332,7 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
         f.num_cr_points < 0 || f.num_cr_points > 16 || f.grain_scaling_minus_8 < 0 ||
         f.grain_scaling_minus_8 > 3 || f.ar_coeff_shift_minus_6 < 0 || f.ar_coeff_shift_minus_6 > 3 ||
         f.grain_scale_shift < 0 || f.grain_scale_shift > 3)
-      return fail(d, AV1B_ERR_SYNTAX, "film grain parameters out of range");
+      return fail_late(AV1B_ERR_SYNTAX, "film grain parameters out of range");
     auto check_points = [&](int n, const int32_t* v) {
       for (int i = 0; i < n; ++i) {
         if (v[i] < 0 || v[i] > 255) return false;
@@ -1403,7 +1343,7 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
     if (!check_points(f.num_y_points, f.point_y_value) ||
         !check_points(f.num_cb_points, f.point_cb_value) ||
         !check_points(f.num_cr_points, f.point_cr_value))
-      return fail(d, AV1B_ERR_SYNTAX, "film grain points must increase strictly within 0..255");
+      return fail_late(AV1B_ERR_SYNTAX, "film grain points must increase strictly within 0..255");
     GrainParamsDev& g = P->gp;
     std::memset(&g, 0, sizeof(g));
     g.seed = f.seed;
@@ -1463,6 +1403,7 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
     t.chroma_w = s.ss_x ? 44 : 82;
     t.chroma_h = s.ss_y ? 38 : 73;
   }
+  phase(kStPlanGrain);
   return AV1B_OK;
 }
 
@@ -1475,19 +1416,6 @@ size_t stage_put(size_t* off, const V& v) {
   *off = align_up(o + v.size() * sizeof(typename V::value_type), 256);
   return o;
 }
-
-/* Stages the profiler reports (av1b_profile). */
-enum Stage {
-  kStOwner, kStInter, kStItx, kStUnits, kStDeblockV, kStDeblockH, kStCdef, kStUpscale, kStLr,
-  kStGrainTemplate, kStGrainBlend, kStNv12, kStRgb, kStCopy,
-  /* host time of plan_frame: records, the wait for the staging buffer, the
-   * copy into it */
-  kStPlanHost, kStWaitHost, kStStageHost, kStageCount
-};
-static_assert(kStageCount <= 24, "profile table");
-const char* const kStageNames[kStageCount] = {
-    "owner", "inter", "itx", "units", "deblock_v", "deblock_h", "cdef", "upscale", "lr",
-    "grain_template", "grain_blend", "nv12", "rgb", "copy", "plan_host", "wait_host", "stage_host"};
 
 cudaEvent_t pool_event(av1b_decoder* d) {
   if (d->ev_used == d->ev_pool.size()) {
@@ -1512,15 +1440,6 @@ cudaError_t timed(av1b_decoder* d, int stage, F launch, cudaStream_t on = nullpt
   cudaEventRecord(b, on);
   d->marks.push_back(std::make_pair(stage, i0));
   return e;
-}
-
-/* Host time since `t0` into a host stage, when profiling. */
-void host_mark(av1b_decoder* d, int stage, std::chrono::steady_clock::time_point t0) {
-  if (!d->profiling) return;
-  std::lock_guard<std::mutex> lk(d->prof_mu);
-  d->prof_ms[stage] +=
-      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-  d->prof_n[stage] += 1;
 }
 
 /* After a synchronisation: folds the recorded stage times into the totals. */
@@ -1567,13 +1486,17 @@ struct av1b_plan {
   av1b::Plan P;                   /* host copy of the counts and constants */
   av1b::DevBuf arena, coef, residual;
   av1b::DevBuf dqsrc;             /* a levels frame's levels, then its QM pool */
+  /* the caller's deblocking edges and CDEF blocks as uploaded, and the
+   * records k_prep_filters makes of them (offsets o_de_raw .. o_prep) */
+  av1b::DevBuf filt;
+  av1b::PrepOut* prep_host = nullptr;   /* page-locked copy of the counts */
   /* ready: the uploads are done; done: the last frame that read this plan has
    * finished on the device (a plan is re-planned only after that) */
   cudaEvent_t ready = nullptr, done = nullptr;
   bool in_flight = false;
   size_t o_blocks = 0, o_txs = 0, o_obmc = 0, o_warps = 0, o_pal = 0, o_units = 0, o_deps = 0;
   size_t o_tiles = 0, o_itx = 0, o_itxb = 0, o_dbv = 0, o_dbh = 0, o_cdef = 0, o_lr[3] = {0, 0, 0};
-  size_t o_map = 0, o_cdef_search = 0, o_dq = 0;
+  size_t o_map = 0, o_cdef_search = 0, o_dq = 0, o_de_raw = 0, o_cb_raw = 0, o_prep = 0;
   int slots_read[kSlots + 1];     /* the reference slots the frame reads, -1 ended */
   int n_blocks = 0;
   bool owned_by_decoder = false;
@@ -1644,6 +1567,9 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
     CK(cudaEventCreateWithFlags(&pl->ready, cudaEventDisableTiming | cudaEventBlockingSync), "event");
     CK(cudaEventCreateWithFlags(&pl->done, cudaEventDisableTiming | cudaEventBlockingSync), "event");
   }
+  if (!pl->prep_host)
+    CK(cudaHostAlloc(reinterpret_cast<void**>(&pl->prep_host), sizeof(PrepOut), cudaHostAllocDefault),
+       "page-locked counts");
   if (pl->in_flight) {
     CK(cudaEventSynchronize(pl->done), "plan reuse wait");
     pl->in_flight = false;
@@ -1672,6 +1598,49 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
       CK(cudaMemcpyAsync(static_cast<uint8_t*>(pl->dqsrc.p) + qm_at, s.qm_pool, s.n_qm_pool,
                          cudaMemcpyHostToDevice, st), "quantiser matrix upload");
   }
+  /* the deblocking edges and CDEF blocks go up as they are and are converted
+   * on the device while the host plans the rest */
+  {
+    const size_t nde = s.n_deblock, ncb = s.n_cdef;
+    size_t fo = 0;
+    auto room = [&](size_t bytes) {
+      const size_t o = fo;
+      fo = align_up(fo + bytes, 256);
+      return o;
+    };
+    pl->o_de_raw = room(nde * sizeof(av1b_deblock_edge));
+    pl->o_cb_raw = room(ncb * sizeof(av1b_cdef_block));
+    pl->o_dbv = room(nde * sizeof(DeblockRec));
+    pl->o_dbh = room(nde * sizeof(DeblockRec));
+    pl->o_cdef = room(ncb * sizeof(CdefRec));
+    pl->o_cdef_search = room(ncb * sizeof(unsigned));
+    pl->o_prep = room(sizeof(PrepOut));
+    if ((rc = dev_ensure(d, pl->filt, fo, fo + fo / 2))) {
+      cudaStreamSynchronize(st);
+      return rc;
+    }
+    uint8_t* fl = static_cast<uint8_t*>(pl->filt.p);
+    if (nde)
+      CK(cudaMemcpyAsync(fl + pl->o_de_raw, s.deblock, nde * sizeof(av1b_deblock_edge),
+                         cudaMemcpyHostToDevice, st), "deblock edge upload");
+    if (ncb)
+      CK(cudaMemcpyAsync(fl + pl->o_cb_raw, s.cdef, ncb * sizeof(av1b_cdef_block),
+                         cudaMemcpyHostToDevice, st), "CDEF block upload");
+    CK(cudaMemsetAsync(fl + pl->o_prep, 0, sizeof(PrepOut), st), "count reset");
+    const int grid_w = c.L.p[0].stride >> 3;
+    CK(launch_prep_filters(reinterpret_cast<const av1b_deblock_edge*>(fl + pl->o_de_raw),
+                           static_cast<int>(nde),
+                           reinterpret_cast<const av1b_cdef_block*>(fl + pl->o_cb_raw),
+                           static_cast<int>(ncb), c.L, grid_w, grid_w * (plane_rows(c.L, 0) >> 3),
+                           reinterpret_cast<DeblockRec*>(fl + pl->o_dbv),
+                           reinterpret_cast<DeblockRec*>(fl + pl->o_dbh),
+                           reinterpret_cast<CdefRec*>(fl + pl->o_cdef),
+                           reinterpret_cast<unsigned*>(fl + pl->o_cdef_search),
+                           reinterpret_cast<PrepOut*>(fl + pl->o_prep), st),
+       "filter record launch");
+    CK(cudaMemcpyAsync(pl->prep_host, fl + pl->o_prep, sizeof(PrepOut), cudaMemcpyDeviceToHost, st),
+       "count read back");
+  }
   if (s.n_residual)
     CK(cudaMemcpyAsync(pl->residual.p, s.residual, s.n_residual * sizeof(int),
                        cudaMemcpyHostToDevice, st), "residual upload");
@@ -1691,10 +1660,6 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
   P.n_tiles = P.R->inter_tiles.size();
   P.n_itx = P.R->itx_jobs.size();
   P.n_itxb = P.R->itx_batches.size();
-  P.n_dbv = P.R->deblock_v.size();
-  P.n_dbh = P.R->deblock_h.size();
-  P.n_cdef = P.R->cdef.size();
-  P.n_cdef_search = P.R->cdef_search.size();
   pl->L = c.L;
   pl->width = s.width;
   pl->height = s.height;
@@ -1728,10 +1693,6 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
   pl->o_tiles = stage_put(&off, P.R->inter_tiles);
   pl->o_itx = stage_put(&off, P.R->itx_jobs);
   pl->o_itxb = stage_put(&off, P.R->itx_batches);
-  pl->o_dbv = stage_put(&off, P.R->deblock_v);
-  pl->o_dbh = stage_put(&off, P.R->deblock_h);
-  pl->o_cdef = stage_put(&off, P.R->cdef);
-  pl->o_cdef_search = stage_put(&off, P.R->cdef_search);
   for (int p = 0; p < 3; ++p) pl->o_lr[p] = stage_put(&off, P.R->lr_units[p]);
   pl->o_dq = stage_put(&off, P.R->dq);
   pl->o_map = off;
@@ -1758,10 +1719,6 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
   CK(put(pl->o_tiles, P.R->inter_tiles), "record upload");
   CK(put(pl->o_itx, P.R->itx_jobs), "record upload");
   CK(put(pl->o_itxb, P.R->itx_batches), "record upload");
-  CK(put(pl->o_dbv, P.R->deblock_v), "record upload");
-  CK(put(pl->o_dbh, P.R->deblock_h), "record upload");
-  CK(put(pl->o_cdef, P.R->cdef), "record upload");
-  CK(put(pl->o_cdef_search, P.R->cdef_search), "record upload");
   for (int p = 0; p < 3; ++p) CK(put(pl->o_lr[p], P.R->lr_units[p]), "record upload");
   CK(put(pl->o_dq, P.R->dq), "record upload");
   if (s.n_palette_map)
@@ -1803,6 +1760,16 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
   t0 = std::chrono::steady_clock::now();
   CK(cudaEventSynchronize(pl->ready), "upload wait");
   host_mark(d, kStWaitHost, t0);
+  const PrepOut po = *pl->prep_host;
+  if (po.bad) {
+    rc = filter_records_error(d, c, s);
+    return rc ? rc : fail(d, AV1B_ERR_SYNTAX, "invalid deblocking edge or CDEF block");
+  }
+  P.n_dbv = po.n_v;
+  P.n_dbh = po.n_h;
+  P.n_cdef = s.n_cdef;
+  P.n_cdef_search = po.n_extra;
+  P.cdef_search_any = po.any_grid != 0;
   P.R = nullptr;
   return AV1B_OK;
 }
@@ -1972,15 +1939,16 @@ int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, cons
 
   /* ---- filters --------------------------------------------------------------------------- */
   px_t* cur = a.cur;
+  const uint8_t* fl = static_cast<const uint8_t*>(pl->filt.p);
   if ((P.n_dbv != 0))
     CK(timed(d, kStDeblockV, [&] {
-         return launch_deblock(cur, reinterpret_cast<const DeblockRec*>(ar + pl->o_dbv),
+         return launch_deblock(cur, reinterpret_cast<const DeblockRec*>(fl + pl->o_dbv),
                                static_cast<int>(P.n_dbv), pl->sharpness, pl->bit_depth,
                                maxv, st);
        }), "deblock V");
   if ((P.n_dbh != 0))
     CK(timed(d, kStDeblockH, [&] {
-         return launch_deblock(cur, reinterpret_cast<const DeblockRec*>(ar + pl->o_dbh),
+         return launch_deblock(cur, reinterpret_cast<const DeblockRec*>(fl + pl->o_dbh),
                                static_cast<int>(P.n_dbh), pl->sharpness, pl->bit_depth,
                                maxv, st);
        }), "deblock H");
@@ -1995,10 +1963,10 @@ int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, cons
          return cudaMemcpyAsync(snap, cur, pic_bytes, cudaMemcpyDeviceToDevice, st);
        }), "CDEF snapshot");
     CK(timed(d, kStCdef, [&] {
-         return launch_cdef(snap, cur, reinterpret_cast<const CdefRec*>(ar + pl->o_cdef),
+         return launch_cdef(snap, cur, reinterpret_cast<const CdefRec*>(fl + pl->o_cdef),
                             static_cast<int>(P.n_cdef), P.cdef_grid_w, P.cdef_grid_n,
                             P.cdef_search_any,
-                            reinterpret_cast<const unsigned*>(ar + pl->o_cdef_search),
+                            reinterpret_cast<const unsigned*>(fl + pl->o_cdef_search),
                             static_cast<int>(P.n_cdef_search),
                             static_cast<int*>(d->cdef_search.p), L, st);
        }), "CDEF");
@@ -2092,6 +2060,8 @@ void release_plan(av1b_decoder* d, av1b_plan* pl) {
   dev_release(d, pl->coef);
   dev_release(d, pl->residual);
   dev_release(d, pl->dqsrc);
+  dev_release(d, pl->filt);
+  if (pl->prep_host) cudaFreeHost(pl->prep_host);
   if (pl->ready) cudaEventDestroy(pl->ready);
   if (pl->done) cudaEventDestroy(pl->done);
   delete pl;

@@ -1357,6 +1357,79 @@ cudaError_t launch_recon_stage(int stage, const FrameArgs& a, int n_sm, cudaStre
   return cudaGetLastError();
 }
 
+/* A frame's deblocking edges and CDEF blocks, converted where the caller's
+ * lists were uploaded: one thread per record validates and converts it
+ * (prep_edge / prep_cdef, the checks the host planner runs too). Edges are
+ * compacted into the V and H lists with one atomic per warp: the edges of one
+ * direction are independent, so their order in a list does not matter. A CDEF
+ * block off the 8x8 search grid gets a search of its own, listed after the
+ * grid. `out` (zeroed by the caller) gets the counts and the invalid flag. */
+__global__ void __launch_bounds__(256) k_prep_filters(
+    const av1b_deblock_edge* __restrict__ de, int nde, const av1b_cdef_block* __restrict__ cb,
+    int ncb, const Layout L, int grid_w, int grid_n, DeblockRec* __restrict__ v,
+    DeblockRec* __restrict__ h, CdefRec* __restrict__ cdef, unsigned* __restrict__ extra,
+    PrepOut* __restrict__ out) {
+  const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const bool is_edge = i < nde, is_cdef = !is_edge && i < static_cast<long long>(nde) + ncb;
+  int code = kPrepSkip, vert = 0, off_grid = 0;
+  DeblockRec er{};
+  CdefRec cr{};
+  unsigned pos = 0;
+  if (is_edge) {
+    code = prep_edge(L, de[i], &er, &vert);
+  } else if (is_cdef) {
+    const av1b_cdef_block& c = cb[i - nde];
+    code = prep_cdef(L, c, grid_w, &cr, &off_grid);
+    if (code == kPrepOk && off_grid) {
+      const int sx = c.plane ? L.ss_x : 0, sy = c.plane ? L.ss_y : 0;
+      pos = static_cast<unsigned>(c.x << sx) | (static_cast<unsigned>(c.y << sy) << 16);
+    }
+  }
+  const bool ok = code == kPrepOk;
+  const unsigned mv = __ballot_sync(0xffffffffu, is_edge && ok && vert);
+  const unsigned mh = __ballot_sync(0xffffffffu, is_edge && ok && !vert);
+  const unsigned me = __ballot_sync(0xffffffffu, is_cdef && ok && off_grid);
+  const unsigned mg = __ballot_sync(0xffffffffu, is_cdef && ok && !off_grid && cr.dir < 0);
+  const unsigned mb = __ballot_sync(0xffffffffu, code >= kPrepErrFirst);
+  unsigned bv = 0, bh = 0, be = 0;
+  if (lane == 0) {
+    if (mv) bv = atomicAdd(&out->n_v, __popc(mv));
+    if (mh) bh = atomicAdd(&out->n_h, __popc(mh));
+    if (me) be = atomicAdd(&out->n_extra, __popc(me));
+    if (mg) atomicOr(&out->any_grid, 1u);
+    if (mb) atomicOr(&out->bad, 1u);
+  }
+  bv = __shfl_sync(0xffffffffu, bv, 0);
+  bh = __shfl_sync(0xffffffffu, bh, 0);
+  be = __shfl_sync(0xffffffffu, be, 0);
+  const unsigned below = (1u << lane) - 1u;
+  if (is_edge && ok) {
+    if (vert)
+      v[bv + __popc(mv & below)] = er;
+    else
+      h[bh + __popc(mh & below)] = er;
+  } else if (is_cdef && ok) {
+    if (off_grid) {
+      const unsigned k = be + __popc(me & below);
+      cr.search = grid_n + static_cast<int>(k);
+      extra[k] = pos;
+    }
+    cdef[i - nde] = cr;
+  }
+}
+
+cudaError_t launch_prep_filters(const av1b_deblock_edge* edges, int n_edges, const av1b_cdef_block* cdef,
+                                int n_cdef, const Layout& L, int grid_w, int grid_n, DeblockRec* v,
+                                DeblockRec* h, CdefRec* cdef_out, unsigned* extra, PrepOut* out,
+                                cudaStream_t s) {
+  const long long n = static_cast<long long>(n_edges) + n_cdef;
+  if (n <= 0) return cudaSuccess;
+  k_prep_filters<<<cdiv(n, 256), 256, 0, s>>>(edges, n_edges, cdef, n_cdef, L, grid_w, grid_n, v, h,
+                                              cdef_out, extra, out);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_deblock(px_t* pic, const DeblockRec* recs, int n, int sharpness, int bd, int maxv,
                            cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
@@ -1441,7 +1514,7 @@ static cudaError_t load_all_kernels() {
       (e = load_kernel(k_upscale)) != cudaSuccess || (e = load_kernel(k_lr_tile)) != cudaSuccess ||
       (e = load_kernel(k_grain_template)) != cudaSuccess || (e = load_kernel(k_grain_blend)) != cudaSuccess ||
       (e = load_kernel(k_nv12)) != cudaSuccess || (e = load_kernel(k_rgb)) != cudaSuccess ||
-      (e = load_kernel(k_dequant)) != cudaSuccess)
+      (e = load_kernel(k_dequant)) != cudaSuccess || (e = load_kernel(k_prep_filters)) != cudaSuccess)
     return e;
   return cudaSuccess;
 }

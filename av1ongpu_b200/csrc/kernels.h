@@ -9,6 +9,7 @@
 
 #include "dev_common.cuh"
 #include "dev_filters.cuh"
+#include "filter_prep.cuh"
 
 namespace av1b {
 
@@ -88,6 +89,10 @@ cudaError_t launch_selftest_wait(const unsigned* flag, int* status, unsigned lon
  * added, phase B residual computed ahead); 3: the dependency-scheduled
  * phase B. */
 cudaError_t launch_recon_stage(int stage, const FrameArgs& a, int n_sm, cudaStream_t s);
+cudaError_t launch_prep_filters(const av1b_deblock_edge* edges, int n_edges, const av1b_cdef_block* cdef,
+                                int n_cdef, const Layout& L, int grid_w, int grid_n, DeblockRec* v,
+                                DeblockRec* h, CdefRec* cdef_out, unsigned* extra, PrepOut* out,
+                                cudaStream_t s);
 cudaError_t launch_dequant(const DqRec* jobs, int n, const short* levels, const unsigned char* qm,
                            int* coef, int bit_depth, cudaStream_t s);
 cudaError_t launch_deblock(px_t* pic, const DeblockRec* recs, int n, int sharpness, int bd,

@@ -301,6 +301,47 @@ __attribute__((visibility("default"))) int av1ref_strip(const uint8_t* blob, siz
   return 0;
 }
 
+/* Test support for the error paths: a copy of a serialized frame with one
+ * record made invalid. `what` 1: deblocking edge `index` gets level 99;
+ * 2: edge `index` reaches outside the picture; 3: CDEF block `index` gets
+ * direction 9; 4: the luma restoration unit size becomes 8 samples (log2 3);
+ * 5: film grain is switched on with a seed out of range. The caller frees the
+ * copy with av1ref_free. Returns 0, or -1 for a malformed blob or index. */
+__attribute__((visibility("default"))) int av1ref_corrupt(const uint8_t* blob, size_t len, int what,
+                                                          size_t index, uint8_t** out,
+                                                          size_t* out_len) {
+  av1b_frame_syntax v;
+  if (!av1b::view_blob(blob, len, &v)) return -1;
+  std::vector<av1b_deblock_edge> edges(v.deblock, v.deblock + v.n_deblock);
+  std::vector<av1b_cdef_block> cdef(v.cdef, v.cdef + v.n_cdef);
+  if ((what == 1 || what == 2) && index >= edges.size()) return -1;
+  if (what == 3 && index >= cdef.size()) return -1;
+  if (what == 1 || what == 2) edges[index].length = std::max(edges[index].length, 4);
+  if (what == 1) edges[index].level = 99;
+  if (what == 2) {
+    edges[index].x = -64;
+    edges[index].vertical = 1;
+    edges[index].level = 10;
+  }
+  if (what == 3) cdef[index].dir = 9;
+  if (what == 4) {
+    v.restoration_type[0] = 1;
+    v.restoration_unit_log2[0] = 3;
+  }
+  if (what == 5) {
+    v.grain.apply = 1;
+    v.grain.seed = -1;
+  }
+  v.deblock = edges.data();
+  v.cdef = cdef.data();
+  std::vector<uint8_t> bytes;
+  av1b::write_blob(v, &bytes);
+  *out = static_cast<uint8_t*>(std::malloc(bytes.size()));
+  std::memcpy(*out, bytes.data(), bytes.size());
+  *out_len = bytes.size();
+  return 0;
+}
+
 /* FNV-1a 64 over `n` bytes, seeded with `h` (0xcbf29ce484222325 to start): the
  * frame hash of the reference's stream tests (tools/av1gpu_decode.cpp:131-140),
  * chainable so a picture can be hashed plane by plane. */

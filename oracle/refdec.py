@@ -51,6 +51,8 @@ def ref_lib():
         L.av1ref_free.argtypes = [ctypes.c_void_p]
         L.av1ref_strip.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_void_p,
                                    ctypes.c_void_p]
+        L.av1ref_corrupt.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_size_t,
+                                     ctypes.c_void_p, ctypes.c_void_p]
         _ref = L
     return _ref
 
@@ -154,6 +156,22 @@ def strip_stages(blob_bytes, drop):
         raise ValueError('malformed blob')
     try:
         return ctypes.string_at(p, n.value)
+    finally:
+        L.av1ref_free(p)
+
+
+CORRUPT_EDGE_LEVEL, CORRUPT_EDGE_OUTSIDE, CORRUPT_CDEF_DIR, CORRUPT_LR_UNIT, CORRUPT_GRAIN = 1, 2, 3, 4, 5
+
+
+def corrupt(blob, what, index=0):
+    """A copy of a serialized frame (an av1ongpu_b200.Blob) with one record
+    made invalid (CORRUPT_*), as a new Blob."""
+    p, n = ctypes.c_void_p(), ctypes.c_size_t()
+    L = ref_lib()
+    if L.av1ref_corrupt(blob.ptr, blob.size, what, index, ctypes.byref(p), ctypes.byref(n)):
+        raise ValueError('malformed blob or index')
+    try:
+        return av1b.Blob.from_bytes(ctypes.string_at(p, n.value))
     finally:
         L.av1ref_free(p)
 

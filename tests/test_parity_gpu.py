@@ -244,6 +244,36 @@ def test_errors_are_reported_not_faulted(av1b, dec):
     dec.release_reference(slot)
 
 
+def test_invalid_records_name_the_first_one(av1b, oracle, dec):
+    """Deblocking edges and CDEF blocks are validated on the device; an invalid
+    one fails the frame with the message of the first invalid record in the
+    frame's validation order (edges, then CDEF blocks, then restoration and
+    film grain), and the decoder stays usable."""
+    b = av1b.synth_frame(2, 8, 3, 0)
+
+    def error_of(blob):
+        with pytest.raises(av1b.Av1bError) as e:
+            dec.decode(blob)
+        assert e.value.code == -4
+        return str(e.value)
+
+    last = oracle.blob_counts(b)['deblock'] - 1
+    assert 'deblock level out of range' in error_of(oracle.corrupt(b, oracle.CORRUPT_EDGE_LEVEL, last))
+    assert 'outside the picture' in error_of(oracle.corrupt(b, oracle.CORRUPT_EDGE_OUTSIDE, 0))
+    assert 'CDEF parameters' in error_of(oracle.corrupt(b, oracle.CORRUPT_CDEF_DIR, 5))
+    both = oracle.corrupt(oracle.corrupt(b, oracle.CORRUPT_CDEF_DIR, 0), oracle.CORRUPT_EDGE_LEVEL, last)
+    assert 'deblock level' in error_of(both)
+    lr_and_cdef = oracle.corrupt(oracle.corrupt(b, oracle.CORRUPT_LR_UNIT), oracle.CORRUPT_CDEF_DIR, 7)
+    assert 'CDEF parameters' in error_of(lr_and_cdef)
+    assert 'restoration unit size' in error_of(oracle.corrupt(b, oracle.CORRUPT_LR_UNIT))
+    assert 'film grain' in error_of(oracle.corrupt(b, oracle.CORRUPT_GRAIN))
+    slot, planes = dec.decode(b)
+    ref_slot, ref_planes = oracle.RefDecoder().decode(b)
+    for p in range(3):
+        assert np.array_equal(planes[p], ref_planes[p])
+    dec.release_reference(slot)
+
+
 def test_bounded_wait_gives_up(dec):
     """A device wait on a flag nothing sets returns an error status after its
     limit instead of hanging (no fault, no trap)."""
