@@ -100,6 +100,9 @@ _SIGNATURES = {
     'av1b_slot_planes_device': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
                                                ctypes.c_void_p]),
     'av1b_last_error': (ctypes.c_char_p, [ctypes.c_void_p]),
+    'av1b_set_unit_trace': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    'av1b_unit_trace': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
+                                       ctypes.POINTER(ctypes.c_size_t)]),
     'av1b_decoder_stream': (ctypes.c_void_p, [ctypes.c_void_p]),
     'av1b_synth_frame': (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_uint64, ctypes.c_int,
                                         ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_size_t)]),
@@ -300,6 +303,21 @@ class Decoder:
 
     def set_profiling(self, on):
         self._check(lib().av1b_set_profiling(self.h, 1 if on else 0), 'set_profiling')
+
+    def set_unit_trace(self, on):
+        self._check(lib().av1b_set_unit_trace(self.h, 1 if on else 0), 'set_unit_trace')
+
+    def unit_trace(self):
+        """The last frame's phase B trace: an (n_blocks, 4) uint64 array of
+        (claimed, ready, published) globaltimer ns and the dependency
+        published last, zero rows for blocks outside phase B."""
+        n = ctypes.c_size_t(0)
+        self._check(lib().av1b_unit_trace(self.h, None, 0, ctypes.byref(n)), 'unit_trace')
+        out = np.zeros(n.value, dtype=np.uint64)
+        if n.value:
+            self._check(lib().av1b_unit_trace(self.h, out.ctypes.data, n.value, ctypes.byref(n)),
+                        'unit_trace')
+        return out.reshape(-1, 4)
 
     def profile(self):
         """{stage: (total_ms, launches)} since profiling was switched on."""

@@ -149,6 +149,11 @@ struct av1b_decoder {
   int next_pack = 0;
   cudaStream_t copy_stream = nullptr;
 
+  /* optional trace of phase B (av1b_set_unit_trace): 4 uint64 per block */
+  bool tracing = false;
+  DevBuf trace;
+  size_t trace_n = 0;
+
   /* optional per-stage device timing (CUDA events on the decoder's stream) */
   unsigned long long wait_ns = 1000000000ull;   /* one dependency wait: 1 s */
   bool profiling = false;
@@ -353,7 +358,8 @@ struct PlanLists {
   pvec<ObmcRec> obmc;
   pvec<WarpRec> warps;
   pvec<int> palette_colors;
-  pvec<int> units;                /* phase B blocks in claim order */
+  pvec<int> units;                /* phase B blocks, chain after chain */
+  pvec<int> chains;               /* where each chain starts in `units`, and the end */
   pvec<int> deps;                 /* per phase B block (dep_first, dep_count): the
                                      phase B blocks it waits for */
   pvec<int2> inter_tiles;
@@ -377,7 +383,7 @@ void sized(V& v, size_t n) {
 struct Plan {
   PlanLists* R = nullptr;         /* while planning: the lists being built */
   size_t n_tiles_simple = 0;      /* inter tiles the lean kernel takes (listed first) */
-  size_t n_blocks = 0, n_units = 0, n_tiles = 0, n_itx = 0, n_itxb = 0, n_dbv = 0, n_dbh = 0,
+  size_t n_blocks = 0, n_units = 0, n_chains = 0, n_tiles = 0, n_itx = 0, n_itxb = 0, n_dbv = 0, n_dbh = 0,
          n_cdef = 0,
          n_cdef_search = 0;
   int unit_depth = 0;             /* dependency depth of the frame */
@@ -752,18 +758,18 @@ int plan_block(const PlanCtx& ctx, const av1b_frame_syntax& s, size_t bi, BlockR
 }
 
 
-/* The deblocking edges of one piece of the frame, vertical and horizontal. */
 /* The planner's per-piece outputs, kept between frames for their capacity. */
 struct PlanScratch {
   std::vector<BlockOut> blocks;
   std::vector<int> owner[3];
   std::vector<std::vector<int>> unit_deps;
   std::vector<int> dep_count, depth, sorted;
+  std::vector<int> chain_of, chain_tail, chain_len, height, crit, best;
+  std::vector<int> units_coding, ui_of, udepth, udeps;
   std::vector<uint8_t> is_b;
   std::vector<uint16_t> itx_key;
   std::vector<int> itx_hist;
-  std::vector<int2> itx_sorted;
-  std::vector<uint8_t> itx_scls;
+  std::vector<int2> itx_unsorted;  /* the blocks' transform jobs, before plan_itx sorts them */
 };
 
 /* Splits [0, n) into pieces of at least `min_piece` for the pool. */
@@ -797,6 +803,8 @@ inline size_t piece_begin(size_t n, int pieces, int i) { return n * i / pieces; 
 int plan_units(av1b_decoder* d, const PlanCtx& c, Plan* P) {
   const Layout& L = c.L;
   P->R->deps.clear();
+  P->n_chains = 0;
+  P->R->chains.clear();
   if (P->R->units.empty()) return AV1B_OK;
   PlanScratch& S = *c.scratch;
   int sh[3], cw[3], ch[3];
@@ -939,7 +947,7 @@ int plan_units(av1b_decoder* d, const PlanCtx& c, Plan* P) {
       /* prediction and residual fuse when the transforms cover disjoint parts
        * of the block (each sample then gets at most one residual) */
       b.fuse_res = 0;
-      if (b.kind == AV1B_U_INTRA && b.w * b.h <= 4096) {
+      if (b.kind == AV1B_U_INTRA && b.w * b.h <= AV1B_UNIT_SCRATCH) {
         bool ok = true, grid4 = true;
         for (int t = 0; t < b.tx_count && ok; ++t) {
           const TxRec& x = P->R->txs[b.tx_first + t];
@@ -1001,14 +1009,94 @@ int plan_units(av1b_decoder* d, const PlanCtx& c, Plan* P) {
     depth[P->R->units[ui]] = dd + 1;
     max_depth = std::max(max_depth, dd + 1);
   }
-  /* claim order: by depth, coding order within one */
+  /* chains: a warp claims a chain and runs its blocks in order, so a block
+   * whose deepest dependency is the block before it in its chain waits on
+   * its own warp's work instead of a flag published on another SM. Blocks
+   * are taken in order of depth (coding order within one depth). A block's
+   * candidate predecessor is its deepest dependency; of the blocks naming
+   * the same candidate, the one with the longest path still ahead of it
+   * (its height) gets it, so chains follow the critical path. It joins the
+   * candidate's chain when the candidate is that chain's last block and
+   * every other block it reads lies earlier in that chain or in an earlier
+   * chain; otherwise it starts a chain. Chains are claimed in the order they
+   * were started, so every wait across chains is on a chain claimed before:
+   * the warp holding the earliest unfinished chain always progresses. The
+   * work is on unit indices (coding order), in arrays of the units alone. */
+  std::vector<int>& U = S.units_coding;
+  U.assign(P->R->units.begin(), P->R->units.end());
+  std::vector<int>& ui_of = S.ui_of;
+  ui_of.resize(nb);
+  std::vector<int>& ud = S.udepth;
+  ud.resize(nu);
+  for (size_t ui = 0; ui < nu; ++ui) {
+    ui_of[U[ui]] = static_cast<int>(ui);
+    ud[ui] = depth[U[ui]];
+  }
   std::vector<int> count(max_depth + 2, 0);
-  for (size_t ui = 0; ui < nu; ++ui) ++count[depth[P->R->units[ui]] + 1];
+  for (size_t ui = 0; ui < nu; ++ui) ++count[ud[ui] + 1];
   for (int k = 0; k <= max_depth; ++k) count[k + 1] += count[k];
   std::vector<int>& sorted = S.sorted;
   sorted.resize(nu);
-  for (size_t ui = 0; ui < nu; ++ui) sorted[count[depth[P->R->units[ui]]]++] = P->R->units[ui];
-  std::copy(sorted.begin(), sorted.end(), P->R->units.begin());
+  for (size_t ui = 0; ui < nu; ++ui) sorted[count[ud[ui]]++] = static_cast<int>(ui);
+  std::vector<int>& chain_of = S.chain_of;
+  std::vector<int>& tail = S.chain_tail;
+  std::vector<int>& clen = S.chain_len;
+  std::vector<int>& height = S.height;
+  std::vector<int>& critv = S.crit;
+  std::vector<int>& best = S.best;
+  std::vector<int>& udeps = S.udeps;   /* the dependency lists as unit indices */
+  udeps.resize(first[nu]);
+  for (size_t k = 0; k < first[nu]; ++k) udeps[k] = ui_of[dl[k]];
+  height.assign(nu, 0);
+  critv.assign(nu, -1);
+  best.assign(nu, -1);
+  for (size_t k = nu; k-- > 0;) {
+    const int u = sorted[k];
+    int cr = -1;
+    for (size_t j = first[u]; j < first[u + 1]; ++j) {
+      const int o = udeps[j];
+      height[o] = std::max(height[o], height[u] + 1);
+      if (cr < 0 || ud[o] > ud[cr] || (ud[o] == ud[cr] && o > cr)) cr = o;
+    }
+    critv[u] = cr;
+  }
+  for (size_t k = 0; k < nu; ++k) {
+    const int u = sorted[k], cr = critv[u];
+    if (cr >= 0 && (best[cr] < 0 || height[u] > height[best[cr]])) best[cr] = u;
+  }
+  chain_of.assign(nu, -1);
+  tail.clear();
+  clen.clear();
+  for (size_t k = 0; k < nu; ++k) {
+    const int u = sorted[k], cr = critv[u];
+    int ch = -1;
+    if (cr >= 0 && best[cr] == u && tail[chain_of[cr]] == cr) {
+      ch = chain_of[cr];
+      for (size_t j = first[u]; j < first[u + 1]; ++j)
+        if (chain_of[udeps[j]] > ch) {
+          ch = -1;
+          break;
+        }
+    }
+    if (ch < 0) {
+      ch = static_cast<int>(tail.size());
+      tail.push_back(u);
+      clen.push_back(0);
+    }
+    chain_of[u] = ch;
+    tail[ch] = u;
+    ++clen[ch];
+  }
+  const size_t nch = tail.size();
+  sized(P->R->chains, nch + 1);
+  P->R->chains[0] = 0;
+  for (size_t k = 0; k < nch; ++k) P->R->chains[k + 1] = P->R->chains[k] + clen[k];
+  for (size_t k = 0; k < nch; ++k) clen[k] = P->R->chains[k];
+  for (size_t k = 0; k < nu; ++k) {
+    const int u = sorted[k];
+    P->R->units[clen[chain_of[u]]++] = U[u];
+  }
+  P->n_chains = nch;
   P->unit_depth = max_depth;
   P->units_inter = false;
   for (size_t ui = 0; ui < nu; ++ui)
@@ -1025,64 +1113,78 @@ int plan_units(av1b_decoder* d, const PlanCtx& c, Plan* P) {
  * into batches of 32 / class transforms (one for 64 and raw). */
 void plan_itx(const PlanCtx& c, Plan* P) {
   PlanLists& R = *P->R;
-  const size_t n = R.itx_jobs.size();
+  PlanScratch& S = *c.scratch;
+  const std::vector<int2>& jobs = S.itx_unsorted;
+  const size_t n = jobs.size();
   R.itx_batches.clear();
   for (int k = 0; k < 8; ++k) P->itx_class_first[k] = P->itx_class_count[k] = 0;
   if (n == 0) return;
-  PlanScratch& S = *c.scratch;
-  constexpr int kKeys = 8 * 7 * 7 * 16;
+  /* keys: the 25 shapes (log2 sides 2..6) ranked by class (the longer side),
+   * then width, then height; 16 types each; raw residual blocks last */
+  struct ShapeRank {
+    unsigned char rank[5][5], cls[25];
+    ShapeRank() {
+      int r = 0;
+      for (int cl = 2; cl <= 6; ++cl)
+        for (int lw = 2; lw <= 6; ++lw)
+          for (int lh = 2; lh <= 6; ++lh)
+            if (std::max(lw, lh) == cl) {
+              rank[lw - 2][lh - 2] = static_cast<unsigned char>(r);
+              cls[r++] = static_cast<unsigned char>(cl);
+            }
+    }
+  };
+  static const ShapeRank shapes;
+  constexpr int kRaw = 25 * 16, kKeys = kRaw + 1;
   std::vector<uint16_t>& key = S.itx_key;
   key.resize(n);
   /* a parallel counting sort: keys and per-piece histograms, offsets per
-   * (key, piece), then every piece scatters its own jobs */
+   * (key, piece), then every piece scatters its own jobs into the list that
+   * is uploaded */
   const int pieces = pieces_for(n, c, 4096);
   std::vector<int>& hist = S.itx_hist;
   hist.assign(static_cast<size_t>(kKeys) * pieces, 0);
   c.pool->run(pieces, [&](int pi) {
     int* h = hist.data() + static_cast<size_t>(pi) * kKeys;
     for (size_t i = piece_begin(n, pieces, pi); i < piece_begin(n, pieces, pi + 1); ++i) {
-      const int2 j = R.itx_jobs[i];
+      const int2 j = jobs[i];
       const TxRec& t = R.txs[j.y];
-      int k = 7 * 7 * 7 * 16;
-      if (!R.blocks[j.x].residual_provided)
-        k = ((std::max(t.log2w, t.log2h) * 7 + t.log2w) * 7 + t.log2h) * 16 + t.type;
+      int k = kRaw;
+      if (!R.blocks[j.x].residual_provided) k = shapes.rank[t.log2w - 2][t.log2h - 2] * 16 + t.type;
       key[i] = static_cast<uint16_t>(k);
       ++h[k];
     }
   });
+  /* offsets; and each class's range of the sorted list (its keys are
+   * contiguous: ranks ascend with the class) */
   int run = 0;
-  for (int k = 0; k < kKeys; ++k)
+  int cls_begin[8], cls_end[8];
+  for (int k = 0; k < 8; ++k) cls_begin[k] = cls_end[k] = -1;
+  for (int k = 0; k < kKeys; ++k) {
+    const int cl = k == kRaw ? 7 : shapes.cls[k >> 4];
+    if (cls_begin[cl] < 0) cls_begin[cl] = run;
     for (int pi = 0; pi < pieces; ++pi) {
       int& h = hist[static_cast<size_t>(pi) * kKeys + k];
       const int c0 = h;
       h = run;
       run += c0;
     }
-  std::vector<int2>& sorted = S.itx_sorted;
-  std::vector<uint8_t>& scls = S.itx_scls;
-  sorted.resize(n);
-  scls.resize(n);
+    cls_end[cl] = run;
+  }
   c.pool->run(pieces, [&](int pi) {
     int* h = hist.data() + static_cast<size_t>(pi) * kKeys;
-    for (size_t i = piece_begin(n, pieces, pi); i < piece_begin(n, pieces, pi + 1); ++i) {
-      const int o = h[key[i]]++;
-      sorted[o] = R.itx_jobs[i];
-      scls[o] = static_cast<uint8_t>(key[i] == 7 * 7 * 7 * 16 ? 7 : key[i] / (7 * 7 * 16));
-    }
+    for (size_t i = piece_begin(n, pieces, pi); i < piece_begin(n, pieces, pi + 1); ++i)
+      R.itx_jobs[h[key[i]]++] = jobs[i];
   });
-  std::copy(sorted.begin(), sorted.end(), R.itx_jobs.begin());
-  for (size_t i = 0; i < n;) {
-    const int cl = scls[i];
-    const size_t per = cl >= 6 ? 1 : static_cast<size_t>(32 >> cl);
-    size_t e = i + 1;
-    while (e < n && e - i < per && scls[e] == cl) ++e;
-    R.itx_batches.push_back(make_int4(static_cast<int>(i), static_cast<int>(e - i), cl, 0));
-    i = e;
-  }
-  /* the batches of each class, for one launch per class */
-  for (size_t bi = 0; bi < R.itx_batches.size(); ++bi) {
-    const int cl = R.itx_batches[bi].z;
-    if (P->itx_class_count[cl]++ == 0) P->itx_class_first[cl] = static_cast<int>(bi);
+  /* batches: runs of 32 / S jobs of one class (one job for the 64-point
+   * class and for raw residual blocks), one launch per class */
+  for (int cl = 2; cl < 8; ++cl) {
+    if (cls_begin[cl] < 0 || cls_end[cl] <= cls_begin[cl]) continue;
+    const int per = cl >= 6 ? 1 : 32 >> cl;
+    P->itx_class_first[cl] = static_cast<int>(R.itx_batches.size());
+    for (int i = cls_begin[cl]; i < cls_end[cl]; i += per)
+      R.itx_batches.push_back(make_int4(i, std::min(per, cls_end[cl] - i), cl, 0));
+    P->itx_class_count[cl] = static_cast<int>(R.itx_batches.size()) - P->itx_class_first[cl];
   }
 }
 
@@ -1223,6 +1325,7 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
     /* the lean kernel's tiles first, then the rest */
     sized(P->R->inter_tiles, o_tile[pieces] + o_tilef[pieces]);
     P->n_tiles_simple = o_tile[pieces];
+    c.scratch->itx_unsorted.resize(o_itx[pieces]);
     sized(P->R->itx_jobs, o_itx[pieces]);
     sized(P->R->dq, o_dq[pieces]);
     P->n_dq = o_dq[pieces];
@@ -1255,7 +1358,7 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
       for (size_t k = 0; k < O.itx_jobs.size(); ++k) {
         int2 j = O.itx_jobs[k];
         j.y += dtx;
-        P->R->itx_jobs[o_itx[i] + k] = j;
+        c.scratch->itx_unsorted[o_itx[i] + k] = j;
       }
       std::copy(O.dq.begin(), O.dq.end(), P->R->dq.begin() + o_dq[i]);
     });
@@ -1495,6 +1598,7 @@ struct av1b_plan {
   cudaEvent_t ready = nullptr, done = nullptr;
   bool in_flight = false;
   size_t o_blocks = 0, o_txs = 0, o_obmc = 0, o_warps = 0, o_pal = 0, o_units = 0, o_deps = 0;
+  size_t o_chains = 0;
   size_t o_tiles = 0, o_itx = 0, o_itxb = 0, o_dbv = 0, o_dbh = 0, o_cdef = 0, o_lr[3] = {0, 0, 0};
   size_t o_map = 0, o_cdef_search = 0, o_dq = 0, o_de_raw = 0, o_cb_raw = 0, o_prep = 0;
   int slots_read[kSlots + 1];     /* the reference slots the frame reads, -1 ended */
@@ -1689,6 +1793,7 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
   pl->o_warps = stage_put(&off, P.R->warps);
   pl->o_pal = stage_put(&off, P.R->palette_colors);
   pl->o_units = stage_put(&off, P.R->units);
+  pl->o_chains = stage_put(&off, P.R->chains);
   pl->o_deps = stage_put(&off, P.R->deps);
   pl->o_tiles = stage_put(&off, P.R->inter_tiles);
   pl->o_itx = stage_put(&off, P.R->itx_jobs);
@@ -1715,6 +1820,7 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
   CK(put(pl->o_warps, P.R->warps), "record upload");
   CK(put(pl->o_pal, P.R->palette_colors), "record upload");
   CK(put(pl->o_units, P.R->units), "record upload");
+  CK(put(pl->o_chains, P.R->chains), "record upload");
   CK(put(pl->o_deps, P.R->deps), "record upload");
   CK(put(pl->o_tiles, P.R->inter_tiles), "record upload");
   CK(put(pl->o_itx, P.R->itx_jobs), "record upload");
@@ -1886,9 +1992,19 @@ int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, cons
   a.epoch = d->epoch;
   a.units = reinterpret_cast<const int*>(ar + pl->o_units);
   a.n_units = static_cast<int>(P.n_units);
+  a.chains = reinterpret_cast<const int*>(ar + pl->o_chains);
+  a.n_chains = static_cast<int>(P.n_chains);
   a.deps = reinterpret_cast<const int*>(ar + pl->o_deps);
   a.units_inter = P.units_inter ? 1 : 0;
   a.queue = static_cast<unsigned*>(d->status_q.p);
+  a.trace = nullptr;
+  if (d->tracing) {
+    const size_t bytes = static_cast<size_t>(pl->n_blocks) * 4 * sizeof(unsigned long long) + 64;
+    if ((rc = dev_ensure(d, d->trace, bytes))) return rc;
+    CK(cudaMemsetAsync(d->trace.p, 0, bytes, st), "trace reset");
+    a.trace = static_cast<unsigned long long*>(d->trace.p);
+    d->trace_n = static_cast<size_t>(pl->n_blocks) * 4;
+  }
   a.status = reinterpret_cast<int*>(static_cast<uint8_t*>(d->status_q.p) + 64);
   a.inter_tiles = reinterpret_cast<const int2*>(ar + pl->o_tiles);
   a.n_inter_tiles = static_cast<int>(P.n_tiles);
@@ -2222,7 +2338,7 @@ int av1b_decoder_destroy(av1b_decoder* d) {
   DevBuf* bufs[] = {&d->cur, &d->snap, &d->lr_pre, &d->lr_pre_up, &d->lr_cdef, &d->disp,
                     &d->slot_ptr_dev, &d->arena, &d->coef, &d->residual, &d->done,
                     &d->status_q, &d->nv12, &d->rgb,
-                    &d->grain_state, &d->orbit, &d->pos, &d->cdef_search, &d->pre_res};
+                    &d->grain_state, &d->orbit, &d->pos, &d->cdef_search, &d->pre_res, &d->trace};
   for (DevBuf* b : bufs) dev_release(d, *b);
   for (int i = 0; i < kSlots; ++i) dev_release(d, d->slot_buf[i]);
   if (d->stream) cudaStreamDestroy(d->stream);
@@ -2565,6 +2681,26 @@ int av1b_selftest_wait(av1b_decoder* d, long long limit_ns, int* status, double*
   dev_release(d, mem);
   *status = st;
   if (elapsed_ms) *elapsed_ms = ms;
+  return AV1B_OK;
+}
+
+int av1b_set_unit_trace(av1b_decoder* d, int on) {
+  if (!d) return AV1B_ERR_ARG;
+  std::lock_guard<std::mutex> lk(d->mu);
+  d->tracing = on != 0;
+  d->trace_n = 0;
+  return AV1B_OK;
+}
+
+int av1b_unit_trace(av1b_decoder* d, uint64_t* out, size_t cap, size_t* n) {
+  if (!d || !n) return AV1B_ERR_ARG;
+  std::lock_guard<std::mutex> lk(d->mu);
+  cudaSetDevice(d->device);
+  *n = d->trace_n;
+  if (!out || d->trace_n == 0) return AV1B_OK;
+  if (cap < d->trace_n) return fail(d, AV1B_ERR_ARG, "trace buffer too small");
+  CK(cudaStreamSynchronize(d->stream), "trace sync");
+  CK(cudaMemcpy(out, d->trace.p, d->trace_n * sizeof(uint64_t), cudaMemcpyDeviceToHost), "trace read");
   return AV1B_OK;
 }
 

@@ -222,10 +222,21 @@ AV1B_DEV int dir_sample(const int* above, const int* left, int w, int h, int pan
  * plane, global memory). `plane` points at the plane origin (for CFL's luma,
  * `luma` at the luma plane origin). `scratch` is warp-private shared memory of
  * 3 * AV1B_EDGE_LEN ints. */
+/* Waits for the asynchronous copies this thread issued (cp.async), then
+ * for the warp: every lane's copies are in shared memory. */
+AV1B_DEV void async_copies_done() {
+  asm volatile("cp.async.wait_all;" ::: "memory");
+  __syncwarp();
+}
+
 AV1B_DEV void intra_predict(const IntraJob& j, px_t* dst, int stride, const px_t* luma,
                             int luma_stride, const uint8_t* palette_map,
                             const int* palette_colors, int* scratch, int lane,
-                            const int* res = nullptr, int* fi_pred = nullptr) {
+                            const int* res = nullptr, int* fi_pred = nullptr,
+                            bool res_in_flight = false) {
+  /* `res_in_flight`: the caller's residual image is still arriving by
+   * asynchronous copies; it is waited for after the edges are read (the two
+   * fetches overlap), before the first sample is written */
   const int w = j.w, h = j.h, n = w * h;
   const int lw = ilog2(w);
   /* the reconstructed sample: the prediction plus, when the caller fused the
@@ -236,6 +247,7 @@ AV1B_DEV void intra_predict(const IntraJob& j, px_t* dst, int stride, const px_t
     dst[i * stride + jj] = (px_t)v;
   };
   if (j.palette) {
+    if (res_in_flight) async_copies_done();
     const uint8_t* map = palette_map + j.palette_off;
     for (int k = lane; k < n; k += 32) {
       const int i = k >> lw, jj = k & (w - 1);
@@ -247,6 +259,7 @@ AV1B_DEV void intra_predict(const IntraJob& j, px_t* dst, int stride, const px_t
   int* left = scratch + AV1B_EDGE_LEN + AV1B_EDGE_OFF;
   int* tmp = scratch + 2 * AV1B_EDGE_LEN;
   intra_edges(j, dst, stride, above, left, lane);
+  if (res_in_flight) async_copies_done();
 
   if (j.mode == 13) { /* chroma from luma */
     const int dc = intra_dc(j, above, left, lane);

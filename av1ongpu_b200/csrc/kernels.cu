@@ -37,6 +37,11 @@ __device__ __forceinline__ unsigned ld_relaxed(const unsigned* p) {
   asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
 __device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 __device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
   asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
@@ -455,24 +460,39 @@ static cudaError_t launch_itx_class(const FrameArgs& a, cudaStream_t s) {
 
 /* ---- phase B -------------------------------------------------------------------------- */
 
+/* How a dependency wait polls: with AV1B_POLL_ACQUIRE every poll is an
+ * acquire load (the load that sees the flag orders what follows, no separate
+ * fence); without, relaxed polls and one acquire fence once the flag is seen.
+ * Between polls the warp sleeps, backing off to AV1B_POLL_PAUSE_MAX ns (0: no
+ * sleep). */
+#ifndef AV1B_POLL_ACQUIRE
+#define AV1B_POLL_ACQUIRE 0
+#endif
+#ifndef AV1B_POLL_PAUSE_MAX
+#define AV1B_POLL_PAUSE_MAX 256
+#endif
+
+__device__ __forceinline__ bool flag_seen(const unsigned* flag, unsigned want) {
+#if AV1B_POLL_ACQUIRE
+  return ld_acquire(flag) == want;
+#else
+  if (ld_relaxed(flag) != want) return false;
+  fence_acq_rel();
+  return true;
+#endif
+}
+
 /* Waits until *flag == want, for at most limit_ns of globaltimer. Once any
  * wait has given up (AV1B_STATUS_TIMEOUT in *status), nothing waits any more:
- * the frame has failed and the kernel only has to run to its end. */
+ * the frame has failed and the kernel only has to run to its end. The status
+ * word and the clock are read every 16th poll. */
 __device__ bool bounded_wait(const unsigned* flag, unsigned want, int* status,
                              unsigned long long limit_ns) {
-  /* relaxed polls and one acquire fence once the flag is seen (the acquire
-   * pattern); the status word and the clock are read every 16th poll, and the
-   * pause between polls backs off to 256 ns, so a thousand waiting warps load
-   * the memory system little while the warp whose flag was just set notices
-   * within a poll */
-  if (ld_relaxed(flag) == want) {
-    fence_acq_rel();
-    return true;
-  }
+  if (flag_seen(flag, want)) return true;
   const unsigned long long t0 = global_ns();
-  unsigned pause = 32;
+  unsigned pause = AV1B_POLL_PAUSE_MAX < 32 ? AV1B_POLL_PAUSE_MAX : 32;
   for (unsigned it = 1;; ++it) {
-    if (ld_relaxed(flag) == want) break;
+    if (flag_seen(flag, want)) return true;
     if ((it & 15) == 0) {
       if (ld_relaxed(reinterpret_cast<const unsigned*>(status)) & AV1B_STATUS_TIMEOUT) return false;
       if (global_ns() - t0 > limit_ns) {
@@ -480,11 +500,9 @@ __device__ bool bounded_wait(const unsigned* flag, unsigned want, int* status,
         return false;
       }
     }
-    __nanosleep(pause);
-    if (pause < 256) pause <<= 1;
+    if (AV1B_POLL_PAUSE_MAX > 0) __nanosleep(pause);
+    if (pause < AV1B_POLL_PAUSE_MAX) pause <<= 1;
   }
-  fence_acq_rel();
-  return true;
 }
 
 /* Waits until block `o` is reconstructed. Returns false on timeout. */
@@ -503,9 +521,11 @@ cudaError_t launch_selftest_wait(const unsigned* flag, int* status, unsigned lon
   return cudaGetLastError();
 }
 
-/* The persistent dependency-scheduled kernel: each warp claims blocks in the
- * planner's order (by dependency depth), waits for the blocks its list names
- * and reconstructs. Everything that does not depend on other blocks - the
+/* The persistent dependency-scheduled kernel: each warp claims chains of
+ * blocks in the planner's order (chains start in order of dependency depth)
+ * and runs a chain's blocks one after another: for each it waits for the
+ * blocks its list names - except the one before it in the chain, its own
+ * work - and reconstructs. Everything that does not depend on other blocks - the
  * block record, its dependency list, its residual - is loaded before the
  * wait. Shared memory per warp: three edge buffers and a 64x64 scratch (the
  * block's residual image, or the transform scratch). */
@@ -532,93 +552,135 @@ __global__ void __launch_bounds__(128) k_units(const __grid_constant__ FrameArgs
   extern __shared__ int smem[];
   const int wib = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
-  int* edges = smem + wib * (3 * AV1B_EDGE_LEN + 4096);
+  int* edges = smem + wib * (3 * AV1B_EDGE_LEN + AV1B_UNIT_SCRATCH);
   int* tmp = edges + 3 * AV1B_EDGE_LEN;
   for (;;) {
-    int u = 0;
-    if (lane == 0) u = atomicAdd(a.queue, 1);
-    u = __shfl_sync(0xffffffffu, u, 0);
-    if (u >= a.n_units) break;
-    const int bi = a.units[u];
-    const BlockRec b = a.blocks[bi];
-    const int p = b.plane;
-    const PlaneGeom& g = a.L.p[p];
-    const bool fused = b.kind == AV1B_U_INTRA && b.fuse_res;
+    int c = 0;
+    if (lane == 0) c = atomicAdd(a.queue, 1);
+    c = __shfl_sync(0xffffffffu, c, 0);
+    if (c >= a.n_chains) break;
+    const int u_end = a.chains[c + 1];
+    int prev = -1;
+    for (int u = a.chains[c]; u < u_end; ++u) {
+      const int bi = a.units[u];
+      const BlockRec b = a.blocks[bi];
+      const int p = b.plane;
+      const PlaneGeom& g = a.L.p[p];
+      const bool fused = b.kind == AV1B_U_INTRA && b.fuse_res;
 
-    /* the residual image, before the wait */
-    if (fused) {
-      const int n = b.w * b.h;
-      for (int k = lane; k < n; k += 32) tmp[k] = 0;
+      /* the residual image, copied asynchronously: it arrives while the
+       * block waits and reads its edges (intra_predict waits for it) */
+      if (fused) {
+        const int n = b.w * b.h;
+        for (int k = lane; k < n; k += 32) tmp[k] = 0;
+        __syncwarp();
+        for (int t = 0; t < b.tx_count; ++t) {
+          const TxRec tx = a.txs[b.tx_first + t];
+          const int* src = b.residual_provided ? a.residual + tx.coef_off : a.pre_res + tx.pre_off;
+          for (int k = lane; k < tx.w * tx.h; k += 32) {
+            const int yy = k / tx.w, xx = k - yy * tx.w;
+            const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(tmp + (tx.y + yy) * b.w + tx.x + xx));
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src + k) : "memory");
+          }
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+      }
+
+      /* the blocks this one reads from: each lane's acquire load of a done flag
+       * orders the samples that block published before that lane's later
+       * reads, and the warp barrier extends the order to every lane (all
+       * picture reads go through L2, never a stale L1 line) */
+      unsigned long long t_claim = 0;
+      if (a.trace) t_claim = global_ns();
+      /* the block before this one in the chain is this warp's own work, already
+       * ordered by the warp barrier that ended it */
+      for (int k = lane; k < b.dep_count; k += 32) {
+        const int o = a.deps[b.dep_first + k];
+        if (o != prev) wait_block(a, o);
+      }
       __syncwarp();
-      for (int t = 0; t < b.tx_count; ++t) {
-        const TxRec tx = a.txs[b.tx_first + t];
-        const int* src = b.residual_provided ? a.residual + tx.coef_off : a.pre_res + tx.pre_off;
-        for (int k = lane; k < tx.w * tx.h; k += 32) {
-          const int yy = k / tx.w, xx = k - yy * tx.w;
-          tmp[(tx.y + yy) * b.w + tx.x + xx] = src[k];
+      if (a.trace) {
+        /* the dependency published last (its record was written before its
+         * flag, so the acquire above made it visible) */
+        unsigned long long last = 0, who = ~0ull;
+        for (int k = lane; k < b.dep_count; k += 32) {
+          const int o = a.deps[b.dep_first + k];
+          const unsigned long long t = __ldcg(a.trace + 4 * (size_t)o + 2);
+          if (t >= last) {
+            last = t;
+            who = static_cast<unsigned long long>(o);
+          }
+        }
+        for (int s = 16; s > 0; s >>= 1) {
+          const unsigned long long lo = __shfl_down_sync(0xffffffffu, last, s);
+          const unsigned long long wo = __shfl_down_sync(0xffffffffu, who, s);
+          if (lo > last) {
+            last = lo;
+            who = wo;
+          }
+        }
+        if (lane == 0) {
+          a.trace[4 * (size_t)bi + 0] = t_claim;
+          a.trace[4 * (size_t)bi + 1] = global_ns();
+          a.trace[4 * (size_t)bi + 3] = who;
         }
       }
-    }
 
-    /* the blocks this one reads from: each lane's acquire load of a done flag
-     * orders the samples that block published before that lane's later
-     * reads, and the warp barrier extends the order to every lane (all
-     * picture reads go through L2, never a stale L1 line) */
-    for (int k = lane; k < b.dep_count; k += 32) wait_block(a, a.deps[b.dep_first + k]);
-    __syncwarp();
-
-    px_t* dst = a.cur + g.off + b.y * g.stride + b.x;
-    if (b.kind == AV1B_U_INTRA) {
-      IntraJob j;
-      j.x = b.x;
-      j.y = b.y;
-      j.w = b.w;
-      j.h = b.h;
-      j.mode = b.mode;
-      j.angle = b.angle_delta;
-      j.bitdepth = a.L.bit_depth;
-      j.maxv = a.maxv;
-      j.have_left = b.have_left;
-      j.have_above = b.have_above;
-      j.have_ar = b.have_ar;
-      j.have_bl = b.have_bl;
-      j.filter_type = b.filter_type;
-      j.filter_intra = b.fi_mode >= 0;
-      j.fi_mode = b.fi_mode >= 0 ? b.fi_mode : 0;
-      j.cfl_alpha = b.cfl_alpha;
-      j.max_x = g.grid_w - 1;
-      j.max_y = g.grid_h - 1;
-      j.ss_x = a.L.ss_x;
-      j.ss_y = a.L.ss_y;
-      j.palette = b.palette;
-      j.palette_off = b.palette_off;
-      j.palette_stride = b.palette_stride;
-      /* filter intra (at most 32x32) keeps its predictions after the
-       * residual image: tmp[1024 ..] */
-      intra_predict(j, dst, g.stride, a.cur + a.L.p[0].off, a.L.p[0].stride, a.palette_map,
-                    a.palette_colors + 8 * b.palette_color_idx, edges, lane,
-                    fused ? tmp : nullptr, tmp + 1024);
-    } else if constexpr (INTER) {
-      InterJob j;
-      make_inter_job(a, b, &j);
-      int dc = 0;
-      if (b.interintra && b.ii_mode == 0) dc = ii_dc(j);
-      for (int k = lane; k < b.w * b.h; k += 32) {
-        const int yy = k / b.w, xx = k - yy * b.w;
-        int v = b.kind == AV1B_U_INTRABC ? inter_core<true>(j, xx, yy) : inter_core(j, xx, yy);
-        v = inter_finish(j, xx, yy, v, dc);
-        dst[yy * g.stride + xx] = (px_t)v;
+      px_t* dst = a.cur + g.off + b.y * g.stride + b.x;
+      if (b.kind == AV1B_U_INTRA) {
+        IntraJob j;
+        j.x = b.x;
+        j.y = b.y;
+        j.w = b.w;
+        j.h = b.h;
+        j.mode = b.mode;
+        j.angle = b.angle_delta;
+        j.bitdepth = a.L.bit_depth;
+        j.maxv = a.maxv;
+        j.have_left = b.have_left;
+        j.have_above = b.have_above;
+        j.have_ar = b.have_ar;
+        j.have_bl = b.have_bl;
+        j.filter_type = b.filter_type;
+        j.filter_intra = b.fi_mode >= 0;
+        j.fi_mode = b.fi_mode >= 0 ? b.fi_mode : 0;
+        j.cfl_alpha = b.cfl_alpha;
+        j.max_x = g.grid_w - 1;
+        j.max_y = g.grid_h - 1;
+        j.ss_x = a.L.ss_x;
+        j.ss_y = a.L.ss_y;
+        j.palette = b.palette;
+        j.palette_off = b.palette_off;
+        j.palette_stride = b.palette_stride;
+        /* filter intra (at most 32x32) keeps its predictions after the
+         * residual image: tmp[1024 ..] */
+        intra_predict(j, dst, g.stride, a.cur + a.L.p[0].off, a.L.p[0].stride, a.palette_map,
+                      a.palette_colors + 8 * b.palette_color_idx, edges, lane,
+                      fused ? tmp : nullptr, tmp + 1024, fused);
+      } else if constexpr (INTER) {
+        InterJob j;
+        make_inter_job(a, b, &j);
+        int dc = 0;
+        if (b.interintra && b.ii_mode == 0) dc = ii_dc(j);
+        for (int k = lane; k < b.w * b.h; k += 32) {
+          const int yy = k / b.w, xx = k - yy * b.w;
+          int v = b.kind == AV1B_U_INTRABC ? inter_core<true>(j, xx, yy) : inter_core(j, xx, yy);
+          v = inter_finish(j, xx, yy, v, dc);
+          dst[yy * g.stride + xx] = (px_t)v;
+        }
       }
-    }
-    __syncwarp();
-    if (!fused)
-      for (int t = 0; t < b.tx_count; ++t) add_residual_cg(a, b, a.txs[b.tx_first + t], lane);
+      __syncwarp();
+      if (!fused)
+        for (int t = 0; t < b.tx_count; ++t) add_residual_cg(a, b, a.txs[b.tx_first + t], lane);
 
-    /* publish: the barrier orders every lane's stores before lane 0's
-     * release, whose fence (cumulative) makes them visible at GPU scope to
-     * any warp that acquires the flag */
-    __syncwarp();
-    if (lane == 0) st_release(a.done + (size_t)bi * AV1B_FLAG_STRIDE, a.epoch);
+      /* publish: the barrier orders every lane's stores before lane 0's
+       * release, whose fence (cumulative) makes them visible at GPU scope to
+       * any warp that acquires the flag */
+      __syncwarp();
+      if (a.trace && lane == 0) a.trace[4 * (size_t)bi + 2] = global_ns();
+      if (lane == 0) st_release(a.done + (size_t)bi * AV1B_FLAG_STRIDE, a.epoch);
+      prev = bi;
+    }
   }
 }
 
@@ -1348,9 +1410,10 @@ cudaError_t launch_recon_stage(int stage, const FrameArgs& a, int n_sm, cudaStre
       break;
     default:
       if (a.n_units > 0) {
-        const size_t smem = 4 * (3 * AV1B_EDGE_LEN + 4096) * sizeof(int);
-        if (a.units_inter) k_units<true><<<2 * n_sm, 128, smem, s>>>(a);
-        else k_units<false><<<2 * n_sm, 128, smem, s>>>(a);
+        const size_t smem = 4 * (3 * AV1B_EDGE_LEN + AV1B_UNIT_SCRATCH) * sizeof(int);
+        const int grid = AV1B_UNIT_CTAS_PER_SM * n_sm;
+        if (a.units_inter) k_units<true><<<grid, 128, smem, s>>>(a);
+        else k_units<false><<<grid, 128, smem, s>>>(a);
       }
       break;
   }
@@ -1525,10 +1588,17 @@ cudaError_t set_kernel_attributes() {
     if (e != cudaSuccess) return e;
   }
   cudaError_t e = cudaFuncSetAttribute(k_units<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       4 * (3 * AV1B_EDGE_LEN + 4096) * (int)sizeof(int));
+                                       4 * (3 * AV1B_EDGE_LEN + AV1B_UNIT_SCRATCH) * (int)sizeof(int));
   if (e != cudaSuccess) return e;
   if ((e = cudaFuncSetAttribute(k_units<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                4 * (3 * AV1B_EDGE_LEN + 4096) * (int)sizeof(int))) != cudaSuccess)
+                                4 * (3 * AV1B_EDGE_LEN + AV1B_UNIT_SCRATCH) * (int)sizeof(int))) != cudaSuccess)
+    return e;
+  /* phase B's picture reads bypass L1: the SM's memory goes to shared memory,
+   * so AV1B_UNIT_CTAS_PER_SM CTAs fit */
+  if ((e = cudaFuncSetAttribute(k_units<true>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                cudaSharedmemCarveoutMaxShared)) != cudaSuccess ||
+      (e = cudaFuncSetAttribute(k_units<false>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                cudaSharedmemCarveoutMaxShared)) != cudaSuccess)
     return e;
   /* the two classes whose scratch passes the 48 KB default */
   if ((e = cudaFuncSetAttribute(k_itx<6>, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -21,6 +21,13 @@ namespace av1b {
  * onto a few L2 slices, slowing every other access there. */
 #define AV1B_FLAG_STRIDE 32
 
+/* Phase B: shared-memory scratch per warp (ints) - the residual image of a
+ * block whose prediction and residual fuse (so blocks of up to this many
+ * samples fuse) and, for filter intra (at most 32x32), its predictions at
+ * offset 1024 - and the CTAs of four warps resident per SM. */
+#define AV1B_UNIT_SCRATCH 2048
+#define AV1B_UNIT_CTAS_PER_SM 4
+
 struct FrameArgs {
   Layout L;
   px_t* cur;                    /* the picture being reconstructed */
@@ -37,7 +44,9 @@ struct FrameArgs {
   unsigned* done;               /* per block, AV1B_FLAG_STRIDE apart: == epoch once
                                    reconstructed (phase B) */
   unsigned epoch;
-  const int* units;             /* phase B block indices, claim order */
+  const int* units;             /* phase B block indices, chain after chain */
+  const int* chains;            /* chain c is units[chains[c] .. chains[c + 1]) */
+  int n_chains;
   const int* deps;              /* the phase B blocks each phase B block waits for */
   int units_inter;              /* some phase B block is an inter kind */
   int n_units;
@@ -56,6 +65,8 @@ struct FrameArgs {
   int maxv;
   int scale_x, scale_y;
   unsigned long long wait_ns;   /* limit of one dependency wait */
+  unsigned long long* trace;    /* null, or 4 per block: claimed, ready, published
+                                   (globaltimer ns), last dependency */
 };
 
 struct LrArgs {

@@ -292,6 +292,16 @@ AV1B_API int av1b_set_profiling(av1b_decoder* dec, int on);
 AV1B_API int av1b_profile(av1b_decoder* dec, int stage, const char** name, double* total_ms,
                           long long* count);
 
+/* Trace of the dependency-scheduled phase: with tracing on, each frame
+ * records, per phase B block, the device time (globaltimer ns) it was
+ * claimed, the time its dependencies were all met, the time it was
+ * published, and which dependency was published last (-1: none). After a
+ * decode, av1b_unit_trace copies the last frame's records - four uint64 per
+ * block of the frame, indexed by block, zero for blocks outside phase B -
+ * into `out` (room for `cap` uint64) and sets *n to the count. */
+AV1B_API int av1b_set_unit_trace(av1b_decoder* dec, int on);
+AV1B_API int av1b_unit_trace(av1b_decoder* dec, uint64_t* out, size_t cap, size_t* n);
+
 /* CUDA stream the decoder runs on (a cudaStream_t), so a caller can order its
  * own work after a decode without a host synchronisation. */
 AV1B_API void* av1b_decoder_stream(av1b_decoder* dec);
