@@ -455,6 +455,12 @@ AV1B_DEV int ii_mask(const InterJob& b, int x, int y) {
 
 /* The composition of the block's two predictions `v0`, `v1` (or one) at
  * (x, y): average, distance weights or a mask, then the clip. */
+/* The compound blend of two predictions with mask value m (0..64), clipped. */
+AV1B_DEV int blend_mask(const InterJob& b, int v0, int v1, int m) {
+  const int post = 7 - (b.ctx.bitdepth >= 12 ? 5 : 3);
+  return clampi((m * v0 + (64 - m) * v1 + (1 << (5 + post))) >> (6 + post), 0, b.maxv);
+}
+
 template <bool CG = false>
 AV1B_DEV int inter_compose(const InterJob& b, int x, int y, int v0, int v1) {
   int out = v0;

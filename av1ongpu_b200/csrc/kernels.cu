@@ -232,11 +232,15 @@ __global__ void __launch_bounds__(128) k_inter_simple(const __grid_constant__ Fr
 }
 
 /* Inter prediction of phase A blocks: one warp per 16x8 tile. Translation
- * predictions (and OBMC strips) go through mc_rect, warped ones per sample;
- * the composition and the OBMC blends run per sample on registers. */
+ * predictions (and OBMC strips) go through mc_rect, warped ones through
+ * warp_block8; the composition and the OBMC blends run per sample on
+ * registers. A chroma tile whose compound mask is difference-weighted takes
+ * its mask from the luma predictions of the area it covers (up to 32x16
+ * luma samples), computed the same separable way into shared memory. */
 __global__ void __launch_bounds__(128, 4) k_inter(const __grid_constant__ FrameArgs a) {
   __shared__ McScratch scr[4];
   __shared__ int pred[4][2][8 * 16];
+  __shared__ int lpred[4][2][4 * 8 * 16];   /* luma predictions, four 16x8 quarters */
   const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int warp = a.n_inter_simple + blockIdx.x * 4 + wib;
   if (warp >= a.n_inter_tiles) return;
@@ -281,14 +285,65 @@ __global__ void __launch_bounds__(128, 4) k_inter(const __grid_constant__ FrameA
       __syncwarp();
     }
   }
+  const bool luma_mask = j.compound && j.mask_kind == 2 && b.plane > 0;
+  if (luma_mask) {
+    InterCtx l;
+    l.sub_x = l.sub_y = 0;
+    l.ref_w = j.luma_ref_w;
+    l.ref_h = j.luma_ref_h;
+    l.bitdepth = j.ctx.bitdepth;
+    l.scale_x = j.ctx.scale_x;
+    l.scale_y = j.ctx.scale_y;
+    const int lx0 = x0 << j.ctx.sub_x, ly0 = y0 << j.ctx.sub_y;
+    const int lw = tw << j.ctx.sub_x, lh = th << j.ctx.sub_y;
+    const int ew = j.w << j.ctx.sub_x, eh = j.h << j.ctx.sub_y;
+    for (int r = 0; r < 2; ++r)
+      for (int qy = 0; qy < lh; qy += 8)
+        for (int qx = 0; qx < lw; qx += 16) {
+          int* out = lpred[wib][r] + ((qy >> 3) * 2 + (qx >> 4)) * 128;
+          const int rw = mini(16, lw - qx), rh = mini(8, lh - qy);
+          if (j.mask_warp[r]) {
+            for (int bx = 0; bx < rw; bx += 8)
+              warp_block8(0, 0, j.luma_ref_w, j.luma_ref_h, *j.model[r], j.luma_ref[r],
+                          j.luma_stride, j.luma_x, j.luma_y, lx0 + qx + bx, ly0 + qy,
+                          j.ctx.bitdepth, 1, scr[wib], out + bx, 16, mini(8, rw - bx), rh, lane);
+          } else if (!mc_rect(l, j.luma_ref[r], j.luma_stride, j.luma_x, j.luma_y, ew, eh,
+                              j.mv[r][0], j.mv[r][1], j.filt, j.filt_v, 1, lx0 + qx, ly0 + qy, rw,
+                              rh, scr[wib], out, lane)) {
+            for (int k = lane; k < rw * rh; k += 32) {
+              const int yy = k / rw, xx = k - yy * rw;
+              out[yy * 16 + xx] = mc_tap(l, j.luma_ref[r], j.luma_stride, j.luma_x, j.luma_y, ew,
+                                         eh, j.mv[r][0], j.mv[r][1], j.filt, j.filt_v,
+                                         lx0 + qx + xx, ly0 + qy + yy, 1);
+            }
+            __syncwarp();
+          }
+        }
+  }
   int acc[4];
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
     const int k = lane + 32 * q;
     if (k < tw * th) {
       const int yy = k / tw, xx = k - yy * tw;
-      acc[q] = inter_compose(j, x0 + xx, y0 + yy, pred[wib][0][yy * 16 + xx],
-                             nref > 1 ? pred[wib][1][yy * 16 + xx] : 0);
+      const int v0 = pred[wib][0][yy * 16 + xx], v1 = nref > 1 ? pred[wib][1][yy * 16 + xx] : 0;
+      if (luma_mask) {
+        /* the chroma sample's mask: the mean over the luma samples it covers */
+        const int sh = 7 - (j.ctx.bitdepth >= 12 ? 5 : 3) + (j.ctx.bitdepth - 8);
+        const int nx = j.ctx.sub_x + 1, ny = j.ctx.sub_y + 1;
+        int sum = 0;
+        for (int jj = 0; jj < ny; ++jj)
+          for (int ii = 0; ii < nx; ++ii) {
+            const int lx = (xx << j.ctx.sub_x) + ii, ly = (yy << j.ctx.sub_y) + jj;
+            const int idx = ((ly >> 3) * 2 + (lx >> 4)) * 128 + (ly & 7) * 16 + (lx & 15);
+            sum += diffwtd_m(absi(lpred[wib][0][idx] - lpred[wib][1][idx]), sh, j.mask_sign);
+          }
+        const int n = nx * ny;
+        const int m = n == 1 ? sum : (n == 2 ? (sum + 1) >> 1 : (sum + 2) >> 2);
+        acc[q] = blend_mask(j, v0, v1, m);
+      } else {
+        acc[q] = inter_compose(j, x0 + xx, y0 + yy, v0, v1);
+      }
     }
   }
   __syncwarp();
