@@ -2281,7 +2281,12 @@ int av1b_decoder_create(int device, size_t hbm_budget_bytes, av1b_decoder** out)
     /* two planners: one plan at a time uses all cores but the one left to
      * the thread that drives the device; two plans at once share them */
     const unsigned hc = std::thread::hardware_concurrency();
+#ifdef AV1B_PLANNER_THREADS
+    const int threads = AV1B_PLANNER_THREADS;
+    (void)hc;
+#else
     const int threads = static_cast<int>(std::min(16u, std::max(2u, hc) - 1));
+#endif
     d->planners.resize(2);
     for (auto& q : d->planners) {
       q.pool = new WorkPool(threads);

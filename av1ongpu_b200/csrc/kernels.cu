@@ -1035,6 +1035,7 @@ __global__ void __launch_bounds__(256) k_lr_tile(const px_t* __restrict__ cdef,
                                                  const __grid_constant__ LrArgs r, int maxv) {
   __shared__ int win[AV1B_LR_WR * AV1B_LR_WC];
   __shared__ int aux[2][2][AV1B_LR_AR * AV1B_LR_AC];  /* Wiener: aux[0][0] = intermediate */
+  __shared__ short xbyx1[256];   /* a2 = ((z << 8) + z / 2) / (z + 1), by z */
   const int p = blockIdx.z;
   if (!r.type[p]) return;
   const PlaneGeom& g = L.p[p];
@@ -1105,6 +1106,9 @@ __global__ void __launch_bounds__(256) k_lr_tile(const px_t* __restrict__ cdef,
     return;
   }
   /* self-guided: A and B of both passes on rows y0-1 .. y1, columns x0-1 .. */
+  for (int z = threadIdx.x; z < 256; z += blockDim.x)
+    xbyx1[z] = static_cast<short>(z >= 255 ? 256 : (z == 0 ? 1 : ((z << 8) + (z / 2)) / (z + 1)));
+  __syncthreads();
   const int ar = th + 2, ac = tw + 2;
   for (int pass = 0; pass < 2; ++pass) {
     const int rad = u.r[pass];
@@ -1117,26 +1121,23 @@ __global__ void __launch_bounds__(256) k_lr_tile(const px_t* __restrict__ cdef,
       const int i = k / ac, j = k - i * ac;
       /* the first pass reads odd rows only */
       if (pass == 0 && !((y0 - 1 + i) & 1)) continue;
-      long long sa = 0;
+      unsigned sq = 0;   /* at most 25 * 4095^2 */
       int sb = 0;
       for (int dy = -rad; dy <= rad; ++dy) {
         const int* w = win + (i + 2 + dy) * AV1B_LR_WC + j + 2;
         for (int dx = -rad; dx <= rad; ++dx) {
           const int c = w[dx];
-          sa += c * c;
+          sq += static_cast<unsigned>(c * c);
           sb += c;
         }
       }
       const int b_sum = sb;
-      sa = rnd2llz(sa, 2 * (bd - 8));
+      const long long sa = rnd2llz(static_cast<long long>(sq), 2 * (bd - 8));
       const long long sbs = rnd2z(sb, bd - 8);
       long long pv = sa * n - sbs * sbs;
       if (pv < 0) pv = 0;
       const int z = rnd2ll(pv * mtable, 20);
-      int a2;
-      if (z >= 255) a2 = 256;
-      else if (z == 0) a2 = 1;
-      else a2 = ((z << 8) + (z / 2)) / (z + 1);
+      const int a2 = xbyx1[mini(z, 255)];
       const long long b2 = (long long)(256 - a2) * b_sum * one_over_n;
       aux[pass][0][i * AV1B_LR_AC + j] = a2;
       aux[pass][1][i * AV1B_LR_AC + j] = rnd2ll(b2, 12);

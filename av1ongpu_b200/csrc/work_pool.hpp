@@ -32,6 +32,11 @@
 #define AV1B_CPU_RELAX() std::this_thread::yield()
 #endif
 
+/* How long an idle worker spins before it sleeps, in microseconds. */
+#ifndef AV1B_POOL_SPIN_US
+#define AV1B_POOL_SPIN_US 40
+#endif
+
 namespace av1b {
 
 class WorkPool {
@@ -96,7 +101,7 @@ class WorkPool {
     unsigned long long seen = 0;
     for (;;) {
       if (gen_.load(std::memory_order_acquire) == seen) {
-        const auto until = std::chrono::steady_clock::now() + std::chrono::microseconds(40);
+        const auto until = std::chrono::steady_clock::now() + std::chrono::microseconds(AV1B_POOL_SPIN_US);
         for (int k = 1; gen_.load(std::memory_order_acquire) == seen; ++k) {
           AV1B_CPU_RELAX();
           if ((k & 63) == 0 && std::chrono::steady_clock::now() > until) break;
