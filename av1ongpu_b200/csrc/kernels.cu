@@ -616,9 +616,18 @@ __global__ void __launch_bounds__(128) k_units(const __grid_constant__ FrameArgs
     if (c >= a.n_chains) break;
     const int u_end = a.chains[c + 1];
     int prev = -1;
+    /* the next block's record is loaded while this one runs: in a chain the
+     * next block usually starts as soon as this one is published (not in
+     * the kernel with inter prediction, whose registers it would spill) */
+    int bi_next = a.units[a.chains[c]];
+    BlockRec b_next = a.blocks[bi_next];
     for (int u = a.chains[c]; u < u_end; ++u) {
-      const int bi = a.units[u];
-      const BlockRec b = a.blocks[bi];
+      const int bi = bi_next;
+      const BlockRec b = INTER ? a.blocks[bi] : b_next;
+      if (u + 1 < u_end) {
+        bi_next = a.units[u + 1];
+        if (!INTER) b_next = a.blocks[bi_next];
+      }
       const int p = b.plane;
       const PlaneGeom& g = a.L.p[p];
       const bool fused = b.kind == AV1B_U_INTRA && b.fuse_res;
