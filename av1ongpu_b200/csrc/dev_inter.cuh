@@ -147,7 +147,28 @@ AV1B_DEV int mc_tap(const InterCtx& c, const px_t* ref, int stride, int base_x, 
 struct McScratch {
   int win[AV1B_MC_WR * AV1B_MC_WC];
   int mid[AV1B_MC_WR * 16];
+  int4 ht[16][2], vt[8][2];   /* the taps of each output column, of each output row */
   int cx[16], xf[16], cy[8], yf[8];
+};
+
+/* Index (r, q) of element k = r * n + q of a row-major walk in steps of 32,
+ * advanced without a division per step. */
+struct Walk32 {
+  int r, q, dr, dq, n;
+  AV1B_DEV Walk32(int lane, int n_) : n(n_) {
+    r = lane / n;
+    q = lane - r * n;
+    dr = 32 / n;
+    dq = 32 - dr * n;
+  }
+  AV1B_DEV void next() {
+    r += dr;
+    q += dq;
+    if (q >= n) {
+      q -= n;
+      ++r;
+    }
+  }
 };
 
 template <bool CG = false>
@@ -182,32 +203,46 @@ AV1B_DEV bool mc_rect(const InterCtx& c, const px_t* ref, int stride, int base_x
     __syncwarp();
     return false;
   }
-  for (int k = lane; k < nrows * ncols; k += 32) {
-    const int r = k / ncols, q = k - r * ncols;
-    s.win[r * AV1B_MC_WC + q] = fetch<CG>(ref, stride, cbase + q, rbase + r, c.ref_w - 1, c.ref_h - 1);
+  {
+    Walk32 wk(lane, ncols);
+    for (int k = lane; k < nrows * ncols; k += 32, wk.next())
+      s.win[wk.r * AV1B_MC_WC + wk.q] =
+          fetch<CG>(ref, stride, cbase + wk.q, rbase + wk.r, c.ref_w - 1, c.ref_h - 1);
+  }
+  const int fh = filt_row(filt, ew), fv = filt_row(filt_v, eh);
+  /* each column's and each row's taps, once */
+  if (lane < rw) {
+    const short* f = kSubpelFilters + (fh * 16 + s.xf[lane]) * 8;
+    s.ht[lane][0] = make_int4(f[0], f[1], f[2], f[3]);
+    s.ht[lane][1] = make_int4(f[4], f[5], f[6], f[7]);
+  } else if (lane >= 16 && lane - 16 < rh) {
+    const short* f = kSubpelFilters + (fv * 16 + s.yf[lane - 16]) * 8;
+    s.vt[lane - 16][0] = make_int4(f[0], f[1], f[2], f[3]);
+    s.vt[lane - 16][1] = make_int4(f[4], f[5], f[6], f[7]);
   }
   __syncwarp();
-  const int fh = filt_row(filt, ew), fv = filt_row(filt_v, eh);
   int r0, r1;
   rounds(c.bitdepth, compound, &r0, &r1);
-  for (int k = lane; k < nrows * rw; k += 32) {
-    const int r = k / rw, x = k - r * rw;
-    const int* w = s.win + r * AV1B_MC_WC + s.cx[x] - 3 - cbase;
-    const short* f = kSubpelFilters + (fh * 16 + s.xf[x]) * 8;
-    int sum = 0;
-#pragma unroll
-    for (int i = 0; i < 8; ++i) sum += w[i] * f[i];
-    s.mid[r * 16 + x] = (sum + (1 << (r0 - 1))) >> r0;
+  {
+    Walk32 wk(lane, rw);
+    for (int k = lane; k < nrows * rw; k += 32, wk.next()) {
+      const int* w = s.win + wk.r * AV1B_MC_WC + s.cx[wk.q] - 3 - cbase;
+      const int4 ta = s.ht[wk.q][0], tb = s.ht[wk.q][1];
+      const int sum = w[0] * ta.x + w[1] * ta.y + w[2] * ta.z + w[3] * ta.w + w[4] * tb.x +
+                      w[5] * tb.y + w[6] * tb.z + w[7] * tb.w;
+      s.mid[wk.r * 16 + wk.q] = (sum + (1 << (r0 - 1))) >> r0;
+    }
   }
   __syncwarp();
-  for (int k = lane; k < rh * rw; k += 32) {
-    const int y = k / rw, x = k - y * rw;
-    const int* m = s.mid + (s.cy[y] - 3 - rbase) * 16 + x;
-    const short* f = kSubpelFilters + (fv * 16 + s.yf[y]) * 8;
-    int acc = 0;
-#pragma unroll
-    for (int j = 0; j < 8; ++j) acc += m[j * 16] * f[j];
-    out[y * 16 + x] = (acc + (1 << (r1 - 1))) >> r1;
+  {
+    Walk32 wk(lane, rw);
+    for (int k = lane; k < rh * rw; k += 32, wk.next()) {
+      const int* m = s.mid + (s.cy[wk.r] - 3 - rbase) * 16 + wk.q;
+      const int4 ta = s.vt[wk.r][0], tb = s.vt[wk.r][1];
+      const int acc = m[0] * ta.x + m[16] * ta.y + m[32] * ta.z + m[48] * ta.w + m[64] * tb.x +
+                      m[80] * tb.y + m[96] * tb.z + m[112] * tb.w;
+      out[wk.r * 16 + wk.q] = (acc + (1 << (r1 - 1))) >> r1;
+    }
   }
   __syncwarp();
   return true;
