@@ -23,6 +23,30 @@ typedef uint16_t px_t; /* one sample, 16 bits at every bit depth */
 
 /* ---- scalar helpers --------------------------------------------------------- */
 AV1B_HD int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+/* A strided walk over a row-major n-wide rectangle: element k = r * n + q,
+ * from `start` in steps of `step`, with (r, q) advanced without a division
+ * per step (step % n < n, so one carry suffices). */
+struct StepWalk {
+  int k, r, q, dr, dq, n;
+  __device__ __forceinline__ StepWalk(int start, int step, int n_) : k(start), n(n_) {
+    r = start / n;
+    q = start - r * n;
+    dr = step / n;
+    dq = step - dr * n;
+    dk = step;
+  }
+  __device__ __forceinline__ void next() {
+    k += dk;
+    r += dr;
+    q += dq;
+    if (q >= n) {
+      q -= n;
+      ++r;
+    }
+  }
+  int dk;
+};
 AV1B_HD int mini(int a, int b) { return a < b ? a : b; }
 AV1B_HD int maxi(int a, int b) { return a > b ? a : b; }
 AV1B_HD int absi(int v) { return v < 0 ? -v : v; }

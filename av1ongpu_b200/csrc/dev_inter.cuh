@@ -151,26 +151,6 @@ struct McScratch {
   int cx[16], xf[16], cy[8], yf[8];
 };
 
-/* Index (r, q) of element k = r * n + q of a row-major walk in steps of 32,
- * advanced without a division per step. */
-struct Walk32 {
-  int r, q, dr, dq, n;
-  AV1B_DEV Walk32(int lane, int n_) : n(n_) {
-    r = lane / n;
-    q = lane - r * n;
-    dr = 32 / n;
-    dq = 32 - dr * n;
-  }
-  AV1B_DEV void next() {
-    r += dr;
-    q += dq;
-    if (q >= n) {
-      q -= n;
-      ++r;
-    }
-  }
-};
-
 template <bool CG = false>
 AV1B_DEV bool mc_rect(const InterCtx& c, const px_t* ref, int stride, int base_x, int base_y,
                       int ew, int eh, int mvx, int mvy, int filt, int filt_v, int compound, int rx,
@@ -204,7 +184,7 @@ AV1B_DEV bool mc_rect(const InterCtx& c, const px_t* ref, int stride, int base_x
     return false;
   }
   {
-    Walk32 wk(lane, ncols);
+    StepWalk wk(lane, 32, ncols);
     for (int k = lane; k < nrows * ncols; k += 32, wk.next())
       s.win[wk.r * AV1B_MC_WC + wk.q] =
           fetch<CG>(ref, stride, cbase + wk.q, rbase + wk.r, c.ref_w - 1, c.ref_h - 1);
@@ -224,7 +204,7 @@ AV1B_DEV bool mc_rect(const InterCtx& c, const px_t* ref, int stride, int base_x
   int r0, r1;
   rounds(c.bitdepth, compound, &r0, &r1);
   {
-    Walk32 wk(lane, rw);
+    StepWalk wk(lane, 32, rw);
     for (int k = lane; k < nrows * rw; k += 32, wk.next()) {
       const int* w = s.win + wk.r * AV1B_MC_WC + s.cx[wk.q] - 3 - cbase;
       const int4 ta = s.ht[wk.q][0], tb = s.ht[wk.q][1];
@@ -235,7 +215,7 @@ AV1B_DEV bool mc_rect(const InterCtx& c, const px_t* ref, int stride, int base_x
   }
   __syncwarp();
   {
-    Walk32 wk(lane, rw);
+    StepWalk wk(lane, 32, rw);
     for (int k = lane; k < rh * rw; k += 32, wk.next()) {
       const int* m = s.mid + (s.cy[wk.r] - 3 - rbase) * 16 + wk.q;
       const int4 ta = s.vt[wk.r][0], tb = s.vt[wk.r][1];

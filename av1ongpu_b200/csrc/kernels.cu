@@ -932,8 +932,8 @@ __global__ void __launch_bounds__(128) k_cdef(const px_t* __restrict__ src, px_t
   int* win = sw[hw];
   /* the block and its halo; rows and columns above or left of the buffer
    * clamp into it (taps outside the plane are never used) */
-  for (int k = hl; k < (h + 4) * (w + 4); k += 16) {
-    const int i = k / (w + 4), j = k - i * (w + 4);
+  for (StepWalk wk(hl, 16, w + 4); wk.k < (h + 4) * (w + 4); wk.next()) {
+    const int i = wk.r, j = wk.q;
     const int y = maxi(r.y - 2 + i, 0), x = maxi(r.x - 2 + j, 0);
     win[i * 12 + j] = src[g.off + y * g.stride + x];
   }
@@ -1069,8 +1069,8 @@ __global__ void __launch_bounds__(256) k_lr_tile(const px_t* __restrict__ cdef,
   const px_t* pc = cdef + g.off;
   const px_t* pp = curr + g.off;
   /* source window: rows y0-3 .., columns x0-3 .. */
-  for (int k = threadIdx.x; k < wr * wc; k += blockDim.x) {
-    const int i = k / wc, j = k - i * wc;
+  for (StepWalk wk(threadIdx.x, blockDim.x, wc); wk.k < wr * wc; wk.next()) {
+    const int i = wk.r, j = wk.q;
     const int x = clampi(x0 - 3 + j, 0, g.out_w - 1);
     const int y = clampi(y0 - 3 + i, 0, g.out_h - 1);
     int v;
@@ -1096,8 +1096,8 @@ __global__ void __launch_bounds__(256) k_lr_tile(const px_t* __restrict__ cdef,
     /* the intermediate has up to 70 rows: it spans aux[0][0] and aux[0][1] */
     static_assert(AV1B_LR_WR * AV1B_LR_AC <= 2 * AV1B_LR_AR * AV1B_LR_AC, "Wiener intermediate");
     int* mid = &aux[0][0][0];
-    for (int k = threadIdx.x; k < wr * tw; k += blockDim.x) {
-      const int i = k / tw, j = k - i * tw;
+    for (StepWalk wk(threadIdx.x, blockDim.x, tw); wk.k < wr * tw; wk.next()) {
+      const int i = wk.r, j = wk.q;
       const int* w = win + i * AV1B_LR_WC + j;
       int acc = 0;
 #pragma unroll
@@ -1105,8 +1105,8 @@ __global__ void __launch_bounds__(256) k_lr_tile(const px_t* __restrict__ cdef,
       mid[i * AV1B_LR_AC + j] = clampi(rnd2(acc, r0), -offset, limit - offset);
     }
     __syncthreads();
-    for (int k = threadIdx.x; k < th * tw; k += blockDim.x) {
-      const int i = k / tw, j = k - i * tw;
+    for (StepWalk wk(threadIdx.x, blockDim.x, tw); wk.k < th * tw; wk.next()) {
+      const int i = wk.r, j = wk.q;
       int acc = 0;
 #pragma unroll
       for (int t = 0; t < 7; ++t) acc += vt[t] * mid[(i + t) * AV1B_LR_AC + j];
@@ -1126,8 +1126,8 @@ __global__ void __launch_bounds__(256) k_lr_tile(const px_t* __restrict__ cdef,
     const long long n2e = (long long)n * n * u.e[pass];
     const long long mtable = ((1LL << 20) + n2e / 2) / n2e;
     const int one_over_n = ((1 << 12) + (n / 2)) / n;
-    for (int k = threadIdx.x; k < ar * ac; k += blockDim.x) {
-      const int i = k / ac, j = k - i * ac;
+    for (StepWalk wk(threadIdx.x, blockDim.x, ac); wk.k < ar * ac; wk.next()) {
+      const int i = wk.r, j = wk.q;
       /* the first pass reads odd rows only */
       if (pass == 0 && !((y0 - 1 + i) & 1)) continue;
       unsigned sq = 0;   /* at most 25 * 4095^2 */
@@ -1154,8 +1154,8 @@ __global__ void __launch_bounds__(256) k_lr_tile(const px_t* __restrict__ cdef,
   }
   __syncthreads();
   const int w0 = u.xqd[0], w1 = u.xqd[1], w2 = 128 - w0 - w1;
-  for (int k = threadIdx.x; k < th * tw; k += blockDim.x) {
-    const int i = k / tw, j = k - i * tw;
+  for (StepWalk wk(threadIdx.x, blockDim.x, tw); wk.k < th * tw; wk.next()) {
+    const int i = wk.r, j = wk.q;
     const int y = y0 + i;
     const int v = win[(i + 3) * AV1B_LR_WC + j + 3];
     int flt[2] = {0, 0};
