@@ -156,6 +156,8 @@ __global__ void __launch_bounds__(128) k_inter_simple(const __grid_constant__ Fr
   c.scale_y = a.scale_y;
   const int x0 = t.y & 0xffff, y0 = t.y >> 16;
   const int tw = mini(16, b.w - x0), th = mini(8, b.h - y0);
+  /* k / tw for the tile's k < 128 as a multiply and a shift (exact there) */
+  const int tmul = (65536 + tw - 1) / tw;
   const int nref = b.compound ? 2 : 1;
   for (int r = 0; r < nref; ++r) {
     int* pr = pred[wib][r];
@@ -185,7 +187,7 @@ __global__ void __launch_bounds__(128) k_inter_simple(const __grid_constant__ Fr
   for (int q = 0; q < 4; ++q) {
     const int k = lane + 32 * q;
     if (k >= tw * th) continue;
-    const int yy = k / tw, xx = k - yy * tw;
+    const int yy = (k * tmul) >> 16, xx = k - yy * tw;
     const int v0 = pred[wib][0][yy * 16 + xx];
     int out = v0;
     if (b.compound == 1) {
@@ -211,7 +213,7 @@ __global__ void __launch_bounds__(128) k_inter_simple(const __grid_constant__ Fr
     for (int q = 0; q < 4; ++q) {
       const int k = lane + 32 * q;
       if (k >= tw * th) continue;
-      const int yy = k / tw, xx = k - yy * tw;
+      const int yy = (k * tmul) >> 16, xx = k - yy * tw;
       const int x = x0 + xx, y = y0 + yy;
       if (x < ix0 || x >= ix1 || y < iy0 || y >= iy1) continue;
       const int pv = ok ? tmp[(y - iy0) * 16 + x - ix0]
@@ -225,7 +227,7 @@ __global__ void __launch_bounds__(128) k_inter_simple(const __grid_constant__ Fr
   for (int q = 0; q < 4; ++q) {
     const int k = lane + 32 * q;
     if (k < tw * th) {
-      const int yy = k / tw, xx = k - yy * tw;
+      const int yy = (k * tmul) >> 16, xx = k - yy * tw;
       dst[yy * g.stride + xx] = (px_t)acc[q];
     }
   }
@@ -250,6 +252,8 @@ __global__ void __launch_bounds__(128, 4) k_inter(const __grid_constant__ FrameA
   make_inter_job(a, b, &j);
   const int x0 = t.y & 0xffff, y0 = t.y >> 16;
   const int tw = mini(16, b.w - x0), th = mini(8, b.h - y0);
+  /* k / tw for the tile's k < 128 as a multiply and a shift (exact there) */
+  const int tmul = (65536 + tw - 1) / tw;
   const PlaneGeom& g = a.L.p[b.plane];
   px_t* dst = a.cur + g.off + (b.y + y0) * g.stride + b.x + x0;
   if (j.interintra) {
@@ -325,7 +329,7 @@ __global__ void __launch_bounds__(128, 4) k_inter(const __grid_constant__ FrameA
   for (int q = 0; q < 4; ++q) {
     const int k = lane + 32 * q;
     if (k < tw * th) {
-      const int yy = k / tw, xx = k - yy * tw;
+      const int yy = (k * tmul) >> 16, xx = k - yy * tw;
       const int v0 = pred[wib][0][yy * 16 + xx], v1 = nref > 1 ? pred[wib][1][yy * 16 + xx] : 0;
       if (luma_mask) {
         /* the chroma sample's mask: the mean over the luma samples it covers */
@@ -360,7 +364,7 @@ __global__ void __launch_bounds__(128, 4) k_inter(const __grid_constant__ FrameA
     for (int q = 0; q < 4; ++q) {
       const int k = lane + 32 * q;
       if (k >= tw * th) continue;
-      const int yy = k / tw, xx = k - yy * tw;
+      const int yy = (k * tmul) >> 16, xx = k - yy * tw;
       const int x = x0 + xx, y = y0 + yy;
       if (x < ix0 || x >= ix1 || y < iy0 || y >= iy1) continue;
       const int pv = ok ? tmp[(y - iy0) * 16 + x - ix0]
@@ -374,7 +378,7 @@ __global__ void __launch_bounds__(128, 4) k_inter(const __grid_constant__ FrameA
   for (int q = 0; q < 4; ++q) {
     const int k = lane + 32 * q;
     if (k < tw * th) {
-      const int yy = k / tw, xx = k - yy * tw;
+      const int yy = (k * tmul) >> 16, xx = k - yy * tw;
       dst[yy * g.stride + xx] = (px_t)acc[q];
     }
   }
