@@ -338,6 +338,16 @@ struct PinnedAlloc {
     return static_cast<T*>(p);
   }
   void deallocate(T* p, size_t) { cudaFreeHost(p); }
+  /* resize() leaves new elements uninitialised: every list is written in
+   * full by the planner, and zeroing megabytes first is serial work */
+  template <class U>
+  void construct(U* p) noexcept {
+    ::new (static_cast<void*>(p)) U;
+  }
+  template <class U, class... Args>
+  void construct(U* p, Args&&... args) {
+    ::new (static_cast<void*>(p)) U(std::forward<Args>(args)...);
+  }
   template <class U>
   bool operator==(const PinnedAlloc<U>&) const { return true; }
   template <class U>
@@ -1178,14 +1188,23 @@ void plan_itx(const PlanCtx& c, Plan* P) {
   });
   /* batches: runs of 32 / S jobs of one class (one job for the 64-point
    * class and for raw residual blocks), one launch per class */
+  int nb = 0;
   for (int cl = 2; cl < 8; ++cl) {
     if (cls_begin[cl] < 0 || cls_end[cl] <= cls_begin[cl]) continue;
     const int per = cl >= 6 ? 1 : 32 >> cl;
-    P->itx_class_first[cl] = static_cast<int>(R.itx_batches.size());
-    for (int i = cls_begin[cl]; i < cls_end[cl]; i += per)
-      R.itx_batches.push_back(make_int4(i, std::min(per, cls_end[cl] - i), cl, 0));
-    P->itx_class_count[cl] = static_cast<int>(R.itx_batches.size()) - P->itx_class_first[cl];
+    P->itx_class_first[cl] = nb;
+    P->itx_class_count[cl] = (cls_end[cl] - cls_begin[cl] + per - 1) / per;
+    nb += P->itx_class_count[cl];
   }
+  sized(R.itx_batches, nb);
+  c.pool->run(6, [&](int k) {
+    const int cl = k + 2;
+    if (P->itx_class_count[cl] == 0) return;
+    const int per = cl >= 6 ? 1 : 32 >> cl;
+    int4* out = R.itx_batches.data() + P->itx_class_first[cl];
+    for (int b = 0, i = cls_begin[cl]; i < cls_end[cl]; ++b, i += per)
+      out[b] = make_int4(i, std::min(per, cls_end[cl] - i), cl, 0);
+  });
 }
 
 /* Stages the profiler reports (av1b_profile). */
@@ -2287,7 +2306,10 @@ int av1b_decoder_create(int device, size_t hbm_budget_bytes, av1b_decoder** out)
 #else
     const int threads = static_cast<int>(std::min(16u, std::max(2u, hc) - 1));
 #endif
-    d->planners.resize(2);
+#ifndef AV1B_PLANNERS
+#define AV1B_PLANNERS 2
+#endif
+    d->planners.resize(AV1B_PLANNERS);
     for (auto& q : d->planners) {
       q.pool = new WorkPool(threads);
       q.scratch = new PlanScratch;

@@ -341,19 +341,22 @@ def run_ours(args):
     e2e_dec = av1b.Decoder(local)
     e2e_ring = [e2e_dec.reserve_reference() for _ in range(4)]
 
-    def e2e_step():
-        """One step through the public plan / decode API, pipelined the way the
-        API is meant for: two planner threads plan frames k + 1 .. k + 3
-        (validation, records, upload from the pinned host blob) while the
-        device decodes frame k; its NV12 goes out through the split pack
-        (av1b_nv12_pack_begin / wait / release: packed on the device, read back
-        into the library's page-locked memory on its copy stream while frame
-        k + 1 decodes). Frames decode in order; the host holds frame k - 1's
-        NV12 once frame k is queued."""
+    def e2e_run(steps):
+        """`steps` steps through the public plan / decode API, pipelined the way
+        the API is meant for and the way a stream runs, without a drain between
+        steps: two planner threads plan frames k + 1 .. k + 3 (validation,
+        records, upload from the pinned host blob) while the device decodes
+        frame k; its NV12 goes out through the split pack (av1b_nv12_pack_begin
+        / wait / release: packed on the device, read back into the library's
+        page-locked memory on its copy stream while frame k + 1 decodes).
+        Frames decode in order; the host holds frame k - 1's NV12 once frame k
+        is queued. Step s decodes the GOP's frames again as frames
+        s * F .. s * F + F - 1 of the stream."""
         ahead = 3
+        n = steps * len(pinned)
 
         def plan(k):
-            b = pinned[k]
+            b = pinned[k % len(pinned)]
             dists = b.get_refs()
             b.set_refs([e2e_ring[(k - d) % 4] for d in dists])
             view = ctypes.create_string_buffer(4096)
@@ -367,10 +370,10 @@ def run_ours(args):
 
         packs = []
         with ThreadPoolExecutor(max_workers=2) as ex:
-            futs = {k: ex.submit(plan, k) for k in range(min(ahead, len(pinned)))}
-            for k in range(len(pinned)):
+            futs = {k: ex.submit(plan, k) for k in range(min(ahead, n))}
+            for k in range(n):
                 h = futs.pop(k).result()
-                if k + ahead < len(pinned):
+                if k + ahead < n:
                     futs[k + ahead] = ex.submit(plan, k + ahead)
                 got = ctypes.c_int(-1)
                 rc = av1b.lib().av1b_decode_planned(e2e_dec.h, h, e2e_ring[k % 4], 1, None,
@@ -390,12 +393,10 @@ def run_ours(args):
 
     e2e_s = float('inf')
     if not args.no_e2e:
-        for _ in range(args.warmup):  # the planners' lists and plans reach their sizes
-            e2e_step()
+        e2e_run(args.warmup)  # the planners' lists and plans reach their sizes
         barrier()
         t0 = time.perf_counter()
-        for _ in range(args.steps):
-            e2e_step()
+        e2e_run(args.steps)
         torch.cuda.synchronize()
         e2e_s = time.perf_counter() - t0
     if dist is not None:
