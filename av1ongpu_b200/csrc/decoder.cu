@@ -99,7 +99,7 @@ struct av1b_decoder {
   Layout L{};
 
   /* pictures */
-  DevBuf cur, snap, lr_pre, lr_pre_up, lr_cdef, disp;
+  DevBuf cur, snap, lr_pre_up, lr_cdef, disp;
   DevBuf cdef_search;             /* CDEF direction search results */
   DevBuf pre_res;                 /* phase B residuals computed ahead */
   bool disp_is_cur = true;
@@ -1951,7 +1951,7 @@ int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, cons
       (rc = dev_ensure(d, d->cdef_search, (P.cdef_grid_n + P.n_cdef_search) * sizeof(int))))
     return rc;
   if (P.use_lr) {
-    if ((rc = dev_ensure(d, d->lr_pre, pic_bytes)) || (rc = dev_ensure(d, d->lr_cdef, pic_bytes)) ||
+    if ((rc = dev_ensure(d, d->lr_cdef, pic_bytes)) ||
         (P.upscaled && (rc = dev_ensure(d, d->lr_pre_up, pic_bytes))))
       return rc;
   }
@@ -2088,15 +2088,16 @@ int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, cons
                                maxv, st);
        }), "deblock H");
   launches += ((P.n_dbv != 0)) + ((P.n_dbh != 0));
+  /* One snapshot of the deblocked picture serves CDEF (its source, CDEF
+   * writes the picture) and loop restoration (the pre-CDEF rows of its
+   * stripe boundaries); with superres the upscaled picture goes out of place
+   * into the restoration's source buffer, so it needs no snapshot of its own */
   px_t* snap = static_cast<px_t*>(d->snap.p);
-  if (P.use_lr)
-    CK(timed(d, kStCopy, [&] {
-         return cudaMemcpyAsync(d->lr_pre.p, cur, pic_bytes, cudaMemcpyDeviceToDevice, st);
-       }), "pre-CDEF copy");
-  if ((P.n_cdef != 0)) {
+  if ((P.n_cdef != 0) || P.use_lr)
     CK(timed(d, kStCopy, [&] {
          return cudaMemcpyAsync(snap, cur, pic_bytes, cudaMemcpyDeviceToDevice, st);
-       }), "CDEF snapshot");
+       }), "deblocked snapshot");
+  if ((P.n_cdef != 0)) {
     CK(timed(d, kStCdef, [&] {
          return launch_cdef(snap, cur, reinterpret_cast<const CdefRec*>(fl + pl->o_cdef),
                             static_cast<int>(P.n_cdef), P.cdef_grid_w, P.cdef_grid_n,
@@ -2107,31 +2108,37 @@ int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, cons
        }), "CDEF");
     ++launches;
   }
-  const px_t* lr_curr = static_cast<px_t*>(d->lr_pre.p);
+  px_t* lr_cdef = static_cast<px_t*>(d->lr_cdef.p);
+  const px_t* lr_curr = snap;
   if (P.upscaled) {
-    CK(timed(d, kStCopy, [&] {
-         return cudaMemcpyAsync(snap, cur, pic_bytes, cudaMemcpyDeviceToDevice, st);
-       }), "superres snapshot");
-    CK(timed(d, kStUpscale, [&] { return launch_upscale(snap, cur, L, maxv, false, st); }), "superres");
-    ++launches;
     if (P.use_lr) {
       CK(timed(d, kStUpscale, [&] {
-           return launch_upscale(static_cast<px_t*>(d->lr_pre.p), static_cast<px_t*>(d->lr_pre_up.p),
-                                 L, maxv, true, st);
+           return launch_upscale(snap, static_cast<px_t*>(d->lr_pre_up.p), L, maxv, true, st);
          }), "superres (pre-CDEF)");
-      ++launches;
+      CK(timed(d, kStUpscale, [&] { return launch_upscale(cur, lr_cdef, L, maxv, false, st); }),
+         "superres");
+      launches += 2;
       lr_curr = static_cast<px_t*>(d->lr_pre_up.p);
+    } else {
+      CK(timed(d, kStCopy, [&] {
+           return cudaMemcpyAsync(snap, cur, pic_bytes, cudaMemcpyDeviceToDevice, st);
+         }), "superres snapshot");
+      CK(timed(d, kStUpscale, [&] { return launch_upscale(snap, cur, L, maxv, false, st); }),
+         "superres");
+      ++launches;
     }
+  } else if (P.use_lr) {
+    CK(timed(d, kStCopy, [&] {
+         return cudaMemcpyAsync(lr_cdef, cur, pic_bytes, cudaMemcpyDeviceToDevice, st);
+       }), "LR snapshot");
   }
   if (P.use_lr) {
-    CK(timed(d, kStCopy, [&] {
-         return cudaMemcpyAsync(d->lr_cdef.p, cur, pic_bytes, cudaMemcpyDeviceToDevice, st);
-       }), "LR snapshot");
     LrArgs lr = P.lr;
     for (int p = 0; p < 3; ++p) lr.units[p] = reinterpret_cast<const LrUnitRec*>(ar + pl->o_lr[p]);
-    CK(timed(d, kStLr, [&] {
-         return launch_lr(static_cast<px_t*>(d->lr_cdef.p), lr_curr, cur, L, lr, maxv, st);
-       }), "loop restoration");
+    /* with superres the restoration's source is the upscaled picture, not
+     * the picture's own content: tiles it does not restore pass through */
+    CK(timed(d, kStLr, [&] { return launch_lr(lr_cdef, lr_curr, cur, L, lr, maxv, P.upscaled, st); }),
+       "loop restoration");
     ++launches;
   }
   if (keep)
@@ -2362,7 +2369,7 @@ int av1b_decoder_destroy(av1b_decoder* d) {
   }
   d->packs.clear();
   if (d->copy_stream) cudaStreamDestroy(d->copy_stream);
-  DevBuf* bufs[] = {&d->cur, &d->snap, &d->lr_pre, &d->lr_pre_up, &d->lr_cdef, &d->disp,
+  DevBuf* bufs[] = {&d->cur, &d->snap, &d->lr_pre_up, &d->lr_cdef, &d->disp,
                     &d->slot_ptr_dev, &d->arena, &d->coef, &d->residual, &d->done,
                     &d->status_q, &d->nv12, &d->rgb,
                     &d->grain_state, &d->orbit, &d->pos, &d->cdef_search, &d->pre_res, &d->trace};

@@ -1045,12 +1045,12 @@ __global__ void k_upscale(const px_t* __restrict__ src, px_t* dst,
 __global__ void __launch_bounds__(256) k_lr_tile(const px_t* __restrict__ cdef,
                                                  const px_t* __restrict__ curr, px_t* dst,
                                                  const __grid_constant__ Layout L,
-                                                 const __grid_constant__ LrArgs r, int maxv) {
+                                                 const __grid_constant__ LrArgs r, int maxv,
+                                                 int copy_rest) {
   __shared__ int win[AV1B_LR_WR * AV1B_LR_WC];
   __shared__ int aux[2][2][AV1B_LR_AR * AV1B_LR_AC];  /* Wiener: aux[0][0] = intermediate */
   __shared__ short xbyx1[256];   /* a2 = ((z << 8) + z / 2) / (z + 1), by z */
   const int p = blockIdx.z;
-  if (!r.type[p]) return;
   const PlaneGeom& g = L.p[p];
   const int sub_y = p > 0 ? L.ss_y : 0;
   const int x0 = blockIdx.x * AV1B_LR_TW;
@@ -1061,14 +1061,23 @@ __global__ void __launch_bounds__(256) k_lr_tile(const px_t* __restrict__ cdef,
   const int s1 = s0 + (64 >> sub_y) - 1;
   const int y0 = maxi(s0, 0), y1 = mini(g.out_h, s1 + 1);
   if (y0 >= y1) return;
-  const int us = r.unit_size[p];
-  const int urow = mini(r.unit_rows[p] - 1, ((((y0 << sub_y) + 8) >> sub_y) / us));
-  const int ucol = mini(r.unit_cols[p] - 1, x0 / us);
-  const int idx = urow * r.unit_cols[p] + ucol;
-  if (idx >= r.n_units[p]) return;
-  const LrUnitRec u = r.units[p][idx];
-  if (u.type != 1 && u.type != 2) return;
   const int tw = mini(AV1B_LR_TW, g.out_w - x0), th = y1 - y0;
+  LrUnitRec u{};
+  if (r.type[p]) {
+    const int us = r.unit_size[p];
+    const int urow = mini(r.unit_rows[p] - 1, ((((y0 << sub_y) + 8) >> sub_y) / us));
+    const int ucol = mini(r.unit_cols[p] - 1, x0 / us);
+    const int idx = urow * r.unit_cols[p] + ucol;
+    if (idx < r.n_units[p]) u = r.units[p][idx];
+  }
+  if (u.type != 1 && u.type != 2) {
+    /* not restored: with `copy_rest` (the source is not the destination's
+     * own content) the tile passes through */
+    if (copy_rest)
+      for (StepWalk wk(threadIdx.x, blockDim.x, tw); wk.k < th * tw; wk.next())
+        dst[g.off + (y0 + wk.r) * g.stride + x0 + wk.q] = cdef[g.off + (y0 + wk.r) * g.stride + x0 + wk.q];
+    return;
+  }
   const int wr = th + 6, wc = tw + 6;
   const px_t* pc = cdef + g.off;
   const px_t* pp = curr + g.off;
@@ -1592,10 +1601,10 @@ cudaError_t launch_upscale(const px_t* src, px_t* dst, const Layout& L, int maxv
 }
 
 cudaError_t launch_lr(const px_t* cdef, const px_t* curr, px_t* dst, const Layout& L,
-                      const LrArgs& r, int maxv, cudaStream_t s) {
+                      const LrArgs& r, int maxv, bool copy_rest, cudaStream_t s) {
   const int stripes = (L.p[0].out_h + 8 + 63) / 64;
   k_lr_tile<<<dim3(cdiv(L.p[0].out_w, AV1B_LR_TW), stripes, 3), 256, 0, s>>>(cdef, curr, dst, L, r,
-                                                                            maxv);
+                                                                            maxv, copy_rest ? 1 : 0);
   return cudaGetLastError();
 }
 

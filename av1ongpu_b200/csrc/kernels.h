@@ -119,7 +119,7 @@ cudaError_t launch_cdef(const px_t* src, px_t* dst, const CdefRec* recs, int n, 
 cudaError_t launch_upscale(const px_t* src, px_t* dst, const Layout& L, int maxv, bool border_rows,
                            cudaStream_t s);
 cudaError_t launch_lr(const px_t* cdef, const px_t* curr, px_t* dst, const Layout& L,
-                      const LrArgs& r, int maxv, cudaStream_t s);
+                      const LrArgs& r, int maxv, bool copy_rest, cudaStream_t s);
 cudaError_t launch_grain_template(GrainState* gs, const GrainParamsDev& prm, const uint16_t* orbit,
                                   const uint16_t* pos, cudaStream_t s);
 cudaError_t launch_grain_blend(const px_t* src, px_t* dst, const Layout& L, const GrainState* gs,
