@@ -261,6 +261,36 @@ AV1B_DEV void intra_predict(const IntraJob& j, px_t* dst, int stride, const px_t
   intra_edges(j, dst, stride, above, left, lane);
   if (res_in_flight) async_copies_done();
 
+  if (j.mode == 13 && fi_pred && n <= 1024) {
+    /* chroma from luma, each sample's luma value read once: kept in the
+     * filter-intra buffer (unused by a CFL block) between the average and the
+     * prediction, and fetched four iterations at a time */
+    const int dc = intra_dc(j, above, left, lane);
+    const int sx = j.ss_x, sy = j.ss_y;
+    const int lxl = ((j.x + w) << sx) - (1 << sx);
+    const int lyl = ((j.y + h) << sy) - (1 << sy);
+    long long sum = 0;
+#pragma unroll 4
+    for (int k = lane; k < n; k += 32) {
+      const int i = k >> lw, jj = k & (w - 1);
+      const int ly = mini((j.y + i) << sy, lyl), lx = mini((j.x + jj) << sx, lxl);
+      int t = 0;
+      for (int a = 0; a <= sy; ++a)
+        for (int b = 0; b <= sx; ++b) t += ldpx(luma + (ly + a) * luma_stride + lx + b);
+      t <<= 3 - sx - sy;
+      fi_pred[k] = t;
+      sum += t;
+    }
+    sum = warp_sum64(sum);
+    const int shift = lw + ilog2(h);
+    const int avg = (int)((sum + (1LL << (shift - 1))) >> shift);
+    __syncwarp();
+    for (int k = lane; k < n; k += 32) {
+      const int i = k >> lw, jj = k & (w - 1);
+      put(i, jj, clampi(dc + rnd2s(j.cfl_alpha * (fi_pred[k] - avg), 6), 0, j.maxv));
+    }
+    return;
+  }
   if (j.mode == 13) { /* chroma from luma */
     const int dc = intra_dc(j, above, left, lane);
     const int sx = j.ss_x, sy = j.ss_y;

@@ -595,10 +595,25 @@ __device__ void add_residual_cg(const FrameArgs& a, const BlockRec& b, const TxR
   const PlaneGeom& g = a.L.p[b.plane];
   px_t* dst = a.cur + g.off + (b.y + tx.y) * g.stride + b.x + tx.x;
   const int* res = b.residual_provided ? a.residual + tx.coef_off : a.pre_res + tx.pre_off;
-  for (int k = lane; k < tx.w * tx.h; k += 32) {
-    const int yy = k / tx.w, xx = k - yy * tx.w;
-    px_t* q = dst + yy * g.stride + xx;
-    *q = (px_t)clampi((int)__ldcg(q) + res[yy * tx.w + xx], 0, a.maxv);
+  /* four samples a lane at a time, every load before any store: the loads
+   * read the picture the stores write, so the compiler cannot overlap one
+   * sample's load with another's store by itself */
+  const int n = tx.w * tx.h;
+  for (int k0 = lane; k0 < n; k0 += 4 * 32) {
+    int v[4];
+    int o[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int k = k0 + 32 * q;
+      if (k < n) {
+        const int yy = k / tx.w, xx = k - yy * tx.w;
+        o[q] = yy * g.stride + xx;
+        v[q] = (int)__ldcg(dst + o[q]) + res[k];
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      if (k0 + 32 * q < n) dst[o[q]] = (px_t)clampi(v[q], 0, a.maxv);
   }
   __syncwarp();
 }
