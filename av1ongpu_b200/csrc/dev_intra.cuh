@@ -397,6 +397,28 @@ AV1B_DEV void intra_predict(const IntraJob& j, px_t* dst, int stride, const px_t
     }
     return;
   }
+  if (mode >= 9 && mode <= 11 && w >= 32) {
+    /* wide blocks: a lane keeps its column's above sample and weight and
+     * walks down the rows */
+    const int bl = left[h - 1], tr = above[w - 1];
+    for (int c = lane; c < w; c += 32) {
+      const int av = above[c], wx = sm_weight(w, c);
+      for (int i = 0; i < h; ++i) {
+        int pred;
+        if (mode == 9) {
+          const int wy = sm_weight(h, i);
+          pred = rnd2(wy * av + (256 - wy) * bl + wx * left[i] + (256 - wx) * tr, 9);
+        } else if (mode == 10) {
+          const int wy = sm_weight(h, i);
+          pred = rnd2(wy * av + (256 - wy) * bl, 8);
+        } else {
+          pred = rnd2(wx * left[i] + (256 - wx) * tr, 8);
+        }
+        put(i, c, clampi(pred, 0, j.maxv));
+      }
+    }
+    return;
+  }
   if (mode >= 9 && mode <= 11) {
     for (int k = lane; k < n; k += 32) {
       const int i = k >> lw, jj = k & (w - 1);

@@ -24,9 +24,13 @@ namespace av1b {
 /* Phase B: shared-memory scratch per warp (ints) - the residual image of a
  * block whose prediction and residual fuse (so blocks of up to this many
  * samples fuse) and, for filter intra (at most 32x32), its predictions at
- * offset 1024 - and the CTAs of four warps resident per SM. */
-#define AV1B_UNIT_SCRATCH 2048
-#define AV1B_UNIT_CTAS_PER_SM 4
+ * offset 1024 - and the CTAs of four warps resident per SM. Blocks up to
+ * 64x64 fuse: the unfused path reads the prediction back through L2, a
+ * round trip a batch of samples that costs a 64x64 block tens of
+ * microseconds on the dependency path, more than the halved residency (two
+ * CTAs a SM instead of four) costs. */
+#define AV1B_UNIT_SCRATCH 4096
+#define AV1B_UNIT_CTAS_PER_SM 2
 
 struct FrameArgs {
   Layout L;
