@@ -274,6 +274,35 @@ def test_invalid_records_name_the_first_one(av1b, oracle, dec):
     dec.release_reference(slot)
 
 
+def test_unit_trace_is_consistent(av1b, oracle, dec):
+    """The opt-in phase B trace: every dependency-scheduled block of a key
+    frame has a record, claimed <= ready <= published, and the dependency it
+    names as published last was published before it became ready. Tracing
+    changes no sample."""
+    b = av1b.synth_frame(2, 4, 11, 0)
+    slot0, plain = dec.decode(b)
+    dec.release_reference(slot0)
+    dec.set_unit_trace(True)
+    try:
+        slot, traced = dec.decode(b)
+        tr = dec.unit_trace().astype(np.int64)
+    finally:
+        dec.set_unit_trace(False)
+    dec.release_reference(slot)
+    for p in range(3):
+        assert np.array_equal(plain[p], traced[p])
+    assert tr.shape == (oracle.blob_counts(b)['blocks'], 4)
+    live = np.nonzero(tr[:, 2])[0]
+    assert len(live) > 100          # a key frame: every block is in phase B
+    assert np.all(tr[live, 0] <= tr[live, 1]) and np.all(tr[live, 1] <= tr[live, 2])
+    who = tr[live, 3]
+    named = who >= 0
+    named &= who < len(tr)
+    deps = who[named]
+    assert np.all(tr[deps, 2] > 0)
+    assert np.all(tr[deps, 2] <= tr[live[named], 1])
+
+
 def test_bounded_wait_gives_up(dec):
     """A device wait on a flag nothing sets returns an error status after its
     limit instead of hanging (no fault, no trap)."""
