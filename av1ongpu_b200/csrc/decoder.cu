@@ -773,7 +773,7 @@ struct PlanScratch {
   std::vector<BlockOut> blocks;
   std::vector<int> owner[3];
   std::vector<std::vector<int>> unit_deps;
-  std::vector<int> dep_count, depth, sorted;
+  std::vector<int> dep_count;
   std::vector<int> chain_of, chain_tail, chain_len, height, crit, best;
   std::vector<int> units_coding, ui_of, udepth, udeps;
   std::vector<uint8_t> is_b;
@@ -855,9 +855,9 @@ int plan_units(av1b_decoder* d, const PlanCtx& c, Plan* P) {
     const int cx0 = std::max<int>(b.x, 0) >> sh[p], cy0 = std::max<int>(b.y, 0) >> sh[p];
     const int cx1 = std::min((b.x + b.w + oc - 1) >> sh[p], cw[p]);
     const int cy1 = std::min((b.y + b.h + oc - 1) >> sh[p], ch[p]);
+    const int w = cw[p], v = static_cast<int>(bi);
     int* o = S.owner[p].data();
-    for (int y = cy0; y < cy1; ++y)
-      for (int x = cx0; x < cx1; ++x) o[static_cast<size_t>(y) * cw[p] + x] = static_cast<int>(bi);
+    for (int y = cy0; y < cy1; ++y) std::fill(o + static_cast<size_t>(y) * w + cx0, o + static_cast<size_t>(y) * w + cx1, v);
   };
   {
     const int pieces = pieces_for(nb, c, 2048);
@@ -869,17 +869,26 @@ int plan_units(av1b_decoder* d, const PlanCtx& c, Plan* P) {
       for (size_t bi = 0; bi < nb; ++bi)
         if (!aligned[P->R->blocks[bi].plane]) fill(bi);
   }
-  auto owner_at = [&](int p, int x, int y) -> int {
-    if (x < 0 || y < 0 || x >= L.p[p].grid_w || y >= L.p[p].grid_h) return -1;
-    return S.owner[p][static_cast<size_t>(y >> sh[p]) * cw[p] + (x >> sh[p])];
-  };
-  /* the cells of [x0, x1] x [y0, y1]: `f(owner)` for each, from the cell
-   * holding (x0, y0) on (the device's wait_rect / decoded_before walk) */
+  /* the cells of [x0, x1] x [y0, y1] inside the plane's grid, row by row
+   * from the cell holding (x0, y0) (the device's wait_rect / decoded_before
+   * walk): `f(owner)` for each cell whose owner differs from the one of the
+   * cell before it. Every caller ignores -1 (no owner: outside the grid, or
+   * no block) and a repeat of the owner it was just given, so neither
+   * changes what it collects. */
   auto each_cell = [&](int p, int x0, int x1, int y0, int y1, auto&& f) {
-    const int oc = 1 << sh[p];
-    const int xs = x0 & ~(oc - 1), ys = y0 & ~(oc - 1);
-    for (int y = ys; y <= y1; y += oc)
-      for (int x = xs; x <= x1; x += oc) f(owner_at(p, x, y));
+    const int s = sh[p], w = cw[p];
+    const int cx0 = std::max(x0 >> s, 0), cx1 = std::min(x1 >> s, w - 1);
+    const int cy0 = std::max(y0 >> s, 0), cy1 = std::min(y1 >> s, ch[p] - 1);
+    const int* o = S.owner[p].data();
+    int last = -1;
+    for (int cy = cy0; cy <= cy1; ++cy) {
+      const int* row = o + static_cast<size_t>(cy) * w;
+      for (int cx = cx0; cx <= cx1; ++cx)
+        if (row[cx] != last) {
+          last = row[cx];
+          f(last);
+        }
+    }
   };
   static const int kAngle[9] = {0, 90, 180, 45, 135, 113, 157, 203, 67};
   const size_t nu = P->R->units.size();
@@ -888,6 +897,9 @@ int plan_units(av1b_decoder* d, const PlanCtx& c, Plan* P) {
   if (pdeps.size() < static_cast<size_t>(pieces)) pdeps.resize(pieces);
   std::vector<int>& dep_count = S.dep_count;
   dep_count.assign(nu, 0);
+  std::vector<int>& ui_of = S.ui_of;  /* a phase B block's unit index */
+  ui_of.resize(nb);
+  std::vector<uint8_t> inter_piece(pieces, 0);
   c.pool->run(pieces, [&](int pi) {
     std::vector<int>& out = pdeps[pi];
     out.clear();
@@ -895,6 +907,8 @@ int plan_units(av1b_decoder* d, const PlanCtx& c, Plan* P) {
     for (size_t ui = piece_begin(nu, pieces, pi); ui < piece_begin(nu, pieces, pi + 1); ++ui) {
       const int bi = P->R->units[ui];
       BlockRec& b = P->R->blocks[bi];
+      ui_of[bi] = static_cast<int>(ui);
+      if (b.kind != AV1B_U_INTRA) inter_piece[pi] = 1;
       const int p = b.plane, oc = 1 << sh[p];
       mine.clear();
       /* neighbouring cells mostly share an owner: skip the repeat at once */
@@ -995,125 +1009,113 @@ int plan_units(av1b_decoder* d, const PlanCtx& c, Plan* P) {
       out.insert(out.end(), mine.begin(), mine.end());
     }
   });
-  /* depths, in coding order (every dependency precedes its dependant) */
-  std::vector<int>& depth = S.depth;
-  depth.assign(nb, 0);
+  /* the lists back to back for the device (block indices), and as unit
+   * indices for the passes below */
   std::vector<size_t> first(nu + 1, 0);
   for (size_t ui = 0; ui < nu; ++ui) first[ui + 1] = first[ui] + dep_count[ui];
   if (first[nu] > static_cast<size_t>(INT32_MAX)) return fail(d, AV1B_ERR_SYNTAX, "frame too large");
   sized(P->R->deps, first[nu]);
+  std::vector<int>& udeps = S.udeps;
+  udeps.resize(first[nu]);
   c.pool->run(pieces, [&](int pi) {
-    std::copy(pdeps[pi].begin(), pdeps[pi].end(),
-              P->R->deps.begin() + first[piece_begin(nu, pieces, pi)]);
-    for (size_t ui = piece_begin(nu, pieces, pi); ui < piece_begin(nu, pieces, pi + 1); ++ui) {
+    const size_t u0 = piece_begin(nu, pieces, pi), u1 = piece_begin(nu, pieces, pi + 1);
+    std::copy(pdeps[pi].begin(), pdeps[pi].end(), P->R->deps.begin() + first[u0]);
+    for (size_t k = first[u0]; k < first[u1]; ++k) udeps[k] = ui_of[pdeps[pi][k - first[u0]]];
+    for (size_t ui = u0; ui < u1; ++ui) {
       BlockRec& b = P->R->blocks[P->R->units[ui]];
       b.dep_first = static_cast<int>(first[ui]);
       b.dep_count = dep_count[ui];
     }
   });
-  int max_depth = 0;
-  const int* dl = P->R->deps.data();
-  for (size_t ui = 0; ui < nu; ++ui) {
-    int dd = 0;
-    for (size_t k = first[ui]; k < first[ui + 1]; ++k) dd = std::max(dd, depth[dl[k]]);
-    depth[P->R->units[ui]] = dd + 1;
-    max_depth = std::max(max_depth, dd + 1);
-  }
   /* chains: a warp claims a chain and runs its blocks in order, so a block
    * whose deepest dependency is the block before it in its chain waits on
-   * its own warp's work instead of a flag published on another SM. Blocks
-   * are taken in order of depth (coding order within one depth). A block's
-   * candidate predecessor is its deepest dependency; of the blocks naming
-   * the same candidate, the one with the longest path still ahead of it
-   * (its height) gets it, so chains follow the critical path. It joins the
-   * candidate's chain when the candidate is that chain's last block and
-   * every other block it reads lies earlier in that chain or in an earlier
-   * chain; otherwise it starts a chain. Chains are claimed in the order they
-   * were started, so every wait across chains is on a chain claimed before:
-   * the warp holding the earliest unfinished chain always progresses. The
-   * work is on unit indices (coding order), in arrays of the units alone. */
+   * its own warp's work instead of a flag published on another SM.
+   *
+   * A block's depth is 1 + the deepest block it waits for, and that block
+   * (the latest in coding order of equally deep ones) is its candidate
+   * predecessor. Of the blocks naming the same candidate, the one with the
+   * longest path still ahead of it (its height; the first in order of depth,
+   * then coding order, of equal ones) gets it, so chains follow the critical
+   * path. It joins the candidate's chain - as its next block: no other block
+   * can take that place - when every other block it waits for lies in that
+   * chain or in one started earlier; otherwise it starts a chain. Chains are
+   * ordered by their first block, by depth then coding order, and claimed in
+   * that order, so every wait across chains is on a chain claimed before: the
+   * warp holding the earliest unfinished chain always progresses. A chain's
+   * blocks are in coding order, which is also their order of depth.
+   *
+   * Every dependency precedes its dependant in coding order, so each pass is
+   * one sweep over the units in coding order (or its reverse, for heights). */
   std::vector<int>& U = S.units_coding;
   U.assign(P->R->units.begin(), P->R->units.end());
-  std::vector<int>& ui_of = S.ui_of;
-  ui_of.resize(nb);
   std::vector<int>& ud = S.udepth;
-  ud.resize(nu);
-  for (size_t ui = 0; ui < nu; ++ui) {
-    ui_of[U[ui]] = static_cast<int>(ui);
-    ud[ui] = depth[U[ui]];
-  }
-  std::vector<int> count(max_depth + 2, 0);
-  for (size_t ui = 0; ui < nu; ++ui) ++count[ud[ui] + 1];
-  for (int k = 0; k <= max_depth; ++k) count[k + 1] += count[k];
-  std::vector<int>& sorted = S.sorted;
-  sorted.resize(nu);
-  for (size_t ui = 0; ui < nu; ++ui) sorted[count[ud[ui]]++] = static_cast<int>(ui);
-  std::vector<int>& chain_of = S.chain_of;
-  std::vector<int>& tail = S.chain_tail;
-  std::vector<int>& clen = S.chain_len;
-  std::vector<int>& height = S.height;
   std::vector<int>& critv = S.crit;
-  std::vector<int>& best = S.best;
-  std::vector<int>& udeps = S.udeps;   /* the dependency lists as unit indices */
-  udeps.resize(first[nu]);
-  for (size_t k = 0; k < first[nu]; ++k) udeps[k] = ui_of[dl[k]];
-  height.assign(nu, 0);
-  critv.assign(nu, -1);
-  best.assign(nu, -1);
-  for (size_t k = nu; k-- > 0;) {
-    const int u = sorted[k];
+  ud.resize(nu);
+  critv.resize(nu);
+  int max_depth = 0;
+  for (size_t u = 0; u < nu; ++u) {
     int cr = -1;
     for (size_t j = first[u]; j < first[u + 1]; ++j) {
       const int o = udeps[j];
-      height[o] = std::max(height[o], height[u] + 1);
       if (cr < 0 || ud[o] > ud[cr] || (ud[o] == ud[cr] && o > cr)) cr = o;
     }
     critv[u] = cr;
+    ud[u] = (cr >= 0 ? ud[cr] : 0) + 1;
+    max_depth = std::max(max_depth, ud[u]);
   }
-  for (size_t k = 0; k < nu; ++k) {
-    const int u = sorted[k], cr = critv[u];
-    if (cr >= 0 && (best[cr] < 0 || height[u] > height[best[cr]])) best[cr] = u;
-  }
-  chain_of.assign(nu, -1);
-  tail.clear();
-  clen.clear();
-  for (size_t k = 0; k < nu; ++k) {
-    const int u = sorted[k], cr = critv[u];
-    int ch = -1;
-    if (cr >= 0 && best[cr] == u && tail[chain_of[cr]] == cr) {
-      ch = chain_of[cr];
-      for (size_t j = first[u]; j < first[u + 1]; ++j)
-        if (chain_of[udeps[j]] > ch) {
-          ch = -1;
-          break;
-        }
+  std::vector<int>& height = S.height;
+  std::vector<int>& best = S.best;
+  height.assign(nu, 0);
+  best.assign(nu, -1);
+  for (size_t k = nu; k-- > 0;) {
+    const int u = static_cast<int>(k);  /* every block waiting for u is done: its height is final */
+    for (size_t j = first[u]; j < first[u + 1]; ++j) {
+      const int o = udeps[j];
+      height[o] = std::max(height[o], height[u] + 1);
     }
-    if (ch < 0) {
-      ch = static_cast<int>(tail.size());
-      tail.push_back(u);
-      clen.push_back(0);
+    const int cr = critv[u];
+    if (cr >= 0) {
+      const int bu = best[cr];  /* later in coding order than u */
+      if (bu < 0 || height[u] > height[bu] || (height[u] == height[bu] && ud[u] <= ud[bu])) best[cr] = u;
     }
-    chain_of[u] = ch;
-    tail[ch] = u;
-    ++clen[ch];
   }
-  const size_t nch = tail.size();
+  std::vector<int>& head = S.chain_of;  /* the first block of each block's chain */
+  head.resize(nu);
+  std::vector<int> count(max_depth + 2, 0);
+  for (size_t u = 0; u < nu; ++u) {
+    const int cr = critv[u];
+    int h = static_cast<int>(u);
+    if (cr >= 0 && best[cr] == static_cast<int>(u)) {
+      const int hc = head[cr];
+      bool ok = true;
+      for (size_t j = first[u]; j < first[u + 1] && ok; ++j) {
+        const int hj = head[udeps[j]];
+        if (ud[hj] > ud[hc] || (ud[hj] == ud[hc] && hj > hc)) ok = false;
+      }
+      if (ok) h = hc;
+    }
+    head[u] = h;
+    if (h == static_cast<int>(u)) ++count[ud[u] + 1];
+  }
+  for (int k = 0; k <= max_depth; ++k) count[k + 1] += count[k];
+  const size_t nch = static_cast<size_t>(count[max_depth + 1]);
+  std::vector<int>& cid = S.chain_tail;  /* a chain's place, by its first block */
+  std::vector<int>& clen = S.chain_len;
+  cid.resize(nu);
+  clen.assign(nch + 1, 0);
+  for (size_t u = 0; u < nu; ++u) {
+    if (head[u] == static_cast<int>(u)) cid[u] = count[ud[u]]++;
+    ++clen[cid[head[u]] + 1];
+  }
   sized(P->R->chains, nch + 1);
-  P->R->chains[0] = 0;
-  for (size_t k = 0; k < nch; ++k) P->R->chains[k + 1] = P->R->chains[k] + clen[k];
-  for (size_t k = 0; k < nch; ++k) clen[k] = P->R->chains[k];
-  for (size_t k = 0; k < nu; ++k) {
-    const int u = sorted[k];
-    P->R->units[clen[chain_of[u]]++] = U[u];
-  }
+  for (size_t k = 0; k < nch; ++k) clen[k + 1] += clen[k];
+  for (size_t k = 0; k <= nch; ++k) P->R->chains[k] = clen[k];
+  for (size_t u = 0; u < nu; ++u) P->R->units[clen[cid[head[u]]]++] = U[u];
   P->n_chains = nch;
   P->unit_depth = max_depth;
   P->units_inter = false;
-  for (size_t ui = 0; ui < nu; ++ui)
-    if (P->R->blocks[P->R->units[ui]].kind != AV1B_U_INTRA) {
-      P->units_inter = true;
-      break;
-    }
+  for (int pi = 0; pi < pieces; ++pi)
+    if (inter_piece[pi]) P->units_inter = true;
   return AV1B_OK;
 }
 
