@@ -2306,8 +2306,10 @@ int av1b_decoder_create(int device, size_t hbm_budget_bytes, av1b_decoder** out)
   }
   *d->status_host = 0;
   {
-    /* two planners: one plan at a time uses all cores but the one left to
-     * the thread that drives the device; two plans at once share them */
+    /* three planners: one plan at a time uses all cores but the one left to
+     * the thread that drives the device; plans at once share them (a key
+     * frame's plan takes several inter frames' time, and the other planners
+     * keep the device fed meanwhile) */
     const unsigned hc = std::thread::hardware_concurrency();
 #ifdef AV1B_PLANNER_THREADS
     const int threads = AV1B_PLANNER_THREADS;
@@ -2316,7 +2318,7 @@ int av1b_decoder_create(int device, size_t hbm_budget_bytes, av1b_decoder** out)
     const int threads = static_cast<int>(std::min(16u, std::max(2u, hc) - 1));
 #endif
 #ifndef AV1B_PLANNERS
-#define AV1B_PLANNERS 2
+#define AV1B_PLANNERS 3
 #endif
     d->planners.resize(AV1B_PLANNERS);
     for (auto& q : d->planners) {

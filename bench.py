@@ -344,7 +344,7 @@ def run_ours(args):
     def e2e_run(steps):
         """`steps` steps through the public plan / decode API, pipelined the way
         the API is meant for and the way a stream runs, without a drain between
-        steps: two planner threads plan frames k + 1 .. k + 3 (validation,
+        steps: three planner threads plan frames k + 1 .. k + 6 (validation,
         records, upload from the pinned host blob) while the device decodes
         frame k; its NV12 goes out through the split pack (av1b_nv12_pack_begin
         / wait / release: packed on the device, read back into the library's
@@ -352,7 +352,7 @@ def run_ours(args):
         Frames decode in order; the host holds frame k - 1's NV12 once frame k
         is queued. Step s decodes the GOP's frames again as frames
         s * F .. s * F + F - 1 of the stream."""
-        ahead = 3
+        ahead = 6
         n = steps * len(pinned)
 
         def plan(k):
@@ -369,7 +369,7 @@ def run_ours(args):
             return h
 
         packs = []
-        with ThreadPoolExecutor(max_workers=2) as ex:
+        with ThreadPoolExecutor(max_workers=3) as ex:
             futs = {k: ex.submit(plan, k) for k in range(min(ahead, n))}
             for k in range(n):
                 h = futs.pop(k).result()
