@@ -1002,40 +1002,86 @@ __global__ void __launch_bounds__(128) k_cdef(const px_t* __restrict__ src, px_t
 }
 
 /* ---- superres ------------------------------------------------------------------------- */
-/* One thread per 4 output samples of a row. `border_rows`: only the rows
- * within two of a loop restoration stripe boundary (the rows the restoration
- * reads from the pre-CDEF picture, av1gpu_kernels.h:2832-2845); the reference
- * upscales the whole pre-CDEF picture and reads only these. */
-__global__ void k_upscale(const px_t* __restrict__ src, px_t* dst,
-                          const __grid_constant__ Layout L,
-                          const __grid_constant__ UpscaleArgs u,
-                          int maxv, int border_rows) {
-  const int p = blockIdx.z;
+/* One CTA of 64 threads per 256 output samples of a row, a thread per 4.
+ * The source span those outputs read (a superres step is at most one source
+ * sample, so at most 256 + 8 samples) is staged in shared memory once, with
+ * the clamp to the coded row applied while staging, and the 8-tap phases
+ * beside it; each output then reads its taps there. Grid rows: the luma
+ * rows, then the chroma rows with plane 1's segments and plane 2's side by
+ * side. `border_rows`: only the rows within two of a loop restoration stripe
+ * boundary (the rows the restoration reads from the pre-CDEF picture,
+ * av1gpu_kernels.h:2832-2845); the reference upscales the whole pre-CDEF
+ * picture and reads only these. */
+#define AV1B_UP_OUT 256
+#define AV1B_UP_SPAN 288
+__global__ void __launch_bounds__(64) k_upscale(const px_t* __restrict__ src, px_t* dst,
+                                                const __grid_constant__ Layout L,
+                                                const __grid_constant__ UpscaleArgs u, int maxv,
+                                                int border_rows, int rows0) {
+  __shared__ __align__(16) short taps[512];
+  __shared__ px_t span[AV1B_UP_SPAN];
+  int y = blockIdx.y, p = 0, xb = blockIdx.x;
+  if (y >= rows0) {
+    y -= rows0;
+    const int xb1 = (L.p[1].out_w + AV1B_UP_OUT - 1) / AV1B_UP_OUT;
+    p = 1;
+    if (xb >= xb1) {
+      xb -= xb1;
+      p = 2;
+    }
+  }
   const PlaneGeom& g = L.p[p];
-  int y = blockIdx.y;
   if (border_rows) {
     const int sub_y = p > 0 ? L.ss_y : 0;
     const int b = (64 * (y / 4 + 1) - 8) >> sub_y;
     y = b - 2 + (y & 3);
     if (y < 0) return;
   }
-  if (y >= g.out_h) return;
-  const int x0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
-  if (x0 >= g.out_w) return;
+  const int xs = xb * AV1B_UP_OUT;
+  if (y >= g.out_h || xs >= g.out_w) return;  /* uniform over the CTA */
   const px_t* row = src + g.off + y * g.stride;
   px_t* out = dst + g.off + y * g.stride;
   const int last = g.coded_w - 1;
+  const int step = u.step[p], init = u.initial[p] - (1 << 14);
+  const int xe = min(xs + AV1B_UP_OUT, g.out_w) - 1;
+  const int p0 = (init + xs * step) >> 14;
+  const int n = ((init + xe * step) >> 14) - p0 + 8;
+  const bool staged = n <= AV1B_UP_SPAN;
+  for (int i = threadIdx.x; i < 512; i += blockDim.x) taps[i] = kUpscaleFilter[i];
+  if (staged)
+    for (int i = threadIdx.x; i < n; i += blockDim.x) span[i] = row[clampi(p0 - 3 + i, 0, last)];
+  __syncthreads();
+  const int x0 = xs + threadIdx.x * 4;
+  if (x0 > xe) return;
+  int o[4];
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
-    const int x = x0 + q;
-    if (x >= g.out_w) break;
-    const int sx = -(1 << 14) + u.initial[p] + x * u.step[p];
+    const int x = min(x0 + q, xe);  /* past the row's end: a repeat, not stored */
+    const int sx = init + x * step;
     const int px = sx >> 14;
-    const short* f = kUpscaleFilter + ((sx & ((1 << 14) - 1)) >> 8) * 8;
+    const int4 fv = *reinterpret_cast<const int4*>(taps + ((sx & ((1 << 14) - 1)) >> 8) * 8);
+    const int f[8] = {(short)fv.x, fv.x >> 16, (short)fv.y, fv.y >> 16,
+                      (short)fv.z, fv.z >> 16, (short)fv.w, fv.w >> 16};
     int sum = 0;
+    if (staged) {
+      const px_t* sp = span + (px - p0);
 #pragma unroll
-    for (int k = 0; k < 8; ++k) sum += (int)row[clampi(px + k - 3, 0, last)] * f[k];
-    out[x] = (px_t)clampi(rnd2(sum, 7), 0, maxv);
+      for (int k = 0; k < 8; ++k) sum += (int)sp[k] * f[k];
+    } else {
+#pragma unroll
+      for (int k = 0; k < 8; ++k) sum += (int)row[clampi(px + k - 3, 0, last)] * f[k];
+    }
+    o[q] = clampi(rnd2(sum, 7), 0, maxv);
+  }
+  if (x0 + 3 <= xe && (reinterpret_cast<uintptr_t>(out) & 7) == 0) {
+    uint2 v;
+    v.x = (unsigned)o[0] | ((unsigned)o[1] << 16);
+    v.y = (unsigned)o[2] | ((unsigned)o[3] << 16);
+    *reinterpret_cast<uint2*>(out + x0) = v;
+  } else {
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      if (x0 + q <= xe) out[x0 + q] = (px_t)o[q];
   }
 }
 
@@ -1320,97 +1366,181 @@ __global__ void __launch_bounds__(256) k_grain_template(GrainState* gs, GrainPar
     }
 }
 
-/* The stripe value of plane `p` at (row, col) of stripe `s` (7.18.3.5, the
- * horizontal half): the grain block that covers the column, blended with the
- * previous block at the two (one for subsampled chroma) overlap columns. */
-__device__ int grain_stripe(const GrainState* gs, const short* grain, int src_w, int sub_x, int sub_y,
-                            int s, int row, int col, const uint16_t* orbit, const uint16_t* pos,
-                            int gmin, int gmax) {
+/* The stripe values of plane `p` (7.18.3.5, the horizontal half: the grain
+ * block that covers the column, blended with the previous block at the two -
+ * one for subsampled chroma - overlap columns) of four samples
+ * x0 .. x0 + 3 of one row, x0 a multiple of 4: they lie in one grain block,
+ * whose random offset is computed once; only a group starting a block has
+ * overlap columns. */
+__device__ __forceinline__ void grain_stripe4(const GrainState* gs, const short* grain, int src_w,
+                                              int sub_x, int sub_y, int s, int row, int x0,
+                                              const uint16_t* orbit, const uint16_t* pos, int gmin,
+                                              int gmax, bool overlap, int n[4]) {
   unsigned st0 = (unsigned)gs->seed & 0xffffu;
   st0 ^= (unsigned)(((s * 37 + 178) & 255) << 8);
   st0 ^= (unsigned)((s * 173 + 105) & 255);
   st0 &= 0xffffu;
   const int bw_log = sub_x ? 4 : 5;
-  const int k = col >> bw_log;
-  const int j = col & ((1 << bw_log) - 1);
-  auto sample = [&](int blk, int jj) {
+  const int k = x0 >> bw_log, j0 = x0 & ((1 << bw_log) - 1);
+  auto block_row = [&](int blk) {
     const int r = (lfsr_after(orbit, pos, st0, blk + 1) >> 8) & 255;
     const int ox = r >> 4, oy = r & 15;
     const int src_x = sub_x ? 6 + ox : 9 + ox * 2;
     const int src_y = sub_y ? 6 + oy : 9 + oy * 2;
-    return (int)grain[(src_y + row) * src_w + src_x + jj];
+    return grain + (src_y + row) * src_w + src_x;
   };
-  int g = sample(k, j);
-  if (gs->overlap && k > 0) {
-    if (!sub_x && j < 2) {
-      const int old = sample(k - 1, j + 32);
-      g = clampi(rnd2z(j == 0 ? old * 27 + g * 17 : old * 17 + g * 27, 5), gmin, gmax);
-    } else if (sub_x && j == 0) {
-      const int old = sample(k - 1, 16);
-      g = clampi(rnd2z(old * 23 + g * 22, 5), gmin, gmax);
+  const short* cur = block_row(k) + j0;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) n[q] = cur[q];
+  if (overlap && k > 0 && j0 == 0) {
+    const short* prev = block_row(k - 1);
+    if (!sub_x) {
+      n[0] = clampi(rnd2z((int)prev[32] * 27 + n[0] * 17, 5), gmin, gmax);
+      n[1] = clampi(rnd2z((int)prev[33] * 17 + n[1] * 27, 5), gmin, gmax);
+    } else {
+      n[0] = clampi(rnd2z((int)prev[16] * 23 + n[0] * 22, 5), gmin, gmax);
     }
   }
-  return g;
 }
 
 /* Film grain blend, out of place: `src` is the decoded picture (luma read
- * before any grain), `dst` gets the output picture. One thread per sample. */
+ * before any grain), `dst` gets the output picture. One thread per four
+ * samples of a row (8-byte loads and stores; a chroma group reads its luma as
+ * one 8- or 16-byte load); the arithmetic per sample is that of
+ * 7.18.3.5 (the no-allocation entry point's grain_sample is the same per
+ * sample). Grid rows are the luma rows, then the chroma rows
+ * with plane 1's groups and plane 2's side by side, so a chroma row of
+ * 4:2:0 fills a grid row as a luma row does. */
 __global__ void k_grain_blend(const px_t* __restrict__ src, px_t* dst,
                               const __grid_constant__ Layout L,
                               const GrainState* gs, const uint16_t* orbit, const uint16_t* pos) {
-  const int p = blockIdx.z;
+  int gi = blockIdx.x * blockDim.x + threadIdx.x;
+  int y = blockIdx.y, p = 0;
+  if (y >= L.p[0].out_h) {
+    y -= L.p[0].out_h;
+    const int g1 = (L.p[1].out_w + 3) >> 2;
+    p = 1;
+    if (gi >= g1) {
+      gi -= g1;
+      p = 2;
+    }
+  }
   const PlaneGeom& g = L.p[p];
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y;
-  if (x >= g.out_w || y >= g.out_h) return;
-  const int idx = g.off + y * g.stride + x;
-  const int orig = src[idx];
+  const int x0 = gi * 4;
+  if (x0 >= g.out_w || y >= g.out_h) return;
+  const int idx = g.off + y * g.stride + x0;
+  const bool vec = ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15) == 0;
+  const int nq = min(4, g.out_w - x0);
+  int orig[4];
+  if (vec) {
+    const uint2 v = *reinterpret_cast<const uint2*>(src + idx);
+    orig[0] = v.x & 0xffff;
+    orig[1] = v.x >> 16;
+    orig[2] = v.y & 0xffff;
+    orig[3] = v.y >> 16;
+  } else {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) orig[q] = q < nq ? src[idx + q] : 0;
+  }
   const int bd = gs->bitdepth;
-  int out = orig;
-  bool active;
-  if (p == 0) active = gs->num_points[0] > 0;
-  else active = gs->chroma_from_luma || gs->num_points[p] > 0;
+  int out[4] = {orig[0], orig[1], orig[2], orig[3]};
+  const bool active = p == 0 ? gs->num_points[0] > 0 : (gs->chroma_from_luma || gs->num_points[p] > 0);
   if (active) {
     const int sub_x = p ? L.ss_x : 0, sub_y = p ? L.ss_y : 0;
     const int gmin = -(128 << (bd - 8)), gmax = (256 << (bd - 8)) - 1 - (128 << (bd - 8));
     const short* grain = p == 0 ? gs->luma : (p == 1 ? gs->cb : gs->cr);
     const int src_w = p == 0 ? 82 : gs->chroma_w;
+    const bool overlap = gs->overlap != 0;
     /* vertical half: stripes of 32 (16) rows, blended with the stripe above */
     const int sh = 5 - sub_y;
     const int s = y >> sh, row = y - (s << sh);
-    int n = grain_stripe(gs, grain, src_w, sub_x, sub_y, s, row, x, orbit, pos, gmin, gmax);
-    if (gs->overlap && s > 0) {
+    int n[4];
+    grain_stripe4(gs, grain, src_w, sub_x, sub_y, s, row, x0, orbit, pos, gmin, gmax, overlap, n);
+    if (overlap && s > 0) {
       if (!sub_y && row < 2) {
-        const int old = grain_stripe(gs, grain, src_w, sub_x, sub_y, s - 1, row + 32, x, orbit, pos,
-                                     gmin, gmax);
-        n = clampi(rnd2z(row == 0 ? old * 27 + n * 17 : old * 17 + n * 27, 5), gmin, gmax);
+        int old[4];
+        grain_stripe4(gs, grain, src_w, sub_x, sub_y, s - 1, row + 32, x0, orbit, pos, gmin, gmax,
+                      overlap, old);
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          n[q] = clampi(rnd2z(row == 0 ? old[q] * 27 + n[q] * 17 : old[q] * 17 + n[q] * 27, 5), gmin,
+                        gmax);
       } else if (sub_y && row == 0) {
-        const int old = grain_stripe(gs, grain, src_w, sub_x, sub_y, s - 1, 16, x, orbit, pos, gmin,
-                                     gmax);
-        n = clampi(rnd2z(old * 23 + n * 22, 5), gmin, gmax);
+        int old[4];
+        grain_stripe4(gs, grain, src_w, sub_x, sub_y, s - 1, 16, x0, orbit, pos, gmin, gmax, overlap,
+                      old);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) n[q] = clampi(rnd2z(old[q] * 23 + n[q] * 22, 5), gmin, gmax);
       }
     }
-    int index;
+    int index[4];
     if (p == 0) {
-      index = orig;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) index[q] = orig[q];
     } else {
+      /* the co-located luma sample and its right neighbour (clamped to the
+       * luma width), before grain */
       const PlaneGeom& gl = L.p[0];
-      const int ly = y << L.ss_y, lx = x << L.ss_x;
-      const int nx = lx + 1 < gl.out_w ? lx + 1 : gl.out_w - 1;
-      const int l0 = src[gl.off + ly * gl.stride + lx];
-      int avg = l0;
-      if (L.ss_x) avg = rnd2z(l0 + src[gl.off + ly * gl.stride + nx], 1);
-      if (gs->chroma_from_luma) {
-        index = avg;
+      const int ly = y << L.ss_y, lx0 = x0 << L.ss_x;
+      const px_t* lrow = src + gl.off + ly * gl.stride;
+      int lum[8];
+      if (vec && L.ss_x) {
+        const uint4 v = *reinterpret_cast<const uint4*>(lrow + lx0);
+        lum[0] = v.x & 0xffff;
+        lum[1] = v.x >> 16;
+        lum[2] = v.y & 0xffff;
+        lum[3] = v.y >> 16;
+        lum[4] = v.z & 0xffff;
+        lum[5] = v.z >> 16;
+        lum[6] = v.w & 0xffff;
+        lum[7] = v.w >> 16;
+      } else if (vec) {
+        const uint2 v = *reinterpret_cast<const uint2*>(lrow + lx0);
+        lum[0] = v.x & 0xffff;
+        lum[1] = v.x >> 16;
+        lum[2] = v.y & 0xffff;
+        lum[3] = v.y >> 16;
+        lum[4] = lum[5] = lum[6] = lum[7] = 0;
       } else {
-        const int comb = avg * (gs->luma_mult[p] - 128) + orig * (gs->mult[p] - 128);
-        index = clampi((comb >> 6) + (gs->offset[p] - 256) * (1 << (bd - 8)), 0, (1 << bd) - 1);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) lum[q] = (L.ss_x || q < 4) ? lrow[min(lx0 + q, gl.out_w - 1)] : 0;
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        int avg;
+        if (L.ss_x) {
+          const int lx = lx0 + 2 * q;
+          const int l0 = lum[2 * q];
+          const int l1 = lx + 1 < gl.out_w ? lum[2 * q + 1] : l0;
+          avg = rnd2z(l0 + l1, 1);
+        } else {
+          avg = lum[q];
+        }
+        if (gs->chroma_from_luma) {
+          index[q] = avg;
+        } else {
+          const int comb = avg * (gs->luma_mult[p] - 128) + orig[q] * (gs->mult[p] - 128);
+          index[q] = clampi((comb >> 6) + (gs->offset[p] - 256) * (1 << (bd - 8)), 0, (1 << bd) - 1);
+        }
       }
     }
-    const int scaled = rnd2z(grain_scale_lut(gs->lut[p], index, bd) * n, gs->scaling_shift);
-    out = clampi(orig + scaled, gs->min_value, p == 0 ? gs->max_luma : gs->max_chroma);
+    const int hi = p == 0 ? gs->max_luma : gs->max_chroma;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int scaled = rnd2z(grain_scale_lut(gs->lut[p], index[q], bd) * n[q], gs->scaling_shift);
+      out[q] = clampi(orig[q] + scaled, gs->min_value, hi);
+    }
   }
-  dst[idx] = (px_t)out;
+  if (vec && nq == 4) {
+    uint2 v;
+    v.x = (unsigned)out[0] | ((unsigned)out[1] << 16);
+    v.y = (unsigned)out[2] | ((unsigned)out[3] << 16);
+    *reinterpret_cast<uint2*>(dst + idx) = v;
+  } else {
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      if (q < nq) dst[idx + q] = (px_t)out[q];
+  }
 }
 
 /* ---- output packing ---------------------------------------------------------------------------- */
@@ -1609,9 +1739,11 @@ cudaError_t launch_upscale(const px_t* src, px_t* dst, const Layout& L, int maxv
                            cudaStream_t s) {
   UpscaleArgs u;
   for (int p = 0; p < 3; ++p) superres_params(L.p[p].coded_w, L.p[p].out_w, &u.step[p], &u.initial[p]);
-  const int rows = border_rows ? 4 * ((L.p[0].out_h + 8) / 64 + 1) : L.p[0].out_h;
-  k_upscale<<<dim3(cdiv(cdiv(L.p[0].out_w, 4), 64), rows, 3), 64, 0, s>>>(src, dst, L, u, maxv,
-                                                                         border_rows ? 1 : 0);
+  /* grid rows: the luma rows, then the chroma rows (planes 1 and 2 side by side) */
+  const int rows0 = border_rows ? 4 * ((L.p[0].out_h + 8) / 64 + 1) : L.p[0].out_h;
+  const int rows1 = L.p[1].out_h > 0 ? (border_rows ? rows0 : L.p[1].out_h) : 0;
+  const int segs = maxi(cdiv(L.p[0].out_w, AV1B_UP_OUT), 2 * cdiv(L.p[1].out_w, AV1B_UP_OUT));
+  k_upscale<<<dim3(segs, rows0 + rows1), 64, 0, s>>>(src, dst, L, u, maxv, border_rows ? 1 : 0, rows0);
   return cudaGetLastError();
 }
 
@@ -1631,8 +1763,10 @@ cudaError_t launch_grain_template(GrainState* gs, const GrainParamsDev& prm, con
 
 cudaError_t launch_grain_blend(const px_t* src, px_t* dst, const Layout& L, const GrainState* gs,
                                const uint16_t* orbit, const uint16_t* pos, cudaStream_t s) {
-  k_grain_blend<<<dim3(cdiv(L.p[0].out_w, 128), L.p[0].out_h, 3), 128, 0, s>>>(src, dst, L, gs,
-                                                                                 orbit, pos);
+  /* grid rows: the luma rows, then the chroma rows (planes 1 and 2 side by side) */
+  const int groups = maxi(cdiv(L.p[0].out_w, 4), 2 * cdiv(L.p[1].out_w, 4));
+  const int rows = L.p[0].out_h + L.p[1].out_h;
+  k_grain_blend<<<dim3(cdiv(groups, 128), rows), 128, 0, s>>>(src, dst, L, gs, orbit, pos);
   return cudaGetLastError();
 }
 

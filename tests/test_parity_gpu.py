@@ -71,6 +71,7 @@ def stage_cases(av1b):
         'loop_restoration': ((240, 136, 0, 10, 64, A.TOOLS_ALL & ~A.TOOL_GRAIN, 30), 3),
         'film_grain': ((240, 136, 0, 10, 64, A.TOOLS_ALL, 30), 3),
         'superres_128sb': ((480, 270, 360, 10, 128, A.TOOLS_ALL, 30), 3),
+        'odd_superres_grain': ((150, 90, 112, 10, 64, A.TOOLS_ALL, 30), 2),
         'interintra_intrabc_residual': ((240, 136, 0, 10, 64, A.TOOLS_ALL | A.TOOL_INTERINTRA |
                                          A.TOOL_INTRABC | A.TOOL_RESIDUAL, 30), 4),
         'lossless': ((160, 96, 0, 8, 64, A.TOOL_LOSSLESS, 0), 2),
@@ -82,7 +83,7 @@ def stage_cases(av1b):
 
 CASES = ['intra_itx_8bit', 'inter_8bit', 'deblock_8bit', 'config1_small', 'odd_size',
          'intra_tools_10bit', 'inter_tools_10bit', 'all_no_lr_grain', 'loop_restoration',
-         'film_grain', 'superres_128sb', 'interintra_intrabc_residual', 'lossless', 'bitdepth_12',
+         'film_grain', 'superres_128sb', 'odd_superres_grain', 'interintra_intrabc_residual', 'lossless', 'bitdepth_12',
          'tiny_16x16', 'key_interval_2']
 
 
