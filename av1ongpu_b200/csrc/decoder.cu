@@ -1054,13 +1054,16 @@ int plan_units(av1b_decoder* d, const PlanCtx& c, Plan* P) {
   critv.resize(nu);
   int max_depth = 0;
   for (size_t u = 0; u < nu; ++u) {
-    int cr = -1;
+    /* (depth, unit) of the deepest dependency, the latest of equally deep
+     * ones, as one 64-bit key: the maximum, without branches */
+    uint64_t key = 0;
     for (size_t j = first[u]; j < first[u + 1]; ++j) {
       const int o = udeps[j];
-      if (cr < 0 || ud[o] > ud[cr] || (ud[o] == ud[cr] && o > cr)) cr = o;
+      key = std::max(key, (static_cast<uint64_t>(ud[o]) << 32) | static_cast<uint32_t>(o + 1));
     }
+    const int cr = static_cast<int>(static_cast<uint32_t>(key)) - 1;
     critv[u] = cr;
-    ud[u] = (cr >= 0 ? ud[cr] : 0) + 1;
+    ud[u] = static_cast<int>(key >> 32) + 1;
     max_depth = std::max(max_depth, ud[u]);
   }
   std::vector<int>& height = S.height;
