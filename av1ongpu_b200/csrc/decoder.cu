@@ -774,7 +774,8 @@ struct PlanScratch {
   std::vector<int> owner[3];
   std::vector<std::vector<int>> unit_deps;
   std::vector<int> dep_count;
-  std::vector<int> chain_of, chain_tail, chain_len, height, crit, best;
+  std::vector<int> chain_id, chain_len, height, crit, best;
+  std::vector<uint64_t> head_key;
   std::vector<int> units_coding, ui_of, udepth, udeps;
   std::vector<uint8_t> is_b;
   std::vector<uint16_t> itx_key;
@@ -1082,38 +1083,38 @@ int plan_units(av1b_decoder* d, const PlanCtx& c, Plan* P) {
       if (bu < 0 || height[u] > height[bu] || (height[u] == height[bu] && ud[u] <= ud[bu])) best[cr] = u;
     }
   }
-  std::vector<int>& head = S.chain_of;  /* the first block of each block's chain */
-  head.resize(nu);
+  /* each block's chain, as the (depth, unit) key of its first block */
+  std::vector<uint64_t>& hk = S.head_key;
+  hk.resize(nu);
   std::vector<int> count(max_depth + 2, 0);
   for (size_t u = 0; u < nu; ++u) {
     const int cr = critv[u];
-    int h = static_cast<int>(u);
+    const uint64_t own = (static_cast<uint64_t>(ud[u]) << 32) | static_cast<uint32_t>(u);
+    uint64_t h = own;
     if (cr >= 0 && best[cr] == static_cast<int>(u)) {
-      const int hc = head[cr];
+      const uint64_t hc = hk[cr];
       bool ok = true;
-      for (size_t j = first[u]; j < first[u + 1] && ok; ++j) {
-        const int hj = head[udeps[j]];
-        if (ud[hj] > ud[hc] || (ud[hj] == ud[hc] && hj > hc)) ok = false;
-      }
+      for (size_t j = first[u]; j < first[u + 1]; ++j) ok &= hk[udeps[j]] <= hc;
       if (ok) h = hc;
     }
-    head[u] = h;
-    if (h == static_cast<int>(u)) ++count[ud[u] + 1];
+    hk[u] = h;
+    if (h == own) ++count[ud[u] + 1];
   }
   for (int k = 0; k <= max_depth; ++k) count[k + 1] += count[k];
   const size_t nch = static_cast<size_t>(count[max_depth + 1]);
-  std::vector<int>& cid = S.chain_tail;  /* a chain's place, by its first block */
+  std::vector<int>& cid = S.chain_id;  /* each block's chain, in claim order */
   std::vector<int>& clen = S.chain_len;
   cid.resize(nu);
   clen.assign(nch + 1, 0);
   for (size_t u = 0; u < nu; ++u) {
-    if (head[u] == static_cast<int>(u)) cid[u] = count[ud[u]]++;
-    ++clen[cid[head[u]] + 1];
+    const int hu = static_cast<int>(static_cast<uint32_t>(hk[u]));
+    cid[u] = hu == static_cast<int>(u) ? count[ud[u]]++ : cid[hu];
+    ++clen[cid[u] + 1];
   }
   sized(P->R->chains, nch + 1);
   for (size_t k = 0; k < nch; ++k) clen[k + 1] += clen[k];
   for (size_t k = 0; k <= nch; ++k) P->R->chains[k] = clen[k];
-  for (size_t u = 0; u < nu; ++u) P->R->units[clen[cid[head[u]]]++] = U[u];
+  for (size_t u = 0; u < nu; ++u) P->R->units[clen[cid[u]]++] = U[u];
   P->n_chains = nch;
   P->unit_depth = max_depth;
   P->units_inter = false;
