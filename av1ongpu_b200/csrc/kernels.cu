@@ -1111,10 +1111,18 @@ __global__ void __launch_bounds__(256) k_lr_tile(const px_t* __restrict__ cdef,
   __shared__ int win[AV1B_LR_WR * AV1B_LR_WC];
   __shared__ int aux[2][2][AV1B_LR_AR * AV1B_LR_AC];  /* Wiener: aux[0][0] = intermediate */
   __shared__ short xbyx1[256];   /* a2 = ((z << 8) + z / 2) / (z + 1), by z */
-  const int p = blockIdx.z;
+  /* grid z: luma, then chroma with plane 1's tiles and plane 2's side by side */
+  int p = blockIdx.z, bx = blockIdx.x;
+  if (p > 0) {
+    const int t1 = (L.p[1].out_w + AV1B_LR_TW - 1) / AV1B_LR_TW;
+    if (bx >= t1) {
+      bx -= t1;
+      p = 2;
+    }
+  }
   const PlaneGeom& g = L.p[p];
   const int sub_y = p > 0 ? L.ss_y : 0;
-  const int x0 = blockIdx.x * AV1B_LR_TW;
+  const int x0 = bx * AV1B_LR_TW;
   if (x0 >= g.out_w) return;
   /* the stripe piece */
   const int stripe = blockIdx.y;
@@ -1750,8 +1758,8 @@ cudaError_t launch_upscale(const px_t* src, px_t* dst, const Layout& L, int maxv
 cudaError_t launch_lr(const px_t* cdef, const px_t* curr, px_t* dst, const Layout& L,
                       const LrArgs& r, int maxv, bool copy_rest, cudaStream_t s) {
   const int stripes = (L.p[0].out_h + 8 + 63) / 64;
-  k_lr_tile<<<dim3(cdiv(L.p[0].out_w, AV1B_LR_TW), stripes, 3), 256, 0, s>>>(cdef, curr, dst, L, r,
-                                                                            maxv, copy_rest ? 1 : 0);
+  const int tiles = maxi(cdiv(L.p[0].out_w, AV1B_LR_TW), 2 * cdiv(L.p[1].out_w, AV1B_LR_TW));
+  k_lr_tile<<<dim3(tiles, stripes, 2), 256, 0, s>>>(cdef, curr, dst, L, r, maxv, copy_rest ? 1 : 0);
   return cudaGetLastError();
 }
 

@@ -392,19 +392,22 @@ def run_ours(args):
                 e2e_dec.nv12_pack_release(hd)
 
     e2e_s = float('inf')
+    # the timed stream starts cold (its key frame's plan before the first
+    # decode) and runs at least the workload's 120 frames (4 GOPs)
+    e2e_steps = max(args.steps, 4)
     if not args.no_e2e:
         e2e_run(args.warmup)  # the planners' lists and plans reach their sizes
         barrier()
         t0 = time.perf_counter()
-        e2e_run(args.steps)
+        e2e_run(e2e_steps)
         torch.cuda.synchronize()
         e2e_s = time.perf_counter() - t0
     if dist is not None:
         t = torch.tensor([e2e_s], device='cuda:%d' % local)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    e2e = {'value': F * args.steps * world / e2e_s, 'unit': UNIT, 'h2d_bytes_per_step': h2d,
-           'd2h_bytes_per_step': geo['nv12'] * F}
+    e2e = {'value': F * e2e_steps * world / e2e_s, 'unit': UNIT, 'h2d_bytes_per_step': h2d,
+           'd2h_bytes_per_step': geo['nv12'] * F, 'frames_timed': F * e2e_steps}
 
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
