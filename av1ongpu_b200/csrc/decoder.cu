@@ -92,6 +92,16 @@ struct av1b_decoder {
   /* freed plans kept with their buffers for the next av1b_plan_frame */
   std::mutex plan_pool_mu;
   std::vector<struct av1b_plan*> plan_pool;
+  /* The largest capacity any planner's record list (elements) and any plan's
+   * arena and filter buffer (bytes) has needed. A planner or plan that has
+   * not held so large a frame grows to it when it is next taken, so the
+   * growth - a page-locked allocation stalls every CUDA call of the process,
+   * a device free waits for the device - happens once, early in a stream
+   * (after its first key frame), not whenever a planner or plan first meets
+   * a key frame. Guarded by hw_mu. */
+  std::mutex hw_mu;
+  size_t list_hw[32] = {};
+  size_t arena_hw = 0, filt_hw = 0;
 
   /* geometry of the pictures currently allocated */
   bool have_geom = false;
@@ -378,6 +388,25 @@ struct PlanLists {
   pvec<LrUnitRec> lr_units[3];
   pvec<DqRec> dq;                 /* coded transforms to dequantise (levels frames) */
 };
+
+/* Calls f(index, list) for every list of R. */
+template <class F>
+void each_list(PlanLists& R, F&& f) {
+  int i = 0;
+  f(i++, R.blocks);
+  f(i++, R.txs);
+  f(i++, R.obmc);
+  f(i++, R.warps);
+  f(i++, R.palette_colors);
+  f(i++, R.units);
+  f(i++, R.chains);
+  f(i++, R.deps);
+  f(i++, R.inter_tiles);
+  f(i++, R.itx_jobs);
+  f(i++, R.itx_batches);
+  for (int p = 0; p < 3; ++p) f(i++, R.lr_units[p]);
+  f(i++, R.dq);
+}
 
 /* One planned frame's constants and record counts (its records live in
  * device memory, uploaded from the PlanLists). */
@@ -1705,6 +1734,33 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
   }
   Plan& P = pl->P;
   P.R = pn->lists;
+  {
+    /* grow to the largest frame planned so far (a failed growth is left to
+     * the planning that needs it, which reports it) */
+    size_t hw[32], arena_hw, filt_hw;
+    {
+      std::lock_guard<std::mutex> lk(d->hw_mu);
+      std::copy(d->list_hw, d->list_hw + 32, hw);
+      arena_hw = d->arena_hw;
+      filt_hw = d->filt_hw;
+    }
+    try {
+      each_list(*P.R, [&](int i, auto& v) {
+        if (v.capacity() < hw[i]) v.reserve(hw[i]);
+      });
+    } catch (const std::bad_alloc&) {
+    }
+    auto pre_grow = [&](DevBuf& b, size_t bytes) {
+      if (b.cap >= bytes) return;
+      {
+        std::lock_guard<std::mutex> lk(d->alloc_mu);
+        if (d->budget && d->allocated - b.cap + align_up(bytes + bytes / 8, 1 << 16) > d->budget) return;
+      }
+      dev_ensure(d, b, bytes);
+    };
+    pre_grow(pl->arena, arena_hw);
+    pre_grow(pl->filt, filt_hw);
+  }
   cudaStream_t st = pn->upload;
   /* the caller's coefficients and raw residuals go up first, while the
    * records are built */
@@ -1748,6 +1804,10 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
       cudaStreamSynchronize(st);
       return rc;
     }
+    {
+      std::lock_guard<std::mutex> lk(d->hw_mu);
+      d->filt_hw = std::max(d->filt_hw, fo);  /* the bytes needed, not the capacity: no runaway */
+    }
     uint8_t* fl = static_cast<uint8_t*>(pl->filt.p);
     if (nde)
       CK(cudaMemcpyAsync(fl + pl->o_de_raw, s.deblock, nde * sizeof(av1b_deblock_edge),
@@ -1782,6 +1842,10 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
   if (rc) {
     cudaStreamSynchronize(st);  /* nothing in flight reads the caller's arrays */
     return rc;
+  }
+  {
+    std::lock_guard<std::mutex> lk(d->hw_mu);
+    each_list(*P.R, [&](int i, auto& v) { d->list_hw[i] = std::max(d->list_hw[i], v.capacity()); });
   }
   host_mark(d, kStPlanHost, t0);
   P.n_blocks = P.R->blocks.size();
@@ -1831,6 +1895,10 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
   if ((rc = dev_ensure(d, pl->arena, total, total + total / 2))) {
     cudaStreamSynchronize(st);
     return rc;
+  }
+  {
+    std::lock_guard<std::mutex> lk(d->hw_mu);
+    d->arena_hw = std::max(d->arena_hw, total);
   }
   /* the record lists upload from where the planner wrote them (page-locked) */
   t0 = std::chrono::steady_clock::now();
