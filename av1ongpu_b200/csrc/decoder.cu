@@ -367,11 +367,12 @@ template <class T>
 using pvec = std::vector<T, PinnedAlloc<T>>;
 
 /* The record lists a plan builds, in page-locked host memory so they upload
- * from where the planner wrote them. One set serves every plan of a decoder:
- * planning is serialized and a plan's uploads finish before the next starts,
- * so the lists are free again once plan_frame returns (and their capacity,
- * grown to the largest frame, is kept - no page-locked allocation, which
- * stalls every CUDA call of the process, in the steady state). */
+ * from where the planner wrote them. One set per planner: a planner plans one
+ * frame at a time and a plan's uploads finish before plan_frame returns, so
+ * its lists are free again then. Their capacity is kept, and grown to the
+ * largest any planner has needed when the planner is next taken - no
+ * page-locked allocation, which stalls every CUDA call of the process, in the
+ * steady state. */
 struct PlanLists {
   pvec<BlockRec> blocks;
   pvec<TxRec> txs;
