@@ -505,8 +505,11 @@ struct BlockOut {
   std::vector<int2> itx_jobs;
   std::vector<DqRec> dq;
   size_t pre_res_pool = 0, coef_end = 0, res_end = 0;
+  uint8_t* is_b = nullptr;        /* the frame's phase B flags, by block */
+  uint8_t unaligned[3] = {0, 0, 0};  /* a block of the plane off its owner-cell grid */
   PlanErr err;
   void clear() {
+    unaligned[0] = unaligned[1] = unaligned[2] = 0;
     txs.clear();
     dq.clear();
     obmc.clear();
@@ -794,6 +797,11 @@ int plan_block(const PlanCtx& ctx, const av1b_frame_syntax& s, size_t bi, BlockR
       for (int x0 = 0; x0 < b.w; x0 += 16)
         tiles.push_back(make_int2(static_cast<int>(bi), x0 | (y0 << 16)));
   }
+  /* for the dependency schedule: owner cells are 4 samples, 2 in a chroma
+   * plane whose axis is subsampled (plane 1 keyed on ss_x, plane 2 on ss_y) */
+  const int cell = b.plane == 0 ? 2 : ((b.plane == 1 ? L.ss_x : L.ss_y) ? 1 : 2);
+  if ((b.x | b.y | b.w | b.h) & ((1 << cell) - 1)) O->unaligned[b.plane] = 1;
+  O->is_b[bi] = r.phase_b;
   return AV1B_OK;
 }
 
@@ -808,6 +816,7 @@ struct PlanScratch {
   std::vector<uint64_t> head_key;
   std::vector<int> units_coding, ui_of, udepth, udeps;
   std::vector<uint8_t> is_b;
+  bool aligned[3] = {true, true, true};  /* every block of the plane on its owner-cell grid */
   std::vector<uint16_t> itx_key;
   std::vector<int> itx_hist;
   std::vector<int2> itx_unsorted;  /* the blocks' transform jobs, before plan_itx sorts them */
@@ -862,24 +871,8 @@ int plan_units(av1b_decoder* d, const PlanCtx& c, Plan* P) {
   /* owner grids: later blocks overwrite earlier ones where cells overlap, so
    * a plane whose blocks are not all cell aligned is filled in order */
   const size_t nb = P->R->blocks.size();
-  std::vector<uint8_t>& is_b = S.is_b;
-  is_b.resize(nb);
-  bool aligned[3] = {true, true, true};
-  {
-    const int pieces = pieces_for(nb, c, 4096);
-    std::vector<uint8_t> unaligned(static_cast<size_t>(pieces) * 3, 0);
-    c.pool->run(pieces, [&](int i) {
-      uint8_t* u = &unaligned[static_cast<size_t>(i) * 3];
-      for (size_t bi = piece_begin(nb, pieces, i); bi < piece_begin(nb, pieces, i + 1); ++bi) {
-        const BlockRec& b = P->R->blocks[bi];
-        const int m = (1 << sh[b.plane]) - 1;
-        if ((b.x | b.y | b.w | b.h) & m) u[b.plane] = 1;
-        is_b[bi] = b.phase_b;
-      }
-    });
-    for (size_t k = 0; k < unaligned.size(); ++k)
-      if (unaligned[k]) aligned[k % 3] = false;
-  }
+  const std::vector<uint8_t>& is_b = S.is_b;  /* filled with the block records */
+  const bool* aligned = S.aligned;
   auto fill = [&](size_t bi) {
     const BlockRec& b = P->R->blocks[bi];
     const int p = b.plane, oc = 1 << sh[p];
@@ -1342,14 +1335,21 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
     const int pieces = pieces_for(nb, c, 512);
     std::vector<BlockOut>& outs = c.scratch->blocks;
     if (outs.size() < static_cast<size_t>(pieces)) outs.resize(pieces);
+    c.scratch->is_b.resize(nb);
     c.pool->run(pieces, [&](int i) {
       BlockOut* O = &outs[i];
       O->clear();
+      O->is_b = c.scratch->is_b.data();
       for (size_t bi = piece_begin(nb, pieces, i); bi < piece_begin(nb, pieces, i + 1); ++bi)
         if (plan_block(c, s, bi, P->R->blocks[bi], O)) break;
     });
     for (int i = 0; i < pieces; ++i)
       if (outs[i].err.code) return fail(d, outs[i].err.code, outs[i].err.msg);
+    for (int p = 0; p < 3; ++p) {
+      c.scratch->aligned[p] = true;
+      for (int i = 0; i < pieces; ++i)
+        if (outs[i].unaligned[p]) c.scratch->aligned[p] = false;
+    }
     /* piece offsets into the frame's lists */
     std::vector<size_t> o_tx(pieces + 1, 0), o_obmc(pieces + 1, 0), o_warp(pieces + 1, 0),
         o_pal(pieces + 1, 0), o_unit(pieces + 1, 0), o_tile(pieces + 1, 0), o_tilef(pieces + 1, 0),
