@@ -811,7 +811,7 @@ struct PlanScratch {
   std::vector<BlockOut> blocks;
   std::vector<int> owner[3];
   std::vector<std::vector<int>> unit_deps;
-  std::vector<int> dep_count;
+  std::vector<int> dep_count, dep_first;
   std::vector<int> chain_id, chain_len, height, crit, best;
   std::vector<uint64_t> head_key;
   std::vector<int> units_coding, ui_of, udepth, udeps;
@@ -1035,9 +1035,15 @@ int plan_units(av1b_decoder* d, const PlanCtx& c, Plan* P) {
   });
   /* the lists back to back for the device (block indices), and as unit
    * indices for the passes below */
-  std::vector<size_t> first(nu + 1, 0);
+  {
+    size_t total = 0;
+    for (size_t ui = 0; ui < nu; ++ui) total += static_cast<size_t>(dep_count[ui]);
+    if (total > static_cast<size_t>(INT32_MAX)) return fail(d, AV1B_ERR_SYNTAX, "frame too large");
+  }
+  std::vector<int>& first = S.dep_first;  /* where each unit's list starts, and the end */
+  first.resize(nu + 1);
+  first[0] = 0;
   for (size_t ui = 0; ui < nu; ++ui) first[ui + 1] = first[ui] + dep_count[ui];
-  if (first[nu] > static_cast<size_t>(INT32_MAX)) return fail(d, AV1B_ERR_SYNTAX, "frame too large");
   sized(P->R->deps, first[nu]);
   std::vector<int>& udeps = S.udeps;
   udeps.resize(first[nu]);
