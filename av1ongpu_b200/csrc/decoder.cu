@@ -506,6 +506,10 @@ struct BlockOut {
   std::vector<DqRec> dq;
   size_t pre_res_pool = 0, coef_end = 0, res_end = 0;
   uint8_t* is_b = nullptr;        /* the frame's phase B flags, by block */
+  /* the owner-cell grids (cells of 1 << cell[p] samples, owner_w x owner_h),
+   * filled as the blocks convert */
+  int* owner[3] = {nullptr, nullptr, nullptr};
+  int owner_w[3] = {0, 0, 0}, owner_h[3] = {0, 0, 0}, cell[3] = {2, 2, 2};
   uint8_t unaligned[3] = {0, 0, 0};  /* a block of the plane off its owner-cell grid */
   PlanErr err;
   void clear() {
@@ -799,9 +803,19 @@ int plan_block(const PlanCtx& ctx, const av1b_frame_syntax& s, size_t bi, BlockR
   }
   /* for the dependency schedule: owner cells are 4 samples, 2 in a chroma
    * plane whose axis is subsampled (plane 1 keyed on ss_x, plane 2 on ss_y) */
-  const int cell = b.plane == 0 ? 2 : ((b.plane == 1 ? L.ss_x : L.ss_y) ? 1 : 2);
-  if ((b.x | b.y | b.w | b.h) & ((1 << cell) - 1)) O->unaligned[b.plane] = 1;
+  const int p = b.plane, cs = O->cell[p], oc = 1 << cs;
+  if ((b.x | b.y | b.w | b.h) & (oc - 1)) O->unaligned[p] = 1;
   O->is_b[bi] = r.phase_b;
+  /* the block's owner cells (a plane whose blocks are not all on the cell
+   * grid is filled again in coding order once every block is converted) */
+  const int cx0 = b.x >> cs, cy0 = b.y >> cs;
+  const int cx1 = std::min((b.x + b.w + oc - 1) >> cs, O->owner_w[p]);
+  const int cy1 = std::min((b.y + b.h + oc - 1) >> cs, O->owner_h[p]);
+  int* o = O->owner[p];
+  if (cx0 < cx1)  /* a block right of the grid (in the border) owns no cell */
+    for (int y = cy0; y < cy1; ++y)
+      std::fill(o + static_cast<size_t>(y) * O->owner_w[p] + cx0, o + static_cast<size_t>(y) * O->owner_w[p] + cx1,
+              static_cast<int>(bi));
   return AV1B_OK;
 }
 
@@ -816,7 +830,6 @@ struct PlanScratch {
   std::vector<uint64_t> head_key;
   std::vector<int> units_coding, ui_of, udepth, udeps;
   std::vector<uint8_t> is_b;
-  bool aligned[3] = {true, true, true};  /* every block of the plane on its owner-cell grid */
   std::vector<uint16_t> itx_key;
   std::vector<int> itx_hist;
   std::vector<int2> itx_unsorted;  /* the blocks' transform jobs, before plan_itx sorts them */
@@ -862,37 +875,10 @@ int plan_units(av1b_decoder* d, const PlanCtx& c, Plan* P) {
     sh[p] = p == 0 ? 2 : (p == 1 ? (L.ss_x ? 1 : 2) : (L.ss_y ? 1 : 2));
     cw[p] = (L.p[p].grid_w + (1 << sh[p]) - 1) >> sh[p];
     ch[p] = (L.p[p].grid_h + (1 << sh[p]) - 1) >> sh[p];
-    S.owner[p].resize(static_cast<size_t>(cw[p]) * ch[p]);
   }
-  c.pool->run(3 * 8, [&](int i) {
-    std::vector<int>& o = S.owner[i / 8];
-    std::fill(o.begin() + piece_begin(o.size(), 8, i % 8), o.begin() + piece_begin(o.size(), 8, i % 8 + 1), -1);
-  });
-  /* owner grids: later blocks overwrite earlier ones where cells overlap, so
-   * a plane whose blocks are not all cell aligned is filled in order */
+  /* the owner grids were filled as the blocks converted (build_plan) */
   const size_t nb = P->R->blocks.size();
-  const std::vector<uint8_t>& is_b = S.is_b;  /* filled with the block records */
-  const bool* aligned = S.aligned;
-  auto fill = [&](size_t bi) {
-    const BlockRec& b = P->R->blocks[bi];
-    const int p = b.plane, oc = 1 << sh[p];
-    const int cx0 = std::max<int>(b.x, 0) >> sh[p], cy0 = std::max<int>(b.y, 0) >> sh[p];
-    const int cx1 = std::min((b.x + b.w + oc - 1) >> sh[p], cw[p]);
-    const int cy1 = std::min((b.y + b.h + oc - 1) >> sh[p], ch[p]);
-    const int w = cw[p], v = static_cast<int>(bi);
-    int* o = S.owner[p].data();
-    for (int y = cy0; y < cy1; ++y) std::fill(o + static_cast<size_t>(y) * w + cx0, o + static_cast<size_t>(y) * w + cx1, v);
-  };
-  {
-    const int pieces = pieces_for(nb, c, 2048);
-    c.pool->run(pieces, [&](int i) {
-      for (size_t bi = piece_begin(nb, pieces, i); bi < piece_begin(nb, pieces, i + 1); ++bi)
-        if (aligned[P->R->blocks[bi].plane]) fill(bi);
-    });
-    if (!aligned[0] || !aligned[1] || !aligned[2])
-      for (size_t bi = 0; bi < nb; ++bi)
-        if (!aligned[P->R->blocks[bi].plane]) fill(bi);
-  }
+  const std::vector<uint8_t>& is_b = S.is_b;
   /* the cells of [x0, x1] x [y0, y1] inside the plane's grid, row by row
    * from the cell holding (x0, y0) (the device's wait_rect / decoded_before
    * walk): `f(owner)` for each cell whose owner differs from the one of the
@@ -1341,20 +1327,59 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
     const int pieces = pieces_for(nb, c, 512);
     std::vector<BlockOut>& outs = c.scratch->blocks;
     if (outs.size() < static_cast<size_t>(pieces)) outs.resize(pieces);
-    c.scratch->is_b.resize(nb);
+    /* the dependency schedule's owner-cell grids (plan_units): square cells
+     * of 4 luma samples, 2 in a chroma plane whose axis is subsampled (plane
+     * 1 keyed on ss_x, plane 2 on ss_y: engine.cpp:737-741), cleared here and
+     * filled as the blocks convert */
+    PlanScratch& S = *c.scratch;
+    int cell[3], ow[3], oh[3];
+    for (int p = 0; p < 3; ++p) {
+      cell[p] = p == 0 ? 2 : ((p == 1 ? L.ss_x : L.ss_y) ? 1 : 2);
+      ow[p] = (L.p[p].grid_w + (1 << cell[p]) - 1) >> cell[p];
+      oh[p] = (L.p[p].grid_h + (1 << cell[p]) - 1) >> cell[p];
+      S.owner[p].resize(static_cast<size_t>(ow[p]) * oh[p]);
+    }
+    c.pool->run(3 * 8, [&](int i) {
+      std::vector<int>& o = S.owner[i / 8];
+      std::fill(o.begin() + piece_begin(o.size(), 8, i % 8), o.begin() + piece_begin(o.size(), 8, i % 8 + 1), -1);
+    });
+    S.is_b.resize(nb);
     c.pool->run(pieces, [&](int i) {
       BlockOut* O = &outs[i];
       O->clear();
-      O->is_b = c.scratch->is_b.data();
+      O->is_b = S.is_b.data();
+      for (int p = 0; p < 3; ++p) {
+        O->owner[p] = S.owner[p].data();
+        O->owner_w[p] = ow[p];
+        O->owner_h[p] = oh[p];
+        O->cell[p] = cell[p];
+      }
       for (size_t bi = piece_begin(nb, pieces, i); bi < piece_begin(nb, pieces, i + 1); ++bi)
         if (plan_block(c, s, bi, P->R->blocks[bi], O)) break;
     });
     for (int i = 0; i < pieces; ++i)
       if (outs[i].err.code) return fail(d, outs[i].err.code, outs[i].err.msg);
+    /* later blocks overwrite earlier ones where cells overlap: a plane whose
+     * blocks are not all on the cell grid is filled again, in coding order */
     for (int p = 0; p < 3; ++p) {
-      c.scratch->aligned[p] = true;
+      bool aligned = true;
       for (int i = 0; i < pieces; ++i)
-        if (outs[i].unaligned[p]) c.scratch->aligned[p] = false;
+        if (outs[i].unaligned[p]) aligned = false;
+      if (aligned) continue;
+      std::fill(S.owner[p].begin(), S.owner[p].end(), -1);
+      const int oc = 1 << cell[p];
+      int* o = S.owner[p].data();
+      for (size_t bi = 0; bi < nb; ++bi) {
+        const BlockRec& b = P->R->blocks[bi];
+        if (b.plane != p) continue;
+        const int cx0 = b.x >> cell[p], cy0 = b.y >> cell[p];
+        const int cx1 = std::min((b.x + b.w + oc - 1) >> cell[p], ow[p]);
+        const int cy1 = std::min((b.y + b.h + oc - 1) >> cell[p], oh[p]);
+        if (cx0 < cx1)
+          for (int y = cy0; y < cy1; ++y)
+            std::fill(o + static_cast<size_t>(y) * ow[p] + cx0, o + static_cast<size_t>(y) * ow[p] + cx1,
+                      static_cast<int>(bi));
+      }
     }
     /* piece offsets into the frame's lists */
     std::vector<size_t> o_tx(pieces + 1, 0), o_obmc(pieces + 1, 0), o_warp(pieces + 1, 0),
