@@ -806,8 +806,14 @@ int plan_block(const PlanCtx& ctx, const av1b_frame_syntax& s, size_t bi, BlockR
   const int p = b.plane, cs = O->cell[p], oc = 1 << cs;
   if ((b.x | b.y | b.w | b.h) & (oc - 1)) O->unaligned[p] = 1;
   O->is_b[bi] = r.phase_b;
-  /* the block's owner cells (a plane whose blocks are not all on the cell
-   * grid is filled again in coding order once every block is converted) */
+  /* the block's owner cells. A plane whose blocks are not all on the cell
+   * grid is filled again, serially and in coding order, once every block is
+   * converted; this piece stops filling it as soon as it meets such a block.
+   * Blocks of other pieces may still write cells such a block shares at the
+   * same moment (the only cells two threads write at once: blocks of valid
+   * syntax on the grid do not overlap), and the serial pass overwrites all of
+   * them before anything reads the grid. */
+  if (O->unaligned[p]) return AV1B_OK;
   const int cx0 = b.x >> cs, cy0 = b.y >> cs;
   const int cx1 = std::min((b.x + b.w + oc - 1) >> cs, O->owner_w[p]);
   const int cy1 = std::min((b.y + b.h + oc - 1) >> cs, O->owner_h[p]);

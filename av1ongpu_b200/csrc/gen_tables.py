@@ -8,14 +8,16 @@ if every value matches. They are read out of the reference checkout's table
 sources (kernels/av1gpu_tables.h, src/core/tables.cpp) so that no value is
 retyped, and written here under this library's own names and layout.
 
-    python3 av1ongpu_b200/csrc/gen_tables.py /root/reference > av1ongpu_b200/csrc/av1b_tables.h
+    python3 av1ongpu_b200/csrc/gen_tables.py <reference checkout> > av1ongpu_b200/csrc/av1b_tables.h
 
 The output is committed; the build does not run this script.
 """
 import re
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else '/root/reference'
+if len(sys.argv) != 2:
+    raise SystemExit('usage: gen_tables.py <reference checkout>')
+REF = sys.argv[1]
 tables_h = open(REF + '/kernels/av1gpu_tables.h').read()
 tables_cpp = open(REF + '/src/core/tables.cpp').read()
 coef_h = open(REF + '/src/frontend/coef_tables.hpp').read()

@@ -29,6 +29,7 @@
  */
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <cstring>
 #include <mutex>
 
@@ -186,6 +187,16 @@ int device_scratch(unsigned char** out) {
   return AV1B_OK;
 }
 
+/* The bytes a plane of w x h samples at `stride` spans: [lo, hi). */
+struct Span {
+  uintptr_t lo, hi;
+};
+Span plane_span(const void* base, int stride, int w, int h) {
+  const uintptr_t lo = reinterpret_cast<uintptr_t>(base);
+  return Span{lo, lo + (static_cast<uintptr_t>(h - 1) * stride + w) * sizeof(uint16_t)};
+}
+bool overlap(const Span& a, const Span& b) { return a.lo < b.hi && b.lo < a.hi; }
+
 bool grain_params_ok(const av1b_film_grain& f) {
   if (f.seed < 0 || f.seed > 65535 || f.ar_coeff_lag < 0 || f.ar_coeff_lag > 3 ||
       f.num_y_points < 0 || f.num_y_points > 16 || f.num_cb_points < 0 || f.num_cb_points > 16 ||
@@ -228,7 +239,26 @@ extern "C" int av1b_apply_film_grain_noalloc(const av1b_frame_syntax* s, const u
     a.src_stride[p] = src_stride[p];
     a.dst_stride[p] = dst_stride[p];
   }
+  /* The blend of a chroma sample reads the co-located luma of the input
+   * while other blocks write the output: an output plane that shares bytes
+   * with any input plane (in-place grain) or with another output plane would
+   * make the result depend on the order the GPU runs the blocks in. */
+  for (int p = 0; p < 3; ++p) {
+    const Span d = plane_span(dst[p], dst_stride[p], a.w[p], a.h[p]);
+    for (int q = 0; q < 3; ++q) {
+      if (overlap(d, plane_span(src[q], src_stride[q], a.w[q], a.h[q]))) return AV1B_ERR_ARG;
+      if (q != p && overlap(d, plane_span(dst[q], dst_stride[q], a.w[q], a.h[q]))) return AV1B_ERR_ARG;
+    }
+  }
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  /* the scratch resolved below is the current device's: a stream of another
+   * device could not reach it */
+  if (st != nullptr) {
+    int cur = -1, sdev = -1;
+    if (cudaGetDevice(&cur) != cudaSuccess || cudaStreamGetDevice(st, &sdev) != cudaSuccess)
+      return AV1B_ERR_CUDA;
+    if (sdev != cur) return AV1B_ERR_ARG;
+  }
   if (!s->grain.apply) {
     /* no grain: the output picture is the input */
     for (int p = 0; p < 3; ++p)

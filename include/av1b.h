@@ -315,8 +315,13 @@ AV1B_API void* av1b_decoder_stream(av1b_decoder* dec);
  * start-up. It applies `syntax`'s film grain (syntax->grain, its size, bit
  * depth, subsampling and colour matrix; nothing else of the syntax is read) to
  * the picture in `src` and writes the output picture to `dst`: three device
- * planes each, strides in samples, queued on `stream` (a cudaStream_t, 0 for
- * the default stream). Without grain (apply == 0) it copies src to dst.
+ * planes each, strides in samples, queued on `stream` (a cudaStream_t of the
+ * current device, 0 for the default stream; a stream of another device is
+ * refused with AV1B_ERR_ARG). Without grain (apply == 0) it copies src to
+ * dst. The output planes must not share a byte with any input plane or with
+ * each other (AV1B_ERR_ARG): grain is not applied in place, because a chroma
+ * sample's grain reads the input luma that an in-place write would already
+ * have changed.
  *
  * It allocates nothing. Its scratch is a file-scope device array of
  * AV1B_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until
@@ -332,19 +337,7 @@ AV1B_API int av1b_apply_film_grain_noalloc(const av1b_frame_syntax* syntax,
                                            uint16_t* const dst[3], const int32_t dst_stride[3],
                                            void* stream);
 
-/* --- synthetic input -------------------------------------------------------
- * The seeded synthetic FrameSyntax the benchmarks and tests decode. `config`
- * selects a workload (1..3, see av1ongpu_b200/csrc/synth.cpp), `scale` divides
- * its picture size (1 = full size). The frame is returned serialized; its
- * reference_slots hold frame *distances* (1 = the previous frame), which the
- * caller rewrites into its own slot ids with av1b_blob_set_refs. The buffer is
- * owned by the library: release it with av1b_blob_free. */
-AV1B_API int av1b_synth_frame(int config, int scale, uint64_t seed, int frame_index,
-                     uint8_t** blob, size_t* len);
-AV1B_API int av1b_synth_frame_ex(int width, int height, int coded_width, int bit_depth, int sb_size,
-                        int tools, uint64_t seed, int frame_index, int key_interval,
-                        uint8_t** blob, size_t* len);
-AV1B_API void av1b_blob_free(uint8_t* blob);
+/* --- a serialized frame's reference slot list ----------------------------- */
 /* Rewrites the reference slot list of a serialized frame in place. */
 AV1B_API int av1b_blob_set_refs(uint8_t* blob, size_t len, const int32_t* slots, int n);
 /* Reads the reference slot list (distances for a synthetic frame). */
