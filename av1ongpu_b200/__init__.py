@@ -5,7 +5,8 @@ the reference library's av1gpu::Decoder (include/av1gpu/av1gpu.hpp:615-787 of
 trprkkk/AV1onGPU): decode / decode_reference with device-resident reference
 slots, release_reference, to_nv12, to_rgb and stats. Frames are passed as
 serialized FrameSyntax blobs (`Blob`), which the seeded workload generator
-(`synth_frame`) produces.
+(`synth_frame`, libav1synth.so, include/av1b_synth.h) produces. Importing the
+package loads neither library; each is loaded at its first use.
 
 There is no CPU path: without the compiled library, or without a CUDA device,
 the calls raise instead of computing anything elsewhere.
@@ -18,6 +19,7 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, 'libav1b.so')
+SYNTH_LIB_PATH = os.path.join(_HERE, 'libav1synth.so')
 
 AV1B_OK = 0
 ERRORS = {
@@ -104,18 +106,42 @@ _SIGNATURES = {
     'av1b_unit_trace': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
                                        ctypes.POINTER(ctypes.c_size_t)]),
     'av1b_decoder_stream': (ctypes.c_void_p, [ctypes.c_void_p]),
-    'av1b_synth_frame': (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_uint64, ctypes.c_int,
-                                        ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_size_t)]),
-    'av1b_synth_frame_ex': (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
-                                           ctypes.c_int, ctypes.c_int, ctypes.c_uint64, ctypes.c_int,
-                                           ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
-                                           ctypes.POINTER(ctypes.c_size_t)]),
-    'av1b_blob_free': (None, [ctypes.c_void_p]),
     'av1b_blob_set_refs': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t,
                                           ctypes.POINTER(ctypes.c_int32), ctypes.c_int]),
     'av1b_blob_get_refs': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t,
                                           ctypes.POINTER(ctypes.c_int32), ctypes.c_int]),
 }
+
+
+_SYNTH_SIGNATURES = {
+    'av1s_synth_frame': (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_uint64, ctypes.c_int,
+                                        ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_size_t)]),
+    'av1s_synth_frame_ex': (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                           ctypes.c_int, ctypes.c_int, ctypes.c_uint64, ctypes.c_int,
+                                           ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
+                                           ctypes.POINTER(ctypes.c_size_t)]),
+    'av1s_synth_frame_refs': (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                             ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint64,
+                                             ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
+                                             ctypes.POINTER(ctypes.c_size_t)]),
+    'av1s_blob_free': (None, [ctypes.c_void_p]),
+}
+_synth = None
+
+
+def synth_lib():
+    """Loads libav1synth.so, the workload generator (raises if it was not built)."""
+    global _synth
+    if _synth is None:
+        if not os.path.exists(SYNTH_LIB_PATH):
+            raise OSError('libav1synth.so is not built: run python -m av1ongpu_b200.build')
+        L = ctypes.CDLL(SYNTH_LIB_PATH)
+        for name, (res, args) in _SYNTH_SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _synth = L
+    return _synth
 
 
 def lib():
@@ -137,12 +163,19 @@ def exported_symbols():
     return list(_SIGNATURES)
 
 
+def synth_exported_symbols():
+    return list(_SYNTH_SIGNATURES)
+
+
 # ---- serialized frames -----------------------------------------------------------------------
 _BLOB_HEADER = 48  # magic, version, reserved, n_refs, ref_slots[8]
+_BLOB_MAGIC = 0x42315641  # "AV1B"
 
 
 class Blob:
-    """A serialized FrameSyntax, 64-byte aligned, owned by the library or by numpy."""
+    """A serialized FrameSyntax, 64-byte aligned, owned by the generator library
+    or by numpy. The header (geometry and the patchable reference slot list)
+    is read and written here directly, without either library."""
 
     def __init__(self, ptr, size, owned_by_lib):
         self.ptr = ptr
@@ -164,9 +197,17 @@ class Blob:
         return ctypes.string_at(self.ptr, self.size)
 
     def __del__(self):
-        if self._lib_owned and self.ptr and _lib is not None:
-            _lib.av1b_blob_free(ctypes.c_void_p(self.ptr))
+        if self._lib_owned and self.ptr and _synth is not None:
+            _synth.av1s_blob_free(ctypes.c_void_p(self.ptr))
             self.ptr = None
+
+    def _head(self):
+        if self.size < _BLOB_HEADER:
+            raise Av1bError(-1, 'malformed blob')
+        magic, _version, _r, n = struct.unpack_from('<4I', ctypes.string_at(self.ptr, 16))
+        if magic != _BLOB_MAGIC or n > 8:
+            raise Av1bError(-1, 'malformed blob')
+        return n
 
     @property
     def header(self):
@@ -174,35 +215,43 @@ class Blob:
         return struct.unpack_from('<6i', ctypes.string_at(self.ptr + _BLOB_HEADER, 24))
 
     def get_refs(self):
-        buf = (ctypes.c_int32 * 8)()
-        n = lib().av1b_blob_get_refs(self.ptr, self.size, buf, 8)
-        if n < 0:
-            raise Av1bError(n, 'malformed blob')
-        return list(buf[:n])
+        n = self._head()
+        return list(struct.unpack_from('<%di' % n, ctypes.string_at(self.ptr + 16, 4 * n)))
 
     def set_refs(self, slots):
-        buf = (ctypes.c_int32 * 8)(*slots)
-        rc = lib().av1b_blob_set_refs(self.ptr, self.size, buf, len(slots))
-        if rc:
-            raise Av1bError(rc, 'malformed blob')
+        self._head()
+        if len(slots) > 8:
+            raise Av1bError(-1, 'more than eight reference slots')
+        ctypes.memmove(self.ptr + 12, struct.pack('<I', len(slots)), 4)
+        vals = list(slots) + [-1] * (8 - len(slots))
+        ctypes.memmove(self.ptr + 16, struct.pack('<8i', *vals), 32)
 
 
 def synth_frame(config, scale, seed, index):
     """One frame of workload `config` (1..3) at 1/scale size."""
     p = ctypes.c_void_p()
     n = ctypes.c_size_t()
-    rc = lib().av1b_synth_frame(config, scale, seed, index, ctypes.byref(p), ctypes.byref(n))
+    rc = synth_lib().av1s_synth_frame(config, scale, seed, index, ctypes.byref(p), ctypes.byref(n))
     if rc:
         raise Av1bError(rc, 'synth_frame')
     return Blob(p.value, n.value, True)
 
 
 def synth_frame_ex(width, height, coded_width, bit_depth, sb_size, tools, seed, index,
-                   key_interval=0):
+                   key_interval=0, max_refs=None):
+    """A frame of any geometry (tools: the TOOL_* bits); `max_refs` the
+    reference slots an inter frame draws from (default: 3 with compound
+    prediction, else 1)."""
     p = ctypes.c_void_p()
     n = ctypes.c_size_t()
-    rc = lib().av1b_synth_frame_ex(width, height, coded_width, bit_depth, sb_size, tools, seed,
-                                   index, key_interval, ctypes.byref(p), ctypes.byref(n))
+    if max_refs is None:
+        rc = synth_lib().av1s_synth_frame_ex(width, height, coded_width, bit_depth, sb_size, tools,
+                                             seed, index, key_interval, ctypes.byref(p),
+                                             ctypes.byref(n))
+    else:
+        rc = synth_lib().av1s_synth_frame_refs(width, height, coded_width, bit_depth, sb_size,
+                                               tools, max_refs, seed, index, key_interval,
+                                               ctypes.byref(p), ctypes.byref(n))
     if rc:
         raise Av1bError(rc, 'synth_frame_ex')
     return Blob(p.value, n.value, True)

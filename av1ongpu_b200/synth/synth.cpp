@@ -27,6 +27,10 @@
  *
  * A synthetic frame lists its references as frame *distances* (1 = previous
  * frame); the caller maps them to its own slot ids (av1b_blob_set_refs).
+ *
+ * The generator is a library of its own (libav1synth.so, include/av1b_synth.h),
+ * apart from the decoder: a process that only needs the workload - the timed
+ * CPU reference, a tool writing fixtures - loads no decoder code.
  */
 #include <algorithm>
 #include <cmath>
@@ -35,6 +39,7 @@
 #include <cstring>
 #include <vector>
 
+#include "../../include/av1b_synth.h"
 #include "flat_syntax.hpp"
 
 namespace av1b {
@@ -777,16 +782,16 @@ static int synth_to_blob(const av1b::Params& p, uint64_t seed, int frame_index, 
   return AV1B_OK;
 }
 
-int av1b_synth_frame(int config, int scale, uint64_t seed, int frame_index, uint8_t** blob,
+int av1s_synth_frame(int config, int scale, uint64_t seed, int frame_index, uint8_t** blob,
                      size_t* len) {
   const av1b::Params p = av1b::config_params(config, scale);
   if (p.width <= 0) return AV1B_ERR_ARG;
   return synth_to_blob(p, seed, frame_index, blob, len);
 }
 
-int av1b_synth_frame_ex(int width, int height, int coded_width, int bit_depth, int sb_size,
-                        int tools, uint64_t seed, int frame_index, int key_interval,
-                        uint8_t** blob, size_t* len) {
+int av1s_synth_frame_refs(int width, int height, int coded_width, int bit_depth, int sb_size,
+                          int tools, int max_refs, uint64_t seed, int frame_index, int key_interval,
+                          uint8_t** blob, size_t* len) {
   av1b::Params p;
   p.width = width;
   p.height = height;
@@ -795,28 +800,20 @@ int av1b_synth_frame_ex(int width, int height, int coded_width, int bit_depth, i
   p.sb = sb_size == 128 ? 128 : 64;
   p.tools = tools;
   p.key_interval = key_interval > 0 ? key_interval : (1 << 30);
-  p.max_refs = (tools & (1 << 5)) ? 3 : 1;
+  p.max_refs = max_refs;
   if (bit_depth != 8 && bit_depth != 10 && bit_depth != 12) return AV1B_ERR_ARG;
+  if (max_refs < 1 || max_refs > 3) return AV1B_ERR_ARG;
   return synth_to_blob(p, seed, frame_index, blob, len);
 }
 
-void av1b_blob_free(uint8_t* blob) { free(blob); }
-
-int av1b_blob_set_refs(uint8_t* blob, size_t len, const int32_t* slots, int n) {
-  return av1b::blob_set_refs(blob, len, slots, n) ? AV1B_OK : AV1B_ERR_ARG;
+int av1s_synth_frame_ex(int width, int height, int coded_width, int bit_depth, int sb_size,
+                        int tools, uint64_t seed, int frame_index, int key_interval,
+                        uint8_t** blob, size_t* len) {
+  return av1s_synth_frame_refs(width, height, coded_width, bit_depth, sb_size, tools,
+                               (tools & (1 << 5)) ? 3 : 1, seed, frame_index, key_interval, blob,
+                               len);
 }
 
-int av1b_blob_get_refs(const uint8_t* blob, size_t len, int32_t* slots, int max_n) {
-  av1b_frame_syntax v;
-  if (!av1b::view_blob(blob, len, &v)) return AV1B_ERR_ARG;
-  const int n = static_cast<int>(v.n_reference_slots);
-  for (int i = 0; i < n && i < max_n; ++i) slots[i] = v.reference_slots[i];
-  return n;
-}
-
-int av1b_syntax_view(const uint8_t* blob, size_t len, av1b_frame_syntax* out) {
-  if (!out) return AV1B_ERR_ARG;
-  return av1b::view_blob(blob, len, out) ? AV1B_OK : AV1B_ERR_ARG;
-}
+void av1s_blob_free(uint8_t* blob) { free(blob); }
 
 }  // extern "C"

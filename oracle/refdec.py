@@ -1,22 +1,67 @@
 """The oracle (TEST INFRASTRUCTURE ONLY; used by tests/, the smoke check and
-bench.py's CPU-baseline leg): the reference's own CPU backend (built by
-oracle/Makefile into oracle/_ref/libav1ref.so) behind a small Python class
-that mirrors av1ongpu_b200.Decoder. Test infrastructure only."""
+bench.py's CPU-baseline leg and reference arm): the reference's own CPU
+backend (built by oracle/Makefile into oracle/_ref/libav1ref.so) behind a
+small Python class that mirrors av1ongpu_b200.Decoder.
+
+Decoding through it loads libav1ref.so and nothing of this repository's
+product: the plane and NV12 sizes are computed here, and a frame is any object
+with the serialized blob's `ptr`, `size`, `header`, `get_refs` and `set_refs`
+(RefBlob below, or av1ongpu_b200.Blob). Only `corrupt`, a fixture helper,
+imports the product package, for its Blob type."""
 import ctypes
-import sys
 import os
+import struct
+import sys
 
 import numpy as np
 
-
-
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 REF_LIB = os.path.join(ROOT, 'oracle', '_ref', 'libav1ref.so')
-if ROOT not in sys.path:
-    sys.path.insert(0, ROOT)
-import av1ongpu_b200 as av1b  # noqa: E402  (plane_shapes, nv12_size)
 
 _ref = None
+
+
+def plane_shapes(width, height, ss_x, ss_y):
+    """(rows, columns) of the three planes (Frame::plane_width / height)."""
+    cw, ch = (width + ss_x) >> ss_x, (height + ss_y) >> ss_y
+    return [(height, width), (ch, cw), (ch, cw)]
+
+
+def nv12_size(width, height, ss_x, ss_y, pitch):
+    """nv12_buffer_size (factory.cpp:236-244 of the reference): 4:2:0 only,
+    an even pitch at least a chroma row wide; 0 otherwise."""
+    if width <= 0 or height <= 0 or ss_x != 1 or ss_y != 1:
+        return 0
+    crow = 2 * ((width + 1) // 2)
+    if pitch & 1 or pitch < crow:
+        return 0
+    return pitch * (height + (height + 1) // 2)
+
+
+class RefBlob:
+    """A serialized frame in a 64-byte aligned numpy buffer (the blob layout of
+    av1ongpu_b200/csrc/flat_syntax.hpp: u32 magic, version, reserved, count,
+    eight int32 reference slots, then the scalars from byte 48)."""
+
+    def __init__(self, data):
+        self._arr = np.zeros(len(data) + 64, dtype=np.uint8)
+        off = (-self._arr.ctypes.data) % 64
+        self._view = self._arr[off:off + len(data)]
+        self._view[:] = np.frombuffer(data, dtype=np.uint8)
+        self.ptr = self._view.ctypes.data
+        self.size = len(data)
+
+    @property
+    def header(self):
+        return struct.unpack_from('<6i', self._view, 48)
+
+    def get_refs(self):
+        n = struct.unpack_from('<I', self._view, 12)[0]
+        return list(struct.unpack_from('<%di' % n, self._view, 16))
+
+    def set_refs(self, slots):
+        struct.pack_into('<I', self._view, 12, len(slots))
+        struct.pack_into('<8i', self._view, 16, *(list(slots) + [-1] * (8 - len(slots))))
 
 
 def available():
@@ -70,7 +115,7 @@ class RefDecoder:
 
     def decode(self, blob, keep=True, read_back=True):
         w, _cw, h, _bd, sx, sy = blob.header
-        shapes = av1b.plane_shapes(w, h, sx, sy)
+        shapes = plane_shapes(w, h, sx, sy)
         total = sum(a * b for a, b in shapes)
         out = np.empty(total, dtype=np.uint16) if read_back else None
         slot = ref_lib().av1ref_decode(self.h, blob.ptr, blob.size, 1 if keep else 0,
@@ -91,7 +136,7 @@ class RefDecoder:
         ref_lib().av1ref_release(self.h, slot)
 
     def to_nv12(self, slot, pitch, width, height):
-        n = av1b.nv12_size(width, height, 1, 1, pitch)
+        n = nv12_size(width, height, 1, 1, pitch)
         out = np.empty(max(n, 1), dtype=np.uint8)
         got = ref_lib().av1ref_to_nv12(self.h, slot, pitch, out.ctypes.data, out.size)
         if got < 0:
@@ -129,7 +174,7 @@ def dequant_pair(blob_bytes, seed):
     """(levels frame with seeded quantiser matrices, the same frame expanded
     into coefficient rasters by the reference front end's host dequantiser),
     both as serialized bytes, from a serialized levels frame."""
-    src = av1b.Blob.from_bytes(blob_bytes)
+    src = RefBlob(blob_bytes)
     pa, pb = ctypes.c_void_p(), ctypes.c_void_p()
     na, nb = ctypes.c_size_t(), ctypes.c_size_t()
     L = ref_lib()
@@ -149,7 +194,7 @@ DROP_DEBLOCK, DROP_CDEF, DROP_LR, DROP_GRAIN = 1, 2, 4, 8
 def strip_stages(blob_bytes, drop):
     """A serialized frame without the in-loop stages named by `drop`
     (DROP_* bits), as bytes."""
-    src = av1b.Blob.from_bytes(blob_bytes)
+    src = RefBlob(blob_bytes)
     p, n = ctypes.c_void_p(), ctypes.c_size_t()
     L = ref_lib()
     if L.av1ref_strip(src.ptr, src.size, drop, ctypes.byref(p), ctypes.byref(n)):
@@ -166,6 +211,9 @@ CORRUPT_EDGE_LEVEL, CORRUPT_EDGE_OUTSIDE, CORRUPT_CDEF_DIR, CORRUPT_LR_UNIT, COR
 def corrupt(blob, what, index=0):
     """A copy of a serialized frame (an av1ongpu_b200.Blob) with one record
     made invalid (CORRUPT_*), as a new Blob."""
+    if ROOT not in sys.path:
+        sys.path.insert(0, ROOT)
+    import av1ongpu_b200 as av1b
     p, n = ctypes.c_void_p(), ctypes.c_size_t()
     L = ref_lib()
     if L.av1ref_corrupt(blob.ptr, blob.size, what, index, ctypes.byref(p), ctypes.byref(n)):

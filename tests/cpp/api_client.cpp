@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "av1b.h"
+#include "av1b_synth.h"
 #include "av1gpu/av1gpu.hpp"
 #include "flat_syntax.hpp"
 
@@ -38,7 +39,7 @@ int main(int argc, char** argv) {
   for (int k = 0; k < frames; ++k) {
     uint8_t* blob = nullptr;
     size_t len = 0;
-    if (av1b_synth_frame_ex(w, h, cw, bd, sb, tools, seed, k, 30, &blob, &len) != 0) return 1;
+    if (av1s_synth_frame_ex(w, h, cw, bd, sb, tools, seed, k, 30, &blob, &len) != 0) return 1;
     av1b_frame_syntax view;
     av1b_syntax_view(blob, len, &view);
     av1gpu::FrameSyntax s;
@@ -58,7 +59,7 @@ int main(int argc, char** argv) {
       }
       slot = dec->decode_reference_planned(plan, slot, &frame, &err);
     }
-    av1b_blob_free(blob);
+    av1s_blob_free(blob);
     if (slot < 0) {
       std::fprintf(stderr, "decode %d: %s\n", k, err.c_str());
       return 1;

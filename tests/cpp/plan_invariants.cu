@@ -28,6 +28,7 @@ static cudaError_t plain_free_host(void* p) {
 #define cudaHostAlloc plain_host_alloc
 #define cudaFreeHost plain_free_host
 #include "decoder.cu"
+#include "../../include/av1b_synth.h"
 #undef cudaHostAlloc
 #undef cudaFreeHost
 #include <cstdio>
@@ -169,7 +170,7 @@ int main() {
     for (int k = 0; k < cs.frames; ++k) {
       uint8_t* blob = nullptr;
       size_t len = 0;
-      if (av1b_synth_frame_ex(cs.w, cs.h, cs.cw, cs.bd, cs.sb, cs.tools, 11, k, cs.key_interval, &blob,
+      if (av1s_synth_frame_ex(cs.w, cs.h, cs.cw, cs.bd, cs.sb, cs.tools, 11, k, cs.key_interval, &blob,
                               &len) != AV1B_OK) {
         std::printf("FAIL: %s frame %d: no synthetic frame\n", cs.name, k);
         return 1;
@@ -180,7 +181,7 @@ int main() {
         std::printf("FAIL: %s frame %d: records differ between 1 and 5 host threads\n", cs.name, k);
         ++failures;
       }
-      av1b_blob_free(blob);
+      av1s_blob_free(blob);
     }
   }
   if (failures) {

@@ -14,7 +14,7 @@ def build_client(tmp_path):
     exe = str(tmp_path / 'api_client')
     cmd = ['/usr/bin/g++', '-std=c++17', '-O1', os.path.join(ROOT, 'tests', 'cpp', 'api_client.cpp'),
            '-I', os.path.join(ROOT, 'include'), '-I', os.path.join(ROOT, 'av1ongpu_b200', 'csrc'),
-           '-L', os.path.join(ROOT, 'av1ongpu_b200'), '-lav1b',
+           '-L', os.path.join(ROOT, 'av1ongpu_b200'), '-lav1b', '-lav1synth',
            '-Wl,-rpath,' + os.path.join(ROOT, 'av1ongpu_b200'), '-o', exe]
     subprocess.run(cmd, check=True, capture_output=True)
     return exe

@@ -12,9 +12,9 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def declared_symbols():
-    text = open(os.path.join(ROOT, 'include', 'av1b.h')).read()
-    return sorted(set(re.findall(r'AV1B_API\s+[\w\s\*]*?\b(av1b_\w+)\s*\(', text)))
+def declared_symbols(header='av1b.h', macro='AV1B_API', prefix='av1b_'):
+    text = open(os.path.join(ROOT, 'include', header)).read()
+    return sorted(set(re.findall(r'%s\s+[\w\s\*]*?\b(%s\w+)\s*\(' % (macro, prefix), text)))
 
 
 def test_library_exports_every_declared_symbol(av1b):
@@ -25,8 +25,21 @@ def test_library_exports_every_declared_symbol(av1b):
         assert hasattr(lib, n), n
 
 
+def test_generator_library_exports_every_declared_symbol(av1b):
+    lib = av1b.synth_lib()
+    names = declared_symbols('av1b_synth.h', 'AV1S_API', 'av1s_')
+    assert len(names) == 4
+    for n in names:
+        assert hasattr(lib, n), n
+    # the generator is host code apart from the decoder: it links no CUDA
+    deps = subprocess.run(['ldd', av1b.SYNTH_LIB_PATH], capture_output=True, text=True).stdout
+    assert 'cuda' not in deps and 'av1b' not in deps
+
+
 def test_python_binds_every_exported_entry(av1b):
     assert set(av1b.exported_symbols()) <= set(declared_symbols())
+    assert set(av1b.synth_exported_symbols()) == set(
+        declared_symbols('av1b_synth.h', 'AV1S_API', 'av1s_'))
 
 
 def test_synth_is_deterministic(av1b):
@@ -44,6 +57,12 @@ def test_blob_view_and_refs(av1b):
     assert b.get_refs() == [1]
     b.set_refs([5])
     assert b.get_refs() == [5]
+    # the library reads the list the Python header code wrote, and the reverse
+    buf = (ctypes.c_int32 * 8)()
+    assert av1b.lib().av1b_blob_get_refs(b.ptr, b.size, buf, 8) == 1 and buf[0] == 5
+    assert av1b.lib().av1b_blob_set_refs(b.ptr, b.size, (ctypes.c_int32 * 2)(3, 9), 2) == 0
+    assert b.get_refs() == [3, 9]
+    b.set_refs([5])
     view = ctypes.create_string_buffer(4096)
     assert av1b.lib().av1b_syntax_view(b.ptr, b.size, view) == 0
     # a truncated buffer is refused

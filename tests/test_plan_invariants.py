@@ -21,7 +21,7 @@ def build_checker(tmp_path, src_dir=None, name='plan_invariants'):
     from av1ongpu_b200 import build as b
     b.build()
     objs = [os.path.join(b.OUT, f) for f in ('kernels.cu.o', 'plan_host.cpp.o', 'synth.cpp.o',
-                                             'api.cpp.o', 'noalloc.cu.o')]
+                                             'blob.cpp.o', 'api.cpp.o', 'noalloc.cu.o')]
     exe = str(tmp_path / name)
     inc = (['-I', src_dir] if src_dir else []) + ['-I', CSRC, '-I', os.path.join(ROOT, 'include')]
     cmd = [NVCC, '-gencode', 'arch=compute_100a,code=sm_100a', '-O2', '-std=c++17',
