@@ -48,6 +48,28 @@ class _Planes(ctypes.Structure):
     _fields_ = [('plane', ctypes.c_void_p * 3), ('stride', ctypes.c_int32 * 3)]
 
 
+class PlanInfo(ctypes.Structure):
+    """av1b_plan_info: a planned frame's geometry and work counts."""
+    _fields_ = [('width', ctypes.c_int32), ('height', ctypes.c_int32),
+                ('coded_width', ctypes.c_int32), ('bit_depth', ctypes.c_int32),
+                ('blocks', ctypes.c_int64), ('phase_b_blocks', ctypes.c_int64),
+                ('chains', ctypes.c_int64), ('phase_b_samples', ctypes.c_int64),
+                ('inter_tiles', ctypes.c_int64), ('inter_samples', ctypes.c_int64),
+                ('inter_ref_samples', ctypes.c_int64), ('transforms', ctypes.c_int64),
+                ('tx_samples', ctypes.c_int64), ('coef_samples', ctypes.c_int64),
+                ('deblock_edges', ctypes.c_int64 * 2), ('cdef_blocks', ctypes.c_int64),
+                ('lr_units', ctypes.c_int64), ('depth', ctypes.c_int32),
+                ('upscaled', ctypes.c_int32), ('restored', ctypes.c_int32),
+                ('grain', ctypes.c_int32)]
+
+    def as_dict(self):
+        out = {}
+        for name, _t in self._fields_:
+            v = getattr(self, name)
+            out[name] = list(v) if name == 'deblock_edges' else v
+        return out
+
+
 class Stats(ctypes.Structure):
     _fields_ = [('blocks', ctypes.c_int32), ('waves', ctypes.c_int32),
                 ('kernel_launches', ctypes.c_int32), ('reconstruct_ms', ctypes.c_double),
@@ -74,6 +96,8 @@ _SIGNATURES = {
                                            ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.c_int]),
     'av1b_plan_free': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     'av1b_sync': (ctypes.c_int, [ctypes.c_void_p]),
+    'av1b_plan_stats': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    'av1b_int_peak': (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     'av1b_set_profiling': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     'av1b_set_wait_limit': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong]),
     'av1b_selftest_wait': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, ctypes.POINTER(ctypes.c_int),
@@ -337,6 +361,12 @@ class Decoder:
         self._check(rc, 'decode_planned')
         return got.value
 
+    def plan_stats(self, plan):
+        """The planned frame's work counts (av1b_plan_stats) as a dict."""
+        info = PlanInfo()
+        self._check(lib().av1b_plan_stats(plan, ctypes.byref(info)), 'plan_stats')
+        return info.as_dict()
+
     def free_plan(self, plan):
         self._check(lib().av1b_plan_free(self.h, plan), 'plan_free')
 
@@ -446,6 +476,16 @@ class Decoder:
         s = Stats()
         self._check(lib().av1b_get_stats(self.h, ctypes.byref(s)), 'stats')
         return s
+
+
+def int_peak(device=0, kind=0):
+    """32-bit operations per second the SMs issue (av1b_int_peak): independent
+    adds (kind 0) or multiply-adds (kind 1)."""
+    v = ctypes.c_double(0)
+    rc = lib().av1b_int_peak(device, kind, ctypes.byref(v))
+    if rc:
+        raise Av1bError(rc, 'int_peak')
+    return v.value
 
 
 def cuda_available():

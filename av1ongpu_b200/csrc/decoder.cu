@@ -436,6 +436,8 @@ struct Plan {
   size_t coef_pool = 0, residual_pool = 0;
   size_t pre_res_pool = 0;        /* ints of residual computed ahead (phase B) */
   size_t n_dq = 0;                /* transforms the device dequantises */
+  size_t unit_samples = 0, inter_samples = 0, inter_ref_samples = 0, tx_samples = 0,
+         coef_samples = 0;        /* work counts, summed over the planner's pieces */
   int scale_x = AV1B_SCALE_ONE, scale_y = AV1B_SCALE_ONE;
   bool upscaled = false;
   bool grain = false;
@@ -505,6 +507,11 @@ struct BlockOut {
   std::vector<int2> itx_jobs;
   std::vector<DqRec> dq;
   size_t pre_res_pool = 0, coef_end = 0, res_end = 0;
+  /* work counts (av1b_plan_stats): samples of phase B blocks, of phase A
+   * inter blocks (and of their reference reads, two for a compound block),
+   * of transforms, and the coefficient raster samples the transforms read */
+  size_t unit_samples = 0, inter_samples = 0, inter_ref_samples = 0, tx_samples = 0,
+         coef_samples = 0;
   uint8_t* is_b = nullptr;        /* the frame's phase B flags, by block */
   /* the owner-cell grids (cells of 1 << cell[p] samples, owner_w x owner_h),
    * filled as the blocks convert */
@@ -524,6 +531,7 @@ struct BlockOut {
     inter_tiles_full.clear();
     itx_jobs.clear();
     pre_res_pool = coef_end = res_end = 0;
+    unit_samples = inter_samples = inter_ref_samples = tx_samples = coef_samples = 0;
     err = PlanErr();
   }
 };
@@ -788,11 +796,17 @@ int plan_block(const PlanCtx& ctx, const av1b_frame_syntax& s, size_t bi, BlockR
         O->itx_jobs.push_back(make_int2(static_cast<int>(bi), static_cast<int>(O->txs.size())));
       O->txs.push_back(x);
       ++r.tx_count;
+      O->tx_samples += static_cast<size_t>(t.w) * t.h;
+      O->coef_samples += b.residual_provided ? static_cast<size_t>(t.w) * t.h
+                                             : static_cast<size_t>(std::min(t.w, 32)) * std::min(t.h, 32);
     }
   }
   if (r.phase_b) {
     O->units.push_back(static_cast<int>(bi));
+    O->unit_samples += static_cast<size_t>(b.w) * b.h;
   } else {
+    O->inter_samples += static_cast<size_t>(b.w) * b.h;
+    O->inter_ref_samples += static_cast<size_t>(b.w) * b.h * (r.compound ? 2 : 1);
     /* blocks without masks (translation or global warp, with or without
      * OBMC) take the lean prediction kernel */
     const bool simple = r.mask_kind == 0 && !r.interintra;
@@ -1405,6 +1419,14 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
       o_dq[i + 1] = o_dq[i] + O.dq.size();
       coef_end = std::max(coef_end, O.coef_end);
       res_end = std::max(res_end, O.res_end);
+    }
+    P->unit_samples = P->inter_samples = P->inter_ref_samples = P->tx_samples = P->coef_samples = 0;
+    for (int i = 0; i < pieces; ++i) {
+      P->unit_samples += outs[i].unit_samples;
+      P->inter_samples += outs[i].inter_samples;
+      P->inter_ref_samples += outs[i].inter_ref_samples;
+      P->tx_samples += outs[i].tx_samples;
+      P->coef_samples += outs[i].coef_samples;
     }
     if (o_pre[pieces] > static_cast<size_t>(INT32_MAX) || o_tx[pieces] > static_cast<size_t>(INT32_MAX))
       return fail(d, AV1B_ERR_SYNTAX, "frame too large");
@@ -2572,6 +2594,35 @@ int av1b_decode_planned(av1b_decoder* d, av1b_plan* pl, int slot, int keep_refer
   clear_err(d);
   if (out_slot) *out_slot = -1;
   return execute_plan(d, pl, keep_reference ? 1 : 0, slot, out, out_slot, wait != 0);
+}
+
+int av1b_plan_stats(const av1b_plan* pl, av1b_plan_info* out) {
+  if (!pl || !out) return AV1B_ERR_ARG;
+  const Plan& P = pl->P;
+  std::memset(out, 0, sizeof(*out));
+  out->width = pl->width;
+  out->height = pl->height;
+  out->coded_width = pl->coded_width;
+  out->bit_depth = pl->bit_depth;
+  out->blocks = static_cast<int64_t>(P.n_blocks);
+  out->phase_b_blocks = static_cast<int64_t>(P.n_units);
+  out->chains = static_cast<int64_t>(P.n_chains);
+  out->depth = P.unit_depth;
+  out->phase_b_samples = static_cast<int64_t>(P.unit_samples);
+  out->inter_tiles = static_cast<int64_t>(P.n_tiles);
+  out->inter_samples = static_cast<int64_t>(P.inter_samples);
+  out->inter_ref_samples = static_cast<int64_t>(P.inter_ref_samples);
+  out->transforms = static_cast<int64_t>(P.n_itx);
+  out->tx_samples = static_cast<int64_t>(P.tx_samples);
+  out->coef_samples = static_cast<int64_t>(P.coef_samples);
+  out->deblock_edges[0] = static_cast<int64_t>(P.n_dbv);
+  out->deblock_edges[1] = static_cast<int64_t>(P.n_dbh);
+  out->cdef_blocks = static_cast<int64_t>(P.n_cdef);
+  for (int p = 0; p < 3; ++p) out->lr_units += P.lr.type[p] ? P.lr.n_units[p] : 0;
+  out->upscaled = P.upscaled ? 1 : 0;
+  out->restored = P.use_lr ? 1 : 0;
+  out->grain = P.grain ? 1 : 0;
+  return AV1B_OK;
 }
 
 int av1b_sync(av1b_decoder* d) {

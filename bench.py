@@ -1,34 +1,48 @@
-"""Benchmark: bit-exact 4K 10-bit AV1 reconstruction fps on B200.
+"""Benchmark: bit-exact 4K 10-bit AV1 reconstruction on one B200.
 
-Workload: the headline single-stream configuration - coded 2880x2160 10-bit
-4:2:0, superres to 3840x2160, 128x128 superblocks, every tool (64-point
-transforms, all transform types, CFL, palette, filter intra, compound with
-wedge / difference-weighted masks, OBMC, global warp, deblocking, CDEF, loop
-restoration after superres, film grain) and an NV12 output at pitch 4096.
-Synthetic FrameSyntax from a seed (the workload generator in
-av1ongpu_b200/csrc/synth.cpp); no bitstream is involved.
+Headline workload (`value`, `e2e`): the single-stream configuration - coded
+2880x2160 10-bit 4:2:0, superres to 3840x2160, 128x128 superblocks, every tool
+(64-point transforms, all transform types, CFL, palette, filter intra,
+compound with wedge / difference-weighted masks, OBMC, global warp,
+deblocking, CDEF, loop restoration after superres, film grain) and an NV12
+output at pitch 4096. Synthetic FrameSyntax from a seed (the workload
+generator, libav1synth.so); no bitstream is involved.
 
 A step is one group of pictures: one key frame and 29 inter frames (the
 configuration's key interval), each decoded into a reference slot and packed
 to NV12.
 
-  value   frames/s with every frame's syntax already planned and resident in
-          HBM (av1b_plan_frame before the timed region), device work only:
-          reconstruction, filters, reference store, grain, NV12 into device
-          memory. Per-frame inputs (~40-75 MB) and pictures exceed the 126 MB
-          L2 over a step, so no flush is needed between steps.
-  e2e     frames/s through the public API with host buffers: every frame's
-          serialized syntax is read from pinned host memory, planned,
-          uploaded, decoded, and its NV12 read back to the host. The API's
-          plan / decode split is used as intended: two threads plan frames
-          k + 1 .. k + 3 (av1b_plan_frame) while frame k decodes, and frame
-          k - 1's NV12 (packed on the device) is read back meanwhile.
+  bitexact  before anything is timed, the step runs once with every frame's
+            output planes and NV12 read back, and each frame's hashes are
+            compared with the oracle's (tests/golden/workloads.json, made by
+            the reference's CPU backend from the same seed). A mismatch
+            prints "bitexact": false and exits 1.
+  value     frames/s with every frame's syntax already planned and resident in
+            HBM (av1b_plan_frame before the timed region), device work only:
+            reconstruction, filters, reference store, grain, NV12 into device
+            memory. Per-frame inputs (~40-75 MB) and pictures exceed the 126 MB
+            L2 over a step, so no flush is needed between steps.
+  e2e       frames/s through the public API with host buffers: every frame's
+            serialized syntax is read from pinned host memory, planned,
+            uploaded, decoded, and its NV12 read back to the host. The API's
+            plan / decode split is used as intended: planner threads plan
+            frames k + 1 .. k + 6 (av1b_plan_frame) while frame k decodes, and
+            frame k - 1's NV12 (packed on the device) is read back meanwhile.
+  stages    per kernel stage: ms per frame (CUDA events around every launch on
+            the decoder's stream), its algorithmic bytes against the measured
+            HBM bandwidth and its counted integer operations against the
+            measured integer-ALU peak (av1b_int_peak), from the work counts of
+            the planned frames (av1b_plan_stats); `roofline` is the dominant
+            stage, bound by whichever fraction is larger.
 
 Multi-GPU (torchrun): replicas only - each rank decodes its own stream; the
 timing is the max over ranks and `value` sums all ranks' frames.
 
 `--impl reference` times the reference's own CPU backend (oracle/_ref, built
-from the reference sources) on the host cores, one frame per step.
+from the reference sources) on all host cores through its public API
+(decode_reference + to_nv12), on the same GOP: each timed step decodes the 30
+frames, one key and 29 inter, from files a separate process wrote, so the
+timing process maps only the reference's library.
 """
 import argparse
 import json
@@ -36,9 +50,10 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import threading
-from concurrent.futures import ThreadPoolExecutor
 import time
+from concurrent.futures import ThreadPoolExecutor
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
@@ -48,6 +63,7 @@ UNIT = 'frames/s'
 PITCH = 4096
 GOP = 30
 SEED = 20261203
+CONFIG = 3
 
 
 def parse():
@@ -60,12 +76,22 @@ def parse():
     ap.add_argument('--frames', type=int, default=GOP, help='frames per step')
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-e2e', action='store_true', help='skip the end-to-end leg (profiling runs)')
+    ap.add_argument('--no-verify', action='store_true', help='skip the bit-exact check (profiling runs)')
     return ap.parse_args()
 
 
 def rank_info():
     return (int(os.environ.get('RANK', '0')), int(os.environ.get('WORLD_SIZE', '1')),
             int(os.environ.get('LOCAL_RANK', '0')))
+
+
+def config_dict(w, h, cw, frames, world):
+    """The `config` of both arms' lines (identical for the same workload)."""
+    return {'workload': 'config3: %dx%d (coded %d) 10-bit 4:2:0 superres, 128x128 SB, all tools, '
+                        'film grain, NV12 pitch %d' % (w, h, cw, PITCH),
+            'seed': SEED, 'frames_per_step': frames, 'gop': '1 key + %d inter' % (frames - 1),
+            'l2': 'inputs larger than L2 (per-step syntax + pictures > 126 MB)',
+            'parallelism': 'replicas x%d' % world}
 
 
 class ClockSampler:
@@ -121,38 +147,131 @@ class ClockSampler:
                 'samples': len(sm)}
 
 
-def workload_blobs(av1b, scale, frames, seed):
-    return [av1b.synth_frame(3, scale, seed, k) for k in range(frames)]
+# ---- the reference arm ---------------------------------------------------------------------
+def reference_frames(scale, frames, seed):
+    """The GOP's frames as bytes, written by a separate process (the generator
+    library is not mapped into this one), and the geometry."""
+    with tempfile.TemporaryDirectory() as tmp:
+        r = subprocess.run([sys.executable, '-m', 'av1ongpu_b200.workload', '--config', str(CONFIG),
+                            '--scale', str(scale), '--seed', str(seed), '--frames', str(frames),
+                            '--out', tmp], capture_output=True, text=True, cwd=ROOT)
+        if r.returncode:
+            raise RuntimeError('workload writer failed: ' + r.stderr[-500:])
+        header = [int(v) for v in r.stdout.split()]
+        data = []
+        for k in range(frames):
+            with open(os.path.join(tmp, 'frame_%04d.av1s' % k), 'rb') as f:
+                data.append(f.read())
+    return header, data
 
 
-def stage_bytes(L, stage):
-    """Algorithmic bytes one launch of `stage` moves for a frame of geometry L
-    (a dict: coded / display sample counts, NV12 bytes). Samples are 2 bytes."""
-    nc, nd, nv12 = L['coded'], L['display'], L['nv12']
+def run_reference(args):
+    rank, world, _ = rank_info()
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+    import refdec
+    if not refdec.available():
+        print(json.dumps({'impl': 'reference', 'unavailable': 'oracle/_ref/libav1ref.so not built'}))
+        return 0
+    (w, cw, h, _bd, _sx, _sy), data = reference_frames(args.scale, args.frames, SEED)
+    cw = cw or w
+    lib = refdec.ref_lib()
+    lib.av1ref_set_threads(os.cpu_count() or 1)
+    cores = lib.av1ref_max_threads()
+    ref = refdec.RefDecoder()
+
+    def gop(n_frames):
+        """Decodes the GOP's first n_frames frames (key frame first) with the
+        reference's decode_reference + to_nv12, slots released as the stream
+        advances; returns the seconds it took."""
+        stream = refdec.Stream(ref)
+        blobs = [refdec.RefBlob(b) for b in data[:n_frames]]
+        t0 = time.perf_counter()
+        for k, b in enumerate(blobs):
+            slot, _ = stream.decode(k, b, read_back=True)
+            ref.to_nv12(slot, PITCH, w, h)
+        dt = time.perf_counter() - t0
+        for s in list(stream.slots.values()):
+            ref.release_reference(s)
+        return dt
+
+    # warm-up steps: the GOP's key frame and first inter frame each (the CPU
+    # path's thread pool and page faults; a full GOP per warm-up step would
+    # only lengthen the run)
+    for _ in range(args.warmup):
+        gop(min(2, args.frames))
+    times = [gop(args.frames) for _ in range(args.steps)]
+    fps = args.frames * len(times) / sum(times)
+    line = {
+        'impl': 'reference', 'metric': METRIC, 'value': fps, 'unit': UNIT, 'n_gpus': args.gpus,
+        'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': 1e3 * sum(times) / len(times),
+        'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'int32',
+        'data': 'synthetic FrameSyntax (seeded generator), written by a separate process',
+        'config': config_dict(w, h, cw, args.frames, 1),
+        'cpu_baseline': {'value': fps, 'unit': UNIT, 'cores': cores, 'kind': 'reference',
+                         'sample': 'each step the whole GOP (1 key + %d inter) of the %dx%d workload, '
+                                   'decode_reference + to_nv12; warm-up steps the key frame and the '
+                                   'first inter frame' % (args.frames - 1, w, h)},
+        'e2e': {'value': fps, 'unit': UNIT, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---- stage rooflines ------------------------------------------------------------------------
+# Counted integer operations per unit of work, one per add, subtract, shift,
+# logic op, compare, min / max and multiply-add (the hardware issues a
+# multiply-add as one instruction), from the stage's arithmetic (the
+# reference's loops, av1gpu_kernels.h); the derivations are in DESIGN.md
+# ("Operation counts"). Units: `ref` a predicted sample per reference,
+# `tx` a transform sample, `unit` a phase B sample, `coded` / `display` a
+# picture sample, `nv12` a display sample.
+OPS = {
+    'inter': ('inter_ref', 31), 'itx': ('tx', 25), 'units': ('unit', 15),
+    'deblock_v': ('coded', 10), 'deblock_h': ('coded', 10), 'cdef': ('coded', 100),
+    'upscale': ('display', 12), 'lr': ('display', 50), 'grain_blend': ('display', 20),
+    'nv12': ('display', 2), 'grain_template': ('grain', 30),
+}
+# film grain templates: 82x73 luma and two chroma templates (44x38 at 4:2:0)
+GRAIN_TEMPLATE_SAMPLES = 82 * 73 + 2 * 44 * 38
+
+
+def frame_counts(info, nv12_bytes):
+    """Per-frame work of one planned frame, by unit (samples)."""
+    w, h, cw = info['width'], info['height'], info['coded_width'] or info['width']
+    coded = cw * h + 2 * ((cw + 1) // 2) * ((h + 1) // 2)
+    display = w * h + 2 * ((w + 1) // 2) * ((h + 1) // 2)
+    return {'coded': coded, 'display': display, 'nv12_bytes': nv12_bytes,
+            'unit': info['phase_b_samples'], 'inter': info['inter_samples'],
+            'inter_ref': info['inter_ref_samples'], 'tx': info['tx_samples'],
+            'coef': info['coef_samples'], 'upscaled': info['upscaled'],
+            'restored': info['restored'], 'grain': GRAIN_TEMPLATE_SAMPLES if info['grain'] else 0}
+
+
+def stage_bytes(c, stage):
+    """Algorithmic bytes of one frame's `stage` (samples are 2 bytes)."""
     return {
-        'deblock_v': 4 * nc, 'deblock_h': 4 * nc,       # read + write every coded sample
-        'cdef': 4 * nc,                                  # snapshot read + picture write
-        'upscale': 2 * nc + 2 * nd,                      # coded read, display write
-        'lr': 4 * nd,                                    # CDEF snapshot read + write
-        'grain_blend': 4 * nd,                           # picture read + display write
-        'nv12': 2 * nd + nv12,                           # picture read + NV12 write
-        'inter': 2 * nc + 4 * nd,                        # write + two references read once
-        'units': 6 * nc,                                 # residual read (4 B) + picture write
-        'itx': 4 * nc + 4 * nc,                          # coefficients (4 B) + picture read/write
-    }.get(stage)
+        'deblock_v': 4 * c['coded'], 'deblock_h': 4 * c['coded'],  # read + write each coded sample
+        'cdef': 4 * c['coded'],                                    # snapshot read + picture write
+        'upscale': (2 * c['coded'] + 2 * c['display']) if c['upscaled'] else 0,
+        'lr': 4 * c['display'] if c['restored'] else 0,            # CDEF output read + write
+        'grain_blend': 4 * c['display'] if c['grain'] else 0,      # picture read + display write
+        'nv12': 2 * c['display'] + c['nv12_bytes'],                # picture read + NV12 write
+        'inter': 2 * c['inter'] + 2 * c['inter_ref'],              # write + each reference read once
+        'units': 6 * c['unit'],                                    # residual (4 B) + picture write
+        'itx': 4 * c['coef'] + 4 * c['tx'],                        # coefficients + picture read/write
+        'grain_template': 2 * c['grain'],                          # the templates written
+    }.get(stage, 0)
 
 
-def geometry(av1b, blob):
-    w, cw, h, bd, sx, sy = blob.header
-    cw = cw if cw > 0 else w
-    c = cw * h + 2 * ((cw + 1) // 2) * ((h + 1) // 2)
-    d = w * h + 2 * ((w + 1) // 2) * ((h + 1) // 2)
-    return {'w': w, 'h': h, 'coded_w': cw, 'coded': c, 'display': d,
-            'nv12': av1b.nv12_size(w, h, sx, sy, PITCH)}
+def stage_ops(c, stage):
+    unit, per = OPS.get(stage, (None, 0))
+    return per * c.get(unit, 0) if unit else 0
 
 
 def read_traffic():
-    """traffic per launch of the dominant kernel, from the committed ncu summary."""
+    """DRAM traffic per launch of each stage, from the committed ncu summary."""
     path = os.path.join(ROOT, 'profiles', 'traffic.json')
     try:
         with open(path) as f:
@@ -161,75 +280,70 @@ def read_traffic():
         return {}
 
 
-def cpu_baseline(av1b, scale, seed, frames=3):
-    """The reference CPU backend on the first `frames` frames of the workload,
-    all host threads, through its public API (decode_reference + to_nv12)."""
-    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
-    import refdec
-    if not refdec.available():
-        return None
-    lib = refdec.ref_lib()
-    lib.av1ref_set_threads(os.cpu_count() or 1)
-    ref = refdec.RefDecoder()
-    stream = refdec.Stream(ref)
-    blobs = workload_blobs(av1b, scale, frames, seed)
-    geo = geometry(av1b, blobs[0])
-    t0 = time.perf_counter()
-    for k, b in enumerate(blobs):
-        slot, _ = stream.decode(k, b, read_back=True)
-        ref.to_nv12(slot, PITCH, geo['w'], geo['h'])
-    dt = time.perf_counter() - t0
-    return {'value': frames / dt, 'unit': UNIT, 'cores': lib.av1ref_max_threads(),
-            'kind': 'reference',
-            'sample': '%d frames (1 key + %d inter) of the %dx%d workload, decode_reference + '
-                      'to_nv12, %.1f s' % (frames, frames - 1, geo['w'], geo['h'], dt)}
-
-
-def run_reference(args):
-    rank, world, _ = rank_info()
-    if rank != 0:
-        return 0
+def peaks(local):
     import av1ongpu_b200 as av1b
-    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
-    import refdec
-    if not refdec.available():
-        print(json.dumps({'impl': 'reference', 'unavailable': 'oracle/_ref/libav1ref.so not built'}))
-        return 0
-    lib = refdec.ref_lib()
-    lib.av1ref_set_threads(os.cpu_count() or 1)
-    cores = lib.av1ref_max_threads()
-    ref = refdec.RefDecoder()
-    stream = refdec.Stream(ref)
-    n = args.warmup + args.steps
-    blobs = workload_blobs(av1b, args.scale, n, SEED)
-    geo = geometry(av1b, blobs[0])
-    times = []
-    for k, b in enumerate(blobs):
-        t0 = time.perf_counter()
-        slot, _ = stream.decode(k, b, read_back=True)
-        ref.to_nv12(slot, PITCH, geo['w'], geo['h'])
-        times.append(time.perf_counter() - t0)
-    timed = times[args.warmup:]
-    fps = len(timed) / sum(timed)
-    line = {
-        'impl': 'reference', 'metric': METRIC, 'value': fps, 'unit': UNIT, 'n_gpus': args.gpus,
-        'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': 1e3 * sum(timed) / len(timed),
-        'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'int32',
-        'data': 'synthetic FrameSyntax (seeded)',
-        'config': {'workload': 'config3: %dx%d (coded %d) 10-bit 4:2:0 superres, 128x128 SB, all '
-                               'tools, NV12 pitch %d' % (geo['w'], geo['h'], geo['coded_w'], PITCH),
-                   'step': 'one frame (bounded CPU sample)', 'frames_per_step': 1},
-        'cpu_baseline': {'value': fps, 'unit': UNIT, 'cores': cores, 'kind': 'reference',
-                         'sample': 'frames %d..%d of the workload, one per step' % (args.warmup, n - 1)},
-        'e2e': {'value': fps, 'unit': UNIT, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
-    }
-    print(json.dumps(line))
-    return 0
+    p = {}
+    try:
+        with open(os.path.join(ROOT, 'MEASURED_PEAKS.json')) as f:
+            p = json.load(f)
+    except (OSError, ValueError):
+        pass
+    hbm = p.get('hbm_gbs')
+    out = {'hbm_gbs': hbm or 6650.0, 'hbm_source': 'measured (MEASURED_PEAKS.json)' if hbm else
+           'fallback (6.65 TB/s, earlier measurement on this pool)'}
+    out['int_add_ops'] = av1b.int_peak(local, 0)
+    out['int_mad_ops'] = av1b.int_peak(local, 1)
+    out['int_source'] = 'measured live (av1b_int_peak: 32-bit add rings on every SM)'
+    return out
+
+
+def stage_report(prof, counts, frames, pk):
+    """{stage: ms per frame, GB/s and fraction of HBM, int-op/s and fraction of
+    the integer peak, bound} from the profiled pass and the frames' counts."""
+    out = {}
+    traffic = read_traffic()
+    for st, (ms, n) in prof.items():
+        if n <= 0 or st.endswith('_host') or st == 'copy':
+            out[st] = {'ms_per_frame': round(ms / frames, 4), 'launches': n}
+            continue
+        b = sum(stage_bytes(c, st) for c in counts)
+        ops = sum(stage_ops(c, st) for c in counts)
+        sec = ms / 1e3
+        gbs = b / sec / 1e9 if b else 0.0
+        iops = ops / sec if ops else 0.0
+        fh = gbs / pk['hbm_gbs']
+        fi = iops / pk['int_add_ops']
+        out[st] = {'ms_per_frame': round(ms / frames, 4), 'launches': n,
+                   'bytes_per_frame': b // frames, 'ops_per_frame': ops // frames,
+                   'gbs': round(gbs, 1), 'hbm_frac': round(fh, 4),
+                   'int_tops': round(iops / 1e12, 3), 'int_frac': round(fi, 4),
+                   'bound': 'hbm' if fh >= fi else 'int-alu',
+                   'traffic_per_launch': traffic.get(st)}
+    return out
+
+
+# ---- our arm ------------------------------------------------------------------------------------
+def verify(av1b, dec, plans, ring, geo, frames):
+    """Runs the step once, untimed, reading back every frame's planes and NV12,
+    and compares their hashes with the oracle's (tests/golden/workloads.json).
+    Returns (ok, frames compared, first mismatch or None)."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, 'tests'))
+    import golden_util
+    want = golden_util.load_workloads()['bench_config3']
+    shapes = av1b.plane_shapes(geo['w'], geo['h'], 1, 1)
+    for k, pl in enumerate(plans):
+        planes = [np.empty(s, dtype=np.uint16) for s in shapes]
+        dec.decode_planned(pl, slot=ring[k % 4], keep=True, wait=True, planes=planes)
+        nv12 = dec.to_nv12(ring[k % 4], PITCH, geo['w'], geo['h'])
+        got = [golden_util.digest(planes), golden_util.digest([nv12])]
+        if got != want['frames'][k]:
+            return False, k + 1, 'frame %d: %s, oracle %s' % (k, got, want['frames'][k])
+    return True, frames, None
 
 
 def run_ours(args):
     import ctypes
-    import numpy as np
     import torch
     import av1ongpu_b200 as av1b
 
@@ -243,12 +357,14 @@ def run_ours(args):
     seed = SEED + 7919 * rank
     F = args.frames
 
-    blobs = workload_blobs(av1b, args.scale, F, seed)
-    geo = geometry(av1b, blobs[0])
+    with ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as ex:
+        blobs = list(ex.map(lambda k: av1b.synth_frame(CONFIG, args.scale, seed, k), range(F)))
+    w, cw, h, _bd, sx, sy = blobs[0].header
+    geo = {'w': w, 'h': h, 'coded_w': cw or w, 'nv12': av1b.nv12_size(w, h, sx, sy, PITCH)}
     dec = av1b.Decoder(local)
     stream = torch.cuda.ExternalStream(dec.stream(), device=local)
 
-    # ---- value: planned frames resident in HBM ---------------------------------------------
+    # ---- planned frames resident in HBM --------------------------------------------------------
     ring = [dec.reserve_reference() for _ in range(4)]
     plans = []
     for k, b in enumerate(blobs):
@@ -256,6 +372,17 @@ def run_ours(args):
         b.set_refs([ring[(k - d) % 4] for d in dists])
         plans.append(dec.plan(b))
         b.set_refs(dists)
+    counts = [frame_counts(dec.plan_stats(pl), geo['nv12']) for pl in plans]
+
+    # ---- bit exactness of the frames the step times ----------------------------------------
+    bitexact, checked, mismatch = None, 0, None
+    exact_workload = args.scale == 1 and F == GOP and seed == SEED
+    if not args.no_verify and exact_workload:
+        bitexact, checked, mismatch = verify(av1b, dec, plans, ring, geo, F)
+        if not bitexact and rank == 0:
+            print(json.dumps({'metric': METRIC, 'bitexact': False, 'mismatch': mismatch}))
+            return 1
+
     nv12_dev = torch.empty(geo['nv12'], dtype=torch.uint8, device='cuda:%d' % local)
 
     def device_step():
@@ -301,32 +428,30 @@ def run_ours(args):
     dec.sync()
     prof = dec.profile()
     dec.set_profiling(False)
-    # the dominant kernel on the frame's critical path: the grain templates
-    # run on a side stream, overlapped with reconstruction
-    kernels = {k: v for k, v in prof.items()
-               if k not in ('copy', 'grain_template') and not k.endswith('_host') and v[1] > 0}
-    dom = max(kernels, key=lambda k: kernels[k][0]) if kernels else None
-    peaks = {}
-    try:
-        with open(os.path.join(ROOT, 'MEASURED_PEAKS.json')) as f:
-            peaks = json.load(f)
-    except (OSError, ValueError):
-        pass
-    hbm_peak = peaks.get('hbm_gbs')
-    peak_note = 'measured' if hbm_peak else 'fallback'
-    hbm_peak = hbm_peak or 6650.0
+    pk = peaks(local)
+    stages = stage_report(prof, counts, F, pk)
+    # the dominant stage: the most device time per frame (the grain templates
+    # included, although they overlap reconstruction on a side stream)
+    timed = {k: v for k, v in stages.items() if 'bound' in v}
+    dom = max(timed, key=lambda k: timed[k]['ms_per_frame']) if timed else None
     roofline = None
     if dom:
-        avg_ms = kernels[dom][0] / kernels[dom][1]
-        bytes_per_launch = stage_bytes(geo, dom)
-        achieved = bytes_per_launch / (avg_ms / 1e3) / 1e9 if bytes_per_launch else None
-        tr = read_traffic().get(dom)
-        roofline = {'bound': 'hbm', 'kernel': dom, 'achieved': achieved, 'peak': hbm_peak,
-                    'peak_source': peak_note, 'unit': 'GB/s',
-                    'frac': achieved / hbm_peak if achieved else None,
-                    'traffic': tr, 'algorithmic_bytes_per_launch': bytes_per_launch,
-                    'avg_launch_ms': avg_ms}
-    stage_ms = {k: round(v[0] / F, 4) for k, v in prof.items() if v[1] > 0}
+        s = timed[dom]
+        avg_ms = prof[dom][0] / prof[dom][1]
+        per_launch_bytes = s['bytes_per_frame'] * F / prof[dom][1]
+        per_launch_ops = s['ops_per_frame'] * F / prof[dom][1]
+        hbm = {'achieved': s['gbs'], 'peak': pk['hbm_gbs'], 'unit': 'GB/s', 'frac': s['hbm_frac'],
+               'peak_source': pk['hbm_source'], 'algorithmic_bytes_per_launch': per_launch_bytes}
+        alu = {'achieved': s['int_tops'], 'peak': round(pk['int_add_ops'] / 1e12, 3),
+               'unit': 'T int-op/s', 'frac': s['int_frac'], 'peak_source': pk['int_source'],
+               'counted_ops_per_launch': per_launch_ops}
+        main = hbm if s['bound'] == 'hbm' else alu
+        roofline = {'bound': s['bound'], 'kernel': dom, 'achieved': main['achieved'],
+                    'peak': main['peak'], 'unit': main['unit'], 'frac': main['frac'],
+                    'traffic': s['traffic_per_launch'], 'avg_launch_ms': avg_ms,
+                    'hbm': hbm, 'int_alu': alu,
+                    'note': 'frac of measured peaks; traffic = ncu dram bytes per launch '
+                            '(profiles/traffic.json)'}
 
     # ---- e2e: public API with host buffers ------------------------------------------------
     pinned = []
@@ -361,26 +486,26 @@ def run_ours(args):
             b.set_refs([e2e_ring[(k - d) % 4] for d in dists])
             view = ctypes.create_string_buffer(4096)
             av1b.lib().av1b_syntax_view(b.ptr, b.size, view)
-            h = ctypes.c_void_p()
-            rc = av1b.lib().av1b_plan_frame(e2e_dec.h, view, ctypes.byref(h))
+            hh = ctypes.c_void_p()
+            rc = av1b.lib().av1b_plan_frame(e2e_dec.h, view, ctypes.byref(hh))
             b.set_refs(dists)
             if rc:
                 raise av1b.Av1bError(rc, 'plan_frame')
-            return h
+            return hh
 
         packs = []
         with ThreadPoolExecutor(max_workers=3) as ex:
             futs = {k: ex.submit(plan, k) for k in range(min(ahead, n))}
             for k in range(n):
-                h = futs.pop(k).result()
+                hh = futs.pop(k).result()
                 if k + ahead < n:
                     futs[k + ahead] = ex.submit(plan, k + ahead)
                 got = ctypes.c_int(-1)
-                rc = av1b.lib().av1b_decode_planned(e2e_dec.h, h, e2e_ring[k % 4], 1, None,
+                rc = av1b.lib().av1b_decode_planned(e2e_dec.h, hh, e2e_ring[k % 4], 1, None,
                                                      ctypes.byref(got), 0)
                 if rc:
                     raise av1b.Av1bError(rc, 'decode_planned')
-                av1b.lib().av1b_plan_free(e2e_dec.h, h)
+                av1b.lib().av1b_plan_free(e2e_dec.h, hh)
                 packs.append(e2e_dec.nv12_pack_begin(e2e_ring[k % 4], PITCH))
                 if len(packs) > 1:
                     hd = packs.pop(0)
@@ -411,7 +536,7 @@ def run_ours(args):
 
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        base = cpu_baseline(av1b, args.scale, SEED)
+        base = cpu_baseline(blobs, geo)
 
     for pl in plans:
         dec.free_plan(pl)
@@ -421,21 +546,45 @@ def run_ours(args):
             'warmup': args.warmup, 'ms_per_step': ms / args.steps, 'higher_is_better': True,
             'scaling': 'weak', 'vs_baseline': None, 'dtype': 'int32',
             'data': 'synthetic FrameSyntax (seeded generator), device-resident plans',
-            'config': {'workload': 'config3: %dx%d (coded %d) 10-bit 4:2:0 superres, 128x128 SB, '
-                                   'all tools, film grain, NV12 pitch %d' %
-                                   (geo['w'], geo['h'], geo['coded_w'], PITCH),
-                       'frames_per_step': F, 'gop': '1 key + %d inter' % (F - 1),
-                       'l2': 'inputs larger than L2 (per-step syntax + pictures > 126 MB)',
-                       'parallelism': 'replicas x%d' % world},
+            'config': config_dict(geo['w'], geo['h'], geo['coded_w'], F, world),
+            'bitexact': bitexact, 'bitexact_frames': checked,
+            'bitexact_ref': 'per-frame hashes of the output planes and NV12 against the oracle '
+                            '(tests/golden/workloads.json)' if bitexact is not None else
+                            'not checked (not the exact workload, or --no-verify)',
             'e2e': e2e, 'roofline': roofline, 'cpu_baseline': base,
             'clocks': clk, 'gpu_launches': launches_per_frame * F * args.steps,
-            'stage_ms_per_frame': stage_ms,
+            'peaks': {k: v for k, v in pk.items()},
+            'stages': stages,
         }
         print(json.dumps(line))
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def cpu_baseline(blobs, geo, frames=3):
+    """The reference CPU backend on the first `frames` frames of the workload
+    (the key frame and two inter frames), all host threads, through its public
+    API (decode_reference + to_nv12)."""
+    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+    import refdec
+    if not refdec.available():
+        return None
+    lib = refdec.ref_lib()
+    lib.av1ref_set_threads(os.cpu_count() or 1)
+    ref = refdec.RefDecoder()
+    stream = refdec.Stream(ref)
+    own = [refdec.RefBlob(b.to_bytes()) for b in blobs[:frames]]
+    t0 = time.perf_counter()
+    for k, b in enumerate(own):
+        slot, _ = stream.decode(k, b, read_back=True)
+        ref.to_nv12(slot, PITCH, geo['w'], geo['h'])
+    dt = time.perf_counter() - t0
+    return {'value': frames / dt, 'unit': UNIT, 'cores': lib.av1ref_max_threads(),
+            'kind': 'reference',
+            'sample': '%d frames (1 key + %d inter) of the %dx%d workload, decode_reference + '
+                      'to_nv12, %.1f s' % (frames, frames - 1, geo['w'], geo['h'], dt)}
 
 
 def main():

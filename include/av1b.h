@@ -215,6 +215,25 @@ AV1B_API int av1b_plan_frame(av1b_decoder* dec, const av1b_frame_syntax* syntax,
 AV1B_API int av1b_decode_planned(av1b_decoder* dec, av1b_plan* plan, int slot, int keep_reference,
                                  const av1b_planes* out, int* out_slot, int wait);
 AV1B_API int av1b_plan_free(av1b_decoder* dec, av1b_plan* plan);
+/* What a planned frame holds: its geometry and the work each stage has, as
+ * the planner counted it (the reference's DecodeStats, av1gpu.hpp:544-552,
+ * counts blocks and waves; a benchmark needs the samples each kernel touches
+ * to state its algorithmic bytes). Phase B is the dependency-scheduled part
+ * (intra, inter-intra and intra block copy blocks), in `chains` chains of
+ * dependency depth `depth`; phase A inter blocks are predicted from
+ * reference pictures only, `inter_ref_samples` counting a compound block's
+ * two predictions. */
+typedef struct av1b_plan_info {
+  int32_t width, height, coded_width, bit_depth;
+  int64_t blocks, phase_b_blocks, chains, phase_b_samples;
+  int64_t inter_tiles, inter_samples, inter_ref_samples;
+  int64_t transforms, tx_samples, coef_samples;
+  int64_t deblock_edges[2];      /* vertical, horizontal */
+  int64_t cdef_blocks, lr_units;
+  int32_t depth, upscaled, restored, grain;
+} av1b_plan_info;
+AV1B_API int av1b_plan_stats(const av1b_plan* plan, av1b_plan_info* out);
+
 /* Waits for queued work and reports a device-side failure of the last frame. */
 AV1B_API int av1b_sync(av1b_decoder* dec);
 
@@ -282,6 +301,13 @@ AV1B_API int av1b_set_wait_limit(av1b_decoder* dec, long long limit_ns);
  * and the elapsed device time. */
 AV1B_API int av1b_selftest_wait(av1b_decoder* dec, long long limit_ns, int* status,
                                 double* elapsed_ms);
+
+/* The integer-ALU roof of `device`: 32-bit operations per second of
+ * independent adds (kind 0) or multiply-adds (kind 1, one instruction each),
+ * measured by a short kernel on every SM. The per-stage report divides each
+ * stage's counted operations by it, beside its bytes by the HBM bandwidth.
+ * No counterpart in the reference. */
+AV1B_API int av1b_int_peak(int device, int kind, double* ops_per_s);
 
 /* Per-stage device timing: with profiling on, every launch (and device copy)
  * is bracketed by CUDA events on the decoder's stream, and the elapsed times

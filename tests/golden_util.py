@@ -53,3 +53,37 @@ def run_case(dec, case, av1b, seed=4242):
 def load():
     with open(GOLDEN) as f:
         return json.load(f)['cases']
+
+
+# The benchmark workloads at full size: name, (config, seed, frames, NV12
+# pitch). bench_config3 is exactly the GOP bench.py times (its SEED, 30
+# frames: 1 key + 29 inter); config 1 and 2 are the first 30 and 60 frames of
+# their streams (seed 1000 * config), config 2 with its key frames at 0 and 30.
+WORKLOADS = [
+    ('bench_config3', (3, 20261203, 30, 4096)),
+    ('config1_full', (1, 1000, 30, 1280)),
+    ('config2_full', (2, 2000, 60, 1920)),
+]
+WORKLOAD_GOLDEN = os.path.join(HERE, 'golden', 'workloads.json')
+
+
+def run_workload(dec, spec, av1b, frames=None):
+    """Decodes a full-size workload with `dec` frame by frame; returns per
+    frame [digest of the output planes, digest of the NV12 pack]."""
+    import refdec
+    config, seed, n, pitch = spec
+    stream = refdec.Stream(dec)
+    out = []
+    for k in range(n if frames is None else frames):
+        b = av1b.synth_frame(config, 1, seed, k)
+        w, _, h, _, _, _ = b.header
+        slot, planes = stream.decode(k, b)
+        out.append([digest(planes), digest([dec.to_nv12(slot, pitch, w, h)])])
+    for s in list(stream.slots.values()):
+        dec.release_reference(s)
+    return out
+
+
+def load_workloads():
+    with open(WORKLOAD_GOLDEN) as f:
+        return json.load(f)['workloads']

@@ -356,3 +356,18 @@ def test_nv12_split_pack(av1b, oracle, dec):
         dec.nv12_pack_wait(older[0])
     for s in list(sg.slots.values()):
         dec.release_reference(s)
+
+
+@pytest.mark.parametrize('name', [n for n, _ in golden_util.WORKLOADS])
+def test_full_size_workload_hashes(av1b, dec, name):
+    """The benchmark workloads at full size, every frame against the oracle's
+    hashes (tests/golden/workloads.json): config 1 (1280x720 8-bit, 30
+    frames), config 2 (1920x1080 10-bit, 60 frames, key frames at 0 and 30,
+    three-slot compound) and the exact GOP bench.py times (config 3, its seed,
+    30 frames)."""
+    spec = dict(golden_util.WORKLOADS)[name]
+    want = golden_util.load_workloads()[name]['frames']
+    got = golden_util.run_workload(dec, spec, av1b)
+    assert len(got) == len(want) == spec[2]
+    for k, (g, w) in enumerate(zip(got, want)):
+        assert g == w, '%s frame %d' % (name, k)
