@@ -136,13 +136,9 @@ __device__ void make_inter_job(const FrameArgs& a, const BlockRec& b, InterJob* 
  * blend, then the OBMC strips in order, each neighbour's prediction of the
  * strip through mc_rect. It carries none of the full kernel's state, so it
  * runs with a fraction of its registers and many more warps in flight. */
-__global__ void __launch_bounds__(128) k_inter_simple(const __grid_constant__ FrameArgs a) {
-  __shared__ McScratch scr[4];
-  __shared__ int pred[4][2][8 * 16];
-  const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int warp = blockIdx.x * 4 + wib;
-  if (warp >= a.n_inter_simple) return;
-  const int2 t = a.inter_tiles[warp];
+__device__ __forceinline__ void inter_simple_tile(const FrameArgs& a, int tile, McScratch& scr,
+                                                  int (&pred)[2][8 * 16], int lane) {
+  const int2 t = a.inter_tiles[tile];
   const BlockRec& b = a.blocks[t.x];
   const int p = b.plane;
   const PlaneGeom& g = a.L.p[p];
@@ -160,18 +156,18 @@ __global__ void __launch_bounds__(128) k_inter_simple(const __grid_constant__ Fr
   const int tmul = (65536 + tw - 1) / tw;
   const int nref = b.compound ? 2 : 1;
   for (int r = 0; r < nref; ++r) {
-    int* pr = pred[wib][r];
+    int* pr = pred[r];
     const px_t* ref = ref_plane(a, b.ref_slot[r], p);
     if (r == 0 ? b.warp0 : b.warp1) {
       /* one or two whole 8x8 warp blocks (x0 is a multiple of 16, y0 of 8) */
       const WarpRec& m = a.warps[b.warp_idx[r] >= 0 ? b.warp_idx[r] : 0];
       for (int bx = 0; bx < tw; bx += 8)
         warp_block8(c.sub_x, c.sub_y, c.ref_w, c.ref_h, m, ref, g.stride, b.x, b.y, x0 + bx, y0,
-                    c.bitdepth, b.compound != 0, scr[wib], pr + bx, 16, mini(8, tw - bx), th, lane);
+                    c.bitdepth, b.compound != 0, scr, pr + bx, 16, mini(8, tw - bx), th, lane);
       continue;
     }
     if (!mc_rect(c, ref, g.stride, b.x, b.y, b.w, b.h, b.mv[r][0], b.mv[r][1], b.filt, b.filt_v,
-                 b.compound != 0, x0, y0, tw, th, scr[wib], pr, lane)) {
+                 b.compound != 0, x0, y0, tw, th, scr, pr, lane)) {
       for (int k = lane; k < tw * th; k += 32) {
         const int yy = k / tw, xx = k - yy * tw;
         pr[yy * 16 + xx] = mc_tap(c, ref, g.stride, b.x, b.y, b.w, b.h, b.mv[r][0], b.mv[r][1],
@@ -188,12 +184,12 @@ __global__ void __launch_bounds__(128) k_inter_simple(const __grid_constant__ Fr
     const int k = lane + 32 * q;
     if (k >= tw * th) continue;
     const int yy = (k * tmul) >> 16, xx = k - yy * tw;
-    const int v0 = pred[wib][0][yy * 16 + xx];
+    const int v0 = pred[0][yy * 16 + xx];
     int out = v0;
     if (b.compound == 1) {
-      out = (v0 + pred[wib][1][yy * 16 + xx] + (1 << post)) >> (1 + post);
+      out = (v0 + pred[1][yy * 16 + xx] + (1 << post)) >> (1 + post);
     } else if (b.compound) {
-      out = (b.w0 * v0 + b.w1 * pred[wib][1][yy * 16 + xx] + (1 << (3 + post))) >> (4 + post);
+      out = (b.w0 * v0 + b.w1 * pred[1][yy * 16 + xx] + (1 << (3 + post))) >> (4 + post);
     }
     acc[q] = clampi(out, 0, a.maxv);
   }
@@ -204,10 +200,10 @@ __global__ void __launch_bounds__(128) k_inter_simple(const __grid_constant__ Fr
     const int ix0 = maxi(o.x, x0), ix1 = mini(o.x + o.w, x0 + tw);
     const int iy0 = maxi(o.y, y0), iy1 = mini(o.y + o.h, y0 + th);
     if (ix0 >= ix1 || iy0 >= iy1) continue;
-    int* tmp = pred[wib][0];
+    int* tmp = pred[0];
     const px_t* oref = ref_plane(a, o.ref_slot, p);
     const bool ok = mc_rect(c, oref, g.stride, b.x + o.x, b.y + o.y, o.w, o.h, o.mv_x, o.mv_y, o.filt,
-                            o.filt_v, 0, ix0 - o.x, iy0 - o.y, ix1 - ix0, iy1 - iy0, scr[wib], tmp,
+                            o.filt_v, 0, ix0 - o.x, iy0 - o.y, ix1 - ix0, iy1 - iy0, scr, tmp,
                             lane);
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
@@ -233,20 +229,25 @@ __global__ void __launch_bounds__(128) k_inter_simple(const __grid_constant__ Fr
   }
 }
 
+__global__ void __launch_bounds__(128) k_inter_simple(const __grid_constant__ FrameArgs a) {
+  __shared__ McScratch scr[4];
+  __shared__ int pred[4][2][8 * 16];
+  const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int warp = blockIdx.x * 4 + wib;
+  if (warp >= a.n_inter_simple) return;
+  inter_simple_tile(a, warp, scr[wib], pred[wib], lane);
+}
+
 /* Inter prediction of phase A blocks: one warp per 16x8 tile. Translation
  * predictions (and OBMC strips) go through mc_rect, warped ones through
  * warp_block8; the composition and the OBMC blends run per sample on
  * registers. A chroma tile whose compound mask is difference-weighted takes
  * its mask from the luma predictions of the area it covers (up to 32x16
  * luma samples), computed the same separable way into shared memory. */
-__global__ void __launch_bounds__(128, 4) k_inter(const __grid_constant__ FrameArgs a) {
-  __shared__ McScratch scr[4];
-  __shared__ int pred[4][2][8 * 16];
-  __shared__ int lpred[4][2][4 * 8 * 16];   /* luma predictions, four 16x8 quarters */
-  const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int warp = a.n_inter_simple + blockIdx.x * 4 + wib;
-  if (warp >= a.n_inter_tiles) return;
-  const int2 t = a.inter_tiles[warp];
+__device__ __forceinline__ void inter_full_tile(const FrameArgs& a, int tile, McScratch& scr,
+                                                int (&pred)[2][8 * 16],
+                                                int (&lpred)[2][4 * 8 * 16], int lane) {
+  const int2 t = a.inter_tiles[tile];
   const BlockRec& b = a.blocks[t.x];
   InterJob j;
   make_inter_job(a, b, &j);
@@ -268,18 +269,18 @@ __global__ void __launch_bounds__(128, 4) k_inter(const __grid_constant__ FrameA
   }
   const int nref = j.compound ? 2 : 1;
   for (int r = 0; r < nref; ++r) {
-    int* pr = pred[wib][r];
+    int* pr = pred[r];
     if (j.warp[r]) {
       /* the tile is one or two whole 8x8 warp blocks (x0 is a multiple of
        * 16, y0 of 8) */
       for (int bx = 0; bx < tw; bx += 8)
         warp_block8(j.ctx.sub_x, j.ctx.sub_y, j.ctx.ref_w, j.ctx.ref_h, *j.model[r], j.ref[r],
-                    j.ref_stride, j.x, j.y, x0 + bx, y0, j.ctx.bitdepth, j.compound != 0, scr[wib],
+                    j.ref_stride, j.x, j.y, x0 + bx, y0, j.ctx.bitdepth, j.compound != 0, scr,
                     pr + bx, 16, mini(8, tw - bx), th, lane);
       continue;
     }
     const bool ok = mc_rect(j.ctx, j.ref[r], j.ref_stride, j.x, j.y, j.w, j.h, j.mv[r][0],
-                            j.mv[r][1], j.filt, j.filt_v, j.compound != 0, x0, y0, tw, th, scr[wib],
+                            j.mv[r][1], j.filt, j.filt_v, j.compound != 0, x0, y0, tw, th, scr,
                             pr, lane);
     if (!ok) {
       for (int k = lane; k < tw * th; k += 32) {
@@ -304,16 +305,16 @@ __global__ void __launch_bounds__(128, 4) k_inter(const __grid_constant__ FrameA
     for (int r = 0; r < 2; ++r)
       for (int qy = 0; qy < lh; qy += 8)
         for (int qx = 0; qx < lw; qx += 16) {
-          int* out = lpred[wib][r] + ((qy >> 3) * 2 + (qx >> 4)) * 128;
+          int* out = lpred[r] + ((qy >> 3) * 2 + (qx >> 4)) * 128;
           const int rw = mini(16, lw - qx), rh = mini(8, lh - qy);
           if (j.mask_warp[r]) {
             for (int bx = 0; bx < rw; bx += 8)
               warp_block8(0, 0, j.luma_ref_w, j.luma_ref_h, *j.model[r], j.luma_ref[r],
                           j.luma_stride, j.luma_x, j.luma_y, lx0 + qx + bx, ly0 + qy,
-                          j.ctx.bitdepth, 1, scr[wib], out + bx, 16, mini(8, rw - bx), rh, lane);
+                          j.ctx.bitdepth, 1, scr, out + bx, 16, mini(8, rw - bx), rh, lane);
           } else if (!mc_rect(l, j.luma_ref[r], j.luma_stride, j.luma_x, j.luma_y, ew, eh,
                               j.mv[r][0], j.mv[r][1], j.filt, j.filt_v, 1, lx0 + qx, ly0 + qy, rw,
-                              rh, scr[wib], out, lane)) {
+                              rh, scr, out, lane)) {
             for (int k = lane; k < rw * rh; k += 32) {
               const int yy = k / rw, xx = k - yy * rw;
               out[yy * 16 + xx] = mc_tap(l, j.luma_ref[r], j.luma_stride, j.luma_x, j.luma_y, ew,
@@ -330,7 +331,7 @@ __global__ void __launch_bounds__(128, 4) k_inter(const __grid_constant__ FrameA
     const int k = lane + 32 * q;
     if (k < tw * th) {
       const int yy = (k * tmul) >> 16, xx = k - yy * tw;
-      const int v0 = pred[wib][0][yy * 16 + xx], v1 = nref > 1 ? pred[wib][1][yy * 16 + xx] : 0;
+      const int v0 = pred[0][yy * 16 + xx], v1 = nref > 1 ? pred[1][yy * 16 + xx] : 0;
       if (luma_mask) {
         /* the chroma sample's mask: the mean over the luma samples it covers */
         const int sh = 7 - (j.ctx.bitdepth >= 12 ? 5 : 3) + (j.ctx.bitdepth - 8);
@@ -340,7 +341,7 @@ __global__ void __launch_bounds__(128, 4) k_inter(const __grid_constant__ FrameA
           for (int ii = 0; ii < nx; ++ii) {
             const int lx = (xx << j.ctx.sub_x) + ii, ly = (yy << j.ctx.sub_y) + jj;
             const int idx = ((ly >> 3) * 2 + (lx >> 4)) * 128 + (ly & 7) * 16 + (lx & 15);
-            sum += diffwtd_m(absi(lpred[wib][0][idx] - lpred[wib][1][idx]), sh, j.mask_sign);
+            sum += diffwtd_m(absi(lpred[0][idx] - lpred[1][idx]), sh, j.mask_sign);
           }
         const int n = nx * ny;
         const int m = n == 1 ? sum : (n == 2 ? (sum + 1) >> 1 : (sum + 2) >> 2);
@@ -356,10 +357,10 @@ __global__ void __launch_bounds__(128, 4) k_inter(const __grid_constant__ FrameA
     const int ix0 = maxi(c.x, x0), ix1 = mini(c.x + c.w, x0 + tw);
     const int iy0 = maxi(c.y, y0), iy1 = mini(c.y + c.h, y0 + th);
     if (ix0 >= ix1 || iy0 >= iy1) continue;
-    int* tmp = pred[wib][0];
+    int* tmp = pred[0];
     const bool ok = mc_rect(j.ctx, j.obmc_ref[kk], j.ref_stride, j.x + c.x, j.y + c.y, c.w, c.h,
                             c.mv_x, c.mv_y, c.filt, c.filt_v, 0, ix0 - c.x, iy0 - c.y, ix1 - ix0,
-                            iy1 - iy0, scr[wib], tmp, lane);
+                            iy1 - iy0, scr, tmp, lane);
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       const int k = lane + 32 * q;
@@ -382,6 +383,16 @@ __global__ void __launch_bounds__(128, 4) k_inter(const __grid_constant__ FrameA
       dst[yy * g.stride + xx] = (px_t)acc[q];
     }
   }
+}
+
+__global__ void __launch_bounds__(128, 4) k_inter(const __grid_constant__ FrameArgs a) {
+  __shared__ McScratch scr[4];
+  __shared__ int pred[4][2][8 * 16];
+  __shared__ int lpred[4][2][4 * 8 * 16];   /* luma predictions, four 16x8 quarters */
+  const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int warp = a.n_inter_simple + blockIdx.x * 4 + wib;
+  if (warp >= a.n_inter_tiles) return;
+  inter_full_tile(a, warp, scr[wib], pred[wib], lpred[wib], lane);
 }
 
 /* Adds one transform's residual (or a raw residual block) to the picture. */
@@ -472,20 +483,21 @@ cudaError_t launch_dequant(const DqRec* jobs, int n, const short* levels, const 
  * precomputed buffer, so the dependency-scheduled kernel only predicts and
  * adds (the residual does not depend on the prediction). Raw residual blocks
  * (class 7) add with the whole warp. */
+/* Scratch ints a warp of class CLS needs. */
 template <int CLS>
-__global__ void __launch_bounds__(128) k_itx(const __grid_constant__ FrameArgs a, int first,
-                                             int count) {
-  extern __shared__ int smem[];
-  constexpr int S = 1 << (CLS < 7 ? CLS : 5), STEP = S < 32 ? S : 32;
-  constexpr int PER_WARP = CLS >= 6 ? 4096 : 32 * S;   /* scratch ints a warp */
-  const int wib = threadIdx.x >> 5;
-  const int bi = blockIdx.x * (blockDim.x >> 5) + wib;
-  const int lane = threadIdx.x & 31;
-  if (bi >= count) return;
-  const int4 bt = a.itx_batches[first + bi];   /* first job, jobs, class */
+struct ItxScratch {
+  static constexpr int S = 1 << (CLS < 7 ? CLS : 5);
+  static constexpr int PER_WARP = CLS >= 6 ? 4096 : 32 * S;
+};
+
+/* One batch of class CLS (`bt`: first job, jobs, class) with the warp's
+ * scratch `wsm`. */
+template <int CLS>
+__device__ __forceinline__ void itx_batch(const FrameArgs& a, const int4 bt, int* wsm, int lane) {
+  constexpr int S = ItxScratch<CLS>::S, STEP = S < 32 ? S : 32;
   if constexpr (CLS == 7) {
     const int2 t = a.itx_jobs[bt.x];
-    apply_tx<false>(a, a.blocks[t.x], a.txs[t.y], smem + wib * 4096, lane);
+    apply_tx<false>(a, a.blocks[t.x], a.txs[t.y], wsm, lane);
   } else {
     const int g = lane / STEP, sub = lane - g * STEP;
     const bool active = g < bt.y;
@@ -499,13 +511,24 @@ __global__ void __launch_bounds__(128) k_itx(const __grid_constant__ FrameArgs a
     p.lossless = b.lossless;
     p.row_shift = tx.row_shift;
     p.bitdepth = a.L.bit_depth;
-    int* tmp = smem + wib * PER_WARP + (S <= 32 ? g * S * S : 0);
+    int* tmp = wsm + (S <= 32 ? g * S * S : 0);
     const PlaneGeom& gm = a.L.p[b.plane];
     px_t* dst = a.cur + gm.off + (b.y + tx.y) * gm.stride + b.x + tx.x;
     int* res = tx.pre_off >= 0 ? a.pre_res + tx.pre_off : nullptr;
     itx_group_cls<CLS, false>(p, a.coef + tx.coef_off, tmp, dst, gm.stride, a.maxv, res, sub, STEP,
                               active);
   }
+}
+
+template <int CLS>
+__global__ void __launch_bounds__(128) k_itx(const __grid_constant__ FrameArgs a, int first,
+                                             int count) {
+  extern __shared__ int smem[];
+  const int wib = threadIdx.x >> 5;
+  const int bi = blockIdx.x * (blockDim.x >> 5) + wib;
+  const int lane = threadIdx.x & 31;
+  if (bi >= count) return;
+  itx_batch<CLS>(a, a.itx_batches[first + bi], smem + wib * ItxScratch<CLS>::PER_WARP, lane);
 }
 
 template <int CLS>
@@ -621,18 +644,12 @@ __device__ void add_residual_cg(const FrameArgs& a, const BlockRec& b, const TxR
 /* INTER: the frame has phase B inter blocks (inter-intra, intra block copy);
  * a frame of intra blocks only (every key frame) runs the instantiation
  * without the inter prediction code, a much smaller kernel. */
+/* Runs chain `c` of the frame: its blocks one after another, each after the
+ * blocks it waits for. `edges` and `tmp` are the warp's shared memory. */
 template <bool INTER>
-__global__ void __launch_bounds__(128) k_units(const __grid_constant__ FrameArgs a) {
-  extern __shared__ int smem[];
-  const int wib = threadIdx.x >> 5;
-  const int lane = threadIdx.x & 31;
-  int* edges = smem + wib * (3 * AV1B_EDGE_LEN + AV1B_UNIT_SCRATCH);
-  int* tmp = edges + 3 * AV1B_EDGE_LEN;
-  for (;;) {
-    int c = 0;
-    if (lane == 0) c = atomicAdd(a.queue, 1);
-    c = __shfl_sync(0xffffffffu, c, 0);
-    if (c >= a.n_chains) break;
+__device__ __forceinline__ void run_chain(const FrameArgs& a, int c, int* edges, int* tmp,
+                                          int lane) {
+  {
     const int u_end = a.chains[c + 1];
     int prev = -1;
     /* the next block's record is loaded while this one runs: in a chain the
@@ -767,16 +784,37 @@ __global__ void __launch_bounds__(128) k_units(const __grid_constant__ FrameArgs
   }
 }
 
+template <bool INTER>
+__global__ void __launch_bounds__(128) k_units(const __grid_constant__ FrameArgs a) {
+  extern __shared__ int smem[];
+  const int wib = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  int* edges = smem + wib * (3 * AV1B_EDGE_LEN + AV1B_UNIT_SCRATCH);
+  int* tmp = edges + 3 * AV1B_EDGE_LEN;
+  for (;;) {
+    int c = 0;
+    if (lane == 0) c = atomicAdd(a.queue, 1);
+    c = __shfl_sync(0xffffffffu, c, 0);
+    if (c >= a.n_chains) break;
+    run_chain<INTER>(a, c, edges, tmp, lane);
+  }
+}
+
 /* ---- deblocking ---------------------------------------------------------------------- */
+__device__ __forceinline__ void deblock_edge(px_t* pic, const DeblockRec& r, int sharpness, int bd,
+                                             int maxv, int lane) {
+  for (int k = lane; k < r.len; k += 32)
+    deblock_px(pic + r.p_off + k * r.along, r.across, r.level, sharpness, r.filter_size, r.chroma,
+               bd, maxv);
+}
+
 __global__ void k_deblock(px_t* pic, const DeblockRec* recs, int n, int sharpness, int bd,
                           int maxv) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= n) return;
   const DeblockRec r = recs[warp];
-  for (int k = lane; k < r.len; k += 32)
-    deblock_px(pic + r.p_off + k * r.along, r.across, r.level, sharpness, r.filter_size, r.chroma,
-               bd, maxv);
+  deblock_edge(pic, r, sharpness, bd, maxv, lane);
 }
 
 /* ---- CDEF ------------------------------------------------------------------------------ */
@@ -787,12 +825,9 @@ __global__ void k_deblock(px_t* pic, const DeblockRec* recs, int n, int sharpnes
  * 8x8 grid (result index = cell), the rest the listed positions off the grid
  * (result index grid_n + k). Chroma blocks read the search of their luma
  * block, so each luma block is searched once. */
-__global__ void __launch_bounds__(128) k_cdef_search(const px_t* __restrict__ src, int grid_w,
-                                                     int grid_n, int n_grid,
-                                                     const unsigned* __restrict__ pos, int n_extra,
-                                                     int* out, const __grid_constant__ Layout L) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n_grid + n_extra) return;
+__device__ __forceinline__ void cdef_search_one(const px_t* __restrict__ src, int grid_w, int grid_n,
+                                                int n_grid, const unsigned* __restrict__ pos,
+                                                int* out, const Layout& L, int t) {
   int x, y, o;
   if (t < n_grid) {
     y = (t / grid_w) << 3;
@@ -880,6 +915,15 @@ __global__ void __launch_bounds__(128) k_cdef_search(const px_t* __restrict__ sr
   out[o] = (((best - opp) >> 10) << 3) | d;
 }
 
+__global__ void __launch_bounds__(128) k_cdef_search(const px_t* __restrict__ src, int grid_w,
+                                                     int grid_n, int n_grid,
+                                                     const unsigned* __restrict__ pos, int n_extra,
+                                                     int* out, const __grid_constant__ Layout L) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n_grid + n_extra) return;
+  cdef_search_one(src, grid_w, grid_n, n_grid, pos, out, L, t);
+}
+
 __constant__ signed char kCdefDirs[8][2][2] = {
     {{-1, 1}, {-2, 2}}, {{0, 1}, {-1, 2}}, {{0, 1}, {0, 2}}, {{0, 1}, {1, 2}},
     {{1, 1}, {2, 2}},   {{1, 0}, {2, 1}},  {{1, 0}, {2, 0}}, {{1, 0}, {2, -1}},
@@ -932,23 +976,17 @@ __device__ __forceinline__ void cdef_samples(const int* win, px_t* d, int stride
   }
 }
 
-__global__ void __launch_bounds__(128) k_cdef(const px_t* __restrict__ src, px_t* dst,
-                                              const CdefRec* recs, int n,
-                                              const int* __restrict__ search,
-                                              const __grid_constant__ Layout L) {
-  __shared__ int sw[8][12 * 12];
-  const int hw = threadIdx.x >> 4, hl = threadIdx.x & 15;
-  const unsigned hmask = 0xffffu << (threadIdx.x & 16);
-  const int ri = blockIdx.x * 8 + hw;
-  if (ri >= n) return;
-  const CdefRec r = recs[ri];
+/* One CDEF record by a half-warp (lanes `hmask`, this thread `hl`) with its
+ * 12x12 window `win` in shared memory. */
+__device__ __forceinline__ void cdef_record(const px_t* __restrict__ src, px_t* dst,
+                                            const CdefRec& r, const int* __restrict__ search,
+                                            const Layout& L, int* win, int hl, unsigned hmask) {
   const int p = r.plane;
   const bool uv = p > 0;
   const PlaneGeom& g = L.p[p];
   const int bd = L.bit_depth, maxv = (1 << bd) - 1, cs = bd - 8;
   const int w = uv ? (8 >> L.ss_x) : 8, h = uv ? (8 >> L.ss_y) : 8;
   const int pw = g.grid_w, ph = g.grid_h;
-  int* win = sw[hw];
   /* the block and its halo; rows and columns above or left of the buffer
    * clamp into it (taps outside the plane are never used) */
   for (StepWalk wk(hl, 16, w + 4); wk.k < (h + 4) * (w + 4); wk.next()) {
@@ -1001,6 +1039,19 @@ __global__ void __launch_bounds__(128) k_cdef(const px_t* __restrict__ src, px_t
                        pt0, pt1, maxv);
 }
 
+__global__ void __launch_bounds__(128) k_cdef(const px_t* __restrict__ src, px_t* dst,
+                                              const CdefRec* recs, int n,
+                                              const int* __restrict__ search,
+                                              const __grid_constant__ Layout L) {
+  __shared__ int sw[8][12 * 12];
+  const int hw = threadIdx.x >> 4, hl = threadIdx.x & 15;
+  const unsigned hmask = 0xffffu << (threadIdx.x & 16);
+  const int ri = blockIdx.x * 8 + hw;
+  if (ri >= n) return;
+  const CdefRec r = recs[ri];
+  cdef_record(src, dst, r, search, L, sw[hw], hl, hmask);
+}
+
 /* ---- superres ------------------------------------------------------------------------- */
 /* One CTA of 64 threads per 256 output samples of a row, a thread per 4.
  * The source span those outputs read (a superres step is at most one source
@@ -1014,13 +1065,15 @@ __global__ void __launch_bounds__(128) k_cdef(const px_t* __restrict__ src, px_t
  * picture and reads only these. */
 #define AV1B_UP_OUT 256
 #define AV1B_UP_SPAN 288
-__global__ void __launch_bounds__(64) k_upscale(const px_t* __restrict__ src, px_t* dst,
-                                                const __grid_constant__ Layout L,
-                                                const __grid_constant__ UpscaleArgs u, int maxv,
-                                                int border_rows, int rows0) {
-  __shared__ __align__(16) short taps[512];
-  __shared__ px_t span[AV1B_UP_SPAN];
-  int y = blockIdx.y, p = 0, xb = blockIdx.x;
+/* One CTA item (segment xb of grid row yb): the caller has filled `taps`
+ * (the 64 filter phases); the body stages the source span, meets the CTA
+ * barrier and writes. Early returns are either uniform over the CTA or after
+ * its last barrier. */
+__device__ __forceinline__ void upscale_item(const px_t* __restrict__ src, px_t* dst, const Layout& L,
+                                             const UpscaleArgs& u, int maxv, int border_rows,
+                                             int rows0, int xb, int yb, const short* taps,
+                                             px_t* span) {
+  int y = yb, p = 0;
   if (y >= rows0) {
     y -= rows0;
     const int xb1 = (L.p[1].out_w + AV1B_UP_OUT - 1) / AV1B_UP_OUT;
@@ -1047,7 +1100,6 @@ __global__ void __launch_bounds__(64) k_upscale(const px_t* __restrict__ src, px
   const int p0 = (init + xs * step) >> 14;
   const int n = ((init + xe * step) >> 14) - p0 + 8;
   const bool staged = n <= AV1B_UP_SPAN;
-  for (int i = threadIdx.x; i < 512; i += blockDim.x) taps[i] = kUpscaleFilter[i];
   if (staged)
     for (int i = threadIdx.x; i < n; i += blockDim.x) span[i] = row[clampi(p0 - 3 + i, 0, last)];
   __syncthreads();
@@ -1085,6 +1137,16 @@ __global__ void __launch_bounds__(64) k_upscale(const px_t* __restrict__ src, px
   }
 }
 
+__global__ void __launch_bounds__(64) k_upscale(const px_t* __restrict__ src, px_t* dst,
+                                                const __grid_constant__ Layout L,
+                                                const __grid_constant__ UpscaleArgs u, int maxv,
+                                                int border_rows, int rows0) {
+  __shared__ __align__(16) short taps[512];
+  __shared__ px_t span[AV1B_UP_SPAN];
+  for (int i = threadIdx.x; i < 512; i += blockDim.x) taps[i] = kUpscaleFilter[i];
+  upscale_item(src, dst, L, u, maxv, border_rows, rows0, blockIdx.x, blockIdx.y, taps, span);
+}
+
 /* ---- loop restoration --------------------------------------------------------------------- */
 /* Loop restoration by tiles: one CTA per (plane, stripe piece, 32 columns).
  * A stripe piece is the rows of one 64-row luma stripe (offset by 8), so every
@@ -1103,16 +1165,25 @@ __global__ void __launch_bounds__(64) k_upscale(const px_t* __restrict__ src, px
 #define AV1B_LR_AR (AV1B_LR_MAXR + 2)
 #define AV1B_LR_AC (AV1B_LR_TW + 2)
 
-__global__ void __launch_bounds__(256) k_lr_tile(const px_t* __restrict__ cdef,
-                                                 const px_t* __restrict__ curr, px_t* dst,
-                                                 const __grid_constant__ Layout L,
-                                                 const __grid_constant__ LrArgs r, int maxv,
-                                                 int copy_rest) {
-  __shared__ int win[AV1B_LR_WR * AV1B_LR_WC];
-  __shared__ int aux[2][2][AV1B_LR_AR * AV1B_LR_AC];  /* Wiener: aux[0][0] = intermediate */
-  __shared__ short xbyx1[256];   /* a2 = ((z << 8) + z / 2) / (z + 1), by z */
+/* Shared memory of one loop restoration tile. */
+struct LrSmem {
+  int win[AV1B_LR_WR * AV1B_LR_WC];
+  int aux[2][2][AV1B_LR_AR * AV1B_LR_AC];  /* Wiener: aux[0][0] = intermediate */
+  short xbyx1[256];   /* a2 = ((z << 8) + z / 2) / (z + 1), by z */
+};
+
+/* One tile (bx, stripe, bz). Early returns are uniform over the CTA or after
+ * its last barrier. */
+__device__ __forceinline__ void lr_tile_item(const px_t* __restrict__ cdef,
+                                             const px_t* __restrict__ curr, px_t* dst,
+                                             const Layout& L, const LrArgs& r, int maxv,
+                                             int copy_rest, int bx, int stripe, int bz,
+                                             LrSmem& sm) {
+  int* win = sm.win;
+  auto& aux = sm.aux;
+  short* xbyx1 = sm.xbyx1;
   /* grid z: luma, then chroma with plane 1's tiles and plane 2's side by side */
-  int p = blockIdx.z, bx = blockIdx.x;
+  int p = bz;
   if (p > 0) {
     const int t1 = (L.p[1].out_w + AV1B_LR_TW - 1) / AV1B_LR_TW;
     if (bx >= t1) {
@@ -1125,7 +1196,6 @@ __global__ void __launch_bounds__(256) k_lr_tile(const px_t* __restrict__ cdef,
   const int x0 = bx * AV1B_LR_TW;
   if (x0 >= g.out_w) return;
   /* the stripe piece */
-  const int stripe = blockIdx.y;
   const int s0 = (-8 + stripe * 64) >> sub_y;
   const int s1 = s0 + (64 >> sub_y) - 1;
   const int y0 = maxi(s0, 0), y1 = mini(g.out_h, s1 + 1);
@@ -1265,6 +1335,15 @@ __global__ void __launch_bounds__(256) k_lr_tile(const px_t* __restrict__ cdef,
   }
 }
 
+__global__ void __launch_bounds__(256) k_lr_tile(const px_t* __restrict__ cdef,
+                                                 const px_t* __restrict__ curr, px_t* dst,
+                                                 const __grid_constant__ Layout L,
+                                                 const __grid_constant__ LrArgs r, int maxv,
+                                                 int copy_rest) {
+  __shared__ LrSmem sm;
+  lr_tile_item(cdef, curr, dst, L, r, maxv, copy_rest, blockIdx.x, blockIdx.y, blockIdx.z, sm);
+}
+
 /* ---- film grain ------------------------------------------------------------------------------- */
 
 /* Generates the three grain templates (7.18.3.3): Gaussian noise from the LFSR
@@ -1272,13 +1351,20 @@ __global__ void __launch_bounds__(256) k_lr_tile(const px_t* __restrict__ cdef,
  * filter as a wavefront: sample (x, y) depends on rows above within +-lag
  * columns and on the lag samples to its left, so t = x + 4y orders it
  * (lag <= 3). One block; luma first, then both chroma planes together. */
-__global__ void __launch_bounds__(256) k_grain_template(GrainState* gs, GrainParamsDev prm,
-                                                        const uint16_t* orbit,
-                                                        const uint16_t* pos) {
-  /* the templates live in shared memory while the auto-regressive wavefront
-   * runs (hundreds of dependent steps: every tap a shared-memory read, not a
-   * global one) and are written out at the end */
-  __shared__ short s_luma[82 * 73], s_cb[82 * 73], s_cr[82 * 73];
+/* The templates live in shared memory while the auto-regressive wavefront
+ * runs (hundreds of dependent steps: every tap a shared-memory read, not a
+ * global one) and are written out at the end. */
+struct GrainTemplateSmem {
+  short luma[82 * 73], cb[82 * 73], cr[82 * 73];
+};
+
+/* Every thread of the CTA runs it; it has no early return. */
+__device__ __forceinline__ void grain_template_body(GrainState* gs, const GrainParamsDev& prm,
+                                                    const uint16_t* orbit, const uint16_t* pos,
+                                                    GrainTemplateSmem& sm) {
+  short* s_luma = sm.luma;
+  short* s_cb = sm.cb;
+  short* s_cr = sm.cr;
   const int tid = threadIdx.x;
   const int bd = prm.bitdepth;
   const int shift = 12 - bd + prm.grain_scale_shift;
@@ -1374,6 +1460,13 @@ __global__ void __launch_bounds__(256) k_grain_template(GrainState* gs, GrainPar
     }
 }
 
+__global__ void __launch_bounds__(256) k_grain_template(GrainState* gs, GrainParamsDev prm,
+                                                        const uint16_t* orbit,
+                                                        const uint16_t* pos) {
+  __shared__ GrainTemplateSmem sm;
+  grain_template_body(gs, prm, orbit, pos, sm);
+}
+
 /* The stripe values of plane `p` (7.18.3.5, the horizontal half: the grain
  * block that covers the column, blended with the previous block at the two -
  * one for subsampled chroma - overlap columns) of four samples
@@ -1419,11 +1512,12 @@ __device__ __forceinline__ void grain_stripe4(const GrainState* gs, const short*
  * sample). Grid rows are the luma rows, then the chroma rows
  * with plane 1's groups and plane 2's side by side, so a chroma row of
  * 4:2:0 fills a grid row as a luma row does. */
-__global__ void k_grain_blend(const px_t* __restrict__ src, px_t* dst,
-                              const __grid_constant__ Layout L,
-                              const GrainState* gs, const uint16_t* orbit, const uint16_t* pos) {
-  int gi = blockIdx.x * blockDim.x + threadIdx.x;
-  int y = blockIdx.y, p = 0;
+/* One thread's four samples: group gi of grid row y (no barrier). */
+__device__ __forceinline__ void grain_blend_item(const px_t* __restrict__ src, px_t* dst,
+                                                 const Layout& L, const GrainState* gs,
+                                                 const uint16_t* orbit, const uint16_t* pos,
+                                                 int gi, int y) {
+  int p = 0;
   if (y >= L.p[0].out_h) {
     y -= L.p[0].out_h;
     const int g1 = (L.p[1].out_w + 3) >> 2;
@@ -1551,6 +1645,12 @@ __global__ void k_grain_blend(const px_t* __restrict__ src, px_t* dst,
   }
 }
 
+__global__ void k_grain_blend(const px_t* __restrict__ src, px_t* dst,
+                              const __grid_constant__ Layout L,
+                              const GrainState* gs, const uint16_t* orbit, const uint16_t* pos) {
+  grain_blend_item(src, dst, L, gs, orbit, pos, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y);
+}
+
 /* ---- output packing ---------------------------------------------------------------------------- */
 
 /* NV12: one thread per 8 output bytes of a `pitch`-byte row; rows [0, h) are
@@ -1560,10 +1660,9 @@ __global__ void k_grain_blend(const px_t* __restrict__ src, px_t* dst,
  * *coded* width into a display-sized frame that starts out zero
  * (cpu_backend.cpp:576-584), so for a superres frame every sample right of the
  * coded width packs as 0. This kernel reproduces that byte for byte. */
-__global__ void k_nv12(const px_t* __restrict__ pic, uint8_t* out, const __grid_constant__ Layout L,
-                       int pitch) {
-  const int row = blockIdx.y;
-  const int x0 = (blockIdx.x * blockDim.x + threadIdx.x) * 8;
+/* One thread's eight bytes at byte x0 of NV12 row `row` (no barrier). */
+__device__ __forceinline__ void nv12_item(const px_t* __restrict__ pic, uint8_t* out, const Layout& L,
+                                          int pitch, int x0, int row) {
   if (x0 >= pitch) return;
   const int w = L.p[0].out_w, h = L.p[0].out_h;
   const int shift = L.bit_depth - 8;
@@ -1594,6 +1693,11 @@ __global__ void k_nv12(const px_t* __restrict__ pic, uint8_t* out, const __grid_
   } else {
     for (int k = 0; k < 8 && x0 + k < pitch; ++k) d[k] = v[k];
   }
+}
+
+__global__ void k_nv12(const px_t* __restrict__ pic, uint8_t* out, const __grid_constant__ Layout L,
+                       int pitch) {
+  nv12_item(pic, out, L, pitch, (blockIdx.x * blockDim.x + threadIdx.x) * 8, blockIdx.y);
 }
 
 __global__ void k_rgb(const px_t* __restrict__ pic, uint8_t* out, const __grid_constant__ Layout L,

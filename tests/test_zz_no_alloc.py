@@ -212,12 +212,17 @@ def test_noalloc_subsampling_and_range_against_oracle(av1b, gpu, oracle, stream,
     b = _planted(av1b, payload, grain, restricted_identity)
     assert all(r < 0 for r in b.get_refs())   # a key frame: no references
     slot, mine = dec.decode(b)
+    # the frame decoded last reads as its output picture (after grain); a
+    # second decode makes `slot` an older slot, which reads as its stored
+    # picture (before grain)
+    again, _ = dec.decode(b)
     _, want = oracle.RefDecoder().decode(b)
-    w, _, h, bd, sx, sy = b.header
+    for p in range(3):
+        assert np.array_equal(mine[p], want[p]), '%s decoder plane %d' % (stream, p)
     for n in range(2):  # two calls in a row
         rc, got, _ = _apply(av1b, lib, torch, dec, b, slot)
         assert rc == 0
         for p in range(3):
             assert np.array_equal(got[p], want[p]), '%s call %d plane %d' % (stream, n, p)
-            assert np.array_equal(mine[p], want[p]), '%s decoder plane %d' % (stream, p)
     dec.release_reference(slot)
+    dec.release_reference(again)
