@@ -70,6 +70,16 @@ class PlanInfo(ctypes.Structure):
         return out
 
 
+class BatchConfig(ctypes.Structure):
+    """av1b_batch_config: the batched step's launch shape."""
+    _fields_ = [('ctas_per_sm', ctypes.c_int32 * 24), ('claim_chunk', ctypes.c_int32),
+                ('fuse_grain_nv12', ctypes.c_int32), ('use_graph', ctypes.c_int32)]
+
+    def as_dict(self):
+        return {'ctas_per_sm': list(self.ctas_per_sm)[:21], 'claim_chunk': self.claim_chunk,
+                'fuse_grain_nv12': self.fuse_grain_nv12, 'use_graph': self.use_graph}
+
+
 class Stats(ctypes.Structure):
     _fields_ = [('blocks', ctypes.c_int32), ('waves', ctypes.c_int32),
                 ('kernel_launches', ctypes.c_int32), ('reconstruct_ms', ctypes.c_double),
@@ -97,6 +107,20 @@ _SIGNATURES = {
     'av1b_plan_free': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     'av1b_sync': (ctypes.c_int, [ctypes.c_void_p]),
     'av1b_plan_stats': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    'av1b_batch_create': (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    'av1b_batch_destroy': (ctypes.c_int, [ctypes.c_void_p]),
+    'av1b_batch_decode': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                         ctypes.c_void_p, ctypes.c_void_p]),
+    'av1b_batch_sync': (ctypes.c_int, [ctypes.c_void_p]),
+    'av1b_batch_get_config': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    'av1b_batch_set_config': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    'av1b_batch_autotune': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                           ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                           ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int,
+                                           ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
+    'av1b_batch_last_error': (ctypes.c_char_p, [ctypes.c_void_p]),
+    'av1b_batch_stream': (ctypes.c_void_p, [ctypes.c_void_p]),
     'av1b_int_peak': (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     'av1b_set_profiling': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     'av1b_set_wait_limit': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong]),
@@ -476,6 +500,86 @@ class Decoder:
         s = Stats()
         self._check(lib().av1b_get_stats(self.h, ctypes.byref(s)), 'stats')
         return s
+
+
+class Batch:
+    """The batched form (av1b_batch_*): one planned frame of each of many
+    streams - each a Decoder of its own - decoded as one step of persistent
+    kernels replayed as a CUDA graph."""
+
+    MAX = 64
+
+    def __init__(self, device=0):
+        h = ctypes.c_void_p()
+        rc = lib().av1b_batch_create(device, ctypes.byref(h))
+        if rc:
+            raise Av1bError(rc, 'av1b_batch_create')
+        self.h = h
+
+    def close(self):
+        if getattr(self, 'h', None):
+            lib().av1b_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc, what):
+        if rc:
+            msg = lib().av1b_batch_last_error(self.h) or b''
+            raise Av1bError(rc, '%s: %s' % (what, msg.decode(errors='replace')))
+
+    @staticmethod
+    def _args(decoders, plans, slots, nv12):
+        n = len(decoders)
+        decs = (ctypes.c_void_p * n)(*[d.h.value for d in decoders])
+        pls = (ctypes.c_void_p * n)(*[p.value for p in plans])
+        sl = (ctypes.c_int * n)(*(slots if slots is not None else [-1] * n))
+        dst = pitch = length = None
+        if nv12 is not None:
+            dst = (ctypes.c_void_p * n)(*[x[0] if x else None for x in nv12])
+            pitch = (ctypes.c_size_t * n)(*[x[1] if x else 0 for x in nv12])
+            length = (ctypes.c_size_t * n)(*[x[2] if x else 0 for x in nv12])
+        return n, decs, pls, sl, dst, pitch, length
+
+    def decode(self, decoders, plans, slots=None, nv12=None):
+        """Queues one step: frame i = plans[i] on decoders[i] into slots[i]
+        (-1: lowest free); nv12[i] = (device pointer, pitch, bytes) or None.
+        Returns the slots."""
+        n, decs, pls, sl, dst, pitch, length = self._args(decoders, plans, slots, nv12)
+        out = (ctypes.c_int * n)()
+        self._check(lib().av1b_batch_decode(self.h, n, decs, pls, sl, out, dst, pitch, length),
+                    'batch_decode')
+        return list(out)
+
+    def sync(self):
+        self._check(lib().av1b_batch_sync(self.h), 'batch_sync')
+
+    def config(self):
+        c = BatchConfig()
+        self._check(lib().av1b_batch_get_config(self.h, ctypes.byref(c)), 'batch_get_config')
+        return c
+
+    def set_config(self, c):
+        self._check(lib().av1b_batch_set_config(self.h, ctypes.byref(c)), 'batch_set_config')
+
+    def autotune(self, decoders, plans, slots=None, nv12=None, cache_path=None, reps=3):
+        """Picks the launch shape for this set of streams (see av1b.h);
+        returns (config dict, best step ms or -1 when taken from the cache)."""
+        n, decs, pls, sl, dst, pitch, length = self._args(decoders, plans, slots, nv12)
+        c = BatchConfig()
+        ms = ctypes.c_double(0)
+        path = cache_path.encode() if cache_path else None
+        self._check(lib().av1b_batch_autotune(self.h, n, decs, pls, sl, dst, pitch, length, path,
+                                              reps, ctypes.byref(c), ctypes.byref(ms)),
+                    'batch_autotune')
+        return c.as_dict(), ms.value
+
+    def stream(self):
+        return lib().av1b_batch_stream(self.h)
 
 
 def int_peak(device=0, kind=0):

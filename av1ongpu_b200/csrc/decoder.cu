@@ -39,6 +39,7 @@
 #include "dev_inter.cuh"
 #include "dev_itx.cuh"
 #include "kernels.h"
+#include "batch.h"
 #include "work_pool.hpp"
 #include "plan_host.h"
 
@@ -113,6 +114,10 @@ struct av1b_decoder {
   DevBuf cdef_search;             /* CDEF direction search results */
   DevBuf pre_res;                 /* phase B residuals computed ahead */
   bool disp_is_cur = true;
+  /* a batched step applied the last frame's film grain inside its NV12 pack:
+   * the display picture is made from cur when an output call asks for it */
+  bool disp_pending = false;
+  cudaEvent_t ev_batch = nullptr;   /* a batched step's wait on this decoder's stream */
   DevBuf slot_buf[kSlots];
   bool slot_used[kSlots] = {false};
   bool slot_valid[kSlots] = {false};
@@ -427,6 +432,10 @@ struct Plan {
          n_cdef = 0,
          n_cdef_search = 0;
   int unit_depth = 0;             /* dependency depth of the frame */
+  /* chains by the depth of their first block: chains [depth_first[k],
+   * depth_first[k + 1]) start at depth k (a batched step interleaves the
+   * streams' chains by it) */
+  std::vector<int> depth_first;
   bool units_inter = false;       /* some phase B block is an inter kind */
   int itx_class_first[8] = {0}, itx_class_count[8] = {0};  /* batches per class */
   int cdef_grid_w = 0, cdef_grid_n = 0;  /* the grid of 8x8 luma searches */
@@ -887,6 +896,7 @@ int plan_units(av1b_decoder* d, const PlanCtx& c, Plan* P) {
   const Layout& L = c.L;
   P->R->deps.clear();
   P->n_chains = 0;
+  P->depth_first.clear();
   P->R->chains.clear();
   if (P->R->units.empty()) return AV1B_OK;
   PlanScratch& S = *c.scratch;
@@ -1137,6 +1147,7 @@ int plan_units(av1b_decoder* d, const PlanCtx& c, Plan* P) {
   }
   for (int k = 0; k <= max_depth; ++k) count[k + 1] += count[k];
   const size_t nch = static_cast<size_t>(count[max_depth + 1]);
+  P->depth_first.assign(count.begin(), count.end());
   std::vector<int>& cid = S.chain_id;  /* each block's chain, in claim order */
   std::vector<int>& clen = S.chain_len;
   cid.resize(nu);
@@ -2038,8 +2049,27 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
  * frame and check its status word before returning. */
 int finish_frame(av1b_decoder* d);
 
-int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, const av1b_planes* out,
-                 int* out_slot, bool sync) {
+/* One frame step's arguments: the destination slot, the reconstruction
+ * kernels' FrameArgs and (in a batched step) the filter chain's FilterArgs. */
+struct StepPrep {
+  int slot = -1;
+  int keep = 0;
+  int launches = 0;
+  FrameArgs a{};
+  FilterArgs f{};
+};
+
+int fill_filter_args(av1b_decoder* d, av1b_plan* pl, StepPrep* sp);
+
+/* The host side of a frame step before anything is launched: the
+ * destination slot, the buffers the frame needs, the done flags, claim
+ * counter and status word (reset on the decoder's stream), the slot table,
+ * and the arguments. In a batched step (`batched`) the film grain constants
+ * are uploaded on the decoder's stream as well, and the filter chain's
+ * arguments are filled for the batched kernels. Called with the decoder's
+ * lock held. */
+int prepare_step(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, bool batched,
+                 StepPrep* sp) {
   int rc;
   av1b_frame_syntax hdr{};
   hdr.width = pl->width;
@@ -2109,7 +2139,7 @@ int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, cons
   uint8_t* ar = static_cast<uint8_t*>(pl->arena.p);
 
   /* done flags, queue and status */
-  FrameArgs a{};
+  FrameArgs& a = sp->a;
   a.L = L;
   const size_t done_bytes =
       static_cast<size_t>(pl->n_blocks) * AV1B_FLAG_STRIDE * sizeof(unsigned) + 256;
@@ -2175,7 +2205,27 @@ int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, cons
   a.scale_x = P.scale_x;
   a.scale_y = P.scale_y;
   a.wait_ns = d->wait_ns;
+  sp->slot = slot;
+  sp->keep = keep;
+  if (batched) {
+    a.trace = nullptr;
+    if ((rc = fill_filter_args(d, pl, sp))) return rc;
+  }
+  return AV1B_OK;
+}
 
+/* The single-stream launch sequence of a prepared frame step on the
+ * decoder's stream (the grain templates on its side stream). */
+int launch_step_plain(av1b_decoder* d, av1b_plan* pl, StepPrep* sp) {
+  const Plan& P = pl->P;
+  const Layout& L = d->L;
+  const int maxv = (1 << pl->bit_depth) - 1;
+  cudaStream_t st = d->stream;
+  cudaEvent_t* ev = d->ev;
+  const FrameArgs& a = sp->a;
+  const int keep = sp->keep, slot = sp->slot;
+  const size_t pic_bytes = static_cast<size_t>(L.size) * sizeof(px_t);
+  uint8_t* ar = static_cast<uint8_t*>(pl->arena.p);
   int launches = 0;
   if (P.grain) {
     /* the grain templates depend only on the parameters: build them on the
@@ -2281,6 +2331,7 @@ int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, cons
        }), "reference store");
   const px_t* display = cur;
   d->disp_is_cur = true;
+  d->disp_pending = false;
   if (P.grain) {
     GrainState* gsd = static_cast<GrainState*>(d->grain_state.p);
     CK(cudaStreamWaitEvent(st, d->ev_join, 0), "join wait");
@@ -2294,6 +2345,24 @@ int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, cons
     d->disp_is_cur = false;
   }
   CK(cudaEventRecord(ev[2], st), "event");
+  sp->launches = launches;
+  return AV1B_OK;
+}
+
+/* After the launches of a frame step: the read back into `out`, the status
+ * word's copy, the stats, the plan's done event and the slot bookkeeping, on
+ * the decoder's stream - which first waits for `after` when the step ran on
+ * another stream (a batched step). Called with the decoder's lock held. */
+int commit_step(av1b_decoder* d, av1b_plan* pl, StepPrep* sp, const av1b_planes* out, int* out_slot,
+                bool sync, cudaEvent_t after) {
+  const Layout& L = d->L;
+  cudaStream_t st = d->stream;
+  const FrameArgs& a = sp->a;
+  const int keep = sp->keep, slot = sp->slot;
+  const int launches = sp->launches;
+  if (after) CK(cudaStreamWaitEvent(st, after, 0), "batch order");
+  const px_t* display = d->disp_is_cur ? static_cast<const px_t*>(d->cur.p)
+                                       : static_cast<const px_t*>(d->disp.p);
 
   /* ---- read back ---------------------------------------------------------------------------- */
   if (out) {
@@ -2311,7 +2380,7 @@ int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, cons
   d->stats.blocks = pl->n_blocks;
   d->stats.waves = 0;
   d->stats.kernel_launches = launches;
-  d->stats_pending = true;
+  d->stats_pending = launches > 0;   /* a batched step times itself */
   CK(cudaEventRecord(pl->done, st), "event");
   pl->in_flight = true;
   if (keep) {
@@ -2327,6 +2396,16 @@ int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, cons
   if (out_slot) *out_slot = slot;
   if (sync) return finish_frame(d);
   return AV1B_OK;
+}
+
+int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, const av1b_planes* out,
+                 int* out_slot, bool sync) {
+  StepPrep sp;
+  int rc;
+  if ((rc = prepare_step(d, pl, keep, forced_slot, false, &sp)) ||
+      (rc = launch_step_plain(d, pl, &sp)))
+    return rc;
+  return commit_step(d, pl, &sp, out, out_slot, sync, nullptr);
 }
 
 /* Frees a plan's buffers and events once no frame reads it any more. */
@@ -2390,6 +2469,16 @@ int run_frame(av1b_decoder* d, const av1b_frame_syntax& s, int keep, int forced_
 int picture_of(av1b_decoder* d, int slot, const px_t** pic) {
   if (slot < 0 || slot == d->last_slot) {
     if (!d->have_last) return fail(d, AV1B_ERR_ARG, "no frame to convert");
+    if (d->disp_pending) {
+      /* the output picture of a frame whose grain a batched step applied
+       * inside its NV12 pack: the blend from the frame's own grain state */
+      CK(launch_grain_blend(static_cast<const px_t*>(d->cur.p), static_cast<px_t*>(d->disp.p), d->L,
+                            static_cast<const GrainState*>(d->grain_state.p),
+                            static_cast<const uint16_t*>(d->orbit.p),
+                            static_cast<const uint16_t*>(d->pos.p), d->stream),
+         "film grain blend");
+      d->disp_pending = false;
+    }
     *pic = d->disp_is_cur ? static_cast<const px_t*>(d->cur.p) : static_cast<const px_t*>(d->disp.p);
     return AV1B_OK;
   }
@@ -2495,6 +2584,7 @@ int av1b_decoder_destroy(av1b_decoder* d) {
   if (d->ev_fork) cudaEventDestroy(d->ev_fork);
   if (d->ev_join) cudaEventDestroy(d->ev_join);
   if (d->ev_block) cudaEventDestroy(d->ev_block);
+  if (d->ev_batch) cudaEventDestroy(d->ev_batch);
   if (d->status_host) cudaFreeHost(d->status_host);
   for (auto& k : d->packs) {
     if (k.copied) cudaEventSynchronize(k.copied);
@@ -2926,3 +3016,6 @@ int av1b_profile(av1b_decoder* d, int stage, const char** name, double* total_ms
 const char* av1b_last_error(av1b_decoder* d) { return d ? d->err.c_str() : ""; }
 
 }  // extern "C"
+
+/* ---- batched form: many streams' frames in one step -------------------------------------- */
+#include "batch_runtime.cuh"

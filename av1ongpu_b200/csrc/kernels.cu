@@ -28,6 +28,7 @@
 #include "dev_intra.cuh"
 #include "dev_itx.cuh"
 #include "kernels.h"
+#include "batch.h"
 
 namespace av1b {
 
@@ -1063,7 +1064,6 @@ __global__ void __launch_bounds__(128) k_cdef(const px_t* __restrict__ src, px_t
  * boundary (the rows the restoration reads from the pre-CDEF picture,
  * av1gpu_kernels.h:2832-2845); the reference upscales the whole pre-CDEF
  * picture and reads only these. */
-#define AV1B_UP_OUT 256
 #define AV1B_UP_SPAN 288
 /* One CTA item (segment xb of grid row yb): the caller has filled `taps`
  * (the 64 filter phases); the body stages the source span, meets the CTA
@@ -1158,7 +1158,6 @@ __global__ void __launch_bounds__(64) k_upscale(const px_t* __restrict__ src, px
  * like the reference's) and a vertical pass. Self-guided computes A and B of
  * every box position the tile needs once - the reference recomputes them nine
  * times per output sample (av1gpu_kernels.h:2928-2970) - then projects. */
-#define AV1B_LR_TW 32
 #define AV1B_LR_MAXR 64
 #define AV1B_LR_WR (AV1B_LR_MAXR + 6)
 #define AV1B_LR_WC (AV1B_LR_TW + 6)
@@ -1512,40 +1511,17 @@ __device__ __forceinline__ void grain_stripe4(const GrainState* gs, const short*
  * sample). Grid rows are the luma rows, then the chroma rows
  * with plane 1's groups and plane 2's side by side, so a chroma row of
  * 4:2:0 fills a grid row as a luma row does. */
-/* One thread's four samples: group gi of grid row y (no barrier). */
-__device__ __forceinline__ void grain_blend_item(const px_t* __restrict__ src, px_t* dst,
-                                                 const Layout& L, const GrainState* gs,
-                                                 const uint16_t* orbit, const uint16_t* pos,
-                                                 int gi, int y) {
-  int p = 0;
-  if (y >= L.p[0].out_h) {
-    y -= L.p[0].out_h;
-    const int g1 = (L.p[1].out_w + 3) >> 2;
-    p = 1;
-    if (gi >= g1) {
-      gi -= g1;
-      p = 2;
-    }
-  }
-  const PlaneGeom& g = L.p[p];
-  const int x0 = gi * 4;
-  if (x0 >= g.out_w || y >= g.out_h) return;
-  const int idx = g.off + y * g.stride + x0;
-  const bool vec = ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15) == 0;
-  const int nq = min(4, g.out_w - x0);
-  int orig[4];
-  if (vec) {
-    const uint2 v = *reinterpret_cast<const uint2*>(src + idx);
-    orig[0] = v.x & 0xffff;
-    orig[1] = v.x >> 16;
-    orig[2] = v.y & 0xffff;
-    orig[3] = v.y >> 16;
-  } else {
-#pragma unroll
-    for (int q = 0; q < 4; ++q) orig[q] = q < nq ? src[idx + q] : 0;
-  }
+/* The film grain output of four samples x0 .. x0 + 3 (x0 a multiple of 4) of
+ * row y of plane p, from their decoded values `orig` (7.18.3.5); `src` is the
+ * picture before grain (a chroma sample reads its luma there), `vec` whether
+ * it is 16-byte aligned. */
+__device__ __forceinline__ void grain_group4(const px_t* __restrict__ src, const Layout& L,
+                                             const GrainState* gs, const uint16_t* orbit,
+                                             const uint16_t* pos, int p, int y, int x0, bool vec,
+                                             const int (&orig)[4], int (&out)[4]) {
   const int bd = gs->bitdepth;
-  int out[4] = {orig[0], orig[1], orig[2], orig[3]};
+#pragma unroll
+  for (int q = 0; q < 4; ++q) out[q] = orig[q];
   const bool active = p == 0 ? gs->num_points[0] > 0 : (gs->chroma_from_luma || gs->num_points[p] > 0);
   if (active) {
     const int sub_x = p ? L.ss_x : 0, sub_y = p ? L.ss_y : 0;
@@ -1633,6 +1609,42 @@ __device__ __forceinline__ void grain_blend_item(const px_t* __restrict__ src, p
       out[q] = clampi(orig[q] + scaled, gs->min_value, hi);
     }
   }
+}
+
+/* One thread's four samples: group gi of grid row y (no barrier). */
+__device__ __forceinline__ void grain_blend_item(const px_t* __restrict__ src, px_t* dst,
+                                                 const Layout& L, const GrainState* gs,
+                                                 const uint16_t* orbit, const uint16_t* pos,
+                                                 int gi, int y) {
+  int p = 0;
+  if (y >= L.p[0].out_h) {
+    y -= L.p[0].out_h;
+    const int g1 = (L.p[1].out_w + 3) >> 2;
+    p = 1;
+    if (gi >= g1) {
+      gi -= g1;
+      p = 2;
+    }
+  }
+  const PlaneGeom& g = L.p[p];
+  const int x0 = gi * 4;
+  if (x0 >= g.out_w || y >= g.out_h) return;
+  const int idx = g.off + y * g.stride + x0;
+  const bool vec = ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15) == 0;
+  const int nq = min(4, g.out_w - x0);
+  int orig[4];
+  if (vec) {
+    const uint2 v = *reinterpret_cast<const uint2*>(src + idx);
+    orig[0] = v.x & 0xffff;
+    orig[1] = v.x >> 16;
+    orig[2] = v.y & 0xffff;
+    orig[3] = v.y >> 16;
+  } else {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) orig[q] = q < nq ? src[idx + q] : 0;
+  }
+  int out[4];
+  grain_group4(src, L, gs, orbit, pos, p, y, x0, vec, orig, out);
   if (vec && nq == 4) {
     uint2 v;
     v.x = (unsigned)out[0] | ((unsigned)out[1] << 16);
@@ -1946,5 +1958,8 @@ cudaError_t set_kernel_attributes() {
   return cudaFuncSetAttribute(k_itx<7>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               4 * 4096 * (int)sizeof(int));
 }
+
+/* ---- batched form: the stage kernels of many streams ------------------------------------- */
+#include "batch_kernels.cuh"
 
 }  // namespace av1b

@@ -30,6 +30,10 @@ namespace av1b {
  * microseconds on the dependency path, more than the halved residency (two
  * CTAs a SM instead of four) costs. */
 #define AV1B_UNIT_SCRATCH 4096
+/* superres: output samples of a row a CTA writes; loop restoration: the
+ * columns of a tile */
+#define AV1B_UP_OUT 256
+#define AV1B_LR_TW 32
 #define AV1B_UNIT_CTAS_PER_SM 2
 
 struct FrameArgs {

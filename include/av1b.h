@@ -332,6 +332,66 @@ AV1B_API int av1b_unit_trace(av1b_decoder* dec, uint64_t* out, size_t cap, size_
  * own work after a decode without a host synchronisation. */
 AV1B_API void* av1b_decoder_stream(av1b_decoder* dec);
 
+/* --- batched form: many streams' frames in one step -------------------------
+ * No counterpart in the reference, which decodes one stream per Decoder
+ * (its nearest mechanism: the per-frame graph capture of its CUDA backend,
+ * src/backends/cuda/cuda_backend.cpp:1212-1227). A batch runs one planned
+ * frame of each of up to AV1B_BATCH_MAX independent streams - each stream its
+ * own decoder, with its own geometry, bit depth, reference slots and
+ * planners, all on the batch's device - as one step: persistent kernels, one
+ * per stage for all the streams, take the frames' work from device
+ * descriptors, and the step is replayed as a CUDA graph. Each stream's
+ * output is the same as decoding its frame alone (av1b_decode_planned).
+ *
+ * av1b_batch_decode queues frame i of the step as plans[i] decoded by
+ * decoders[i] into slots[i] (a reserved or held slot, -1: the lowest free
+ * one; the slot gets the picture as av1b_decode_planned with keep_reference
+ * does), and, when nv12_device[i] is non-null, its NV12 pack into that device
+ * buffer (nv12_pitch[i] bytes a row, nv12_len[i] bytes of room;
+ * av1b_nv12_size). out_slots[i] (nullable) gets the slot. A decoder appears
+ * at most once a step. The call returns when the step is queued on the
+ * batch's stream; the decoders' own streams are ordered after it, so their
+ * later calls see the step's results. av1b_batch_sync waits for the step and
+ * reports the first failed stream. */
+#define AV1B_BATCH_MAX 64
+typedef struct av1b_batch av1b_batch;
+/* The step's launch shape: CTAs per SM of each stage kernel (0: keep the
+ * current value; stages in launch order, 21 of them), the work items a warp
+ * claims at once, whether the film grain of a stream whose only output is
+ * its NV12 pack is applied inside the pack (its display picture is then made
+ * when an output call asks for it), and whether steps replay as a CUDA graph. */
+typedef struct av1b_batch_config {
+  int32_t ctas_per_sm[24];
+  int32_t claim_chunk;
+  int32_t fuse_grain_nv12;
+  int32_t use_graph;
+} av1b_batch_config;
+AV1B_API int av1b_batch_create(int device, av1b_batch** out);
+AV1B_API int av1b_batch_destroy(av1b_batch* batch);
+AV1B_API int av1b_batch_decode(av1b_batch* batch, int n, av1b_decoder* const* decoders,
+                               av1b_plan* const* plans, const int* slots, int* out_slots,
+                               uint8_t* const* nv12_device, const size_t* nv12_pitch,
+                               const size_t* nv12_len);
+AV1B_API int av1b_batch_sync(av1b_batch* batch);
+AV1B_API int av1b_batch_get_config(av1b_batch* batch, av1b_batch_config* out);
+AV1B_API int av1b_batch_set_config(av1b_batch* batch, const av1b_batch_config* config);
+/* The autotuner: picks the launch shape for a set of streams by timing the
+ * given step (decoded again and again: its slots must not be among the
+ * slots its frames read) with each candidate - CTAs per SM per stage group,
+ * the claim size, the grain-in-pack fusion - by coordinate descent, `reps`
+ * timed steps each. The result is kept in `cache_path` (nullable), one line
+ * per signature of the step (GPU, SM count, each stream's geometry, bit
+ * depth and tools), and a later call with the same signature takes it from
+ * there without timing (*best_ms = -1). The batch keeps the result. */
+AV1B_API int av1b_batch_autotune(av1b_batch* batch, int n, av1b_decoder* const* decoders,
+                                 av1b_plan* const* plans, const int* slots,
+                                 uint8_t* const* nv12_device, const size_t* nv12_pitch,
+                                 const size_t* nv12_len, const char* cache_path, int reps,
+                                 av1b_batch_config* out, double* best_ms);
+AV1B_API const char* av1b_batch_last_error(av1b_batch* batch);
+/* The CUDA stream the batch's steps run on (a cudaStream_t). */
+AV1B_API void* av1b_batch_stream(av1b_batch* batch);
+
 /* --- film grain without allocation -----------------------------------------
  * No counterpart in the reference: its film grain runs inside decode only.
  * For callers that cannot allocate device memory where they need a frame's
