@@ -93,6 +93,8 @@ _lib = None
 _SIGNATURES = {
     'av1b_syntax_view': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]),
     'av1b_decoder_create': (ctypes.c_int, [ctypes.c_int, ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p)]),
+    'av1b_decoder_create_ex': (ctypes.c_int, [ctypes.c_int, ctypes.c_size_t, ctypes.c_void_p,
+                                              ctypes.POINTER(ctypes.c_void_p)]),
     'av1b_decoder_destroy': (ctypes.c_int, [ctypes.c_void_p]),
     'av1b_decoder_reset': (ctypes.c_int, [ctypes.c_void_p]),
     'av1b_decode': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
@@ -318,9 +320,10 @@ def nv12_size(width, height, ss_x, ss_y, pitch):
 class Decoder:
     """av1gpu::Decoder on one CUDA device."""
 
-    def __init__(self, device=0, hbm_budget=0):
+    def __init__(self, device=0, hbm_budget=0, planners=0, planner_threads=0):
         h = ctypes.c_void_p()
-        rc = lib().av1b_decoder_create(device, hbm_budget, ctypes.byref(h))
+        opt = (ctypes.c_int32 * 2)(planners, planner_threads)
+        rc = lib().av1b_decoder_create_ex(device, hbm_budget, opt, ctypes.byref(h))
         if rc:
             raise Av1bError(rc, 'av1b_decoder_create')
         self.h = h

@@ -181,6 +181,8 @@ void default_tuning(BatchTuning* t) {
   for (int k = 0; k < kBStageCount; ++k) t->ctas_per_sm[k] = ctas[k];
   t->claim_chunk = 1;
   t->fuse_grain_nv12 = 0;
+  /* never more CTAs an SM than the kernel's resources let one SM hold */
+  for (int k = 0; k < kBStageCount; ++k) t->ctas_per_sm[k] = std::min(t->ctas_per_sm[k], batch_stage_max_ctas(k));
 }
 
 std::string tuning_key(const BatchTuning& t, bool units_inter) {
@@ -508,7 +510,6 @@ int av1b_batch_create(int device, av1b_batch** out) {
   b->device = device;
   cudaDeviceProp prop;
   if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) b->n_sm = prop.multiProcessorCount;
-  default_tuning(&b->tuning);
   bool ok = set_kernel_attributes() == cudaSuccess && set_batch_kernel_attributes() == cudaSuccess &&
             cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess &&
             cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) == cudaSuccess &&
@@ -519,6 +520,7 @@ int av1b_batch_create(int device, av1b_batch** out) {
             cudaMalloc(&b->d_steps, sizeof(StreamStep) * AV1B_BATCH_MAX) == cudaSuccess &&
             cudaMalloc(&b->d_hdr, sizeof(BatchHeader)) == cudaSuccess;
   for (auto& r : b->ring) ok = ok && cudaEventCreateWithFlags(&r.used, cudaEventDisableTiming) == cudaSuccess;
+  if (ok) default_tuning(&b->tuning);   /* after the kernels' attributes: it reads their occupancy */
   if (!ok) {
     av1b_batch_destroy(b);
     return AV1B_ERR_CUDA;

@@ -2501,7 +2501,15 @@ void copy_error(const av1b_decoder* d, char* error, size_t len) {
 extern "C" {
 
 int av1b_decoder_create(int device, size_t hbm_budget_bytes, av1b_decoder** out) {
+  return av1b_decoder_create_ex(device, hbm_budget_bytes, nullptr, out);
+}
+
+int av1b_decoder_create_ex(int device, size_t hbm_budget_bytes, const av1b_decoder_options* opt,
+                           av1b_decoder** out) {
   if (!out) return AV1B_ERR_ARG;
+  if (opt && (opt->planners < 0 || opt->planners > 8 || opt->planner_threads < 0 ||
+              opt->planner_threads > 64))
+    return AV1B_ERR_ARG;
   *out = nullptr;
   int n = 0;
   if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) return AV1B_ERR_NO_DEVICE;
@@ -2533,15 +2541,18 @@ int av1b_decoder_create(int device, size_t hbm_budget_bytes, av1b_decoder** out)
      * keep the device fed meanwhile) */
     const unsigned hc = std::thread::hardware_concurrency();
 #ifdef AV1B_PLANNER_THREADS
-    const int threads = AV1B_PLANNER_THREADS;
+    int threads = AV1B_PLANNER_THREADS;
     (void)hc;
 #else
-    const int threads = static_cast<int>(std::min(16u, std::max(2u, hc) - 1));
+    int threads = static_cast<int>(std::min(16u, std::max(2u, hc) - 1));
 #endif
 #ifndef AV1B_PLANNERS
 #define AV1B_PLANNERS 3
 #endif
-    d->planners.resize(AV1B_PLANNERS);
+    int planners = AV1B_PLANNERS;
+    if (opt && opt->planner_threads > 0) threads = opt->planner_threads;
+    if (opt && opt->planners > 0) planners = opt->planners;
+    d->planners.resize(planners);
     for (auto& q : d->planners) {
       q.pool = new WorkPool(threads);
       q.scratch = new PlanScratch;

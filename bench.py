@@ -77,6 +77,8 @@ def parse():
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-e2e', action='store_true', help='skip the end-to-end leg (profiling runs)')
     ap.add_argument('--no-verify', action='store_true', help='skip the bit-exact check (profiling runs)')
+    ap.add_argument('--no-batched', action='store_true', help='skip the batched leg')
+    ap.add_argument('--batch-frames', type=int, default=120, help='frames per stream, batched leg')
     return ap.parse_args()
 
 
@@ -537,6 +539,9 @@ def run_ours(args):
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         base = cpu_baseline(blobs, geo)
+    batched = None
+    if not args.no_batched:
+        batched = run_batched_leg(args, av1b, torch, local)
 
     for pl in plans:
         dec.free_plan(pl)
@@ -555,12 +560,149 @@ def run_ours(args):
             'clocks': clk, 'gpu_launches': launches_per_frame * F * args.steps,
             'peaks': {k: v for k, v in pk.items()},
             'stages': stages,
+            'batched': batched,
         }
         print(json.dumps(line))
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+# ---- batched form (config 4) ---------------------------------------------------------------
+# 16 streams: (width, height, bit depth, reference slots an inter frame draws from)
+BATCH_STREAMS = ([(640, 360, 8, 2)] * 4 + [(1280, 720, 8, 2)] * 6 + [(1920, 1080, 10, 3)] * 4 +
+                 [(3840, 2160, 10, 3)] * 2)
+BATCH_KEY = 60
+
+
+def plan_streams(av1b, decs, rings, streams, frames, seed0):
+    """Every stream's frames planned into device memory (generated and
+    planned on all host cores; a frame's blob is dropped once planned)."""
+    plans = [[None] * frames for _ in streams]
+
+    def one(job):
+        i, k = job
+        w, h, bd, refs = streams[i]
+        b = av1b.synth_frame_ex(w, h, 0, bd, 64, av1b.TOOLS_ALL, seed0 + 1000 * i, k, BATCH_KEY,
+                                max_refs=refs)
+        d = b.get_refs()
+        b.set_refs([rings[i][(k - x) % 4] for x in d])
+        plans[i][k] = decs[i].plan(b)
+
+    jobs = [(i, k) for k in range(frames) for i in range(len(streams))]
+    with ThreadPoolExecutor(max_workers=max(2, (os.cpu_count() or 2) // 2)) as ex:
+        list(ex.map(one, jobs))
+    return plans
+
+
+def run_batched_leg(args, av1b, torch, local):
+    """Aggregate megapixels/s of the 16 mixed streams: one at a time through
+    the plain path, and together through the batched form (autotuned, one
+    CUDA graph replay a frame-set), device-resident plans in both."""
+    streams = BATCH_STREAMS
+    F = args.batch_frames
+    decs = [av1b.Decoder(local, planners=1, planner_threads=2) for _ in streams]
+    rings = [[d.reserve_reference() for _ in range(4)] for d in decs]
+    t0 = time.perf_counter()
+    plans = plan_streams(av1b, decs, rings, streams, F, 4000)
+    plan_s = time.perf_counter() - t0
+    nv = []
+    for (w, h, bd, _r) in streams:
+        pitch = (w + 63) // 64 * 64
+        n = av1b.nv12_size(w, h, 1, 1, pitch)
+        nv.append((torch.empty(n, dtype=torch.uint8, device='cuda:%d' % local), pitch, n))
+    mpx = sum(w * h for (w, h, _b, _r) in streams) * F / 1e6
+
+    def plain(frames):
+        for i, d in enumerate(decs):
+            for k in frames:
+                s = rings[i][k % 4]
+                d.decode_planned(plans[i][k], slot=s, keep=True, wait=False)
+                d.to_nv12_device(s, nv[i][1], nv[i][0].data_ptr(), nv[i][2])
+            d.sync()
+
+    batch = av1b.Batch(local)
+    bstream = torch.cuda.ExternalStream(batch.stream(), device=local)
+
+    def batched(frames):
+        for k in frames:
+            batch.decode(decs, [plans[i][k] for i in range(len(streams))],
+                         slots=[r[k % 4] for r in rings],
+                         nv12=[(t.data_ptr(), p, n) for t, p, n in nv])
+        batch.sync()
+
+    # bit exactness: the first two frame-sets (key frames, then inter frames)
+    # batched against plain, every stream's NV12 byte for byte
+    exact = True
+    for k in range(min(2, F)):
+        plain([k])
+        want = [t.clone() for t, _p, _n in nv]
+        for t, _p, _n in nv:
+            t.zero_()
+        batched([k])
+        exact = exact and all(torch.equal(a, t) for a, (t, _p, _n) in zip(want, nv))
+    # the autotuner, on the inter frame-set 1 (its references are frame 0's)
+    tuned, tune_ms = None, None
+    default_ms = None
+    if F >= 2:
+        cache = os.environ.get('AV1B_TUNE_CACHE') or os.path.join(tempfile.gettempdir(),
+                                                                 'av1b_batch_tuning.txt')
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(bstream)
+        for _ in range(3):
+            batched([1])
+        e1.record(bstream)
+        torch.cuda.synchronize()
+        default_ms = e0.elapsed_time(e1) / 3
+        tuned, tune_ms = batch.autotune(decs, [plans[i][1] for i in range(len(streams))],
+                                        slots=[r[1] for r in rings],
+                                        nv12=[(t.data_ptr(), p, n) for t, p, n in nv],
+                                        cache_path=cache, reps=3)
+    frames = list(range(F))
+    plain(frames[:2])  # warm-up
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in decs]
+    torch.cuda.synchronize()
+    for i, d in enumerate(decs):
+        st = torch.cuda.ExternalStream(d.stream(), device=local)
+        ev[i][0].record(st)
+        for k in frames:
+            s = rings[i][k % 4]
+            d.decode_planned(plans[i][k], slot=s, keep=True, wait=False)
+            d.to_nv12_device(s, nv[i][1], nv[i][0].data_ptr(), nv[i][2])
+        ev[i][1].record(st)
+        d.sync()
+    plain_ms = sum(a.elapsed_time(b) for a, b in ev)
+    batched(frames[:2])  # warm-up (graph captured)
+    b0 = torch.cuda.Event(enable_timing=True)
+    b1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    b0.record(bstream)
+    batched(frames)
+    b1.record(bstream)
+    torch.cuda.synchronize()
+    batch_ms = b0.elapsed_time(b1)
+    for i, d in enumerate(decs):
+        for pl in plans[i]:
+            d.free_plan(pl)
+        d.close()
+    batch.close()
+    return {
+        'metric': 'batched Mpx/s vs plain path (16 mixed streams)', 'unit': 'Mpx/s',
+        'value': mpx / (batch_ms / 1e3), 'plain_value': mpx / (plain_ms / 1e3),
+        'speedup': plain_ms / batch_ms, 'bitexact_vs_plain': exact,
+        'bitexact_frames': '%d streams x %d frame-sets' % (len(streams), min(2, F)),
+        'frames_per_stream': F, 'key_interval': BATCH_KEY, 'mpx': mpx,
+        'batched_ms': batch_ms, 'plain_ms': plain_ms,
+        'ms_per_frame_set': batch_ms / F, 'plain_ms_per_frame_set': plain_ms / F,
+        'streams': '4x 640x360 8-bit, 6x 1280x720 8-bit, 4x 1920x1080 10-bit, 2x 3840x2160 10-bit; '
+                   'all tools, 64x64 SB, 2 (8-bit) / 3 (10-bit) reference slots, NV12 out',
+        'plan_s': plan_s, 'autotune': {'config': tuned, 'best_step_ms': tune_ms,
+                                       'default_step_ms': default_ms},
+        'timing': 'device (CUDA events): plain = sum over streams decoded one at a time, each on '
+                  'its decoder stream; batched = one graph replay a frame-set on the batch stream',
+    }
 
 
 def cpu_baseline(blobs, geo, frames=3):

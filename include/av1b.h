@@ -183,6 +183,17 @@ AV1B_API int av1b_syntax_view(const uint8_t* blob, size_t len, av1b_frame_syntax
  * allocate (0: no cap). A missing device is an error (AV1B_ERR_NO_DEVICE):
  * there is no CPU path in this library. */
 AV1B_API int av1b_decoder_create(int device, size_t hbm_budget_bytes, av1b_decoder** out);
+/* The same with the decoder's host planning resources set: `planners` frames
+ * planned at once (1..8; 0: 3) by `planner_threads` host threads each
+ * (0: all cores but one, at most 16). A process decoding many streams - the
+ * batched and served forms - gives each decoder one or two planners of a few
+ * threads, so the streams' planners together do not oversubscribe the host. */
+typedef struct av1b_decoder_options {
+  int32_t planners;
+  int32_t planner_threads;
+} av1b_decoder_options;
+AV1B_API int av1b_decoder_create_ex(int device, size_t hbm_budget_bytes,
+                                    const av1b_decoder_options* options, av1b_decoder** out);
 AV1B_API int av1b_decoder_destroy(av1b_decoder* dec);
 /* Decoder::reset (engine.cpp:65-71): drops every slot. */
 AV1B_API int av1b_decoder_reset(av1b_decoder* dec);
