@@ -2726,6 +2726,32 @@ int av1b_plan_stats(const av1b_plan* pl, av1b_plan_info* out) {
   return AV1B_OK;
 }
 
+size_t av1b_stream_hbm_estimate(int width, int height, int coded_width, int bit_depth, int ss_x,
+                                 int ss_y, int n_slots, int plans) {
+  if (width <= 0 || height <= 0 || n_slots < 0 || plans < 0) return 0;
+  const Layout L = make_layout(width, height, coded_width > 0 ? coded_width : width, bit_depth, ss_x,
+                               ss_y);
+  const size_t pic = static_cast<size_t>(L.size) * sizeof(px_t);
+  const int cw = coded_width > 0 ? coded_width : width;
+  const size_t nc = static_cast<size_t>(cw) * height +
+                    2 * static_cast<size_t>((cw + ss_x) >> ss_x) * ((height + ss_y) >> ss_y);
+  /* pictures: the one reconstructed, the snapshot, the display picture, the
+   * two loop restoration sources, and the reference slots; per sample: the
+   * phase B residuals (4 B) and the done flags (128 B a block, blocks of 16
+   * samples or more); per plan: its records, coefficient pool and filter
+   * lists (at most 10 B a coded sample); 1 MB of small buffers */
+  return (5 + static_cast<size_t>(n_slots)) * pic + 12 * nc + static_cast<size_t>(plans) * 10 * nc +
+         (1u << 20);
+}
+
+int av1b_decoder_memory(av1b_decoder* d, size_t* allocated, size_t* budget) {
+  if (!d) return AV1B_ERR_ARG;
+  std::lock_guard<std::mutex> lk(d->alloc_mu);
+  if (allocated) *allocated = d->allocated;
+  if (budget) *budget = d->budget;
+  return AV1B_OK;
+}
+
 int av1b_sync(av1b_decoder* d) {
   if (!d) return AV1B_ERR_ARG;
   std::lock_guard<std::mutex> lk(d->mu);
@@ -2934,7 +2960,17 @@ int av1b_get_stats(av1b_decoder* d, av1b_stats* out) {
 
 int av1b_poll_status(av1b_decoder* d, int* status) {
   if (!d || !status) return AV1B_ERR_ARG;
-  *status = 0;
+  std::lock_guard<std::mutex> lk(d->mu);
+  cudaSetDevice(d->device);
+  /* the status word of the frames whose work has finished: its copy into
+   * page-locked memory is queued after each frame */
+  const cudaError_t q = cudaStreamQuery(d->stream);
+  if (q != cudaSuccess && q != cudaErrorNotReady) return cuda_fail(d, q, "status poll");
+  *status = *static_cast<volatile int*>(d->status_host);
+  if (q == cudaSuccess && *status) {
+    *d->status_host = 0;
+    CK(cudaMemsetAsync(static_cast<uint8_t*>(d->status_q.p) + 64, 0, sizeof(int), d->stream), "status clear");
+  }
   return AV1B_OK;
 }
 

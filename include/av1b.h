@@ -248,6 +248,15 @@ AV1B_API int av1b_plan_stats(const av1b_plan* plan, av1b_plan_info* out);
 /* Waits for queued work and reports a device-side failure of the last frame. */
 AV1B_API int av1b_sync(av1b_decoder* dec);
 
+/* The device memory a decoder needs for a stream of this geometry with
+ * `n_slots` reference slots and `plans` frames planned ahead at once - an
+ * upper bound for frames whose blocks are 4x4 or larger - and what a decoder
+ * holds now against its budget. A server admitting streams by HBM sizes
+ * each stream's decoder budget with the first and checks the second. */
+AV1B_API size_t av1b_stream_hbm_estimate(int width, int height, int coded_width, int bit_depth,
+                                         int ss_x, int ss_y, int n_slots, int plans);
+AV1B_API int av1b_decoder_memory(av1b_decoder* dec, size_t* allocated, size_t* budget);
+
 /* Decoder::reserve_reference / decode_reference_reserved (av1gpu.hpp:645-661). */
 AV1B_API int av1b_reserve_reference(av1b_decoder* dec, int* out_slot);
 AV1B_API int av1b_decode_reserved(av1b_decoder* dec, const av1b_frame_syntax* syntax, int slot,
@@ -402,6 +411,69 @@ AV1B_API int av1b_batch_autotune(av1b_batch* batch, int n, av1b_decoder* const* 
 AV1B_API const char* av1b_batch_last_error(av1b_batch* batch);
 /* The CUDA stream the batch's steps run on (a cudaStream_t). */
 AV1B_API void* av1b_batch_stream(av1b_batch* batch);
+
+/* --- served form: a request loop over many streams --------------------------
+ * No counterpart in the reference (its nearest mechanisms: the pipelined
+ * plan / decode API, av1gpu.hpp:656-689, and its DirectShow filter's job
+ * loop for one stream, dsfilter/decode_core.hpp:47-68). A server admits
+ * streams by the device memory their decoder needs (their HBM budget is
+ * reserved at av1b_server_open, which refuses with AV1B_ERR_NOMEM when it
+ * does not fit; av1b_server_close returns it), plans frame requests on host
+ * threads as they arrive, and runs the planned frames of all streams in
+ * batched steps (av1b_batch_*) as they become ready: continuous batching, one
+ * frame a stream a step, at most max_inflight steps queued on the GPU.
+ *
+ * A request is a serialized FrameSyntax (av1b_syntax_view) whose
+ * reference_slots hold frame *distances* within its stream (1 = the
+ * previous frame submitted on it, at most max_refs); the server maps them to
+ * the stream's device slots. A stream's first frame reads no reference.
+ * Results come back through av1b_server_poll in completion order: the
+ * frame's arrival and device-completion times on the host clock (ms since
+ * the server started) and their difference, and its NV12 pack in device
+ * memory (a ring of eight buffers a stream: valid until eight more frames
+ * of the stream complete). `status` is a failure of the frame's planning or
+ * launch; a device-side failure surfaces at av1b_server_drain, which waits
+ * for every submitted frame and checks every decoder. */
+typedef struct av1b_server av1b_server;
+typedef struct av1b_server_options {
+  int32_t device;
+  int32_t max_batch;        /* frames a step (1..64; 0: 64) */
+  int32_t max_inflight;     /* steps queued on the GPU at once (1..8; 0: 2) */
+  int32_t planner_threads;  /* host threads planning requests (0: cores - 2) */
+  size_t hbm_budget;        /* device memory the streams may hold (0: 90 % of the free memory) */
+} av1b_server_options;
+typedef struct av1b_stream_desc {
+  int32_t width, height, coded_width, bit_depth, ss_x, ss_y;
+  int32_t max_refs;         /* reference frames a frame may read (1..7) */
+  int32_t nv12_pitch;       /* 0: no NV12 output */
+} av1b_stream_desc;
+typedef struct av1b_server_result {
+  int32_t stream_id, status, slot, batch_size;
+  uint64_t tag, frame_index;
+  int64_t step;
+  double arrival_ms, done_ms, latency_ms;
+  const uint8_t* nv12_device;
+  size_t nv12_bytes;
+} av1b_server_result;
+typedef struct av1b_server_stats {
+  uint64_t submitted, completed, steps, stepped_frames;
+  size_t hbm_used, hbm_budget;
+  int32_t streams;
+  double now_ms;
+} av1b_server_stats;
+AV1B_API int av1b_server_create(const av1b_server_options* options, av1b_server** out);
+AV1B_API int av1b_server_destroy(av1b_server* server);
+AV1B_API int av1b_server_open(av1b_server* server, const av1b_stream_desc* desc, int* stream_id,
+                              size_t* hbm_bytes);
+AV1B_API int av1b_server_close(av1b_server* server, int stream_id);
+AV1B_API int av1b_server_submit(av1b_server* server, int stream_id, const uint8_t* blob, size_t len,
+                                uint64_t tag);
+AV1B_API int av1b_server_poll(av1b_server* server, av1b_server_result* out, int max, int wait_ms,
+                              int* n);
+AV1B_API int av1b_server_drain(av1b_server* server, int timeout_ms);
+AV1B_API int av1b_server_get_stats(av1b_server* server, av1b_server_stats* out);
+/* The server's batch (an av1b_batch*), e.g. to set or tune its launch shape. */
+AV1B_API void* av1b_server_batch(av1b_server* server);
 
 /* --- film grain without allocation -----------------------------------------
  * No counterpart in the reference: its film grain runs inside decode only.
