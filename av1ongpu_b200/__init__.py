@@ -80,6 +80,23 @@ class BatchConfig(ctypes.Structure):
                 'fuse_grain_nv12': self.fuse_grain_nv12, 'use_graph': self.use_graph}
 
 
+class ServerResult(ctypes.Structure):
+    """av1b_server_result: one completed frame of the served form."""
+    _fields_ = [('stream_id', ctypes.c_int32), ('status', ctypes.c_int32), ('slot', ctypes.c_int32),
+                ('batch_size', ctypes.c_int32), ('tag', ctypes.c_uint64),
+                ('frame_index', ctypes.c_uint64), ('step', ctypes.c_int64),
+                ('arrival_ms', ctypes.c_double), ('done_ms', ctypes.c_double),
+                ('latency_ms', ctypes.c_double), ('nv12_device', ctypes.c_void_p),
+                ('nv12_bytes', ctypes.c_size_t)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [('submitted', ctypes.c_uint64), ('completed', ctypes.c_uint64),
+                ('steps', ctypes.c_uint64), ('stepped_frames', ctypes.c_uint64),
+                ('hbm_used', ctypes.c_size_t), ('hbm_budget', ctypes.c_size_t),
+                ('streams', ctypes.c_int32), ('now_ms', ctypes.c_double)]
+
+
 class Stats(ctypes.Structure):
     _fields_ = [('blocks', ctypes.c_int32), ('waves', ctypes.c_int32),
                 ('kernel_launches', ctypes.c_int32), ('reconstruct_ms', ctypes.c_double),
@@ -122,6 +139,21 @@ _SIGNATURES = {
                                            ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int,
                                            ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
     'av1b_batch_last_error': (ctypes.c_char_p, [ctypes.c_void_p]),
+    'av1b_server_create': (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
+    'av1b_server_destroy': (ctypes.c_int, [ctypes.c_void_p]),
+    'av1b_server_open': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
+                                        ctypes.POINTER(ctypes.c_size_t)]),
+    'av1b_server_close': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    'av1b_server_submit': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t,
+                                          ctypes.c_uint64]),
+    'av1b_server_poll': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                        ctypes.POINTER(ctypes.c_int)]),
+    'av1b_server_drain': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    'av1b_server_get_stats': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    'av1b_server_batch': (ctypes.c_void_p, [ctypes.c_void_p]),
+    'av1b_stream_hbm_estimate': (ctypes.c_size_t, [ctypes.c_int] * 8),
+    'av1b_decoder_memory': (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_size_t),
+                                           ctypes.POINTER(ctypes.c_size_t)]),
     'av1b_batch_stream': (ctypes.c_void_p, [ctypes.c_void_p]),
     'av1b_int_peak': (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     'av1b_set_profiling': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
@@ -583,6 +615,77 @@ class Batch:
 
     def stream(self):
         return lib().av1b_batch_stream(self.h)
+
+
+class Server:
+    """The served form (av1b_server_*): streams admitted by HBM, frame
+    requests planned as they arrive and run in continuously batched steps."""
+
+    def __init__(self, device=0, max_batch=0, max_inflight=0, planner_threads=0, hbm_budget=0):
+        opt = (ctypes.c_int32 * 4)(device, max_batch, max_inflight, planner_threads)
+        buf = ctypes.create_string_buffer(bytes(opt) + bytes(ctypes.c_size_t(hbm_budget)))
+        h = ctypes.c_void_p()
+        rc = lib().av1b_server_create(buf, ctypes.byref(h))
+        if rc:
+            raise Av1bError(rc, 'av1b_server_create')
+        self.h = h
+
+    def close(self):
+        if getattr(self, 'h', None):
+            lib().av1b_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def open(self, width, height, bit_depth, coded_width=0, ss_x=1, ss_y=1, max_refs=3,
+             nv12_pitch=0):
+        """Admits a stream; returns (stream id, HBM bytes reserved). Raises
+        Av1bError(-3) when it does not fit the server's budget now."""
+        desc = (ctypes.c_int32 * 8)(width, height, coded_width, bit_depth, ss_x, ss_y, max_refs,
+                                    nv12_pitch)
+        sid = ctypes.c_int(-1)
+        hbm = ctypes.c_size_t(0)
+        rc = lib().av1b_server_open(self.h, desc, ctypes.byref(sid), ctypes.byref(hbm))
+        if rc:
+            raise Av1bError(rc, 'server_open')
+        return sid.value, hbm.value
+
+    def close_stream(self, sid):
+        rc = lib().av1b_server_close(self.h, sid)
+        if rc:
+            raise Av1bError(rc, 'server_close')
+
+    def submit(self, sid, blob, tag=0):
+        rc = lib().av1b_server_submit(self.h, sid, blob.ptr, blob.size, tag)
+        if rc:
+            raise Av1bError(rc, 'server_submit')
+
+    def poll(self, max_results=256, wait_ms=0):
+        out = (ServerResult * max_results)()
+        n = ctypes.c_int(0)
+        rc = lib().av1b_server_poll(self.h, out, max_results, wait_ms, ctypes.byref(n))
+        if rc:
+            raise Av1bError(rc, 'server_poll')
+        return [out[i] for i in range(n.value)]
+
+    def drain(self, timeout_ms=60000):
+        rc = lib().av1b_server_drain(self.h, timeout_ms)
+        if rc:
+            raise Av1bError(rc, 'server_drain')
+
+    def stats(self):
+        st = ServerStats()
+        rc = lib().av1b_server_get_stats(self.h, ctypes.byref(st))
+        if rc:
+            raise Av1bError(rc, 'server_stats')
+        return st
+
+    def batch_handle(self):
+        return lib().av1b_server_batch(self.h)
 
 
 def int_peak(device=0, kind=0):

@@ -49,7 +49,8 @@ constexpr int kMaxRefs = 7;
 struct Request {
   int stream = -1;
   uint64_t tag = 0, index = 0;
-  std::vector<uint8_t> blob;
+  const uint8_t* blob = nullptr;   /* the caller's, read until the frame is planned */
+  size_t len = 0;
   double arrival_ms = 0;
   av1b_plan* plan = nullptr;
   int plan_rc = AV1B_OK;
@@ -77,6 +78,7 @@ struct Step {
   cudaEvent_t ev = nullptr;
   std::vector<Request*> reqs;
   std::vector<int> slots;
+  std::vector<int> rcs;          /* each frame's launch */
   int launch_rc = AV1B_OK;
 };
 
@@ -123,24 +125,30 @@ void plan_loop(av1b_server* s) {
       s->plan_q.pop_front();
       st = s->streams[r->stream];
     }
-    /* references: frame distances -> the stream's ring of slots */
+    /* a view into the caller's blob, its references (frame distances)
+     * mapped to the stream's ring of slots in an array of its own, so the
+     * blob is only read (several streams may share one) */
     int rc = AV1B_OK;
+    av1b_frame_syntax view;
     int32_t refs[8];
-    const int n = av1b_blob_get_refs(r->blob.data(), r->blob.size(), refs, 8);
-    if (n < 0 || n > 8) rc = AV1B_ERR_SYNTAX;
-    for (int i = 0; rc == AV1B_OK && i < n; ++i) {
-      if (refs[i] < 0) continue;   /* an unused entry */
-      if (refs[i] < 1 || static_cast<uint64_t>(refs[i]) > r->index || refs[i] >= st->ring_n) {
+    if (av1b_syntax_view(r->blob, r->len, &view) || view.n_reference_slots > 8) rc = AV1B_ERR_SYNTAX;
+    for (size_t i = 0; rc == AV1B_OK && i < view.n_reference_slots; ++i) {
+      const int32_t dist = view.reference_slots[i];
+      if (dist < 0) {
+        refs[i] = -1;   /* an unused entry */
+        continue;
+      }
+      if (dist < 1 || static_cast<uint64_t>(dist) > r->index || dist >= st->ring_n) {
         rc = AV1B_ERR_SYNTAX;
         break;
       }
-      refs[i] = st->ring[(r->index - refs[i]) % st->ring_n];
+      refs[i] = st->ring[(r->index - dist) % st->ring_n];
     }
-    av1b_frame_syntax view;
-    if (rc == AV1B_OK && av1b_blob_set_refs(r->blob.data(), r->blob.size(), refs, n)) rc = AV1B_ERR_SYNTAX;
-    if (rc == AV1B_OK && av1b_syntax_view(r->blob.data(), r->blob.size(), &view)) rc = AV1B_ERR_SYNTAX;
-    if (rc == AV1B_OK) rc = av1b_plan_frame(st->dec, &view, &r->plan);
-    std::vector<uint8_t>().swap(r->blob);   /* the plan holds its own copy on the device */
+    if (rc == AV1B_OK) {
+      view.reference_slots = refs;
+      /* returns once the frame's records and coefficients are on the device */
+      rc = av1b_plan_frame(st->dec, &view, &r->plan);
+    }
     {
       std::lock_guard<std::mutex> lk(s->mu);
       r->planned = true;
@@ -251,6 +259,15 @@ void sched_loop(av1b_server* s) {
     }
     step->launch_rc = av1b_batch_decode(s->batch, n, decs.data(), plans.data(), slots.data(), out.data(),
                                         nv.data(), pitch.data(), len.data());
+    step->rcs.assign(n, step->launch_rc);
+    if (step->launch_rc != AV1B_OK && n > 1) {
+      /* a frame the step could not take (checked before anything was
+       * launched) fails alone: the others run as steps of their own */
+      step->launch_rc = AV1B_OK;
+      for (int i = 0; i < n; ++i)
+        step->rcs[i] = av1b_batch_decode(s->batch, 1, &decs[i], &plans[i], &slots[i], &out[i], &nv[i],
+                                         &pitch[i], &len[i]);
+    }
     step->slots = out;
     cudaEventRecord(step->ev, s->bstream);
     {
@@ -285,7 +302,7 @@ void done_loop(av1b_server* s) {
       const int n = static_cast<int>(step->reqs.size());
       for (int i = 0; i < n; ++i) {
         Request* r = step->reqs[i];
-        post_result(s, r, rc, done_ms, step->slots[i], n, step->id);
+        post_result(s, r, rc != AV1B_OK ? rc : step->rcs[i], done_ms, step->slots[i], n, step->id);
         --s->streams[r->stream]->in_steps;
       }
       s->completed += n;
@@ -474,7 +491,8 @@ int av1b_server_submit(av1b_server* s, int id, const uint8_t* blob, size_t len, 
   auto* r = new Request;
   r->arrival_ms = now_ms(s);
   r->tag = tag;
-  r->blob.assign(blob, blob + len);
+  r->blob = blob;
+  r->len = len;
   {
     std::lock_guard<std::mutex> lk(s->mu);
     if (id < 0 || id >= static_cast<int>(s->streams.size()) || !s->streams[id] || !s->streams[id]->open) {

@@ -79,6 +79,8 @@ def parse():
     ap.add_argument('--no-verify', action='store_true', help='skip the bit-exact check (profiling runs)')
     ap.add_argument('--no-batched', action='store_true', help='skip the batched leg')
     ap.add_argument('--batch-frames', type=int, default=120, help='frames per stream, batched leg')
+    ap.add_argument('--no-serve', action='store_true', help='skip the served leg')
+    ap.add_argument('--serve-seconds', type=float, default=1.5, help='arrival window per load point')
     return ap.parse_args()
 
 
@@ -542,6 +544,9 @@ def run_ours(args):
     batched = None
     if not args.no_batched:
         batched = run_batched_leg(args, av1b, torch, local)
+    serving = None
+    if not args.no_serve and world == 1:
+        serving = run_serving_leg(args, av1b, local)
 
     for pl in plans:
         dec.free_plan(pl)
@@ -561,6 +566,7 @@ def run_ours(args):
             'peaks': {k: v for k, v in pk.items()},
             'stages': stages,
             'batched': batched,
+            'serving': serving,
         }
         print(json.dumps(line))
     if dist is not None:
@@ -702,6 +708,131 @@ def run_batched_leg(args, av1b, torch, local):
                                        'default_step_ms': default_ms},
         'timing': 'device (CUDA events): plain = sum over streams decoded one at a time, each on '
                   'its decoder stream; batched = one graph replay a frame-set on the batch stream',
+    }
+
+
+# ---- served form (config 5) -----------------------------------------------------------------
+# 64 streams: (width, height, bit depth, reference slots), how many
+SERVE_CLASSES = [((640, 360, 8, 2), 19), ((1280, 720, 8, 2), 22), ((1920, 1080, 10, 3), 16),
+                 ((3840, 2160, 10, 3), 7)]
+SERVE_GOP = 30          # each stream cycles through a 30-frame group (key frame first)
+SERVE_LOADS = (0.25, 0.5, 0.75, 1.0, 1.2)
+
+
+def percentile(v, q):
+    if not v:
+        return None
+    v = sorted(v)
+    return v[min(len(v) - 1, int(round(q / 100.0 * (len(v) - 1))))]
+
+
+def run_serving_leg(args, av1b, local):
+    """The request loop over 64 streams: Poisson arrivals at 30 or 60 frames/s
+    a stream, scaled so that the offered load sweeps 25 %..120 % of the
+    served capacity (a saturation run first); p50 / p99 of each frame's
+    latency (arrival to device completion) and the delivered Mpx/s."""
+    import random
+    streams = []
+    for (geo, count) in SERVE_CLASSES:
+        streams += [geo] * count
+    classes = sorted(set(streams))
+    with ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as ex:
+        pools = {}
+        for c, (w, h, bd, refs) in enumerate(classes):
+            pools[(w, h, bd, refs)] = list(ex.map(
+                lambda k: av1b.synth_frame_ex(w, h, 0, bd, 64, av1b.TOOLS_ALL, 5000 + c, k, SERVE_GOP,
+                                              max_refs=refs), range(SERVE_GOP)))
+    srv = av1b.Server(local, max_inflight=2, planner_threads=max(2, (os.cpu_count() or 4) // 2))
+    sids = []
+    for (w, h, bd, refs) in streams:
+        sid, _ = srv.open(w, h, bd, max_refs=refs, nv12_pitch=(w + 63) // 64 * 64)
+        sids.append(sid)
+    fps = [30 if j % 2 == 0 else 60 for j in range(len(streams))]
+    px = [w * h for (w, h, _b, _r) in streams]
+    natural = sum(f * p for f, p in zip(fps, px)) / 1e6
+    index = [0] * len(streams)
+    cls_name = {(640, 360, 8, 2): '360p', (1280, 720, 8, 2): '720p', (1920, 1080, 10, 3): '1080p',
+                (3840, 2160, 10, 3): '2160p'}
+
+    def run(events):
+        """Submits (time s, stream) events at their times; returns the results."""
+        out = []
+        tags = {}
+        t0 = time.perf_counter()
+        for t, j in events:
+            while True:
+                dt = t0 + t - time.perf_counter()
+                if dt <= 0:
+                    break
+                time.sleep(dt if dt > 0.0005 else 0)
+            k = index[j]
+            index[j] += 1
+            tag = len(tags)
+            tags[tag] = j
+            srv.submit(sids[j], pools[streams[j]][k % SERVE_GOP], tag=tag)
+            if tag % 64 == 0:
+                out += srv.poll(4096)
+        srv.drain(120000)
+        out += srv.poll(1 << 16)
+        while True:
+            more = srv.poll(1 << 16)
+            if not more:
+                break
+            out += more
+        return out, tags
+
+    def summarize(res, tags, offered):
+        lat = [r.latency_ms for r in res if r.status == 0]
+        first = min(r.arrival_ms for r in res)
+        last = max(r.done_ms for r in res)
+        mpx = sum(px[tags[r.tag]] for r in res if r.status == 0) / 1e6
+        by = {}
+        for r in res:
+            by.setdefault(cls_name[streams[tags[r.tag]]], []).append(r.latency_ms)
+        return {'offered_mpx_s': offered, 'delivered_mpx_s': mpx / ((last - first) / 1e3),
+                'frames': len(res), 'failed': sum(1 for r in res if r.status != 0),
+                'p50_ms': percentile(lat, 50), 'p99_ms': percentile(lat, 99),
+                'mean_batch': sum(r.batch_size for r in res) / max(1, len(res)),
+                'by_class': {c: {'p50_ms': percentile(v, 50), 'p99_ms': percentile(v, 99),
+                                 'frames': len(v)} for c, v in sorted(by.items())}}
+
+    # bring every stream to steady state (key frames, planner and plan pools)
+    run([(0.0, j) for j in range(len(streams))])
+    # capacity: every stream's next 30 frames at once, as fast as they can go
+    burst = [(0.0, j) for _ in range(SERVE_GOP) for j in range(len(streams))]
+    res, tags = run(burst)
+    cap = summarize(res, tags, None)
+    capacity = cap['delivered_mpx_s']
+    sweep = []
+    rng = random.Random(11)
+    duration = args.serve_seconds
+    for load in SERVE_LOADS:
+        alpha = load * capacity / natural
+        events = []
+        for j in range(len(streams)):
+            t = rng.expovariate(alpha * fps[j])
+            while t < duration:
+                events.append((t, j))
+                t += rng.expovariate(alpha * fps[j])
+        events.sort()
+        res, tags = run(events)
+        row = summarize(res, tags, load * capacity)
+        row['load'] = load
+        sweep.append(row)
+    st = srv.stats()
+    srv.close()
+    at100 = [r for r in sweep if r['load'] == 1.0]
+    return {
+        'metric': 'p50/p99 frame ms and delivered Mpx/s (64 streams, Poisson arrivals)',
+        'streams': '19x 640x360 8-bit, 22x 1280x720 8-bit, 16x 1920x1080 10-bit, 7x 3840x2160 10-bit; '
+                   'all tools, key frame every %d, half at 30 and half at 60 frames/s, NV12 out'
+                   % SERVE_GOP,
+        'latency': 'arrival (submit) to the device completion of the frame\'s step, host clock; '
+                   'host planning included',
+        'capacity_mpx_s': capacity, 'capacity_run': cap, 'natural_load_mpx_s': natural,
+        'seconds_per_load': duration, 'sweep': sweep,
+        'p99_1080p_ms_at_100': at100[0]['by_class'].get('1080p', {}).get('p99_ms') if at100 else None,
+        'steps': st.steps, 'frames': st.completed, 'hbm_reserved_gb': st.hbm_used / 1e9,
     }
 
 

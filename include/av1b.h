@@ -426,7 +426,10 @@ AV1B_API void* av1b_batch_stream(av1b_batch* batch);
  * A request is a serialized FrameSyntax (av1b_syntax_view) whose
  * reference_slots hold frame *distances* within its stream (1 = the
  * previous frame submitted on it, at most max_refs); the server maps them to
- * the stream's device slots. A stream's first frame reads no reference.
+ * the stream's device slots. A stream's first frame reads no reference. The
+ * server reads the caller's bytes in place, never writing them (streams may
+ * share a buffer): they must stay unchanged until the frame's result has
+ * been polled.
  * Results come back through av1b_server_poll in completion order: the
  * frame's arrival and device-completion times on the host clock (ms since
  * the server started) and their difference, and its NV12 pack in device
