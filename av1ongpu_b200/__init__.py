@@ -139,6 +139,9 @@ _SIGNATURES = {
                                            ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int,
                                            ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
     'av1b_batch_last_error': (ctypes.c_char_p, [ctypes.c_void_p]),
+    'av1b_batch_set_profiling': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    'av1b_batch_profile': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                          ctypes.POINTER(ctypes.c_longlong)]),
     'av1b_server_create': (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
     'av1b_server_destroy': (ctypes.c_int, [ctypes.c_void_p]),
     'av1b_server_open': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
@@ -615,6 +618,25 @@ class Batch:
 
     def stream(self):
         return lib().av1b_batch_stream(self.h)
+
+    STAGES = ('inter_simple', 'inter', 'itx4', 'itx8', 'itx16', 'itx32', 'itx64', 'itx_raw', 'units',
+              'deblock_v', 'deblock_h', 'copy_snapshot', 'cdef_search', 'cdef', 'copy_post_cdef',
+              'upscale', 'lr', 'copy_reference', 'grain_template', 'grain_blend', 'nv12')
+
+    def set_profiling(self, on):
+        self._check(lib().av1b_batch_set_profiling(self.h, 1 if on else 0), 'batch_set_profiling')
+
+    def profile(self):
+        """{stage: total ms} over the steps timed, and the step count."""
+        out, n = {}, 0
+        for k, name in enumerate(self.STAGES):
+            ms = ctypes.c_double(0)
+            steps = ctypes.c_longlong(0)
+            self._check(lib().av1b_batch_profile(self.h, k, ctypes.byref(ms), ctypes.byref(steps)),
+                        'batch_profile')
+            out[name] = ms.value
+            n = steps.value
+        return out, n
 
 
 class Server:

@@ -124,7 +124,7 @@ int batch_stage_max_ctas(int stage);
  * inter blocks. */
 cudaError_t launch_batch_step(const StreamStep* steps, BatchHeader* hdr, const BatchTuning& t,
                               int n_sm, bool units_inter, cudaStream_t s, cudaStream_t side,
-                              cudaEvent_t fork, cudaEvent_t join);
+                              cudaEvent_t fork, cudaEvent_t join, cudaEvent_t* prof = nullptr);
 
 }  // namespace av1b
 

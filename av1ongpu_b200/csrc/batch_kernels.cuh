@@ -349,11 +349,18 @@ static void launch_kb_itx(const StreamStep* steps, BatchHeader* hdr, const Batch
       steps, hdr, t.claim_chunk);
 }
 
+/* With `prof` (kBStageCount + 2 events), stage k's launch is bracketed by
+ * prof[k] and the next stage's event on `s`, prof[kBStageCount] ends the
+ * step, and prof[kBStageCount + 1] ends the grain templates on `side` (they
+ * start at prof[0]). */
 cudaError_t launch_batch_step(const StreamStep* steps, BatchHeader* hdr, const BatchTuning& t,
                               int n_sm, bool units_inter, cudaStream_t s, cudaStream_t side,
-                              cudaEvent_t fork, cudaEvent_t join) {
+                              cudaEvent_t fork, cudaEvent_t join, cudaEvent_t* prof) {
   cudaError_t e;
   const int chunk = t.claim_chunk > 0 ? t.claim_chunk : 1;
+  auto mark = [&](int k) {
+    if (prof) cudaEventRecord(prof[k], k == kBStageCount + 1 ? side : s);
+  };
   /* the claim counters restart every step */
   if ((e = cudaMemsetAsync(hdr->claim, 0, sizeof(hdr->claim), s)) != cudaSuccess) return e;
   /* the grain templates depend only on the parameters: a side branch, joined
@@ -361,33 +368,55 @@ cudaError_t launch_batch_step(const StreamStep* steps, BatchHeader* hdr, const B
   if ((e = cudaEventRecord(fork, s)) != cudaSuccess || (e = cudaStreamWaitEvent(side, fork, 0)) != cudaSuccess)
     return e;
   kb_grain_template<<<batch_grid(t, kBGrainTemplate, n_sm), 256, 0, side>>>(steps, hdr);
+  mark(kBStageCount + 1);
   if ((e = cudaEventRecord(join, side)) != cudaSuccess) return e;
+  mark(kBInterSimple);
   kb_inter_simple<<<batch_grid(t, kBInterSimple, n_sm), 128, 0, s>>>(steps, hdr, chunk);
+  mark(kBInter);
   kb_inter<<<batch_grid(t, kBInter, n_sm), 128, 0, s>>>(steps, hdr, chunk);
+  mark(kBItx2);
   launch_kb_itx<2>(steps, hdr, t, n_sm, s);
+  mark(kBItx3);
   launch_kb_itx<3>(steps, hdr, t, n_sm, s);
+  mark(kBItx4);
   launch_kb_itx<4>(steps, hdr, t, n_sm, s);
+  mark(kBItx5);
   launch_kb_itx<5>(steps, hdr, t, n_sm, s);
+  mark(kBItx6);
   launch_kb_itx<6>(steps, hdr, t, n_sm, s);
+  mark(kBItx7);
   launch_kb_itx<7>(steps, hdr, t, n_sm, s);
+  mark(kBUnits);
   {
     const size_t smem = 4 * (3 * AV1B_EDGE_LEN + AV1B_UNIT_SCRATCH) * sizeof(int);
     const int grid = mini(batch_grid(t, kBUnits, n_sm), AV1B_UNIT_CTAS_PER_SM * n_sm);
     if (units_inter) kb_units<true><<<grid, 128, smem, s>>>(steps, hdr);
     else kb_units<false><<<grid, 128, smem, s>>>(steps, hdr);
   }
+  mark(kBDeblockV);
   kb_deblock<<<batch_grid(t, kBDeblockV, n_sm), 256, 0, s>>>(steps, hdr, 1, chunk);
+  mark(kBDeblockH);
   kb_deblock<<<batch_grid(t, kBDeblockH, n_sm), 256, 0, s>>>(steps, hdr, 0, chunk);
+  mark(kBCopySnap);
   kb_copy<<<batch_grid(t, kBCopySnap, n_sm), 256, 0, s>>>(steps, hdr, 0);
+  mark(kBCdefSearch);
   kb_cdef_search<<<batch_grid(t, kBCdefSearch, n_sm), 128, 0, s>>>(steps, hdr);
+  mark(kBCdef);
   kb_cdef<<<batch_grid(t, kBCdef, n_sm), 128, 0, s>>>(steps, hdr);
+  mark(kBCopyPost);
   kb_copy<<<batch_grid(t, kBCopyPost, n_sm), 256, 0, s>>>(steps, hdr, 1);
+  mark(kBUpscale);
   kb_upscale<<<batch_grid(t, kBUpscale, n_sm), 64, 0, s>>>(steps, hdr);
+  mark(kBLr);
   kb_lr<<<batch_grid(t, kBLr, n_sm), 256, 0, s>>>(steps, hdr);
+  mark(kBCopyRef);
   kb_copy<<<batch_grid(t, kBCopyRef, n_sm), 256, 0, s>>>(steps, hdr, 2);
   if ((e = cudaStreamWaitEvent(s, join, 0)) != cudaSuccess) return e;
+  mark(kBGrain);
   kb_grain_blend<<<batch_grid(t, kBGrain, n_sm), 128, 0, s>>>(steps, hdr);
+  mark(kBNv12);
   kb_nv12<<<batch_grid(t, kBNv12, n_sm), 128, 0, s>>>(steps, hdr);
+  mark(kBStageCount);
   return cudaGetLastError();
 }
 

@@ -145,6 +145,12 @@ struct av1b_batch {
   };
   std::vector<Graph> graphs;
   std::vector<av1b_decoder*> last;   /* the decoders of the last step */
+  /* per-stage timing (av1b_batch_set_profiling): a set of events a step,
+   * summed when the batch is synchronized */
+  bool profiling = false;
+  std::vector<std::vector<cudaEvent_t>> prof_free, prof_pending;
+  double prof_ms[av1b::kBStageCount] = {0};
+  long long prof_n = 0;
   std::mutex mu;
   std::string err;
 };
@@ -362,7 +368,18 @@ int batch_step(av1b_batch* b, int n, av1b_decoder* const* decs, av1b_plan* const
         "chain upload");
   BCK(cudaEventRecord(stg.used, b->stream), "staging event");
   stg.pending = true;
-  if (b->use_graph) {
+  if (b->profiling) {
+    if (b->prof_free.empty()) {
+      std::vector<cudaEvent_t> set(kBStageCount + 2, nullptr);
+      for (auto& e : set) BCK(cudaEventCreate(&e), "event");
+      b->prof_free.push_back(set);
+    }
+    std::vector<cudaEvent_t> set = b->prof_free.back();
+    b->prof_free.pop_back();
+    BCK(launch_batch_step(b->d_steps, b->d_hdr, b->tuning, b->n_sm, units_inter, b->stream, b->side,
+                          b->fork, b->join, set.data()), "batched step");
+    b->prof_pending.push_back(set);
+  } else if (b->use_graph) {
     cudaGraphExec_t exec = nullptr;
     int rc = step_graph(b, units_inter, &exec);
     if (rc) return rc;
@@ -540,6 +557,10 @@ int av1b_batch_destroy(av1b_batch* b) {
     if (r.host) cudaFreeHost(r.host);
     if (r.used) cudaEventDestroy(r.used);
   }
+  for (auto* sets : {&b->prof_free, &b->prof_pending})
+    for (auto& set : *sets)
+      for (cudaEvent_t e : set)
+        if (e) cudaEventDestroy(e);
   cudaEvent_t evs[] = {b->fork, b->join, b->done, b->t0, b->t1};
   for (cudaEvent_t e : evs)
     if (e) cudaEventDestroy(e);
@@ -559,6 +580,46 @@ int av1b_batch_decode(av1b_batch* b, int n, av1b_decoder* const* decoders, av1b_
   std::lock_guard<std::mutex> lk(b->mu);
   b->err.clear();
   return batch_step(b, n, decoders, plans, slots, out_slots, nv12_device, nv12_pitch, nv12_len);
+}
+
+static void collect_batch_profile(av1b_batch* b) {
+  for (auto& set : b->prof_pending) {
+    if (cudaEventSynchronize(set[kBStageCount]) == cudaSuccess &&
+        cudaEventSynchronize(set[kBStageCount + 1]) == cudaSuccess) {
+      for (int k = kBInterSimple; k < kBStageCount; ++k) {
+        float ms = 0.f;
+        /* the stage's own launch to the next stage's (the templates on the
+         * side stream from the step's start to their end) */
+        if (k == kBGrainTemplate)
+          cudaEventElapsedTime(&ms, set[kBInterSimple], set[kBStageCount + 1]);
+        else
+          cudaEventElapsedTime(&ms, set[k], set[k == kBCopyRef ? kBGrain : (k == kBNv12 ? kBStageCount : k + 1)]);
+        b->prof_ms[k] += ms;
+      }
+      ++b->prof_n;
+    }
+    b->prof_free.push_back(set);
+  }
+  b->prof_pending.clear();
+}
+
+int av1b_batch_set_profiling(av1b_batch* b, int on) {
+  if (!b) return AV1B_ERR_ARG;
+  std::lock_guard<std::mutex> lk(b->mu);
+  collect_batch_profile(b);
+  b->profiling = on != 0;
+  for (double& v : b->prof_ms) v = 0;
+  b->prof_n = 0;
+  return AV1B_OK;
+}
+
+int av1b_batch_profile(av1b_batch* b, int stage, double* total_ms, long long* steps) {
+  if (!b || stage < 0 || stage >= kBStageCount) return AV1B_ERR_ARG;
+  std::lock_guard<std::mutex> lk(b->mu);
+  collect_batch_profile(b);
+  if (total_ms) *total_ms = b->prof_ms[stage];
+  if (steps) *steps = b->prof_n;
+  return AV1B_OK;
 }
 
 int av1b_batch_sync(av1b_batch* b) {

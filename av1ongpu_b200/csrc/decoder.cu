@@ -2735,13 +2735,16 @@ size_t av1b_stream_hbm_estimate(int width, int height, int coded_width, int bit_
   const int cw = coded_width > 0 ? coded_width : width;
   const size_t nc = static_cast<size_t>(cw) * height +
                     2 * static_cast<size_t>((cw + ss_x) >> ss_x) * ((height + ss_y) >> ss_y);
+  /* every buffer as dev_ensure sizes it: an eighth of room, 64 KB granules */
+  auto rounded = [](size_t b) { return align_up(b + b / 8, size_t(1) << 16); };
   /* pictures: the one reconstructed, the snapshot, the display picture, the
    * two loop restoration sources, and the reference slots; per sample: the
    * phase B residuals (4 B) and the done flags (128 B a block, blocks of 16
-   * samples or more); per plan: its records, coefficient pool and filter
-   * lists (at most 10 B a coded sample); 1 MB of small buffers */
-  return (5 + static_cast<size_t>(n_slots)) * pic + 12 * nc + static_cast<size_t>(plans) * 10 * nc +
-         (1u << 20);
+   * samples or more); per plan: its five buffers - records, coefficient
+   * pool, residuals, levels, filter lists - at most 10 B a coded sample in
+   * all; the grain tables and small buffers, 2 MB */
+  return (5 + static_cast<size_t>(n_slots)) * rounded(pic) + rounded(4 * nc) + rounded(8 * nc) +
+         static_cast<size_t>(plans) * (5 * (size_t(1) << 16) + rounded(10 * nc)) + (size_t(2) << 20);
 }
 
 int av1b_decoder_memory(av1b_decoder* d, size_t* allocated, size_t* budget) {

@@ -45,6 +45,8 @@ namespace {
 using Clock = std::chrono::steady_clock;
 constexpr int kOutRing = 8;        /* NV12 buffers a stream cycles through */
 constexpr int kMaxRefs = 7;
+constexpr int kPlanAhead = 4;      /* frames of a stream planned and not yet complete */
+constexpr int kPlansAlive = 8;     /* a decoder's plans: kPlanAhead, or its pool of freed ones */
 
 struct Request {
   int stream = -1;
@@ -68,6 +70,7 @@ struct Stream {
   uint64_t next_index = 0;       /* given to the next submitted frame */
   uint64_t next_launch = 0;      /* the next frame a step may take */
   std::deque<Request*> pending;  /* submitted, not yet in a step, in order */
+  int planning = 0;              /* frames taken by a planner and not yet complete */
   uint8_t* nv12[kOutRing] = {nullptr};
   size_t nv12_bytes = 0;
   int in_steps = 0;              /* frames of the stream in steps not yet complete */
@@ -118,12 +121,22 @@ void plan_loop(av1b_server* s) {
     Request* r = nullptr;
     Stream* st = nullptr;
     {
+      /* the oldest request of a stream with fewer than kPlanAhead frames
+       * planned and not complete: a stream whose requests pile up holds a
+       * bounded number of plans (and so of device memory) */
       std::unique_lock<std::mutex> lk(s->mu);
-      s->cv_plan.wait(lk, [&] { return s->stop || !s->plan_q.empty(); });
-      if (s->stop && s->plan_q.empty()) return;
-      r = s->plan_q.front();
-      s->plan_q.pop_front();
+      std::deque<Request*>::iterator it;
+      auto pick = [&] {
+        for (it = s->plan_q.begin(); it != s->plan_q.end(); ++it)
+          if (s->streams[(*it)->stream]->planning < kPlanAhead) return true;
+        return false;
+      };
+      s->cv_plan.wait(lk, [&] { return s->stop || pick(); });
+      if (s->stop) return;   /* requests left unplanned are freed with the server */
+      r = *it;
+      s->plan_q.erase(it);
       st = s->streams[r->stream];
+      ++st->planning;
     }
     /* a view into the caller's blob, its references (frame distances)
      * mapped to the stream's ring of slots in an array of its own, so the
@@ -157,6 +170,8 @@ void plan_loop(av1b_server* s) {
     s->cv_sched.notify_one();
   }
 }
+
+Stream* st_of(av1b_server* s, const Request* r) { return s->streams[r->stream]; }
 
 cudaEvent_t take_event(av1b_server* s) {
   if (!s->ev_pool.empty()) {
@@ -228,7 +243,11 @@ void sched_loop(av1b_server* s) {
         ++st->in_steps;
         step->reqs.push_back(r);
       }
-      for (Request* r : failed) post_result(s, r, r->plan_rc, now_ms(s), -1, 0, 0);
+      for (Request* r : failed) {
+        post_result(s, r, r->plan_rc, now_ms(s), -1, 0, 0);
+        --st_of(s, r)->planning;
+      }
+      if (!failed.empty()) s->cv_plan.notify_all();
       s->completed += failed.size();
       if (!failed.empty()) s->cv_result.notify_all();
       if (step->reqs.empty()) {
@@ -304,6 +323,7 @@ void done_loop(av1b_server* s) {
         Request* r = step->reqs[i];
         post_result(s, r, rc != AV1B_OK ? rc : step->rcs[i], done_ms, step->slots[i], n, step->id);
         --s->streams[r->stream]->in_steps;
+        --s->streams[r->stream]->planning;
       }
       s->completed += n;
       --s->inflight;
@@ -315,6 +335,7 @@ void done_loop(av1b_server* s) {
     }
     delete step;
     s->cv_sched.notify_one();
+    s->cv_plan.notify_all();
     s->cv_result.notify_all();
   }
 }
@@ -415,10 +436,10 @@ int av1b_server_open(av1b_server* s, const av1b_stream_desc* desc, int* stream_i
   const int ring_n = d.max_refs + 1;
   const size_t nv12 = d.nv12_pitch ? av1b_nv12_size(d.width, d.height, d.ss_x, d.ss_y, d.nv12_pitch) : 0;
   if (d.nv12_pitch && !nv12) return AV1B_ERR_ARG;
-  /* the decoder's pictures, slots and up to four planned frames, plus the
+  /* the decoder's pictures, slots and up to kPlansAlive plans, plus the
    * output ring */
   const size_t need = av1b_stream_hbm_estimate(d.width, d.height, d.coded_width, d.bit_depth, d.ss_x,
-                                               d.ss_y, ring_n, 4) +
+                                               d.ss_y, ring_n, kPlansAlive) +
                       kOutRing * nv12;
   if (hbm_bytes) *hbm_bytes = need;
   {

@@ -689,6 +689,18 @@ def run_batched_leg(args, av1b, torch, local):
     b1.record(bstream)
     torch.cuda.synchronize()
     batch_ms = b0.elapsed_time(b1)
+    # per-stage device time of the batched step (ungraphed, events between
+    # stages): the key frame-set alone, then the inter frame-sets
+    stage_ms = {}
+    for name, fr in (('key', frames[:1]), ('inter', frames[1:min(F, 31)])):
+        if not fr:
+            continue
+        batch.set_profiling(True)
+        batched(fr)
+        prof, n = batch.profile()
+        batch.set_profiling(False)
+        stage_ms[name] = {k: round(v / max(1, n), 4) for k, v in prof.items() if v > 0}
+        stage_ms[name]['frame_sets'] = n
     for i, d in enumerate(decs):
         for pl in plans[i]:
             d.free_plan(pl)
@@ -706,6 +718,7 @@ def run_batched_leg(args, av1b, torch, local):
                    'all tools, 64x64 SB, 2 (8-bit) / 3 (10-bit) reference slots, NV12 out',
         'plan_s': plan_s, 'autotune': {'config': tuned, 'best_step_ms': tune_ms,
                                        'default_step_ms': default_ms},
+        'stage_ms_per_frame_set': stage_ms,
         'timing': 'device (CUDA events): plain = sum over streams decoded one at a time, each on '
                   'its decoder stream; batched = one graph replay a frame-set on the batch stream',
     }

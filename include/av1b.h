@@ -249,7 +249,8 @@ AV1B_API int av1b_plan_stats(const av1b_plan* plan, av1b_plan_info* out);
 AV1B_API int av1b_sync(av1b_decoder* dec);
 
 /* The device memory a decoder needs for a stream of this geometry with
- * `n_slots` reference slots and `plans` frames planned ahead at once - an
+ * `n_slots` reference slots and `plans` plans alive at once (planned ahead,
+ * in flight, or kept for reuse: a decoder keeps up to 8 freed plans) - an
  * upper bound for frames whose blocks are 4x4 or larger - and what a decoder
  * holds now against its budget. A server admitting streams by HBM sizes
  * each stream's decoder budget with the first and checks the second. */
@@ -409,6 +410,13 @@ AV1B_API int av1b_batch_autotune(av1b_batch* batch, int n, av1b_decoder* const* 
                                  const size_t* nv12_len, const char* cache_path, int reps,
                                  av1b_batch_config* out, double* best_ms);
 AV1B_API const char* av1b_batch_last_error(av1b_batch* batch);
+/* Per-stage device time of batched steps: with profiling on, steps launch
+ * without the graph, each stage bracketed by CUDA events, and
+ * av1b_batch_profile gives stage `stage`'s summed milliseconds (in launch
+ * order, 0..20; the grain templates run beside the others) and the steps
+ * timed. Switching profiling clears the sums. */
+AV1B_API int av1b_batch_set_profiling(av1b_batch* batch, int on);
+AV1B_API int av1b_batch_profile(av1b_batch* batch, int stage, double* total_ms, long long* steps);
 /* The CUDA stream the batch's steps run on (a cudaStream_t). */
 AV1B_API void* av1b_batch_stream(av1b_batch* batch);
 

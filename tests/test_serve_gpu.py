@@ -109,7 +109,7 @@ def test_served_frames_match_solo(av1b, solo):
 def test_admission_is_gated_by_hbm(av1b):
     if not av1b.cuda_available():
         pytest.skip('no CUDA device')
-    one = av1b.lib().av1b_stream_hbm_estimate(1920, 1080, 0, 10, 1, 1, 4, 4)
+    one = av1b.lib().av1b_stream_hbm_estimate(1920, 1080, 0, 10, 1, 1, 4, 8)
     assert one > 0
     srv = av1b.Server(0, hbm_budget=int(one * 2.5) + 8 * 3110400)
     a, _ = srv.open(1920, 1080, 10, max_refs=3, nv12_pitch=1920)
