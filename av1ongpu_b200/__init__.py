@@ -643,8 +643,9 @@ class Server:
     """The served form (av1b_server_*): streams admitted by HBM, frame
     requests planned as they arrive and run in continuously batched steps."""
 
-    def __init__(self, device=0, max_batch=0, max_inflight=0, planner_threads=0, hbm_budget=0):
-        opt = (ctypes.c_int32 * 4)(device, max_batch, max_inflight, planner_threads)
+    def __init__(self, device=0, max_batch=0, max_inflight=0, planner_threads=0, hbm_budget=0,
+                 decoder_threads=0):
+        opt = (ctypes.c_int32 * 6)(device, max_batch, max_inflight, planner_threads, decoder_threads, 0)
         buf = ctypes.create_string_buffer(bytes(opt) + bytes(ctypes.c_size_t(hbm_budget)))
         h = ctypes.c_void_p()
         rc = lib().av1b_server_create(buf, ctypes.byref(h))

@@ -51,7 +51,9 @@ __global__ void __launch_bounds__(128) kb_inter_simple(const StreamStep* __restr
   }
 }
 
-__global__ void __launch_bounds__(128, 4) kb_inter(const StreamStep* __restrict__ st, BatchHeader* h,
+/* Three CTAs an SM: the tile body needs the registers of the single-stream
+ * kernel plus the loop's, which at four CTAs spilled. */
+__global__ void __launch_bounds__(128, 3) kb_inter(const StreamStep* __restrict__ st, BatchHeader* h,
                                                    int chunk) {
   __shared__ McScratch scr[4];
   __shared__ int pred[4][2][8 * 16];

@@ -1349,7 +1349,8 @@ __global__ void __launch_bounds__(256) k_lr_tile(const px_t* __restrict__ cdef,
  * (every draw independent through the orbit table), then the auto-regressive
  * filter as a wavefront: sample (x, y) depends on rows above within +-lag
  * columns and on the lag samples to its left, so t = x + 4y orders it
- * (lag <= 3). One block; luma first, then both chroma planes together. */
+ * (lag <= 3). One block: the Gaussian fill on all its threads, the filters
+ * (luma first, then both chroma planes together) on its first warp. */
 /* The templates live in shared memory while the auto-regressive wavefront
  * runs (hundreds of dependent steps: every tap a shared-memory read, not a
  * global one) and are written out at the end. */
@@ -1357,7 +1358,8 @@ struct GrainTemplateSmem {
   short luma[82 * 73], cb[82 * 73], cr[82 * 73];
 };
 
-/* Every thread of the CTA runs it; it has no early return. */
+/* Every thread of the CTA runs it (the filters on its first warp); it has
+ * no early return. */
 __device__ __forceinline__ void grain_template_body(GrainState* gs, const GrainParamsDev& prm,
                                                     const uint16_t* orbit, const uint16_t* pos,
                                                     GrainTemplateSmem& sm) {
@@ -1396,12 +1398,17 @@ __device__ __forceinline__ void grain_template_body(GrainState* gs, const GrainP
   __syncthreads();
   const int lag = prm.ar_coeff_lag;
   const int arshift = prm.ar_coeff_shift_minus_6 + 6;
+  /* The auto-regressive filters run on one warp: a step of a wavefront has
+   * at most 73 samples (a row each), and its hundreds of dependent steps
+   * then meet a warp barrier instead of a CTA barrier each. The samples of
+   * a step depend only on earlier steps, so each step's order is free. */
+  if (tid < 32) {
   /* luma AR filter */
   if (prm.num_y_points > 0) {
     const int W = 82, H = 73;
     const int tmax = (W - 4) + 4 * (H - 1);
     for (int t = 3 + 4 * 3; t <= tmax; ++t) {
-      for (int y = 3 + tid; y < H; y += blockDim.x) {
+      for (int y = 3 + tid; y < H; y += 32) {
         const int x = t - 4 * y;
         if (x < 3 || x >= W - 3) continue;
         int sum = 0, pos_ = 0;
@@ -1414,14 +1421,14 @@ __device__ __forceinline__ void grain_template_body(GrainState* gs, const GrainP
       done_l:
         luma[y * W + x] = (short)clampi(luma[y * W + x] + rnd2z(sum, arshift), gmin, gmax);
       }
-      __syncthreads();
+      __syncwarp();
     }
   }
   if (chroma) {
     const int sx = prm.ss_x, sy = prm.ss_y;
     const int tmax = (cw - 4) + 4 * (ch - 1);
     for (int t = 3 + 4 * 3; t <= tmax; ++t) {
-      for (int k = tid; k < 2 * ch; k += blockDim.x) {
+      for (int k = tid; k < 2 * ch; k += 32) {
         const int plane = k & 1, y = k >> 1;
         if (y < 3) continue;
         const int x = t - 4 * y;
@@ -1447,8 +1454,9 @@ __device__ __forceinline__ void grain_template_body(GrainState* gs, const GrainP
       done_c:
         gp[y * cw + x] = (short)clampi(gp[y * cw + x] + rnd2z(sum, arshift), gmin, gmax);
       }
-      __syncthreads();
+      __syncwarp();
     }
+  }
   }
   __syncthreads();
   for (int k = tid; k < 82 * 73; k += blockDim.x) gs->luma[k] = luma[k];

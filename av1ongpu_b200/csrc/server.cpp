@@ -351,12 +351,14 @@ int av1b_server_create(const av1b_server_options* options, av1b_server** out) {
   if (options) o = *options;
   if (o.max_batch <= 0) o.max_batch = AV1B_BATCH_MAX;
   if (o.max_inflight <= 0) o.max_inflight = 2;
-  if (o.max_batch > AV1B_BATCH_MAX || o.max_inflight > 8 || o.planner_threads < 0 || o.planner_threads > 64)
+  if (o.max_batch > AV1B_BATCH_MAX || o.max_inflight > 8 || o.planner_threads < 0 ||
+      o.planner_threads > 64 || o.decoder_threads < 0 || o.decoder_threads > 64)
     return AV1B_ERR_ARG;
   if (o.planner_threads == 0) {
     const unsigned hc = std::thread::hardware_concurrency();
-    o.planner_threads = static_cast<int>(std::max(2u, hc > 2 ? hc - 2 : 2u));
+    o.planner_threads = static_cast<int>(std::max(2u, hc / 2));
   }
+  if (o.decoder_threads == 0) o.decoder_threads = 4;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return AV1B_ERR_NO_DEVICE;
   if (o.device < 0 || o.device >= ndev) return AV1B_ERR_ARG;
@@ -451,7 +453,7 @@ int av1b_server_open(av1b_server* s, const av1b_stream_desc* desc, int* stream_i
   st->desc = d;
   st->ring_n = ring_n;
   st->hbm = need;
-  av1b_decoder_options dopt{1, 2};
+  av1b_decoder_options dopt{1, s->opt.decoder_threads};
   int rc = av1b_decoder_create_ex(s->opt.device, need - kOutRing * nv12, &dopt, &st->dec);
   for (int i = 0; rc == AV1B_OK && i < ring_n; ++i) rc = av1b_reserve_reference(st->dec, &st->ring[i]);
   if (rc == AV1B_OK && nv12) {

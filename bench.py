@@ -809,8 +809,9 @@ def run_serving_leg(args, av1b, local):
                 'by_class': {c: {'p50_ms': percentile(v, 50), 'p99_ms': percentile(v, 99),
                                  'frames': len(v)} for c, v in sorted(by.items())}}
 
-    # bring every stream to steady state (key frames, planner and plan pools)
-    run([(0.0, j) for j in range(len(streams))])
+    # bring every stream to steady state: its key frame, and enough frames at
+    # once that its decoder's plan pool and buffers reach their sizes
+    run([(0.0, j) for _ in range(8) for j in range(len(streams))])
     # capacity: every stream's next 30 frames at once, as fast as they can go
     burst = [(0.0, j) for _ in range(SERVE_GOP) for j in range(len(streams))]
     res, tags = run(burst)

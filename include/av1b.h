@@ -450,7 +450,8 @@ typedef struct av1b_server_options {
   int32_t device;
   int32_t max_batch;        /* frames a step (1..64; 0: 64) */
   int32_t max_inflight;     /* steps queued on the GPU at once (1..8; 0: 2) */
-  int32_t planner_threads;  /* host threads planning requests (0: cores - 2) */
+  int32_t planner_threads;  /* requests planned at once (0: cores / 2) */
+  int32_t decoder_threads;  /* host threads planning one request (0: 4) */
   size_t hbm_budget;        /* device memory the streams may hold (0: 90 % of the free memory) */
 } av1b_server_options;
 typedef struct av1b_stream_desc {
