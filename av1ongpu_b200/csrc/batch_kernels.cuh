@@ -258,69 +258,6 @@ __global__ void __launch_bounds__(128) kb_grain_blend(const StreamStep* __restri
   }
 }
 
-/* NV12 with the film grain of the packed samples applied while packing:
- * eight bytes of row `row` at byte x0, from the picture before grain. The
- * same arithmetic per sample as grain_blend_item followed by nv12_item. */
-__device__ __forceinline__ void nv12_grain_item(const px_t* __restrict__ pic, uint8_t* out,
-                                                const Layout& L, int pitch, int x0, int row,
-                                                const GrainState* gs, const uint16_t* orbit,
-                                                const uint16_t* pos) {
-  if (x0 >= pitch) return;
-  const int w = L.p[0].out_w, h = L.p[0].out_h;
-  const int shift = L.bit_depth - 8;
-  const bool vec = (reinterpret_cast<uintptr_t>(pic) & 15) == 0;
-  uint8_t v[8];
-  if (row < h) {
-    const px_t* src = pic + L.p[0].off + row * L.p[0].stride;
-    const int lim = mini(w, L.p[0].coded_w);
-#pragma unroll
-    for (int half = 0; half < 2; ++half) {
-      const int xs = x0 + 4 * half;
-      int orig[4] = {0, 0, 0, 0}, o[4] = {0, 0, 0, 0};
-      if (xs < lim) {
-#pragma unroll
-        for (int q = 0; q < 4; ++q) orig[q] = xs + q < w ? src[xs + q] : 0;
-        grain_group4(pic, L, gs, orbit, pos, 0, row, xs, vec, orig, o);
-      }
-#pragma unroll
-      for (int q = 0; q < 4; ++q) v[4 * half + q] = xs + q < lim ? (uint8_t)(o[q] >> shift) : 0;
-    }
-  } else {
-    const int cr = row - h;
-    const int cw = (w + 1) >> 1;
-    const int ccw = L.p[1].coded_w;
-    const int cx0 = x0 >> 1;
-    int ou[4] = {0, 0, 0, 0}, ov[4] = {0, 0, 0, 0};
-    if (cx0 < mini(cw, ccw)) {
-      const px_t* u = pic + L.p[1].off + cr * L.p[1].stride;
-      const px_t* vv = pic + L.p[2].off + cr * L.p[2].stride;
-      int origu[4], origv[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        origu[q] = cx0 + q < L.p[1].out_w ? u[cx0 + q] : 0;
-        origv[q] = cx0 + q < L.p[2].out_w ? vv[cx0 + q] : 0;
-      }
-      grain_group4(pic, L, gs, orbit, pos, 1, cr, cx0, vec, origu, ou);
-      grain_group4(pic, L, gs, orbit, pos, 2, cr, cx0, vec, origv, ov);
-    }
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      const int x = x0 + k;
-      const int c = (x >> 1) - cx0;
-      v[k] = (x < 2 * cw && (x >> 1) < ccw) ? (uint8_t)(((x & 1) ? ov[c] : ou[c]) >> shift) : 0;
-    }
-  }
-  uint8_t* d = out + (size_t)row * pitch + x0;
-  if (x0 + 8 <= pitch && ((reinterpret_cast<uintptr_t>(d) & 7) == 0)) {
-    uint2 pk;
-    pk.x = v[0] | (v[1] << 8) | (v[2] << 16) | ((unsigned)v[3] << 24);
-    pk.y = v[4] | (v[5] << 8) | (v[6] << 16) | ((unsigned)v[7] << 24);
-    *reinterpret_cast<uint2*>(d) = pk;
-  } else {
-    for (int k = 0; k < 8 && x0 + k < pitch; ++k) d[k] = v[k];
-  }
-}
-
 __global__ void __launch_bounds__(128) kb_nv12(const StreamStep* __restrict__ st,
                                                const BatchHeader* __restrict__ h) {
   const int* pfx = h->pfx[kBNv12];

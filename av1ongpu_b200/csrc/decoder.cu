@@ -2055,6 +2055,10 @@ struct StepPrep {
   int slot = -1;
   int keep = 0;
   int launches = 0;
+  /* the frame's film grain is applied when an output call asks for it (its
+   * decode reads nothing back): the NV12 pack of the frame then applies it
+   * while packing, and no display picture is written */
+  bool defer_grain = false;
   FrameArgs a{};
   FilterArgs f{};
 };
@@ -2335,12 +2339,16 @@ int launch_step_plain(av1b_decoder* d, av1b_plan* pl, StepPrep* sp) {
   if (P.grain) {
     GrainState* gsd = static_cast<GrainState*>(d->grain_state.p);
     CK(cudaStreamWaitEvent(st, d->ev_join, 0), "join wait");
-    CK(timed(d, kStGrainBlend, [&] {
-         return launch_grain_blend(cur, static_cast<px_t*>(d->disp.p), L, gsd,
-                                   static_cast<const uint16_t*>(d->orbit.p),
-                                   static_cast<const uint16_t*>(d->pos.p), st);
-       }), "film grain blend");
-    launches += 1;
+    if (sp->defer_grain) {
+      d->disp_pending = true;
+    } else {
+      CK(timed(d, kStGrainBlend, [&] {
+           return launch_grain_blend(cur, static_cast<px_t*>(d->disp.p), L, gsd,
+                                     static_cast<const uint16_t*>(d->orbit.p),
+                                     static_cast<const uint16_t*>(d->pos.p), st);
+         }), "film grain blend");
+      launches += 1;
+    }
     display = static_cast<px_t*>(d->disp.p);
     d->disp_is_cur = false;
   }
@@ -2401,6 +2409,7 @@ int commit_step(av1b_decoder* d, av1b_plan* pl, StepPrep* sp, const av1b_planes*
 int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, const av1b_planes* out,
                  int* out_slot, bool sync) {
   StepPrep sp;
+  sp.defer_grain = out == nullptr;
   int rc;
   if ((rc = prepare_step(d, pl, keep, forced_slot, false, &sp)) ||
       (rc = launch_step_plain(d, pl, &sp)))
@@ -2804,14 +2813,40 @@ size_t av1b_nv12_size(int width, int height, int ss_x, int ss_y, size_t pitch) {
   return nv12_bytes(width, height, ss_x, ss_y, pitch);
 }
 
+/* Packs `slot` as NV12 into device memory on the decoder's stream: the
+ * frame decoded last whose grain is still to be applied goes through the
+ * pack that applies it; any other picture through the plain pack. */
+int launch_pack(av1b_decoder* d, int slot, uint8_t* target, size_t pitch) {
+  if ((slot < 0 || slot == d->last_slot) && d->have_last && d->disp_pending) {
+    CK(timed(d, kStNv12, [&] {
+         return launch_nv12_grain(static_cast<const px_t*>(d->cur.p), target, d->L,
+                                  static_cast<int>(pitch),
+                                  static_cast<const GrainState*>(d->grain_state.p),
+                                  static_cast<const uint16_t*>(d->orbit.p),
+                                  static_cast<const uint16_t*>(d->pos.p), d->stream);
+       }), "NV12 pack with film grain");
+    return AV1B_OK;
+  }
+  const px_t* pic = nullptr;
+  const int rc = picture_of(d, slot, &pic);
+  if (rc) return rc;
+  CK(timed(d, kStNv12, [&] { return launch_nv12(pic, target, d->L, static_cast<int>(pitch), d->stream); }),
+     "NV12 pack");
+  return AV1B_OK;
+}
+
 static int to_nv12_impl(av1b_decoder* d, int slot, size_t pitch, uint8_t* dst, size_t dst_len,
                         bool device_dst) {
   if (!d || !dst) return AV1B_ERR_ARG;
   std::lock_guard<std::mutex> lk(d->mu);
   cudaSetDevice(d->device);
-  const px_t* pic = nullptr;
-  int rc = picture_of(d, slot, &pic);
-  if (rc) return rc;
+  int rc;
+  {
+    /* the slot check of picture_of, before any buffer is sized */
+    const bool last = slot < 0 || slot == d->last_slot;
+    if (last ? !d->have_last : (slot >= kSlots || !d->slot_used[slot] || !d->slot_valid[slot]))
+      return fail(d, AV1B_ERR_ARG, last ? "no frame to convert" : "invalid reference slot");
+  }
   const size_t bytes = nv12_bytes(d->width, d->height, d->ss_x, d->ss_y, pitch);
   if (bytes == 0 || pitch > (1u << 30))
     return fail(d, AV1B_ERR_ARG, "NV12 output needs a 4:2:0 frame and an even pitch at least as wide");
@@ -2821,8 +2856,7 @@ static int to_nv12_impl(av1b_decoder* d, int slot, size_t pitch, uint8_t* dst, s
     if ((rc = dev_ensure(d, d->nv12, bytes))) return rc;
     target = static_cast<uint8_t*>(d->nv12.p);
   }
-  CK(timed(d, kStNv12, [&] { return launch_nv12(pic, target, d->L, static_cast<int>(pitch), d->stream); }),
-     "NV12 pack");
+  if ((rc = launch_pack(d, slot, target, pitch))) return rc;
   if (!device_dst) {
     CK(cudaMemcpyAsync(dst, target, bytes, cudaMemcpyDeviceToHost, d->stream), "NV12 read back");
     CK(wait_stream(d), "NV12 sync");
@@ -2849,9 +2883,13 @@ int av1b_nv12_pack_begin(av1b_decoder* d, int slot, size_t pitch, int* out_handl
   *out_handle = -1;
   std::lock_guard<std::mutex> lk(d->mu);
   cudaSetDevice(d->device);
-  const px_t* pic = nullptr;
-  int rc = picture_of(d, slot, &pic);
-  if (rc) return rc;
+  int rc;
+  {
+    /* the slot check of picture_of, without making a pending display picture */
+    const bool last = slot < 0 || slot == d->last_slot;
+    if (last ? !d->have_last : (slot >= kSlots || !d->slot_used[slot] || !d->slot_valid[slot]))
+      return fail(d, AV1B_ERR_ARG, last ? "no frame to convert" : "invalid reference slot");
+  }
   const size_t bytes = nv12_bytes(d->width, d->height, d->ss_x, d->ss_y, pitch);
   if (bytes == 0 || pitch > (1u << 30))
     return fail(d, AV1B_ERR_ARG, "NV12 output needs a 4:2:0 frame and an even pitch at least as wide");
@@ -2883,8 +2921,7 @@ int av1b_nv12_pack_begin(av1b_decoder* d, int slot, size_t pitch, int* out_handl
     e->host_cap = bytes;
   }
   uint8_t* dev = static_cast<uint8_t*>(e->dev.p);
-  CK(timed(d, kStNv12, [&] { return launch_nv12(pic, dev, d->L, static_cast<int>(pitch), d->stream); }),
-     "NV12 pack");
+  if ((rc = launch_pack(d, slot, dev, pitch))) return rc;
   CK(cudaEventRecord(e->packed, d->stream), "event");
   CK(cudaStreamWaitEvent(d->copy_stream, e->packed, 0), "copy stream wait");
   CK(cudaMemcpyAsync(e->host, dev, bytes, cudaMemcpyDeviceToHost, d->copy_stream), "NV12 read back");

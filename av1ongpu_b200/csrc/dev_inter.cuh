@@ -183,7 +183,28 @@ AV1B_DEV bool mc_rect(const InterCtx& c, const px_t* ref, int stride, int base_x
     __syncwarp();
     return false;
   }
-  {
+  if (cbase >= 0 && rbase >= 0 && cbase + ncols <= c.ref_w && rbase + nrows <= c.ref_h) {
+    /* the window lies inside the reference (no sample clamps): four samples
+     * a load from the 8-byte boundary at or left of it - the rows of a plane
+     * start on 128-byte boundaries and run a border past the picture, so the
+     * load never leaves the row; samples left or right of the window are
+     * dropped */
+    const int a0 = cbase & ~3;
+    const int groups = (cbase + ncols - a0 + 3) >> 2;
+    StepWalk wk(lane, 32, groups);
+    for (int k = lane; k < nrows * groups; k += 32, wk.next()) {
+      const uint2* src =
+          reinterpret_cast<const uint2*>(ref + (rbase + wk.r) * stride + a0 + 4 * wk.q);
+      const uint2 v = CG ? __ldcg(src) : __ldg(src);
+      const int vals[4] = {static_cast<int>(v.x & 0xffff), static_cast<int>(v.x >> 16),
+                           static_cast<int>(v.y & 0xffff), static_cast<int>(v.y >> 16)};
+      const int q0 = a0 + 4 * wk.q - cbase;
+      int* row = s.win + wk.r * AV1B_MC_WC;
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (q0 + j >= 0 && q0 + j < ncols) row[q0 + j] = vals[j];
+    }
+  } else {
     StepWalk wk(lane, 32, ncols);
     for (int k = lane; k < nrows * ncols; k += 32, wk.next())
       s.win[wk.r * AV1B_MC_WC + wk.q] =

@@ -133,6 +133,10 @@ cudaError_t launch_grain_template(GrainState* gs, const GrainParamsDev& prm, con
 cudaError_t launch_grain_blend(const px_t* src, px_t* dst, const Layout& L, const GrainState* gs,
                                const uint16_t* orbit, const uint16_t* pos, cudaStream_t s);
 cudaError_t launch_nv12(const px_t* pic, uint8_t* out, const Layout& L, int pitch, cudaStream_t s);
+/* NV12 of `pic` before film grain, the grain (state `gs`) applied while packing. */
+cudaError_t launch_nv12_grain(const px_t* pic, uint8_t* out, const Layout& L, int pitch,
+                              const GrainState* gs, const uint16_t* orbit, const uint16_t* pos,
+                              cudaStream_t s);
 cudaError_t launch_rgb(const px_t* pic, uint8_t* out, const Layout& L, const RgbArgs& m,
                        cudaStream_t s);
 

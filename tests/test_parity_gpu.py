@@ -371,3 +371,43 @@ def test_full_size_workload_hashes(av1b, dec, name):
     assert len(got) == len(want) == spec[2]
     for k, (g, w) in enumerate(zip(got, want)):
         assert g == w, '%s frame %d' % (name, k)
+
+
+def test_deferred_grain_outputs(av1b, oracle, dec):
+    """A planned decode that reads nothing back leaves the frame's film grain
+    to its outputs: the NV12 pack applies it while packing, and the display
+    picture is made when asked for (device planes, RGB); all equal the oracle."""
+    import ctypes
+    blobs = [av1b.synth_frame(2, 4, 61, k) for k in range(3)]
+    w, _, h, _, sx, sy = blobs[0].header
+    ref = oracle.RefDecoder()
+    sr = oracle.Stream(ref)
+    ring = [dec.reserve_reference() for _ in range(4)]
+    rt = ctypes.CDLL('libcudart.so')
+    pitch = (w + 63) & ~63
+    for k, b in enumerate(blobs):
+        d = b.get_refs()
+        b.set_refs([ring[(k - x) % 4] for x in d])
+        pl = dec.plan(b)
+        b.set_refs(d)
+        dec.decode_planned(pl, slot=ring[k], keep=True, wait=True)
+        dec.free_plan(pl)
+        # the oracle's frame k decoded now, so that it too is the frame decoded last
+        rslot, rplanes = sr.decode(k, b)
+        if k == 0:   # NV12 first: packed with the grain applied while packing
+            assert np.array_equal(dec.to_nv12(ring[k], pitch, w, h), ref.to_nv12(rslot, pitch, w, h))
+        if k == 1:   # planes first: the display picture is made on demand
+            ptr = (ctypes.c_void_p * 3)()
+            stride = (ctypes.c_int32 * 3)()
+            assert av1b.lib().av1b_slot_planes_device(dec.h, ring[k], ptr, stride) == 0
+            for p, (rows, cols) in enumerate(av1b.plane_shapes(w, h, sx, sy)):
+                a = np.empty((rows, cols), dtype=np.uint16)
+                assert rt.cudaMemcpy2D(ctypes.c_void_p(a.ctypes.data), ctypes.c_size_t(cols * 2),
+                                       ctypes.c_void_p(ptr[p]), ctypes.c_size_t(stride[p] * 2),
+                                       ctypes.c_size_t(cols * 2), ctypes.c_size_t(rows), 2) == 0
+                assert np.array_equal(a, rplanes[p]), (k, p)
+            assert np.array_equal(dec.to_nv12(ring[k], pitch, w, h), ref.to_nv12(rslot, pitch, w, h))
+        if k == 2:   # RGB
+            assert np.array_equal(dec.to_rgb(ring[k], 1, 0, w, h), ref.to_rgb(rslot, 1, 0, w, h))
+    for s in ring:
+        dec.release_reference(s)
