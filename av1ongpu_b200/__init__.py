@@ -94,7 +94,8 @@ class ServerStats(ctypes.Structure):
     _fields_ = [('submitted', ctypes.c_uint64), ('completed', ctypes.c_uint64),
                 ('steps', ctypes.c_uint64), ('stepped_frames', ctypes.c_uint64),
                 ('hbm_used', ctypes.c_size_t), ('hbm_budget', ctypes.c_size_t),
-                ('streams', ctypes.c_int32), ('now_ms', ctypes.c_double)]
+                ('streams', ctypes.c_int32), ('now_ms', ctypes.c_double),
+                ('plan_ms', ctypes.c_double), ('launch_ms', ctypes.c_double)]
 
 
 class Stats(ctypes.Structure):
@@ -644,8 +645,9 @@ class Server:
     requests planned as they arrive and run in continuously batched steps."""
 
     def __init__(self, device=0, max_batch=0, max_inflight=0, planner_threads=0, hbm_budget=0,
-                 decoder_threads=0):
-        opt = (ctypes.c_int32 * 6)(device, max_batch, max_inflight, planner_threads, decoder_threads, 0)
+                 decoder_threads=0, batch_wait_us=0):
+        opt = (ctypes.c_int32 * 6)(device, max_batch, max_inflight, planner_threads, decoder_threads,
+                                   batch_wait_us)
         buf = ctypes.create_string_buffer(bytes(opt) + bytes(ctypes.c_size_t(hbm_budget)))
         h = ctypes.c_void_p()
         rc = lib().av1b_server_create(buf, ctypes.byref(h))

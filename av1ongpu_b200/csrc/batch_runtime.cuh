@@ -98,9 +98,8 @@ int fill_filter_args(av1b_decoder* d, av1b_plan* pl, StepPrep* sp) {
   if (P.grain) {
     GrainState* gsd = static_cast<GrainState*>(d->grain_state.p);
     const size_t tail = offsetof(GrainState, lut);
-    CK(cudaMemcpyAsync(reinterpret_cast<uint8_t*>(gsd) + tail,
-                       reinterpret_cast<const uint8_t*>(&P.gs_tail) + tail, sizeof(GrainState) - tail,
-                       cudaMemcpyHostToDevice, d->stream), "grain constants");
+    CK(cudaMemcpyAsync(reinterpret_cast<uint8_t*>(gsd) + tail, ar + pl->o_gs, sizeof(GrainState) - tail,
+                       cudaMemcpyDeviceToDevice, d->stream), "grain constants");
     f.grain = 1;
     f.gs = gsd;
     f.gp = P.gp;

@@ -1726,6 +1726,7 @@ struct av1b_plan {
   size_t o_chains = 0;
   size_t o_tiles = 0, o_itx = 0, o_itxb = 0, o_dbv = 0, o_dbh = 0, o_cdef = 0, o_lr[3] = {0, 0, 0};
   size_t o_map = 0, o_cdef_search = 0, o_dq = 0, o_de_raw = 0, o_cb_raw = 0, o_prep = 0;
+  size_t o_gs = 0;                /* the film grain constants and scaling tables */
   int slots_read[kSlots + 1];     /* the reference slots the frame reads, -1 ended */
   int n_blocks = 0;
   bool owned_by_decoder = false;
@@ -1960,6 +1961,9 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
   pl->o_itxb = stage_put(&off, P.R->itx_batches);
   for (int p = 0; p < 3; ++p) pl->o_lr[p] = stage_put(&off, P.R->lr_units[p]);
   pl->o_dq = stage_put(&off, P.R->dq);
+  const size_t gs_tail = offsetof(GrainState, lut);
+  pl->o_gs = off;
+  off = align_up(off + (sizeof(GrainState) - gs_tail), 256);
   pl->o_map = off;
   off = align_up(off + s.n_palette_map + 64, 256);
   const size_t total = off;
@@ -1991,6 +1995,12 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
   CK(put(pl->o_itxb, P.R->itx_batches), "record upload");
   for (int p = 0; p < 3; ++p) CK(put(pl->o_lr[p], P.R->lr_units[p]), "record upload");
   CK(put(pl->o_dq, P.R->dq), "record upload");
+  /* the grain constants: from the plan's own memory (its upload is waited
+   * for before plan_frame returns), copied into the decoder's grain state on
+   * the device when the frame runs */
+  if (P.grain)
+    CK(cudaMemcpyAsync(ar + pl->o_gs, reinterpret_cast<const uint8_t*>(&P.gs_tail) + gs_tail,
+                       sizeof(GrainState) - gs_tail, cudaMemcpyHostToDevice, st), "grain constants upload");
   if (s.n_palette_map)
     CK(cudaMemcpyAsync(ar + pl->o_map, s.palette_map, s.n_palette_map, cudaMemcpyHostToDevice, st),
        "palette map upload");
@@ -2239,9 +2249,8 @@ int launch_step_plain(av1b_decoder* d, av1b_plan* pl, StepPrep* sp) {
     const size_t tail = offsetof(GrainState, lut);
     CK(cudaEventRecord(d->ev_fork, st), "fork");
     CK(cudaStreamWaitEvent(d->aux, d->ev_fork, 0), "fork wait");
-    CK(cudaMemcpyAsync(reinterpret_cast<uint8_t*>(gsd) + tail,
-                       reinterpret_cast<const uint8_t*>(&P.gs_tail) + tail, sizeof(GrainState) - tail,
-                       cudaMemcpyHostToDevice, d->aux), "grain constants");
+    CK(cudaMemcpyAsync(reinterpret_cast<uint8_t*>(gsd) + tail, ar + pl->o_gs, sizeof(GrainState) - tail,
+                       cudaMemcpyDeviceToDevice, d->aux), "grain constants");
     CK(timed(d, kStGrainTemplate, [&] {
          return launch_grain_template(gsd, P.gp, static_cast<const uint16_t*>(d->orbit.p),
                                       static_cast<const uint16_t*>(d->pos.p), d->aux);

@@ -1350,7 +1350,83 @@ __global__ void __launch_bounds__(256) k_lr_tile(const px_t* __restrict__ cdef,
  * filter as a wavefront: sample (x, y) depends on rows above within +-lag
  * columns and on the lag samples to its left, so t = x + 4y orders it
  * (lag <= 3). One block: the Gaussian fill on all its threads, the filters
- * (luma first, then both chroma planes together) on its first warp. */
+ * (luma first, then both chroma planes together) on its first five warps. */
+/* Threads of the template CTA that run the auto-regressive filters. */
+constexpr int kGrainArThreads = 160;
+
+__device__ __forceinline__ void grain_ar_barrier() {
+  asm volatile("bar.sync 1, 160;" ::: "memory");
+}
+
+/* The auto-regressive filters of the three templates (7.18.3.3) with lag
+ * LAG, by wavefront: sample (x, y) reads the LAG rows above within +-LAG
+ * columns and the LAG samples to its left, so the steps t = x + 4y order
+ * it, and the samples of one step are independent. Thread `tid` of
+ * kGrainArThreads takes luma row 3 + tid, then chroma item tid (plane
+ * tid & 1, row tid >> 1); every one of them meets the named barrier after
+ * each step. */
+template <int LAG>
+__device__ void grain_ar(const GrainParamsDev& prm, short* luma, short* cb, short* cr, int cw, int ch,
+                         bool chroma, int arshift, int gmin, int gmax, int tid) {
+  constexpr int NT = 2 * LAG * (LAG + 1);   /* taps before the sample itself */
+  if (prm.num_y_points > 0) {
+    constexpr int W = 82, H = 73;
+    int co[NT > 0 ? NT : 1];
+#pragma unroll
+    for (int i = 0; i < NT; ++i) co[i] = prm.ar_y[i];
+    const int y = 3 + tid;
+    const int tmax = (W - 4) + 4 * (H - 1);
+    for (int t = 3 + 4 * 3; t <= tmax; ++t) {
+      const int x = t - 4 * y;
+      if (y < H && x >= 3 && x < W - 3) {
+        int sum = 0, k = 0;
+#pragma unroll
+        for (int dr = -LAG; dr <= 0; ++dr)
+#pragma unroll
+          for (int dc = -LAG; dc <= LAG; ++dc) {
+            if (dr == 0 && dc == 0) break;
+            sum += luma[(y + dr) * W + x + dc] * co[k++];
+          }
+        luma[y * W + x] = (short)clampi(luma[y * W + x] + rnd2z(sum, arshift), gmin, gmax);
+      }
+      grain_ar_barrier();
+    }
+  }
+  if (chroma) {
+    const int sx = prm.ss_x, sy = prm.ss_y;
+    const int plane = tid & 1, y = tid >> 1;
+    const bool mine = tid < 2 * ch && y >= 3;
+    short* gp = plane ? cr : cb;
+    const int* cp = plane ? prm.ar_cr : prm.ar_cb;
+    int co[NT + 1];
+#pragma unroll
+    for (int i = 0; i <= NT; ++i) co[i] = cp[i];
+    const int tmax = (cw - 4) + 4 * (ch - 1);
+    for (int t = 3 + 4 * 3; t <= tmax; ++t) {
+      const int x = t - 4 * y;
+      if (mine && x >= 3 && x < cw - 3) {
+        int sum = 0, k = 0;
+#pragma unroll
+        for (int dr = -LAG; dr <= 0; ++dr)
+#pragma unroll
+          for (int dc = -LAG; dc <= LAG; ++dc) {
+            if (dr == 0 && dc == 0) break;
+            sum += gp[(y + dr) * cw + x + dc] * co[k++];
+          }
+        if (prm.num_y_points > 0) {
+          const int lx = ((x - 3) << sx) + 3, ly = ((y - 3) << sy) + 3;
+          int acc = 0;
+          for (int i = 0; i <= sy; ++i)
+            for (int j = 0; j <= sx; ++j) acc += luma[(ly + i) * 82 + lx + j];
+          sum += rnd2z(acc, sx + sy) * co[NT];
+        }
+        gp[y * cw + x] = (short)clampi(gp[y * cw + x] + rnd2z(sum, arshift), gmin, gmax);
+      }
+      grain_ar_barrier();
+    }
+  }
+}
+
 /* The templates live in shared memory while the auto-regressive wavefront
  * runs (hundreds of dependent steps: every tap a shared-memory read, not a
  * global one) and are written out at the end. */
@@ -1358,8 +1434,8 @@ struct GrainTemplateSmem {
   short luma[82 * 73], cb[82 * 73], cr[82 * 73];
 };
 
-/* Every thread of the CTA runs it (the filters on its first warp); it has
- * no early return. */
+/* Every thread of the CTA runs it (the filters on its first five warps);
+ * it has no early return. */
 __device__ __forceinline__ void grain_template_body(GrainState* gs, const GrainParamsDev& prm,
                                                     const uint16_t* orbit, const uint16_t* pos,
                                                     GrainTemplateSmem& sm) {
@@ -1396,67 +1472,18 @@ __device__ __forceinline__ void grain_template_body(GrainState* gs, const GrainP
     }
   }
   __syncthreads();
-  const int lag = prm.ar_coeff_lag;
   const int arshift = prm.ar_coeff_shift_minus_6 + 6;
-  /* The auto-regressive filters run on one warp: a step of a wavefront has
-   * at most 73 samples (a row each), and its hundreds of dependent steps
-   * then meet a warp barrier instead of a CTA barrier each. The samples of
-   * a step depend only on earlier steps, so each step's order is free. */
-  if (tid < 32) {
-  /* luma AR filter */
-  if (prm.num_y_points > 0) {
-    const int W = 82, H = 73;
-    const int tmax = (W - 4) + 4 * (H - 1);
-    for (int t = 3 + 4 * 3; t <= tmax; ++t) {
-      for (int y = 3 + tid; y < H; y += 32) {
-        const int x = t - 4 * y;
-        if (x < 3 || x >= W - 3) continue;
-        int sum = 0, pos_ = 0;
-        for (int dr = -lag; dr <= 0; ++dr)
-          for (int dc = -lag; dc <= lag; ++dc) {
-            if (dr == 0 && dc == 0) goto done_l;
-            sum += luma[(y + dr) * W + x + dc] * prm.ar_y[pos_];
-            ++pos_;
-          }
-      done_l:
-        luma[y * W + x] = (short)clampi(luma[y * W + x] + rnd2z(sum, arshift), gmin, gmax);
-      }
-      __syncwarp();
+  /* the auto-regressive filters on the first five warps (a step of a
+   * wavefront has at most 73 luma or 146 chroma samples, one a thread), a
+   * named barrier between steps; the lag as a constant, so a sample's taps
+   * are independent loads */
+  if (tid < kGrainArThreads) {
+    switch (prm.ar_coeff_lag) {
+      case 0: grain_ar<0>(prm, luma, cb, cr, cw, ch, chroma, arshift, gmin, gmax, tid); break;
+      case 1: grain_ar<1>(prm, luma, cb, cr, cw, ch, chroma, arshift, gmin, gmax, tid); break;
+      case 2: grain_ar<2>(prm, luma, cb, cr, cw, ch, chroma, arshift, gmin, gmax, tid); break;
+      default: grain_ar<3>(prm, luma, cb, cr, cw, ch, chroma, arshift, gmin, gmax, tid); break;
     }
-  }
-  if (chroma) {
-    const int sx = prm.ss_x, sy = prm.ss_y;
-    const int tmax = (cw - 4) + 4 * (ch - 1);
-    for (int t = 3 + 4 * 3; t <= tmax; ++t) {
-      for (int k = tid; k < 2 * ch; k += 32) {
-        const int plane = k & 1, y = k >> 1;
-        if (y < 3) continue;
-        const int x = t - 4 * y;
-        if (x < 3 || x >= cw - 3) continue;
-        short* gp = plane ? cr : cb;
-        const int* co = plane ? prm.ar_cr : prm.ar_cb;
-        int sum = 0, pos_ = 0;
-        for (int dr = -lag; dr <= 0; ++dr)
-          for (int dc = -lag; dc <= lag; ++dc) {
-            if (dr == 0 && dc == 0) {
-              if (prm.num_y_points > 0) {
-                const int lx = ((x - 3) << sx) + 3, ly = ((y - 3) << sy) + 3;
-                int acc = 0;
-                for (int i = 0; i <= sy; ++i)
-                  for (int j = 0; j <= sx; ++j) acc += luma[(ly + i) * 82 + lx + j];
-                sum += rnd2z(acc, sx + sy) * co[pos_];
-              }
-              goto done_c;
-            }
-            sum += gp[(y + dr) * cw + x + dc] * co[pos_];
-            ++pos_;
-          }
-      done_c:
-        gp[y * cw + x] = (short)clampi(gp[y * cw + x] + rnd2z(sum, arshift), gmin, gmax);
-      }
-      __syncwarp();
-    }
-  }
   }
   __syncthreads();
   for (int k = tid; k < 82 * 73; k += blockDim.x) gs->luma[k] = luma[k];

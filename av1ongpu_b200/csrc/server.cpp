@@ -104,6 +104,7 @@ struct av1b_server {
   size_t hbm_used = 0, hbm_budget = 0;
   int inflight = 0;
   uint64_t submitted = 0, completed = 0, steps = 0, stepped_frames = 0;
+  double plan_ms = 0, launch_ms = 0;
   bool stop = false;
   std::vector<std::thread> planners;
   std::thread sched, completer;
@@ -157,6 +158,7 @@ void plan_loop(av1b_server* s) {
       }
       refs[i] = st->ring[(r->index - dist) % st->ring_n];
     }
+    const double t0 = now_ms(s);
     if (rc == AV1B_OK) {
       view.reference_slots = refs;
       /* returns once the frame's records and coefficients are on the device */
@@ -166,6 +168,7 @@ void plan_loop(av1b_server* s) {
       std::lock_guard<std::mutex> lk(s->mu);
       r->planned = true;
       r->plan_rc = rc;
+      s->plan_ms += now_ms(s) - t0;
     }
     s->cv_sched.notify_one();
   }
@@ -224,6 +227,28 @@ void sched_loop(av1b_server* s) {
         delete step;
         return;
       }
+      /* a batching window: with a step already queued on the GPU, a new one
+       * waits (up to batch_wait_us, or until the queued one completes) for a
+       * quarter of the open streams to have their next frame ready, so that
+       * steps do not shrink to a frame or two while the GPU is busy anyway */
+      if (s->inflight > 0 && s->opt.batch_wait_us > 0) {
+        auto count = [&] {
+          int ready_n = 0, open_n = 0;
+          for (const Stream* st : s->streams)
+            if (st && st->open) {
+              ++open_n;
+              ready_n += ready(st);
+            }
+          return ready_n * 4 >= open_n;
+        };
+        const int before = s->inflight;
+        s->cv_sched.wait_for(lk, std::chrono::microseconds(s->opt.batch_wait_us),
+                             [&] { return s->stop || s->inflight < before || count(); });
+        if (s->stop) {
+          delete step;
+          return;
+        }
+      }
       /* the oldest frames first, one a stream */
       std::vector<Stream*> cand;
       for (Stream* st : s->streams)
@@ -276,6 +301,7 @@ void sched_loop(av1b_server* s) {
       pitch[i] = static_cast<size_t>(st->desc.nv12_pitch);
       len[i] = st->nv12_bytes;
     }
+    const double t0 = now_ms(s);
     step->launch_rc = av1b_batch_decode(s->batch, n, decs.data(), plans.data(), slots.data(), out.data(),
                                         nv.data(), pitch.data(), len.data());
     step->rcs.assign(n, step->launch_rc);
@@ -292,6 +318,7 @@ void sched_loop(av1b_server* s) {
     {
       std::lock_guard<std::mutex> lk(s->mu);
       s->stepped_frames += n;
+      s->launch_ms += now_ms(s) - t0;
       s->done_q.push_back(step);
     }
     s->cv_done.notify_one();
@@ -359,6 +386,7 @@ int av1b_server_create(const av1b_server_options* options, av1b_server** out) {
     o.planner_threads = static_cast<int>(std::max(2u, hc / 2));
   }
   if (o.decoder_threads == 0) o.decoder_threads = 4;
+  if (o.batch_wait_us == 0) o.batch_wait_us = 1000;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return AV1B_ERR_NO_DEVICE;
   if (o.device < 0 || o.device >= ndev) return AV1B_ERR_ARG;
@@ -581,6 +609,8 @@ int av1b_server_get_stats(av1b_server* s, av1b_server_stats* out) {
   out->hbm_used = s->hbm_used;
   out->hbm_budget = s->hbm_budget;
   out->now_ms = now_ms(s);
+  out->plan_ms = s->plan_ms;
+  out->launch_ms = s->launch_ms;
   for (const Stream* st : s->streams)
     if (st) ++out->streams;
   return AV1B_OK;

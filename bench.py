@@ -836,6 +836,9 @@ def run_serving_leg(args, av1b, local):
     st = srv.stats()
     srv.close()
     at100 = [r for r in sweep if r['load'] == 1.0]
+    host = {'plan_ms_per_frame': st.plan_ms / max(1, st.completed),
+            'launch_ms_per_step': st.launch_ms / max(1, st.steps),
+            'frames_per_step': st.stepped_frames / max(1, st.steps)}
     return {
         'metric': 'p50/p99 frame ms and delivered Mpx/s (64 streams, Poisson arrivals)',
         'streams': '19x 640x360 8-bit, 22x 1280x720 8-bit, 16x 1920x1080 10-bit, 7x 3840x2160 10-bit; '
@@ -847,6 +850,7 @@ def run_serving_leg(args, av1b, local):
         'seconds_per_load': duration, 'sweep': sweep,
         'p99_1080p_ms_at_100': at100[0]['by_class'].get('1080p', {}).get('p99_ms') if at100 else None,
         'steps': st.steps, 'frames': st.completed, 'hbm_reserved_gb': st.hbm_used / 1e9,
+        'host': host,
     }
 
 

@@ -449,9 +449,12 @@ typedef struct av1b_server av1b_server;
 typedef struct av1b_server_options {
   int32_t device;
   int32_t max_batch;        /* frames a step (1..64; 0: 64) */
-  int32_t max_inflight;     /* steps queued on the GPU at once (1..8; 0: 2) */
+  int32_t max_inflight;     /* steps queued on the GPU at once (1..8; 0: 2); while one is
+                               queued, the next waits up to batch_wait_us for a quarter of
+                               the open streams to have a frame ready */
   int32_t planner_threads;  /* requests planned at once (0: cores / 2) */
   int32_t decoder_threads;  /* host threads planning one request (0: 4) */
+  int32_t batch_wait_us;    /* (0: 1000; negative: no wait) */
   size_t hbm_budget;        /* device memory the streams may hold (0: 90 % of the free memory) */
 } av1b_server_options;
 typedef struct av1b_stream_desc {
@@ -472,6 +475,8 @@ typedef struct av1b_server_stats {
   size_t hbm_used, hbm_budget;
   int32_t streams;
   double now_ms;
+  double plan_ms;           /* host time planning requests, summed over planner threads */
+  double launch_ms;         /* host time queueing steps (av1b_batch_decode) */
 } av1b_server_stats;
 AV1B_API int av1b_server_create(const av1b_server_options* options, av1b_server** out);
 AV1B_API int av1b_server_destroy(av1b_server* server);
