@@ -73,6 +73,7 @@ struct FilterArgs {
   LrArgs lr;
   /* film grain: templates from the parameters, then the blend cur -> disp */
   int grain;
+  const int* gs_src;              /* the plan's grain constants (GrainState from lut on) */
   GrainState* gs;
   GrainParamsDev gp;
   const uint16_t* orbit;

@@ -239,6 +239,14 @@ __global__ void __launch_bounds__(256) kb_grain_template(const StreamStep* __res
   for (int item = blockIdx.x; item < total; item += gridDim.x) {
     const int s = batch_stream(pfx, n, item);
     const FilterArgs& f = st[s].f;
+    /* the frame's grain constants and scaling tables, from its plan */
+    {
+      constexpr int tail = static_cast<int>(offsetof(GrainState, lut));
+      constexpr int words = static_cast<int>((sizeof(GrainState) - tail) / 4);
+      int* dst = reinterpret_cast<int*>(reinterpret_cast<char*>(f.gs) + tail);
+      for (int k = threadIdx.x; k < words; k += blockDim.x) dst[k] = f.gs_src[k];
+    }
+    __syncthreads();
     grain_template_body(f.gs, f.gp, f.orbit, f.pos, sm);
     __syncthreads();
   }

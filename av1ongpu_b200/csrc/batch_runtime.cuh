@@ -97,9 +97,8 @@ int fill_filter_args(av1b_decoder* d, av1b_plan* pl, StepPrep* sp) {
   d->disp_pending = false;
   if (P.grain) {
     GrainState* gsd = static_cast<GrainState*>(d->grain_state.p);
-    const size_t tail = offsetof(GrainState, lut);
-    CK(cudaMemcpyAsync(reinterpret_cast<uint8_t*>(gsd) + tail, ar + pl->o_gs, sizeof(GrainState) - tail,
-                       cudaMemcpyDeviceToDevice, d->stream), "grain constants");
+    /* the constants are copied from the plan by the template kernel */
+    f.gs_src = reinterpret_cast<const int*>(ar + pl->o_gs);
     f.grain = 1;
     f.gs = gsd;
     f.gp = P.gp;
@@ -255,7 +254,14 @@ int batch_step(av1b_batch* b, int n, av1b_decoder* const* decs, av1b_plan* const
   for (int i = 0; i < n; ++i) {
     av1b_decoder* d = decs[i];
     clear_err(d);
-    int rc = prepare_step(d, plans[i], 1, slots ? slots[i] : -1, true, &sp[i]);
+    /* the decoder's own stream, when a call queued work there since its last
+     * batched step: the step waits for it */
+    if (!d->batch_pending) {
+      if (!d->ev_batch) BCK(cudaEventCreateWithFlags(&d->ev_batch, cudaEventDisableTiming), "event");
+      BCK(cudaEventRecord(d->ev_batch, d->stream), "decoder order");
+      BCK(cudaStreamWaitEvent(b->stream, d->ev_batch, 0), "decoder order");
+    }
+    int rc = prepare_step(d, plans[i], 1, slots ? slots[i] : -1, true, &sp[i], b->stream);
     if (rc) return bfail(b, rc, "stream " + std::to_string(i) + ": " + d->err);
     FilterArgs& f = sp[i].f;
     const Plan& P = plans[i]->P;
@@ -275,8 +281,6 @@ int batch_step(av1b_batch* b, int n, av1b_decoder* const* decs, av1b_plan* const
                                             : static_cast<const px_t*>(d->disp.p);
       if (f.fuse_grain) d->disp_pending = true;
     }
-    if (!d->ev_batch) BCK(cudaEventCreateWithFlags(&d->ev_batch, cudaEventDisableTiming), "event");
-    BCK(cudaEventRecord(d->ev_batch, d->stream), "prepare order");
     units_inter = units_inter || P.units_inter;
     n_chains += P.n_chains;
   }
@@ -359,7 +363,6 @@ int batch_step(av1b_batch* b, int n, av1b_decoder* const* decs, av1b_plan* const
   }
   hh->chain_order = b->d_chains;
 
-  for (int i = 0; i < n; ++i) BCK(cudaStreamWaitEvent(b->stream, decs[i]->ev_batch, 0), "prepare wait");
   BCK(cudaMemcpyAsync(b->d_steps, hs, steps_bytes, cudaMemcpyHostToDevice, b->stream), "step upload");
   BCK(cudaMemcpyAsync(b->d_hdr, hh, sizeof(BatchHeader), cudaMemcpyHostToDevice, b->stream), "header upload");
   if (n_chains)
@@ -391,7 +394,7 @@ int batch_step(av1b_batch* b, int n, av1b_decoder* const* decs, av1b_plan* const
   b->last.assign(decs, decs + n);
   for (int i = 0; i < n; ++i) {
     int got = -1;
-    const int rc = commit_step(decs[i], plans[i], &sp[i], nullptr, &got, false, b->done);
+    const int rc = commit_step(decs[i], plans[i], &sp[i], nullptr, &got, false, b->stream);
     if (rc) return bfail(b, rc, "stream " + std::to_string(i) + ": " + decs[i]->err);
     if (out_slots) out_slots[i] = got;
   }

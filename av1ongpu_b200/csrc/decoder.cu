@@ -118,6 +118,11 @@ struct av1b_decoder {
    * the display picture is made from cur when an output call asks for it */
   bool disp_pending = false;
   cudaEvent_t ev_batch = nullptr;   /* a batched step's wait on this decoder's stream */
+  /* a batched step ran this decoder's frame on the batch's stream: the
+   * decoder's own stream joins it (waits for ev_after_batch) only when a call
+   * next queues work there, so back-to-back batched steps never wait on it */
+  bool batch_pending = false;
+  cudaEvent_t ev_after_batch = nullptr;
   DevBuf slot_buf[kSlots];
   bool slot_used[kSlots] = {false};
   bool slot_valid[kSlots] = {false};
@@ -204,6 +209,15 @@ void clear_err(av1b_decoder* d) {
 cudaError_t wait_stream(av1b_decoder* d) {
   const cudaError_t e = cudaEventRecord(d->ev_block, d->stream);
   return e != cudaSuccess ? e : cudaEventSynchronize(d->ev_block);
+}
+
+/* Orders the decoder's stream after its last batched step (see
+ * batch_pending). Called with the decoder lock, before queueing work. */
+void join_batch(av1b_decoder* d) {
+  if (d->batch_pending) {
+    cudaStreamWaitEvent(d->stream, d->ev_after_batch, 0);
+    d->batch_pending = false;
+  }
 }
 
 #define CK(call, what)                                     \
@@ -2083,7 +2097,7 @@ int fill_filter_args(av1b_decoder* d, av1b_plan* pl, StepPrep* sp);
  * arguments are filled for the batched kernels. Called with the decoder's
  * lock held. */
 int prepare_step(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, bool batched,
-                 StepPrep* sp) {
+                 StepPrep* sp, cudaStream_t st) {
   int rc;
   av1b_frame_syntax hdr{};
   hdr.width = pl->width;
@@ -2103,7 +2117,6 @@ int prepare_step(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, bool
   const Plan& P = pl->P;
   const Layout& L = d->L;
   const int maxv = (1 << pl->bit_depth) - 1;
-  cudaStream_t st = d->stream;
   cudaEvent_t* ev = d->ev;
 
   /* the destination slot */
@@ -2172,7 +2185,8 @@ int prepare_step(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, bool
   }
   /* the claim counter restarts every frame; the status word is sticky until
    * finish_frame has read it, so frames queued without a wait are covered */
-  CK(cudaMemsetAsync(d->status_q.p, 0, sizeof(unsigned), st), "queue reset");
+  if (!batched)   /* a batched step claims chains from its own counter */
+    CK(cudaMemsetAsync(d->status_q.p, 0, sizeof(unsigned), st), "queue reset");
 
   a.cur = static_cast<px_t*>(d->cur.p);
   a.slot_ptr = static_cast<px_t* const*>(d->slot_ptr_dev.p);
@@ -2371,13 +2385,13 @@ int launch_step_plain(av1b_decoder* d, av1b_plan* pl, StepPrep* sp) {
  * the decoder's stream - which first waits for `after` when the step ran on
  * another stream (a batched step). Called with the decoder's lock held. */
 int commit_step(av1b_decoder* d, av1b_plan* pl, StepPrep* sp, const av1b_planes* out, int* out_slot,
-                bool sync, cudaEvent_t after) {
+                bool sync, cudaStream_t batch_stream) {
   const Layout& L = d->L;
-  cudaStream_t st = d->stream;
+  /* a batched step's status copy and plan event go on the batch's stream */
+  cudaStream_t st = batch_stream ? batch_stream : d->stream;
   const FrameArgs& a = sp->a;
   const int keep = sp->keep, slot = sp->slot;
   const int launches = sp->launches;
-  if (after) CK(cudaStreamWaitEvent(st, after, 0), "batch order");
   const px_t* display = d->disp_is_cur ? static_cast<const px_t*>(d->cur.p)
                                        : static_cast<const px_t*>(d->disp.p);
 
@@ -2400,6 +2414,12 @@ int commit_step(av1b_decoder* d, av1b_plan* pl, StepPrep* sp, const av1b_planes*
   d->stats_pending = launches > 0;   /* a batched step times itself */
   CK(cudaEventRecord(pl->done, st), "event");
   pl->in_flight = true;
+  if (batch_stream) {
+    if (!d->ev_after_batch)
+      CK(cudaEventCreateWithFlags(&d->ev_after_batch, cudaEventDisableTiming), "event");
+    CK(cudaEventRecord(d->ev_after_batch, batch_stream), "event");
+    d->batch_pending = true;
+  }
   if (keep) {
     std::lock_guard<std::mutex> lk(d->slot_mu);
     d->slot_used[slot] = true;
@@ -2420,7 +2440,8 @@ int execute_plan(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, cons
   StepPrep sp;
   sp.defer_grain = out == nullptr;
   int rc;
-  if ((rc = prepare_step(d, pl, keep, forced_slot, false, &sp)) ||
+  join_batch(d);
+  if ((rc = prepare_step(d, pl, keep, forced_slot, false, &sp, d->stream)) ||
       (rc = launch_step_plain(d, pl, &sp)))
     return rc;
   return commit_step(d, pl, &sp, out, out_slot, sync, nullptr);
@@ -2590,7 +2611,10 @@ int av1b_decoder_create_ex(int device, size_t hbm_budget_bytes, const av1b_decod
 int av1b_decoder_destroy(av1b_decoder* d) {
   if (!d) return AV1B_ERR_ARG;
   cudaSetDevice(d->device);
-  if (d->stream) cudaStreamSynchronize(d->stream);
+  if (d->stream) {
+    join_batch(d);
+    cudaStreamSynchronize(d->stream);
+  }
   if (d->own_plan) release_plan(d, d->own_plan);
   for (av1b_plan* pl : d->plan_pool) release_plan(d, pl);
   d->plan_pool.clear();
@@ -2614,6 +2638,7 @@ int av1b_decoder_destroy(av1b_decoder* d) {
   if (d->ev_join) cudaEventDestroy(d->ev_join);
   if (d->ev_block) cudaEventDestroy(d->ev_block);
   if (d->ev_batch) cudaEventDestroy(d->ev_batch);
+  if (d->ev_after_batch) cudaEventDestroy(d->ev_after_batch);
   if (d->status_host) cudaFreeHost(d->status_host);
   for (auto& k : d->packs) {
     if (k.copied) cudaEventSynchronize(k.copied);
@@ -2638,6 +2663,7 @@ int av1b_decoder_destroy(av1b_decoder* d) {
 int av1b_decoder_reset(av1b_decoder* d) {
   if (!d) return AV1B_ERR_ARG;
   std::lock_guard<std::mutex> lk(d->mu);
+  join_batch(d);
   std::lock_guard<std::mutex> slk(d->slot_mu);
   for (int i = 0; i < kSlots; ++i) {
     d->slot_used[i] = false;
@@ -2776,6 +2802,7 @@ int av1b_decoder_memory(av1b_decoder* d, size_t* allocated, size_t* budget) {
 int av1b_sync(av1b_decoder* d) {
   if (!d) return AV1B_ERR_ARG;
   std::lock_guard<std::mutex> lk(d->mu);
+  join_batch(d);
   cudaSetDevice(d->device);
   return finish_frame(d);
 }
@@ -2848,6 +2875,7 @@ static int to_nv12_impl(av1b_decoder* d, int slot, size_t pitch, uint8_t* dst, s
                         bool device_dst) {
   if (!d || !dst) return AV1B_ERR_ARG;
   std::lock_guard<std::mutex> lk(d->mu);
+  join_batch(d);
   cudaSetDevice(d->device);
   int rc;
   {
@@ -2891,6 +2919,7 @@ int av1b_nv12_pack_begin(av1b_decoder* d, int slot, size_t pitch, int* out_handl
   if (!d || !out_handle) return AV1B_ERR_ARG;
   *out_handle = -1;
   std::lock_guard<std::mutex> lk(d->mu);
+  join_batch(d);
   cudaSetDevice(d->device);
   int rc;
   {
@@ -2984,6 +3013,7 @@ int av1b_nv12_pack_release(av1b_decoder* d, int handle) {
 int av1b_to_rgb(av1b_decoder* d, int slot, int matrix, int range, uint8_t* dst, size_t dst_len) {
   if (!d || !dst) return AV1B_ERR_ARG;
   std::lock_guard<std::mutex> lk(d->mu);
+  join_batch(d);
   cudaSetDevice(d->device);
   const px_t* pic = nullptr;
   int rc = picture_of(d, slot, &pic);
@@ -3010,6 +3040,7 @@ int av1b_get_stats(av1b_decoder* d, av1b_stats* out) {
 int av1b_poll_status(av1b_decoder* d, int* status) {
   if (!d || !status) return AV1B_ERR_ARG;
   std::lock_guard<std::mutex> lk(d->mu);
+  join_batch(d);
   cudaSetDevice(d->device);
   /* the status word of the frames whose work has finished: its copy into
    * page-locked memory is queued after each frame */
@@ -3026,6 +3057,7 @@ int av1b_poll_status(av1b_decoder* d, int* status) {
 int av1b_slot_planes_device(av1b_decoder* d, int slot, uint16_t* plane_ptr[3], int32_t stride[3]) {
   if (!d || !plane_ptr || !stride) return AV1B_ERR_ARG;
   std::lock_guard<std::mutex> lk(d->mu);
+  join_batch(d);
   const px_t* pic = nullptr;
   const int rc = picture_of(d, slot, &pic);
   if (rc) return rc;
@@ -3047,6 +3079,7 @@ int av1b_set_wait_limit(av1b_decoder* d, long long limit_ns) {
 int av1b_selftest_wait(av1b_decoder* d, long long limit_ns, int* status, double* elapsed_ms) {
   if (!d || !status || limit_ns <= 0 || limit_ns > 10000000000LL) return AV1B_ERR_ARG;
   std::lock_guard<std::mutex> lk(d->mu);
+  join_batch(d);
   cudaSetDevice(d->device);
   DevBuf mem;
   int rc = dev_ensure(d, mem, 256);
@@ -3080,6 +3113,7 @@ int av1b_set_unit_trace(av1b_decoder* d, int on) {
 int av1b_unit_trace(av1b_decoder* d, uint64_t* out, size_t cap, size_t* n) {
   if (!d || !n) return AV1B_ERR_ARG;
   std::lock_guard<std::mutex> lk(d->mu);
+  join_batch(d);
   cudaSetDevice(d->device);
   *n = d->trace_n;
   if (!out || d->trace_n == 0) return AV1B_OK;
