@@ -86,7 +86,8 @@ class ServerResult(ctypes.Structure):
                 ('batch_size', ctypes.c_int32), ('tag', ctypes.c_uint64),
                 ('frame_index', ctypes.c_uint64), ('step', ctypes.c_int64),
                 ('arrival_ms', ctypes.c_double), ('done_ms', ctypes.c_double),
-                ('latency_ms', ctypes.c_double), ('nv12_device', ctypes.c_void_p),
+                ('latency_ms', ctypes.c_double), ('planned_ms', ctypes.c_double),
+                ('nv12_device', ctypes.c_void_p),
                 ('nv12_bytes', ctypes.c_size_t)]
 
 

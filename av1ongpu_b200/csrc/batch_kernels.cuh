@@ -32,7 +32,9 @@ __device__ __forceinline__ int warp_claim(unsigned* ctr, int chunk, int lane) {
   return __shfl_sync(0xffffffffu, c, 0);
 }
 
-__global__ void __launch_bounds__(128) kb_inter_simple(const StreamStep* __restrict__ st,
+/* Five CTAs an SM: the lean tile body plus the loop fit 96 registers
+ * without spilling (unbounded, the compiler spilled). */
+__global__ void __launch_bounds__(128, 5) kb_inter_simple(const StreamStep* __restrict__ st,
                                                        BatchHeader* h, int chunk) {
   __shared__ McScratch scr[4];
   __shared__ int pred[4][2][8 * 16];

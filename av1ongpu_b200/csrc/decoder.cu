@@ -2592,11 +2592,16 @@ int av1b_decoder_create_ex(int device, size_t hbm_budget_bytes, const av1b_decod
     if (opt && opt->planner_threads > 0) threads = opt->planner_threads;
     if (opt && opt->planners > 0) planners = opt->planners;
     d->planners.resize(planners);
+    /* the planners' uploads and record conversions at the highest stream
+     * priority: a plan waits for them, and on a busy GPU (a batched step's
+     * persistent kernels) their few CTAs then go first */
+    int prio_lo = 0, prio_hi = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
     for (auto& q : d->planners) {
       q.pool = new WorkPool(threads);
       q.scratch = new PlanScratch;
       q.lists = new PlanLists;
-      if (cudaStreamCreateWithFlags(&q.upload, cudaStreamNonBlocking) != cudaSuccess) {
+      if (cudaStreamCreateWithPriority(&q.upload, cudaStreamNonBlocking, prio_hi) != cudaSuccess) {
         av1b_decoder_destroy(d);
         return AV1B_ERR_CUDA;
       }

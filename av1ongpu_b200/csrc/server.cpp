@@ -53,7 +53,7 @@ struct Request {
   uint64_t tag = 0, index = 0;
   const uint8_t* blob = nullptr;   /* the caller's, read until the frame is planned */
   size_t len = 0;
-  double arrival_ms = 0;
+  double arrival_ms = 0, planned_ms = 0;
   av1b_plan* plan = nullptr;
   int plan_rc = AV1B_OK;
   bool planned = false;
@@ -168,7 +168,8 @@ void plan_loop(av1b_server* s) {
       std::lock_guard<std::mutex> lk(s->mu);
       r->planned = true;
       r->plan_rc = rc;
-      s->plan_ms += now_ms(s) - t0;
+      r->planned_ms = now_ms(s);
+      s->plan_ms += r->planned_ms - t0;
     }
     s->cv_sched.notify_one();
   }
@@ -198,6 +199,7 @@ void post_result(av1b_server* s, const Request* r, int status, double done_ms, i
   res.arrival_ms = r->arrival_ms;
   res.done_ms = done_ms;
   res.latency_ms = done_ms - r->arrival_ms;
+  res.planned_ms = r->planned_ms;
   res.slot = slot;
   res.batch_size = batch;
   res.step = static_cast<int64_t>(step);

@@ -80,6 +80,9 @@ def parse():
     ap.add_argument('--no-batched', action='store_true', help='skip the batched leg')
     ap.add_argument('--batch-frames', type=int, default=120, help='frames per stream, batched leg')
     ap.add_argument('--no-serve', action='store_true', help='skip the served leg')
+    ap.add_argument('--only-batched', action='store_true',
+                    help='the batched leg alone, without the plain comparison or autotuning '
+                         '(a short run to profile the batched kernels)')
     ap.add_argument('--serve-seconds', type=float, default=1.5, help='arrival window per load point')
     return ap.parse_args()
 
@@ -346,10 +349,37 @@ def verify(av1b, dec, plans, ring, geo, frames):
     return True, frames, None
 
 
+def run_only_batched(args):
+    """A short batched run for profilers: plans, then every frame-set once."""
+    import torch
+    import av1ongpu_b200 as av1b
+    local = rank_info()[2]
+    torch.cuda.set_device(local)
+    streams = BATCH_STREAMS
+    F = args.batch_frames
+    decs = [av1b.Decoder(local, planners=1, planner_threads=2) for _ in streams]
+    rings = [[d.reserve_reference() for _ in range(4)] for d in decs]
+    plans = plan_streams(av1b, decs, rings, streams, F, 4000)
+    nv = []
+    for (w, h, _bd, _r) in streams:
+        pitch = (w + 63) // 64 * 64
+        n = av1b.nv12_size(w, h, 1, 1, pitch)
+        nv.append((torch.empty(n, dtype=torch.uint8, device='cuda:%d' % local), pitch, n))
+    batch = av1b.Batch(local)
+    for k in range(F):
+        batch.decode(decs, [plans[i][k] for i in range(len(streams))], slots=[r[k % 4] for r in rings],
+                     nv12=[(t.data_ptr(), p, n) for t, p, n in nv])
+    batch.sync()
+    print(json.dumps({'only_batched': True, 'frame_sets': F, 'streams': len(streams)}))
+    return 0
+
+
 def run_ours(args):
     import ctypes
     import torch
     import av1ongpu_b200 as av1b
+    if args.only_batched:
+        return run_only_batched(args)
 
     rank, world, local = rank_info()
     dist = None
@@ -755,7 +785,8 @@ def run_serving_leg(args, av1b, local):
             pools[(w, h, bd, refs)] = list(ex.map(
                 lambda k: av1b.synth_frame_ex(w, h, 0, bd, 64, av1b.TOOLS_ALL, 5000 + c, k, SERVE_GOP,
                                               max_refs=refs), range(SERVE_GOP)))
-    srv = av1b.Server(local, max_inflight=2, planner_threads=max(2, (os.cpu_count() or 4) // 2))
+    srv = av1b.Server(local, max_inflight=2, planner_threads=max(2, (os.cpu_count() or 4) // 2),
+                      decoder_threads=3)
     sids = []
     for (w, h, bd, refs) in streams:
         sid, _ = srv.open(w, h, bd, max_refs=refs, nv12_pitch=(w + 63) // 64 * 64)
@@ -800,11 +831,15 @@ def run_serving_leg(args, av1b, local):
         last = max(r.done_ms for r in res)
         mpx = sum(px[tags[r.tag]] for r in res if r.status == 0) / 1e6
         by = {}
+        plan_wait = {}
         for r in res:
-            by.setdefault(cls_name[streams[tags[r.tag]]], []).append(r.latency_ms)
+            c = cls_name[streams[tags[r.tag]]]
+            by.setdefault(c, []).append(r.latency_ms)
+            plan_wait.setdefault(c, []).append(r.planned_ms - r.arrival_ms)
         return {'offered_mpx_s': offered, 'delivered_mpx_s': mpx / ((last - first) / 1e3),
                 'frames': len(res), 'failed': sum(1 for r in res if r.status != 0),
                 'p50_ms': percentile(lat, 50), 'p99_ms': percentile(lat, 99),
+                'arrival_to_planned_p50_ms': {c: percentile(v, 50) for c, v in sorted(plan_wait.items())},
                 'mean_batch': sum(r.batch_size for r in res) / max(1, len(res)),
                 'by_class': {c: {'p50_ms': percentile(v, 50), 'p99_ms': percentile(v, 99),
                                  'frames': len(v)} for c, v in sorted(by.items())}}

@@ -467,6 +467,7 @@ typedef struct av1b_server_result {
   uint64_t tag, frame_index;
   int64_t step;
   double arrival_ms, done_ms, latency_ms;
+  double planned_ms;        /* when the frame's plan was ready (host clock) */
   const uint8_t* nv12_device;
   size_t nv12_bytes;
 } av1b_server_result;
