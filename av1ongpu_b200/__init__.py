@@ -73,11 +73,13 @@ class PlanInfo(ctypes.Structure):
 class BatchConfig(ctypes.Structure):
     """av1b_batch_config: the batched step's launch shape."""
     _fields_ = [('ctas_per_sm', ctypes.c_int32 * 24), ('claim_chunk', ctypes.c_int32),
-                ('fuse_grain_nv12', ctypes.c_int32), ('use_graph', ctypes.c_int32)]
+                ('fuse_grain_nv12', ctypes.c_int32), ('use_graph', ctypes.c_int32),
+                ('inter_variant', ctypes.c_int32)]
 
     def as_dict(self):
         return {'ctas_per_sm': list(self.ctas_per_sm)[:21], 'claim_chunk': self.claim_chunk,
-                'fuse_grain_nv12': self.fuse_grain_nv12, 'use_graph': self.use_graph}
+                'fuse_grain_nv12': self.fuse_grain_nv12, 'use_graph': self.use_graph,
+                'inter_variant': self.inter_variant}
 
 
 class ServerResult(ctypes.Structure):

@@ -106,13 +106,15 @@ struct BatchHeader {
   const int2* chain_order;
 };
 
-/* CTAs per SM of each persistent stage kernel and the items a warp claims at
- * once (the autotuner's knobs); fuse_grain_nv12: the grain of a frame whose
- * output is only its NV12 pack is applied inside the pack. */
+/* CTAs per SM of each persistent stage kernel, the items a warp claims at
+ * once, the build of the full prediction kernel (the autotuner's knobs);
+ * fuse_grain_nv12: the grain of a frame whose output is only its NV12 pack
+ * is applied inside the pack. */
 struct BatchTuning {
   int ctas_per_sm[kBStageCount];
   int claim_chunk;
   int fuse_grain_nv12;
+  int inter_variant;              /* the build of the full prediction kernel: 0 / 1 */
 };
 
 cudaError_t set_batch_kernel_attributes();

@@ -53,10 +53,13 @@ __global__ void __launch_bounds__(128, 5) kb_inter_simple(const StreamStep* __re
   }
 }
 
-/* Three CTAs an SM: the tile body needs the registers of the single-stream
- * kernel plus the loop's, which at four CTAs spilled. */
-__global__ void __launch_bounds__(128, 3) kb_inter(const StreamStep* __restrict__ st, BatchHeader* h,
-                                                   int chunk) {
+/* Two builds, the autotuner's choice (BatchTuning::inter_variant): at
+ * three CTAs an SM the tile body gets the registers it needs without
+ * spilling, at four it spills a little but more warps are resident and its
+ * code is smaller. */
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB) kb_inter(const StreamStep* __restrict__ st, BatchHeader* h,
+                                                      int chunk) {
   __shared__ McScratch scr[4];
   __shared__ int pred[4][2][8 * 16];
   __shared__ int lpred[4][2][4 * 8 * 16];
@@ -322,7 +325,8 @@ cudaError_t launch_batch_step(const StreamStep* steps, BatchHeader* hdr, const B
   mark(kBInterSimple);
   kb_inter_simple<<<batch_grid(t, kBInterSimple, n_sm), 128, 0, s>>>(steps, hdr, chunk);
   mark(kBInter);
-  kb_inter<<<batch_grid(t, kBInter, n_sm), 128, 0, s>>>(steps, hdr, chunk);
+  if (t.inter_variant) kb_inter<4><<<batch_grid(t, kBInter, n_sm), 128, 0, s>>>(steps, hdr, chunk);
+  else kb_inter<3><<<batch_grid(t, kBInter, n_sm), 128, 0, s>>>(steps, hdr, chunk);
   mark(kBItx2);
   launch_kb_itx<2>(steps, hdr, t, n_sm, s);
   mark(kBItx3);
@@ -387,7 +391,8 @@ cudaError_t set_batch_kernel_attributes() {
    * launch, inside a step, waiting for the kernels running) */
   cudaFuncAttributes fa;
   const void* ks[] = {
-      reinterpret_cast<const void*>(kb_inter_simple), reinterpret_cast<const void*>(kb_inter),
+      reinterpret_cast<const void*>(kb_inter_simple), reinterpret_cast<const void*>(kb_inter<3>),
+      reinterpret_cast<const void*>(kb_inter<4>),
       reinterpret_cast<const void*>(kb_itx<2>), reinterpret_cast<const void*>(kb_itx<3>),
       reinterpret_cast<const void*>(kb_itx<4>), reinterpret_cast<const void*>(kb_itx<5>),
       reinterpret_cast<const void*>(kb_deblock), reinterpret_cast<const void*>(kb_copy),
@@ -406,7 +411,7 @@ int batch_stage_max_ctas(int stage) {
   size_t smem = 0;
   switch (stage) {
     case kBInterSimple: k = reinterpret_cast<const void*>(kb_inter_simple); break;
-    case kBInter: k = reinterpret_cast<const void*>(kb_inter); break;
+    case kBInter: k = reinterpret_cast<const void*>(kb_inter<4>); break;
     case kBItx2: k = reinterpret_cast<const void*>(kb_itx<2>); smem = 4 * ItxScratch<2>::PER_WARP * sizeof(int); break;
     case kBItx3: k = reinterpret_cast<const void*>(kb_itx<3>); smem = 4 * ItxScratch<3>::PER_WARP * sizeof(int); break;
     case kBItx4: k = reinterpret_cast<const void*>(kb_itx<4>); smem = 4 * ItxScratch<4>::PER_WARP * sizeof(int); break;

@@ -185,6 +185,7 @@ void default_tuning(BatchTuning* t) {
   for (int k = 0; k < kBStageCount; ++k) t->ctas_per_sm[k] = ctas[k];
   t->claim_chunk = 1;
   t->fuse_grain_nv12 = 0;
+  t->inter_variant = 0;
   /* never more CTAs an SM than the kernel's resources let one SM hold */
   for (int k = 0; k < kBStageCount; ++k) t->ctas_per_sm[k] = std::min(t->ctas_per_sm[k], batch_stage_max_ctas(k));
 }
@@ -196,7 +197,7 @@ std::string tuning_key(const BatchTuning& t, bool units_inter) {
     std::snprintf(buf, sizeof(buf), ",%d", t.ctas_per_sm[s]);
     k += buf;
   }
-  std::snprintf(buf, sizeof(buf), ";%d", t.claim_chunk);
+  std::snprintf(buf, sizeof(buf), ";%d;%d", t.claim_chunk, t.inter_variant);
   return k + buf;
 }
 
@@ -450,19 +451,21 @@ std::string tune_signature(av1b_batch* b, int n, av1b_plan* const* plans, uint8_
 std::string tuning_text(const BatchTuning& t) {
   std::string s;
   for (int k = 0; k < kBStageCount; ++k) s += std::to_string(t.ctas_per_sm[k]) + " ";
-  return s + std::to_string(t.claim_chunk) + " " + std::to_string(t.fuse_grain_nv12);
+  return s + std::to_string(t.claim_chunk) + " " + std::to_string(t.fuse_grain_nv12) + " " +
+         std::to_string(t.inter_variant);
 }
 
 bool parse_tuning(const std::string& s, BatchTuning* t) {
   BatchTuning r{};
   const char* p = s.c_str();
   char* end = nullptr;
-  for (int k = 0; k < kBStageCount + 2; ++k) {
+  for (int k = 0; k < kBStageCount + 3; ++k) {
     const long v = std::strtol(p, &end, 10);
     if (end == p || v < 0 || v > 64) return false;
     if (k < kBStageCount) r.ctas_per_sm[k] = static_cast<int>(v);
     else if (k == kBStageCount) r.claim_chunk = static_cast<int>(v);
-    else r.fuse_grain_nv12 = static_cast<int>(v);
+    else if (k == kBStageCount + 1) r.fuse_grain_nv12 = static_cast<int>(v);
+    else r.inter_variant = static_cast<int>(v) ? 1 : 0;
     p = end;
   }
   if (r.claim_chunk < 1) return false;
@@ -646,6 +649,7 @@ static void to_config(const av1b_batch* b, av1b_batch_config* c) {
   c->claim_chunk = b->tuning.claim_chunk;
   c->fuse_grain_nv12 = b->tuning.fuse_grain_nv12;
   c->use_graph = b->use_graph ? 1 : 0;
+  c->inter_variant = b->tuning.inter_variant;
 }
 
 int av1b_batch_get_config(av1b_batch* b, av1b_batch_config* out) {
@@ -666,6 +670,7 @@ int av1b_batch_set_config(av1b_batch* b, const av1b_batch_config* c) {
   if (c->claim_chunk < 0 || c->claim_chunk > 64) return bfail(b, AV1B_ERR_ARG, "claim chunk out of range");
   if (c->claim_chunk > 0) t.claim_chunk = c->claim_chunk;
   t.fuse_grain_nv12 = c->fuse_grain_nv12 ? 1 : 0;
+  t.inter_variant = c->inter_variant ? 1 : 0;
   b->tuning = t;
   b->use_graph = c->use_graph != 0;
   return AV1B_OK;
@@ -730,6 +735,15 @@ int av1b_batch_autotune(av1b_batch* b, int n, av1b_decoder* const* decoders,
   for (int chunk : {2, 4}) {
     BatchTuning keep = b->tuning;
     b->tuning.claim_chunk = chunk;
+    double ms = 0;
+    if ((rc = time_step(b, n, decoders, plans, slots, nv12_device, nv12_pitch, nv12_len, reps, &ms)))
+      return rc;
+    if (ms < best) best = ms;
+    else b->tuning = keep;
+  }
+  {
+    BatchTuning keep = b->tuning;
+    b->tuning.inter_variant = 1 - keep.inter_variant;
     double ms = 0;
     if ((rc = time_step(b, n, decoders, plans, slots, nv12_device, nv12_pitch, nv12_len, reps, &ms)))
       return rc;

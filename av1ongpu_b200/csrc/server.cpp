@@ -71,6 +71,7 @@ struct Stream {
   uint64_t next_launch = 0;      /* the next frame a step may take */
   std::deque<Request*> pending;  /* submitted, not yet in a step, in order */
   int planning = 0;              /* frames taken by a planner and not yet complete */
+  double plan_cost_ms = 0;       /* expected planning time of one of its frames */
   uint8_t* nv12[kOutRing] = {nullptr};
   size_t nv12_bytes = 0;
   int in_steps = 0;              /* frames of the stream in steps not yet complete */
@@ -127,10 +128,24 @@ void plan_loop(av1b_server* s) {
        * bounded number of plans (and so of device memory) */
       std::unique_lock<std::mutex> lk(s->mu);
       std::deque<Request*>::iterator it;
+      /* of the requests whose stream may plan another frame, the one whose
+       * plan is expected to finish first (arrival + a cost by frame size):
+       * a small frame does not queue behind the plans of 4K frames that
+       * arrived just before it, and a large one waits at most its own cost */
       auto pick = [&] {
-        for (it = s->plan_q.begin(); it != s->plan_q.end(); ++it)
-          if (s->streams[(*it)->stream]->planning < kPlanAhead) return true;
-        return false;
+        double best = 0;
+        bool found = false;
+        for (auto i = s->plan_q.begin(); i != s->plan_q.end(); ++i) {
+          const Stream* q = s->streams[(*i)->stream];
+          if (q->planning >= kPlanAhead) continue;
+          const double key = (*i)->arrival_ms + q->plan_cost_ms;
+          if (!found || key < best) {
+            best = key;
+            it = i;
+            found = true;
+          }
+        }
+        return found;
       };
       s->cv_plan.wait(lk, [&] { return s->stop || pick(); });
       if (s->stop) return;   /* requests left unplanned are freed with the server */
@@ -387,7 +402,6 @@ int av1b_server_create(const av1b_server_options* options, av1b_server** out) {
     const unsigned hc = std::thread::hardware_concurrency();
     o.planner_threads = static_cast<int>(std::max(2u, hc / 2));
   }
-  if (o.decoder_threads == 0) o.decoder_threads = 4;
   if (o.batch_wait_us == 0) o.batch_wait_us = 1000;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return AV1B_ERR_NO_DEVICE;
@@ -483,7 +497,13 @@ int av1b_server_open(av1b_server* s, const av1b_stream_desc* desc, int* stream_i
   st->desc = d;
   st->ring_n = ring_n;
   st->hbm = need;
-  av1b_decoder_options dopt{1, s->opt.decoder_threads};
+  /* planner threads by frame size (0: a thread per 1.5 million samples, 1..6) */
+  const double px = static_cast<double>(d.width) * d.height;
+  const int threads = s->opt.decoder_threads > 0
+                          ? s->opt.decoder_threads
+                          : std::min(6, std::max(1, static_cast<int>(px / 1.5e6 + 0.5)));
+  st->plan_cost_ms = px * 1.6e-6 / std::min(threads, 4);
+  av1b_decoder_options dopt{1, threads};
   int rc = av1b_decoder_create_ex(s->opt.device, need - kOutRing * nv12, &dopt, &st->dec);
   for (int i = 0; rc == AV1B_OK && i < ring_n; ++i) rc = av1b_reserve_reference(st->dec, &st->ring[i]);
   if (rc == AV1B_OK && nv12) {

@@ -785,8 +785,7 @@ def run_serving_leg(args, av1b, local):
             pools[(w, h, bd, refs)] = list(ex.map(
                 lambda k: av1b.synth_frame_ex(w, h, 0, bd, 64, av1b.TOOLS_ALL, 5000 + c, k, SERVE_GOP,
                                               max_refs=refs), range(SERVE_GOP)))
-    srv = av1b.Server(local, max_inflight=2, planner_threads=max(2, (os.cpu_count() or 4) // 2),
-                      decoder_threads=3)
+    srv = av1b.Server(local, max_inflight=2, planner_threads=max(2, (os.cpu_count() or 4) // 2))
     sids = []
     for (w, h, bd, refs) in streams:
         sid, _ = srv.open(w, h, bd, max_refs=refs, nv12_pitch=(w + 63) // 64 * 64)

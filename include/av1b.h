@@ -386,6 +386,7 @@ typedef struct av1b_batch_config {
   int32_t claim_chunk;
   int32_t fuse_grain_nv12;
   int32_t use_graph;
+  int32_t inter_variant;    /* the build of the full prediction kernel (0: fewer CTAs, more registers) */
 } av1b_batch_config;
 AV1B_API int av1b_batch_create(int device, av1b_batch** out);
 AV1B_API int av1b_batch_destroy(av1b_batch* batch);
@@ -399,7 +400,8 @@ AV1B_API int av1b_batch_set_config(av1b_batch* batch, const av1b_batch_config* c
 /* The autotuner: picks the launch shape for a set of streams by timing the
  * given step (decoded again and again: its slots must not be among the
  * slots its frames read) with each candidate - CTAs per SM per stage group,
- * the claim size, the grain-in-pack fusion - by coordinate descent, `reps`
+ * the claim size, the build of the full prediction kernel, the grain-in-pack
+ * fusion - by coordinate descent, `reps`
  * timed steps each. The result is kept in `cache_path` (nullable), one line
  * per signature of the step (GPU, SM count, each stream's geometry, bit
  * depth and tools), and a later call with the same signature takes it from
@@ -453,7 +455,7 @@ typedef struct av1b_server_options {
                                queued, the next waits up to batch_wait_us for a quarter of
                                the open streams to have a frame ready */
   int32_t planner_threads;  /* requests planned at once (0: cores / 2) */
-  int32_t decoder_threads;  /* host threads planning one request (0: 4) */
+  int32_t decoder_threads;  /* host threads planning one request (0: by frame size, 1..6) */
   int32_t batch_wait_us;    /* (0: 1000; negative: no wait) */
   size_t hbm_budget;        /* device memory the streams may hold (0: 90 % of the free memory) */
 } av1b_server_options;
