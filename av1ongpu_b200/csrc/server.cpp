@@ -497,11 +497,11 @@ int av1b_server_open(av1b_server* s, const av1b_stream_desc* desc, int* stream_i
   st->desc = d;
   st->ring_n = ring_n;
   st->hbm = need;
-  /* planner threads by frame size (0: a thread per 1.5 million samples, 1..6) */
+  /* planner threads by frame size (0: a thread per 0.7 million samples, 1..6) */
   const double px = static_cast<double>(d.width) * d.height;
   const int threads = s->opt.decoder_threads > 0
                           ? s->opt.decoder_threads
-                          : std::min(6, std::max(1, static_cast<int>(px / 1.5e6 + 0.5)));
+                          : std::min(6, std::max(1, static_cast<int>(px / 0.7e6 + 0.5)));
   st->plan_cost_ms = px * 1.6e-6 / std::min(threads, 4);
   av1b_decoder_options dopt{1, threads};
   int rc = av1b_decoder_create_ex(s->opt.device, need - kOutRing * nv12, &dopt, &st->dec);

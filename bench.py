@@ -785,6 +785,20 @@ def run_serving_leg(args, av1b, local):
             pools[(w, h, bd, refs)] = list(ex.map(
                 lambda k: av1b.synth_frame_ex(w, h, 0, bd, 64, av1b.TOOLS_ALL, 5000 + c, k, SERVE_GOP,
                                               max_refs=refs), range(SERVE_GOP)))
+    # the requests in page-locked memory, as a server receives them: a plan's
+    # upload of the frame's coefficients then runs at the copy engines' rate
+    import ctypes
+    import torch
+    for key, blobs in pools.items():
+        pinned = []
+        for b in blobs:
+            t = torch.empty(b.size + 64, dtype=torch.uint8, pin_memory=True)
+            off = (-t.data_ptr()) % 64
+            ctypes.memmove(t.data_ptr() + off, b.ptr, b.size)
+            pb = av1b.Blob(t.data_ptr() + off, b.size, False)
+            pb._keep = t
+            pinned.append(pb)
+        pools[key] = pinned
     srv = av1b.Server(local, max_inflight=2, planner_threads=max(2, (os.cpu_count() or 4) // 2))
     sids = []
     for (w, h, bd, refs) in streams:

@@ -455,7 +455,8 @@ typedef struct av1b_server_options {
                                queued, the next waits up to batch_wait_us for a quarter of
                                the open streams to have a frame ready */
   int32_t planner_threads;  /* requests planned at once (0: cores / 2) */
-  int32_t decoder_threads;  /* host threads planning one request (0: by frame size, 1..6) */
+  int32_t decoder_threads;  /* host threads planning one request (0: one per 0.7 million
+                               samples of the stream's frames, 1..6) */
   int32_t batch_wait_us;    /* (0: 1000; negative: no wait) */
   size_t hbm_budget;        /* device memory the streams may hold (0: 90 % of the free memory) */
 } av1b_server_options;
