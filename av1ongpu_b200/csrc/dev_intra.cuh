@@ -264,7 +264,10 @@ AV1B_DEV void intra_predict(const IntraJob& j, px_t* dst, int stride, const px_t
   if (j.mode == 13 && fi_pred && n <= 1024) {
     /* chroma from luma, each sample's luma value read once: kept in the
      * filter-intra buffer (unused by a CFL block) between the average and the
-     * prediction, and fetched four iterations at a time */
+     * prediction. The (up to four) luma samples of a chroma sample are read
+     * from neighbouring positions clamped to the block: every load of an
+     * iteration is issued before any is used (one round trip to L2, not one
+     * per sample), four iterations at a time. */
     const int dc = intra_dc(j, above, left, lane);
     const int sx = j.ss_x, sy = j.ss_y;
     const int lxl = ((j.x + w) << sx) - (1 << sx);
@@ -274,10 +277,15 @@ AV1B_DEV void intra_predict(const IntraJob& j, px_t* dst, int stride, const px_t
     for (int k = lane; k < n; k += 32) {
       const int i = k >> lw, jj = k & (w - 1);
       const int ly = mini((j.y + i) << sy, lyl), lx = mini((j.x + jj) << sx, lxl);
-      int t = 0;
-      for (int a = 0; a <= sy; ++a)
-        for (int b = 0; b <= sx; ++b) t += ldpx(luma + (ly + a) * luma_stride + lx + b);
-      t <<= 3 - sx - sy;
+      const px_t* p0 = luma + ly * luma_stride + lx;
+      const px_t* p1 = p0 + (sy ? luma_stride : 0);
+      const int v00 = ldpx(p0), v01 = ldpx(p0 + sx), v10 = ldpx(p1), v11 = ldpx(p1 + sx);
+      /* the sum of the 1, 2 or 4 samples the subsampling averages, scaled to 8x */
+      int t;
+      if (sx && sy) t = (v00 + v01 + v10 + v11) << 1;
+      else if (sx) t = (v00 + v01) << 2;
+      else if (sy) t = (v00 + v10) << 2;
+      else t = v00 << 3;
       fi_pred[k] = t;
       sum += t;
     }

@@ -59,13 +59,19 @@ w('''/*
  * AV1B_TABLE is the storage class: __device__ for the CUDA build (global
  * memory, read through the L1 so that divergent indices do not serialize the
  * way a __constant__ bank would), plain static const for host code.
+ * AV1B_CTABLE: the constant bank, for the small tables a warp reads at one
+ * index at a time on the dependency-scheduled path (the mode's angle, its
+ * derivative, the edge kernel), whose every L1 miss there is a round trip on
+ * the frame's critical path.
  */
 #ifndef AV1B_TABLES_H
 #define AV1B_TABLES_H
 #if defined(__CUDACC__)
 #define AV1B_TABLE static __device__ const
+#define AV1B_CTABLE static __constant__ const
 #else
 #define AV1B_TABLE static const
+#define AV1B_CTABLE static const
 #endif
 ''')
 w('#define AV1B_SINPI_1_9 %d' % define(tables_h, 'AV1G_SINPI_1_9'))
@@ -76,16 +82,16 @@ w('')
 w('/* cos128(a) = round(4096 cos(a pi / 128)) for a = 0..64 */')
 w(emit('kCos128', 'short', [65], numbers(tables_h, r'av1g_tbl_cos128\[65\]', 65)))
 w('/* Mode_To_Angle for the thirteen non-CFL intra modes */')
-w(emit('kModeAngle', 'short', [13], numbers(tables_h, r'av1g_tbl_mode_to_angle\[13\]', 13)))
+w(emit('kModeAngle', 'short', [13], numbers(tables_h, r'av1g_tbl_mode_to_angle\[13\]', 13), storage='AV1B_CTABLE'))
 w('/* Dr_Intra_Derivative, indexed by the angle in degrees (0..89) */')
-w(emit('kDrDeriv', 'short', [90], numbers(tables_h, r'av1g_tbl_dr_deriv\[90\]', 90)))
+w(emit('kDrDeriv', 'short', [90], numbers(tables_h, r'av1g_tbl_dr_deriv\[90\]', 90), storage='AV1B_CTABLE'))
 sm = []
 for n in (4, 8, 16, 32, 64):
     sm += numbers(tables_h, r'av1g_tbl_sm_w%d\[%d\]' % (n, n), n)
 w('/* Sm_Weights_Tx_4x4 .. 64x64 back to back: size n starts at n - 4 */')
 w(emit('kSmWeights', 'short', [124], sm))
 w('/* Intra_Edge_Kernel[strength - 1][tap] */')
-w(emit('kEdgeKernel', 'short', [15], numbers(tables_h, r'av1g_tbl_edge_kernel\[3\]\[5\]', 15)))
+w(emit('kEdgeKernel', 'short', [15], numbers(tables_h, r'av1g_tbl_edge_kernel\[3\]\[5\]', 15), storage='AV1B_CTABLE'))
 w('/* Intra_Filter_Taps[mode][position 0..7][tap 0..6] */')
 w(emit('kFilterIntraTaps', 'signed char', [280],
        numbers(tables_h, r'av1g_tbl_filter_intra\[5\]\[8\]\[7\]', 280), per_line=14))
