@@ -14,15 +14,14 @@
  * barrier between items.
  */
 
-/* The stream of item `item` of a stage: the s with pfx[s] <= item < pfx[s + 1]. */
-__device__ __forceinline__ int batch_stream(const int* __restrict__ pfx, int n, int item) {
-  int lo = 0, hi = n;
-  while (hi - lo > 1) {
-    const int mid = (lo + hi) >> 1;
-    if (pfx[mid] <= item) lo = mid;
-    else hi = mid;
-  }
-  return lo;
+/* The stream of item `item` of a stage - the s with pfx[s] <= item <
+ * pfx[s + 1] - for items a warp or CTA visits in increasing order (claims
+ * from a counter, or strides): the search starts at the stream of the item
+ * before, `s`, and moves forward over the streams in between, one comparison
+ * for most items. */
+__device__ __forceinline__ int batch_stream_next(const int* __restrict__ pfx, int n, int item, int s) {
+  while (s + 1 < n && pfx[s + 1] <= item) ++s;
+  return s;
 }
 
 /* The first of `chunk` consecutive items the warp claims (uniform over it). */
@@ -41,12 +40,13 @@ __global__ void __launch_bounds__(128, 5) kb_inter_simple(const StreamStep* __re
   const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int* pfx = h->pfx[kBInterSimple];
   const int n = h->n, total = pfx[n];
+  int s = 0;
   for (;;) {
     const int i0 = warp_claim(&h->claim[kBInterSimple], chunk, lane);
     if (i0 >= total) break;
     const int i1 = mini(i0 + chunk, total);
     for (int i = i0; i < i1; ++i) {
-      const int s = batch_stream(pfx, n, i);
+      s = batch_stream_next(pfx, n, i, s);
       inter_simple_tile(st[s].a, i - pfx[s], scr[wib], pred[wib], lane);
       __syncwarp();
     }
@@ -66,12 +66,13 @@ __global__ void __launch_bounds__(128, MINB) kb_inter(const StreamStep* __restri
   const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int* pfx = h->pfx[kBInter];
   const int n = h->n, total = pfx[n];
+  int s = 0;
   for (;;) {
     const int i0 = warp_claim(&h->claim[kBInter], chunk, lane);
     if (i0 >= total) break;
     const int i1 = mini(i0 + chunk, total);
     for (int i = i0; i < i1; ++i) {
-      const int s = batch_stream(pfx, n, i);
+      s = batch_stream_next(pfx, n, i, s);
       const FrameArgs& a = st[s].a;
       inter_full_tile(a, a.n_inter_simple + (i - pfx[s]), scr[wib], pred[wib], lpred[wib], lane);
       __syncwarp();
@@ -88,12 +89,13 @@ __global__ void __launch_bounds__(128) kb_itx(const StreamStep* __restrict__ st,
   int* wsm = smem + wib * ItxScratch<CLS>::PER_WARP;
   const int* pfx = h->pfx[STAGE];
   const int n = h->n, total = pfx[n];
+  int s = 0;
   for (;;) {
     const int i0 = warp_claim(&h->claim[STAGE], chunk, lane);
     if (i0 >= total) break;
     const int i1 = mini(i0 + chunk, total);
     for (int i = i0; i < i1; ++i) {
-      const int s = batch_stream(pfx, n, i);
+      s = batch_stream_next(pfx, n, i, s);
       const FrameArgs& a = st[s].a;
       itx_batch<CLS>(a, a.itx_batches[a.itx_class_first[CLS] + (i - pfx[s])], wsm, lane);
       __syncwarp();
@@ -122,22 +124,21 @@ __global__ void __launch_bounds__(128) kb_units(const StreamStep* __restrict__ s
   }
 }
 
+/* Deblocking edges, a warp each: the warps stride over the edges (an edge
+ * is a few cycles of work, so a claim from a counter would cost as much) */
 __global__ void __launch_bounds__(256) kb_deblock(const StreamStep* __restrict__ st, BatchHeader* h,
-                                                  int vertical, int chunk) {
+                                                  int vertical) {
   const int lane = threadIdx.x & 31;
   const int stage = vertical ? kBDeblockV : kBDeblockH;
   const int* pfx = h->pfx[stage];
   const int n = h->n, total = pfx[n];
-  for (;;) {
-    const int i0 = warp_claim(&h->claim[stage], chunk, lane);
-    if (i0 >= total) break;
-    const int i1 = mini(i0 + chunk, total);
-    for (int i = i0; i < i1; ++i) {
-      const int s = batch_stream(pfx, n, i);
-      const FilterArgs& f = st[s].f;
-      const DeblockRec r = (vertical ? f.dbv : f.dbh)[i - pfx[s]];
-      deblock_edge(st[s].a.cur, r, f.sharpness, f.bd, f.maxv, lane);
-    }
+  int s = 0;
+  const int warps = static_cast<int>(gridDim.x * (blockDim.x >> 5));
+  for (int i = static_cast<int>(blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)); i < total; i += warps) {
+    s = batch_stream_next(pfx, n, i, s);
+    const FilterArgs& f = st[s].f;
+    const DeblockRec r = (vertical ? f.dbv : f.dbh)[i - pfx[s]];
+    deblock_edge(st[s].a.cur, r, f.sharpness, f.bd, f.maxv, lane);
   }
 }
 
@@ -147,8 +148,9 @@ __global__ void __launch_bounds__(256) kb_copy(const StreamStep* __restrict__ st
   const int stage = which == 0 ? kBCopySnap : (which == 1 ? kBCopyPost : kBCopyRef);
   const int* pfx = h->pfx[stage];
   const int n = h->n, total = pfx[n];
+  int s = 0;
   for (int item = blockIdx.x; item < total; item += gridDim.x) {
-    const int s = batch_stream(pfx, n, item);
+    s = batch_stream_next(pfx, n, item, s);
     const FilterArgs& f = st[s].f;
     const long long off = static_cast<long long>(item - pfx[s]) * AV1B_COPY_ITEM;
     const long long left = f.copy_bytes[which] - off;
@@ -164,8 +166,9 @@ __global__ void __launch_bounds__(128) kb_cdef_search(const StreamStep* __restri
                                                       const BatchHeader* __restrict__ h) {
   const int* pfx = h->pfx[kBCdefSearch];
   const int n = h->n, total = pfx[n];
+  int s = 0;
   for (int item = blockIdx.x; item < total; item += gridDim.x) {
-    const int s = batch_stream(pfx, n, item);
+    s = batch_stream_next(pfx, n, item, s);
     const FilterArgs& f = st[s].f;
     const int t = (item - pfx[s]) * 128 + static_cast<int>(threadIdx.x);
     if (t < f.cdef_n_grid + f.n_cdef_extra)
@@ -182,8 +185,9 @@ __global__ void __launch_bounds__(128) kb_cdef(const StreamStep* __restrict__ st
   const unsigned hmask = 0xffffu << (threadIdx.x & 16);
   const int* pfx = h->pfx[kBCdef];
   const int n = h->n, total = pfx[n];
+  int s = 0;
   for (int item = blockIdx.x; item < total; item += gridDim.x) {
-    const int s = batch_stream(pfx, n, item);
+    s = batch_stream_next(pfx, n, item, s);
     const FilterArgs& f = st[s].f;
     const int ri = (item - pfx[s]) * 8 + hw;
     if (ri < f.n_cdef) {
@@ -203,8 +207,9 @@ __global__ void __launch_bounds__(64) kb_upscale(const StreamStep* __restrict__ 
   __syncthreads();
   const int* pfx = h->pfx[kBUpscale];
   const int n = h->n, total = pfx[n];
+  int s = 0;
   for (int item = blockIdx.x; item < total; item += gridDim.x) {
-    const int s = batch_stream(pfx, n, item);
+    s = batch_stream_next(pfx, n, item, s);
     const FilterArgs& f = st[s].f;
     int local = item - pfx[s];
     const int pass = local < f.up_items[0] ? 0 : 1;
@@ -222,8 +227,9 @@ __global__ void __launch_bounds__(256) kb_lr(const StreamStep* __restrict__ st,
   __shared__ LrSmem sm;
   const int* pfx = h->pfx[kBLr];
   const int n = h->n, total = pfx[n];
+  int s = 0;
   for (int item = blockIdx.x; item < total; item += gridDim.x) {
-    const int s = batch_stream(pfx, n, item);
+    s = batch_stream_next(pfx, n, item, s);
     const FilterArgs& f = st[s].f;
     int local = item - pfx[s];
     const int bx = local % f.lr_tiles;
@@ -241,8 +247,9 @@ __global__ void __launch_bounds__(256) kb_grain_template(const StreamStep* __res
   __shared__ GrainTemplateSmem sm;
   const int* pfx = h->pfx[kBGrainTemplate];
   const int n = h->n, total = pfx[n];
+  int s = 0;
   for (int item = blockIdx.x; item < total; item += gridDim.x) {
-    const int s = batch_stream(pfx, n, item);
+    s = batch_stream_next(pfx, n, item, s);
     const FilterArgs& f = st[s].f;
     /* the frame's grain constants and scaling tables, from its plan */
     {
@@ -261,8 +268,9 @@ __global__ void __launch_bounds__(128) kb_grain_blend(const StreamStep* __restri
                                                       const BatchHeader* __restrict__ h) {
   const int* pfx = h->pfx[kBGrain];
   const int n = h->n, total = pfx[n];
+  int s = 0;
   for (int item = blockIdx.x; item < total; item += gridDim.x) {
-    const int s = batch_stream(pfx, n, item);
+    s = batch_stream_next(pfx, n, item, s);
     const FilterArgs& f = st[s].f;
     const int local = item - pfx[s];
     const int y = local / f.grain_xblocks, xb = local - y * f.grain_xblocks;
@@ -275,8 +283,9 @@ __global__ void __launch_bounds__(128) kb_nv12(const StreamStep* __restrict__ st
                                                const BatchHeader* __restrict__ h) {
   const int* pfx = h->pfx[kBNv12];
   const int n = h->n, total = pfx[n];
+  int s = 0;
   for (int item = blockIdx.x; item < total; item += gridDim.x) {
-    const int s = batch_stream(pfx, n, item);
+    s = batch_stream_next(pfx, n, item, s);
     const FilterArgs& f = st[s].f;
     const int local = item - pfx[s];
     const int row = local / f.nv12_xblocks, xb = local - row * f.nv12_xblocks;
@@ -347,9 +356,9 @@ cudaError_t launch_batch_step(const StreamStep* steps, BatchHeader* hdr, const B
     else kb_units<false><<<grid, 128, smem, s>>>(steps, hdr);
   }
   mark(kBDeblockV);
-  kb_deblock<<<batch_grid(t, kBDeblockV, n_sm), 256, 0, s>>>(steps, hdr, 1, chunk);
+  kb_deblock<<<batch_grid(t, kBDeblockV, n_sm), 256, 0, s>>>(steps, hdr, 1);
   mark(kBDeblockH);
-  kb_deblock<<<batch_grid(t, kBDeblockH, n_sm), 256, 0, s>>>(steps, hdr, 0, chunk);
+  kb_deblock<<<batch_grid(t, kBDeblockH, n_sm), 256, 0, s>>>(steps, hdr, 0);
   mark(kBCopySnap);
   kb_copy<<<batch_grid(t, kBCopySnap, n_sm), 256, 0, s>>>(steps, hdr, 0);
   mark(kBCdefSearch);
