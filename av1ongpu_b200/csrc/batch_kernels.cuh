@@ -124,8 +124,9 @@ __global__ void __launch_bounds__(128) kb_units(const StreamStep* __restrict__ s
   }
 }
 
-/* Deblocking edges, a warp each: the warps stride over the edges (an edge
- * is a few cycles of work, so a claim from a counter would cost as much) */
+/* Deblocking edges, AV1B_DB_GROUP records an item, a warp each: the warps
+ * stride over the items (an item is a few cycles of work, so a claim from a
+ * counter would cost as much) */
 __global__ void __launch_bounds__(256) kb_deblock(const StreamStep* __restrict__ st, BatchHeader* h,
                                                   int vertical) {
   const int lane = threadIdx.x & 31;
@@ -137,8 +138,10 @@ __global__ void __launch_bounds__(256) kb_deblock(const StreamStep* __restrict__
   for (int i = static_cast<int>(blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)); i < total; i += warps) {
     s = batch_stream_next(pfx, n, i, s);
     const FilterArgs& f = st[s].f;
-    const DeblockRec r = (vertical ? f.dbv : f.dbh)[i - pfx[s]];
-    deblock_edge(st[s].a.cur, r, f.sharpness, f.bd, f.maxv, lane);
+    const int r0 = (i - pfx[s]) * AV1B_DB_GROUP;
+    const int nr = vertical ? f.n_dbv : f.n_dbh;
+    deblock_group(st[s].a.cur, (vertical ? f.dbv : f.dbh) + r0, mini(AV1B_DB_GROUP, nr - r0), f.sharpness,
+                  f.bd, f.maxv, lane);
   }
 }
 

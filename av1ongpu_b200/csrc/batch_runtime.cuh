@@ -321,8 +321,8 @@ int batch_step(av1b_batch* b, int n, av1b_decoder* const* decs, av1b_plan* const
     items[kBInter] = a.n_inter_tiles - a.n_inter_simple;
     for (int c = 2; c <= 7; ++c) items[kBItx2 + c - 2] = a.n_itx_batches > 0 ? a.itx_class_count[c] : 0;
     items[kBUnits] = a.n_chains;
-    items[kBDeblockV] = f.n_dbv;
-    items[kBDeblockH] = f.n_dbh;
+    items[kBDeblockV] = (f.n_dbv + AV1B_DB_GROUP - 1) / AV1B_DB_GROUP;
+    items[kBDeblockH] = (f.n_dbh + AV1B_DB_GROUP - 1) / AV1B_DB_GROUP;
     items[kBCopySnap] = f.copy_items[0];
     items[kBCopyPost] = f.copy_items[1];
     items[kBCopyRef] = f.copy_items[2];

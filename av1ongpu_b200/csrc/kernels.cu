@@ -802,20 +802,57 @@ __global__ void __launch_bounds__(128) k_units(const __grid_constant__ FrameArgs
 }
 
 /* ---- deblocking ---------------------------------------------------------------------- */
-__device__ __forceinline__ void deblock_edge(px_t* pic, const DeblockRec& r, int sharpness, int bd,
-                                             int maxv, int lane) {
-  for (int k = lane; k < r.len; k += 32)
-    deblock_px(pic + r.p_off + k * r.along, r.across, r.level, sharpness, r.filter_size, r.chroma,
-               bd, maxv);
+/* Deblocks records recs[0 .. m), m <= AV1B_DB_GROUP, with the warp's lanes
+ * spread over their samples: most edges are 4 or 8 samples long, so a warp
+ * per edge would leave three lanes of four idle. Lane j < m holds record j;
+ * an inclusive scan of the lengths maps each sample to its record, whose
+ * fields the sample's lane takes by shuffle, and the warp steps 32 samples at
+ * a time. The edges of one pass never filter the same sample (a filter is
+ * never longer than the transforms on its sides), so their samples run in
+ * any order. */
+template <int G = AV1B_DB_GROUP>
+__device__ __forceinline__ void deblock_group(px_t* pic, const DeblockRec* recs, int m, int sharpness,
+                                              int bd, int maxv, int lane) {
+  DeblockRec r{};
+  int len = 0;
+  if (lane < m) {
+    r = recs[lane];
+    len = r.len;
+  }
+  int cum = len;
+#pragma unroll
+  for (int o = 1; o < G; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, cum, o);
+    if (lane >= o) cum += v;
+  }
+  const int total = __shfl_sync(0xffffffffu, cum, G - 1);
+  const int fc = r.filter_size | (r.chroma << 8);
+  for (int base = 0; base < total; base += 32) {
+    const int t = base + lane;
+    int j = 0;
+#pragma unroll
+    for (int q = 0; q < G - 1; ++q) j += __shfl_sync(0xffffffffu, cum, q) <= t;
+    const int start = __shfl_sync(0xffffffffu, cum - len, j);
+    const int p_off = __shfl_sync(0xffffffffu, r.p_off, j);
+    const int across = __shfl_sync(0xffffffffu, r.across, j);
+    const int along = __shfl_sync(0xffffffffu, r.along, j);
+    const int level = __shfl_sync(0xffffffffu, static_cast<int>(r.level), j);
+    const int fcj = __shfl_sync(0xffffffffu, fc, j);
+    if (t < total)
+      deblock_px(pic + p_off + (t - start) * along, across, level, sharpness, fcj & 255, fcj >> 8, bd,
+                 maxv);
+  }
 }
 
+/* A warp per G records. */
+template <int G>
 __global__ void k_deblock(px_t* pic, const DeblockRec* recs, int n, int sharpness, int bd,
                           int maxv) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
-  if (warp >= n) return;
-  const DeblockRec r = recs[warp];
-  deblock_edge(pic, r, sharpness, bd, maxv, lane);
+  const long long r0 = static_cast<long long>(warp) * G;
+  if (r0 >= n) return;
+  deblock_group<G>(pic, recs + r0, mini(G, n - static_cast<int>(r0)), sharpness, bd, maxv, lane);
 }
 
 /* ---- CDEF ------------------------------------------------------------------------------ */
@@ -1951,7 +1988,8 @@ cudaError_t launch_prep_filters(const av1b_deblock_edge* edges, int n_edges, con
 cudaError_t launch_deblock(px_t* pic, const DeblockRec* recs, int n, int sharpness, int bd, int maxv,
                            cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
-  k_deblock<<<cdiv((long long)n * 32, 256), 256, 0, s>>>(pic, recs, n, sharpness, bd, maxv);
+  k_deblock<AV1B_DB_PLAIN><<<cdiv(cdiv(n, AV1B_DB_PLAIN) * 32, 256), 256, 0, s>>>(pic, recs, n, sharpness, bd,
+                                                                                  maxv);
   return cudaGetLastError();
 }
 
@@ -2039,7 +2077,7 @@ static cudaError_t load_all_kernels() {
       (e = load_kernel(k_itx<4>)) != cudaSuccess || (e = load_kernel(k_itx<5>)) != cudaSuccess ||
       (e = load_kernel(k_itx<6>)) != cudaSuccess || (e = load_kernel(k_itx<7>)) != cudaSuccess ||
       (e = load_kernel(k_units<true>)) != cudaSuccess || (e = load_kernel(k_units<false>)) != cudaSuccess ||
-      (e = load_kernel(k_selftest_wait)) != cudaSuccess || (e = load_kernel(k_deblock)) != cudaSuccess ||
+      (e = load_kernel(k_selftest_wait)) != cudaSuccess || (e = load_kernel(k_deblock<AV1B_DB_PLAIN>)) != cudaSuccess ||
       (e = load_kernel(k_cdef_search)) != cudaSuccess || (e = load_kernel(k_cdef)) != cudaSuccess ||
       (e = load_kernel(k_upscale)) != cudaSuccess || (e = load_kernel(k_lr_tile)) != cudaSuccess ||
       (e = load_kernel(k_grain_template)) != cudaSuccess || (e = load_kernel(k_grain_blend)) != cudaSuccess ||

@@ -35,6 +35,12 @@ namespace av1b {
 #define AV1B_UP_OUT 256
 #define AV1B_LR_TW 32
 #define AV1B_UNIT_CTAS_PER_SM 2
+/* deblocking: the edge records a warp takes at once in the batched form and
+ * in a single stream's launch */
+#define AV1B_DB_GROUP 8
+#ifndef AV1B_DB_PLAIN
+#define AV1B_DB_PLAIN 2
+#endif
 
 struct FrameArgs {
   Layout L;
