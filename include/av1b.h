@@ -304,7 +304,11 @@ AV1B_API int av1b_get_stats(av1b_decoder* dec, av1b_stats* out);
 AV1B_API int av1b_poll_status(av1b_decoder* dec, int* status);
 
 /* Device pointer and layout of a slot's planes (for callers that hand the
- * picture on without a host copy). */
+ * picture on without a host copy). The planes hold the picture once the work
+ * queued on the decoder's stream (av1b_decoder_stream) up to this call has
+ * run - the display picture of a frame whose film grain was left to its
+ * outputs is made here, on that stream - so a reader orders itself after
+ * that stream (an event on it, or av1b_sync). */
 AV1B_API int av1b_slot_planes_device(av1b_decoder* dec, int slot, uint16_t* plane_ptr[3],
                             int32_t stride[3]);
 

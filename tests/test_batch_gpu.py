@@ -47,6 +47,7 @@ def read_planes(av1b, rt, dec, slot, header):
     ptr = (ctypes.c_void_p * 3)()
     stride = (ctypes.c_int32 * 3)()
     assert av1b.lib().av1b_slot_planes_device(dec.h, slot, ptr, stride) == 0
+    dec.sync()   # a display picture left to the outputs is made on the decoder's stream
     out = []
     for p, (rows, cols) in enumerate(av1b.plane_shapes(w, h, sx, sy)):
         a = np.empty((rows, cols), dtype=np.uint16)

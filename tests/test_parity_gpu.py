@@ -400,6 +400,7 @@ def test_deferred_grain_outputs(av1b, oracle, dec):
             ptr = (ctypes.c_void_p * 3)()
             stride = (ctypes.c_int32 * 3)()
             assert av1b.lib().av1b_slot_planes_device(dec.h, ring[k], ptr, stride) == 0
+            dec.sync()   # the display picture is made on the decoder's stream
             for p, (rows, cols) in enumerate(av1b.plane_shapes(w, h, sx, sy)):
                 a = np.empty((rows, cols), dtype=np.uint16)
                 assert rt.cudaMemcpy2D(ctypes.c_void_p(a.ctypes.data), ctypes.c_size_t(cols * 2),

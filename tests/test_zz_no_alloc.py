@@ -71,6 +71,7 @@ def _apply(av1b, lib, torch, dec, blob, slot, outs=None, src=None, src_stride=No
         src = (ctypes.c_void_p * 3)()
         src_stride = (ctypes.c_int32 * 3)()
         assert lib.av1b_slot_planes_device(dec.h, slot, src, src_stride) == 0
+        dec.sync()
     if outs is None:
         outs = [torch.empty(s, dtype=torch.int16, device='cuda:0') for s in shapes]
     dst = (ctypes.c_void_p * 3)(*[t.data_ptr() for t in outs])
