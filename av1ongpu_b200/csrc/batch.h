@@ -97,7 +97,8 @@ struct StreamStep {
 /* The step's header: stream count, item prefix sums per stage, the claim
  * counters (zeroed at the start of every step) and the merged chain order of
  * the dependency-scheduled phase: (stream, chain) pairs, each stream's chains
- * in its own claim order, streams interleaved by chain depth. */
+ * in its own claim order, streams interleaved by chain depth (aligned at the
+ * ends of their dependency paths). */
 struct BatchHeader {
   int n;
   int pfx[kBStageCount][AV1B_BATCH_MAX + 1];

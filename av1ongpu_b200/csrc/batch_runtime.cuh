@@ -340,7 +340,11 @@ int batch_step(av1b_batch* b, int n, av1b_decoder* const* decs, av1b_plan* const
     }
   }
   /* the streams' chains interleaved by the depth of their first block, each
-   * stream's in its own order */
+   * stream's in its own order, the streams aligned at their ends: a stream
+   * whose dependency path is shorter than the deepest one's starts that many
+   * levels later, so the chains on the longest paths (a large key frame's)
+   * are claimed first and do not wait behind warps holding chains of short
+   * paths that could have run later */
   {
     size_t m = 0;
     size_t levels = 0;
@@ -348,8 +352,10 @@ int batch_step(av1b_batch* b, int n, av1b_decoder* const* decs, av1b_plan* const
     for (size_t k = 0; k + 1 < levels; ++k)
       for (int i = 0; i < n; ++i) {
         const std::vector<int>& df = plans[i]->P.depth_first;
-        if (k + 1 >= df.size()) continue;
-        for (int c = df[k]; c < df[k + 1]; ++c) hc[m++] = make_int2(i, c);
+        const size_t late = levels - std::max<size_t>(df.size(), 1);   /* >= 0 */
+        if (k < late || k - late + 1 >= df.size()) continue;
+        const size_t kk = k - late;
+        for (int c = df[kk]; c < df[kk + 1]; ++c) hc[m++] = make_int2(i, c);
       }
     if (m != n_chains) return bfail(b, AV1B_ERR_SYNTAX, "chain order of a plan is inconsistent");
   }

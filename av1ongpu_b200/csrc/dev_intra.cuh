@@ -273,7 +273,7 @@ AV1B_DEV void intra_predict(const IntraJob& j, px_t* dst, int stride, const px_t
     const int lxl = ((j.x + w) << sx) - (1 << sx);
     const int lyl = ((j.y + h) << sy) - (1 << sy);
     long long sum = 0;
-#pragma unroll 4
+#pragma unroll 2
     for (int k = lane; k < n; k += 32) {
       const int i = k >> lw, jj = k & (w - 1);
       const int ly = mini((j.y + i) << sy, lyl), lx = mini((j.x + jj) << sx, lxl);
