@@ -1387,80 +1387,79 @@ __global__ void __launch_bounds__(256) k_lr_tile(const px_t* __restrict__ cdef,
  * filter as a wavefront: sample (x, y) depends on rows above within +-lag
  * columns and on the lag samples to its left, so t = x + 4y orders it
  * (lag <= 3). One block: the Gaussian fill on all its threads, the filters
- * (luma first, then both chroma planes together) on its first five warps. */
-/* Threads of the template CTA that run the auto-regressive filters. */
-constexpr int kGrainArThreads = 160;
+ * of the three templates on its first warps, luma and chroma in the same
+ * steps. */
 
-__device__ __forceinline__ void grain_ar_barrier() {
-  asm volatile("bar.sync 1, 160;" ::: "memory");
+/* Luma rows the auto-regressive filter runs (3 .. 72 of the 82x73
+ * template), a thread each. */
+constexpr int kGrainLumaRows = 70;
+
+/* The step by which the chroma wavefront trails the luma one: a chroma
+ * sample (x, y) of step x + 4y + delay reads the luma samples it averages
+ * (columns ((x - 3) << ss_x) + 3 .. + ss_x, rows likewise), whose own step
+ * X + 4Y is at most delay - 1 before it; the lag grows with x (y) when
+ * ss_x (ss_y) doubles the luma coordinate, largest at the template's last
+ * column (row). */
+__host__ __device__ __forceinline__ int grain_chroma_delay(int ss_x, int ss_y, int cw, int ch) {
+  return (ss_x ? cw - 6 : 0) + 4 * (ss_y ? ch - 3 : 0) + 1;
 }
 
 /* The auto-regressive filters of the three templates (7.18.3.3) with lag
  * LAG, by wavefront: sample (x, y) reads the LAG rows above within +-LAG
  * columns and the LAG samples to its left, so the steps t = x + 4y order
- * it, and the samples of one step are independent. Thread `tid` of
- * kGrainArThreads takes luma row 3 + tid, then chroma item tid (plane
- * tid & 1, row tid >> 1); every one of them meets the named barrier after
- * each step. */
+ * it, and the samples of one step are independent. Thread tid <
+ * kGrainLumaRows takes luma row 3 + tid; thread kGrainLumaRows + i takes
+ * chroma item i (plane i & 1, row i >> 1), its wavefront `delay` steps
+ * behind (grain_chroma_delay) so that every luma sample it reads is final.
+ * All `nthreads` threads (a multiple of 32) meet a named barrier after each
+ * step. */
 template <int LAG>
 __device__ void grain_ar(const GrainParamsDev& prm, short* luma, short* cb, short* cr, int cw, int ch,
-                         bool chroma, int arshift, int gmin, int gmax, int tid) {
+                         bool chroma, int arshift, int gmin, int gmax, int tid, int nthreads) {
   constexpr int NT = 2 * LAG * (LAG + 1);   /* taps before the sample itself */
-  if (prm.num_y_points > 0) {
-    constexpr int W = 82, H = 73;
-    int co[NT > 0 ? NT : 1];
+  constexpr int W = 82, H = 73;
+  const bool do_luma = prm.num_y_points > 0;
+  const int sx = prm.ss_x, sy = prm.ss_y;
+  const int delay = chroma && do_luma ? grain_chroma_delay(sx, sy, cw, ch) : 0;
+  const bool luma_thread = tid < kGrainLumaRows;
+  const int ci = tid - kGrainLumaRows;
+  const int plane = ci & 1;
+  /* this thread's row of its template, and its work */
+  const int y = luma_thread ? 3 + tid : ci >> 1;
+  const bool mine = luma_thread ? do_luma : (chroma && ci >= 0 && ci < 2 * ch && y >= 3);
+  short* gp = luma_thread ? luma : (plane ? cr : cb);
+  const int gw = luma_thread ? W : cw;
+  const int off = luma_thread ? 0 : delay;
+  int co[NT + 1];
+  {
+    const int* cp = luma_thread ? prm.ar_y : (plane ? prm.ar_cr : prm.ar_cb);
 #pragma unroll
-    for (int i = 0; i < NT; ++i) co[i] = prm.ar_y[i];
-    const int y = 3 + tid;
-    const int tmax = (W - 4) + 4 * (H - 1);
-    for (int t = 3 + 4 * 3; t <= tmax; ++t) {
-      const int x = t - 4 * y;
-      if (y < H && x >= 3 && x < W - 3) {
-        int sum = 0, k = 0;
-#pragma unroll
-        for (int dr = -LAG; dr <= 0; ++dr)
-#pragma unroll
-          for (int dc = -LAG; dc <= LAG; ++dc) {
-            if (dr == 0 && dc == 0) break;
-            sum += luma[(y + dr) * W + x + dc] * co[k++];
-          }
-        luma[y * W + x] = (short)clampi(luma[y * W + x] + rnd2z(sum, arshift), gmin, gmax);
-      }
-      grain_ar_barrier();
-    }
+    for (int i = 0; i <= NT; ++i) co[i] = (luma_thread && i == NT) ? 0 : cp[i];
   }
-  if (chroma) {
-    const int sx = prm.ss_x, sy = prm.ss_y;
-    const int plane = tid & 1, y = tid >> 1;
-    const bool mine = tid < 2 * ch && y >= 3;
-    short* gp = plane ? cr : cb;
-    const int* cp = plane ? prm.ar_cr : prm.ar_cb;
-    int co[NT + 1];
+  const int tl = do_luma ? (W - 4) + 4 * (H - 1) : 0;
+  const int tc = chroma ? (cw - 4) + 4 * (ch - 1) + delay : 0;
+  const int tmax = tl > tc ? tl : tc;
+  for (int t = 3 + 4 * 3; t <= tmax; ++t) {
+    const int x = t - off - 4 * y;
+    if (mine && x >= 3 && x < gw - 3) {
+      int sum = 0, k = 0;
 #pragma unroll
-    for (int i = 0; i <= NT; ++i) co[i] = cp[i];
-    const int tmax = (cw - 4) + 4 * (ch - 1);
-    for (int t = 3 + 4 * 3; t <= tmax; ++t) {
-      const int x = t - 4 * y;
-      if (mine && x >= 3 && x < cw - 3) {
-        int sum = 0, k = 0;
+      for (int dr = -LAG; dr <= 0; ++dr)
 #pragma unroll
-        for (int dr = -LAG; dr <= 0; ++dr)
-#pragma unroll
-          for (int dc = -LAG; dc <= LAG; ++dc) {
-            if (dr == 0 && dc == 0) break;
-            sum += gp[(y + dr) * cw + x + dc] * co[k++];
-          }
-        if (prm.num_y_points > 0) {
-          const int lx = ((x - 3) << sx) + 3, ly = ((y - 3) << sy) + 3;
-          int acc = 0;
-          for (int i = 0; i <= sy; ++i)
-            for (int j = 0; j <= sx; ++j) acc += luma[(ly + i) * 82 + lx + j];
-          sum += rnd2z(acc, sx + sy) * co[NT];
+        for (int dc = -LAG; dc <= LAG; ++dc) {
+          if (dr == 0 && dc == 0) break;
+          sum += gp[(y + dr) * gw + x + dc] * co[k++];
         }
-        gp[y * cw + x] = (short)clampi(gp[y * cw + x] + rnd2z(sum, arshift), gmin, gmax);
+      if (!luma_thread && do_luma) {
+        const int lx = ((x - 3) << sx) + 3, ly = ((y - 3) << sy) + 3;
+        int acc = 0;
+        for (int i = 0; i <= sy; ++i)
+          for (int j = 0; j <= sx; ++j) acc += luma[(ly + i) * W + lx + j];
+        sum += rnd2z(acc, sx + sy) * co[NT];
       }
-      grain_ar_barrier();
+      gp[y * gw + x] = (short)clampi(gp[y * gw + x] + rnd2z(sum, arshift), gmin, gmax);
     }
+    asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory");
   }
 }
 
@@ -1510,16 +1509,17 @@ __device__ __forceinline__ void grain_template_body(GrainState* gs, const GrainP
   }
   __syncthreads();
   const int arshift = prm.ar_coeff_shift_minus_6 + 6;
-  /* the auto-regressive filters on the first five warps (a step of a
-   * wavefront has at most 73 luma or 146 chroma samples, one a thread), a
-   * named barrier between steps; the lag as a constant, so a sample's taps
-   * are independent loads */
-  if (tid < kGrainArThreads) {
+  /* the auto-regressive filters on the first warps (a step of a wavefront
+   * has at most 70 luma and 146 chroma samples, one a thread: 96 threads for
+   * luma alone, up to 224 with chroma), a named barrier between steps; the
+   * lag as a constant, so a sample's taps are independent loads */
+  const int ar_threads = ((kGrainLumaRows + (chroma ? 2 * ch : 0)) + 31) & ~31;
+  if (tid < ar_threads) {
     switch (prm.ar_coeff_lag) {
-      case 0: grain_ar<0>(prm, luma, cb, cr, cw, ch, chroma, arshift, gmin, gmax, tid); break;
-      case 1: grain_ar<1>(prm, luma, cb, cr, cw, ch, chroma, arshift, gmin, gmax, tid); break;
-      case 2: grain_ar<2>(prm, luma, cb, cr, cw, ch, chroma, arshift, gmin, gmax, tid); break;
-      default: grain_ar<3>(prm, luma, cb, cr, cw, ch, chroma, arshift, gmin, gmax, tid); break;
+      case 0: grain_ar<0>(prm, luma, cb, cr, cw, ch, chroma, arshift, gmin, gmax, tid, ar_threads); break;
+      case 1: grain_ar<1>(prm, luma, cb, cr, cw, ch, chroma, arshift, gmin, gmax, tid, ar_threads); break;
+      case 2: grain_ar<2>(prm, luma, cb, cr, cw, ch, chroma, arshift, gmin, gmax, tid, ar_threads); break;
+      default: grain_ar<3>(prm, luma, cb, cr, cw, ch, chroma, arshift, gmin, gmax, tid, ar_threads); break;
     }
   }
   __syncthreads();
