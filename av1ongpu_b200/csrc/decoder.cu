@@ -1025,7 +1025,15 @@ int plan_units(av1b_decoder* d, const PlanCtx& c, Plan* P) {
       /* prediction and residual fuse when the transforms cover disjoint parts
        * of the block (each sample then gets at most one residual) */
       b.fuse_res = 0;
-      if (b.kind == AV1B_U_INTRA && b.w * b.h <= AV1B_UNIT_SCRATCH) {
+      if (b.kind == AV1B_U_INTRA && b.w * b.h <= AV1B_UNIT_SCRATCH && b.tx_count <= 1) {
+        /* none or one transform: disjoint by itself once it lies in the block */
+        bool ok = true;
+        if (b.tx_count == 1) {
+          const TxRec& x = P->R->txs[b.tx_first];
+          ok = x.x >= 0 && x.y >= 0 && x.x + x.w <= b.w && x.y + x.h <= b.h;
+        }
+        b.fuse_res = ok ? 1 : 0;
+      } else if (b.kind == AV1B_U_INTRA && b.w * b.h <= AV1B_UNIT_SCRATCH) {
         bool ok = true, grid4 = true;
         for (int t = 0; t < b.tx_count && ok; ++t) {
           const TxRec& x = P->R->txs[b.tx_first + t];
