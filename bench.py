@@ -92,6 +92,24 @@ def rank_info():
             int(os.environ.get('LOCAL_RANK', '0')))
 
 
+def slowest_rank(x, dist, device):
+    """The largest of every rank's `x` (a time), the same on every rank; `x`
+    itself without a process group. Every rank must call it, in the same
+    order."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(units_per_rank, world, seconds):
+    """Whole-job throughput of `world` replicas that each processed
+    `units_per_rank` units: all ranks' units over the slowest rank's time."""
+    return units_per_rank * world / seconds
+
+
 def config_dict(w, h, cw, frames, world):
     """The `config` of both arms' lines (identical for the same workload)."""
     return {'workload': 'config3: %dx%d (coded %d) 10-bit 4:2:0 superres, 128x128 SB, all tools, '
@@ -446,14 +464,9 @@ def run_ours(args):
     dec.sync()
     torch.cuda.synchronize()
     clk = clocks.stop()
-    ms = e0.elapsed_time(e1)
-    if dist is not None:
-        t = torch.tensor([ms], device='cuda:%d' % local)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        barrier()
-    frames_total = F * args.steps * world
-    value = frames_total / (ms / 1e3)
+    ms = slowest_rank(e0.elapsed_time(e1), dist, 'cuda:%d' % local)
+    barrier()
+    value = replica_rate(F * args.steps, world, ms / 1e3)
     launches_per_frame = dec.stats().kernel_launches + 1  # + the NV12 pack
 
     # ---- per-stage device times (a separate profiled pass over the same step) ----------
@@ -561,11 +574,8 @@ def run_ours(args):
         e2e_run(e2e_steps)
         torch.cuda.synchronize()
         e2e_s = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([e2e_s], device='cuda:%d' % local)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = {'value': F * e2e_steps * world / e2e_s, 'unit': UNIT, 'h2d_bytes_per_step': h2d,
+    e2e_s = slowest_rank(e2e_s, dist, 'cuda:%d' % local)
+    e2e = {'value': replica_rate(F * e2e_steps, world, e2e_s), 'unit': UNIT, 'h2d_bytes_per_step': h2d,
            'd2h_bytes_per_step': geo['nv12'] * F, 'frames_timed': F * e2e_steps}
 
     base = None
