@@ -109,7 +109,7 @@ __global__ void __launch_bounds__(128) kb_itx(const StreamStep* __restrict__ st,
  * the argument of the single-stream kernel holds: the warp holding the
  * earliest unfinished chain always progresses. */
 template <bool INTER>
-__global__ void __launch_bounds__(128) kb_units(const StreamStep* __restrict__ st, BatchHeader* h) {
+__global__ void __launch_bounds__(128, AV1B_UNIT_CTAS_PER_SM) kb_units(const StreamStep* __restrict__ st, BatchHeader* h) {
   extern __shared__ int smem[];
   const int wib = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;

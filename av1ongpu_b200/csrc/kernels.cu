@@ -786,7 +786,7 @@ __device__ __forceinline__ void run_chain(const FrameArgs& a, int c, int* edges,
 }
 
 template <bool INTER>
-__global__ void __launch_bounds__(128) k_units(const __grid_constant__ FrameArgs a) {
+__global__ void __launch_bounds__(128, AV1B_UNIT_CTAS_PER_SM) k_units(const __grid_constant__ FrameArgs a) {
   extern __shared__ int smem[];
   const int wib = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
