@@ -59,22 +59,26 @@ __global__ void __launch_bounds__(128, 5) kb_inter_simple(const StreamStep* __re
  * code is smaller. */
 template <int MINB>
 __global__ void __launch_bounds__(128, MINB) kb_inter(const StreamStep* __restrict__ st, BatchHeader* h,
-                                                      int chunk) {
+                                                      int chunk, int part) {
   __shared__ McScratch scr[4];
   __shared__ int pred[4][2][8 * 16];
   __shared__ int lpred[4][2][4 * 8 * 16];
   const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int* pfx = h->pfx[kBInter];
+  /* part 0: the full kernel's tiles but the chroma tiles that read a luma
+   * mask; part 1 (a stage of its own, after part 0): those */
+  const int stage = part ? kBInterMask : kBInter;
+  const int* pfx = h->pfx[stage];
   const int n = h->n, total = pfx[n];
   int s = 0;
   for (;;) {
-    const int i0 = warp_claim(&h->claim[kBInter], chunk, lane);
+    const int i0 = warp_claim(&h->claim[stage], chunk, lane);
     if (i0 >= total) break;
     const int i1 = mini(i0 + chunk, total);
     for (int i = i0; i < i1; ++i) {
       s = batch_stream_next(pfx, n, i, s);
       const FrameArgs& a = st[s].a;
-      inter_full_tile(a, a.n_inter_simple + (i - pfx[s]), scr[wib], pred[wib], lpred[wib], lane);
+      const int t0 = part ? a.n_inter_tiles - a.n_inter_cmask : a.n_inter_simple;
+      inter_full_tile(a, t0 + (i - pfx[s]), scr[wib], pred[wib], lpred[wib], lane);
       __syncwarp();
     }
   }
@@ -337,8 +341,11 @@ cudaError_t launch_batch_step(const StreamStep* steps, BatchHeader* hdr, const B
   mark(kBInterSimple);
   kb_inter_simple<<<batch_grid(t, kBInterSimple, n_sm), 128, 0, s>>>(steps, hdr, chunk);
   mark(kBInter);
-  if (t.inter_variant) kb_inter<4><<<batch_grid(t, kBInter, n_sm), 128, 0, s>>>(steps, hdr, chunk);
-  else kb_inter<3><<<batch_grid(t, kBInter, n_sm), 128, 0, s>>>(steps, hdr, chunk);
+  if (t.inter_variant) kb_inter<4><<<batch_grid(t, kBInter, n_sm), 128, 0, s>>>(steps, hdr, chunk, 0);
+  else kb_inter<3><<<batch_grid(t, kBInter, n_sm), 128, 0, s>>>(steps, hdr, chunk, 0);
+  mark(kBInterMask);
+  if (t.inter_variant) kb_inter<4><<<batch_grid(t, kBInterMask, n_sm), 128, 0, s>>>(steps, hdr, chunk, 1);
+  else kb_inter<3><<<batch_grid(t, kBInterMask, n_sm), 128, 0, s>>>(steps, hdr, chunk, 1);
   mark(kBItx2);
   launch_kb_itx<2>(steps, hdr, t, n_sm, s);
   mark(kBItx3);
@@ -423,7 +430,7 @@ int batch_stage_max_ctas(int stage) {
   size_t smem = 0;
   switch (stage) {
     case kBInterSimple: k = reinterpret_cast<const void*>(kb_inter_simple); break;
-    case kBInter: k = reinterpret_cast<const void*>(kb_inter<4>); break;
+    case kBInter: case kBInterMask: k = reinterpret_cast<const void*>(kb_inter<4>); break;
     case kBItx2: k = reinterpret_cast<const void*>(kb_itx<2>); smem = 4 * ItxScratch<2>::PER_WARP * sizeof(int); break;
     case kBItx3: k = reinterpret_cast<const void*>(kb_itx<3>); smem = 4 * ItxScratch<3>::PER_WARP * sizeof(int); break;
     case kBItx4: k = reinterpret_cast<const void*>(kb_itx<4>); smem = 4 * ItxScratch<4>::PER_WARP * sizeof(int); break;

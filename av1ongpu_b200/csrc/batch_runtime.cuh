@@ -175,7 +175,7 @@ int bcuda(av1b_batch* b, cudaError_t e, const char* what) {
 /* Launch shapes before tuning: CTAs per SM of each stage kernel. */
 void default_tuning(BatchTuning* t) {
   static const int ctas[kBStageCount] = {
-      4, 4,                 /* prediction */
+      4, 4, 4,              /* prediction: lean, full, chroma tiles reading luma masks */
       4, 4, 4, 4, 2, 2,     /* transforms by class */
       AV1B_UNIT_CTAS_PER_SM,
       8, 8,                 /* deblocking */
@@ -318,7 +318,8 @@ int batch_step(av1b_batch* b, int n, av1b_decoder* const* decs, av1b_plan* const
     const FilterArgs& f = sp[i].f;
     long long items[kBStageCount] = {};
     items[kBInterSimple] = a.n_inter_simple;
-    items[kBInter] = a.n_inter_tiles - a.n_inter_simple;
+    items[kBInter] = a.n_inter_tiles - a.n_inter_simple - a.n_inter_cmask;
+    items[kBInterMask] = a.n_inter_cmask;
     for (int c = 2; c <= 7; ++c) items[kBItx2 + c - 2] = a.n_itx_batches > 0 ? a.itx_class_count[c] : 0;
     items[kBUnits] = a.n_chains;
     items[kBDeblockV] = (f.n_dbv + AV1B_DB_GROUP - 1) / AV1B_DB_GROUP;
@@ -707,7 +708,7 @@ int av1b_batch_autotune(av1b_batch* b, int n, av1b_decoder* const* decoders,
   /* coordinate descent over groups of stages that share a launch shape,
    * then the claim size, then the grain-in-pack fusion */
   const std::vector<std::vector<int>> groups = {
-      {kBInterSimple, kBInter},
+      {kBInterSimple, kBInter, kBInterMask},
       {kBItx2, kBItx3, kBItx4, kBItx5, kBItx6, kBItx7},
       {kBUnits},
       {kBDeblockV, kBDeblockH},

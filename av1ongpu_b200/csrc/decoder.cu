@@ -113,6 +113,7 @@ struct av1b_decoder {
   DevBuf cur, snap, lr_pre_up, lr_cdef, disp;
   DevBuf cdef_search;             /* CDEF direction search results */
   DevBuf pre_res;                 /* phase B residuals computed ahead */
+  DevBuf mask_pool;               /* difference-weighted luma masks chroma tiles read */
   bool disp_is_cur = true;
   /* a batched step applied the last frame's film grain inside its NV12 pack:
    * the display picture is made from cur when an output call asks for it */
@@ -442,6 +443,8 @@ void sized(V& v, size_t n) {
 struct Plan {
   PlanLists* R = nullptr;         /* while planning: the lists being built */
   size_t n_tiles_simple = 0;      /* inter tiles the lean kernel takes (listed first) */
+  size_t n_tiles_cmask = 0;       /* chroma tiles reading a luma block's mask (listed last) */
+  size_t mask_pool = 0;           /* bytes of the difference-weighted luma masks */
   size_t n_blocks = 0, n_units = 0, n_chains = 0, n_tiles = 0, n_itx = 0, n_itxb = 0, n_dbv = 0, n_dbh = 0,
          n_cdef = 0,
          n_cdef_search = 0;
@@ -1345,6 +1348,74 @@ int filter_records_error(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syn
   return AV1B_OK;
 }
 
+/* A chroma block of a difference-weighted compound blends with a mask made
+ * from the luma predictions of the area it covers. When the luma block there
+ * is that very prediction - the same position and size, references, motion,
+ * filters, warp models (compared by value) and mask sign - its tiles write
+ * the mask (a byte a luma sample, in the frame's mask pool) and the chroma
+ * block's tiles read it, instead of predicting the luma again (two
+ * references, up to four 16x8 areas each, per chroma tile). Any other chroma
+ * block predicts the luma itself. The chroma tiles that read a mask go last
+ * in the tile list: they run after every luma tile (a launch, or a stage, of
+ * their own). */
+void plan_shared_masks(const PlanCtx& c, Plan* P) {
+  const Layout& L = c.L;
+  PlanLists& R = *P->R;
+  PlanScratch& S = *c.scratch;
+  P->mask_pool = 0;
+  P->n_tiles_cmask = 0;
+  const size_t nt = R.inter_tiles.size();
+  if (nt == P->n_tiles_simple) return;
+  const int ow = static_cast<int>((L.p[0].grid_w + 3) >> 2);
+  const int oh = static_cast<int>((L.p[0].grid_h + 3) >> 2);
+  if (S.owner[0].size() < static_cast<size_t>(ow) * oh) return;
+  size_t pool = 0;
+  bool any = false;
+  for (size_t i = P->n_tiles_simple; i < nt; ++i) {
+    const int bi = R.inter_tiles[i].x;
+    BlockRec& b = R.blocks[bi];
+    if (b.plane == 0 || b.mask_role || b.mask_kind != 2 || !b.compound || b.interintra) continue;
+    const int lx = b.x << L.ss_x, ly = b.y << L.ss_y;
+    if ((lx | ly) & 3 || (lx >> 2) >= ow || (ly >> 2) >= oh) continue;
+    const int li = S.owner[0][static_cast<size_t>(ly >> 2) * ow + (lx >> 2)];
+    if (li < 0) continue;
+    BlockRec& l = R.blocks[li];
+    bool same = l.plane == 0 && l.is_inter && !l.phase_b && l.x == lx && l.y == ly &&
+                l.w == (b.w << L.ss_x) && l.h == (b.h << L.ss_y) && l.compound && l.mask_kind == 2 &&
+                l.mask_sign == b.mask_sign && l.filt == b.filt && l.filt_v == b.filt_v;
+    for (int r = 0; r < 2 && same; ++r) {
+      const int lw = r ? l.warp1 : l.warp0, cw = r ? b.mask_warp1 : b.mask_warp0;
+      same = l.ref_slot[r] == b.ref_slot[r] && l.mv[r][0] == b.mv[r][0] && l.mv[r][1] == b.mv[r][1] &&
+             lw == cw;
+      /* warped: the same model (each block has an entry of its own) */
+      if (same && lw) {
+        const int li_w = l.warp_idx[r] >= 0 ? l.warp_idx[r] : 0, bi_w = b.warp_idx[r] >= 0 ? b.warp_idx[r] : 0;
+        same = li_w < static_cast<int>(R.warps.size()) && bi_w < static_cast<int>(R.warps.size()) &&
+               std::memcmp(&R.warps[li_w], &R.warps[bi_w], sizeof(WarpRec)) == 0;
+      }
+    }
+    if (!same) continue;
+    if (l.mask_role != 1) {
+      if (pool + static_cast<size_t>(l.w) * l.h > static_cast<size_t>(INT32_MAX)) continue;
+      l.mask_role = 1;
+      l.mask_off = static_cast<int>(pool);
+      l.mask_w = l.w;
+      pool += static_cast<size_t>(l.w) * l.h;
+    }
+    b.mask_role = 2;
+    b.mask_off = l.mask_off;
+    b.mask_w = l.w;
+    any = true;
+  }
+  if (!any) return;
+  P->mask_pool = pool;
+  /* the tiles reading a mask to the end, the others in their order */
+  auto first = R.inter_tiles.begin() + static_cast<std::ptrdiff_t>(P->n_tiles_simple);
+  auto mid = std::stable_partition(first, R.inter_tiles.end(),
+                                   [&](const int2& t) { return R.blocks[t.x].mask_role != 2; });
+  P->n_tiles_cmask = static_cast<size_t>(R.inter_tiles.end() - mid);
+}
+
 /* Validates a frame and builds its device records. The blocks, deblocking
  * edges and CDEF blocks are converted in pieces on the pool; each piece stops
  * at its first invalid record and the error of the earliest piece is the one
@@ -1510,6 +1581,7 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
       std::copy(O.dq.begin(), O.dq.end(), P->R->dq.begin() + o_dq[i]);
     });
   }
+  plan_shared_masks(c, P);
   phase(kStPlanBlocks);
   if ((rc_units = plan_units(d, c, P))) return rc_units;
   phase(kStPlanUnits);
@@ -2146,6 +2218,7 @@ int prepare_step(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, bool
   }
   const size_t pic_bytes = static_cast<size_t>(L.size) * sizeof(px_t);
   if (P.pre_res_pool && (rc = dev_ensure(d, d->pre_res, P.pre_res_pool * sizeof(int)))) return rc;
+  if (P.mask_pool && (rc = dev_ensure(d, d->mask_pool, P.mask_pool))) return rc;
   if ((P.cdef_search_any || (P.n_cdef_search != 0)) &&
       (rc = dev_ensure(d, d->cdef_search, (P.cdef_grid_n + P.n_cdef_search) * sizeof(int))))
     return rc;
@@ -2228,6 +2301,8 @@ int prepare_step(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, bool
   a.inter_tiles = reinterpret_cast<const int2*>(ar + pl->o_tiles);
   a.n_inter_tiles = static_cast<int>(P.n_tiles);
   a.n_inter_simple = static_cast<int>(P.n_tiles_simple);
+  a.n_inter_cmask = static_cast<int>(P.n_tiles_cmask);
+  a.mask_pool = static_cast<unsigned char*>(d->mask_pool.p);
   a.itx_jobs = reinterpret_cast<const int2*>(ar + pl->o_itx);
   a.n_itx = static_cast<int>(P.n_itx);
   a.itx_batches = reinterpret_cast<const int4*>(ar + pl->o_itxb);
@@ -2665,7 +2740,8 @@ int av1b_decoder_destroy(av1b_decoder* d) {
   DevBuf* bufs[] = {&d->cur, &d->snap, &d->lr_pre_up, &d->lr_cdef, &d->disp,
                     &d->slot_ptr_dev, &d->arena, &d->coef, &d->residual, &d->done,
                     &d->status_q, &d->nv12, &d->rgb,
-                    &d->grain_state, &d->orbit, &d->pos, &d->cdef_search, &d->pre_res, &d->trace};
+                    &d->grain_state, &d->orbit, &d->pos, &d->cdef_search, &d->pre_res, &d->mask_pool,
+                    &d->trace};
   for (DevBuf* b : bufs) dev_release(d, *b);
   for (int i = 0; i < kSlots; ++i) dev_release(d, d->slot_buf[i]);
   if (d->stream) cudaStreamDestroy(d->stream);
@@ -2796,12 +2872,14 @@ size_t av1b_stream_hbm_estimate(int width, int height, int coded_width, int bit_
   auto rounded = [](size_t b) { return align_up(b + b / 8, size_t(1) << 16); };
   /* pictures: the one reconstructed, the snapshot, the display picture, the
    * two loop restoration sources, and the reference slots; per sample: the
-   * phase B residuals (4 B) and the done flags (128 B a block, blocks of 16
-   * samples or more); per plan: its five buffers - records, coefficient
-   * pool, residuals, levels, filter lists - at most 10 B a coded sample in
-   * all; the grain tables and small buffers, 2 MB */
+   * phase B residuals (4 B), the done flags (128 B a block, blocks of 16
+   * samples or more) and the difference-weighted luma masks (1 B); per plan:
+   * its five buffers - records, coefficient pool, residuals, levels, filter
+   * lists - at most 10 B a coded sample in all; the grain tables and small
+   * buffers, 2 MB */
   return (5 + static_cast<size_t>(n_slots)) * rounded(pic) + rounded(4 * nc) + rounded(8 * nc) +
-         static_cast<size_t>(plans) * (5 * (size_t(1) << 16) + rounded(10 * nc)) + (size_t(2) << 20);
+         rounded(nc) + static_cast<size_t>(plans) * (5 * (size_t(1) << 16) + rounded(10 * nc)) +
+         (size_t(2) << 20);
 }
 
 int av1b_decoder_memory(av1b_decoder* d, size_t* allocated, size_t* budget) {

@@ -142,6 +142,13 @@ struct BlockRec {
   int obmc_first, obmc_count;
   int palette_color_idx;      /* into the palette colour table */
   int dep_first, dep_count;   /* phase B: the blocks it waits for (frame's dep list) */
+  /* a difference-weighted compound: 1 - a luma block that writes its blend
+   * mask (a byte a sample, mask_w a row) at mask_off of the frame's mask
+   * pool; 2 - a chroma block whose luma block is the same prediction, which
+   * reads that mask instead of predicting the luma itself; 0 - neither */
+  int mask_off;
+  short mask_w;
+  unsigned char mask_role, pad_mask;
 };
 
 /* One coded transform of a frame whose coefficients arrive as coded levels:

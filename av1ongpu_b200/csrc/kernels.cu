@@ -292,7 +292,9 @@ __device__ __forceinline__ void inter_full_tile(const FrameArgs& a, int tile, Mc
     }
   }
   const bool luma_mask = j.compound && j.mask_kind == 2 && b.plane > 0;
-  if (luma_mask) {
+  /* the luma block is the same prediction and has written its mask */
+  const bool shared_mask = luma_mask && b.mask_role == 2;
+  if (luma_mask && !shared_mask) {
     InterCtx l;
     l.sub_x = l.sub_y = 0;
     l.ref_w = j.luma_ref_w;
@@ -334,21 +336,33 @@ __device__ __forceinline__ void inter_full_tile(const FrameArgs& a, int tile, Mc
       const int yy = (k * tmul) >> 16, xx = k - yy * tw;
       const int v0 = pred[0][yy * 16 + xx], v1 = nref > 1 ? pred[1][yy * 16 + xx] : 0;
       if (luma_mask) {
-        /* the chroma sample's mask: the mean over the luma samples it covers */
+        /* the chroma sample's mask: the mean over the luma samples it covers,
+         * from the luma block's mask or from the luma predictions */
         const int sh = 7 - (j.ctx.bitdepth >= 12 ? 5 : 3) + (j.ctx.bitdepth - 8);
         const int nx = j.ctx.sub_x + 1, ny = j.ctx.sub_y + 1;
         int sum = 0;
         for (int jj = 0; jj < ny; ++jj)
           for (int ii = 0; ii < nx; ++ii) {
             const int lx = (xx << j.ctx.sub_x) + ii, ly = (yy << j.ctx.sub_y) + jj;
-            const int idx = ((ly >> 3) * 2 + (lx >> 4)) * 128 + (ly & 7) * 16 + (lx & 15);
-            sum += diffwtd_m(absi(lpred[0][idx] - lpred[1][idx]), sh, j.mask_sign);
+            if (shared_mask) {
+              const int bx = (x0 << j.ctx.sub_x) + lx, by = (y0 << j.ctx.sub_y) + ly;
+              sum += a.mask_pool[b.mask_off + by * b.mask_w + bx];
+            } else {
+              const int idx = ((ly >> 3) * 2 + (lx >> 4)) * 128 + (ly & 7) * 16 + (lx & 15);
+              sum += diffwtd_m(absi(lpred[0][idx] - lpred[1][idx]), sh, j.mask_sign);
+            }
           }
         const int n = nx * ny;
         const int m = n == 1 ? sum : (n == 2 ? (sum + 1) >> 1 : (sum + 2) >> 2);
         acc[q] = blend_mask(j, v0, v1, m);
       } else {
         acc[q] = inter_compose(j, x0 + xx, y0 + yy, v0, v1);
+        if (b.mask_role == 1) {
+          /* the mask its chroma blocks read (the one inter_compose blends with) */
+          const int sh = 7 - (j.ctx.bitdepth >= 12 ? 5 : 3) + (j.ctx.bitdepth - 8);
+          a.mask_pool[b.mask_off + (y0 + yy) * b.mask_w + x0 + xx] =
+              static_cast<unsigned char>(diffwtd_m(absi(v0 - v1), sh, j.mask_sign));
+        }
       }
     }
   }
@@ -386,13 +400,16 @@ __device__ __forceinline__ void inter_full_tile(const FrameArgs& a, int tile, Mc
   }
 }
 
-__global__ void __launch_bounds__(128, 4) k_inter(const __grid_constant__ FrameArgs a) {
+/* Tiles [first, end) of the full kernel's: the tiles before the chroma
+ * tiles that read a luma mask, then those (a launch of their own, after the
+ * luma tiles that write the masks). */
+__global__ void __launch_bounds__(128, 4) k_inter(const __grid_constant__ FrameArgs a, int first, int end) {
   __shared__ McScratch scr[4];
   __shared__ int pred[4][2][8 * 16];
   __shared__ int lpred[4][2][4 * 8 * 16];   /* luma predictions, four 16x8 quarters */
   const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int warp = a.n_inter_simple + blockIdx.x * 4 + wib;
-  if (warp >= a.n_inter_tiles) return;
+  const int warp = first + blockIdx.x * 4 + wib;
+  if (warp >= end) return;
   inter_full_tile(a, warp, scr[wib], pred[wib], lpred[wib], lane);
 }
 
@@ -1887,8 +1904,13 @@ cudaError_t launch_recon_stage(int stage, const FrameArgs& a, int n_sm, cudaStre
       if (a.n_inter_tiles > 0)
       {
         if (a.n_inter_simple > 0) k_inter_simple<<<cdiv(a.n_inter_simple, 4), 128, 0, s>>>(a);
-        const int rest = a.n_inter_tiles - a.n_inter_simple;
-        if (rest > 0) k_inter<<<cdiv(rest, 4), 128, 0, s>>>(a);
+        /* the full kernel's tiles, then the chroma tiles that read the masks
+         * the luma tiles wrote */
+        const int cm_first = a.n_inter_tiles - a.n_inter_cmask;
+        const int rest = cm_first - a.n_inter_simple;
+        if (rest > 0) k_inter<<<cdiv(rest, 4), 128, 0, s>>>(a, a.n_inter_simple, cm_first);
+        if (a.n_inter_cmask > 0)
+          k_inter<<<cdiv(a.n_inter_cmask, 4), 128, 0, s>>>(a, cm_first, a.n_inter_tiles);
       }
       break;
     case 2:

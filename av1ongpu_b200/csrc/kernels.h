@@ -68,6 +68,8 @@ struct FrameArgs {
   const int2* inter_tiles;      /* phase A: (block, x0 | y0 << 16) */
   int n_inter_tiles;
   int n_inter_simple;           /* the first ones: translation-only blocks */
+  int n_inter_cmask;            /* the last ones: chroma tiles reading a luma mask */
+  unsigned char* mask_pool;     /* blend masks of difference-weighted luma blocks */
   const int2* itx_jobs;         /* phase A: (block, transform); the transforms of
                                    phase B blocks compute their residual ahead */
   int n_itx;
