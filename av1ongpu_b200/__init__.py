@@ -623,7 +623,7 @@ class Batch:
     def stream(self):
         return lib().av1b_batch_stream(self.h)
 
-    STAGES = ('inter_simple', 'inter', 'inter_mask', 'itx4', 'itx8', 'itx16', 'itx32', 'itx64', 'itx_raw', 'units',
+    STAGES = ('inter_simple', 'inter_lean_mask', 'inter', 'inter_mask', 'itx4', 'itx8', 'itx16', 'itx32', 'itx64', 'itx_raw', 'units',
               'deblock_v', 'deblock_h', 'copy_snapshot', 'cdef_search', 'cdef', 'copy_post_cdef',
               'upscale', 'lr', 'copy_reference', 'grain_template', 'grain_blend', 'nv12')
 

@@ -26,7 +26,7 @@ namespace av1b {
 
 /* The stages of a batched step, in launch order. */
 enum BatchStage {
-  kBInterSimple, kBInter, kBInterMask,
+  kBInterSimple, kBInterLeanMask, kBInter, kBInterMask,
   kBItx2, kBItx3, kBItx4, kBItx5, kBItx6, kBItx7,
   kBUnits,
   kBDeblockV, kBDeblockH,

@@ -33,21 +33,29 @@ __device__ __forceinline__ int warp_claim(unsigned* ctr, int chunk, int lane) {
 
 /* Five CTAs an SM: the lean tile body plus the loop fit 96 registers
  * without spilling (unbounded, the compiler spilled). */
+/* The lean kernel's stages: its unmasked tiles (MASK false, listed first);
+ * with the masked build, the wedge and luma difference-weighted tiles listed
+ * next (part 0) and, a stage of its own after the luma tiles that write the
+ * masks, the chroma tiles that read a luma mask, listed last (part 1). */
+template <bool MASK>
 __global__ void __launch_bounds__(128, 5) kb_inter_simple(const StreamStep* __restrict__ st,
-                                                       BatchHeader* h, int chunk) {
+                                                       BatchHeader* h, int chunk, int part) {
   __shared__ McScratch scr[4];
   __shared__ int pred[4][2][8 * 16];
   const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int* pfx = h->pfx[kBInterSimple];
+  const int stage = !MASK ? kBInterSimple : (part ? kBInterMask : kBInterLeanMask);
+  const int* pfx = h->pfx[stage];
   const int n = h->n, total = pfx[n];
   int s = 0;
   for (;;) {
-    const int i0 = warp_claim(&h->claim[kBInterSimple], chunk, lane);
+    const int i0 = warp_claim(&h->claim[stage], chunk, lane);
     if (i0 >= total) break;
     const int i1 = mini(i0 + chunk, total);
     for (int i = i0; i < i1; ++i) {
       s = batch_stream_next(pfx, n, i, s);
-      inter_simple_tile(st[s].a, i - pfx[s], scr[wib], pred[wib], lane);
+      const FrameArgs& a = st[s].a;
+      const int t0 = !MASK ? 0 : (part ? a.n_inter_tiles - a.n_inter_cmask : a.n_inter_simple);
+      inter_simple_tile<MASK>(a, t0 + (i - pfx[s]), scr[wib], pred[wib], lane);
       __syncwarp();
     }
   }
@@ -59,14 +67,12 @@ __global__ void __launch_bounds__(128, 5) kb_inter_simple(const StreamStep* __re
  * code is smaller. */
 template <int MINB>
 __global__ void __launch_bounds__(128, MINB) kb_inter(const StreamStep* __restrict__ st, BatchHeader* h,
-                                                      int chunk, int part) {
+                                                      int chunk) {
   __shared__ McScratch scr[4];
   __shared__ int pred[4][2][8 * 16];
   __shared__ int lpred[4][2][4 * 8 * 16];
   const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  /* part 0: the full kernel's tiles but the chroma tiles that read a luma
-   * mask; part 1 (a stage of its own, after part 0): those */
-  const int stage = part ? kBInterMask : kBInter;
+  const int stage = kBInter;
   const int* pfx = h->pfx[stage];
   const int n = h->n, total = pfx[n];
   int s = 0;
@@ -77,8 +83,8 @@ __global__ void __launch_bounds__(128, MINB) kb_inter(const StreamStep* __restri
     for (int i = i0; i < i1; ++i) {
       s = batch_stream_next(pfx, n, i, s);
       const FrameArgs& a = st[s].a;
-      const int t0 = part ? a.n_inter_tiles - a.n_inter_cmask : a.n_inter_simple;
-      inter_full_tile(a, t0 + (i - pfx[s]), scr[wib], pred[wib], lpred[wib], lane);
+      inter_full_tile(a, a.n_inter_simple + a.n_inter_lmask + (i - pfx[s]), scr[wib], pred[wib],
+                      lpred[wib], lane);
       __syncwarp();
     }
   }
@@ -339,13 +345,14 @@ cudaError_t launch_batch_step(const StreamStep* steps, BatchHeader* hdr, const B
   mark(kBStageCount + 1);
   if ((e = cudaEventRecord(join, side)) != cudaSuccess) return e;
   mark(kBInterSimple);
-  kb_inter_simple<<<batch_grid(t, kBInterSimple, n_sm), 128, 0, s>>>(steps, hdr, chunk);
+  kb_inter_simple<false><<<batch_grid(t, kBInterSimple, n_sm), 128, 0, s>>>(steps, hdr, chunk, 0);
+  mark(kBInterLeanMask);
+  kb_inter_simple<true><<<batch_grid(t, kBInterLeanMask, n_sm), 128, 0, s>>>(steps, hdr, chunk, 0);
   mark(kBInter);
-  if (t.inter_variant) kb_inter<4><<<batch_grid(t, kBInter, n_sm), 128, 0, s>>>(steps, hdr, chunk, 0);
-  else kb_inter<3><<<batch_grid(t, kBInter, n_sm), 128, 0, s>>>(steps, hdr, chunk, 0);
+  if (t.inter_variant) kb_inter<4><<<batch_grid(t, kBInter, n_sm), 128, 0, s>>>(steps, hdr, chunk);
+  else kb_inter<3><<<batch_grid(t, kBInter, n_sm), 128, 0, s>>>(steps, hdr, chunk);
   mark(kBInterMask);
-  if (t.inter_variant) kb_inter<4><<<batch_grid(t, kBInterMask, n_sm), 128, 0, s>>>(steps, hdr, chunk, 1);
-  else kb_inter<3><<<batch_grid(t, kBInterMask, n_sm), 128, 0, s>>>(steps, hdr, chunk, 1);
+  kb_inter_simple<true><<<batch_grid(t, kBInterMask, n_sm), 128, 0, s>>>(steps, hdr, chunk, 1);
   mark(kBItx2);
   launch_kb_itx<2>(steps, hdr, t, n_sm, s);
   mark(kBItx3);
@@ -410,7 +417,8 @@ cudaError_t set_batch_kernel_attributes() {
    * launch, inside a step, waiting for the kernels running) */
   cudaFuncAttributes fa;
   const void* ks[] = {
-      reinterpret_cast<const void*>(kb_inter_simple), reinterpret_cast<const void*>(kb_inter<3>),
+      reinterpret_cast<const void*>(kb_inter_simple<false>),
+      reinterpret_cast<const void*>(kb_inter_simple<true>), reinterpret_cast<const void*>(kb_inter<3>),
       reinterpret_cast<const void*>(kb_inter<4>),
       reinterpret_cast<const void*>(kb_itx<2>), reinterpret_cast<const void*>(kb_itx<3>),
       reinterpret_cast<const void*>(kb_itx<4>), reinterpret_cast<const void*>(kb_itx<5>),
@@ -429,8 +437,9 @@ int batch_stage_max_ctas(int stage) {
   int threads = 128;
   size_t smem = 0;
   switch (stage) {
-    case kBInterSimple: k = reinterpret_cast<const void*>(kb_inter_simple); break;
-    case kBInter: case kBInterMask: k = reinterpret_cast<const void*>(kb_inter<4>); break;
+    case kBInterSimple: k = reinterpret_cast<const void*>(kb_inter_simple<false>); break;
+    case kBInterLeanMask: case kBInterMask: k = reinterpret_cast<const void*>(kb_inter_simple<true>); break;
+    case kBInter: k = reinterpret_cast<const void*>(kb_inter<4>); break;
     case kBItx2: k = reinterpret_cast<const void*>(kb_itx<2>); smem = 4 * ItxScratch<2>::PER_WARP * sizeof(int); break;
     case kBItx3: k = reinterpret_cast<const void*>(kb_itx<3>); smem = 4 * ItxScratch<3>::PER_WARP * sizeof(int); break;
     case kBItx4: k = reinterpret_cast<const void*>(kb_itx<4>); smem = 4 * ItxScratch<4>::PER_WARP * sizeof(int); break;

@@ -172,10 +172,14 @@ int bcuda(av1b_batch* b, cudaError_t e, const char* what) {
     if (e_ != cudaSuccess) return bcuda(b, e_, what);      \
   } while (0)
 
+static_assert(kBStageCount <= static_cast<int>(sizeof(av1b_batch_config::ctas_per_sm) / sizeof(int32_t)),
+              "the public launch-shape array holds every stage");
+
 /* Launch shapes before tuning: CTAs per SM of each stage kernel. */
 void default_tuning(BatchTuning* t) {
   static const int ctas[kBStageCount] = {
-      4, 4, 4,              /* prediction: lean, full, chroma tiles reading luma masks */
+      4, 4, 4, 4,           /* prediction: lean unmasked, lean masked, full, chroma
+                               tiles reading luma masks */
       4, 4, 4, 4, 2, 2,     /* transforms by class */
       AV1B_UNIT_CTAS_PER_SM,
       8, 8,                 /* deblocking */
@@ -318,7 +322,8 @@ int batch_step(av1b_batch* b, int n, av1b_decoder* const* decs, av1b_plan* const
     const FilterArgs& f = sp[i].f;
     long long items[kBStageCount] = {};
     items[kBInterSimple] = a.n_inter_simple;
-    items[kBInter] = a.n_inter_tiles - a.n_inter_simple - a.n_inter_cmask;
+    items[kBInterLeanMask] = a.n_inter_lmask;
+    items[kBInter] = a.n_inter_tiles - a.n_inter_simple - a.n_inter_lmask - a.n_inter_cmask;
     items[kBInterMask] = a.n_inter_cmask;
     for (int c = 2; c <= 7; ++c) items[kBItx2 + c - 2] = a.n_itx_batches > 0 ? a.itx_class_count[c] : 0;
     items[kBUnits] = a.n_chains;
@@ -708,7 +713,7 @@ int av1b_batch_autotune(av1b_batch* b, int n, av1b_decoder* const* decoders,
   /* coordinate descent over groups of stages that share a launch shape,
    * then the claim size, then the grain-in-pack fusion */
   const std::vector<std::vector<int>> groups = {
-      {kBInterSimple, kBInter, kBInterMask},
+      {kBInterSimple, kBInterLeanMask, kBInter, kBInterMask},
       {kBItx2, kBItx3, kBItx4, kBItx5, kBItx6, kBItx7},
       {kBUnits},
       {kBDeblockV, kBDeblockH},

@@ -442,7 +442,8 @@ void sized(V& v, size_t n) {
 
 struct Plan {
   PlanLists* R = nullptr;         /* while planning: the lists being built */
-  size_t n_tiles_simple = 0;      /* inter tiles the lean kernel takes (listed first) */
+  size_t n_tiles_simple = 0;      /* unmasked inter tiles (the lean kernel, listed first) */
+  size_t n_tiles_lmask = 0;       /* masked tiles the lean kernel takes (listed next) */
   size_t n_tiles_cmask = 0;       /* chroma tiles reading a luma block's mask (listed last) */
   size_t mask_pool = 0;           /* bytes of the difference-weighted luma masks */
   size_t n_blocks = 0, n_units = 0, n_chains = 0, n_tiles = 0, n_itx = 0, n_itxb = 0, n_dbv = 0, n_dbh = 0,
@@ -529,7 +530,7 @@ struct BlockOut {
   std::vector<WarpRec> warps;
   std::vector<int> palette_colors;
   std::vector<int> units;
-  std::vector<int2> inter_tiles, inter_tiles_full;
+  std::vector<int2> inter_tiles, inter_tiles_mask, inter_tiles_full;
   std::vector<int2> itx_jobs;
   std::vector<DqRec> dq;
   size_t pre_res_pool = 0, coef_end = 0, res_end = 0;
@@ -554,6 +555,7 @@ struct BlockOut {
     palette_colors.clear();
     units.clear();
     inter_tiles.clear();
+    inter_tiles_mask.clear();
     inter_tiles_full.clear();
     itx_jobs.clear();
     pre_res_pool = coef_end = res_end = 0;
@@ -833,10 +835,14 @@ int plan_block(const PlanCtx& ctx, const av1b_frame_syntax& s, size_t bi, BlockR
   } else {
     O->inter_samples += static_cast<size_t>(b.w) * b.h;
     O->inter_ref_samples += static_cast<size_t>(b.w) * b.h * (r.compound ? 2 : 1);
-    /* blocks without masks (translation or global warp, with or without
-     * OBMC) take the lean prediction kernel */
-    const bool simple = r.mask_kind == 0 && !r.interintra;
-    auto& tiles = simple ? O->inter_tiles : O->inter_tiles_full;
+    /* the lean prediction kernel takes every block but inter-intra ones
+     * and the chroma of difference-weighted compounds, whose masks come from
+     * luma predictions (those of them that read the luma block's mask return
+     * to the lean kernel, last): unmasked blocks (translation or global warp,
+     * OBMC, average or distance compound) in one build, wedge and luma
+     * difference-weighted compounds in the masked one */
+    const bool full = r.interintra || (r.mask_kind == 2 && r.plane > 0);
+    auto& tiles = full ? O->inter_tiles_full : (r.mask_kind ? O->inter_tiles_mask : O->inter_tiles);
     for (int y0 = 0; y0 < b.h; y0 += 8)
       for (int x0 = 0; x0 < b.w; x0 += 16)
         tiles.push_back(make_int2(static_cast<int>(bi), x0 | (y0 << 16)));
@@ -1365,13 +1371,14 @@ void plan_shared_masks(const PlanCtx& c, Plan* P) {
   P->mask_pool = 0;
   P->n_tiles_cmask = 0;
   const size_t nt = R.inter_tiles.size();
-  if (nt == P->n_tiles_simple) return;
+  const size_t full0 = P->n_tiles_simple + P->n_tiles_lmask;
+  if (nt == full0) return;
   const int ow = static_cast<int>((L.p[0].grid_w + 3) >> 2);
   const int oh = static_cast<int>((L.p[0].grid_h + 3) >> 2);
   if (S.owner[0].size() < static_cast<size_t>(ow) * oh) return;
   size_t pool = 0;
   bool any = false;
-  for (size_t i = P->n_tiles_simple; i < nt; ++i) {
+  for (size_t i = full0; i < nt; ++i) {
     const int bi = R.inter_tiles[i].x;
     BlockRec& b = R.blocks[bi];
     if (b.plane == 0 || b.mask_role || b.mask_kind != 2 || !b.compound || b.interintra) continue;
@@ -1410,7 +1417,7 @@ void plan_shared_masks(const PlanCtx& c, Plan* P) {
   if (!any) return;
   P->mask_pool = pool;
   /* the tiles reading a mask to the end, the others in their order */
-  auto first = R.inter_tiles.begin() + static_cast<std::ptrdiff_t>(P->n_tiles_simple);
+  auto first = R.inter_tiles.begin() + static_cast<std::ptrdiff_t>(full0);
   auto mid = std::stable_partition(first, R.inter_tiles.end(),
                                    [&](const int2& t) { return R.blocks[t.x].mask_role != 2; });
   P->n_tiles_cmask = static_cast<size_t>(R.inter_tiles.end() - mid);
@@ -1507,7 +1514,8 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
     }
     /* piece offsets into the frame's lists */
     std::vector<size_t> o_tx(pieces + 1, 0), o_obmc(pieces + 1, 0), o_warp(pieces + 1, 0),
-        o_pal(pieces + 1, 0), o_unit(pieces + 1, 0), o_tile(pieces + 1, 0), o_tilef(pieces + 1, 0),
+        o_pal(pieces + 1, 0), o_unit(pieces + 1, 0), o_tile(pieces + 1, 0), o_tilem(pieces + 1, 0),
+        o_tilef(pieces + 1, 0),
         o_itx(pieces + 1, 0), o_pre(pieces + 1, 0), o_dq(pieces + 1, 0);
     for (int i = 0; i < pieces; ++i) {
       const BlockOut& O = outs[i];
@@ -1517,6 +1525,7 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
       o_pal[i + 1] = o_pal[i] + O.palette_colors.size();
       o_unit[i + 1] = o_unit[i] + O.units.size();
       o_tile[i + 1] = o_tile[i] + O.inter_tiles.size();
+      o_tilem[i + 1] = o_tilem[i] + O.inter_tiles_mask.size();
       o_tilef[i + 1] = o_tilef[i] + O.inter_tiles_full.size();
       o_itx[i + 1] = o_itx[i] + O.itx_jobs.size();
       o_pre[i + 1] = o_pre[i] + O.pre_res_pool;
@@ -1540,9 +1549,10 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
     P->R->warps[0] = WarpRec{};
     sized(P->R->palette_colors, o_pal[pieces]);
     sized(P->R->units, o_unit[pieces]);
-    /* the lean kernel's tiles first, then the rest */
-    sized(P->R->inter_tiles, o_tile[pieces] + o_tilef[pieces]);
+    /* the lean kernel's unmasked tiles, its masked ones, then the rest */
+    sized(P->R->inter_tiles, o_tile[pieces] + o_tilem[pieces] + o_tilef[pieces]);
     P->n_tiles_simple = o_tile[pieces];
+    P->n_tiles_lmask = o_tilem[pieces];
     c.scratch->itx_unsorted.resize(o_itx[pieces]);
     sized(P->R->itx_jobs, o_itx[pieces]);
     sized(P->R->dq, o_dq[pieces]);
@@ -1571,8 +1581,10 @@ int build_plan(av1b_decoder* d, const PlanCtx& c, const av1b_frame_syntax& s, Pl
       std::copy(O.palette_colors.begin(), O.palette_colors.end(), P->R->palette_colors.begin() + o_pal[i]);
       std::copy(O.units.begin(), O.units.end(), P->R->units.begin() + o_unit[i]);
       std::copy(O.inter_tiles.begin(), O.inter_tiles.end(), P->R->inter_tiles.begin() + o_tile[i]);
+      std::copy(O.inter_tiles_mask.begin(), O.inter_tiles_mask.end(),
+                P->R->inter_tiles.begin() + o_tile[pieces] + o_tilem[i]);
       std::copy(O.inter_tiles_full.begin(), O.inter_tiles_full.end(),
-                P->R->inter_tiles.begin() + o_tile[pieces] + o_tilef[i]);
+                P->R->inter_tiles.begin() + o_tile[pieces] + o_tilem[pieces] + o_tilef[i]);
       for (size_t k = 0; k < O.itx_jobs.size(); ++k) {
         int2 j = O.itx_jobs[k];
         j.y += dtx;
@@ -2301,6 +2313,7 @@ int prepare_step(av1b_decoder* d, av1b_plan* pl, int keep, int forced_slot, bool
   a.inter_tiles = reinterpret_cast<const int2*>(ar + pl->o_tiles);
   a.n_inter_tiles = static_cast<int>(P.n_tiles);
   a.n_inter_simple = static_cast<int>(P.n_tiles_simple);
+  a.n_inter_lmask = static_cast<int>(P.n_tiles_lmask);
   a.n_inter_cmask = static_cast<int>(P.n_tiles_cmask);
   a.mask_pool = static_cast<unsigned char*>(d->mask_pool.p);
   a.itx_jobs = reinterpret_cast<const int2*>(ar + pl->o_itx);

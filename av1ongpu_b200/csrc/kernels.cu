@@ -131,12 +131,56 @@ __device__ void make_inter_job(const FrameArgs& a, const BlockRec& b, InterJob* 
 
 /* ---- phase A ------------------------------------------------------------------------ */
 
-/* Inter prediction of the phase A blocks without masks (almost every inter
- * block): one warp per 16x8 tile, each reference through mc_rect or, for a
- * globally warped one, warp_block8, then the average or distance-weighted
- * blend, then the OBMC strips in order, each neighbour's prediction of the
- * strip through mc_rect. It carries none of the full kernel's state, so it
- * runs with a fraction of its registers and many more warps in flight. */
+/* The compound mask of a block the lean kernel predicts, its fields read
+ * once into registers (the mask pool's byte stores could alias the block
+ * record, so fields read from it would be loaded again after every store). */
+struct LeanMask {
+  int kind, sign, role, off, mw, dir, xoff, yoff, flip;
+  __device__ __forceinline__ explicit LeanMask(const BlockRec& b)
+      : kind(b.compound ? b.mask_kind : 0), sign(b.mask_sign), role(b.mask_role), off(b.mask_off),
+        mw(b.mask_w), dir(b.wedge_dir), xoff(b.wedge_xoff), yoff(b.wedge_yoff), flip(b.wedge_flip) {}
+};
+
+/* The mask (0..64) of sample (x, y): a wedge (a chroma sample averages the
+ * luma positions it covers), a luma difference-weighted mask from the two
+ * predictions - written to the mask pool when chroma blocks read it - or a
+ * chroma difference-weighted mask read from the pool its luma block wrote. */
+__device__ __forceinline__ int lean_mask(const FrameArgs& a, const LeanMask& k, int plane, int sub_x,
+                                         int sub_y, int bitdepth, int x, int y, int v0, int v1) {
+  if (k.kind == 2 && plane == 0) {
+    const int sh = 7 - (bitdepth >= 12 ? 5 : 3) + (bitdepth - 8);
+    const int m = diffwtd_m(absi(v0 - v1), sh, k.sign);
+    if (k.role == 1) a.mask_pool[k.off + y * k.mw + x] = static_cast<unsigned char>(m);
+    return m;
+  }
+  const int nx = sub_x + 1, ny = sub_y + 1;
+  int sum = 0;
+  for (int jj = 0; jj < ny; ++jj)
+    for (int ii = 0; ii < nx; ++ii) {
+      const int lx = (x << sub_x) + ii, ly = (y << sub_y) + jj;
+      if (k.kind == 1) {
+        const int m = wedge_px(k.dir, k.xoff, k.yoff, k.flip, ly, lx);
+        sum += k.sign ? 64 - m : m;
+      } else {
+        sum += a.mask_pool[k.off + ly * k.mw + lx];
+      }
+    }
+  const int n = nx * ny;
+  return n == 1 ? sum : (n == 2 ? (sum + 1) >> 1 : (sum + 2) >> 2);
+}
+
+/* Inter prediction of the phase A blocks but inter-intra ones and chroma
+ * blocks of difference-weighted compounds without a luma mask to read (they
+ * take the full kernel): one warp per 16x8 tile, each reference through
+ * mc_rect or, for a globally warped one, warp_block8, then the blend, then
+ * the OBMC strips in order, each neighbour's prediction of the strip through
+ * mc_rect. It carries none of the full kernel's state, so it runs with a
+ * fraction of its registers and many more warps in flight. Two builds: the
+ * average and distance-weighted blends (MASK false: translation, global
+ * warp and OBMC blocks, almost every tile), and the masked blends (MASK
+ * true: wedge and difference-weighted compounds) - the mask code in the
+ * first build slows its tiles by a fifth. */
+template <bool MASK>
 __device__ __forceinline__ void inter_simple_tile(const FrameArgs& a, int tile, McScratch& scr,
                                                   int (&pred)[2][8 * 16], int lane) {
   const int2 t = a.inter_tiles[tile];
@@ -180,19 +224,32 @@ __device__ __forceinline__ void inter_simple_tile(const FrameArgs& a, int tile, 
   px_t* dst = a.cur + g.off + (b.y + y0) * g.stride + b.x + x0;
   const int post = 7 - (c.bitdepth >= 12 ? 5 : 3);
   int acc[4];
+  if constexpr (MASK) {
+    const LeanMask mk(b);
 #pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const int k = lane + 32 * q;
-    if (k >= tw * th) continue;
-    const int yy = (k * tmul) >> 16, xx = k - yy * tw;
-    const int v0 = pred[0][yy * 16 + xx];
-    int out = v0;
-    if (b.compound == 1) {
-      out = (v0 + pred[1][yy * 16 + xx] + (1 << post)) >> (1 + post);
-    } else if (b.compound) {
-      out = (b.w0 * v0 + b.w1 * pred[1][yy * 16 + xx] + (1 << (3 + post))) >> (4 + post);
+    for (int q = 0; q < 4; ++q) {
+      const int k = lane + 32 * q;
+      if (k >= tw * th) continue;
+      const int yy = (k * tmul) >> 16, xx = k - yy * tw;
+      const int v0 = pred[0][yy * 16 + xx], v1 = pred[1][yy * 16 + xx];
+      const int m = lean_mask(a, mk, p, c.sub_x, c.sub_y, c.bitdepth, x0 + xx, y0 + yy, v0, v1);
+      acc[q] = clampi((m * v0 + (64 - m) * v1 + (1 << (5 + post))) >> (6 + post), 0, a.maxv);
     }
-    acc[q] = clampi(out, 0, a.maxv);
+  } else {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int k = lane + 32 * q;
+      if (k >= tw * th) continue;
+      const int yy = (k * tmul) >> 16, xx = k - yy * tw;
+      const int v0 = pred[0][yy * 16 + xx];
+      int out = v0;
+      if (b.compound == 1) {
+        out = (v0 + pred[1][yy * 16 + xx] + (1 << post)) >> (1 + post);
+      } else if (b.compound) {
+        out = (b.w0 * v0 + b.w1 * pred[1][yy * 16 + xx] + (1 << (3 + post))) >> (4 + post);
+      }
+      acc[q] = clampi(out, 0, a.maxv);
+    }
   }
   __syncwarp();
   /* OBMC: the strips in order, each blended onto the samples it covers */
@@ -230,13 +287,19 @@ __device__ __forceinline__ void inter_simple_tile(const FrameArgs& a, int tile, 
   }
 }
 
-__global__ void __launch_bounds__(128) k_inter_simple(const __grid_constant__ FrameArgs a) {
+/* Tiles [first, end) of the lean kernel's: the unmasked tiles listed first;
+ * the masked build takes the wedge and luma difference-weighted tiles listed
+ * next and (a launch of their own, after the luma tiles that write the
+ * masks) the chroma tiles that read a luma mask, listed last. */
+template <bool MASK>
+__global__ void __launch_bounds__(128) k_inter_simple(const __grid_constant__ FrameArgs a, int first,
+                                                      int end) {
   __shared__ McScratch scr[4];
   __shared__ int pred[4][2][8 * 16];
   const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int warp = blockIdx.x * 4 + wib;
-  if (warp >= a.n_inter_simple) return;
-  inter_simple_tile(a, warp, scr[wib], pred[wib], lane);
+  const int warp = first + blockIdx.x * 4 + wib;
+  if (warp >= end) return;
+  inter_simple_tile<MASK>(a, warp, scr[wib], pred[wib], lane);
 }
 
 /* Inter prediction of phase A blocks: one warp per 16x8 tile. Translation
@@ -400,9 +463,8 @@ __device__ __forceinline__ void inter_full_tile(const FrameArgs& a, int tile, Mc
   }
 }
 
-/* Tiles [first, end) of the full kernel's: the tiles before the chroma
- * tiles that read a luma mask, then those (a launch of their own, after the
- * luma tiles that write the masks). */
+/* Tiles [first, end) of the full kernel's (between the lean kernel's two
+ * ranges). */
 __global__ void __launch_bounds__(128, 4) k_inter(const __grid_constant__ FrameArgs a, int first, int end) {
   __shared__ McScratch scr[4];
   __shared__ int pred[4][2][8 * 16];
@@ -565,13 +627,15 @@ static cudaError_t launch_itx_class(const FrameArgs& a, cudaStream_t s) {
  * fence); without, relaxed polls and one acquire fence once the flag is seen.
  * Between polls the warp sleeps, backing off to AV1B_POLL_PAUSE_MAX ns (0: no
  * sleep). Acquire polls take about 6 % off the dependency-scheduled phase
- * (the fence after a relaxed poll is a round trip of its own on the path);
- * the pause, between 0 and 64 ns, changes nothing measurable. */
+ * (the fence after a relaxed poll is a round trip of its own on the path).
+ * Shorter pauses gain nothing on one stream, and with many streams' chains
+ * waiting at once (a batched key frame-set) 64 ns pauses saw occasional
+ * steps of twice the usual time, 256 ns none. */
 #ifndef AV1B_POLL_ACQUIRE
 #define AV1B_POLL_ACQUIRE 1
 #endif
 #ifndef AV1B_POLL_PAUSE_MAX
-#define AV1B_POLL_PAUSE_MAX 64
+#define AV1B_POLL_PAUSE_MAX 256
 #endif
 
 __device__ __forceinline__ bool flag_seen(const unsigned* flag, unsigned want) {
@@ -1905,14 +1969,17 @@ cudaError_t launch_recon_stage(int stage, const FrameArgs& a, int n_sm, cudaStre
     case 1:
       if (a.n_inter_tiles > 0)
       {
-        if (a.n_inter_simple > 0) k_inter_simple<<<cdiv(a.n_inter_simple, 4), 128, 0, s>>>(a);
+        if (a.n_inter_simple > 0)
+          k_inter_simple<false><<<cdiv(a.n_inter_simple, 4), 128, 0, s>>>(a, 0, a.n_inter_simple);
+        const int lm_end = a.n_inter_simple + a.n_inter_lmask;
+        if (a.n_inter_lmask > 0)
+          k_inter_simple<true><<<cdiv(a.n_inter_lmask, 4), 128, 0, s>>>(a, a.n_inter_simple, lm_end);
         /* the full kernel's tiles, then the chroma tiles that read the masks
          * the luma tiles wrote */
         const int cm_first = a.n_inter_tiles - a.n_inter_cmask;
-        const int rest = cm_first - a.n_inter_simple;
-        if (rest > 0) k_inter<<<cdiv(rest, 4), 128, 0, s>>>(a, a.n_inter_simple, cm_first);
+        if (cm_first > lm_end) k_inter<<<cdiv(cm_first - lm_end, 4), 128, 0, s>>>(a, lm_end, cm_first);
         if (a.n_inter_cmask > 0)
-          k_inter<<<cdiv(a.n_inter_cmask, 4), 128, 0, s>>>(a, cm_first, a.n_inter_tiles);
+          k_inter_simple<true><<<cdiv(a.n_inter_cmask, 4), 128, 0, s>>>(a, cm_first, a.n_inter_tiles);
       }
       break;
     case 2:
@@ -2096,7 +2163,8 @@ static cudaError_t load_kernel(K k) {
 
 static cudaError_t load_all_kernels() {
   cudaError_t e;
-  if ((e = load_kernel(k_inter_simple)) != cudaSuccess || (e = load_kernel(k_inter)) != cudaSuccess ||
+  if ((e = load_kernel(k_inter_simple<false>)) != cudaSuccess ||
+      (e = load_kernel(k_inter_simple<true>)) != cudaSuccess || (e = load_kernel(k_inter)) != cudaSuccess ||
       (e = load_kernel(k_itx<2>)) != cudaSuccess || (e = load_kernel(k_itx<3>)) != cudaSuccess ||
       (e = load_kernel(k_itx<4>)) != cudaSuccess || (e = load_kernel(k_itx<5>)) != cudaSuccess ||
       (e = load_kernel(k_itx<6>)) != cudaSuccess || (e = load_kernel(k_itx<7>)) != cudaSuccess ||

@@ -67,7 +67,9 @@ struct FrameArgs {
   unsigned* queue;
   const int2* inter_tiles;      /* phase A: (block, x0 | y0 << 16) */
   int n_inter_tiles;
-  int n_inter_simple;           /* the first ones: translation-only blocks */
+  int n_inter_simple;           /* the first ones: unmasked blocks (the lean kernel) */
+  int n_inter_lmask;            /* the next ones: wedge and luma difference-weighted
+                                   compounds (the lean kernel's masked build) */
   int n_inter_cmask;            /* the last ones: chroma tiles reading a luma mask */
   unsigned char* mask_pool;     /* blend masks of difference-weighted luma blocks */
   const int2* itx_jobs;         /* phase A: (block, transform); the transforms of

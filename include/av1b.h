@@ -381,7 +381,7 @@ AV1B_API void* av1b_decoder_stream(av1b_decoder* dec);
 #define AV1B_BATCH_MAX 64
 typedef struct av1b_batch av1b_batch;
 /* The step's launch shape: CTAs per SM of each stage kernel (0: keep the
- * current value; stages in launch order, 22 of them), the work items a warp
+ * current value; stages in launch order, 23 of them), the work items a warp
  * claims at once, whether the film grain of a stream whose only output is
  * its NV12 pack is applied inside the pack (its display picture is then made
  * when an output call asks for it), and whether steps replay as a CUDA graph. */
@@ -419,7 +419,7 @@ AV1B_API const char* av1b_batch_last_error(av1b_batch* batch);
 /* Per-stage device time of batched steps: with profiling on, steps launch
  * without the graph, each stage bracketed by CUDA events, and
  * av1b_batch_profile gives stage `stage`'s summed milliseconds (in launch
- * order, 0..21; the grain templates run beside the others) and the steps
+ * order, 0..22; the grain templates run beside the others) and the steps
  * timed. Switching profiling clears the sums. */
 AV1B_API int av1b_batch_set_profiling(av1b_batch* batch, int on);
 AV1B_API int av1b_batch_profile(av1b_batch* batch, int stage, double* total_ms, long long* steps);
