@@ -163,6 +163,7 @@ _SIGNATURES = {
                                            ctypes.POINTER(ctypes.c_size_t)]),
     'av1b_batch_stream': (ctypes.c_void_p, [ctypes.c_void_p]),
     'av1b_int_peak': (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
+    'av1b_handoff_peak': (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     'av1b_set_profiling': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     'av1b_set_wait_limit': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong]),
     'av1b_selftest_wait': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, ctypes.POINTER(ctypes.c_int),
@@ -723,6 +724,17 @@ def int_peak(device=0, kind=0):
     rc = lib().av1b_int_peak(device, kind, ctypes.byref(v))
     if rc:
         raise Av1bError(rc, 'int_peak')
+    return v.value
+
+
+def handoff_peak(device=0):
+    """The floor of a dependency step (av1b_handoff_peak): the median one-way
+    ns of a flag handed between warps on two SMs by a release store and
+    acquire polls."""
+    v = ctypes.c_double(0)
+    rc = lib().av1b_handoff_peak(device, ctypes.byref(v))
+    if rc:
+        raise Av1bError(rc, 'handoff_peak')
     return v.value
 
 

@@ -10,6 +10,12 @@
  *
  * Each ring step is one source operation (a + b, or a * b + c, which the
  * hardware issues as one instruction); the result counts steps per second.
+ *
+ * The dependency-scheduled phase is bound by neither: each step of its
+ * critical path is a block published on one SM and seen by a waiter on
+ * another. Its floor is measured too: the one-way time of a flag handed
+ * between warps on two SMs with the phase's own release store and acquire
+ * polls, nothing else in the step.
  */
 #include <cuda_runtime.h>
 
@@ -37,8 +43,118 @@ __global__ void __launch_bounds__(256) k_int_peak(int* out, int iters, int seed)
   if (r == 0x7fffffff) out[0] = r;  /* keeps the work live; practically never stores */
 }
 
+__device__ __forceinline__ unsigned handoff_ld(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void handoff_st(unsigned* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long handoff_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+/* CTA 0 hands a flag back and forth with CTA j = 1 .. partners in turn,
+ * `rounds` round trips each; ns[j] = the round trips' total time. Flags sit
+ * 128 bytes apart (ping and reply of partner j at flags[64 j], flags[64 j +
+ * 32]). Every wait gives up after `limit` polls and sets *err; the launch is
+ * cooperative, so the partners are resident while CTA 0 waits for them. */
+__global__ void k_handoff(unsigned* flags, unsigned long long* ns, int partners, int rounds,
+                          unsigned limit, int* err) {
+  if (threadIdx.x != 0) return;
+  const int me = blockIdx.x;
+  for (int j = 1; j <= partners; ++j) {
+    unsigned* ping = flags + 64 * j;
+    unsigned* reply = ping + 32;
+    if (me == 0) {
+      const unsigned long long t0 = handoff_ns();
+      for (int k = 0; k < rounds; ++k) {
+        handoff_st(ping, 2u * k + 1u);
+        unsigned it = 0;
+        while (handoff_ld(reply) != 2u * k + 2u)
+          if (++it > limit) {
+            atomicExch(err, 1);
+            return;
+          }
+      }
+      ns[j] = handoff_ns() - t0;
+    } else if (me == j) {
+      for (int k = 0; k < rounds; ++k) {
+        unsigned it = 0;
+        while (handoff_ld(ping) != 2u * k + 1u)
+          if (++it > limit) {
+            atomicExch(err, 1);
+            return;
+          }
+        handoff_st(reply, 2u * k + 2u);
+      }
+    }
+    if (*reinterpret_cast<volatile int*>(err)) return;
+  }
+}
+
 }  // namespace
 }  // namespace av1b
+
+/* The median one-way time, in ns, of a flag handed between warps on two SMs
+ * with release stores and acquire polls (CTA 0 against up to 16 partners, 32
+ * round trips each). */
+extern "C" AV1B_API int av1b_handoff_peak(int device, double* one_way_ns) {
+  if (!one_way_ns) return AV1B_ERR_ARG;
+  int prev = 0;
+  if (cudaGetDevice(&prev) != cudaSuccess) return AV1B_ERR_NO_DEVICE;
+  if (cudaSetDevice(device) != cudaSuccess) return AV1B_ERR_NO_DEVICE;
+  int n_sm = 0, coop = 0;
+  cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, device);
+  cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
+  int rc = AV1B_ERR_CUDA;
+  const int partners = n_sm - 1 < 16 ? n_sm - 1 : 16, rounds = 32;
+  unsigned* flags = nullptr;
+  unsigned long long* ns = nullptr;
+  int* err = nullptr;
+  if (coop && partners >= 1 && cudaMalloc(&flags, 64 * sizeof(unsigned) * (partners + 1)) == cudaSuccess &&
+      cudaMalloc(&ns, sizeof(unsigned long long) * (partners + 1)) == cudaSuccess &&
+      cudaMalloc(&err, sizeof(int)) == cudaSuccess &&
+      cudaMemset(flags, 0, 64 * sizeof(unsigned) * (partners + 1)) == cudaSuccess &&
+      cudaMemset(ns, 0, sizeof(unsigned long long) * (partners + 1)) == cudaSuccess &&
+      cudaMemset(err, 0, sizeof(int)) == cudaSuccess) {
+    int np = partners, nr = rounds;
+    unsigned limit = 1u << 22;
+    void* args[] = {&flags, &ns, &np, &nr, &limit, &err};
+    /* one CTA of one warp on each SM */
+    if (cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(av1b::k_handoff), dim3(n_sm), dim3(32),
+                                    args, 0, nullptr) == cudaSuccess &&
+        cudaDeviceSynchronize() == cudaSuccess) {
+      unsigned long long h[17] = {0};
+      int herr = 0;
+      if (cudaMemcpy(h, ns, sizeof(unsigned long long) * (partners + 1), cudaMemcpyDeviceToHost) ==
+              cudaSuccess &&
+          cudaMemcpy(&herr, err, sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess && !herr) {
+        /* median over the partners */
+        for (int a = 1; a <= partners; ++a)
+          for (int b = a + 1; b <= partners; ++b)
+            if (h[b] < h[a]) {
+              const unsigned long long t = h[a];
+              h[a] = h[b];
+              h[b] = t;
+            }
+        const unsigned long long mid = h[1 + (partners - 1) / 2];
+        *one_way_ns = static_cast<double>(mid) / (2.0 * rounds);
+        rc = AV1B_OK;
+      } else if (herr) {
+        rc = AV1B_ERR_TIMEOUT;
+      }
+    }
+  }
+  if (flags) cudaFree(flags);
+  if (ns) cudaFree(ns);
+  if (err) cudaFree(err);
+  cudaSetDevice(prev);
+  return rc;
+}
 
 /* Ring steps per second of `kind` (0: add, 1: multiply-add) on `device`. */
 extern "C" AV1B_API int av1b_int_peak(int device, int kind, double* ops_per_s) {

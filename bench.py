@@ -271,7 +271,8 @@ def frame_counts(info, nv12_bytes):
             'unit': info['phase_b_samples'], 'inter': info['inter_samples'],
             'inter_ref': info['inter_ref_samples'], 'tx': info['tx_samples'],
             'coef': info['coef_samples'], 'upscaled': info['upscaled'],
-            'restored': info['restored'], 'grain': GRAIN_TEMPLATE_SAMPLES if info['grain'] else 0}
+            'restored': info['restored'], 'grain': GRAIN_TEMPLATE_SAMPLES if info['grain'] else 0,
+            'depth': info['depth']}
 
 
 def stage_bytes(c, stage):
@@ -319,7 +320,28 @@ def peaks(local):
     out['int_add_ops'] = av1b.int_peak(local, 0)
     out['int_mad_ops'] = av1b.int_peak(local, 1)
     out['int_source'] = 'measured live (av1b_int_peak: 32-bit add rings on every SM)'
+    try:
+        out['handoff_ns'] = av1b.handoff_peak(local)
+    except av1b.Av1bError:
+        out['handoff_ns'] = None
     return out
+
+
+def dependency_roof(prof, counts, pk):
+    """The dependency-scheduled phase against its own floor: each launch
+    walks its frame's critical path (`depth` blocks, each published on one SM
+    and waited for on another), and no step can take less than one flag
+    handoff between SMs (av1b_handoff_peak)."""
+    ms, n = prof['units']
+    steps = sum(c['depth'] for c in counts) / max(1, n)
+    floor_us = pk['handoff_ns'] / 1e3 if pk.get('handoff_ns') else None
+    achieved_us = ms / max(1, n) * 1e3 / max(1.0, steps)
+    return {'bound': 'latency', 'steps_per_launch': round(steps, 1),
+            'achieved_us_per_step': round(achieved_us, 3),
+            'floor_us_per_step': round(floor_us, 3) if floor_us else None,
+            'frac': round(floor_us / achieved_us, 4) if floor_us else None,
+            'peak_source': 'measured live (av1b_handoff_peak: release store / acquire polls '
+                           'between warps on two SMs, median of 16 SM pairs)'}
 
 
 def stage_report(prof, counts, frames, pk):
@@ -499,6 +521,8 @@ def run_ours(args):
                     'hbm': hbm, 'int_alu': alu,
                     'note': 'frac of measured peaks; traffic = ncu dram bytes per launch '
                             '(profiles/traffic.json)'}
+        if dom == 'units':
+            roofline['dependency'] = dependency_roof(prof, counts, pk)
 
     # ---- e2e: public API with host buffers ------------------------------------------------
     pinned = []

@@ -333,6 +333,12 @@ AV1B_API int av1b_selftest_wait(av1b_decoder* dec, long long limit_ns, int* stat
  * stage's counted operations by it, beside its bytes by the HBM bandwidth.
  * No counterpart in the reference. */
 AV1B_API int av1b_int_peak(int device, int kind, double* ops_per_s);
+/* The floor of one step of the dependency-scheduled phase's critical path:
+ * the median one-way time, in ns, of a flag handed between warps on two SMs
+ * by a release store and acquire polls (the publication and wait that phase
+ * uses), measured by a short cooperative kernel. No counterpart in the
+ * reference. */
+AV1B_API int av1b_handoff_peak(int device, double* one_way_ns);
 
 /* Per-stage device timing: with profiling on, every launch (and device copy)
  * is bracketed by CUDA events on the decoder's stream, and the elapsed times

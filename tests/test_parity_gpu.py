@@ -312,6 +312,14 @@ def test_bounded_wait_gives_up(dec):
     assert 1.0 < ms < 1000.0
 
 
+def test_measured_peaks(av1b):
+    """The roofs the stage report divides by: the integer-ALU peak and the
+    floor of a dependency step (one flag handed between two SMs)."""
+    assert av1b.int_peak(0, 0) > 1e12
+    ns = av1b.handoff_peak(0)
+    assert 50.0 < ns < 20000.0
+
+
 def test_hbm_budget_is_enforced(av1b):
     d = av1b.Decoder(0, hbm_budget=1 << 20)
     with pytest.raises(av1b.Av1bError) as e:
