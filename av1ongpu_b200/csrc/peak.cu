@@ -58,50 +58,54 @@ __device__ __forceinline__ unsigned long long handoff_ns() {
 }
 
 /* CTA 0 hands a flag back and forth with CTA j = 1 .. partners in turn,
- * `rounds` round trips each; ns[j] = the round trips' total time. Flags sit
- * 128 bytes apart (ping and reply of partner j at flags[64 j], flags[64 j +
- * 32]). Every wait gives up after `limit` polls and sets *err; the launch is
- * cooperative, so the partners are resident while CTA 0 waits for them. */
+ * `rounds` round trips each, with the flags at each of `places` places in
+ * memory (`place_stride` words apart: the L2 slice that holds a flag, against
+ * where the two SMs sit, changes the time); ns[place * (partners + 1) + j] =
+ * the round trips' total time. The ping and reply of partner j sit 128 bytes
+ * apart at place + 64 j and place + 64 j + 32. Every wait gives up after
+ * `limit` polls and sets *err; the launch is cooperative, so the partners are
+ * resident while CTA 0 waits for them. */
 __global__ void k_handoff(unsigned* flags, unsigned long long* ns, int partners, int rounds,
-                          unsigned limit, int* err) {
+                          int places, int place_stride, unsigned limit, int* err) {
   if (threadIdx.x != 0) return;
   const int me = blockIdx.x;
-  for (int j = 1; j <= partners; ++j) {
-    unsigned* ping = flags + 64 * j;
-    unsigned* reply = ping + 32;
-    if (me == 0) {
-      const unsigned long long t0 = handoff_ns();
-      for (int k = 0; k < rounds; ++k) {
-        handoff_st(ping, 2u * k + 1u);
-        unsigned it = 0;
-        while (handoff_ld(reply) != 2u * k + 2u)
-          if (++it > limit) {
-            atomicExch(err, 1);
-            return;
-          }
+  for (int pl = 0; pl < places; ++pl)
+    for (int j = 1; j <= partners; ++j) {
+      unsigned* ping = flags + static_cast<size_t>(pl) * place_stride + 64 * j;
+      unsigned* reply = ping + 32;
+      if (me == 0) {
+        const unsigned long long t0 = handoff_ns();
+        for (int k = 0; k < rounds; ++k) {
+          handoff_st(ping, 2u * k + 1u);
+          unsigned it = 0;
+          while (handoff_ld(reply) != 2u * k + 2u)
+            if (++it > limit) {
+              atomicExch(err, 1);
+              return;
+            }
+        }
+        ns[pl * (partners + 1) + j] = handoff_ns() - t0;
+      } else if (me == j) {
+        for (int k = 0; k < rounds; ++k) {
+          unsigned it = 0;
+          while (handoff_ld(ping) != 2u * k + 1u)
+            if (++it > limit) {
+              atomicExch(err, 1);
+              return;
+            }
+          handoff_st(reply, 2u * k + 2u);
+        }
       }
-      ns[j] = handoff_ns() - t0;
-    } else if (me == j) {
-      for (int k = 0; k < rounds; ++k) {
-        unsigned it = 0;
-        while (handoff_ld(ping) != 2u * k + 1u)
-          if (++it > limit) {
-            atomicExch(err, 1);
-            return;
-          }
-        handoff_st(reply, 2u * k + 2u);
-      }
+      if (*reinterpret_cast<volatile int*>(err)) return;
     }
-    if (*reinterpret_cast<volatile int*>(err)) return;
-  }
 }
 
 }  // namespace
 }  // namespace av1b
 
 /* The median one-way time, in ns, of a flag handed between warps on two SMs
- * with release stores and acquire polls (CTA 0 against up to 16 partners, 32
- * round trips each). */
+ * with release stores and acquire polls: CTA 0 against up to 16 partners,
+ * the flags at 8 places in memory, 32 round trips each. */
 extern "C" AV1B_API int av1b_handoff_peak(int device, double* one_way_ns) {
   if (!one_way_ns) return AV1B_ERR_ARG;
   int prev = 0;
@@ -111,38 +115,48 @@ extern "C" AV1B_API int av1b_handoff_peak(int device, double* one_way_ns) {
   cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, device);
   cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
   int rc = AV1B_ERR_CUDA;
+  constexpr int kPlaces = 8;
   const int partners = n_sm - 1 < 16 ? n_sm - 1 : 16, rounds = 32;
+  /* places 16 KB + 384 bytes apart (different address bits each), each
+   * holding 64 words a partner */
+  const int place_stride = 4096 + 96;
+  const size_t words = static_cast<size_t>(kPlaces) * place_stride;
+  const size_t n_ns = static_cast<size_t>(kPlaces) * (partners + 1);
   unsigned* flags = nullptr;
   unsigned long long* ns = nullptr;
   int* err = nullptr;
-  if (coop && partners >= 1 && cudaMalloc(&flags, 64 * sizeof(unsigned) * (partners + 1)) == cudaSuccess &&
-      cudaMalloc(&ns, sizeof(unsigned long long) * (partners + 1)) == cudaSuccess &&
+  if (coop && partners >= 1 && 64 * (partners + 1) <= place_stride &&
+      cudaMalloc(&flags, words * sizeof(unsigned)) == cudaSuccess &&
+      cudaMalloc(&ns, n_ns * sizeof(unsigned long long)) == cudaSuccess &&
       cudaMalloc(&err, sizeof(int)) == cudaSuccess &&
-      cudaMemset(flags, 0, 64 * sizeof(unsigned) * (partners + 1)) == cudaSuccess &&
-      cudaMemset(ns, 0, sizeof(unsigned long long) * (partners + 1)) == cudaSuccess &&
+      cudaMemset(flags, 0, words * sizeof(unsigned)) == cudaSuccess &&
+      cudaMemset(ns, 0, n_ns * sizeof(unsigned long long)) == cudaSuccess &&
       cudaMemset(err, 0, sizeof(int)) == cudaSuccess) {
-    int np = partners, nr = rounds;
+    int np = partners, nr = rounds, npl = kPlaces, ps = place_stride;
     unsigned limit = 1u << 22;
-    void* args[] = {&flags, &ns, &np, &nr, &limit, &err};
+    void* args[] = {&flags, &ns, &np, &nr, &npl, &ps, &limit, &err};
     /* one CTA of one warp on each SM */
     if (cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(av1b::k_handoff), dim3(n_sm), dim3(32),
                                     args, 0, nullptr) == cudaSuccess &&
         cudaDeviceSynchronize() == cudaSuccess) {
-      unsigned long long h[17] = {0};
+      unsigned long long h[kPlaces * 17] = {0};
       int herr = 0;
-      if (cudaMemcpy(h, ns, sizeof(unsigned long long) * (partners + 1), cudaMemcpyDeviceToHost) ==
-              cudaSuccess &&
+      if (cudaMemcpy(h, ns, n_ns * sizeof(unsigned long long), cudaMemcpyDeviceToHost) == cudaSuccess &&
           cudaMemcpy(&herr, err, sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess && !herr) {
-        /* median over the partners */
-        for (int a = 1; a <= partners; ++a)
-          for (int b = a + 1; b <= partners; ++b)
-            if (h[b] < h[a]) {
-              const unsigned long long t = h[a];
-              h[a] = h[b];
-              h[b] = t;
+        /* the median over every place and partner (slot 0 of each place is
+         * CTA 0's own, unused) */
+        unsigned long long v[kPlaces * 16];
+        int m = 0;
+        for (int pl = 0; pl < kPlaces; ++pl)
+          for (int j = 1; j <= partners; ++j) v[m++] = h[pl * (partners + 1) + j];
+        for (int a = 0; a < m; ++a)
+          for (int b = a + 1; b < m; ++b)
+            if (v[b] < v[a]) {
+              const unsigned long long t = v[a];
+              v[a] = v[b];
+              v[b] = t;
             }
-        const unsigned long long mid = h[1 + (partners - 1) / 2];
-        *one_way_ns = static_cast<double>(mid) / (2.0 * rounds);
+        *one_way_ns = static_cast<double>(v[(m - 1) / 2]) / (2.0 * rounds);
         rc = AV1B_OK;
       } else if (herr) {
         rc = AV1B_ERR_TIMEOUT;

@@ -341,7 +341,7 @@ def dependency_roof(prof, counts, pk):
             'floor_us_per_step': round(floor_us, 3) if floor_us else None,
             'frac': round(floor_us / achieved_us, 4) if floor_us else None,
             'peak_source': 'measured live (av1b_handoff_peak: release store / acquire polls '
-                           'between warps on two SMs, median of 16 SM pairs)'}
+                           'between warps on two SMs, median of 16 SM pairs x 8 flag places)'}
 
 
 def stage_report(prof, counts, frames, pk):
