@@ -164,6 +164,7 @@ _SIGNATURES = {
     'av1b_batch_stream': (ctypes.c_void_p, [ctypes.c_void_p]),
     'av1b_int_peak': (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     'av1b_handoff_peak': (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
+    'av1b_set_shared_masks': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     'av1b_set_profiling': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     'av1b_set_wait_limit': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong]),
     'av1b_selftest_wait': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, ctypes.POINTER(ctypes.c_int),
@@ -449,6 +450,12 @@ class Decoder:
 
     def set_profiling(self, on):
         self._check(lib().av1b_set_profiling(self.h, 1 if on else 0), 'set_profiling')
+
+    def set_shared_masks(self, on):
+        """Chroma blocks of difference-weighted compounds read their luma
+        block's mask (on, the default) or predict the luma themselves (off):
+        the same samples either way."""
+        self._check(lib().av1b_set_shared_masks(self.h, 1 if on else 0), 'set_shared_masks')
 
     def set_unit_trace(self, on):
         self._check(lib().av1b_set_unit_trace(self.h, 1 if on else 0), 'set_unit_trace')

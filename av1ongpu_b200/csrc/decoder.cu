@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -169,6 +170,10 @@ struct av1b_decoder {
   std::vector<Pack> packs;
   int next_pack = 0;
   cudaStream_t copy_stream = nullptr;
+
+  /* chroma blocks of difference-weighted compounds read their luma block's
+   * mask when it is the same prediction (av1b_set_shared_masks) */
+  std::atomic<bool> share_masks{true};
 
   /* optional trace of phase B (av1b_set_unit_trace): 4 uint64 per block */
   bool tracing = false;
@@ -485,6 +490,7 @@ struct PlanCtx {
    * rasters from them (and the frame's coefficient array is not read) */
   bool levels = false;
   size_t n_levels = 0, n_qm = 0;
+  bool share_masks = true;        /* plan_shared_masks runs */
 };
 
 /* The first error one piece of the planner met. */
@@ -1370,6 +1376,7 @@ void plan_shared_masks(const PlanCtx& c, Plan* P) {
   PlanScratch& S = *c.scratch;
   P->mask_pool = 0;
   P->n_tiles_cmask = 0;
+  if (!c.share_masks) return;
   const size_t nt = R.inter_tiles.size();
   const size_t full0 = P->n_tiles_simple + P->n_tiles_lmask;
   if (nt == full0) return;
@@ -1896,6 +1903,7 @@ int plan_frame(av1b_decoder* d, const av1b_frame_syntax& s, av1b_plan* pl) {
   c.levels = s.n_levels > 0;
   c.n_levels = s.n_levels;
   c.n_qm = s.n_qm_pool;
+  c.share_masks = d->share_masks.load();
   const size_t n_coef = c.levels ? 0 : s.n_coefficients;
   if (!pl->ready) {
     /* blocking-sync events: a waiting planner sleeps instead of spinning on
@@ -3203,6 +3211,12 @@ int av1b_selftest_wait(av1b_decoder* d, long long limit_ns, int* status, double*
   dev_release(d, mem);
   *status = st;
   if (elapsed_ms) *elapsed_ms = ms;
+  return AV1B_OK;
+}
+
+int av1b_set_shared_masks(av1b_decoder* d, int on) {
+  if (!d) return AV1B_ERR_ARG;
+  d->share_masks.store(on != 0);
   return AV1B_OK;
 }
 

@@ -359,6 +359,14 @@ AV1B_API int av1b_profile(av1b_decoder* dec, int stage, const char** name, doubl
 AV1B_API int av1b_set_unit_trace(av1b_decoder* dec, int on);
 AV1B_API int av1b_unit_trace(av1b_decoder* dec, uint64_t* out, size_t cap, size_t* n);
 
+/* Whether frames planned from now on let a chroma block of a difference-
+ * weighted compound read the blend mask its luma block wrote when that block
+ * is the same prediction (on by default), instead of predicting the luma it
+ * covers itself. Both give the same samples; off, every such chroma tile
+ * takes the full prediction kernel (tests compare the two paths). No
+ * counterpart in the reference. */
+AV1B_API int av1b_set_shared_masks(av1b_decoder* dec, int on);
+
 /* CUDA stream the decoder runs on (a cudaStream_t), so a caller can order its
  * own work after a decode without a host synchronisation. */
 AV1B_API void* av1b_decoder_stream(av1b_decoder* dec);

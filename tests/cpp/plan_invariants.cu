@@ -134,6 +134,48 @@ uint64_t plan_and_check(av1b_decoder* d, WorkPool* pool, uint8_t* blob, size_t l
               o, chain_of[o]);
       }
     }
+    /* the prediction tiles: the lean kernel's unmasked tiles, its masked
+     * ones (wedge, luma difference-weighted), the full kernel's (inter-intra,
+     * chroma difference-weighted predicting its luma), then the chroma tiles
+     * that read their luma block's mask - whose luma block writes it, at the
+     * same place of the frame's mask pool */
+    const auto& T = lists.inter_tiles;
+    const size_t ns = P.n_tiles_simple, nl = P.n_tiles_lmask, nc = P.n_tiles_cmask;
+    CHECK(ns + nl + nc <= T.size(), "%s frame %d: tile groups exceed the %zu tiles", name, k, T.size());
+    std::vector<size_t> tiles_of(B.size(), 0);
+    for (size_t i = 0; i < T.size(); ++i) {
+      const int bi = T[i].x;
+      CHECK(bi >= 0 && static_cast<size_t>(bi) < B.size() && !B[bi].phase_b && B[bi].is_inter,
+            "%s frame %d: tile %zu names block %d, not a parallel inter block", name, k, i, bi);
+      ++tiles_of[bi];
+      const BlockRec& b = B[bi];
+      const bool masked = b.compound && b.mask_kind;
+      const bool full = b.interintra || (b.mask_kind == 2 && b.plane > 0 && b.mask_role != 2);
+      const int group = i < ns ? 0 : (i < ns + nl ? 1 : (i < T.size() - nc ? 2 : 3));
+      const int want = full ? 2 : (b.mask_role == 2 ? 3 : (masked ? 1 : 0));
+      CHECK(group == want, "%s frame %d: tile %zu (block %d) in group %d, not %d", name, k, i, bi, group,
+            want);
+      if (b.mask_role) {
+        CHECK(b.mask_off >= 0 && b.mask_w > 0 && static_cast<size_t>(b.mask_off) + static_cast<size_t>(b.mask_w) *
+                                                           (b.mask_role == 1 ? b.h : (b.h << c.L.ss_y)) <=
+                                                       P.mask_pool,
+              "%s frame %d: block %d's mask lies outside the %zu-byte pool", name, k, bi, P.mask_pool);
+      }
+    }
+    for (size_t bi = 0; bi < B.size(); ++bi) {
+      const BlockRec& b = B[bi];
+      if (b.phase_b || !b.is_inter) continue;
+      const size_t want = static_cast<size_t>((b.w + 15) / 16) * ((b.h + 7) / 8);
+      CHECK(tiles_of[bi] == want, "%s frame %d: block %zu has %zu tiles, not %zu", name, k, bi, tiles_of[bi],
+            want);
+    }
+    /* the luma masks do not overlap in the pool */
+    std::vector<std::pair<int, int>> spans;
+    for (const BlockRec& b : B)
+      if (b.mask_role == 1) spans.emplace_back(b.mask_off, b.mask_off + b.mask_w * b.h);
+    std::sort(spans.begin(), spans.end());
+    for (size_t i = 1; i < spans.size(); ++i)
+      CHECK(spans[i - 1].second <= spans[i].first, "%s frame %d: two luma masks overlap in the pool", name, k);
     h = 1469598103934665603ull;
     h = hash_list(h, lists.blocks);
     h = hash_list(h, lists.txs);
@@ -143,8 +185,9 @@ uint64_t plan_and_check(av1b_decoder* d, WorkPool* pool, uint8_t* blob, size_t l
     h = hash_list(h, lists.itx_jobs);
     h = hash_list(h, lists.itx_batches);
     h = hash_list(h, lists.inter_tiles);
-    std::printf("%s frame %d: %zu blocks, %zu phase B in %zu chains, depth %d\n", name, k, B.size(),
-                U.size(), P.n_chains, P.unit_depth);
+    std::printf("%s frame %d: %zu blocks, %zu phase B in %zu chains, depth %d; tiles %zu lean, %zu lean "
+                "masked, %zu full, %zu reading a luma mask\n",
+                name, k, B.size(), U.size(), P.n_chains, P.unit_depth, ns, nl, T.size() - ns - nl - nc, nc);
   }();
   return h;
 }

@@ -77,7 +77,7 @@ def solo(av1b):
     return out
 
 
-def run_batched(av1b, solo, config=None, fuse=False, graph=True):
+def run_batched(av1b, solo, config=None, fuse=False, graph=True, share_masks=True):
     import torch
     rt = _Rt()
     spec = streams_spec(av1b)
@@ -90,6 +90,8 @@ def run_batched(av1b, solo, config=None, fuse=False, graph=True):
     c.use_graph = 1 if graph else 0
     batch.set_config(c)
     decs = [av1b.Decoder(0) for _ in spec]
+    for d in decs:
+        d.set_shared_masks(share_masks)
     rings = [[d.reserve_reference() for _ in range(4)] for d in decs]
     nv_bufs = []
     for prm in spec:
@@ -135,6 +137,13 @@ def test_batched_step_matches_solo(av1b, solo):
 def test_batched_step_without_graph_and_with_grain_in_pack(av1b, solo):
     run_batched(av1b, solo, fuse=True, graph=False)
     run_batched(av1b, solo, fuse=True, graph=True)
+
+
+def test_batched_step_with_chroma_masks_predicted(av1b, solo):
+    """Chroma blocks of difference-weighted compounds predicting the luma they
+    cover (the full kernel's stage) instead of reading their luma block's
+    mask: the same frames as the solo decodes, which read the masks."""
+    run_batched(av1b, solo, share_masks=False)
 
 
 def test_batched_step_launch_shapes(av1b, solo):

@@ -108,6 +108,18 @@ def test_config_parity_reduced(av1b, oracle, dec, config, scale, frames):
         dec.release_reference(s)
 
 
+def test_masks_predicted_or_shared(av1b, oracle):
+    """Chroma blocks of difference-weighted compounds: reading the luma
+    block's mask (the default) and predicting the luma they cover in the full
+    kernel (sharing off) both match the oracle."""
+    params, n = stage_cases(av1b)['inter_tools_10bit']
+    for share in (False, True):
+        d = av1b.Decoder(0)
+        d.set_shared_masks(share)
+        run_pair(av1b, oracle, d, params, n, seed=77, check_outputs=False)
+        d.close()
+
+
 def test_golden_hashes(av1b, dec):
     """Against the committed fixtures: works without the oracle build."""
     for case in golden_util.load():

@@ -3,9 +3,12 @@ plan_invariants.cu compiles the planner with plain host allocations and checks,
 on seeded frames of five geometries, that every phase B block's dependencies
 lie earlier in its own chain or in a chain claimed before it - the property
 that lets the device's warps finish without a cooperative launch - and that
-the records do not depend on the number of host threads. A second build with
-the chain admission check removed from a copy of the planner must fail the
-same checks."""
+the records do not depend on the number of host threads, and that the
+prediction tiles are grouped for the kernels that take them (the lean
+kernel's unmasked and masked builds, the full kernel, the chroma tiles that
+read a luma mask last) with every luma mask inside the frame's mask pool.
+Builds with the chain admission check, or the tile grouping, broken in a copy
+of the planner must fail the same checks."""
 import os
 import shutil
 import subprocess
@@ -57,3 +60,16 @@ def test_checker_catches_an_unchecked_chain_admission(tmp_path, have_nvcc):
     r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
     assert r.returncode != 0
     assert 'waits for' in r.stdout
+
+
+def test_checker_catches_a_misgrouped_tile(tmp_path, have_nvcc):
+    src = open(os.path.join(CSRC, 'decoder.cu')).read()
+    grouping = '(r.mask_kind ? O->inter_tiles_mask : O->inter_tiles)'
+    assert src.count(grouping) == 1
+    bad = tmp_path / 'bad'
+    bad.mkdir()
+    (bad / 'decoder.cu').write_text(src.replace(grouping, 'O->inter_tiles'))
+    exe = build_checker(tmp_path, str(bad), 'plan_invariants_badtiles')
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    assert r.returncode != 0
+    assert 'in group 0, not 1' in r.stdout
