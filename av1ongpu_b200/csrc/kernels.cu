@@ -1284,6 +1284,76 @@ __global__ void __launch_bounds__(64) k_upscale(const px_t* __restrict__ src, px
 #define AV1B_LR_AR (AV1B_LR_MAXR + 2)
 #define AV1B_LR_AC (AV1B_LR_TW + 2)
 
+/* A and B of one self-guided box position (i, j) from its box sums `sq`
+ * (squares) and `sb` (samples). */
+__device__ __forceinline__ void sgr_ab(unsigned sq, int sb, int bd, int n, long long mtable, int one_over_n,
+                                       const short* xbyx1, int* a_out, int* b_out) {
+  const long long sa = rnd2llz(static_cast<long long>(sq), 2 * (bd - 8));
+  const long long sbs = rnd2z(sb, bd - 8);
+  long long pv = sa * n - sbs * sbs;
+  if (pv < 0) pv = 0;
+  const int z = rnd2ll(pv * mtable, 20);
+  const int a2 = xbyx1[mini(z, 255)];
+  const long long b2 = (long long)(256 - a2) * sb * one_over_n;
+  *a_out = a2;
+  *b_out = rnd2ll(b2, 12);
+}
+
+/* The box sums of a self-guided pass of radius RAD, register blocked: a
+ * thread takes one column and LR_G box positions STEP rows apart (the first
+ * pass of radius 2 keeps every other row, the second of radius 1 every row),
+ * sums each window row it needs across the box once, and adds those row sums
+ * down each box - (2 RAD + 1) (STEP (LR_G - 1) + 2 RAD + 1) loads for LR_G
+ * positions instead of (2 RAD + 1)^2 each. Positions i = first, first + STEP,
+ * ... below `ar` and columns below `ac`; window rows below `wr` are read. */
+#define AV1B_LR_G 4
+template <int RAD, int STEP>
+__device__ __forceinline__ void sgr_box_pass(const int* win, int* a_out, int* b_out, int first, int ar,
+                                             int ac, int wr, int bd, int n, long long mtable,
+                                             int one_over_n, const short* xbyx1) {
+  constexpr int NR = STEP * (AV1B_LR_G - 1) + 2 * RAD + 1;
+  const int rows = ar > first ? (ar - first + STEP - 1) / STEP : 0;
+  const int groups = (rows + AV1B_LR_G - 1) / AV1B_LR_G;
+  for (int it = threadIdx.x; it < groups * ac; it += blockDim.x) {
+    const int g = it / ac, j = it - g * ac;
+    const int i0 = first + g * AV1B_LR_G * STEP;
+    int hs[NR];
+    unsigned hq[NR];
+#pragma unroll
+    for (int t = 0; t < NR; ++t) {
+      const int row = i0 + 2 - RAD + t;
+      int sum = 0;
+      unsigned sq = 0;
+      if (row < wr) {
+        const int* w = win + row * AV1B_LR_WC + j + 2 - RAD;
+#pragma unroll
+        for (int dx = 0; dx <= 2 * RAD; ++dx) {
+          const int c = w[dx];
+          sum += c;
+          sq += static_cast<unsigned>(c * c);
+        }
+      }
+      hs[t] = sum;
+      hq[t] = sq;
+    }
+#pragma unroll
+    for (int k = 0; k < AV1B_LR_G; ++k) {
+      const int i = i0 + k * STEP;
+      if (i < ar) {
+        int sb = 0;
+        unsigned sq = 0;   /* at most 25 * 4095^2 */
+#pragma unroll
+        for (int t = 0; t <= 2 * RAD; ++t) {
+          sb += hs[k * STEP + t];
+          sq += hq[k * STEP + t];
+        }
+        sgr_ab(sq, sb, bd, n, mtable, one_over_n, xbyx1, a_out + i * AV1B_LR_AC + j,
+               b_out + i * AV1B_LR_AC + j);
+      }
+    }
+  }
+}
+
 /* Shared memory of one loop restoration tile. */
 struct LrSmem {
   int win[AV1B_LR_WR * AV1B_LR_WC];
@@ -1397,6 +1467,15 @@ __device__ __forceinline__ void lr_tile_item(const px_t* __restrict__ cdef,
     const long long n2e = (long long)n * n * u.e[pass];
     const long long mtable = ((1LL << 20) + n2e / 2) / n2e;
     const int one_over_n = ((1 << 12) + (n / 2)) / n;
+    /* the first pass keeps the odd rows of the picture only */
+    if (pass == 0 && rad == 2) {
+      sgr_box_pass<2, 2>(win, aux[0][0], aux[0][1], y0 & 1, ar, ac, wr, bd, n, mtable, one_over_n, xbyx1);
+      continue;
+    }
+    if (pass == 1 && rad == 1) {
+      sgr_box_pass<1, 1>(win, aux[1][0], aux[1][1], 0, ar, ac, wr, bd, n, mtable, one_over_n, xbyx1);
+      continue;
+    }
     for (StepWalk wk(threadIdx.x, blockDim.x, ac); wk.k < ar * ac; wk.next()) {
       const int i = wk.r, j = wk.q;
       /* the first pass reads odd rows only */
@@ -1411,16 +1490,8 @@ __device__ __forceinline__ void lr_tile_item(const px_t* __restrict__ cdef,
           sb += c;
         }
       }
-      const int b_sum = sb;
-      const long long sa = rnd2llz(static_cast<long long>(sq), 2 * (bd - 8));
-      const long long sbs = rnd2z(sb, bd - 8);
-      long long pv = sa * n - sbs * sbs;
-      if (pv < 0) pv = 0;
-      const int z = rnd2ll(pv * mtable, 20);
-      const int a2 = xbyx1[mini(z, 255)];
-      const long long b2 = (long long)(256 - a2) * b_sum * one_over_n;
-      aux[pass][0][i * AV1B_LR_AC + j] = a2;
-      aux[pass][1][i * AV1B_LR_AC + j] = rnd2ll(b2, 12);
+      sgr_ab(sq, sb, bd, n, mtable, one_over_n, xbyx1, &aux[pass][0][i * AV1B_LR_AC + j],
+             &aux[pass][1][i * AV1B_LR_AC + j]);
     }
   }
   __syncthreads();
