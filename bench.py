@@ -248,8 +248,9 @@ def run_reference(args):
 # Counted integer operations per unit of work, one per add, subtract, shift,
 # logic op, compare, min / max and multiply-add (the hardware issues a
 # multiply-add as one instruction), from the stage's arithmetic (the
-# reference's loops, av1gpu_kernels.h); the derivations are in DESIGN.md
-# ("Operation counts"). Units: `ref` a predicted sample per reference,
+# reference's loops, av1gpu_kernels.h): each figure is the sum of the
+# operations one unit of the stage's loop body performs. Units: `ref` a
+# predicted sample per reference,
 # `tx` a transform sample, `unit` a phase B sample, `coded` / `display` a
 # picture sample, `nv12` a display sample.
 OPS = {
