@@ -1065,6 +1065,15 @@ __device__ __forceinline__ int cdef_cst(int diff, int th, int sh) {
   return diff < 0 ? -v : v;
 }
 
+/* The same with the hardware's three-input and add-min-relu integer
+ * instructions (max(min(th - s, m), 0) is the clamp of th - s to [0, m] for
+ * m >= 0). */
+__device__ __forceinline__ int cdef_cst3(int diff, int th, int sh) {
+  const int m = absi(diff);
+  const int v = __viaddmin_s32_relu(th, -(m >> sh), m);
+  return diff < 0 ? -v : v;
+}
+
 template <bool EDGE>
 __device__ __forceinline__ void cdef_samples(const int* win, px_t* d, int stride, int w, int h,
                                              int hl, int x0, int y0, int pw, int ph,
@@ -1076,6 +1085,21 @@ __device__ __forceinline__ void cdef_samples(const int* win, px_t* d, int stride
     if (EDGE && (y0 + i >= ph || x0 + j >= pw)) continue;
     const int x = win[(i + 2) * 12 + j + 2];
     int sum = 0, lo = x, hi = x;
+    if (!EDGE) {
+      /* every tap lies in the plane: both taps of a direction at once */
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        const int tap = q == 0 ? pt0 : (q == 1 ? pt1 : (q & 1 ? 1 : 2));
+        const int th = q < 2 ? pri : sec, sh = q < 2 ? psh : ssh;
+        const int o = oy[q] * 12 + ox[q];
+        const int va = win[(i + 2) * 12 + j + 2 - o], vb = win[(i + 2) * 12 + j + 2 + o];
+        if (th) sum += tap * (cdef_cst3(va - x, th, sh) + cdef_cst3(vb - x, th, sh));
+        lo = __vimin3_s32(lo, va, vb);
+        hi = __vimax3_s32(hi, va, vb);
+      }
+      d[i * stride + j] = (px_t)clampi(clampi(x + ((8 + sum - (sum < 0)) >> 4), lo, hi), 0, maxv);
+      continue;
+    }
 #pragma unroll
     for (int q = 0; q < 6; ++q) {
       const int tap = q == 0 ? pt0 : (q == 1 ? pt1 : (q & 1 ? 1 : 2));
