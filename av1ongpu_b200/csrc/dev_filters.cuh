@@ -32,6 +32,29 @@ struct DeblockRec {
 AV1B_DEV int f4clamp(int v, int bd) { return clampi(v, -(1 << (bd - 1)), (1 << (bd - 1)) - 1); }
 
 /* One sample position of an edge; `b` points at p1. */
+/* The wide filters (6-tap chroma, 8-tap and 16-tap luma): `N` samples each
+ * side written, taps of weight 2 within `N2` of the centre, a 2^LOG2N sum.
+ * One build per filter, so the sample and output arrays stay in registers. */
+template <int N, int N2, int LOG2N>
+AV1B_DEV void deblock_wide(px_t* b, int s, int maxv) {
+  int v[2 * N + 2];
+#pragma unroll
+  for (int k = -(N + 1); k <= N; ++k) v[k + N + 1] = b[(2 + k) * s];
+  int out[2 * N];
+#pragma unroll
+  for (int i = -N; i < N; ++i) {
+    int t = 0;
+#pragma unroll
+    for (int j = -N; j <= N; ++j) {
+      const int tap = clampi(i + j, -(N + 1), N);
+      t += v[tap + N + 1] * (absi(j) <= N2 ? 2 : 1);
+    }
+    out[i + N] = rnd2(t, LOG2N);
+  }
+#pragma unroll
+  for (int i = -N; i < N; ++i) b[(2 + i) * s] = (px_t)clampi(out[i + N], 0, maxv);
+}
+
 AV1B_DEV void deblock_px(px_t* b, int s, int level, int sharpness, int filter_size, int chroma,
                          int bd, int maxv) {
   if (level == 0) return;
@@ -86,21 +109,11 @@ AV1B_DEV void deblock_px(px_t* b, int s, int level, int sharpness, int filter_si
     }
     return;
   }
+  /* log2n 4: n 6, n2 1; log2n 3: n 2, n2 1 (chroma) or n 3, n2 0 (luma) */
   const int log2n = (filter_size == 8 || !flat2) ? 3 : 4;
-  const int n = log2n == 4 ? 6 : (chroma ? 2 : 3);
-  const int n2 = (log2n == 3 && !chroma) ? 0 : 1;
-  int v[14];
-  for (int k = -(n + 1); k <= n; ++k) v[k + 7] = b[(2 + k) * s];
-  int out[12];
-  for (int i = -n; i < n; ++i) {
-    int t = 0;
-    for (int j = -n; j <= n; ++j) {
-      const int tap = clampi(i + j, -(n + 1), n);
-      t += v[tap + 7] * (absi(j) <= n2 ? 2 : 1);
-    }
-    out[i + n] = rnd2(t, log2n);
-  }
-  for (int i = -n; i < n; ++i) b[(2 + i) * s] = (px_t)clampi(out[i + n], 0, maxv);
+  if (log2n == 4) deblock_wide<6, 1, 4>(b, s, maxv);
+  else if (chroma) deblock_wide<2, 1, 3>(b, s, maxv);
+  else deblock_wide<3, 0, 3>(b, s, maxv);
 }
 
 /* ---- CDEF -------------------------------------------------------------------- */
