@@ -235,7 +235,7 @@ __global__ void __launch_bounds__(64) kb_upscale(const StreamStep* __restrict__ 
   }
 }
 
-__global__ void __launch_bounds__(256) kb_lr(const StreamStep* __restrict__ st,
+__global__ void __launch_bounds__(256, 4) kb_lr(const StreamStep* __restrict__ st,
                                              const BatchHeader* __restrict__ h) {
   __shared__ LrSmem sm;
   const int* pfx = h->pfx[kBLr];

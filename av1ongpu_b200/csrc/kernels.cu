@@ -1484,6 +1484,9 @@ __device__ __forceinline__ void lr_tile_item(const px_t* __restrict__ cdef,
     xbyx1[z] = static_cast<short>(z >= 255 ? 256 : (z == 0 ? 1 : ((z << 8) + (z / 2)) / (z + 1)));
   __syncthreads();
   const int ar = th + 2, ac = tw + 2;
+  /* unrolled: the unit record stays in registers (indexed by a loop
+   * variable it would live in local memory) */
+#pragma unroll
   for (int pass = 0; pass < 2; ++pass) {
     const int rad = u.r[pass];
     if (rad == 0) continue;
@@ -1525,6 +1528,7 @@ __device__ __forceinline__ void lr_tile_item(const px_t* __restrict__ cdef,
     const int y = y0 + i;
     const int v = win[(i + 3) * AV1B_LR_WC + j + 3];
     int flt[2] = {0, 0};
+#pragma unroll
     for (int pass = 0; pass < 2; ++pass) {
       if (u.r[pass] == 0) continue;
       int a = 0, b = 0;
