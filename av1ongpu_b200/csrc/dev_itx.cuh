@@ -416,8 +416,24 @@ AV1B_DEV void itx_row(const ItxParams& p, const int* __restrict__ coef, int y, i
     for (int j = 0; j < W; ++j) tmp[y * W + j] = 0;
     return;
   }
+  const int* row = coef + y * CS;
+  if ((reinterpret_cast<uintptr_t>(row) & 15) == 0) {
+    /* a 16-byte aligned row (every row of a raster that starts aligned):
+     * four coefficients a load */
 #pragma unroll
-  for (int j = 0; j < W; ++j) t[j] = j < CS ? coef[y * CS + j] : 0;
+    for (int j = 0; j < CS; j += 4) {
+      const int4 v = *reinterpret_cast<const int4*>(row + j);
+      t[j] = v.x;
+      t[j + 1] = v.y;
+      t[j + 2] = v.z;
+      t[j + 3] = v.w;
+    }
+#pragma unroll
+    for (int j = CS; j < W; ++j) t[j] = 0;
+  } else {
+#pragma unroll
+    for (int j = 0; j < W; ++j) t[j] = j < CS ? row[j] : 0;
+  }
   if (absi(LW - p.lh) == 1) {
 #pragma unroll
     for (int j = 0; j < W; ++j) t[j] = rnd2ll((long long)t[j] * 2896, 12);
