@@ -212,7 +212,7 @@ __global__ void __launch_bounds__(128) kb_cdef(const StreamStep* __restrict__ st
 }
 
 /* Superres: a stream's items are its first pass's CTAs, then its second's. */
-__global__ void __launch_bounds__(64) kb_upscale(const StreamStep* __restrict__ st,
+__global__ void __launch_bounds__(128) kb_upscale(const StreamStep* __restrict__ st,
                                                  const BatchHeader* __restrict__ h) {
   __shared__ __align__(16) short taps[512];
   __shared__ px_t span[AV1B_UP_SPAN];
@@ -385,7 +385,7 @@ cudaError_t launch_batch_step(const StreamStep* steps, BatchHeader* hdr, const B
   mark(kBCopyPost);
   kb_copy<<<batch_grid(t, kBCopyPost, n_sm), 256, 0, s>>>(steps, hdr, 1);
   mark(kBUpscale);
-  kb_upscale<<<batch_grid(t, kBUpscale, n_sm), 64, 0, s>>>(steps, hdr);
+  kb_upscale<<<batch_grid(t, kBUpscale, n_sm), 128, 0, s>>>(steps, hdr);
   mark(kBLr);
   kb_lr<<<batch_grid(t, kBLr, n_sm), 256, 0, s>>>(steps, hdr);
   mark(kBCopyRef);
@@ -451,7 +451,7 @@ int batch_stage_max_ctas(int stage) {
     case kBCopySnap: case kBCopyPost: case kBCopyRef: k = reinterpret_cast<const void*>(kb_copy); threads = 256; break;
     case kBCdefSearch: k = reinterpret_cast<const void*>(kb_cdef_search); break;
     case kBCdef: k = reinterpret_cast<const void*>(kb_cdef); break;
-    case kBUpscale: k = reinterpret_cast<const void*>(kb_upscale); threads = 64; break;
+    case kBUpscale: k = reinterpret_cast<const void*>(kb_upscale); threads = 128; break;
     case kBLr: k = reinterpret_cast<const void*>(kb_lr); threads = 256; break;
     case kBGrainTemplate: k = reinterpret_cast<const void*>(kb_grain_template); threads = 256; break;
     case kBGrain: k = reinterpret_cast<const void*>(kb_grain_blend); break;

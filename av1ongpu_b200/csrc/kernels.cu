@@ -1198,9 +1198,11 @@ __global__ void __launch_bounds__(128) k_cdef(const px_t* __restrict__ src, px_t
 }
 
 /* ---- superres ------------------------------------------------------------------------- */
-/* One CTA of 64 threads per 256 output samples of a row, a thread per 4.
- * The source span those outputs read (a superres step is at most one source
- * sample, so at most 256 + 8 samples) is staged in shared memory once, with
+/* One CTA of 128 threads per 512 output samples of a row, a thread per 4
+ * (CTAs of half that, 64 threads, took 11 % longer: twice the CTAs,
+ * each staging the taps and its span). The source span those outputs read (a
+ * superres step is at most one source sample, so at most 512 + 8 samples) is
+ * staged in shared memory once, with
  * the clamp to the coded row applied while staging, and the 8-tap phases
  * beside it; each output then reads its taps there. Grid rows: the luma
  * rows, then the chroma rows with plane 1's segments and plane 2's side by
@@ -1208,7 +1210,7 @@ __global__ void __launch_bounds__(128) k_cdef(const px_t* __restrict__ src, px_t
  * boundary (the rows the restoration reads from the pre-CDEF picture,
  * av1gpu_kernels.h:2832-2845); the reference upscales the whole pre-CDEF
  * picture and reads only these. */
-#define AV1B_UP_SPAN 288
+#define AV1B_UP_SPAN 544
 /* One CTA item (segment xb of grid row yb): the caller has filled `taps`
  * (the 64 filter phases); the body stages the source span, meets the CTA
  * barrier and writes. Early returns are either uniform over the CTA or after
@@ -1281,7 +1283,7 @@ __device__ __forceinline__ void upscale_item(const px_t* __restrict__ src, px_t*
   }
 }
 
-__global__ void __launch_bounds__(64) k_upscale(const px_t* __restrict__ src, px_t* dst,
+__global__ void __launch_bounds__(128) k_upscale(const px_t* __restrict__ src, px_t* dst,
                                                 const __grid_constant__ Layout L,
                                                 const __grid_constant__ UpscaleArgs u, int maxv,
                                                 int border_rows, int rows0) {
@@ -2203,7 +2205,7 @@ cudaError_t launch_upscale(const px_t* src, px_t* dst, const Layout& L, int maxv
   const int rows0 = border_rows ? 4 * ((L.p[0].out_h + 8) / 64 + 1) : L.p[0].out_h;
   const int rows1 = L.p[1].out_h > 0 ? (border_rows ? rows0 : L.p[1].out_h) : 0;
   const int segs = maxi(cdiv(L.p[0].out_w, AV1B_UP_OUT), 2 * cdiv(L.p[1].out_w, AV1B_UP_OUT));
-  k_upscale<<<dim3(segs, rows0 + rows1), 64, 0, s>>>(src, dst, L, u, maxv, border_rows ? 1 : 0, rows0);
+  k_upscale<<<dim3(segs, rows0 + rows1), 128, 0, s>>>(src, dst, L, u, maxv, border_rows ? 1 : 0, rows0);
   return cudaGetLastError();
 }
 

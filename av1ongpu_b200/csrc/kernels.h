@@ -32,7 +32,7 @@ namespace av1b {
 #define AV1B_UNIT_SCRATCH 4096
 /* superres: output samples of a row a CTA writes; loop restoration: the
  * columns of a tile */
-#define AV1B_UP_OUT 256
+#define AV1B_UP_OUT 512
 #define AV1B_LR_TW 32
 #define AV1B_UNIT_CTAS_PER_SM 2
 /* deblocking: the edge records a warp takes at once in the batched form and
