@@ -120,7 +120,9 @@ def config_dict(w, h, cw, frames, world):
 
 
 class ClockSampler:
-    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+    """Samples nvidia-smi clocks and throttle reasons every 100 ms. Started
+    before the warm-up (nvidia-smi takes a moment to begin), it keeps only the
+    samples taken between begin() and stop(): the timed region."""
     FIELDS = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
               'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
               'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
@@ -129,12 +131,13 @@ class ClockSampler:
         self.device = device
         self.proc = None
         self.lines = []
+        self.t0 = None
 
     def start(self):
         try:
             self.proc = subprocess.Popen(
                 ['nvidia-smi', '-i', str(self.device), '--query-gpu=' + self.FIELDS,
-                 '--format=csv,noheader,nounits', '-lms', '200'],
+                 '--format=csv,noheader,nounits', '-lms', '100'],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -143,9 +146,13 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.monotonic(), line.strip()))
+
+    def begin(self):
+        self.t0 = time.monotonic()
 
     def stop(self):
+        t1 = time.monotonic()
         if not self.proc:
             return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['nvidia-smi unavailable']}
         self.proc.terminate()
@@ -155,7 +162,10 @@ class ClockSampler:
             self.proc.kill()
         sm, smax, reasons = [], [], set()
         names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
-        for ln in self.lines:
+        t0 = self.t0 if self.t0 is not None else 0.0
+        for ts, ln in self.lines:
+            if ts < t0 or ts > t1:
+                continue
             f = [x.strip() for x in ln.split(',')]
             if len(f) < 9:
                 continue
@@ -466,6 +476,8 @@ def run_ours(args):
             dec.decode_planned(pl, slot=s, keep=True, wait=False)
             dec.to_nv12_device(s, PITCH, nv12_dev.data_ptr(), geo['nv12'])
 
+    clocks = ClockSampler(local)
+    clocks.start()
     for _ in range(args.warmup):
         device_step()
     dec.sync()
@@ -474,10 +486,9 @@ def run_ours(args):
         if dist is not None:
             dist.barrier()
 
-    clocks = ClockSampler(local)
     barrier()
     torch.cuda.synchronize()
-    clocks.start()
+    clocks.begin()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)

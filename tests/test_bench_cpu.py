@@ -91,3 +91,32 @@ def test_reference_arm_runs_on_rank_zero_only():
                        capture_output=True, text=True, cwd=ROOT, env=env, timeout=120)
     assert r.returncode == 0, r.stderr[-2000:]
     assert r.stdout.strip() == ''
+
+
+def test_clock_samples_only_from_the_timed_region():
+    """Clock samples taken before begin() (during warm-up) or after stop() do
+    not count; throttle reasons are read from the timed region's samples."""
+    import statistics
+    import time
+    import bench
+
+    class _Proc:
+        def terminate(self):
+            pass
+
+        def wait(self, timeout=None):
+            return 0
+
+    c = bench.ClockSampler(0)
+    c.proc = _Proc()
+    now = time.monotonic()
+    row = '0, {sm}, 1965, 700, 0x0, Not Active, Not Active, Not Active, {cap}'
+    c.lines = [(now - 10.0, row.format(sm=900, cap='Active')),      # warm-up
+               (now - 0.02, row.format(sm=1965, cap='Not Active')),
+               (now - 0.01, row.format(sm=1950, cap='Not Active')),
+               (now + 60.0, row.format(sm=800, cap='Active'))]       # after the region
+    c.t0 = now - 1.0
+    out = c.stop()
+    assert out['samples'] == 2
+    assert out['sm_mhz'] == statistics.median([1965.0, 1950.0])
+    assert out['reasons'] == []
