@@ -45,8 +45,10 @@ frames, one key and 29 inter, from files a separate process wrote, so the
 timing process maps only the reference's library.
 """
 import argparse
+import datetime
 import json
 import os
+import shutil
 import statistics
 import subprocess
 import sys
@@ -122,23 +124,28 @@ def config_dict(w, h, cw, frames, world):
 class ClockSampler:
     """Samples nvidia-smi clocks and throttle reasons every 100 ms. Started
     before the warm-up (nvidia-smi takes a moment to begin), it keeps only the
-    samples taken between begin() and stop(): the timed region."""
-    FIELDS = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+    samples whose own timestamps lie between begin() and stop(): the timed
+    region (nvidia-smi's output to a pipe may arrive in bursts, so the time a
+    line is read says nothing about when it was sampled)."""
+    FIELDS = ('timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
               'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
               'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
 
     def __init__(self, device):
         self.device = device
         self.proc = None
+        self.t = None
         self.lines = []
         self.t0 = None
 
     def start(self):
+        cmd = ['nvidia-smi', '-i', str(self.device), '--query-gpu=' + self.FIELDS,
+               '--format=csv,noheader,nounits', '-lms', '100']
+        if shutil.which('stdbuf'):
+            cmd = ['stdbuf', '-oL'] + cmd   # a line at a time, not in blocks
         try:
-            self.proc = subprocess.Popen(
-                ['nvidia-smi', '-i', str(self.device), '--query-gpu=' + self.FIELDS,
-                 '--format=csv,noheader,nounits', '-lms', '100'],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                                         text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
         except OSError:
@@ -146,13 +153,22 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append((time.monotonic(), line.strip()))
+            self.lines.append(line.strip())
 
     def begin(self):
-        self.t0 = time.monotonic()
+        self.t0 = time.time()
+
+    @staticmethod
+    def sample_time(field):
+        """nvidia-smi's timestamp (local time, 'YYYY/MM/DD HH:MM:SS.fff') as
+        seconds since the epoch, or None."""
+        try:
+            return datetime.datetime.strptime(field, '%Y/%m/%d %H:%M:%S.%f').timestamp()
+        except ValueError:
+            return None
 
     def stop(self):
-        t1 = time.monotonic()
+        t1 = time.time()
         if not self.proc:
             return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['nvidia-smi unavailable']}
         self.proc.terminate()
@@ -160,21 +176,27 @@ class ClockSampler:
             self.proc.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
+        if self.t is not None:
+            self.t.join(timeout=2)
+        return self.summarize(self.lines, self.t0 if self.t0 is not None else 0.0, t1)
+
+    @classmethod
+    def summarize(cls, lines, t0, t1):
         sm, smax, reasons = [], [], set()
         names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
-        t0 = self.t0 if self.t0 is not None else 0.0
-        for ts, ln in self.lines:
-            if ts < t0 or ts > t1:
-                continue
+        for ln in lines:
             f = [x.strip() for x in ln.split(',')]
-            if len(f) < 9:
+            if len(f) < 10:
+                continue
+            ts = cls.sample_time(f[0])
+            if ts is None or ts < t0 or ts > t1:
                 continue
             try:
-                sm.append(float(f[1]))
-                smax.append(float(f[2]))
+                sm.append(float(f[2]))
+                smax.append(float(f[3]))
             except ValueError:
                 continue
-            for n, v in zip(names, f[5:9]):
+            for n, v in zip(names, f[6:10]):
                 if v.lower().startswith('active'):
                     reasons.add(n)
         return {'sm_mhz': statistics.median(sm) if sm else None,

@@ -94,29 +94,25 @@ def test_reference_arm_runs_on_rank_zero_only():
 
 
 def test_clock_samples_only_from_the_timed_region():
-    """Clock samples taken before begin() (during warm-up) or after stop() do
-    not count; throttle reasons are read from the timed region's samples."""
+    """Clock samples whose own timestamps fall before begin() (the warm-up)
+    or after stop() do not count, whenever their lines were read; throttle
+    reasons come from the timed region's samples only."""
+    import datetime
     import statistics
-    import time
     import bench
 
-    class _Proc:
-        def terminate(self):
-            pass
+    def row(t, sm, cap):
+        stamp = datetime.datetime.fromtimestamp(t).strftime('%Y/%m/%d %H:%M:%S.%f')[:-3]
+        return '%s, 0, %d, 1965, 700, 0x0, Not Active, Not Active, Not Active, %s' % (stamp, sm, cap)
 
-        def wait(self, timeout=None):
-            return 0
-
-    c = bench.ClockSampler(0)
-    c.proc = _Proc()
-    now = time.monotonic()
-    row = '0, {sm}, 1965, 700, 0x0, Not Active, Not Active, Not Active, {cap}'
-    c.lines = [(now - 10.0, row.format(sm=900, cap='Active')),      # warm-up
-               (now - 0.02, row.format(sm=1965, cap='Not Active')),
-               (now - 0.01, row.format(sm=1950, cap='Not Active')),
-               (now + 60.0, row.format(sm=800, cap='Active'))]       # after the region
-    c.t0 = now - 1.0
-    out = c.stop()
+    t0 = 1_800_000_000.0
+    lines = [row(t0 - 5.0, 900, 'Active'),        # warm-up
+             row(t0 + 0.2, 1965, 'Not Active'),
+             row(t0 + 0.3, 1950, 'Not Active'),
+             row(t0 + 9.0, 800, 'Active'),         # after the region
+             'garbage line']
+    out = bench.ClockSampler.summarize(lines, t0, t0 + 1.0)
     assert out['samples'] == 2
     assert out['sm_mhz'] == statistics.median([1965.0, 1950.0])
     assert out['reasons'] == []
+    assert bench.ClockSampler.summarize(lines, t0 - 6.0, t0 + 1.0)['reasons'] == ['sw_power_cap']
