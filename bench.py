@@ -71,8 +71,8 @@ CONFIG = 3
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
-    ap.add_argument('--steps', type=int, default=2)
-    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--steps', type=int, default=20)
+    ap.add_argument('--warmup', type=int, default=5)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--scale', type=int, default=1, help='divide the picture size (tests only)')
     ap.add_argument('--frames', type=int, default=GOP, help='frames per step')
