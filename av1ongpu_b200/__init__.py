@@ -77,7 +77,7 @@ class BatchConfig(ctypes.Structure):
                 ('inter_variant', ctypes.c_int32)]
 
     def as_dict(self):
-        return {'ctas_per_sm': list(self.ctas_per_sm)[:21], 'claim_chunk': self.claim_chunk,
+        return {'ctas_per_sm': list(self.ctas_per_sm)[:len(Batch.STAGES)], 'claim_chunk': self.claim_chunk,
                 'fuse_grain_nv12': self.fuse_grain_nv12, 'use_graph': self.use_graph,
                 'inter_variant': self.inter_variant}
 

@@ -117,3 +117,13 @@ def test_oracle_matches_golden(oracle, av1b):
     for case in cases[:4]:
         got = golden_util.run_case(oracle.RefDecoder(), case, av1b)
         assert got == case['frames'], case['name']
+
+
+def test_batch_config_lists_every_stage(av1b):
+    """The launch shape's dictionary view has one entry per stage of the
+    batched step, the stages the header counts."""
+    import re
+    header = open(os.path.join(ROOT, 'include', 'av1b.h')).read()
+    n = int(re.search(r'stages in launch order, (\d+) of them', header).group(1))
+    assert len(av1b.Batch.STAGES) == n
+    assert len(av1b.BatchConfig().as_dict()['ctas_per_sm']) == n
