@@ -2383,7 +2383,18 @@ int launch_step_plain(av1b_decoder* d, av1b_plan* pl, StepPrep* sp) {
     if (!any) continue;
     CK(timed(d, kStOwner + stage, [&] { return launch_recon_stage(stage, a, d->n_sm, st); }),
        "reconstruction launch");
-    ++launches;
+    /* the kernels each stage launches (launch_recon_stage): prediction up
+     * to four (the lean kernel's unmasked and masked tiles, the full
+     * kernel's, the chroma tiles reading luma masks), one transform kernel
+     * a size class present, one dependency-scheduled kernel */
+    if (stage == 1) {
+      const int lm_end = a.n_inter_simple + a.n_inter_lmask, cm_first = a.n_inter_tiles - a.n_inter_cmask;
+      launches += (a.n_inter_simple > 0) + (a.n_inter_lmask > 0) + (cm_first > lm_end) + (a.n_inter_cmask > 0);
+    } else if (stage == 2) {
+      for (int c = 2; c <= 7; ++c) launches += a.itx_class_count[c] > 0;
+    } else {
+      ++launches;
+    }
   }
   CK(cudaEventRecord(ev[1], st), "event");
 
@@ -2421,7 +2432,8 @@ int launch_step_plain(av1b_decoder* d, av1b_plan* pl, StepPrep* sp) {
                             static_cast<int>(P.n_cdef_search),
                             static_cast<int*>(d->cdef_search.p), L, st);
        }), "CDEF");
-    ++launches;
+    /* the direction searches, when any record reads them, then the filter */
+    launches += 1 + ((P.cdef_search_any ? P.cdef_grid_n : 0) + static_cast<int>(P.n_cdef_search) > 0);
   }
   px_t* lr_cdef = static_cast<px_t*>(d->lr_cdef.p);
   const px_t* lr_curr = snap;

@@ -492,10 +492,13 @@ def run_ours(args):
 
     nv12_dev = torch.empty(geo['nv12'], dtype=torch.uint8, device='cuda:%d' % local)
 
-    def device_step():
+    def device_step(launch_counts=None):
         for k, pl in enumerate(plans):
             s = ring[k % 4]
             dec.decode_planned(pl, slot=s, keep=True, wait=False)
+            if launch_counts is not None:
+                # the frame's kernels (the decoder counts each launch) and the NV12 pack
+                launch_counts.append(dec.stats().kernel_launches + 1)
             dec.to_nv12_device(s, PITCH, nv12_dev.data_ptr(), geo['nv12'])
 
     clocks = ClockSampler(local)
@@ -523,11 +526,11 @@ def run_ours(args):
     ms = slowest_rank(e0.elapsed_time(e1), dist, 'cuda:%d' % local)
     barrier()
     value = replica_rate(F * args.steps, world, ms / 1e3)
-    launches_per_frame = dec.stats().kernel_launches + 1  # + the NV12 pack
 
     # ---- per-stage device times (a separate profiled pass over the same step) ----------
     dec.set_profiling(True)
-    device_step()
+    step_launches = []
+    device_step(step_launches)
     dec.sync()
     prof = dec.profile()
     dec.set_profiling(False)
@@ -660,7 +663,7 @@ def run_ours(args):
                             '(tests/golden/workloads.json)' if bitexact is not None else
                             'not checked (not the exact workload, or --no-verify)',
             'e2e': e2e, 'roofline': roofline, 'cpu_baseline': base,
-            'clocks': clk, 'gpu_launches': launches_per_frame * F * args.steps,
+            'clocks': clk, 'gpu_launches': sum(step_launches) * args.steps,
             'peaks': {k: v for k, v in pk.items()},
             'stages': stages,
             'batched': batched,
